@@ -1,0 +1,606 @@
+// Test-oracle driver around the reference's own explicit RDS solver.
+//
+// Linked against the reference sources compiled in place (oracle/Makefile). It is our code,
+// written against the reference's public API exactly the way its examples drive it
+// (examples/testcases-rdm/Advection-Continuous-RDS-2D-Explicit.cpp:37-174):
+//   GmshReader -> DofMap::clone_continuous -> PGRDMethodExplicit<MeshConfig, Physics, Scheme>
+//   configure_mesh_data / initialize_work_data / set_vec_function / add_boundary_condition
+//   assemble_lhs_and_rhs(CFL) + solve()                 (src/solver/rdm/PGRDMethodExplicit.hpp:417-477)
+//
+// Two jobs:
+//   dump  -- write golden inputs (mesh arrays, reference-element tables, boundary facets,
+//            initial state) and outputs (nodal residual, wave speed, dt, dual volume, states
+//            after k iterations, residual norms) as raw little-endian arrays + meta.json.
+//   time  -- time K explicit iterations (the CPU baseline), print one JSON line.
+//
+// Usage:
+//   rds_ref_harness dump|time <physics> <scheme> <p> <quad> <mesh.msh> <outdir|-> <iters> <cfl>
+//                   <init> <bcspec> [threads]
+//     physics: advconst (a = (0.5,1)/|(0.5,1)|) | burgers | euler2d | euler3d
+//     scheme : lda | n | b
+//     init   : name of an initial-state function of the node coordinates (see init_state)
+//     bcspec : comma-separated Type:condition_name:boundary:expr, or "none"
+//
+// The only addition to the reference is the constant-direction advection policy below: the
+// reference's ConstAdvection2D is hard-wired to a = (0,1) (physics/scalar/RotationAdvection2D.hpp:17-30),
+// and RotationAdvection2D takes the direction as a template policy, so a new policy class is
+// plugged in without editing the reference.
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "interpolation/FEValues.hpp"
+#include "mesh/io/gmsh/GmshReader.hpp"
+#include "mesh/point_set/StdPointSet.hpp"
+#include "mesh/std_region/StdRegion.hpp"
+#include "physics/euler/Euler2DCons.hpp"
+#include "physics/euler/Euler3DCons.hpp"
+#include "physics/scalar/Burgers2D.hpp"
+#include "physics/scalar/RotationAdvection2D.hpp"
+#include "solver/rdm/PGRDMethodExplicit.hpp"
+#include "solver/rdm/cellsplitters/CellSplitters.hpp"
+
+using namespace pdekit;
+using namespace pdekit::mesh;
+using namespace pdekit::solver;
+
+using vec_fn    = interpolation::VectorMeshFunction<Real>;
+using coord_v   = math::DenseConstVecView<Real>;
+using state_v   = interpolation::VectorMeshFunction<Real>::const_entry_type;
+
+// ----------------------------------------------------------------------------
+// Constant advection direction a = (0.5, 1) / |(0.5, 1)|
+// ----------------------------------------------------------------------------
+
+class ConstDirection2D
+{
+  public:
+  template <typename V1, typename V2>
+  inline static void rotation_vector(const V1 &, V2 &adv_vector)
+  {
+    const Real inv_norm = 1.0 / std::sqrt(0.5 * 0.5 + 1.0 * 1.0);
+    adv_vector[X0]      = 0.5 * inv_norm;
+    adv_vector[X1]      = 1.0 * inv_norm;
+  }
+};
+
+// ----------------------------------------------------------------------------
+// Boundary expressions (our definitions of the configs' inflow data)
+// ----------------------------------------------------------------------------
+
+static Real bc_zero(const coord_v &, const state_v &, const Uint)
+{
+  return 0.0;
+}
+static Real bc_sin2pix(const coord_v &x, const state_v &, const Uint)
+{
+  return std::sin(2.0 * M_PI * x[0]);
+}
+static Real bc_burgers_inlet(const coord_v &x, const state_v &, const Uint)
+{
+  return 1.5 - 2.0 * x[0];
+}
+static Real bc_const_1p5(const coord_v &, const state_v &, const Uint)
+{
+  return 1.5;
+}
+static Real bc_const_m0p5(const coord_v &, const state_v &, const Uint)
+{
+  return -0.5;
+}
+
+using expr_fn = Real (*)(const coord_v &, const state_v &, const Uint);
+
+static expr_fn find_expr(const std::string &name)
+{
+  if (name == "zero")
+    return &bc_zero;
+  if (name == "sin2pix")
+    return &bc_sin2pix;
+  if (name == "burgers_inlet")
+    return &bc_burgers_inlet;
+  if (name == "c1.5")
+    return &bc_const_1p5;
+  if (name == "c-0.5")
+    return &bc_const_m0p5;
+  std::cerr << "unknown expression " << name << std::endl;
+  std::exit(2);
+}
+
+// ----------------------------------------------------------------------------
+// Initial states as functions of physical coordinates (so that a different node numbering
+// of the same mesh reproduces the same state). Each writes NEQ values.
+// ----------------------------------------------------------------------------
+
+static void init_state(const std::string &name, const Real *x, Uint dim, Uint neq, Real *u)
+{
+  if (name == "zero")
+  {
+    for (Uint e = 0; e < neq; ++e)
+      u[e] = 0.0;
+  }
+  else if (name == "smooth")
+  {
+    // scalar: smooth field with both signs and O(1) gradients
+    u[0] = 0.3 * std::sin(3.1 * x[0] + 1.7 * x[1]) + 0.2 * std::cos(5.3 * x[0] * x[1]) +
+           0.1 * x[0] - 0.05;
+  }
+  else if (name == "burgers")
+  {
+    // inflow profile 1.5 - 2x with a smooth perturbation
+    u[0] = 1.5 - 2.0 * x[0] + 0.1 * std::sin(7.0 * x[0] + 3.0 * x[1]) * x[1];
+  }
+  else if (name == "euler2d")
+  {
+    // freestream M = 0.5 along x with a smooth O(1%) perturbation
+    const Real gamma = 1.4, rho = 1.0 + 0.01 * std::sin(4.0 * x[0] + 3.0 * x[1]);
+    const Real p = 1.0 / gamma * (1.0 + 0.01 * std::cos(5.0 * x[0] - 2.0 * x[1]));
+    const Real c = std::sqrt(gamma * p / rho), ux = 0.5 * c, uy = 0.01 * std::sin(6.0 * x[1]);
+    u[0] = rho;
+    u[1] = rho * ux;
+    u[2] = rho * uy;
+    u[3] = p / (gamma - 1.0) + 0.5 * rho * (ux * ux + uy * uy);
+  }
+  else if (name == "euler3d")
+  {
+    const Real gamma = 1.4, rho = 1.0 + 0.01 * std::sin(4.0 * x[0] + 3.0 * x[1] - x[2]);
+    const Real p  = 1.0 / gamma * (1.0 + 0.01 * std::cos(5.0 * x[0] - 2.0 * x[2]));
+    const Real c  = std::sqrt(gamma * p / rho), ux = 0.6 * c;
+    const Real uy = 0.01 * std::sin(6.0 * x[1]), uz = 0.01 * std::cos(5.0 * x[2]);
+    u[0] = rho;
+    u[1] = rho * ux;
+    u[2] = rho * uy;
+    u[3] = rho * uz;
+    u[4] = p / (gamma - 1.0) + 0.5 * rho * (ux * ux + uy * uy + uz * uz);
+  }
+  else
+  {
+    std::cerr << "unknown init " << name << std::endl;
+    std::exit(2);
+  }
+  (void)dim;
+}
+
+// ----------------------------------------------------------------------------
+// Raw array output
+// ----------------------------------------------------------------------------
+
+struct Dumper
+{
+  std::string dir;
+  std::ostringstream manifest;
+  bool first = true;
+
+  template <typename T>
+  void put(const std::string &name, const std::vector<T> &v, const std::vector<Uint> &shape)
+  {
+    const std::string path = dir + "/" + name + (sizeof(T) == 8 ? ".f64" : ".i32");
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char *>(v.data()), v.size() * sizeof(T));
+    manifest << (first ? "" : ",\n") << "  \"" << name << "\": [";
+    for (Uint i = 0; i < shape.size(); ++i)
+      manifest << (i ? ", " : "") << shape[i];
+    manifest << "]";
+    first = false;
+  }
+};
+
+static std::vector<Real> mat_to_vec(const math::DenseDMat<Real> &m)
+{
+  std::vector<Real> v(m.rows() * m.cols());
+  for (Uint r = 0; r < m.rows(); ++r)
+    for (Uint c = 0; c < m.cols(); ++c)
+      v[r * m.cols() + c] = m(r, c);
+  return v;
+}
+
+// ----------------------------------------------------------------------------
+// Probe subclass: the reference keeps the time-update object protected in RDMethod.
+// ----------------------------------------------------------------------------
+
+template <typename MC, typename Phys, typename Scheme>
+class ProbeSolver : public rdm::PGRDMethodExplicit<MC, Phys, Scheme>
+{
+  public:
+  const rdm::RDTimeUpdate &time_update() const
+  {
+    return this->m_rd_time_update;
+  }
+};
+
+struct Args
+{
+  std::string mode, physics, scheme, mesh, outdir, init, bcspec;
+  Uint p = 1, quad = 1, iters = 1, threads = 1;
+  Real cfl = 0.5;
+};
+
+static ElemShape facet_shape_of(ElemShape s)
+{
+  if (s == ElemShape::Triag || s == ElemShape::Quad)
+    return ElemShape::Line;
+  return ElemShape::Triag;
+}
+
+template <typename MC, typename Phys, typename Scheme>
+int run(const Args &a)
+{
+  using MeshType  = Tria<MC>;
+  constexpr Uint D   = MC::GDIM;
+  constexpr Uint NEQ = Phys::NEQ;
+
+  auto mesh = std::make_shared<MeshType>("mesh");
+  gmsh::GmshReader reader;
+  reader.read_mesh_from_file(a.mesh, *mesh, "geo_dofs");
+  auto geo = mesh->dof_storage("geo_dofs");
+  auto sol = mesh->create_dof_storage("sol_dofs");
+  MeshType::dof_storage_type::clone_continuous(*mesh, *geo, *sol, static_cast<PolyOrderID>(a.p),
+                                               PointSetID::Equidist);
+
+  const Uint nsol   = (*sol).nb_nodes();
+  const Uint ncells = (*sol).nb_active_cells();
+
+  auto u   = std::make_shared<vec_fn>("", "solution");
+  auto res = std::make_shared<vec_fn>("", "residual");
+  u->resize(NEQ, nsol);
+  res->resize(NEQ, nsol);
+
+  auto solver = std::make_shared<ProbeSolver<MC, Phys, Scheme>>();
+  solver->configure_mesh_data(mesh, geo, sol);
+  solver->initialize_work_data(SFunc::Lagrange, PointSetID::Gauss, a.quad, a.threads, 100);
+  solver->set_vec_function(SolverVecFn::solution, u);
+  solver->set_vec_function(SolverVecFn::residuals, res);
+
+  // ---- boundary conditions: "Type:cond_name:boundary:expr,..."
+  struct BCDesc
+  {
+    std::string type, name, boundary, expr;
+  };
+  std::vector<BCDesc> bcs;
+  if (a.bcspec != "none")
+  {
+    std::stringstream ss(a.bcspec);
+    std::string item;
+    while (std::getline(ss, item, ','))
+    {
+      BCDesc b;
+      std::stringstream is(item);
+      std::getline(is, b.type, ':');
+      std::getline(is, b.name, ':');
+      std::getline(is, b.boundary, ':');
+      std::getline(is, b.expr, ':');
+      bcs.push_back(b);
+    }
+  }
+  for (const BCDesc &b : bcs)
+  {
+    auto bc = solver->add_boundary_condition(b.type, b.name, b.boundary);
+    if (!b.expr.empty() && b.expr != "-")
+      bc->set_expression(find_expr(b.expr));
+  }
+
+  // ---- element types (this harness drives single-type meshes)
+  const MeshEntity cell0     = (*sol).active_cell(ActiveIdx(0));
+  const MeshEntity geo_cell0 = (*geo).active_cell(ActiveIdx(0));
+  const ElemShape shape      = cell0.pt_set_id().elem_shape();
+  const Uint ndof            = cell0.nb_vert();
+  const Uint ngeo            = geo_cell0.nb_vert();
+  const Uint geo_order       = geo_cell0.pt_set_id().poly_order();
+
+  // ---- geometry nodes (coordinates indexed by geometry dof id)
+  const Uint ngeo_nodes = (*geo).nb_nodes();
+  std::vector<Real> geo_coords(ngeo_nodes * D, 0.0);
+  std::vector<int> geo_conn(ncells * ngeo), sol_conn(ncells * ndof);
+  for (Uint c = 0; c < ncells; ++c)
+  {
+    const MeshEntity gc = (*geo).active_cell(ActiveIdx(c));
+    const MeshEntity sc = (*sol).active_cell(ActiveIdx(c));
+    const auto coords   = mesh->active_cell(ActiveIdx(c)).coordinates();
+    for (Uint v = 0; v < ngeo; ++v)
+    {
+      geo_conn[c * ngeo + v] = gc.vertex(v);
+      const auto node        = coords.const_node_view(v);
+      for (Uint d = 0; d < D; ++d)
+        geo_coords[gc.vertex(v) * D + d] = node[d];
+    }
+    for (Uint n = 0; n < ndof; ++n)
+      sol_conn[c * ndof + n] = sc.vertex(n);
+  }
+
+  // ---- reference-element tables, built through the reference's own classes
+  StdPointSet quad;
+  quad.change_type(shape, a.quad, PointSetID::Gauss);
+  const math::DenseDMat<Real> &qp = quad.get().coordinates();
+  const math::DenseDVec<Real> &qw = quad.get().weights();
+  const Uint nq                   = qp.rows();
+
+  interpolation::FEValues fe_sol, fe_geo, fe_flux, fe_sol_at_flux, fe_geo_at_flux;
+  fe_sol.configure(PointSetTag(shape, a.p, PointSetID::Equidist),
+                   sf::SFTag(shape, SFunc::Lagrange, a.p, ModalBasis::Modal));
+  fe_sol.fill_Vandermonde(qp, qw);
+  fe_geo.configure(PointSetTag(shape, geo_order, PointSetID::Equidist),
+                   sf::SFTag(shape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
+  fe_geo.fill_Vandermonde(qp, qw);
+  fe_flux.configure(PointSetTag(shape, a.p + 1, PointSetID::Equidist),
+                    sf::SFTag(shape, SFunc::Lagrange, a.p + 1, ModalBasis::Modal));
+  fe_flux.fill_Vandermonde(qp, qw);
+
+  StdRegion flux_region;
+  flux_region.change_type(PointSetTag(shape, a.p + 1, PointSetID::Equidist));
+  const math::DenseDMat<Real> &flux_nodes = flux_region.get().coordinates();
+  const Uint nfl                          = flux_nodes.rows();
+  math::DenseDVec<Real> dummy_w(nfl);
+  dummy_w.fill(1.0);
+  fe_sol_at_flux.configure(PointSetTag(shape, a.p, PointSetID::Equidist),
+                           sf::SFTag(shape, SFunc::Lagrange, a.p, ModalBasis::Modal));
+  fe_sol_at_flux.fill_Vandermonde(flux_nodes, dummy_w);
+  fe_geo_at_flux.configure(PointSetTag(shape, geo_order, PointSetID::Equidist),
+                           sf::SFTag(shape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
+  fe_geo_at_flux.fill_Vandermonde(flux_nodes, dummy_w);
+
+  StdRegion sol_region;
+  sol_region.change_type(PointSetTag(shape, a.p, PointSetID::Equidist));
+  const math::DenseDMat<Real> &sol_nodes = sol_region.get().coordinates();
+
+  // Facet tables (boundary quadrature order = cell quadrature order + 1,
+  // solver/rdm/bc/RDMBCBase.hpp:261-263)
+  const ElemShape fshape = facet_shape_of(shape);
+  StdPointSet fquad;
+  fquad.change_type(fshape, a.quad + 1, PointSetID::Gauss);
+  const math::DenseDMat<Real> &fqp = fquad.get().coordinates();
+  const math::DenseDVec<Real> &fqw = fquad.get().weights();
+  interpolation::FEValues fe_fsol, fe_fgeo;
+  fe_fsol.configure(PointSetTag(fshape, a.p, PointSetID::Equidist),
+                    sf::SFTag(fshape, SFunc::Lagrange, a.p, ModalBasis::Modal));
+  fe_fsol.fill_Vandermonde(fqp, fqw);
+  fe_fgeo.configure(PointSetTag(fshape, geo_order, PointSetID::Equidist),
+                    sf::SFTag(fshape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
+  fe_fgeo.fill_Vandermonde(fqp, fqw);
+
+  // ---- initial state from coordinates of solution dofs (geometry basis at sol nodes)
+  interpolation::FEValues fe_geo_at_sol;
+  math::DenseDVec<Real> dummy_ws(ndof);
+  dummy_ws.fill(1.0);
+  fe_geo_at_sol.configure(PointSetTag(shape, geo_order, PointSetID::Equidist),
+                          sf::SFTag(shape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
+  fe_geo_at_sol.fill_Vandermonde(sol_nodes, dummy_ws);
+  const math::DenseDMat<Real> &Vgs = fe_geo_at_sol.Vandermonde();
+
+  std::vector<Real> sol_coords(nsol * D, 0.0);
+  for (Uint c = 0; c < ncells; ++c)
+  {
+    for (Uint n = 0; n < ndof; ++n)
+    {
+      Real x[3] = {0.0, 0.0, 0.0};
+      for (Uint g = 0; g < ngeo; ++g)
+        for (Uint d = 0; d < D; ++d)
+          x[d] += Vgs(n, g) * geo_coords[geo_conn[c * ngeo + g] * D + d];
+      for (Uint d = 0; d < D; ++d)
+        sol_coords[sol_conn[c * ndof + n] * D + d] = x[d];
+    }
+  }
+  std::vector<Real> u0(nsol * NEQ);
+  for (Uint i = 0; i < nsol; ++i)
+  {
+    init_state(a.init, &sol_coords[i * D], D, NEQ, &u0[i * NEQ]);
+    auto e = u->value(i);
+    for (Uint k = 0; k < NEQ; ++k)
+      e[k] = u0[i * NEQ + k];
+  }
+
+  auto grab = [&](const vec_fn &f) {
+    std::vector<Real> v(nsol * NEQ);
+    for (Uint i = 0; i < nsol; ++i)
+    {
+      const auto e = f.const_value(i);
+      for (Uint k = 0; k < NEQ; ++k)
+        v[i * NEQ + k] = e[k];
+    }
+    return v;
+  };
+  auto grab_scalar = [&](const interpolation::ScalarMeshFunction<Real> &f) {
+    std::vector<Real> v(nsol);
+    for (Uint i = 0; i < nsol; ++i)
+      v[i] = f[i];
+    return v;
+  };
+
+  if (a.mode == "time")
+  {
+    solver->assemble_lhs_and_rhs(a.cfl); // warm-up
+    const auto t0 = std::chrono::steady_clock::now();
+    for (Uint it = 0; it < a.iters; ++it)
+    {
+      solver->assemble_lhs_and_rhs(a.cfl);
+      solver->solve({});
+    }
+    const double s =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    math::DenseDVec<Real> nrm(NEQ);
+    solver->compute_residual_norm(nrm);
+    std::printf("{\"cells\": %u, \"nodes\": %u, \"iters\": %u, \"threads\": %u, \"seconds\": %.9g, "
+                "\"cell_updates_per_s\": %.9g, \"norm0\": %.17g}\n",
+                ncells, nsol, a.iters, a.threads, s, double(ncells) * a.iters / s, nrm[0]);
+    return 0;
+  }
+
+  // ---- dump mode
+  mkdir(a.outdir.c_str(), 0755);
+  Dumper out;
+  out.dir = a.outdir;
+
+  out.put("geo_coords", geo_coords, {ngeo_nodes, D});
+  out.put("geo_conn", geo_conn, {ncells, ngeo});
+  out.put("sol_conn", sol_conn, {ncells, ndof});
+  out.put("sol_coords", sol_coords, {nsol, D});
+  out.put("qp", mat_to_vec(qp), {nq, qp.cols()});
+  std::vector<Real> w(nq);
+  for (Uint q = 0; q < nq; ++q)
+    w[q] = qw[q];
+  out.put("w", w, {nq});
+  out.put("V", mat_to_vec(fe_sol.Vandermonde()), {nq, ndof});
+  out.put("Vgeo", mat_to_vec(fe_geo.Vandermonde()), {nq, ngeo});
+  out.put("Vf", mat_to_vec(fe_flux.Vandermonde()), {nq, nfl});
+  out.put("Vsf", mat_to_vec(fe_sol_at_flux.Vandermonde()), {nfl, ndof});
+  out.put("Vgf", mat_to_vec(fe_geo_at_flux.Vandermonde()), {nfl, ngeo});
+  for (Uint d = 0; d < D; ++d)
+  {
+    const std::string s = std::to_string(d);
+    out.put("dV" + s, mat_to_vec(fe_sol.deriv_Vandermonde(d)), {nq, ndof});
+    out.put("dVgeo" + s, mat_to_vec(fe_geo.deriv_Vandermonde(d)), {nq, ngeo});
+    out.put("dVf" + s, mat_to_vec(fe_flux.deriv_Vandermonde(d)), {nq, nfl});
+    out.put("dVgf" + s, mat_to_vec(fe_geo_at_flux.deriv_Vandermonde(d)), {nfl, ngeo});
+    out.put("dVsf" + s, mat_to_vec(fe_sol_at_flux.deriv_Vandermonde(d)), {nfl, ndof});
+  }
+  out.put("flux_nodes", mat_to_vec(flux_nodes), {nfl, flux_nodes.cols()});
+  out.put("sol_nodes", mat_to_vec(sol_nodes), {ndof, sol_nodes.cols()});
+
+  const Uint nfq = fqp.rows();
+  out.put("fqp", mat_to_vec(fqp), {nfq, fqp.cols()});
+  std::vector<Real> fw(nfq);
+  for (Uint q = 0; q < nfq; ++q)
+    fw[q] = fqw[q];
+  out.put("fw", fw, {nfq});
+  out.put("fV", mat_to_vec(fe_fsol.Vandermonde()), {nfq, fe_fsol.nb_nodes()});
+  out.put("fVgeo", mat_to_vec(fe_fgeo.Vandermonde()), {nfq, fe_fgeo.nb_nodes()});
+  for (Uint d = 0; d + 1 < D; ++d)
+    out.put("fdVgeo" + std::to_string(d), mat_to_vec(fe_fgeo.deriv_Vandermonde(d)),
+            {nfq, fe_fgeo.nb_nodes()});
+
+  // ---- boundary facets in the order the weak BCs traverse them (WeakBC.hpp:227-360)
+  std::ostringstream bcmeta;
+  for (Uint ib = 0; ib < bcs.size(); ++ib)
+  {
+    const auto &bdry = *(mesh->all_boundaries().domain(bcs[ib].boundary));
+    using dof_it     = typename BoundaryFacets<MC, D - 1>::const_dof_iterator_typed;
+    std::vector<common::IteratorRange<dof_it>> sranges, granges;
+    bdry.all_bdry_dof_ranges(*sol, sranges);
+    bdry.all_bdry_dof_ranges(*geo, granges);
+    std::vector<int> fsol, fgeo;
+    Uint nfsol = 0, nfgeo = 0, nfac = 0;
+    for (Uint r = 0; r < sranges.size(); ++r)
+    {
+      auto git = granges[r].begin();
+      for (auto it = sranges[r].begin(); it != sranges[r].end(); ++it, ++git)
+      {
+        const MeshEntity se = it->mesh_entity();
+        const MeshEntity ge = git->mesh_entity();
+        nfsol               = se.nb_vert();
+        nfgeo               = ge.nb_vert();
+        for (Uint n = 0; n < se.nb_vert(); ++n)
+          fsol.push_back(se.vertex(n));
+        for (Uint n = 0; n < ge.nb_vert(); ++n)
+          fgeo.push_back(ge.vertex(n));
+        nfac++;
+      }
+    }
+    out.put("bc" + std::to_string(ib) + "_sol", fsol, {nfac, nfsol});
+    out.put("bc" + std::to_string(ib) + "_geo", fgeo, {nfac, nfgeo});
+    bcmeta << (ib ? ", " : "") << "{\"type\": \"" << bcs[ib].type << "\", \"name\": \""
+           << bcs[ib].name << "\", \"boundary\": \"" << bcs[ib].boundary << "\", \"expr\": \""
+           << bcs[ib].expr << "\", \"nfacets\": " << nfac << "}";
+  }
+
+  out.put("u0", u0, {nsol, NEQ});
+
+  // first iteration: residual, wave speed, dt, dual volume at u0
+  solver->assemble_lhs_and_rhs(a.cfl);
+  out.put("res1", grab(*res), {nsol, NEQ});
+  out.put("ws1", grab_scalar(solver->time_update().nodal_wave_speed()), {nsol});
+  out.put("dt1", grab_scalar(*solver->scal_function(SolverScalFn::time_step)), {nsol});
+  out.put("dual_volume", grab_scalar(solver->time_update().nodal_dual_volume()), {nsol});
+  math::DenseDVec<Real> nrm(NEQ);
+  solver->compute_residual_norm(nrm);
+  std::vector<Real> norms;
+  for (Uint k = 0; k < NEQ; ++k)
+    norms.push_back(nrm[k]);
+  solver->solve({});
+  out.put("u1", grab(*u), {nsol, NEQ});
+
+  for (Uint it = 1; it < a.iters; ++it)
+  {
+    solver->assemble_lhs_and_rhs(a.cfl);
+    solver->compute_residual_norm(nrm);
+    for (Uint k = 0; k < NEQ; ++k)
+      norms.push_back(nrm[k]);
+    solver->solve({});
+  }
+  out.put("uK", grab(*u), {nsol, NEQ});
+  out.put("norms", norms, {Uint(norms.size() / NEQ), NEQ});
+
+  const char *shape_name = shape == ElemShape::Triag   ? "triag"
+                           : shape == ElemShape::Quad  ? "quad"
+                           : shape == ElemShape::Tetra ? "tetra"
+                                                       : "other";
+  std::ofstream meta(a.outdir + "/meta.json");
+  meta.precision(17);
+  meta << "{\n \"physics\": \"" << a.physics << "\", \"scheme\": \"" << a.scheme
+       << "\", \"p\": " << a.p << ", \"quad\": " << a.quad << ", \"shape\": \"" << shape_name
+       << "\", \"dim\": " << D << ", \"neq\": " << NEQ << ",\n \"ncells\": " << ncells
+       << ", \"nsol\": " << nsol << ", \"ngeo_nodes\": " << ngeo_nodes << ", \"ndof\": " << ndof
+       << ", \"ngeo\": " << ngeo << ", \"nq\": " << nq << ", \"nfl\": " << nfl
+       << ", \"nfq\": " << nfq << ",\n \"iters\": " << a.iters << ", \"cfl\": " << a.cfl
+       << ", \"init\": \"" << a.init << "\",\n \"bcs\": [" << bcmeta.str()
+       << "],\n \"arrays\": {\n"
+       << out.manifest.str() << "\n }\n}\n";
+  return 0;
+}
+
+int main(int argc, char **argv)
+{
+  if (argc < 12)
+  {
+    std::fprintf(stderr, "usage: %s dump|time physics scheme p quad mesh outdir iters cfl init "
+                         "bcspec [threads]\n",
+                 argv[0]);
+    return 2;
+  }
+  Args a;
+  a.mode    = argv[1];
+  a.physics = argv[2];
+  a.scheme  = argv[3];
+  a.p       = std::atoi(argv[4]);
+  a.quad    = std::atoi(argv[5]);
+  a.mesh    = argv[6];
+  a.outdir  = argv[7];
+  a.iters   = std::atoi(argv[8]);
+  a.cfl     = std::atof(argv[9]);
+  a.init    = argv[10];
+  a.bcspec  = argv[11];
+  a.threads = argc > 12 ? std::atoi(argv[12]) : 1;
+
+  using Adv   = physics::RotationAdvection2D<ConstDirection2D>;
+  using Burg  = physics::Burgers2D;
+  using Eul2D = physics::Euler2DCons;
+  using Eul3D = physics::Euler3DCons;
+
+#define DISPATCH(PHYS_NAME, MC, PHYS)                                                              \
+  if (a.physics == PHYS_NAME)                                                                      \
+  {                                                                                                \
+    if (a.scheme == "lda")                                                                         \
+      return run<MC, PHYS, solver::rdm::PGLDA>(a);                                                 \
+    if (a.scheme == "n")                                                                           \
+      return run<MC, PHYS, solver::rdm::PGN>(a);                                                   \
+    if (a.scheme == "b")                                                                           \
+      return run<MC, PHYS, solver::rdm::PGB>(a);                                                   \
+  }
+
+  DISPATCH("advconst", Cart2D, Adv)
+  DISPATCH("burgers", Cart2D, Burg)
+  DISPATCH("euler2d", Cart2D, Eul2D)
+  DISPATCH("euler3d", Cart3D, Eul3D)
+#undef DISPATCH
+
+  std::fprintf(stderr, "unknown physics/scheme %s/%s\n", a.physics.c_str(), a.scheme.c_str());
+  return 2;
+}
