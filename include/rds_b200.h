@@ -1,0 +1,199 @@
+/* rds_b200 -- B200 (sm_100a) implementation of pdekit's explicit continuous
+ * residual-distribution (RDS) cell-residual + pseudo-time update path.
+ *
+ * C ABI: plain pointers and sizes, no exceptions, every call returns an rds_status.
+ * Host arrays are owned by the caller and copied in/out; the context owns all device memory.
+ * Nodal fields cross the ABI in the reference's AoS layout [node][neq]
+ * (interpolation::VectorMeshFunction, src/interpolation/mesh_function/VectorMeshFunction.hpp:210-248);
+ * the device keeps them as SoA [neq][node].
+ *
+ * Entry point -> reference interface it replaces (file:line in martinv/pdekit):
+ *   rds_create / rds_add_cell_group / rds_finalize
+ *       RDMethod::configure_mesh_data + initialize_work_data
+ *       (src/solver/rdm/RDMethod.hpp:60-67,159-207; PGRDMethodExplicit.hpp:232-299)
+ *   rds_add_bc            RDMethod::add_boundary_condition + set_expression
+ *       (src/solver/rdm/RDMethod.hpp:230-243; bc/RDMBCBase.hpp:112-114)
+ *   rds_set_state / rds_get_state
+ *       set_vec_function(SolverVecFn::solution, ...) (src/solver/rdm/PGRDMethodExplicit.hpp:324-358)
+ *   rds_assemble          PGRDMethodExplicit::assemble_lhs_and_rhs(CFL) (PGRDMethodExplicit.hpp:417-423)
+ *   rds_assemble_rhs      PGRDMethodExplicit::assemble_rhs() (PGRDMethodExplicit.hpp:428-463)
+ *   rds_update            PGRDMethodExplicit::solve() (PGRDMethodExplicit.hpp:468-477)
+ *   rds_residual_norm     PGRDMethodExplicit::compute_residual_norm (PGRDMethodExplicit.hpp:482-514)
+ *   rds_get_fields        residual / time-step / wave-speed / dual-volume mesh functions
+ *       (RDMethod::vec_function, scal_function(SolverScalFn::time_step), RDTimeUpdate.hpp:30-40)
+ *   rds_iterate           the examples' loop "assemble_lhs_and_rhs(CFL); solve()" run to a residual drop
+ *       (examples/testcases-rdm/Advection-Continuous-RDS-2D-Explicit.cpp:133-174;
+ *        src/solver/time/ExplicitTimeStepper.cpp:36-40)
+ */
+#ifndef RDS_B200_H
+#define RDS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RDS_API __attribute__((visibility("default")))
+#else
+#define RDS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct rds_ctx rds_ctx;
+
+typedef enum
+{
+  RDS_OK                 = 0,
+  RDS_ERR_INVALID        = 1, /* invalid descriptor / argument / call order */
+  RDS_ERR_CUDA           = 2, /* CUDA runtime failure (message in rds_last_error) */
+  RDS_ERR_NONFINITE      = 3, /* NaN/Inf in the residual or state */
+  RDS_ERR_NEG_PRESSURE   = 4, /* non-positive pressure met (Euler) */
+  RDS_ERR_ITER_CAP       = 5, /* rds_iterate reached max_iter without the requested drop */
+  RDS_ERR_UNSUPPORTED    = 6, /* configuration not compiled into this library */
+  RDS_ERR_TOO_LARGE      = 7  /* size above a documented limit */
+} rds_status;
+
+/* Physics: template argument of PGRDMethodExplicit<MeshConfig, Physics, Scheme>. */
+typedef enum
+{
+  RDS_ADVECTION_CONST = 0, /* physics::RotationAdvection2D with a constant direction policy */
+  RDS_BURGERS2D       = 1, /* physics::Burgers2D (src/physics/scalar/Burgers2D.hpp) */
+  RDS_EULER2D         = 2, /* physics::Euler2DCons (src/physics/euler/Euler2DCons.hpp) */
+  RDS_EULER3D         = 3  /* physics::Euler3DCons (src/physics/euler/Euler3DCons.hpp) */
+} rds_physics;
+
+/* Scheme: SchemeTraits tag (src/solver/rdm/cellsplitters/PGLDA.hpp:24, PGN.hpp:24, PGB.hpp:24). */
+typedef enum
+{
+  RDS_PGLDA = 0,
+  RDS_PGN   = 1,
+  RDS_PGB   = 2
+} rds_scheme;
+
+typedef enum
+{
+  RDS_FP64  = 0, /* plain path: FP64 everywhere (parity with the reference CPU path) */
+  RDS_MIXED = 1  /* FP32 interpolation/flux/upwind arithmetic, FP64 accumulation, inverse and norms */
+} rds_precision;
+
+/* Element shapes, numbered as the reference's ElemShape (src/common/Constants.hpp:29-40). */
+typedef enum
+{
+  RDS_LINE  = 2,
+  RDS_TRIAG = 3,
+  RDS_QUAD  = 4,
+  RDS_TETRA = 10
+} rds_shape;
+
+typedef enum
+{
+  RDS_BC_WEAK_DIRICHLET = 0 /* bc/WeakDirichletBC.hpp */
+} rds_bc_kind;
+
+typedef struct
+{
+  int physics;   /* rds_physics */
+  int scheme;    /* rds_scheme */
+  int precision; /* rds_precision */
+  int dim;       /* 2 or 3 */
+  int neq;       /* 1 (scalar), 4 (Euler 2D), 5 (Euler 3D) */
+  int nnodes;    /* number of solution nodes (dofs) */
+  int ngeo_nodes;
+  const double *geo_coords; /* [ngeo_nodes][dim] */
+  double adv[3];            /* RDS_ADVECTION_CONST: advection direction */
+  double gamma;             /* Euler: ratio of specific heats (1.4) */
+} rds_desc;
+
+/* One element type: connectivity and reference-element tables as the reference's FEValues /
+ * FluxSpaceMetric hold them (src/interpolation/FEValues.hpp:45-114,
+ * src/interpolation/FluxSpaceMetric.hpp:237-456). Row-major; derivative tables stacked
+ * [dim][rows][cols]. */
+typedef struct
+{
+  int shape;   /* rds_shape */
+  int order;   /* solution polynomial order p */
+  int ncells;
+  int ndof;    /* solution dofs per cell */
+  int ngeo;    /* geometry nodes per cell */
+  int nq;      /* quadrature points */
+  int nfl;     /* flux nodes (Lagrange order p+1) */
+  const int32_t *sol_conn; /* [ncells][ndof], reference local dof order */
+  const int32_t *geo_conn; /* [ncells][ngeo] */
+  const double *w;     /* [nq]             quadrature weights */
+  const double *V;     /* [nq][ndof]       solution basis at quadrature points */
+  const double *dV;    /* [dim][nq][ndof]  reference derivatives of the solution basis */
+  const double *dVgeo; /* [dim][nq][ngeo]  reference derivatives of the geometry basis */
+  const double *dVf;   /* [dim][nq][nfl]   reference derivatives of the flux basis */
+  const double *Vsf;   /* [nfl][ndof]      solution basis at the flux nodes */
+} rds_cell_group;
+
+/* One weak boundary condition on a set of boundary facets, traversed in the given order
+ * (src/solver/rdm/bc/WeakBC.hpp:227-360). 'gq' is the boundary state g(x) evaluated by the
+ * caller at the facet quadrature points (the reference evaluates its expression pointer at the
+ * same points, bc/WeakDirichletBC.hpp:225-228). */
+typedef struct
+{
+  int kind; /* rds_bc_kind */
+  int nfacets;
+  int nfdof;
+  int nfgeo;
+  int nfq;
+  const int32_t *sol_conn; /* [nfacets][nfdof] */
+  const int32_t *geo_conn; /* [nfacets][nfgeo] */
+  const double *fw;        /* [nfq] */
+  const double *fV;        /* [nfq][nfdof] */
+  const double *fdVgeo;    /* [dim-1][nfq][nfgeo] */
+  const double *gq;        /* [nfacets][nfq][neq] */
+} rds_bc_group;
+
+/* Create a context on the current CUDA device. 'stream' is a cudaStream_t to run on, or NULL
+ * for a stream owned by the context. */
+RDS_API rds_status rds_create(rds_ctx **ctx, const rds_desc *desc, void *stream);
+RDS_API rds_status rds_add_cell_group(rds_ctx *ctx, const rds_cell_group *group);
+/* Boundary conditions are applied in the order they are added. */
+RDS_API rds_status rds_add_bc(rds_ctx *ctx, const rds_bc_group *bc);
+/* Build the node-centred gather lists and the dual volumes. Required before any solve call. */
+RDS_API rds_status rds_finalize(rds_ctx *ctx);
+
+RDS_API rds_status rds_set_state(rds_ctx *ctx, const double *u_aos);
+RDS_API rds_status rds_get_state(rds_ctx *ctx, double *u_aos);
+/* assemble_lhs_and_rhs(CFL): residual, wave speed and local time step. */
+RDS_API rds_status rds_assemble(rds_ctx *ctx, double cfl);
+/* assemble_rhs(): residual and wave speed only. */
+RDS_API rds_status rds_assemble_rhs(rds_ctx *ctx);
+/* solve(): u -= dt * res */
+RDS_API rds_status rds_update(rds_ctx *ctx);
+/* compute_residual_norm(): sqrt(sum_n (res_n dt_n)^2 / N) per equation, into norm[neq]. */
+RDS_API rds_status rds_residual_norm(rds_ctx *ctx, double *norm);
+/* Copy out any of: residual [node][neq], dt [node], nodal wave speed [node], dual volume [node]
+ * (NULL skips). */
+RDS_API rds_status rds_get_fields(rds_ctx *ctx, double *res_aos, double *dt, double *ws, double *vol);
+
+/* Pseudo-time loop on the device: up to max_iter x (assemble_lhs_and_rhs(cfl) + solve()),
+ * stopping after the first iteration whose norm satisfies max_eq norm/norm(iter 0) <= drop
+ * (drop <= 0: run exactly max_iter). The loop is captured once in a CUDA graph and replayed.
+ * it_done: iterations executed; hist (may be NULL): [max_iter][neq] norms. Returns
+ * RDS_ERR_ITER_CAP when drop > 0 was not reached. */
+RDS_API rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int *it_done,
+                       double *hist);
+
+/* Diagnostics. */
+RDS_API void *rds_stream(rds_ctx *ctx); /* the cudaStream_t the context launches on */
+/* Per-kernel device time over the launches since the last reset (enable = 1 starts event
+ * timing around every launch, 0 stops it). names: up to max entries of 32 chars. */
+RDS_API rds_status rds_kernel_timing(rds_ctx *ctx, int enable);
+RDS_API int rds_kernel_times(rds_ctx *ctx, char (*names)[32], double *ms, int *launches, int max);
+/* Kernel launches issued by this context since creation. */
+RDS_API long long rds_launch_count(rds_ctx *ctx);
+
+RDS_API rds_status rds_destroy(rds_ctx *ctx);
+RDS_API const char *rds_last_error(rds_ctx *ctx);
+RDS_API const char *rds_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

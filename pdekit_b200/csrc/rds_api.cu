@@ -1,0 +1,960 @@
+// Host runtime behind the C ABI (include/rds_b200.h): device buffers, the node-centred gather
+// lists, launch sequencing, the CUDA-graph pseudo-time loop, error reporting and per-kernel
+// event timing.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "rds_internal.h"
+
+using namespace rds;
+
+namespace
+{
+
+struct TimingRec
+{
+  const char *name;
+  cudaEvent_t a, b;
+};
+
+} // namespace
+
+struct rds_ctx
+{
+  rds_desc desc{};
+  int device             = 0;
+  cudaStream_t stream    = nullptr;
+  bool own_stream        = false;
+  bool finalized         = false;
+  std::string err;
+  long long launches = 0;
+
+  std::vector<HostCellGroup> groups;
+  std::vector<HostBC> bcs;
+
+  double *d_X       = nullptr; // SoA coords [dim][ngeo_nodes]
+  double *d_u       = nullptr; // SoA [neq][nnodes]
+  double *d_res     = nullptr;
+  double *d_ws      = nullptr;
+  double *d_dt      = nullptr;
+  double *d_vol     = nullptr;
+  double *d_inv_vol = nullptr;
+  double *d_contrib = nullptr; // [neq][S]
+  double *d_wsc     = nullptr; // [W]
+  double *d_stage   = nullptr; // AoS staging [nnodes*neq]
+  int32_t *d_row = nullptr, *d_ent_slot = nullptr, *d_ent_ws = nullptr;
+  double *d_part = nullptr, *d_norm = nullptr, *d_norm0 = nullptr, *d_hist = nullptr;
+  int *d_iter = nullptr, *d_stop = nullptr, *d_zero = nullptr;
+  unsigned *d_status = nullptr;
+  long long S = 0, W = 0, E = 0;
+  int gblocks   = 0;
+  int hist_cap  = 0;
+
+  // pinned host scalars for the loop's stop test
+  int *h_stop = nullptr;
+
+  // CUDA graph of the fused iteration
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_chunk            = 0;
+  double graph_cfl           = -1.0;
+  int graph_max_iter         = -1;
+  double graph_drop          = 0.0;
+
+  bool timing = false;
+  std::vector<TimingRec> trecs;
+  std::vector<cudaEvent_t> ev_pool;
+};
+
+namespace
+{
+
+rds_status fail(rds_ctx *c, rds_status st, const std::string &msg)
+{
+  if (c)
+    c->err = msg;
+  return st;
+}
+
+#define RDS_CUDA(call)                                                                             \
+  do                                                                                               \
+  {                                                                                                \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return fail(ctx, RDS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));          \
+  } while (0)
+
+cudaEvent_t get_event(rds_ctx *ctx)
+{
+  if (!ctx->ev_pool.empty())
+  {
+    cudaEvent_t e = ctx->ev_pool.back();
+    ctx->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Launch wrapper: optional event timing around the launch, launch counting, error text.
+template <typename F>
+rds_status launch(rds_ctx *ctx, F &&f)
+{
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (ctx->timing)
+  {
+    a = get_event(ctx);
+    b = get_event(ctx);
+    cudaEventRecord(a, ctx->stream);
+  }
+  const char *name = "?";
+  cudaError_t e    = f(&name);
+  if (e == cudaErrorNotSupported)
+    return fail(ctx, RDS_ERR_UNSUPPORTED,
+                std::string("no kernel compiled for this configuration (") + name + ")");
+  if (e != cudaSuccess)
+    return fail(ctx, RDS_ERR_CUDA, std::string(name) + ": " + cudaGetErrorString(e));
+  ctx->launches++;
+  if (ctx->timing)
+  {
+    cudaEventRecord(b, ctx->stream);
+    ctx->trecs.push_back({name, a, b});
+  }
+  return RDS_OK;
+}
+
+template <typename T>
+rds_status dalloc(rds_ctx *ctx, T **p, size_t n)
+{
+  if (n == 0)
+    n = 1;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess)
+    return fail(ctx, RDS_ERR_CUDA,
+                std::string("cudaMalloc(") + std::to_string(n * sizeof(T)) +
+                    " bytes): " + cudaGetErrorString(e));
+  return RDS_OK;
+}
+
+template <typename T>
+rds_status upload(rds_ctx *ctx, T *d, const T *h, size_t n)
+{
+  RDS_CUDA(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  return RDS_OK;
+}
+
+// SoA transposition of a [rows][cols] int32 table to [cols][rows] on the host.
+std::vector<int32_t> transpose_i32(const int32_t *a, int rows, int cols)
+{
+  std::vector<int32_t> t((size_t)rows * cols);
+  for (int r = 0; r < rows; ++r)
+    for (int c = 0; c < cols; ++c)
+      t[(size_t)c * rows + r] = a[(size_t)r * cols + c];
+  return t;
+}
+
+bool supported_physics(const rds_desc &d)
+{
+  switch (d.physics)
+  {
+  case RDS_ADVECTION_CONST:
+  case RDS_BURGERS2D:
+    return d.dim == 2 && d.neq == 1;
+  case RDS_EULER2D:
+    return d.dim == 2 && d.neq == 4;
+  case RDS_EULER3D:
+    return d.dim == 3 && d.neq == 5;
+  default:
+    return false;
+  }
+}
+
+CellArgs cell_args(rds_ctx *ctx, const HostCellGroup &g, const int *stop)
+{
+  CellArgs a{};
+  a.ncells     = g.desc.ncells;
+  a.nnodes     = ctx->desc.nnodes;
+  a.sol_conn   = g.d_sol_conn;
+  a.geo_conn   = g.d_geo_conn;
+  a.X          = ctx->d_X;
+  a.ngeo_nodes = ctx->desc.ngeo_nodes;
+  a.u          = ctx->d_u;
+  a.contrib    = ctx->d_contrib;
+  a.S          = ctx->S;
+  a.slot_base  = g.slot_base;
+  a.wsc        = ctx->d_wsc;
+  a.ws_base    = g.ws_base;
+  a.adv0       = ctx->desc.adv[0];
+  a.adv1       = ctx->desc.adv[1];
+  a.adv2       = ctx->desc.adv[2];
+  a.gamma      = ctx->desc.gamma;
+  a.status     = ctx->d_status;
+  a.stop       = stop;
+  return a;
+}
+
+BCArgs bc_args(rds_ctx *ctx, const HostBC &b, const int *stop)
+{
+  BCArgs a{};
+  a.nfacets    = b.desc.nfacets;
+  a.sol_conn   = b.d_sol_conn;
+  a.geo_conn   = b.d_geo_conn;
+  a.X          = ctx->d_X;
+  a.ngeo_nodes = ctx->desc.ngeo_nodes;
+  a.u          = ctx->d_u;
+  a.nnodes     = ctx->desc.nnodes;
+  a.gq         = b.d_gq;
+  a.vol        = ctx->d_vol;
+  a.contrib    = ctx->d_contrib;
+  a.S          = ctx->S;
+  a.slot_base  = b.slot_base;
+  a.wsc        = ctx->d_wsc;
+  a.ws_base    = b.ws_base;
+  a.adv0       = ctx->desc.adv[0];
+  a.adv1       = ctx->desc.adv[1];
+  a.gamma      = ctx->desc.gamma;
+  a.status     = ctx->d_status;
+  a.stop       = stop;
+  return a;
+}
+
+GatherArgs gather_args(rds_ctx *ctx, double cfl, const int *stop)
+{
+  GatherArgs a{};
+  a.nnodes   = ctx->desc.nnodes;
+  a.neq      = ctx->desc.neq;
+  a.row      = ctx->d_row;
+  a.ent_slot = ctx->d_ent_slot;
+  a.ent_ws   = ctx->d_ent_ws;
+  a.contrib  = ctx->d_contrib;
+  a.S        = ctx->S;
+  a.wsc      = ctx->d_wsc;
+  a.vol      = ctx->d_vol;
+  a.inv_vol  = ctx->d_inv_vol;
+  a.res      = ctx->d_res;
+  a.ws       = ctx->d_ws;
+  a.dt       = ctx->d_dt;
+  a.u        = ctx->d_u;
+  a.part     = ctx->d_part;
+  a.cfl      = cfl;
+  a.stop     = stop;
+  return a;
+}
+
+// Residual contributions of all cells and boundary facets (assemble_rhs without the gather).
+rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
+{
+  const rds_desc &d = ctx->desc;
+  for (const HostCellGroup &g : ctx->groups)
+  {
+    const CellArgs a = cell_args(ctx, g, stop);
+    rds_status st    = launch(ctx, [&](const char **name) {
+      return launch_cells(g, a, d.physics, d.scheme, d.precision, d.dim, d.neq, ctx->stream, name);
+    });
+    if (st != RDS_OK)
+      return st;
+  }
+  for (const HostBC &b : ctx->bcs)
+  {
+    const BCArgs a = bc_args(ctx, b, stop);
+    rds_status st  = launch(ctx, [&](const char **name) {
+      return launch_bc(b, a, d.physics, d.dim, d.neq, ctx->stream, name);
+    });
+    if (st != RDS_OK)
+      return st;
+  }
+  return RDS_OK;
+}
+
+rds_status check_status(rds_ctx *ctx)
+{
+  unsigned st = 0;
+  RDS_CUDA(cudaMemcpyAsync(&st, ctx->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (st & kFlagNonFinite)
+    return fail(ctx, RDS_ERR_NONFINITE, "non-finite residual norm");
+  if (st & kFlagNegPressure)
+    return fail(ctx, RDS_ERR_NEG_PRESSURE, "non-positive pressure met");
+  return RDS_OK;
+}
+
+void release_graph(rds_ctx *ctx)
+{
+  if (ctx->graph_exec)
+  {
+    cudaGraphExecDestroy(ctx->graph_exec);
+    ctx->graph_exec = nullptr;
+  }
+}
+
+} // namespace
+
+namespace rds
+{
+
+cudaError_t launch_cells(const HostCellGroup &g, const CellArgs &a, int physics, int scheme,
+                         int precision, int dim, int neq, cudaStream_t s, const char **name)
+{
+  bool ok         = false;
+  cudaError_t err = cudaSuccess;
+  if (physics == RDS_ADVECTION_CONST || physics == RDS_BURGERS2D)
+    err = launch_cells_scalar(g, a, physics, scheme, precision, s, name, &ok);
+  else
+    err = launch_cells_euler(g, a, physics, scheme, precision, s, name, &ok);
+  (void)dim;
+  (void)neq;
+  if (!ok)
+    return cudaErrorNotSupported;
+  return err;
+}
+
+} // namespace rds
+
+// ============================================================================================
+// C ABI
+// ============================================================================================
+
+extern "C" {
+
+const char *rds_version(void)
+{
+  return "rds_b200 0.1 (sm_100a)";
+}
+
+const char *rds_last_error(rds_ctx *ctx)
+{
+  return ctx ? ctx->err.c_str() : "null context";
+}
+
+void *rds_stream(rds_ctx *ctx)
+{
+  return ctx ? (void *)ctx->stream : nullptr;
+}
+
+long long rds_launch_count(rds_ctx *ctx)
+{
+  return ctx ? ctx->launches : 0;
+}
+
+rds_status rds_create(rds_ctx **out, const rds_desc *desc, void *stream)
+{
+  if (!out || !desc)
+    return RDS_ERR_INVALID;
+  *out         = nullptr;
+  rds_ctx *ctx = new rds_ctx();
+  ctx->desc    = *desc;
+  const rds_desc &d = ctx->desc;
+  if (!supported_physics(d) || d.scheme < RDS_PGLDA || d.scheme > RDS_PGB ||
+      (d.precision != RDS_FP64 && d.precision != RDS_MIXED) || d.nnodes <= 0 ||
+      d.ngeo_nodes <= 0 || !desc->geo_coords)
+  {
+    rds_status st = RDS_ERR_INVALID;
+    *out          = ctx;
+    return fail(ctx, st, "invalid descriptor (physics/dim/neq/scheme/precision/sizes)");
+  }
+  *out = ctx;
+  if (cudaGetDevice(&ctx->device) != cudaSuccess)
+    return fail(ctx, RDS_ERR_CUDA, "no CUDA device");
+  if (stream)
+    ctx->stream = (cudaStream_t)stream;
+  else
+  {
+    RDS_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->own_stream = true;
+  }
+  rds_status st;
+  const size_t ng = (size_t)d.ngeo_nodes;
+  std::vector<double> X(ng * d.dim);
+  for (size_t i = 0; i < ng; ++i)
+    for (int k = 0; k < d.dim; ++k)
+      X[k * ng + i] = desc->geo_coords[i * d.dim + k];
+  if ((st = dalloc(ctx, &ctx->d_X, X.size())) != RDS_OK)
+    return st;
+  if ((st = upload(ctx, ctx->d_X, X.data(), X.size())) != RDS_OK)
+    return st;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->desc.geo_coords = nullptr;
+  return RDS_OK;
+}
+
+rds_status rds_add_cell_group(rds_ctx *ctx, const rds_cell_group *g)
+{
+  if (!ctx || !g)
+    return RDS_ERR_INVALID;
+  if (ctx->finalized)
+    return fail(ctx, RDS_ERR_INVALID, "rds_add_cell_group after rds_finalize");
+  const int D = ctx->desc.dim;
+  if (g->ncells <= 0 || g->ndof <= 0 || g->ndof > 32 || g->ngeo <= 0 || g->ngeo > 27 ||
+      g->nq <= 0 || g->nq > 64 || g->nfl <= 0 || g->nfl > 64 || !g->sol_conn || !g->geo_conn ||
+      !g->w || !g->V || !g->dV || !g->dVgeo || !g->dVf || !g->Vsf)
+    return fail(ctx, RDS_ERR_INVALID, "invalid cell group");
+  for (size_t i = 0; i < (size_t)g->ncells * g->ndof; ++i)
+    if (g->sol_conn[i] < 0 || g->sol_conn[i] >= ctx->desc.nnodes)
+      return fail(ctx, RDS_ERR_INVALID, "solution connectivity out of range");
+  for (size_t i = 0; i < (size_t)g->ncells * g->ngeo; ++i)
+    if (g->geo_conn[i] < 0 || g->geo_conn[i] >= ctx->desc.ngeo_nodes)
+      return fail(ctx, RDS_ERR_INVALID, "geometry connectivity out of range");
+  HostCellGroup h;
+  h.desc = *g;
+  h.w.assign(g->w, g->w + g->nq);
+  h.V.assign(g->V, g->V + (size_t)g->nq * g->ndof);
+  h.dV.assign(g->dV, g->dV + (size_t)D * g->nq * g->ndof);
+  h.dVgeo.assign(g->dVgeo, g->dVgeo + (size_t)D * g->nq * g->ngeo);
+  h.dVf.assign(g->dVf, g->dVf + (size_t)D * g->nq * g->nfl);
+  h.Vsf.assign(g->Vsf, g->Vsf + (size_t)g->nfl * g->ndof);
+  h.affine = (g->shape == RDS_TRIAG && g->ngeo == 3) || (g->shape == RDS_TETRA && g->ngeo == 4);
+  rds_status st;
+  const std::vector<int32_t> sc = transpose_i32(g->sol_conn, g->ncells, g->ndof);
+  const std::vector<int32_t> gc = transpose_i32(g->geo_conn, g->ncells, g->ngeo);
+  if ((st = dalloc(ctx, &h.d_sol_conn, sc.size())) != RDS_OK)
+    return st;
+  if ((st = dalloc(ctx, &h.d_geo_conn, gc.size())) != RDS_OK)
+    return st;
+  if ((st = upload(ctx, h.d_sol_conn, sc.data(), sc.size())) != RDS_OK)
+    return st;
+  if ((st = upload(ctx, h.d_geo_conn, gc.data(), gc.size())) != RDS_OK)
+    return st;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  h.desc.sol_conn = h.desc.geo_conn = nullptr;
+  h.desc.w = h.desc.V = h.desc.dV = h.desc.dVgeo = h.desc.dVf = h.desc.Vsf = nullptr;
+  ctx->groups.push_back(h);
+  return RDS_OK;
+}
+
+rds_status rds_add_bc(rds_ctx *ctx, const rds_bc_group *b)
+{
+  if (!ctx || !b)
+    return RDS_ERR_INVALID;
+  if (ctx->finalized)
+    return fail(ctx, RDS_ERR_INVALID, "rds_add_bc after rds_finalize");
+  const int D = ctx->desc.dim, NEQ = ctx->desc.neq;
+  if (b->kind != RDS_BC_WEAK_DIRICHLET || b->nfacets <= 0 || b->nfdof <= 0 || b->nfdof > 16 ||
+      b->nfgeo <= 0 || b->nfgeo > 16 || b->nfq <= 0 || b->nfq > 32 || !b->sol_conn ||
+      !b->geo_conn || !b->fw || !b->fV || !b->fdVgeo || !b->gq)
+    return fail(ctx, RDS_ERR_INVALID, "invalid boundary group");
+  for (size_t i = 0; i < (size_t)b->nfacets * b->nfdof; ++i)
+    if (b->sol_conn[i] < 0 || b->sol_conn[i] >= ctx->desc.nnodes)
+      return fail(ctx, RDS_ERR_INVALID, "boundary solution connectivity out of range");
+  for (size_t i = 0; i < (size_t)b->nfacets * b->nfgeo; ++i)
+    if (b->geo_conn[i] < 0 || b->geo_conn[i] >= ctx->desc.ngeo_nodes)
+      return fail(ctx, RDS_ERR_INVALID, "boundary geometry connectivity out of range");
+  HostBC h;
+  h.desc = *b;
+  h.fw.assign(b->fw, b->fw + b->nfq);
+  h.fV.assign(b->fV, b->fV + (size_t)b->nfq * b->nfdof);
+  h.fdVgeo.assign(b->fdVgeo, b->fdVgeo + (size_t)(D - 1) * b->nfq * b->nfgeo);
+  const std::vector<int32_t> sc = transpose_i32(b->sol_conn, b->nfacets, b->nfdof);
+  const std::vector<int32_t> gc = transpose_i32(b->geo_conn, b->nfacets, b->nfgeo);
+  std::vector<double> gq((size_t)NEQ * b->nfq * b->nfacets);
+  for (int f = 0; f < b->nfacets; ++f)
+    for (int q = 0; q < b->nfq; ++q)
+      for (int e = 0; e < NEQ; ++e)
+        gq[((size_t)e * b->nfq + q) * b->nfacets + f] = b->gq[((size_t)f * b->nfq + q) * NEQ + e];
+  rds_status st;
+  if ((st = dalloc(ctx, &h.d_sol_conn, sc.size())) != RDS_OK ||
+      (st = dalloc(ctx, &h.d_geo_conn, gc.size())) != RDS_OK ||
+      (st = dalloc(ctx, &h.d_gq, gq.size())) != RDS_OK)
+    return st;
+  if ((st = upload(ctx, h.d_sol_conn, sc.data(), sc.size())) != RDS_OK ||
+      (st = upload(ctx, h.d_geo_conn, gc.data(), gc.size())) != RDS_OK ||
+      (st = upload(ctx, h.d_gq, gq.data(), gq.size())) != RDS_OK)
+    return st;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  h.desc.sol_conn = h.desc.geo_conn = nullptr;
+  h.desc.fw = h.desc.fV = h.desc.fdVgeo = h.desc.gq = nullptr;
+  ctx->bcs.push_back(h);
+  return RDS_OK;
+}
+
+rds_status rds_finalize(rds_ctx *ctx)
+{
+  if (!ctx)
+    return RDS_ERR_INVALID;
+  if (ctx->finalized)
+    return RDS_OK;
+  if (ctx->groups.empty())
+    return fail(ctx, RDS_ERR_INVALID, "no cell group");
+  const rds_desc &d = ctx->desc;
+  const int N       = d.nnodes;
+
+  // Slot layout: per group n-major [ndof][ncells], then per BC [nfdof][nfacets].
+  long long S = 0, W = 0;
+  for (HostCellGroup &g : ctx->groups)
+  {
+    g.slot_base = S;
+    g.ws_base   = W;
+    S += (long long)g.desc.ndof * g.desc.ncells;
+    W += g.desc.ncells;
+  }
+  for (HostBC &b : ctx->bcs)
+  {
+    b.slot_base = S;
+    b.ws_base   = W;
+    S += (long long)b.desc.nfdof * b.desc.nfacets;
+    W += (long long)b.desc.nfdof * b.desc.nfacets;
+  }
+  if (S >= (1LL << 31) || W >= (1LL << 31))
+    return fail(ctx, RDS_ERR_TOO_LARGE, "more than 2^31 contribution slots");
+  ctx->S = S;
+  ctx->W = W;
+
+  // Gather lists (CSR over nodes): cells of each group in ascending order, then BC facets in
+  // the order the conditions were added. Host copies of the connectivity are rebuilt from the
+  // device (they were transposed on upload).
+  std::vector<int32_t> count(N + 1, 0);
+  std::vector<std::vector<int32_t>> gconn(ctx->groups.size()), bconn(ctx->bcs.size());
+  for (size_t ig = 0; ig < ctx->groups.size(); ++ig)
+  {
+    const HostCellGroup &g = ctx->groups[ig];
+    gconn[ig].resize((size_t)g.desc.ncells * g.desc.ndof);
+    RDS_CUDA(cudaMemcpy(gconn[ig].data(), g.d_sol_conn, gconn[ig].size() * 4,
+                        cudaMemcpyDeviceToHost));
+    for (int32_t v : gconn[ig])
+      count[v + 1]++;
+  }
+  for (size_t ib = 0; ib < ctx->bcs.size(); ++ib)
+  {
+    const HostBC &b = ctx->bcs[ib];
+    bconn[ib].resize((size_t)b.desc.nfacets * b.desc.nfdof);
+    RDS_CUDA(cudaMemcpy(bconn[ib].data(), b.d_sol_conn, bconn[ib].size() * 4,
+                        cudaMemcpyDeviceToHost));
+    for (int32_t v : bconn[ib])
+      count[v + 1]++;
+  }
+  for (int i = 0; i < N; ++i)
+    count[i + 1] += count[i];
+  const long long E = count[N];
+  ctx->E            = E;
+  std::vector<int32_t> pos(count.begin(), count.end() - 1);
+  std::vector<int32_t> ent_slot(E), ent_ws(E);
+  for (size_t ig = 0; ig < ctx->groups.size(); ++ig)
+  {
+    const HostCellGroup &g = ctx->groups[ig];
+    const int nc = g.desc.ncells, nd = g.desc.ndof;
+    for (int c = 0; c < nc; ++c)
+      for (int n = 0; n < nd; ++n)
+      {
+        const int v      = gconn[ig][(size_t)n * nc + c];
+        const int p      = pos[v]++;
+        ent_slot[p]      = (int32_t)(g.slot_base + (long long)n * nc + c);
+        ent_ws[p]        = (int32_t)(g.ws_base + c);
+      }
+  }
+  for (size_t ib = 0; ib < ctx->bcs.size(); ++ib)
+  {
+    const HostBC &b = ctx->bcs[ib];
+    const int nf = b.desc.nfacets, nd = b.desc.nfdof;
+    for (int f = 0; f < nf; ++f)
+      for (int n = 0; n < nd; ++n)
+      {
+        const int v = bconn[ib][(size_t)n * nf + f];
+        const int p = pos[v]++;
+        ent_slot[p] = (int32_t)(b.slot_base + (long long)n * nf + f);
+        ent_ws[p]   = (int32_t)(b.ws_base + (long long)n * nf + f);
+      }
+  }
+  for (int v = 0; v < N; ++v)
+    if (count[v + 1] == count[v])
+      return fail(ctx, RDS_ERR_INVALID, "solution node " + std::to_string(v) +
+                                            " belongs to no cell");
+
+  rds_status st;
+  const int NEQ = d.neq;
+  ctx->gblocks  = (N + kGBlock - 1) / kGBlock;
+  if ((st = dalloc(ctx, &ctx->d_u, (size_t)N * NEQ)) || (st = dalloc(ctx, &ctx->d_res, (size_t)N * NEQ)) ||
+      (st = dalloc(ctx, &ctx->d_ws, N)) || (st = dalloc(ctx, &ctx->d_dt, N)) ||
+      (st = dalloc(ctx, &ctx->d_vol, N)) || (st = dalloc(ctx, &ctx->d_inv_vol, N)) ||
+      (st = dalloc(ctx, &ctx->d_contrib, (size_t)S * NEQ)) || (st = dalloc(ctx, &ctx->d_wsc, W)) ||
+      (st = dalloc(ctx, &ctx->d_stage, (size_t)N * NEQ)) || (st = dalloc(ctx, &ctx->d_row, N + 1)) ||
+      (st = dalloc(ctx, &ctx->d_ent_slot, E)) || (st = dalloc(ctx, &ctx->d_ent_ws, E)) ||
+      (st = dalloc(ctx, &ctx->d_part, (size_t)ctx->gblocks * NEQ)) ||
+      (st = dalloc(ctx, &ctx->d_norm, NEQ)) || (st = dalloc(ctx, &ctx->d_norm0, NEQ)) ||
+      (st = dalloc(ctx, &ctx->d_iter, 1)) || (st = dalloc(ctx, &ctx->d_stop, 1)) ||
+      (st = dalloc(ctx, &ctx->d_zero, 1)) || (st = dalloc(ctx, &ctx->d_status, 1)))
+    return st;
+  RDS_CUDA(cudaMallocHost(&ctx->h_stop, sizeof(int)));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_u, 0, (size_t)N * NEQ * sizeof(double), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_res, 0, (size_t)N * NEQ * sizeof(double), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_dt, 0, (size_t)N * sizeof(double), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_ws, 0, (size_t)N * sizeof(double), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_zero, 0, sizeof(int), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_stop, 0, sizeof(int), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_wsc, 0, (size_t)W * sizeof(double), ctx->stream));
+  if ((st = upload(ctx, ctx->d_row, count.data(), N + 1)) ||
+      (st = upload(ctx, ctx->d_ent_slot, ent_slot.data(), E)) ||
+      (st = upload(ctx, ctx->d_ent_ws, ent_ws.data(), E)))
+    return st;
+
+  // Dual volumes: per-cell volume into the wave-speed slot space, then a gather (boundary
+  // slots hold zero).
+  for (const HostCellGroup &g : ctx->groups)
+  {
+    double *dw = nullptr, *ddv = nullptr;
+    if ((st = dalloc(ctx, &dw, g.w.size())) || (st = dalloc(ctx, &ddv, g.dVgeo.size())))
+      return st;
+    if ((st = upload(ctx, dw, g.w.data(), g.w.size())) ||
+        (st = upload(ctx, ddv, g.dVgeo.data(), g.dVgeo.size())))
+      return st;
+    RDS_CUDA(launch_cell_volume_raw(g.desc.ncells, d.dim, g.desc.nq, g.desc.ngeo, g.d_geo_conn,
+                                    ctx->d_X, d.ngeo_nodes, dw, ddv, ctx->d_wsc + g.ws_base,
+                                    ctx->stream));
+    RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaFree(dw);
+    cudaFree(ddv);
+  }
+  RDS_CUDA(launch_dual_volume(N, ctx->d_row, ctx->d_ent_ws, ctx->d_wsc, ctx->d_vol,
+                              ctx->d_inv_vol, ctx->stream));
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->finalized = true;
+  return RDS_OK;
+}
+
+rds_status rds_set_state(rds_ctx *ctx, const double *u)
+{
+  if (!ctx || !u || !ctx->finalized)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_set_state: not finalized or null") : RDS_ERR_INVALID;
+  const int N = ctx->desc.nnodes, NEQ = ctx->desc.neq;
+  if (NEQ == 1)
+  {
+    RDS_CUDA(cudaMemcpyAsync(ctx->d_u, u, (size_t)N * sizeof(double), cudaMemcpyHostToDevice,
+                             ctx->stream));
+  }
+  else
+  {
+    RDS_CUDA(cudaMemcpyAsync(ctx->d_stage, u, (size_t)N * NEQ * sizeof(double),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    // strided device-to-device copies: AoS column e -> SoA row e
+    for (int e = 0; e < NEQ; ++e)
+      RDS_CUDA(cudaMemcpy2DAsync(ctx->d_u + (size_t)e * N, sizeof(double), ctx->d_stage + e,
+                                 NEQ * sizeof(double), sizeof(double), N,
+                                 cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  return RDS_OK;
+}
+
+static rds_status get_soa(rds_ctx *ctx, const double *d_soa, double *h_aos, int neq)
+{
+  const int N = ctx->desc.nnodes;
+  if (neq == 1)
+  {
+    RDS_CUDA(cudaMemcpyAsync(h_aos, d_soa, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+  }
+  else
+  {
+    for (int e = 0; e < neq; ++e)
+      RDS_CUDA(cudaMemcpy2DAsync(ctx->d_stage + e, neq * sizeof(double), d_soa + (size_t)e * N,
+                                 sizeof(double), sizeof(double), N, cudaMemcpyDeviceToDevice,
+                                 ctx->stream));
+    RDS_CUDA(cudaMemcpyAsync(h_aos, ctx->d_stage, (size_t)N * neq * sizeof(double),
+                             cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  return RDS_OK;
+}
+
+rds_status rds_get_state(rds_ctx *ctx, double *u)
+{
+  if (!ctx || !u || !ctx->finalized)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_get_state: not finalized or null") : RDS_ERR_INVALID;
+  rds_status st = get_soa(ctx, ctx->d_u, u, ctx->desc.neq);
+  if (st != RDS_OK)
+    return st;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RDS_OK;
+}
+
+static rds_status assemble_impl(rds_ctx *ctx, double cfl, int mode)
+{
+  if (!ctx || !ctx->finalized)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "not finalized") : RDS_ERR_INVALID;
+  rds_status st = launch_residual_kernels(ctx, ctx->d_zero);
+  if (st != RDS_OK)
+    return st;
+  const GatherArgs ga = gather_args(ctx, cfl, ctx->d_zero);
+  return launch(ctx, [&](const char **name) {
+    return launch_gather(ga, mode, ctx->gblocks, ctx->stream, name);
+  });
+}
+
+rds_status rds_assemble(rds_ctx *ctx, double cfl)
+{
+  return assemble_impl(ctx, cfl, 1);
+}
+
+rds_status rds_assemble_rhs(rds_ctx *ctx)
+{
+  return assemble_impl(ctx, 0.0, 0);
+}
+
+rds_status rds_update(rds_ctx *ctx)
+{
+  if (!ctx || !ctx->finalized)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "not finalized") : RDS_ERR_INVALID;
+  return launch(ctx, [&](const char **name) {
+    return launch_update(ctx->desc.nnodes, ctx->desc.neq, ctx->d_dt, ctx->d_res, ctx->d_u,
+                         ctx->stream, name);
+  });
+}
+
+rds_status rds_residual_norm(rds_ctx *ctx, double *norm)
+{
+  if (!ctx || !norm || !ctx->finalized)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "not finalized or null") : RDS_ERR_INVALID;
+  const int N = ctx->desc.nnodes, NEQ = ctx->desc.neq;
+  rds_status st = launch(ctx, [&](const char **name) {
+    *name = "norm_partials";
+    return launch_norm_partials(N, NEQ, ctx->d_res, ctx->d_dt, ctx->d_part, ctx->gblocks,
+                                ctx->stream);
+  });
+  if (st != RDS_OK)
+    return st;
+  st = launch(ctx, [&](const char **name) {
+    return launch_norm_final(ctx->d_part, ctx->gblocks, NEQ, N, ctx->d_norm, nullptr, nullptr,
+                             nullptr, 0, 0.0, nullptr, nullptr, ctx->stream, name);
+  });
+  if (st != RDS_OK)
+    return st;
+  RDS_CUDA(cudaMemcpyAsync(norm, ctx->d_norm, NEQ * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RDS_OK;
+}
+
+rds_status rds_get_fields(rds_ctx *ctx, double *res, double *dt, double *ws, double *vol)
+{
+  if (!ctx || !ctx->finalized)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "not finalized") : RDS_ERR_INVALID;
+  const int N = ctx->desc.nnodes;
+  rds_status st;
+  if (res && (st = get_soa(ctx, ctx->d_res, res, ctx->desc.neq)) != RDS_OK)
+    return st;
+  if (dt)
+    RDS_CUDA(cudaMemcpyAsync(dt, ctx->d_dt, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (ws)
+    RDS_CUDA(cudaMemcpyAsync(ws, ctx->d_ws, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (vol)
+    RDS_CUDA(cudaMemcpyAsync(vol, ctx->d_vol, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return check_status(ctx);
+}
+
+// One fused iteration: cell + facet kernels, gather with time step, update and norm partials,
+// final norm with the stop test. All launches honour the device stop flag.
+static rds_status enqueue_iteration(rds_ctx *ctx, double cfl, int max_iter, double drop)
+{
+  rds_status st = launch_residual_kernels(ctx, ctx->d_stop);
+  if (st != RDS_OK)
+    return st;
+  const GatherArgs ga = gather_args(ctx, cfl, ctx->d_stop);
+  st = launch(ctx, [&](const char **name) {
+    return launch_gather(ga, 7, ctx->gblocks, ctx->stream, name);
+  });
+  if (st != RDS_OK)
+    return st;
+  return launch(ctx, [&](const char **name) {
+    return launch_norm_final(ctx->d_part, ctx->gblocks, ctx->desc.neq, ctx->desc.nnodes,
+                             ctx->d_norm, ctx->d_norm0, ctx->d_hist, ctx->d_iter, max_iter, drop,
+                             ctx->d_stop, ctx->d_status, ctx->stream, name);
+  });
+}
+
+rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int *it_done,
+                       double *hist)
+{
+  if (!ctx || !ctx->finalized || max_iter <= 0)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_iterate: not finalized or max_iter <= 0")
+               : RDS_ERR_INVALID;
+  const int NEQ = ctx->desc.neq;
+  rds_status st;
+  if (max_iter > ctx->hist_cap)
+  {
+    if (ctx->d_hist)
+      cudaFree(ctx->d_hist);
+    ctx->d_hist = nullptr;
+    if ((st = dalloc(ctx, &ctx->d_hist, (size_t)max_iter * NEQ)) != RDS_OK)
+      return st;
+    ctx->hist_cap = max_iter;
+    release_graph(ctx);
+  }
+  RDS_CUDA(cudaMemsetAsync(ctx->d_iter, 0, sizeof(int), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_stop, 0, sizeof(int), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
+
+  const int chunk = std::min(max_iter, 16);
+  if (ctx->timing)
+  {
+    // event timing wants plain launches: run the loop without a graph
+    for (int it = 0; it < max_iter; ++it)
+      if ((st = enqueue_iteration(ctx, cfl, max_iter, drop)) != RDS_OK)
+        return st;
+  }
+  else
+  {
+    if (!ctx->graph_exec || ctx->graph_cfl != cfl || ctx->graph_max_iter != max_iter ||
+        ctx->graph_drop != drop || ctx->graph_chunk != chunk)
+    {
+      release_graph(ctx);
+      cudaGraph_t graph;
+      RDS_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      const long long l0 = ctx->launches;
+      for (int k = 0; k < chunk; ++k)
+      {
+        st = enqueue_iteration(ctx, cfl, max_iter, drop);
+        if (st != RDS_OK)
+        {
+          cudaStreamEndCapture(ctx->stream, &graph);
+          if (graph)
+            cudaGraphDestroy(graph);
+          return st;
+        }
+      }
+      ctx->launches = l0; // launches are counted when the graph runs
+      RDS_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
+      cudaError_t e = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess)
+        return fail(ctx, RDS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      ctx->graph_cfl      = cfl;
+      ctx->graph_max_iter = max_iter;
+      ctx->graph_drop     = drop;
+      ctx->graph_chunk    = chunk;
+    }
+    const long long per_iter = (long long)ctx->groups.size() + (long long)ctx->bcs.size() + 2;
+    const int nchunks        = (max_iter + chunk - 1) / chunk;
+    for (int k = 0; k < nchunks; ++k)
+    {
+      RDS_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+      ctx->launches += per_iter * chunk;
+      if (drop > 0.0 && k + 1 < nchunks && (k % 4) == 3)
+      {
+        // poll the device stop flag now and then; chunks after convergence exit at once
+        RDS_CUDA(cudaMemcpyAsync(ctx->h_stop, ctx->d_stop, sizeof(int), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (*ctx->h_stop)
+          break;
+      }
+    }
+  }
+  int done = 0;
+  RDS_CUDA(cudaMemcpyAsync(&done, ctx->d_iter, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (it_done)
+    *it_done = done;
+  if (hist && done > 0)
+  {
+    RDS_CUDA(cudaMemcpy(hist, ctx->d_hist, (size_t)done * NEQ * sizeof(double),
+                        cudaMemcpyDeviceToHost));
+  }
+  st = check_status(ctx);
+  if (st != RDS_OK)
+    return st;
+  if (drop > 0.0)
+  {
+    std::vector<double> h((size_t)NEQ * 2);
+    RDS_CUDA(cudaMemcpy(h.data(), ctx->d_norm, NEQ * sizeof(double), cudaMemcpyDeviceToHost));
+    RDS_CUDA(cudaMemcpy(h.data() + NEQ, ctx->d_norm0, NEQ * sizeof(double), cudaMemcpyDeviceToHost));
+    double rel = 0.0;
+    for (int e = 0; e < NEQ; ++e)
+      rel = std::max(rel, h[NEQ + e] > 0 ? h[e] / h[NEQ + e] : 0.0);
+    if (rel > drop)
+      return fail(ctx, RDS_ERR_ITER_CAP, "residual drop not reached within max_iter");
+  }
+  return RDS_OK;
+}
+
+rds_status rds_kernel_timing(rds_ctx *ctx, int enable)
+{
+  if (!ctx)
+    return RDS_ERR_INVALID;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (TimingRec &r : ctx->trecs)
+  {
+    ctx->ev_pool.push_back(r.a);
+    ctx->ev_pool.push_back(r.b);
+  }
+  ctx->trecs.clear();
+  ctx->timing = enable != 0;
+  return RDS_OK;
+}
+
+int rds_kernel_times(rds_ctx *ctx, char (*names)[32], double *ms, int *launches, int max)
+{
+  if (!ctx)
+    return 0;
+  cudaStreamSynchronize(ctx->stream);
+  std::vector<std::string> order;
+  std::map<std::string, std::pair<double, int>> acc;
+  for (TimingRec &r : ctx->trecs)
+  {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, r.a, r.b);
+    if (!acc.count(r.name))
+      order.push_back(r.name);
+    acc[r.name].first += t;
+    acc[r.name].second += 1;
+  }
+  int n = 0;
+  for (const std::string &k : order)
+  {
+    if (n >= max)
+      break;
+    std::snprintf(names[n], 32, "%s", k.c_str());
+    ms[n]       = acc[k].first;
+    launches[n] = acc[k].second;
+    ++n;
+  }
+  return n;
+}
+
+rds_status rds_destroy(rds_ctx *ctx)
+{
+  if (!ctx)
+    return RDS_OK;
+  if (ctx->stream)
+    cudaStreamSynchronize(ctx->stream);
+  release_graph(ctx);
+  for (HostCellGroup &g : ctx->groups)
+  {
+    cudaFree(g.d_sol_conn);
+    cudaFree(g.d_geo_conn);
+  }
+  for (HostBC &b : ctx->bcs)
+  {
+    cudaFree(b.d_sol_conn);
+    cudaFree(b.d_geo_conn);
+    cudaFree(b.d_gq);
+  }
+  void *bufs[] = {ctx->d_X,     ctx->d_u,     ctx->d_res,     ctx->d_ws,       ctx->d_dt,
+                  ctx->d_vol,   ctx->d_inv_vol, ctx->d_contrib, ctx->d_wsc,    ctx->d_stage,
+                  ctx->d_row,   ctx->d_ent_slot, ctx->d_ent_ws, ctx->d_part,   ctx->d_norm,
+                  ctx->d_norm0, ctx->d_hist,  ctx->d_iter,    ctx->d_stop,     ctx->d_zero,
+                  ctx->d_status};
+  for (void *p : bufs)
+    if (p)
+      cudaFree(p);
+  if (ctx->h_stop)
+    cudaFreeHost(ctx->h_stop);
+  for (TimingRec &r : ctx->trecs)
+  {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (cudaEvent_t e : ctx->ev_pool)
+    cudaEventDestroy(e);
+  if (ctx->own_stream && ctx->stream)
+    cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return RDS_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,280 @@
+// Cell residual kernels for the scalar 2D physics (constant-direction advection, Burgers) with
+// the PGLDA / PGN / PGB distribution schemes. One thread per cell.
+//
+// Per cell this fuses what the reference does in three batched metric passes and one per-cell
+// scheme call (src/solver/rdm/assembly/PGRDMExplicitCellWorker.hpp:406-545):
+//   geometry   J = dVgeo X, detJ, invJ          (src/interpolation/GeometryMetric.hpp:364-440)
+//   solution   u_q = V u                        (src/interpolation/SolutionSpaceMetric.hpp:288-327)
+//   flux       F(Vsf u) at the p+1 flux nodes, d F_d / d x_d at q via invJ dVf F
+//                                               (src/interpolation/FluxSpaceMetric.hpp:545-746)
+//   scheme     k_n = a(u_q) . grad phi_n, K+ = max(k_n, 0), beta_n = K+_n / sum K+,
+//              LDA part  sum_q w_q detJ_q beta_n r_q,
+//              N part    sum_q w_q detJ_q beta_n sum_{m != n} K+_m (u_n - u_m)
+//              PGB blends with theta = |Phi| / (sum_n |lda_n + diss_n| + 1e-6)
+//                                               (src/solver/rdm/cellsplitters/PGLDA.hpp:171-310,
+//                                                PGN.hpp:154-289, PGB.hpp:314-498)
+//   wave speed |K| max_{q,n} max(1e-6, |k_n|)   (PGLDA.hpp:207-214,301-310)
+// and writes the cell's nodal residuals and wave speed to its contribution slots; the node
+// gather (rds_gather.cu) sums them in ascending cell order.
+//
+// Precision: T = double is the plain path. T = float evaluates interpolation, flux, upwind
+// coefficients in FP32 and keeps the sum of K+ inverse, the accumulation over quadrature points
+// and the nodal residual in FP64.
+
+#include "rds_internal.h"
+#include "rds_tables.cuh"
+
+namespace rds
+{
+
+namespace
+{
+
+template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, bool AFFINE>
+__global__ void __launch_bounds__(kBlock)
+    cells_scalar2d(const CellArgs a, const Tables<T, 2, NDOF, NQ, NFL, NGEO> tb)
+{
+  if (*a.stop)
+    return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncells)
+    return;
+
+  // ---- gather nodal state and geometry (SoA connectivity: coalesced index loads)
+  double ud[NDOF];
+  T un[NDOF];
+#pragma unroll
+  for (int n = 0; n < NDOF; ++n)
+  {
+    const int v = __ldg(a.sol_conn + (size_t)n * a.ncells + c);
+    ud[n]       = __ldg(a.u + v);
+    un[n]       = T(ud[n]);
+  }
+  T X0[NGEO], X1[NGEO];
+#pragma unroll
+  for (int g = 0; g < NGEO; ++g)
+  {
+    const int v = __ldg(a.geo_conn + (size_t)g * a.ncells + c);
+    X0[g]       = T(__ldg(a.X + v));
+    X1[g]       = T(__ldg(a.X + a.ngeo_nodes + v));
+  }
+
+  // ---- physical flux at the flux nodes (order p+1 Lagrange interpolant of F)
+  T F0[NFL], F1[NFL];
+#pragma unroll
+  for (int f = 0; f < NFL; ++f)
+  {
+    T s = tb.Vsf[f][0] * un[0];
+#pragma unroll
+    for (int n = 1; n < NDOF; ++n)
+      s = s + tb.Vsf[f][n] * un[n];
+    if (PHYS == RDS_BURGERS2D)
+    {
+      F0[f] = T(0.5) * s * s;
+      F1[f] = s;
+    }
+    else
+    {
+      F0[f] = T(a.adv0) * s;
+      F1[f] = T(a.adv1) * s;
+    }
+  }
+
+  T ij00 = 0, ij01 = 0, ij10 = 0, ij11 = 0, detj = 0;
+  auto jacobian = [&](int q) {
+    T J00 = tb.dVgeo[0][q][0] * X0[0], J01 = tb.dVgeo[0][q][0] * X1[0];
+    T J10 = tb.dVgeo[1][q][0] * X0[0], J11 = tb.dVgeo[1][q][0] * X1[0];
+#pragma unroll
+    for (int g = 1; g < NGEO; ++g)
+    {
+      J00 = J00 + tb.dVgeo[0][q][g] * X0[g];
+      J01 = J01 + tb.dVgeo[0][q][g] * X1[g];
+      J10 = J10 + tb.dVgeo[1][q][g] * X0[g];
+      J11 = J11 + tb.dVgeo[1][q][g] * X1[g];
+    }
+    detj           = J00 * J11 - J01 * J10;
+    const T inv_det = T(1) / detj;
+    ij00            = inv_det * J11;
+    ij11            = inv_det * J00;
+    ij01            = -inv_det * J01;
+    ij10            = -inv_det * J10;
+  };
+  if (AFFINE)
+    jacobian(0);
+
+  double lda[NDOF], diss[NDOF];
+#pragma unroll
+  for (int n = 0; n < NDOF; ++n)
+  {
+    lda[n]  = 0.0;
+    diss[n] = 0.0;
+  }
+  double phi = 0.0, vol = 0.0;
+  T wsmax    = T(0);
+
+#pragma unroll
+  for (int q = 0; q < NQ; ++q)
+  {
+    if (!AFFINE)
+      jacobian(q);
+    const T wjT     = tb.w[q] * detj;
+    const double wj = double(wjT);
+    vol += wj;
+
+    // flux divergence at q
+    T d00 = tb.dVf[0][q][0] * F0[0], d01 = tb.dVf[1][q][0] * F0[0];
+    T d10 = tb.dVf[0][q][0] * F1[0], d11 = tb.dVf[1][q][0] * F1[0];
+#pragma unroll
+    for (int f = 1; f < NFL; ++f)
+    {
+      d00 = d00 + tb.dVf[0][q][f] * F0[f];
+      d01 = d01 + tb.dVf[1][q][f] * F0[f];
+      d10 = d10 + tb.dVf[0][q][f] * F1[f];
+      d11 = d11 + tb.dVf[1][q][f] * F1[f];
+    }
+    const T rT      = (ij00 * d00 + ij01 * d01) + (ij10 * d10 + ij11 * d11);
+    const double rq = double(rT);
+
+    // advection speed at q
+    T ax, ay;
+    if (PHYS == RDS_BURGERS2D)
+    {
+      T uq = tb.V[q][0] * un[0];
+#pragma unroll
+      for (int n = 1; n < NDOF; ++n)
+        uq = uq + tb.V[q][n] * un[n];
+      ax = uq;
+      ay = T(1);
+    }
+    else
+    {
+      ax = T(a.adv0);
+      ay = T(a.adv1);
+    }
+
+    // upwind coefficients k+_n and their sum
+    T kp[NDOF];
+    T sumkp = T(0);
+#pragma unroll
+    for (int n = 0; n < NDOF; ++n)
+    {
+      const T gx = ij00 * tb.dV[0][q][n] + ij01 * tb.dV[1][q][n];
+      const T gy = ij10 * tb.dV[0][q][n] + ij11 * tb.dV[1][q][n];
+      const T k  = ax * gx + ay * gy;
+      kp[n]      = k > T(0) ? k : T(0);
+      const T ak = fabs(k);
+      wsmax      = fmax(wsmax, fmax(T(1.e-6), ak));
+      sumkp      = sumkp + kp[n];
+    }
+    const double inv = 1.0 / double(sumkp); // FP64 inverse in both precisions
+
+    phi += wj * rq;
+#pragma unroll
+    for (int n = 0; n < NDOF; ++n)
+    {
+      const double beta = double(kp[n]) * inv;
+      lda[n] += wj * (beta * rq);
+    }
+    if (SCHEME != RDS_PGLDA)
+    {
+#pragma unroll
+      for (int n = 0; n < NDOF; ++n)
+      {
+        // sum_{m != n} K+_m (u_n - u_m), differences taken on the FP64 nodal values
+        double s = 0.0;
+#pragma unroll
+        for (int m = 0; m < NDOF; ++m)
+          if (m != n)
+            s += double(kp[m]) * (ud[n] - ud[m]);
+        diss[n] += wj * ((double(kp[n]) * inv) * s);
+      }
+    }
+  }
+
+  double theta = 1.0;
+  if (SCHEME == RDS_PGB)
+  {
+    double abs_phiN = 0.0;
+#pragma unroll
+    for (int n = 0; n < NDOF; ++n)
+      abs_phiN += fabs(lda[n] + diss[n]);
+    theta = fabs(phi) / (abs_phiN + 1.e-6);
+  }
+
+  double *out = a.contrib + a.slot_base + c;
+#pragma unroll
+  for (int n = 0; n < NDOF; ++n)
+  {
+    const double r = (SCHEME == RDS_PGLDA) ? lda[n] : lda[n] + theta * diss[n];
+    __stcs(out + (size_t)n * a.ncells, r);
+  }
+  __stcs(a.wsc + a.ws_base + c, vol * double(wsmax));
+}
+
+template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO>
+cudaError_t launch_one(const HostCellGroup &g, const CellArgs &a, cudaStream_t s)
+{
+  Tables<T, 2, NDOF, NQ, NFL, NGEO> tb;
+  fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
+  const int grid = (a.ncells + kBlock - 1) / kBlock;
+  if (g.affine)
+    cells_scalar2d<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, true><<<grid, kBlock, 0, s>>>(a, tb);
+  else
+    cells_scalar2d<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, false><<<grid, kBlock, 0, s>>>(a, tb);
+  return cudaGetLastError();
+}
+
+template <int PHYS, int SCHEME, typename T>
+cudaError_t dispatch_shape(const HostCellGroup &g, const CellArgs &a, cudaStream_t s, bool *ok)
+{
+  const rds_cell_group &d = g.desc;
+  *ok                     = true;
+  if (d.shape == RDS_TRIAG && d.ngeo == 3)
+  {
+    // (order, quadrature points, flux nodes): P1/P4-rule, P1/P5, P2/P4, P2/P5, P3/P8
+    if (d.ndof == 3 && d.nq == 6 && d.nfl == 6)
+      return launch_one<PHYS, SCHEME, T, 3, 6, 6, 3>(g, a, s);
+    if (d.ndof == 3 && d.nq == 7 && d.nfl == 6)
+      return launch_one<PHYS, SCHEME, T, 3, 7, 6, 3>(g, a, s);
+    if (d.ndof == 6 && d.nq == 6 && d.nfl == 10)
+      return launch_one<PHYS, SCHEME, T, 6, 6, 10, 3>(g, a, s);
+    if (d.ndof == 6 && d.nq == 7 && d.nfl == 10)
+      return launch_one<PHYS, SCHEME, T, 6, 7, 10, 3>(g, a, s);
+    if (d.ndof == 10 && d.nq == 16 && d.nfl == 15)
+      return launch_one<PHYS, SCHEME, T, 10, 16, 15, 3>(g, a, s);
+  }
+  *ok = false;
+  return cudaSuccess;
+}
+
+const char *kernel_name(int physics, int scheme)
+{
+  static const char *names[2][3] = {{"cells_adv_lda", "cells_adv_n", "cells_adv_b"},
+                                    {"cells_burgers_lda", "cells_burgers_n", "cells_burgers_b"}};
+  return names[physics == RDS_BURGERS2D ? 1 : 0][scheme];
+}
+
+} // namespace
+
+// Scalar-physics part of launch_cells (the Euler kernels live in rds_cells_euler.cu).
+cudaError_t launch_cells_scalar(const HostCellGroup &g, const CellArgs &a, int physics,
+                                int scheme, int precision, cudaStream_t s, const char **name,
+                                bool *ok)
+{
+  *name = kernel_name(physics, scheme);
+#define RDS_SCALAR_CASE(PH, SC)                                                                    \
+  if (physics == PH && scheme == SC)                                                               \
+    return precision == RDS_MIXED ? dispatch_shape<PH, SC, float>(g, a, s, ok)                     \
+                                  : dispatch_shape<PH, SC, double>(g, a, s, ok);
+  RDS_SCALAR_CASE(RDS_ADVECTION_CONST, RDS_PGLDA)
+  RDS_SCALAR_CASE(RDS_ADVECTION_CONST, RDS_PGN)
+  RDS_SCALAR_CASE(RDS_ADVECTION_CONST, RDS_PGB)
+  RDS_SCALAR_CASE(RDS_BURGERS2D, RDS_PGLDA)
+  RDS_SCALAR_CASE(RDS_BURGERS2D, RDS_PGN)
+  RDS_SCALAR_CASE(RDS_BURGERS2D, RDS_PGB)
+#undef RDS_SCALAR_CASE
+  *ok = false;
+  return cudaSuccess;
+}
+
+} // namespace rds

@@ -1,0 +1,142 @@
+// Internal declarations shared by the host runtime (rds_api.cu) and the kernel files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rds_b200.h"
+
+namespace rds
+{
+
+constexpr int kMaxNeq  = 5;
+constexpr int kMaxDim  = 3;
+constexpr int kBlock   = 128; // threads per block of the cell/facet kernels
+constexpr int kGBlock  = 256; // threads per block of the node gather kernel
+
+// Device-side status word bits (ORed by kernels, read by the host).
+enum : unsigned
+{
+  kFlagNonFinite   = 1u,
+  kFlagNegPressure = 2u
+};
+
+// Host copy of one element type's tables; passed to kernels by value through the parameter
+// space (constant bank), see rds_tables.cuh.
+struct HostCellGroup
+{
+  rds_cell_group desc{};
+  std::vector<double> w, V, dV, dVgeo, dVf, Vsf;
+  int32_t *d_sol_conn = nullptr; // SoA [ndof][ncells]
+  int32_t *d_geo_conn = nullptr; // SoA [ngeo][ncells]
+  long long slot_base = 0;       // first contribution slot of this group
+  long long ws_base   = 0;       // first wave-speed slot of this group
+  bool affine         = false;   // simplex with straight edges: Jacobian constant per cell
+};
+
+struct HostBC
+{
+  rds_bc_group desc{};
+  std::vector<double> fw, fV, fdVgeo;
+  int32_t *d_sol_conn = nullptr; // SoA [nfdof][nfacets]
+  int32_t *d_geo_conn = nullptr; // SoA [nfgeo][nfacets]
+  double *d_gq        = nullptr; // [neq][nfq][nfacets]
+  long long slot_base = 0;
+  long long ws_base   = 0;
+};
+
+// Arguments common to every cell kernel.
+struct CellArgs
+{
+  int ncells;
+  int nnodes;
+  const int32_t *__restrict__ sol_conn; // SoA [ndof][ncells]
+  const int32_t *__restrict__ geo_conn; // SoA [ngeo][ncells]
+  const double *__restrict__ X;         // geometry coords SoA [dim][ngeo_nodes]
+  int ngeo_nodes;
+  const double *__restrict__ u; // state SoA [neq][nnodes]
+  double *__restrict__ contrib; // [neq][S], this group's slots start at slot_base
+  long long S;                  // total contribution slots
+  long long slot_base;
+  double *__restrict__ wsc; // wave-speed contributions, this group at ws_base
+  long long ws_base;
+  double adv0, adv1, adv2, gamma;
+  unsigned *status;
+  const int *stop; // nonzero: skip the work (converged loop)
+};
+
+struct BCArgs
+{
+  int nfacets;
+  const int32_t *__restrict__ sol_conn;
+  const int32_t *__restrict__ geo_conn;
+  const double *__restrict__ X;
+  int ngeo_nodes;
+  const double *__restrict__ u;
+  int nnodes;
+  const double *__restrict__ gq; // [neq][nfq][nfacets]
+  const double *__restrict__ vol;
+  double *__restrict__ contrib;
+  long long S;
+  long long slot_base;
+  double *__restrict__ wsc;
+  long long ws_base;
+  double adv0, adv1, gamma;
+  unsigned *status;
+  const int *stop;
+};
+
+struct GatherArgs
+{
+  int nnodes;
+  int neq;
+  const int32_t *__restrict__ row;     // [nnodes+1]
+  const int32_t *__restrict__ ent_slot; // [E]
+  const int32_t *__restrict__ ent_ws;   // [E]
+  const double *__restrict__ contrib;   // [neq][S]
+  long long S;
+  const double *__restrict__ wsc;
+  const double *__restrict__ vol;
+  const double *__restrict__ inv_vol;
+  double *__restrict__ res; // SoA [neq][nnodes]
+  double *__restrict__ ws;  // [nnodes]
+  double *__restrict__ dt;  // [nnodes]
+  double *__restrict__ u;   // SoA [neq][nnodes]
+  double *__restrict__ part; // [nblocks][neq] norm partial sums
+  double cfl;
+  const int *stop;
+};
+
+// ---- launchers (return cudaError_t of the launch) --------------------------------------
+// Cell residual kernels: dispatch over (physics, scheme, element type, order, precision).
+cudaError_t launch_cells(const HostCellGroup &g, const CellArgs &a, int physics, int scheme,
+                         int precision, int dim, int neq, cudaStream_t s, const char **name);
+cudaError_t launch_bc(const HostBC &b, const BCArgs &a, int physics, int dim, int neq,
+                      cudaStream_t s, const char **name);
+// Node gather: mode bit 0 = compute dt, bit 1 = update u, bit 2 = norm partials.
+cudaError_t launch_gather(const GatherArgs &a, int mode, int nblocks, cudaStream_t s,
+                          const char **name);
+cudaError_t launch_norm_final(const double *part, int nblocks, int neq, int nnodes,
+                              double *norm, double *norm0, double *hist, int *iter,
+                              int max_hist, double drop, int *stop, unsigned *status,
+                              cudaStream_t s, const char **name);
+cudaError_t launch_norm_partials(int nnodes, int neq, const double *res, const double *dt,
+                                 double *part, int nblocks, cudaStream_t s);
+cudaError_t launch_cell_volume_raw(int ncells, int dim, int nq, int ngeo, const int32_t *geo_conn,
+                                   const double *X, int ngeo_nodes, const double *w,
+                                   const double *dVgeo, double *cvol, cudaStream_t s);
+cudaError_t launch_cells_scalar(const HostCellGroup &g, const CellArgs &a, int physics,
+                                int scheme, int precision, cudaStream_t s, const char **name,
+                                bool *ok);
+cudaError_t launch_cells_euler(const HostCellGroup &g, const CellArgs &a, int physics,
+                               int scheme, int precision, cudaStream_t s, const char **name,
+                               bool *ok);
+cudaError_t launch_dual_volume(int nnodes, const int32_t *row, const int32_t *ent_ws,
+                               const double *cvol, double *vol, double *inv_vol, cudaStream_t s);
+cudaError_t launch_update(int nnodes, int neq, const double *dt, const double *res, double *u,
+                          cudaStream_t s, const char **name);
+
+} // namespace rds

@@ -1,0 +1,257 @@
+"""Host-side mirror of pdekit's explicit RDS solver interface over the librds_b200 C ABI.
+
+`PGRDMethodExplicit` keeps the reference's call sequence and names
+(src/solver/rdm/PGRDMethodExplicit.hpp:38-93, src/solver/rdm/RDMethod.hpp:60-139):
+
+    scheme = PGRDMethodExplicit(physics="burgers", scheme="b")
+    scheme.configure_mesh_data(problem)      # mesh, geometry and solution dofs, tables
+    scheme.add_boundary_condition(...)       # optional, weak BCs (or carried by the problem)
+    scheme.initialize_work_data()            # -> rds_finalize (gather lists, dual volumes)
+    scheme.set_solution(u)                   # SolverVecFn::solution
+    scheme.assemble_lhs_and_rhs(cfl); scheme.solve()
+    scheme.compute_residual_norm()
+
+Every call goes through librds_b200.so; there is no CPU fallback. If the library is absent the
+import fails loudly.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .problem import Problem
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librds_b200.so")
+
+PHYSICS = {"advconst": 0, "burgers": 1, "euler2d": 2, "euler3d": 3}
+SCHEME = {"lda": 0, "n": 1, "b": 2}
+PRECISION = {"fp64": 0, "mixed": 1}
+SHAPE = {"line": 2, "triag": 3, "quad": 4, "tetra": 10}
+BC_KIND = {"WeakDirichlet": 0}
+
+STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "NONFINITE", 4: "NEG_PRESSURE", 5: "ITER_CAP",
+          6: "UNSUPPORTED", 7: "TOO_LARGE"}
+
+# Symbols the C ABI exports (include/rds_b200.h).
+EXPORTS = ["rds_create", "rds_add_cell_group", "rds_add_bc", "rds_finalize", "rds_set_state",
+           "rds_get_state", "rds_assemble", "rds_assemble_rhs", "rds_update",
+           "rds_residual_norm", "rds_get_fields", "rds_iterate", "rds_stream",
+           "rds_kernel_timing", "rds_kernel_times", "rds_launch_count", "rds_destroy",
+           "rds_last_error", "rds_version"]
+
+
+class RDSError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"rds status {STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class _Desc(C.Structure):
+    _fields_ = [("physics", C.c_int), ("scheme", C.c_int), ("precision", C.c_int),
+                ("dim", C.c_int), ("neq", C.c_int), ("nnodes", C.c_int),
+                ("ngeo_nodes", C.c_int), ("geo_coords", C.c_void_p),
+                ("adv", C.c_double * 3), ("gamma", C.c_double)]
+
+
+class _CellGroup(C.Structure):
+    _fields_ = [("shape", C.c_int), ("order", C.c_int), ("ncells", C.c_int), ("ndof", C.c_int),
+                ("ngeo", C.c_int), ("nq", C.c_int), ("nfl", C.c_int),
+                ("sol_conn", C.c_void_p), ("geo_conn", C.c_void_p), ("w", C.c_void_p),
+                ("V", C.c_void_p), ("dV", C.c_void_p), ("dVgeo", C.c_void_p),
+                ("dVf", C.c_void_p), ("Vsf", C.c_void_p)]
+
+
+class _BCGroup(C.Structure):
+    _fields_ = [("kind", C.c_int), ("nfacets", C.c_int), ("nfdof", C.c_int),
+                ("nfgeo", C.c_int), ("nfq", C.c_int), ("sol_conn", C.c_void_p),
+                ("geo_conn", C.c_void_p), ("fw", C.c_void_p), ("fV", C.c_void_p),
+                ("fdVgeo", C.c_void_p), ("gq", C.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    """Load librds_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m pdekit_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, ip, dp = C.c_void_p, C.c_int, C.c_double
+    sig = {
+        "rds_create": ([C.POINTER(vp), vp, vp], ip),
+        "rds_add_cell_group": ([vp, vp], ip),
+        "rds_add_bc": ([vp, vp], ip),
+        "rds_finalize": ([vp], ip),
+        "rds_set_state": ([vp, vp], ip),
+        "rds_get_state": ([vp, vp], ip),
+        "rds_assemble": ([vp, dp], ip),
+        "rds_assemble_rhs": ([vp], ip),
+        "rds_update": ([vp], ip),
+        "rds_residual_norm": ([vp, vp], ip),
+        "rds_get_fields": ([vp, vp, vp, vp, vp], ip),
+        "rds_iterate": ([vp, dp, ip, dp, C.POINTER(ip), vp], ip),
+        "rds_stream": ([vp], vp),
+        "rds_kernel_timing": ([vp, ip], ip),
+        "rds_kernel_times": ([vp, vp, vp, vp, ip], ip),
+        "rds_launch_count": ([vp], C.c_longlong),
+        "rds_destroy": ([vp], ip),
+        "rds_last_error": ([vp], C.c_char_p),
+        "rds_version": ([], C.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class PGRDMethodExplicit:
+    """GPU drop-in for PGRDMethodExplicit<MeshConfig, Physics, Scheme> (one CUDA context)."""
+
+    def __init__(self, physics: str = "burgers", scheme: str = "b", precision: str = "fp64"):
+        self.physics, self.scheme, self.precision = physics, scheme, precision
+        self._ctx = None
+        self._keep = []
+        self.problem = None
+
+    # ---- set-up -------------------------------------------------------------------------------
+    def configure_mesh_data(self, prob: Problem):
+        """RDMethod::configure_mesh_data + the reference tables of initialize_work_data."""
+        L = lib()
+        if prob.physics != self.physics or prob.scheme != self.scheme:
+            # the problem description carries its physics; the scheme tag can be overridden
+            prob = Problem(**{**prob.__dict__, "physics": self.physics, "scheme": self.scheme})
+        self.problem = prob
+        coords = np.ascontiguousarray(prob.geo_coords, dtype=np.float64)
+        self._keep.append(coords)
+        d = _Desc()
+        d.physics = PHYSICS[self.physics]
+        d.scheme = SCHEME[self.scheme]
+        d.precision = PRECISION[self.precision]
+        d.dim, d.neq, d.nnodes = prob.dim, prob.neq, prob.nnodes
+        d.ngeo_nodes = coords.shape[0]
+        d.geo_coords = _ptr(coords)
+        for i, v in enumerate(prob.adv):
+            d.adv[i] = v
+        d.gamma = prob.gamma
+        ctx = C.c_void_p()
+        st = L.rds_create(C.byref(ctx), C.byref(d), None)
+        self._ctx = ctx
+        self._check(st)
+        for g in prob.groups:
+            arrs = [np.ascontiguousarray(g.sol_conn, dtype=np.int32),
+                    np.ascontiguousarray(g.geo_conn, dtype=np.int32)] + \
+                   [np.ascontiguousarray(x, dtype=np.float64) for x in
+                    (g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf)]
+            self._keep += arrs
+            cg = _CellGroup(SHAPE[g.shape], g.order, g.ncells, g.ndof, g.ngeo, g.nq, g.nfl,
+                            *[_ptr(a) for a in arrs])
+            self._check(L.rds_add_cell_group(self._ctx, C.byref(cg)))
+        for b in prob.bcs:
+            self.add_boundary_condition(b)
+        return self
+
+    def add_boundary_condition(self, b):
+        """RDMethod::add_boundary_condition for a weak condition with its boundary data."""
+        arrs = [np.ascontiguousarray(b.sol_conn, dtype=np.int32),
+                np.ascontiguousarray(b.geo_conn, dtype=np.int32)] + \
+               [np.ascontiguousarray(x, dtype=np.float64) for x in (b.fw, b.fV, b.fdVgeo, b.gq)]
+        self._keep += arrs
+        cb = _BCGroup(BC_KIND[b.kind], b.nfacets, b.nfdof, b.nfgeo, b.nfq,
+                      *[_ptr(a) for a in arrs])
+        self._check(lib().rds_add_bc(self._ctx, C.byref(cb)))
+
+    def initialize_work_data(self):
+        self._check(lib().rds_finalize(self._ctx))
+        return self
+
+    # ---- fields -------------------------------------------------------------------------------
+    def set_solution(self, u):
+        p = self.problem
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(p.nnodes, p.neq)
+        self._check(lib().rds_set_state(self._ctx, _ptr(u)))
+
+    def solution(self):
+        p = self.problem
+        u = np.empty((p.nnodes, p.neq))
+        self._check(lib().rds_get_state(self._ctx, _ptr(u)))
+        return u
+
+    def fields(self):
+        """(residual [n,neq], dt [n], nodal wave speed [n], dual volume [n])."""
+        p = self.problem
+        res = np.empty((p.nnodes, p.neq))
+        dt, ws, vol = np.empty(p.nnodes), np.empty(p.nnodes), np.empty(p.nnodes)
+        self._check(lib().rds_get_fields(self._ctx, _ptr(res), _ptr(dt), _ptr(ws), _ptr(vol)))
+        return res, dt, ws, vol
+
+    # ---- iteration ----------------------------------------------------------------------------
+    def assemble_lhs_and_rhs(self, cfl: float):
+        self._check(lib().rds_assemble(self._ctx, float(cfl)))
+
+    def assemble_rhs(self):
+        self._check(lib().rds_assemble_rhs(self._ctx))
+
+    def solve(self):
+        self._check(lib().rds_update(self._ctx))
+
+    def compute_residual_norm(self):
+        out = np.zeros(self.problem.neq)
+        self._check(lib().rds_residual_norm(self._ctx, _ptr(out)))
+        return out
+
+    def iterate(self, cfl: float, max_iter: int, drop: float = 0.0, raise_on_cap=True):
+        """Device loop of assemble_lhs_and_rhs + solve; returns (iterations, norm history)."""
+        hist = np.zeros((max_iter, self.problem.neq))
+        done = C.c_int(0)
+        st = lib().rds_iterate(self._ctx, float(cfl), int(max_iter), float(drop),
+                               C.byref(done), _ptr(hist))
+        if st == 5 and not raise_on_cap:
+            return done.value, hist[:done.value]
+        self._check(st)
+        return done.value, hist[:done.value]
+
+    # ---- diagnostics --------------------------------------------------------------------------
+    def stream_handle(self) -> int:
+        return lib().rds_stream(self._ctx) or 0
+
+    def kernel_timing(self, enable: bool):
+        self._check(lib().rds_kernel_timing(self._ctx, int(enable)))
+
+    def kernel_times(self):
+        names = (C.c_char * 32 * 64)()
+        ms = np.zeros(64)
+        cnt = np.zeros(64, dtype=np.int32)
+        n = lib().rds_kernel_times(self._ctx, names, _ptr(ms), _ptr(cnt), 64)
+        return {names[i].value.decode(): (float(ms[i]), int(cnt[i])) for i in range(n)}
+
+    def launch_count(self) -> int:
+        return int(lib().rds_launch_count(self._ctx))
+
+    def _check(self, st):
+        if st != 0:
+            msg = lib().rds_last_error(self._ctx).decode() if self._ctx else ""
+            raise RDSError(st, msg)
+
+    def close(self):
+        if self._ctx:
+            lib().rds_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

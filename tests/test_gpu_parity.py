@@ -1,0 +1,91 @@
+"""GPU parity through the C ABI: the CUDA path against the reference's golden vectors and the
+oracle, on the reference's own meshes, tables and states (tests/golden)."""
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden_cases
+from helpers import rel_err
+from oracle.rds_oracle import Oracle
+from pdekit_b200.problem import load_golden
+from pdekit_b200.rds import PGRDMethodExplicit
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12  # FP64 plain path: summation order only
+
+
+def _solver(prob, precision="fp64"):
+    s = PGRDMethodExplicit(prob.physics, prob.scheme, precision)
+    s.configure_mesh_data(prob)
+    s.initialize_work_data()
+    return s
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_first_assemble_matches_reference(case):
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    s = _solver(prob)
+    s.set_solution(a["u0"])
+    s.assemble_lhs_and_rhs(meta["cfl"])
+    res, dt, ws, vol = s.fields()
+    assert rel_err(vol, a["dual_volume"]) < TOL
+    assert rel_err(res, a["res1"]) < TOL
+    assert rel_err(ws, a["ws1"]) < TOL
+    assert rel_err(dt, a["dt1"]) < TOL
+    norm = s.compute_residual_norm()
+    np.testing.assert_allclose(norm, a["norms"][0], rtol=1e-11)
+    s.solve()
+    assert rel_err(s.solution(), a["u1"]) < TOL
+    s.close()
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_device_loop_matches_reference(case):
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    s = _solver(prob)
+    s.set_solution(a["u0"])
+    it, hist = s.iterate(meta["cfl"], meta["iters"])
+    assert it == meta["iters"]
+    assert rel_err(s.solution(), a["uK"]) < TOL
+    np.testing.assert_allclose(hist, a["norms"], rtol=1e-11)
+    s.close()
+
+
+@pytest.mark.parametrize("case", ["burgers_p2_b", "adv_p1_lda"])
+def test_bitwise_repeatable(case):
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    outs = []
+    for _ in range(2):
+        s = _solver(prob)
+        s.set_solution(a["u0"])
+        s.iterate(meta["cfl"], 7)
+        outs.append(s.solution())
+        s.close()
+    assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("case", ["burgers_p2_b", "adv_p1_lda", "adv_p2_b", "burgers_p3_b"])
+def test_gpu_matches_oracle_many_iterations(case):
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    s = _solver(prob)
+    s.set_solution(a["u0"])
+    s.iterate(meta["cfl"], 40)
+    u_gpu = s.solution()
+    s.close()
+    u_ref, _ = Oracle(prob).iterate(a["u0"], meta["cfl"], 40)
+    assert rel_err(u_gpu, u_ref) < 1e-11
+
+
+@pytest.mark.parametrize("case", ["burgers_p2_b", "adv_p1_lda"])
+def test_mixed_precision_close_to_fp64(case):
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    s = _solver(prob, "mixed")
+    s.set_solution(a["u0"])
+    s.assemble_lhs_and_rhs(meta["cfl"])
+    res, dt, ws, vol = s.fields()
+    s.close()
+    assert rel_err(res, a["res1"]) < 1e-5  # FP32 interpolation / flux / upwind terms
+    assert rel_err(ws, a["ws1"]) < 1e-6
