@@ -179,7 +179,15 @@ RDS_API rds_status rds_get_fields(rds_ctx *ctx, double *res_aos, double *dt, dou
 RDS_API rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int *it_done,
                        double *hist);
 
+/* Enqueue n fused iterations (assemble_lhs_and_rhs(cfl) + solve()) on the context's stream and
+ * return without waiting: no residual-drop test, no copies back. For timing with events on
+ * rds_stream(); the norms of these iterations are not kept. */
+RDS_API rds_status rds_run(rds_ctx *ctx, double cfl, int n);
+
 /* Diagnostics. */
+/* Measured CUDA-core FMA throughput of this GPU in TFLOP/s (precision: RDS_FP64 or RDS_MIXED
+ * for FP32), the roofline denominator of the cell kernels. */
+RDS_API rds_status rds_measure_peak(int precision, double *tflops);
 RDS_API void *rds_stream(rds_ctx *ctx); /* the cudaStream_t the context launches on */
 /* Per-kernel device time over the launches since the last reset (enable = 1 starts event
  * timing around every launch, 0 stops it). names: up to max entries of 32 chars. */

@@ -872,6 +872,32 @@ rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int 
   return RDS_OK;
 }
 
+rds_status rds_run(rds_ctx *ctx, double cfl, int n)
+{
+  if (!ctx || !ctx->finalized || n <= 0)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_run: not finalized or n <= 0") : RDS_ERR_INVALID;
+  // plain launches (event timing, if enabled, brackets each kernel); the stop flag stays 0
+  rds_status st;
+  if (!ctx->d_hist)
+  {
+    if ((st = dalloc(ctx, &ctx->d_hist, (size_t)ctx->desc.neq)) != RDS_OK)
+      return st;
+    ctx->hist_cap = 1;
+  }
+  for (int i = 0; i < n; ++i)
+  {
+    if ((st = launch_residual_kernels(ctx, ctx->d_zero)) != RDS_OK)
+      return st;
+    const GatherArgs ga = gather_args(ctx, cfl, ctx->d_zero);
+    st = launch(ctx, [&](const char **name) {
+      return launch_gather(ga, 7, ctx->gblocks, ctx->stream, name);
+    });
+    if (st != RDS_OK)
+      return st;
+  }
+  return RDS_OK;
+}
+
 rds_status rds_kernel_timing(rds_ctx *ctx, int enable)
 {
   if (!ctx)

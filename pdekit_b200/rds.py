@@ -41,7 +41,7 @@ EXPORTS = ["rds_create", "rds_add_cell_group", "rds_add_bc", "rds_finalize", "rd
            "rds_get_state", "rds_assemble", "rds_assemble_rhs", "rds_update",
            "rds_residual_norm", "rds_get_fields", "rds_iterate", "rds_stream",
            "rds_kernel_timing", "rds_kernel_times", "rds_launch_count", "rds_destroy",
-           "rds_last_error", "rds_version"]
+           "rds_last_error", "rds_version", "rds_run", "rds_measure_peak"]
 
 
 class RDSError(RuntimeError):
@@ -104,6 +104,8 @@ def lib():
         "rds_destroy": ([vp], ip),
         "rds_last_error": ([vp], C.c_char_p),
         "rds_version": ([], C.c_char_p),
+        "rds_run": ([vp, dp, ip], ip),
+        "rds_measure_peak": ([ip, vp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -115,6 +117,15 @@ def lib():
 
 def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
+
+
+def measure_peak(precision: str = "fp64") -> float:
+    """Measured CUDA-core FMA peak of the current GPU in TFLOP/s."""
+    out = np.zeros(1)
+    st = lib().rds_measure_peak(PRECISION[precision], _ptr(out))
+    if st != 0:
+        raise RDSError(st, "rds_measure_peak failed")
+    return float(out[0])
 
 
 class PGRDMethodExplicit:
@@ -183,9 +194,9 @@ class PGRDMethodExplicit:
         u = np.ascontiguousarray(u, dtype=np.float64).reshape(p.nnodes, p.neq)
         self._check(lib().rds_set_state(self._ctx, _ptr(u)))
 
-    def solution(self):
+    def solution(self, out=None):
         p = self.problem
-        u = np.empty((p.nnodes, p.neq))
+        u = np.empty((p.nnodes, p.neq)) if out is None else out
         self._check(lib().rds_get_state(self._ctx, _ptr(u)))
         return u
 
@@ -222,6 +233,10 @@ class PGRDMethodExplicit:
             return done.value, hist[:done.value]
         self._check(st)
         return done.value, hist[:done.value]
+
+    def run(self, cfl: float, n: int):
+        """Enqueue n fused iterations without waiting (for event timing on stream_handle())."""
+        self._check(lib().rds_run(self._ctx, float(cfl), int(n)))
 
     # ---- diagnostics --------------------------------------------------------------------------
     def stream_handle(self) -> int:

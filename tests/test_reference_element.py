@@ -1,0 +1,69 @@
+"""Host-side reference-element tables against the reference's own tables (golden) and against
+polynomial exactness (CPU)."""
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from pdekit_b200 import reference_element as re_
+from pdekit_b200.problem import load_golden
+
+CASES = {(1, 4): "adv_p1_lda", (2, 5): "burgers_p2_b", (3, 8): "burgers_p3_b"}
+
+
+def _match_rows(a, b, tol=1e-13):
+    """Permutation mapping rows of a onto rows of b (points of a rule in another order)."""
+    perm = []
+    for row in a:
+        d = np.abs(b - row).max(axis=1)
+        k = int(np.argmin(d))
+        assert d[k] < tol, (row, d[k])
+        perm.append(k)
+    assert len(set(perm)) == len(perm)
+    return np.asarray(perm)
+
+
+@pytest.mark.parametrize("p,q", sorted(CASES))
+def test_tables_match_reference(p, q):
+    _, a, _ = load_golden(os.path.join(GOLDEN, CASES[(p, q)]))
+    t = re_.triag_tables(p, q)
+    perm = _match_rows(t["qp"], a["qp"])  # same point set, possibly another order
+    np.testing.assert_allclose(t["w"], a["w"][perm], rtol=0, atol=1e-14)
+    np.testing.assert_allclose(t["V"], a["V"][perm], rtol=0, atol=1e-13)
+    for d in range(2):
+        np.testing.assert_allclose(t["dV"][d], a[f"dV{d}"][perm], rtol=0, atol=1e-12)
+        np.testing.assert_allclose(t["dVgeo"][d], a[f"dVgeo{d}"][perm], rtol=0, atol=1e-13)
+        np.testing.assert_allclose(t["dVf"][d], a[f"dVf{d}"][perm], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(t["Vsf"], a["Vsf"], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(t["fqp"], a["fqp"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(t["fw"], a["fw"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(t["fV"], a["fV"], rtol=0, atol=1e-14)
+    np.testing.assert_allclose(t["fdVgeo"][0], a["fdVgeo0"], rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("order", [1, 2, 4, 5, 8])
+def test_triangle_rules_exact(order):
+    qp, w = re_.triag_gauss(order)
+    assert abs(w.sum() - 2.0) < 1e-14
+    # integrate (1+xi)^a (1+eta)^b over the reference triangle exactly:
+    # 2^(a+b+2) a! b! / (a+b+2)! on the triangle of area 2
+    from math import factorial
+    for a_ in range(order + 1):
+        for b_ in range(order + 1 - a_):
+            exact = 2.0 ** (a_ + b_ + 2) * factorial(a_) * factorial(b_) / factorial(a_ + b_ + 2)
+            got = (w * (1 + qp[:, 0]) ** a_ * (1 + qp[:, 1]) ** b_).sum()
+            assert abs(got - exact) < 1e-13 * max(1.0, exact), (a_, b_)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_lagrange_partition_of_unity_and_kronecker(p):
+    from pdekit_b200 import meshgen
+    nodes = meshgen.equidist_triag_nodes(p)
+    V, dV = re_.lagrange_triag(p, nodes)
+    np.testing.assert_allclose(V, np.eye(nodes.shape[0]), atol=1e-14)
+    qp, _ = re_.triag_gauss(8)
+    V, dV = re_.lagrange_triag(p, qp)
+    np.testing.assert_allclose(V.sum(axis=1), 1.0, atol=1e-14)
+    np.testing.assert_allclose(dV.sum(axis=2), 0.0, atol=1e-12)
