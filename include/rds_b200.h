@@ -196,6 +196,22 @@ RDS_API int rds_kernel_times(rds_ctx *ctx, char (*names)[32], double *ms, int *l
 /* Kernel launches issued by this context since creation. */
 RDS_API long long rds_launch_count(rds_ctx *ctx);
 
+/* Residual norm for callers that cannot allocate device memory (no counterpart in the
+ * reference, whose norm runs on the host). For a solver whose device memory belongs to
+ * another allocator, or a loop that cannot take the device-wide synchronisation of
+ * cudaMalloc/cudaFree: the same result as rds_residual_norm, computed from caller-owned DEVICE
+ * arrays, with no context and no allocation of any kind.
+ *   res  [neq][nnodes] (SoA), dt [nnodes], norm [neq] output: device pointers
+ *   stream: cudaStream_t to run on (NULL = default stream); the call only enqueues work.
+ * Scratch is a fixed device array inside this library, sized for RDS_NOALLOC_MAX_NODES nodes
+ * and 5 equations (1.25 MiB per GPU, held until the process exits); larger inputs get
+ * RDS_ERR_TOO_LARGE. Its address is looked up in the first call on each device, so make that
+ * first call before any stream capture. All calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller. */
+#define RDS_NOALLOC_MAX_NODES (32768 * 256)
+RDS_API rds_status rds_residual_norm_noalloc(const double *res, const double *dt, int nnodes,
+                                             int neq, double *norm, void *stream);
+
 RDS_API rds_status rds_destroy(rds_ctx *ctx);
 RDS_API const char *rds_last_error(rds_ctx *ctx);
 RDS_API const char *rds_version(void);
