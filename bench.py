@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--n", type=int, default=512, help="squares per side (512 = configuration 2)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-drop", action="store_true", help="skip the time-to-drop runs")
+    ap.add_argument("--drop-max-iter", type=int, default=400000)
     ap.add_argument("--quick", action="store_true",
                     help="only warm-up + timed steps (profiling runs): no e2e, mixed, drop, CPU")
     return ap.parse_args()
@@ -188,11 +189,11 @@ def roofline_cell_kernel(ms_per_launch, ncells, peak_fp64, hbm_gbs):
     Per cell (ndof 6, nq 7, nfl 10, affine P1 geometry), counting an FMA as 2 flops:
       flux nodes 10 x (11 + 2) = 130, Jacobian + inverse 28,
       per quadrature point: weights 2, flux divergence 76 + 7, u_q 11, upwind coefficients
-      6 x 10, LDA part 2 + 6 x 4, N dissipation 6 x 19  -> 297, x 7 = 2079,
-      blending and output 27            => 2264 flop / cell.
+      6 x 10, LDA part 2 + 6 x 4, N dissipation 12 + 6 x 6  -> 231, x 7 = 1617,
+      blending and output 27            => 1802 flop / cell.
     Bytes per cell (each touched once): dof + vertex indices 9 x 4, coordinates 3 x 16,
       nodal states 6 x 8, contribution writes 6 x 8 + wave speed 8 => 188 B / cell."""
-    flop = 2264.0 * ncells
+    flop = 1802.0 * ncells
     byts = 188.0 * ncells
     s = ms_per_launch * 1e-3
     achieved = flop / s / 1e12
@@ -201,7 +202,7 @@ def roofline_cell_kernel(ms_per_launch, ncells, peak_fp64, hbm_gbs):
             "peak_source": "measured in this run: rds_measure_peak (FP64 FMA micro-kernel)",
             "hbm_achieved_gbs": round(byts / s / 1e9, 1), "hbm_peak_gbs": hbm_gbs,
             "hbm_frac": round(byts / s / 1e9 / hbm_gbs, 4),
-            "traffic": None, "kernel": "cells_burgers_b", "flop_per_cell": 2264,
+            "traffic": None, "kernel": "cells_burgers_b", "flop_per_cell": 1802,
             "bytes_per_cell": 188}
 
 
@@ -290,13 +291,13 @@ def run_ours(args, rank, world, local):
 
     # time to a 1e-10 residual drop (device loop with the device-side stop test)
     drop = None
-    if not args.no_drop:
+    if not args.no_drop and world == 1:
         drop = {}
         for name, s in (("fp64", solver),):
             s.set_solution(u0)
             torch.cuda.synchronize()
             t0 = time.time()
-            it, hist = s.iterate(CFL, 20000, 1e-10, raise_on_cap=False)
+            it, hist = s.iterate(CFL, args.drop_max_iter, 1e-10, raise_on_cap=False)
             torch.cuda.synchronize()
             rel = float((hist[-1] / hist[0]).max()) if len(hist) else None
             drop[name] = {"seconds": round(time.time() - t0, 4), "iterations": it,

@@ -31,6 +31,8 @@ struct rds_ctx
   rds_desc desc{};
   int device             = 0;
   cudaStream_t stream    = nullptr;
+  cudaStream_t side      = nullptr; // boundary kernels, concurrent with the cell kernels
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool own_stream        = false;
   bool finalized         = false;
   std::string err;
@@ -53,6 +55,7 @@ struct rds_ctx
   double *d_part = nullptr, *d_norm = nullptr, *d_norm0 = nullptr, *d_hist = nullptr;
   int *d_iter = nullptr, *d_stop = nullptr, *d_zero = nullptr;
   unsigned *d_status = nullptr;
+  unsigned *d_counter = nullptr; // blocks done in the fused gather (last-block reduction)
   long long S = 0, W = 0, E = 0;
   int gblocks   = 0;
   int hist_cap  = 0;
@@ -103,16 +106,17 @@ cudaEvent_t get_event(rds_ctx *ctx)
   return e;
 }
 
-// Launch wrapper: optional event timing around the launch, launch counting, error text.
+// Launch wrapper: optional event timing around the launch (on the stream it is issued to),
+// launch counting, error text.
 template <typename F>
-rds_status launch(rds_ctx *ctx, F &&f)
+rds_status launch_on(rds_ctx *ctx, cudaStream_t s, F &&f)
 {
   cudaEvent_t a = nullptr, b = nullptr;
   if (ctx->timing)
   {
     a = get_event(ctx);
     b = get_event(ctx);
-    cudaEventRecord(a, ctx->stream);
+    cudaEventRecord(a, s);
   }
   const char *name = "?";
   cudaError_t e    = f(&name);
@@ -124,10 +128,16 @@ rds_status launch(rds_ctx *ctx, F &&f)
   ctx->launches++;
   if (ctx->timing)
   {
-    cudaEventRecord(b, ctx->stream);
+    cudaEventRecord(b, s);
     ctx->trecs.push_back({name, a, b});
   }
   return RDS_OK;
+}
+
+template <typename F>
+rds_status launch(rds_ctx *ctx, F &&f)
+{
+  return launch_on(ctx, ctx->stream, f);
 }
 
 template <typename T>
@@ -249,9 +259,27 @@ GatherArgs gather_args(rds_ctx *ctx, double cfl, const int *stop)
 }
 
 // Residual contributions of all cells and boundary facets (assemble_rhs without the gather).
+// The boundary-facet kernels only touch their own contribution slots, so they run on a side
+// stream concurrently with the cell kernels (a parallel branch when captured in a graph) and
+// join the main stream before the gather.
 rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
 {
   const rds_desc &d = ctx->desc;
+  const bool fork   = !ctx->bcs.empty();
+  if (fork)
+  {
+    RDS_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
+    RDS_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+  }
+  for (const HostBC &b : ctx->bcs)
+  {
+    const BCArgs a = bc_args(ctx, b, stop);
+    rds_status st  = launch_on(ctx, ctx->side, [&](const char **name) {
+      return launch_bc(b, a, d.physics, d.dim, d.neq, ctx->side, name);
+    });
+    if (st != RDS_OK)
+      return st;
+  }
   for (const HostCellGroup &g : ctx->groups)
   {
     const CellArgs a = cell_args(ctx, g, stop);
@@ -261,14 +289,10 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
     if (st != RDS_OK)
       return st;
   }
-  for (const HostBC &b : ctx->bcs)
+  if (fork)
   {
-    const BCArgs a = bc_args(ctx, b, stop);
-    rds_status st  = launch(ctx, [&](const char **name) {
-      return launch_bc(b, a, d.physics, d.dim, d.neq, ctx->stream, name);
-    });
-    if (st != RDS_OK)
-      return st;
+    RDS_CUDA(cudaEventRecord(ctx->ev_join, ctx->side));
+    RDS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
   }
   return RDS_OK;
 }
@@ -370,6 +394,9 @@ rds_status rds_create(rds_ctx **out, const rds_desc *desc, void *stream)
     RDS_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     ctx->own_stream = true;
   }
+  RDS_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+  RDS_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+  RDS_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
   rds_status st;
   const size_t ng = (size_t)d.ngeo_nodes;
   std::vector<double> X(ng * d.dim);
@@ -578,7 +605,8 @@ rds_status rds_finalize(rds_ctx *ctx)
       (st = dalloc(ctx, &ctx->d_part, (size_t)ctx->gblocks * NEQ)) ||
       (st = dalloc(ctx, &ctx->d_norm, NEQ)) || (st = dalloc(ctx, &ctx->d_norm0, NEQ)) ||
       (st = dalloc(ctx, &ctx->d_iter, 1)) || (st = dalloc(ctx, &ctx->d_stop, 1)) ||
-      (st = dalloc(ctx, &ctx->d_zero, 1)) || (st = dalloc(ctx, &ctx->d_status, 1)))
+      (st = dalloc(ctx, &ctx->d_zero, 1)) || (st = dalloc(ctx, &ctx->d_status, 1)) ||
+      (st = dalloc(ctx, &ctx->d_counter, 1)))
     return st;
   RDS_CUDA(cudaMallocHost(&ctx->h_stop, sizeof(int)));
   RDS_CUDA(cudaMemsetAsync(ctx->d_u, 0, (size_t)N * NEQ * sizeof(double), ctx->stream));
@@ -588,6 +616,7 @@ rds_status rds_finalize(rds_ctx *ctx)
   RDS_CUDA(cudaMemsetAsync(ctx->d_zero, 0, sizeof(int), ctx->stream));
   RDS_CUDA(cudaMemsetAsync(ctx->d_stop, 0, sizeof(int), ctx->stream));
   RDS_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned), ctx->stream));
   RDS_CUDA(cudaMemsetAsync(ctx->d_wsc, 0, (size_t)W * sizeof(double), ctx->stream));
   if ((st = upload(ctx, ctx->d_row, count.data(), N + 1)) ||
       (st = upload(ctx, ctx->d_ent_slot, ent_slot.data(), E)) ||
@@ -754,16 +783,19 @@ static rds_status enqueue_iteration(rds_ctx *ctx, double cfl, int max_iter, doub
   rds_status st = launch_residual_kernels(ctx, ctx->d_stop);
   if (st != RDS_OK)
     return st;
-  const GatherArgs ga = gather_args(ctx, cfl, ctx->d_stop);
-  st = launch(ctx, [&](const char **name) {
-    return launch_gather(ga, 7, ctx->gblocks, ctx->stream, name);
-  });
-  if (st != RDS_OK)
-    return st;
+  // gather + dt + update + norm, with the final reduction and stop test done by the last block
+  GatherArgs ga = gather_args(ctx, cfl, ctx->d_stop);
+  ga.counter    = ctx->d_counter;
+  ga.norm       = ctx->d_norm;
+  ga.norm0      = ctx->d_norm0;
+  ga.hist       = ctx->d_hist;
+  ga.iter       = ctx->d_iter;
+  ga.max_iter   = max_iter;
+  ga.drop       = drop;
+  ga.stop_w     = ctx->d_stop;
+  ga.status     = ctx->d_status;
   return launch(ctx, [&](const char **name) {
-    return launch_norm_final(ctx->d_part, ctx->gblocks, ctx->desc.neq, ctx->desc.nnodes,
-                             ctx->d_norm, ctx->d_norm0, ctx->d_hist, ctx->d_iter, max_iter, drop,
-                             ctx->d_stop, ctx->d_status, ctx->stream, name);
+    return launch_gather(ga, 15, ctx->gblocks, ctx->stream, name);
   });
 }
 
@@ -828,7 +860,7 @@ rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int 
       ctx->graph_drop     = drop;
       ctx->graph_chunk    = chunk;
     }
-    const long long per_iter = (long long)ctx->groups.size() + (long long)ctx->bcs.size() + 2;
+    const long long per_iter = (long long)ctx->groups.size() + (long long)ctx->bcs.size() + 1;
     const int nchunks        = (max_iter + chunk - 1) / chunk;
     for (int k = 0; k < nchunks; ++k)
     {
@@ -948,6 +980,8 @@ rds_status rds_destroy(rds_ctx *ctx)
     return RDS_OK;
   if (ctx->stream)
     cudaStreamSynchronize(ctx->stream);
+  if (ctx->side)
+    cudaStreamSynchronize(ctx->side);
   release_graph(ctx);
   for (HostCellGroup &g : ctx->groups)
   {
@@ -964,7 +998,7 @@ rds_status rds_destroy(rds_ctx *ctx)
                   ctx->d_vol,   ctx->d_inv_vol, ctx->d_contrib, ctx->d_wsc,    ctx->d_stage,
                   ctx->d_row,   ctx->d_ent_slot, ctx->d_ent_ws, ctx->d_part,   ctx->d_norm,
                   ctx->d_norm0, ctx->d_hist,  ctx->d_iter,    ctx->d_stop,     ctx->d_zero,
-                  ctx->d_status};
+                  ctx->d_status, ctx->d_counter};
   for (void *p : bufs)
     if (p)
       cudaFree(p);
@@ -977,6 +1011,12 @@ rds_status rds_destroy(rds_ctx *ctx)
   }
   for (cudaEvent_t e : ctx->ev_pool)
     cudaEventDestroy(e);
+  if (ctx->ev_fork)
+    cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join)
+    cudaEventDestroy(ctx->ev_join);
+  if (ctx->side)
+    cudaStreamDestroy(ctx->side);
   if (ctx->own_stream && ctx->stream)
     cudaStreamDestroy(ctx->stream);
   delete ctx;

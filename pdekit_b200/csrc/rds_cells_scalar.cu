@@ -177,15 +177,17 @@ __global__ void __launch_bounds__(kBlock)
     }
     if (SCHEME != RDS_PGLDA)
     {
+      // sum_{m != n} K+_m (u_n - u_m) = u_n sum_m K+_m - sum_m K+_m u_m (the m = n terms
+      // cancel), so the N dissipation costs O(ndof) per point instead of O(ndof^2)
+      double tku = 0.0;
+#pragma unroll
+      for (int m = 0; m < NDOF; ++m)
+        tku += double(kp[m]) * ud[m];
+      const double sk = double(sumkp);
 #pragma unroll
       for (int n = 0; n < NDOF; ++n)
       {
-        // sum_{m != n} K+_m (u_n - u_m), differences taken on the FP64 nodal values
-        double s = 0.0;
-#pragma unroll
-        for (int m = 0; m < NDOF; ++m)
-          if (m != n)
-            s += double(kp[m]) * (ud[n] - ud[m]);
+        const double s = ud[n] * sk - tku;
         diss[n] += wj * ((double(kp[n]) * inv) * s);
       }
     }

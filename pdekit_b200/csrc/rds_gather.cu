@@ -39,7 +39,11 @@ __device__ __forceinline__ double block_sum(double v, double *smem)
   return s; // valid in thread 0
 }
 
-template <int NEQ, bool DT, bool UPDATE, bool NORM>
+__device__ void reduce_final(const double *part, int nblocks, int neq, int nnodes, double *norm,
+                             double *norm0, double *hist, int *iter, int max_iter, double drop,
+                             int *stop, unsigned *status, double *smem, double *nv);
+
+template <int NEQ, bool DT, bool UPDATE, bool NORM, bool FINAL>
 __global__ void __launch_bounds__(kGBlock) gather_nodes(const GatherArgs a)
 {
   __shared__ double smem[kGBlock / 32];
@@ -101,6 +105,28 @@ __global__ void __launch_bounds__(kGBlock) gather_nodes(const GatherArgs a)
       if (threadIdx.x == 0)
         a.part[(size_t)blockIdx.x * NEQ + e] = s;
     }
+    if (FINAL)
+    {
+      // last-block-done: the block that finishes last reduces all partials (fixed order), so
+      // the norm needs no separate launch; no block ever waits for another
+      __shared__ bool last;
+      __shared__ double nv[kMaxNeq];
+      if (threadIdx.x == 0)
+      {
+        __threadfence();
+        const unsigned done = atomicAdd(a.counter, 1u);
+        last                = (done == gridDim.x - 1);
+      }
+      __syncthreads();
+      if (last)
+      {
+        __threadfence();
+        reduce_final(a.part, gridDim.x, NEQ, a.nnodes, a.norm, a.norm0, a.hist, a.iter,
+                     a.max_iter, a.drop, a.stop_w, a.status, smem, nv);
+        if (threadIdx.x == 0)
+          *a.counter = 0u;
+      }
+    }
   }
 }
 
@@ -128,19 +154,16 @@ __global__ void __launch_bounds__(kGBlock)
 
 // Final reduction of the block partials in a fixed order, norm = sqrt(sum / N), the
 // iteration counter, the history and the device-side residual-drop / finiteness test.
-__global__ void __launch_bounds__(kGBlock)
-    norm_final(const double *part, int nblocks, int neq, int nnodes, double *norm, double *norm0,
-               double *hist, int *iter, int max_iter, double drop, int *stop, unsigned *status)
+// Executed by one whole block (norm_final, or the last block of a fused gather).
+__device__ void reduce_final(const double *part, int nblocks, int neq, int nnodes, double *norm,
+                             double *norm0, double *hist, int *iter, int max_iter, double drop,
+                             int *stop, unsigned *status, double *smem, double *nv)
 {
-  __shared__ double smem[kGBlock / 32];
-  __shared__ double nv[kMaxNeq];
-  if (stop != nullptr && *stop)
-    return;
   for (int e = 0; e < neq; ++e)
   {
     double s = 0.0;
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-      s += part[(size_t)b * neq + e];
+      s += __ldcg(part + (size_t)b * neq + e);
     s = block_sum<kGBlock>(s, smem);
     if (threadIdx.x == 0)
       nv[e] = sqrt(s / nnodes);
@@ -180,6 +203,18 @@ __global__ void __launch_bounds__(kGBlock)
   {
     *stop = 1;
   }
+}
+
+__global__ void __launch_bounds__(kGBlock)
+    norm_final(const double *part, int nblocks, int neq, int nnodes, double *norm, double *norm0,
+               double *hist, int *iter, int max_iter, double drop, int *stop, unsigned *status)
+{
+  __shared__ double smem[kGBlock / 32];
+  __shared__ double nv[kMaxNeq];
+  if (stop != nullptr && *stop)
+    return;
+  reduce_final(part, nblocks, neq, nnodes, norm, norm0, hist, iter, max_iter, drop, stop, status,
+               smem, nv);
 }
 
 __global__ void update_kernel(int n, const double *dt, const double *res, double *u, int neq)
@@ -254,13 +289,16 @@ cudaError_t launch_gather_neq(const GatherArgs &a, int mode, int nblocks, cudaSt
   switch (mode)
   {
   case 0:
-    gather_nodes<NEQ, false, false, false><<<nblocks, kGBlock, 0, s>>>(a);
+    gather_nodes<NEQ, false, false, false, false><<<nblocks, kGBlock, 0, s>>>(a);
     break;
   case 1:
-    gather_nodes<NEQ, true, false, false><<<nblocks, kGBlock, 0, s>>>(a);
+    gather_nodes<NEQ, true, false, false, false><<<nblocks, kGBlock, 0, s>>>(a);
     break;
   case 7:
-    gather_nodes<NEQ, true, true, true><<<nblocks, kGBlock, 0, s>>>(a);
+    gather_nodes<NEQ, true, true, true, false><<<nblocks, kGBlock, 0, s>>>(a);
+    break;
+  case 15:
+    gather_nodes<NEQ, true, true, true, true><<<nblocks, kGBlock, 0, s>>>(a);
     break;
   default:
     return cudaErrorInvalidValue;
@@ -273,7 +311,8 @@ cudaError_t launch_gather_neq(const GatherArgs &a, int mode, int nblocks, cudaSt
 cudaError_t launch_gather(const GatherArgs &a, int mode, int nblocks, cudaStream_t s,
                           const char **name)
 {
-  *name = (mode == 7) ? "gather_update_norm" : "gather_nodes";
+  *name = (mode == 15) ? "gather_update_norm_final" : (mode == 7) ? "gather_update_norm"
+                                                                   : "gather_nodes";
   switch (a.neq)
   {
   case 1:

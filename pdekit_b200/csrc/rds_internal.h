@@ -108,6 +108,14 @@ struct GatherArgs
   double *__restrict__ part; // [nblocks][neq] norm partial sums
   double cfl;
   const int *stop;
+  // fused final reduction (mode bit 3): the last block to finish reduces the partials
+  unsigned *counter; // blocks done; reset to 0 by the last block
+  double *norm, *norm0, *hist;
+  int *iter;
+  int max_iter;
+  double drop;
+  int *stop_w;
+  unsigned *status;
 };
 
 // ---- launchers (return cudaError_t of the launch) --------------------------------------
