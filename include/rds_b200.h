@@ -127,6 +127,12 @@ typedef struct
   const double *dVgeo; /* [dim][nq][ngeo]  reference derivatives of the geometry basis */
   const double *dVf;   /* [dim][nq][nfl]   reference derivatives of the flux basis */
   const double *Vsf;   /* [nfl][ndof]      solution basis at the flux nodes */
+  /* Optional rule for the dual (cell) volumes, sum_q wv_q detJ_q: the reference uses the Gauss
+   * rule of the cell's own polynomial order (src/solver/rdm/RDTimeUpdate.hpp:85-150). nqv = 0
+   * uses the rule above. */
+  int nqv;
+  const double *wv;      /* [nqv] */
+  const double *dVgeo_v; /* [dim][nqv][ngeo] */
 } rds_cell_group;
 
 /* One weak boundary condition on a set of boundary facets, traversed in the given order

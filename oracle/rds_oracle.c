@@ -675,11 +675,15 @@ void rdso_dual_volume(const rdso_model *m, const rdso_cells *groups, int ngroups
         for (int d = 0; d < D; ++d)
           X[k * D + d] = geo_coords[(size_t)g->geo_conn[(size_t)c * g->ngeo + k] * D + d];
       double cv = 0.0;
-      for (int q = 0; q < g->nq; ++q)
+      /* RDTimeUpdate::setup (RDTimeUpdate.hpp:118-177): Gauss rule of the cell's order */
+      const int nqv        = g->nqv > 0 ? g->nqv : g->nq;
+      const double *wv     = g->nqv > 0 ? g->wv : g->w;
+      const double *dvgeo  = g->nqv > 0 ? g->dVgeo_v : g->dVgeo;
+      for (int q = 0; q < nqv; ++q)
       {
         double invJ[DIM_MAX][DIM_MAX];
-        const double dj = jacobian(D, g->dVgeo, g->nq, g->ngeo, q, X, invJ);
-        cv += g->w[q] * dj;
+        const double dj = jacobian(D, dvgeo, nqv, g->ngeo, q, X, invJ);
+        cv += wv[q] * dj;
       }
       for (int n = 0; n < g->ndof; ++n)
         vol[g->sol_conn[(size_t)c * g->ndof + n]] += cv;
@@ -687,9 +691,24 @@ void rdso_dual_volume(const rdso_model *m, const rdso_cells *groups, int ngroups
   }
 }
 
-/* Weak Dirichlet facet residual (WeakDirichletBC.hpp:159-265) plus the rescaling to the
- * facet total (WeakBC.hpp:786-832) and the nodal accumulation (WeakBC.hpp:315-352). */
-static int apply_weak_dirichlet(const rdso_model *m, const rdso_bc *b, const double *geo_coords,
+/* Euler flux through a direction n (Euler2DCons::flux(p, direction, flux),
+ * physics/euler/Euler2DCons.hpp:253-266; Euler3DCons.hpp:267-285). */
+static void euler_flux_normal(const rdso_model *m, const props_t *p, const double *n, double *F)
+{
+  const int D = m->dim;
+  double rhoum = p->vars[1] * n[0] + p->vars[2] * n[1];
+  if (D == 3)
+    rhoum = p->vars[1] * n[0] + p->vars[2] * n[1] + p->vars[3] * n[2];
+  F[0] = rhoum;
+  for (int d = 0; d < D; ++d)
+    F[1 + d] = rhoum * p->V[d] + p->P * n[d];
+  F[D + 1] = rhoum * p->H;
+}
+
+/* Weak boundary-facet residuals: WeakDirichlet (WeakDirichletBC.hpp:159-265), WeakWall,
+ * WeakSubInlet, WeakSubOutlet, plus the rescaling to the facet total (WeakBC.hpp:786-832) and
+ * the nodal accumulation (WeakBC.hpp:315-352). */
+static int apply_weak_bc(const rdso_model *m, const rdso_bc *b, const double *geo_coords,
                                 const double *vol, const double *u, double *res, double *ws)
 {
   const int D = m->dim, NEQ = m->neq;
@@ -768,29 +787,92 @@ static int apply_weak_dirichlet(const rdso_model *m, const rdso_bc *b, const dou
       double eig[NEQ_MAX], Km[NEQ_MAX][NEQ_MAX];
       build_K(m, &p, nrm, -1, eig, Km);
 
-      double eig_max = 1.e-9, ghost[NEQ_MAX];
-      const double *gq = b->gq + ((size_t)f * b->nfq + q) * NEQ;
+      double eig_max = 1.e-9, ghost[NEQ_MAX], gflux[NEQ_MAX];
       for (int e = 0; e < NEQ; ++e)
       {
         const double ae = fabs(eig[e]);
         eig_max         = eig_max > ae ? eig_max : ae;
-        ghost[e]        = gq[e] - uqf[e];
       }
       for (int n = 0; n < b->nfdof; ++n)
         coeff[n] = coeff[n] > eig_max ? coeff[n] : eig_max;
-      double gflux[NEQ_MAX];
-      for (int i = 0; i < NEQ; ++i)
+
+      double relax = 1.0;
+      if (b->kind == RDSO_BC_WEAK_WALL)
       {
-        double s = Km[i][0] * ghost[0];
-        for (int k = 1; k < NEQ; ++k)
-          s = s + Km[i][k] * ghost[k];
-        gflux[i] = s;
+        /* WeakWall.hpp:93-250 (active branch): mirror state with the normal velocity removed,
+         * same density and pressure; residual = relax V w (F(u_ghost).n - F(u).n), relax = 1
+         * for P1 facets, 1/(3p) otherwise; total without relax */
+        relax = (b->order <= 1) ? 1.0 : 1. / (3. * b->order);
+        double Fn[NEQ_MAX], Fg[NEQ_MAX], ug[NEQ_MAX];
+        euler_flux_normal(m, &p, nrm, Fn);
+        double vn = 0.0, v2_new = 0.0;
+        for (int d = 0; d < D; ++d)
+          vn += p.V[d] * nrm[d];
+        ug[0] = p.rho;
+        for (int d = 0; d < D; ++d)
+        {
+          ug[d + 1] = p.V[d] - vn * nrm[d];
+          v2_new += ug[d + 1] * ug[d + 1];
+          ug[d + 1] *= p.rho;
+        }
+        ug[D + 1] = uqf[D + 1] + 0.5 * p.rho * (v2_new - p.v2);
+        props_t pg;
+        bad += props(m, ug, &pg);
+        euler_flux_normal(m, &pg, nrm, Fg);
+        for (int e = 0; e < NEQ; ++e)
+          gflux[e] = Fg[e] - Fn[e];
+      }
+      else
+      {
+        if (b->kind == RDSO_BC_WEAK_DIRICHLET)
+        {
+          const double *gq = b->gq + ((size_t)f * b->nfq + q) * NEQ;
+          for (int e = 0; e < NEQ; ++e)
+            ghost[e] = gq[e];
+        }
+        else if (b->kind == RDSO_BC_WEAK_SUB_INLET)
+        {
+          /* WeakSubInlet.hpp:113-215: total conditions at the local Mach number */
+          const double gm1 = m->gamma - 1.;
+          const double Ma  = sqrt(p.v2) / p.a;
+          const double fac = 1. + 0.5 * gm1 * Ma * Ma;
+          const double Tg  = b->params[0] / fac;
+          const double pg  = b->params[1] / pow(fac, m->gamma / (m->gamma - 1.));
+          ghost[0]         = pg / (287.046 * Tg);
+          ghost[1]         = Ma * sqrt(m->gamma * 287.046 * Tg) * ghost[0];
+          for (int d = 1; d < D; ++d)
+            ghost[d + 1] = 0.0;
+          double rho2u2 = 0.0;
+          for (int d = 0; d < D; ++d)
+            rho2u2 += ghost[d + 1] * ghost[d + 1];
+          ghost[NEQ - 1] = pg / gm1 + 0.5 * (rho2u2 / ghost[0]);
+        }
+        else
+        {
+          /* WeakSubOutlet.hpp:105-190: interior state with the outlet pressure */
+          const double gm1 = m->gamma - 1.;
+          for (int i = 0; i < NEQ - 1; ++i)
+            ghost[i] = uqf[i];
+          double rho2u2 = 0.0;
+          for (int d = 0; d < D; ++d)
+            rho2u2 += uqf[d + 1] * uqf[d + 1];
+          ghost[NEQ - 1] = b->params[0] / gm1 + 0.5 * rho2u2 / uqf[0];
+        }
+        for (int e = 0; e < NEQ; ++e)
+          ghost[e] -= uqf[e];
+        for (int i = 0; i < NEQ; ++i)
+        {
+          double s = Km[i][0] * ghost[0];
+          for (int k = 1; k < NEQ; ++k)
+            s = s + Km[i][k] * ghost[k];
+          gflux[i] = s;
+        }
       }
       for (int e = 0; e < NEQ; ++e)
         total[e] += wq * gflux[e];
       for (int n = 0; n < b->nfdof; ++n)
         for (int e = 0; e < NEQ; ++e)
-          bres[n][e] += b->fV[(size_t)q * b->nfdof + n] * wq * gflux[e];
+          bres[n][e] += relax * b->fV[(size_t)q * b->nfdof + n] * wq * gflux[e];
     }
 
     for (int e = 0; e < NEQ; ++e)
@@ -859,8 +941,7 @@ int rdso_assemble(const rdso_model *m, const rdso_cells *groups, int ngroups, co
 
   for (int ib = 0; ib < nbcs; ++ib)
   {
-    if (bcs[ib].kind == RDSO_BC_WEAK_DIRICHLET)
-      bad += apply_weak_dirichlet(m, &bcs[ib], geo_coords, vol, u, res, ws);
+    bad += apply_weak_bc(m, &bcs[ib], geo_coords, vol, u, res, ws);
   }
 
   /* RDTimeUpdate::compute_local_time_step (RDTimeUpdate.cpp:41-53) */

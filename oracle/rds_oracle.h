@@ -46,7 +46,10 @@ enum
 
 enum
 {
-  RDSO_BC_WEAK_DIRICHLET = 0
+  RDSO_BC_WEAK_DIRICHLET  = 0, /* bc/WeakDirichletBC.hpp */
+  RDSO_BC_WEAK_WALL       = 1, /* bc/WeakWall.hpp */
+  RDSO_BC_WEAK_SUB_INLET  = 2, /* bc/WeakSubInlet.hpp, params: total temperature, pressure */
+  RDSO_BC_WEAK_SUB_OUTLET = 3  /* bc/WeakSubOutlet.hpp, params: outlet pressure */
 };
 
 typedef struct
@@ -71,6 +74,9 @@ typedef struct
   const double *dVgeo; /* [dim][nq][ngeo]    geometry basis derivatives */
   const double *dVf;   /* [dim][nq][nfl]     flux (order p+1) basis derivatives */
   const double *Vsf;   /* [nfl][ndof]        solution basis at flux nodes */
+  int nqv;              /* dual-volume rule (0: use the rule above) */
+  const double *wv;     /* [nqv] */
+  const double *dVgeo_v; /* [dim][nqv][ngeo] */
 } rdso_cells;
 
 typedef struct
@@ -83,6 +89,8 @@ typedef struct
   const double *fV;     /* [nfq][nfdof] */
   const double *fdVgeo; /* [dim-1][nfq][nfgeo] */
   const double *gq;     /* [nfacets][nfq][neq] boundary state at facet quadrature points */
+  int order;            /* polynomial order of the facet's solution basis */
+  double params[4];     /* kind-specific parameters */
 } rdso_bc;
 
 /* Dual volume: every dof of a cell receives the full cell volume sum_q w_q detJ_q. */

@@ -19,6 +19,7 @@ HARNESS_PATH = os.path.join(_HERE, "_ref", "rds_ref_harness")
 
 PHYSICS = {"advconst": 0, "burgers": 1, "euler2d": 2, "euler3d": 3}
 SCHEME = {"lda": 0, "n": 1, "b": 2}
+BC_KIND = {"WeakDirichlet": 0, "WeakWall": 1, "WeakSubInlet": 2, "WeakSubOutlet": 3}
 
 
 class _Model(C.Structure):
@@ -30,14 +31,15 @@ class _Cells(C.Structure):
     _fields_ = [("ncells", C.c_int), ("ndof", C.c_int), ("ngeo", C.c_int), ("nq", C.c_int),
                 ("nfl", C.c_int), ("sol_conn", C.c_void_p), ("geo_conn", C.c_void_p),
                 ("w", C.c_void_p), ("V", C.c_void_p), ("dV", C.c_void_p),
-                ("dVgeo", C.c_void_p), ("dVf", C.c_void_p), ("Vsf", C.c_void_p)]
+                ("dVgeo", C.c_void_p), ("dVf", C.c_void_p), ("Vsf", C.c_void_p),
+                ("nqv", C.c_int), ("wv", C.c_void_p), ("dVgeo_v", C.c_void_p)]
 
 
 class _BC(C.Structure):
     _fields_ = [("kind", C.c_int), ("nfacets", C.c_int), ("nfdof", C.c_int), ("nfgeo", C.c_int),
                 ("nfq", C.c_int), ("sol_conn", C.c_void_p), ("geo_conn", C.c_void_p),
                 ("fw", C.c_void_p), ("fV", C.c_void_p), ("fdVgeo", C.c_void_p),
-                ("gq", C.c_void_p)]
+                ("gq", C.c_void_p), ("order", C.c_int), ("params", C.c_double * 4)]
 
 
 def build() -> None:
@@ -94,6 +96,11 @@ class Oracle:
             c = self.groups[i]
             c.ncells, c.ndof, c.ngeo, c.nq, c.nfl = g.ncells, g.ndof, g.ngeo, g.nq, g.nfl
             (c.sol_conn, c.geo_conn, c.w, c.V, c.dV, c.dVgeo, c.dVf, c.Vsf) = [_p(a) for a in arrs]
+            if g.wv is not None:
+                va = [np.ascontiguousarray(g.wv, dtype=np.float64),
+                      np.ascontiguousarray(g.dVgeo_v, dtype=np.float64)]
+                self._keep += va
+                c.nqv, c.wv, c.dVgeo_v = va[0].shape[0], _p(va[0]), _p(va[1])
         nb = max(1, len(prob.bcs))
         self.bcs = (_BC * nb)()
         for i, b in enumerate(prob.bcs):
@@ -101,7 +108,11 @@ class Oracle:
                     (b.sol_conn, b.geo_conn, b.fw, b.fV, b.fdVgeo, b.gq)]
             self._keep += arrs
             s = self.bcs[i]
-            s.kind, s.nfacets, s.nfdof, s.nfgeo, s.nfq = 0, b.nfacets, b.nfdof, b.nfgeo, b.nfq
+            s.kind, s.nfacets, s.nfdof, s.nfgeo, s.nfq = (BC_KIND[b.kind], b.nfacets, b.nfdof,
+                                                          b.nfgeo, b.nfq)
+            s.order = b.order
+            for k, v in enumerate(b.params[:4]):
+                s.params[k] = v
             (s.sol_conn, s.geo_conn, s.fw, s.fV, s.fdVgeo, s.gq) = [_p(a) for a in arrs]
         self.coords = np.ascontiguousarray(prob.geo_coords, dtype=np.float64)
         self.vol = np.zeros(prob.nnodes)

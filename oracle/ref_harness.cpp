@@ -140,6 +140,30 @@ static void init_state(const std::string &name, const Real *x, Uint dim, Uint ne
     // inflow profile 1.5 - 2x with a smooth perturbation
     u[0] = 1.5 - 2.0 * x[0] + 0.1 * std::sin(7.0 * x[0] + 3.0 * x[1]) * x[1];
   }
+  else if (name == "bump2d" || name == "bump3d")
+  {
+    // Freestream of the reference's bump case (examples/testcases-rdm/Bump-RDS-2D-Explicit.cpp:
+    // 100-131): total temperature / pressure 307.6488978 K / 120195.4453 Pa, R = 287.046,
+    // Mach 0.5 (2D) or 0.6 (3D) along x, with a +-1% perturbation of density and pressure that
+    // is a fixed pseudo-random function of the coordinates.
+    const Real gamma = 1.4, R = 287.046, Ttot = 307.6488978, Ptot = 120195.4453;
+    const Real M  = (name == "bump2d") ? 0.5 : 0.6;
+    const Real f  = 1. + 0.5 * (gamma - 1.) * M * M;
+    const Real T  = Ttot / f, p0 = Ptot / std::pow(f, gamma / (gamma - 1.));
+    const Real z  = dim == 3 ? x[2] : 0.0;
+    auto hash     = [](Real a, Real b, Real c) {
+      const Real s = std::sin(12.9898 * a + 78.233 * b + 37.719 * c) * 43758.5453;
+      return 2.0 * (s - std::floor(s)) - 1.0;
+    };
+    const Real rho = p0 / (R * T) * (1. + 0.01 * hash(x[0], x[1], z));
+    const Real p   = p0 * (1. + 0.01 * hash(x[1], z, x[0]));
+    const Real ux  = M * std::sqrt(gamma * R * T);
+    u[0]           = rho;
+    u[1]           = rho * ux;
+    for (Uint d = 1; d < dim; ++d)
+      u[1 + d] = 0.0;
+    u[dim + 1] = p / (gamma - 1.) + 0.5 * rho * ux * ux;
+  }
   else if (name == "euler2d")
   {
     // freestream M = 0.5 along x with a smooth O(1%) perturbation
@@ -285,7 +309,18 @@ int run(const Args &a)
   for (const BCDesc &b : bcs)
   {
     auto bc = solver->add_boundary_condition(b.type, b.name, b.boundary);
-    if (!b.expr.empty() && b.expr != "-")
+    if (b.expr.find('=') != std::string::npos)
+    {
+      // parameters "name=value;name=value" (WeakSubInlet / WeakSubOutlet)
+      std::stringstream ps(b.expr);
+      std::string kv;
+      while (std::getline(ps, kv, ';'))
+      {
+        const size_t eq = kv.find('=');
+        bc->set_parameter(kv.substr(0, eq), std::atof(kv.substr(eq + 1).c_str()));
+      }
+    }
+    else if (!b.expr.empty() && b.expr != "-")
       bc->set_expression(find_expr(b.expr));
   }
 
@@ -464,6 +499,26 @@ int run(const Args &a)
   }
   out.put("flux_nodes", mat_to_vec(flux_nodes), {nfl, flux_nodes.cols()});
   out.put("sol_nodes", mat_to_vec(sol_nodes), {ndof, sol_nodes.cols()});
+
+  // dual-volume rule: Gauss rule of the cell's own order (RDTimeUpdate.hpp:85-150)
+  {
+    StdPointSet vquad;
+    vquad.change_type(shape, a.p, PointSetID::Gauss);
+    const math::DenseDMat<Real> &vqp = vquad.get().coordinates();
+    const math::DenseDVec<Real> &vqw = vquad.get().weights();
+    interpolation::FEValues fe_vgeo;
+    fe_vgeo.configure(PointSetTag(shape, geo_order, PointSetID::Equidist),
+                      sf::SFTag(shape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
+    fe_vgeo.fill_Vandermonde(vqp, vqw);
+    std::vector<Real> vw(vqp.rows());
+    for (Uint q = 0; q < vqp.rows(); ++q)
+      vw[q] = vqw[q];
+    out.put("vqp", mat_to_vec(vqp), {vqp.rows(), vqp.cols()});
+    out.put("vw", vw, {vqp.rows()});
+    for (Uint d = 0; d < D; ++d)
+      out.put("vdVgeo" + std::to_string(d), mat_to_vec(fe_vgeo.deriv_Vandermonde(d)),
+              {vqp.rows(), ngeo});
+  }
 
   const Uint nfq = fqp.rows();
   out.put("fqp", mat_to_vec(fqp), {nfq, fqp.cols()});

@@ -437,6 +437,13 @@ rds_status rds_add_cell_group(rds_ctx *ctx, const rds_cell_group *g)
   h.dVgeo.assign(g->dVgeo, g->dVgeo + (size_t)D * g->nq * g->ngeo);
   h.dVf.assign(g->dVf, g->dVf + (size_t)D * g->nq * g->nfl);
   h.Vsf.assign(g->Vsf, g->Vsf + (size_t)g->nfl * g->ndof);
+  if (g->nqv > 0)
+  {
+    if (!g->wv || !g->dVgeo_v || g->nqv > 64)
+      return fail(ctx, RDS_ERR_INVALID, "invalid dual-volume rule");
+    h.wv.assign(g->wv, g->wv + g->nqv);
+    h.dVgeo_v.assign(g->dVgeo_v, g->dVgeo_v + (size_t)D * g->nqv * g->ngeo);
+  }
   h.affine = (g->shape == RDS_TRIAG && g->ngeo == 3) || (g->shape == RDS_TETRA && g->ngeo == 4);
   rds_status st;
   const std::vector<int32_t> sc = transpose_i32(g->sol_conn, g->ncells, g->ndof);
@@ -452,6 +459,7 @@ rds_status rds_add_cell_group(rds_ctx *ctx, const rds_cell_group *g)
   RDS_CUDA(cudaStreamSynchronize(ctx->stream));
   h.desc.sol_conn = h.desc.geo_conn = nullptr;
   h.desc.w = h.desc.V = h.desc.dV = h.desc.dVgeo = h.desc.dVf = h.desc.Vsf = nullptr;
+  h.desc.wv = h.desc.dVgeo_v = nullptr;
   ctx->groups.push_back(h);
   return RDS_OK;
 }
@@ -627,13 +635,18 @@ rds_status rds_finalize(rds_ctx *ctx)
   // slots hold zero).
   for (const HostCellGroup &g : ctx->groups)
   {
+    // the cell's own-order rule when given (as the reference), else the residual rule
+    const bool own                  = !g.wv.empty();
+    const std::vector<double> &w    = own ? g.wv : g.w;
+    const std::vector<double> &dvg  = own ? g.dVgeo_v : g.dVgeo;
+    const int nqv                   = (int)w.size();
     double *dw = nullptr, *ddv = nullptr;
-    if ((st = dalloc(ctx, &dw, g.w.size())) || (st = dalloc(ctx, &ddv, g.dVgeo.size())))
+    if ((st = dalloc(ctx, &dw, w.size())) || (st = dalloc(ctx, &ddv, dvg.size())))
       return st;
-    if ((st = upload(ctx, dw, g.w.data(), g.w.size())) ||
-        (st = upload(ctx, ddv, g.dVgeo.data(), g.dVgeo.size())))
+    if ((st = upload(ctx, dw, w.data(), w.size())) ||
+        (st = upload(ctx, ddv, dvg.data(), dvg.size())))
       return st;
-    RDS_CUDA(launch_cell_volume_raw(g.desc.ncells, d.dim, g.desc.nq, g.desc.ngeo, g.d_geo_conn,
+    RDS_CUDA(launch_cell_volume_raw(g.desc.ncells, d.dim, nqv, g.desc.ngeo, g.d_geo_conn,
                                     ctx->d_X, d.ngeo_nodes, dw, ddv, ctx->d_wsc + g.ws_base,
                                     ctx->stream));
     RDS_CUDA(cudaStreamSynchronize(ctx->stream));

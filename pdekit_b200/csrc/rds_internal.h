@@ -30,6 +30,7 @@ struct HostCellGroup
 {
   rds_cell_group desc{};
   std::vector<double> w, V, dV, dVgeo, dVf, Vsf;
+  std::vector<double> wv, dVgeo_v; // dual-volume rule (empty: use w, dVgeo)
   int32_t *d_sol_conn = nullptr; // SoA [ndof][ncells]
   int32_t *d_geo_conn = nullptr; // SoA [ngeo][ncells]
   long long slot_base = 0;       // first contribution slot of this group

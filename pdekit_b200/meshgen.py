@@ -202,3 +202,191 @@ def boundary_facets_tri(mesh: Mesh2D, sol_conn: np.ndarray, p: int, name: str):
             dofs += list(sol_conn[c, start:start + p - 1])
         sol[k] = dofs
     return geo, sol
+
+
+# ---------------------------------------------------------------------------------------------
+# General meshes (triangles, quadrilaterals, tetrahedra) for the Euler configurations
+# ---------------------------------------------------------------------------------------------
+
+GMSH_TYPE = {"line": 1, "triag": 2, "quad": 3, "tetra": 4}
+GMSH_FACET = {"triag": "line", "quad": "line", "tetra": "triag"}
+
+
+@dataclasses.dataclass
+class Mesh:
+    """P1 geometry: coords [nv, dim]; cell groups {shape: [nc, nvert]} (reference vertex
+    order, positive orientation); named boundaries {name: (facet shape, [nf, nvert])}."""
+    coords: np.ndarray
+    cells: dict
+    boundaries: dict
+
+    @property
+    def dim(self):
+        return self.coords.shape[1]
+
+
+def bump_profile(x, h=0.1, k=25.0):
+    return h * np.exp(-k * x * x)
+
+
+def channel_2d(nx_tri: int, nx_quad: int, ny: int, x0=-1.5, xm=0.0, x1=1.5, bump_h=0.1,
+               jitter=0.0, seed=0) -> Mesh:
+    """Bump channel [x0,x1] x [0,1] with bottom wall y = bump_h exp(-25 x^2): triangles on
+    [x0,xm] (nx_tri columns of squares split along the (i,j)->(i+1,j+1) diagonal) and
+    quadrilaterals on [xm,x1] (nx_quad columns); ny rows; the two halves share the vertical
+    line x = xm. y is mapped as y' = yb(x) + y (1 - yb(x)). Interior vertices jittered by
+    U(+-jitter h). Boundaries: bottom_wall, top_wall, inlet (x = x0), outlet (x = x1)."""
+    xs = np.concatenate([np.linspace(x0, xm, nx_tri + 1) if nx_tri > 0 else np.array([x0]),
+                         np.linspace(xm, x1, nx_quad + 1)[1:] if nx_quad > 0 else np.array([])])
+    if nx_tri == 0:
+        xs = np.linspace(xm, x1, nx_quad + 1) if x0 == xm else np.linspace(x0, x1, nx_quad + 1)
+    nxv = xs.size
+    ys = np.linspace(0.0, 1.0, ny + 1)
+    X, Y = np.meshgrid(xs, ys, indexing="xy")  # [ny+1, nxv]
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        hx = np.diff(xs).min()
+        hy = 1.0 / ny
+        interior = np.zeros_like(X, dtype=bool)
+        interior[1:-1, 1:-1] = True
+        X = X + np.where(interior, rng.uniform(-jitter * hx, jitter * hx, X.shape), 0.0)
+        Y = Y + np.where(interior, rng.uniform(-jitter * hy, jitter * hy, Y.shape), 0.0)
+    yb = bump_profile(X, bump_h)
+    Y = yb + Y * (1.0 - yb)
+    coords = np.stack([X.ravel(), Y.ravel()], axis=1)
+
+    def vid(i, j):
+        return j * nxv + i
+
+    tris, quads = [], []
+    ntri_cols = nx_tri if nx_tri > 0 else 0
+    for j in range(ny):
+        for i in range(nxv - 1):
+            a, b, c, d = vid(i, j), vid(i + 1, j), vid(i + 1, j + 1), vid(i, j + 1)
+            if i < ntri_cols:
+                tris.append((a, b, c))
+                tris.append((a, c, d))
+            else:
+                quads.append((a, b, c, d))
+    cells = {}
+    if tris:
+        cells["triag"] = np.asarray(tris, dtype=np.int32)
+    if quads:
+        cells["quad"] = np.asarray(quads, dtype=np.int32)
+    bnd = {
+        "bottom_wall": ("line", np.asarray([(vid(i, 0), vid(i + 1, 0)) for i in range(nxv - 1)],
+                                           dtype=np.int32)),
+        "outlet": ("line", np.asarray([(vid(nxv - 1, j), vid(nxv - 1, j + 1)) for j in range(ny)],
+                                      dtype=np.int32)),
+        "top_wall": ("line", np.asarray([(vid(i + 1, ny), vid(i, ny)) for i in range(nxv - 1)],
+                                        dtype=np.int32)),
+        "inlet": ("line", np.asarray([(vid(0, j + 1), vid(0, j)) for j in range(ny)],
+                                     dtype=np.int32)),
+    }
+    return Mesh(coords=coords, cells=cells, boundaries=bnd)
+
+
+# Kuhn split of the unit cube into 6 tetrahedra along the (0,0,0)-(1,1,1) diagonal; hex vertex
+# k = i + 2 j + 4 l at (i, j, l). Every tetrahedron is (v0, v0+e_a, v0+e_a+e_b, v7).
+_KUHN = [(0, 1, 3, 7), (0, 1, 5, 7), (0, 2, 3, 7), (0, 2, 6, 7), (0, 4, 5, 7), (0, 4, 6, 7)]
+
+
+def box_tet(nx: int, ny: int, nz: int, x0=-2.0, x1=2.0, bump_h=0.05, bump_k=16.0, jitter=0.0,
+            seed=0) -> Mesh:
+    """[x0,x1] x [0,1] x [0,1] hexahedra split into 6 tetrahedra each (Kuhn split, conforming),
+    bottom y = bump_h exp(-bump_k (x^2 + z^2)), y' = yb + y (1 - yb). Boundaries: bottom_wall
+    (y=0), top_wall (y=1), side_walls (z=0, z=1), inlet (x=x0), outlet (x=x1)."""
+    xs = np.linspace(x0, x1, nx + 1)
+    ys = np.linspace(0.0, 1.0, ny + 1)
+    zs = np.linspace(0.0, 1.0, nz + 1)
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")  # [nz+1, ny+1, nx+1]
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        interior = np.zeros_like(X, dtype=bool)
+        interior[1:-1, 1:-1, 1:-1] = True
+        h = (np.diff(xs).min(), 1.0 / ny, 1.0 / nz)
+        X = X + np.where(interior, rng.uniform(-jitter * h[0], jitter * h[0], X.shape), 0.0)
+        Y = Y + np.where(interior, rng.uniform(-jitter * h[1], jitter * h[1], Y.shape), 0.0)
+        Z = Z + np.where(interior, rng.uniform(-jitter * h[2], jitter * h[2], Z.shape), 0.0)
+    yb = bump_h * np.exp(-bump_k * (X * X + Z * Z))
+    Y = yb + Y * (1.0 - yb)
+    coords = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    nxv, nyv = nx + 1, ny + 1
+
+    def vid(i, j, l):
+        return (l * nyv + j) * nxv + i
+
+    tets = []
+    for l in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                hexv = [vid(i + (k & 1), j + ((k >> 1) & 1), l + ((k >> 2) & 1)) for k in range(8)]
+                for t in _KUHN:
+                    tets.append([hexv[k] for k in t])
+    tets = np.asarray(tets, dtype=np.int32)
+    # positive orientation
+    P = coords[tets]
+    vol6 = np.einsum("ij,ij->i", np.cross(P[:, 1] - P[:, 0], P[:, 2] - P[:, 0]), P[:, 3] - P[:, 0])
+    neg = vol6 < 0
+    tets[neg] = tets[neg][:, [0, 2, 1, 3]]
+    # boundary faces: faces of tets that lie on the box sides
+    faces = {}
+    for t in tets:
+        for f in ((t[1], t[2], t[3]), (t[0], t[3], t[2]), (t[0], t[1], t[3]), (t[0], t[2], t[1])):
+            key = tuple(sorted(f))
+            faces[key] = None if key in faces else f
+    bnd = {k: [] for k in ("bottom_wall", "top_wall", "side_walls", "inlet", "outlet")}
+    Xr, Yr, Zr = (np.meshgrid(zs, ys, xs, indexing="ij")[2].ravel(),
+                  np.meshgrid(zs, ys, xs, indexing="ij")[1].ravel(),
+                  np.meshgrid(zs, ys, xs, indexing="ij")[0].ravel())
+    for key, f in faces.items():
+        if f is None:
+            continue
+        f = np.asarray(f)
+        if np.all(Yr[f] == 0.0):
+            bnd["bottom_wall"].append(f)
+        elif np.all(Yr[f] == 1.0):
+            bnd["top_wall"].append(f)
+        elif np.all(Xr[f] == x0):
+            bnd["inlet"].append(f)
+        elif np.all(Xr[f] == x1):
+            bnd["outlet"].append(f)
+        else:
+            bnd["side_walls"].append(f)
+    boundaries = {k: ("triag", np.asarray(sorted(v, key=lambda a: tuple(sorted(a))),
+                                          dtype=np.int32)) for k, v in bnd.items()}
+    return Mesh(coords=coords, cells={"tetra": tets}, boundaries=boundaries)
+
+
+def write_gmsh22_mesh(path: str, mesh: Mesh, domain_name: str = "domain") -> None:
+    """Gmsh 2.2 ASCII of a general P1 Mesh (one physical group per boundary and one for the
+    cells)."""
+    names = list(mesh.boundaries.keys())
+    tdim = mesh.dim
+    lines = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat", "$PhysicalNames", str(len(names) + 1)]
+    for k, nm in enumerate(names):
+        lines.append(f'{tdim - 1} {k + 1} "{nm}"')
+    cell_tag = len(names) + 1
+    lines.append(f'{tdim} {cell_tag} "{domain_name}"')
+    lines += ["$EndPhysicalNames", "$Nodes", str(mesh.coords.shape[0])]
+    for i, xyz in enumerate(mesh.coords):
+        c = [float(v) for v in xyz] + [0.0] * (3 - len(xyz))
+        lines.append(f"{i + 1} {c[0]!r} {c[1]!r} {c[2]!r}")
+    lines.append("$EndNodes")
+    nel = sum(len(v[1]) for v in mesh.boundaries.values()) + sum(len(c) for c in mesh.cells.values())
+    lines += ["$Elements", str(nel)]
+    eid = 1
+    for k, nm in enumerate(names):
+        shape, facets = mesh.boundaries[nm]
+        for f in facets:
+            lines.append(f"{eid} {GMSH_TYPE[shape]} 2 {k + 1} {k + 1} " +
+                         " ".join(str(v + 1) for v in f))
+            eid += 1
+    for shape, cells in mesh.cells.items():
+        for c in cells:
+            lines.append(f"{eid} {GMSH_TYPE[shape]} 2 {cell_tag} {cell_tag} " +
+                         " ".join(str(v + 1) for v in c))
+            eid += 1
+    lines.append("$EndElements")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")

@@ -32,6 +32,8 @@ class CellGroup:
     Vsf: np.ndarray  # [nfl, ndof]
     shape: str = "triag"
     order: int = 1
+    wv: np.ndarray = None  # [nqv] dual-volume rule (Gauss rule of the cell order), optional
+    dVgeo_v: np.ndarray = None  # [dim, nqv, ngeo]
 
     @property
     def ncells(self):
@@ -56,7 +58,7 @@ class CellGroup:
 
 @dataclasses.dataclass
 class BCGroup:
-    kind: str  # "WeakDirichlet"
+    kind: str  # WeakDirichlet | WeakWall | WeakSubInlet | WeakSubOutlet
     name: str
     sol_conn: np.ndarray  # [nfacets, nfdof] int32
     geo_conn: np.ndarray  # [nfacets, nfgeo] int32
@@ -65,6 +67,8 @@ class BCGroup:
     fVgeo: np.ndarray  # [nfq, nfgeo]
     fdVgeo: np.ndarray  # [dim-1, nfq, nfgeo]
     gq: np.ndarray  # [nfacets, nfq, neq] boundary state at facet quadrature points
+    order: int = 1  # polynomial order of the facet's solution basis
+    params: tuple = (0.0, 0.0, 0.0, 0.0)  # WeakSubInlet: (T_tot, p_tot); WeakSubOutlet: (p,)
 
     @property
     def nfacets(self):
@@ -129,6 +133,9 @@ def load_golden(path: str):
                   dVgeo=np.stack([arrs[f"dVgeo{d}"] for d in range(D)]),
                   dVf=np.stack([arrs[f"dVf{d}"] for d in range(D)]), Vsf=arrs["Vsf"],
                   shape=meta["shape"], order=meta["p"])
+    if "vw" in arrs:
+        g.wv = arrs["vw"]
+        g.dVgeo_v = np.stack([arrs[f"vdVgeo{d}"] for d in range(D)])
     prob = Problem(physics=meta["physics"], scheme=meta["scheme"], dim=D, neq=meta["neq"],
                    nnodes=meta["nsol"], geo_coords=arrs["geo_coords"], groups=[g], bcs=[],
                    adv=ADV_CONST_DIR if meta["physics"] == "advconst" else (0.0, 0.0, 0.0))
@@ -139,8 +146,17 @@ def load_golden(path: str):
                     fVgeo=arrs["fVgeo"],
                     fdVgeo=np.stack([arrs[f"fdVgeo{d}"] for d in range(D - 1)]),
                     gq=np.zeros((arrs[f"bc{ib}_sol"].shape[0], arrs["fw"].shape[0], meta["neq"])))
-        xq = b.quadrature_coords(prob.geo_coords)
-        b.gq = bcexpr.evaluate(bc["expr"], xq, meta["neq"])
+        b.order = meta["p"]
+        expr = bc["expr"]
+        if "=" in expr:  # parameters of WeakSubInlet / WeakSubOutlet
+            kv = dict(item.split("=") for item in expr.split(";"))
+            if bc["type"] == "WeakSubInlet":
+                b.params = (float(kv["total_temperature"]), float(kv["total_pressure"]), 0.0, 0.0)
+            else:
+                b.params = (float(kv["total_pressure"]), 0.0, 0.0, 0.0)
+        elif bc["type"] == "WeakDirichlet":
+            xq = b.quadrature_coords(prob.geo_coords)
+            b.gq = bcexpr.evaluate(expr, xq, meta["neq"])
         prob.bcs.append(b)
     # boundary conditions are applied in the order of their names (std::map in
     # src/solver/rdm/bc/RDMBCManager.hpp:146)

@@ -62,7 +62,8 @@ class _CellGroup(C.Structure):
                 ("ngeo", C.c_int), ("nq", C.c_int), ("nfl", C.c_int),
                 ("sol_conn", C.c_void_p), ("geo_conn", C.c_void_p), ("w", C.c_void_p),
                 ("V", C.c_void_p), ("dV", C.c_void_p), ("dVgeo", C.c_void_p),
-                ("dVf", C.c_void_p), ("Vsf", C.c_void_p)]
+                ("dVf", C.c_void_p), ("Vsf", C.c_void_p), ("nqv", C.c_int),
+                ("wv", C.c_void_p), ("dVgeo_v", C.c_void_p)]
 
 
 class _BCGroup(C.Structure):
@@ -169,6 +170,11 @@ class PGRDMethodExplicit:
             self._keep += arrs
             cg = _CellGroup(SHAPE[g.shape], g.order, g.ncells, g.ndof, g.ngeo, g.nq, g.nfl,
                             *[_ptr(a) for a in arrs])
+            if g.wv is not None:
+                va = [np.ascontiguousarray(g.wv, dtype=np.float64),
+                      np.ascontiguousarray(g.dVgeo_v, dtype=np.float64)]
+                self._keep += va
+                cg.nqv, cg.wv, cg.dVgeo_v = va[0].shape[0], _ptr(va[0]), _ptr(va[1])
             self._check(L.rds_add_cell_group(self._ctx, C.byref(cg)))
         for b in prob.bcs:
             self.add_boundary_condition(b)

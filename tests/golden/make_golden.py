@@ -30,7 +30,20 @@ ADV_BCS = "WeakDirichlet:inlet_bottom:bottom:sin2pix,WeakDirichlet:inlet_left:le
 BURG_BCS = ("WeakDirichlet:inlet:bottom:burgers_inlet,WeakDirichlet:left:left:c1.5,"
             "WeakDirichlet:right:right:c-0.5")
 
+EULER2D_BCS = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakWall:top_wall_bc:top_wall:-,"
+               "WeakSubInlet:inlet_bc:inlet:total_temperature=307.6488978;"
+               "total_pressure=120195.4453,"
+               "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
+EULER3D_BCS = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakWall:top_wall_bc:top_wall:-,"
+               "WeakWall:side_walls_bc:side_walls:-,"
+               "WeakSubInlet:inlet_bc:inlet:total_temperature=307.6488978;"
+               "total_pressure=120195.4453,"
+               "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
+
 # name: (physics, scheme, p, quad order, n, jitter, seed, init, bcs, cfl, iters)
+# n is the squares per side of the unit square, or a tuple naming another mesh:
+#   ("channel_tri", nx, ny) / ("channel_quad", nx, ny): bump channel [-1.5,1.5] x [0,1]
+#   ("box_tet", nx, ny, nz): bump box [-2,2] x [0,1]^2, hexahedra split into 6 tetrahedra
 CASES = {
     # configuration 1 (advection, P1, LDA, P4 rule, jitter 0.2h, CFL 0.9) on a small mesh
     "adv_p1_lda_zero": ("advconst", "lda", 1, 4, 8, 0.2, 11, "zero", ADV_BCS, 0.9, 5),
@@ -44,6 +57,18 @@ CASES = {
     "burgers_p2_lda": ("burgers", "lda", 2, 5, 5, 0.15, 23, "burgers", BURG_BCS, 0.5, 3),
     "burgers_p1_b": ("burgers", "b", 1, 4, 6, 0.2, 24, "burgers", BURG_BCS, 0.5, 3),
     "burgers_p3_b": ("burgers", "b", 3, 8, 4, 0.2, 25, "burgers", BURG_BCS, 0.5, 3),
+    # configuration 3 (Euler 2D bump channel, P3 triangles / P3 quadrilaterals, blended B)
+    "euler2d_tri_p3_b": ("euler2d", "b", 3, 8, ("channel_tri", 4, 3), 0.15, 31, "bump2d",
+                         EULER2D_BCS, 0.5, 3),
+    "euler2d_quad_p3_b": ("euler2d", "b", 3, 8, ("channel_quad", 4, 3), 0.15, 32, "bump2d",
+                          EULER2D_BCS, 0.5, 3),
+    "euler2d_tri_p1_lda": ("euler2d", "lda", 1, 4, ("channel_tri", 5, 3), 0.15, 33, "bump2d",
+                           EULER2D_BCS, 0.5, 3),
+    "euler2d_tri_p2_n": ("euler2d", "n", 2, 5, ("channel_tri", 4, 3), 0.15, 34, "bump2d",
+                         EULER2D_BCS, 0.5, 3),
+    # configuration 4 (Euler 3D bump box, P2 tetrahedra, LDA)
+    "euler3d_tet_p2_lda": ("euler3d", "lda", 2, 5, ("box_tet", 3, 2, 2), 0.1, 41, "bump3d",
+                           EULER3D_BCS, 0.5, 3),
 }
 
 
@@ -53,9 +78,19 @@ def make(name, spec):
     if os.path.isdir(out):
         shutil.rmtree(out)
     os.makedirs(out)
-    mesh = meshgen.unit_square_tri(n, jit, seed=seed)
     msh = os.path.join(out, "mesh.msh")
-    meshgen.write_gmsh22(msh, mesh)
+    if isinstance(n, tuple):
+        if n[0] == "channel_tri":
+            mesh = meshgen.channel_2d(n[1], 0, n[2], x0=-1.5, xm=1.5, x1=1.5, jitter=jit,
+                                      seed=seed)
+        elif n[0] == "channel_quad":
+            mesh = meshgen.channel_2d(0, n[1], n[2], x0=-1.5, xm=-1.5, x1=1.5, jitter=jit,
+                                      seed=seed)
+        else:
+            mesh = meshgen.box_tet(n[1], n[2], n[3], jitter=jit, seed=seed)
+        meshgen.write_gmsh22_mesh(msh, mesh)
+    else:
+        meshgen.write_gmsh22(msh, meshgen.unit_square_tri(n, jit, seed=seed))
     cmd = [HARNESS, "dump", physics, scheme, str(p), str(quad), msh, out, str(iters), str(cfl),
            init, bcs]
     subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
