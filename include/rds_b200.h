@@ -89,7 +89,10 @@ typedef enum
 
 typedef enum
 {
-  RDS_BC_WEAK_DIRICHLET = 0 /* bc/WeakDirichletBC.hpp */
+  RDS_BC_WEAK_DIRICHLET  = 0, /* bc/WeakDirichletBC.hpp: gq = boundary state */
+  RDS_BC_WEAK_WALL       = 1, /* bc/WeakWall.hpp (Euler) */
+  RDS_BC_WEAK_SUB_INLET  = 2, /* bc/WeakSubInlet.hpp (Euler): params = total temperature, pressure */
+  RDS_BC_WEAK_SUB_OUTLET = 3  /* bc/WeakSubOutlet.hpp (Euler): params[0] = outlet pressure */
 } rds_bc_kind;
 
 typedef struct
@@ -151,7 +154,9 @@ typedef struct
   const double *fw;        /* [nfq] */
   const double *fV;        /* [nfq][nfdof] */
   const double *fdVgeo;    /* [dim-1][nfq][nfgeo] */
-  const double *gq;        /* [nfacets][nfq][neq] */
+  const double *gq;        /* [nfacets][nfq][neq] (RDS_BC_WEAK_DIRICHLET; NULL otherwise) */
+  int order;               /* polynomial order of the facet basis (WeakWall relaxation) */
+  double params[4];        /* kind-specific parameters (set_parameter of the reference) */
 } rds_bc_group;
 
 /* Create a context on the current CUDA device. 'stream' is a cudaStream_t to run on, or NULL

@@ -230,6 +230,10 @@ BCArgs bc_args(rds_ctx *ctx, const HostBC &b, const int *stop)
   a.adv0       = ctx->desc.adv[0];
   a.adv1       = ctx->desc.adv[1];
   a.gamma      = ctx->desc.gamma;
+  // WeakWall relaxation of the dof residuals (bc/WeakWall.hpp:112-116)
+  a.relax = (b.desc.order <= 1) ? 1.0 : 1. / (3. * b.desc.order);
+  for (int k = 0; k < 4; ++k)
+    a.params[k] = b.desc.params[k];
   a.status     = ctx->d_status;
   a.stop       = stop;
   return a;
@@ -471,9 +475,11 @@ rds_status rds_add_bc(rds_ctx *ctx, const rds_bc_group *b)
   if (ctx->finalized)
     return fail(ctx, RDS_ERR_INVALID, "rds_add_bc after rds_finalize");
   const int D = ctx->desc.dim, NEQ = ctx->desc.neq;
-  if (b->kind != RDS_BC_WEAK_DIRICHLET || b->nfacets <= 0 || b->nfdof <= 0 || b->nfdof > 16 ||
+  const bool dirichlet = b->kind == RDS_BC_WEAK_DIRICHLET;
+  if (b->kind < RDS_BC_WEAK_DIRICHLET || b->kind > RDS_BC_WEAK_SUB_OUTLET ||
+      (!dirichlet && NEQ == 1) || b->nfacets <= 0 || b->nfdof <= 0 || b->nfdof > 16 ||
       b->nfgeo <= 0 || b->nfgeo > 16 || b->nfq <= 0 || b->nfq > 32 || !b->sol_conn ||
-      !b->geo_conn || !b->fw || !b->fV || !b->fdVgeo || !b->gq)
+      !b->geo_conn || !b->fw || !b->fV || !b->fdVgeo || (dirichlet && !b->gq))
     return fail(ctx, RDS_ERR_INVALID, "invalid boundary group");
   for (size_t i = 0; i < (size_t)b->nfacets * b->nfdof; ++i)
     if (b->sol_conn[i] < 0 || b->sol_conn[i] >= ctx->desc.nnodes)
@@ -488,11 +494,13 @@ rds_status rds_add_bc(rds_ctx *ctx, const rds_bc_group *b)
   h.fdVgeo.assign(b->fdVgeo, b->fdVgeo + (size_t)(D - 1) * b->nfq * b->nfgeo);
   const std::vector<int32_t> sc = transpose_i32(b->sol_conn, b->nfacets, b->nfdof);
   const std::vector<int32_t> gc = transpose_i32(b->geo_conn, b->nfacets, b->nfgeo);
-  std::vector<double> gq((size_t)NEQ * b->nfq * b->nfacets);
-  for (int f = 0; f < b->nfacets; ++f)
-    for (int q = 0; q < b->nfq; ++q)
-      for (int e = 0; e < NEQ; ++e)
-        gq[((size_t)e * b->nfq + q) * b->nfacets + f] = b->gq[((size_t)f * b->nfq + q) * NEQ + e];
+  std::vector<double> gq(dirichlet ? (size_t)NEQ * b->nfq * b->nfacets : 1, 0.0);
+  if (dirichlet)
+    for (int f = 0; f < b->nfacets; ++f)
+      for (int q = 0; q < b->nfq; ++q)
+        for (int e = 0; e < NEQ; ++e)
+          gq[((size_t)e * b->nfq + q) * b->nfacets + f] =
+              b->gq[((size_t)f * b->nfq + q) * NEQ + e];
   rds_status st;
   if ((st = dalloc(ctx, &h.d_sol_conn, sc.size())) != RDS_OK ||
       (st = dalloc(ctx, &h.d_geo_conn, gc.size())) != RDS_OK ||

@@ -1,12 +1,17 @@
 // Weak boundary-condition kernels: one thread per boundary facet.
 //
-// WeakDirichlet (src/solver/rdm/bc/WeakDirichletBC.hpp:159-265): at each facet quadrature
-// point, K- = R min(Lambda,0) L for the facet normal, ghost flux K- (g - u_q), accumulated as
-// V(q,n) w_q |J_q| K-(g - u_q) per facet dof and as the facet total; the dof residuals are then
-// rescaled so that they sum to the facet total (src/solver/rdm/bc/WeakBC.hpp:786-832). The
-// facet's wave speed is max_q max(1e-9, |lambda|) for every dof, entering the nodal wave speed
-// multiplied by the dual volume (WeakBC.hpp:315-352).
-//
+// Per facet quadrature point a ghost flux is formed and distributed to the facet dofs with the
+// facet basis, V(q,n) w_q |J_q| (ghost flux), and summed into the facet total; the dof
+// residuals are then rescaled so that they sum to the facet total (src/solver/rdm/bc/
+// WeakBC.hpp:786-832). The facet's wave speed is max_q max(1e-9, |lambda|) for every dof and
+// enters the nodal wave speed multiplied by the dual volume (WeakBC.hpp:315-352).
+//   WeakDirichlet (bc/WeakDirichletBC.hpp:159-265): K-(n) (g - u_q).
+//   WeakWall (bc/WeakWall.hpp:93-250): F(u_mirror).n - F(u_q).n, u_mirror with the normal
+//     velocity removed, same density and pressure; the dof part is scaled by 1/(3p) for p > 1.
+//   WeakSubInlet (bc/WeakSubInlet.hpp:113-215): K-(n) (u_in - u_q), u_in from the total
+//     temperature and pressure at the local Mach number (gas constant 287.046 as there).
+//   WeakSubOutlet (bc/WeakSubOutlet.hpp:105-190): K-(n) (u_out - u_q), u_out = u_q with the
+//     energy of the outlet pressure.
 // Facet normals are (dy/dxi, -dx/dxi)/|.| in 2D and the normalised cross product of the two
 // tangents in 3D, with |J| the length / area factor (src/interpolation/GeometryMetric.hpp:560-660).
 
@@ -27,9 +32,9 @@ struct FacetTables
   T fdVgeo[D - 1][NFQ][NFGEO];
 };
 
-template <int PHYS, int D, int NEQ, int NFDOF, int NFQ, int NFGEO>
+template <int KIND, int PHYS, int D, int NEQ, int NFDOF, int NFQ, int NFGEO>
 __global__ void __launch_bounds__(kBlock)
-    bc_weak_dirichlet(const BCArgs a, const FacetTables<double, D, NFDOF, NFQ, NFGEO> tb)
+    bc_weak(const BCArgs a, const FacetTables<double, D, NFDOF, NFQ, NFGEO> tb)
 {
   if (*a.stop)
     return;
@@ -66,14 +71,15 @@ __global__ void __launch_bounds__(kBlock)
     for (int n = 0; n < NFDOF; ++n)
       bres[n][e] = 0.0;
   }
-  double coeff = 0.0;
-  bool bad     = false;
+  double coeff       = 0.0;
+  bool bad           = false;
+  const double relax = (KIND == RDS_BC_WEAK_WALL) ? a.relax : 1.0;
 
 #pragma unroll
   for (int q = 0; q < NFQ; ++q)
   {
     double nrm[D], jd;
-    if (D == 2)
+    if constexpr (D == 2)
     {
       double tx = tb.fdVgeo[0][q][0] * X[0][0], ty = tb.fdVgeo[0][q][0] * X[0][1];
 #pragma unroll
@@ -126,45 +132,99 @@ __global__ void __launch_bounds__(kBlock)
 
     double eig_max = 1.e-9;
     double gflux[NEQ];
+    if constexpr (NEQ == 1)
     {
+      // scalar: K = 1 * op(V . n) * 1
+      const double ax  = (PHYS == RDS_BURGERS2D) ? uq[0] : a.adv0;
+      const double ay  = (PHYS == RDS_BURGERS2D) ? 1.0 : a.adv1;
+      const double lam = ax * nrm[0] + ay * nrm[1];
+      const double km  = lam < 0.0 ? lam : 0.0;
+      eig_max          = fmax(eig_max, fabs(lam));
+      gflux[0]         = km * (a.gq[(size_t)q * a.nfacets + f] - uq[0]);
+    }
+    else
+    {
+      EulerProps<double, D> p;
+      bad |= euler_props<double, D>(uq, a.gamma, p);
       double K[NEQ][NEQ], lam[NEQ];
-      if constexpr (NEQ == 1)
+      euler_K<-1, double, D>(p, nrm, a.gamma, K, lam);
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+        eig_max = fmax(eig_max, fabs(lam[e]));
+      if constexpr (KIND == RDS_BC_WEAK_WALL)
       {
-        const double ax = (PHYS == RDS_BURGERS2D) ? uq[0] : a.adv0;
-        const double ay = (PHYS == RDS_BURGERS2D) ? 1.0 : a.adv1;
-        lam[0]  = ax * nrm[0] + ay * nrm[1];
-        K[0][0] = lam[0] < 0.0 ? lam[0] : 0.0;
+        double Fn[NEQ], Fg[NEQ], ug[NEQ];
+        euler_flux_n<double, D>(uq, p, nrm, Fn);
+        double vn = 0.0, v2_new = 0.0;
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+          vn += p.V[d] * nrm[d];
+        ug[0] = p.rho;
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+        {
+          ug[d + 1] = p.V[d] - vn * nrm[d];
+          v2_new += ug[d + 1] * ug[d + 1];
+          ug[d + 1] *= p.rho;
+        }
+        ug[D + 1] = uq[D + 1] + 0.5 * p.rho * (v2_new - p.v2);
+        EulerProps<double, D> pg;
+        bad |= euler_props<double, D>(ug, a.gamma, pg);
+        euler_flux_n<double, D>(ug, pg, nrm, Fg);
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          gflux[e] = Fg[e] - Fn[e];
       }
       else
       {
-        EulerProps<double, D> p;
-        bad |= euler_props<double, D>(uq, a.gamma, p);
-        double Kf[D + 2][D + 2], lamf[D + 2];
-        euler_K<-1, double, D>(p, nrm, a.gamma, Kf, lamf);
+        double ghost[NEQ];
+        const double gm1 = a.gamma - 1.0;
+        if constexpr (KIND == RDS_BC_WEAK_SUB_INLET)
+        {
+          const double Ma  = sqrt(p.v2) / p.a;
+          const double fac = 1. + 0.5 * gm1 * Ma * Ma;
+          const double Tg  = a.params[0] / fac;
+          const double pg  = a.params[1] / pow(fac, a.gamma / (a.gamma - 1.));
+          ghost[0]         = pg / (287.046 * Tg);
+          ghost[1]         = Ma * sqrt(a.gamma * 287.046 * Tg) * ghost[0];
+#pragma unroll
+          for (int d = 1; d < D; ++d)
+            ghost[d + 1] = 0.0;
+          double rho2u2 = 0.0;
+#pragma unroll
+          for (int d = 0; d < D; ++d)
+            rho2u2 += ghost[d + 1] * ghost[d + 1];
+          ghost[NEQ - 1] = pg / gm1 + 0.5 * (rho2u2 / ghost[0]);
+        }
+        else if constexpr (KIND == RDS_BC_WEAK_SUB_OUTLET)
+        {
+#pragma unroll
+          for (int i = 0; i < NEQ - 1; ++i)
+            ghost[i] = uq[i];
+          double rho2u2 = 0.0;
+#pragma unroll
+          for (int d = 0; d < D; ++d)
+            rho2u2 += uq[d + 1] * uq[d + 1];
+          ghost[NEQ - 1] = a.params[0] / gm1 + 0.5 * rho2u2 / uq[0];
+        }
+        else
+        {
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e)
+            ghost[e] = a.gq[((size_t)e * NFQ + q) * a.nfacets + f];
+        }
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          ghost[e] -= uq[e];
 #pragma unroll
         for (int i = 0; i < NEQ; ++i)
         {
-          lam[i] = lamf[i];
+          double s = K[i][0] * ghost[0];
 #pragma unroll
-          for (int j = 0; j < NEQ; ++j)
-            K[i][j] = Kf[i][j];
+          for (int k = 1; k < NEQ; ++k)
+            s = s + K[i][k] * ghost[k];
+          gflux[i] = s;
         }
-      }
-      double ghost[NEQ];
-#pragma unroll
-      for (int e = 0; e < NEQ; ++e)
-      {
-        eig_max  = fmax(eig_max, fabs(lam[e]));
-        ghost[e] = a.gq[((size_t)e * NFQ + q) * a.nfacets + f] - uq[e];
-      }
-#pragma unroll
-      for (int i = 0; i < NEQ; ++i)
-      {
-        double s = K[i][0] * ghost[0];
-#pragma unroll
-        for (int k = 1; k < NEQ; ++k)
-          s = s + K[i][k] * ghost[k];
-        gflux[i] = s;
       }
     }
     coeff = fmax(coeff, eig_max);
@@ -174,7 +234,7 @@ __global__ void __launch_bounds__(kBlock)
       total[e] += wq * gflux[e];
 #pragma unroll
       for (int n = 0; n < NFDOF; ++n)
-        bres[n][e] += tb.fV[q][n] * wq * gflux[e];
+        bres[n][e] += relax * tb.fV[q][n] * wq * gflux[e];
     }
   }
 
@@ -207,8 +267,8 @@ __global__ void __launch_bounds__(kBlock)
     atomicOr(a.status, kFlagNegPressure);
 }
 
-template <int PHYS, int D, int NEQ, int NFDOF, int NFQ, int NFGEO>
-cudaError_t launch_wd(const HostBC &b, const BCArgs &a, cudaStream_t s)
+template <int KIND, int PHYS, int D, int NEQ, int NFDOF, int NFQ, int NFGEO>
+cudaError_t launch_weak(const HostBC &b, const BCArgs &a, cudaStream_t s)
 {
   FacetTables<double, D, NFDOF, NFQ, NFGEO> tb;
   for (int q = 0; q < NFQ; ++q)
@@ -221,30 +281,80 @@ cudaError_t launch_wd(const HostBC &b, const BCArgs &a, cudaStream_t s)
         tb.fdVgeo[xi][q][g] = b.fdVgeo[(xi * NFQ + q) * NFGEO + g];
   }
   const int grid = (a.nfacets + kBlock - 1) / kBlock;
-  bc_weak_dirichlet<PHYS, D, NEQ, NFDOF, NFQ, NFGEO><<<grid, kBlock, 0, s>>>(a, tb);
+  bc_weak<KIND, PHYS, D, NEQ, NFDOF, NFQ, NFGEO><<<grid, kBlock, 0, s>>>(a, tb);
   return cudaGetLastError();
 }
 
-template <int PHYS, int D, int NEQ>
-cudaError_t dispatch_wd(const HostBC &b, const BCArgs &a, cudaStream_t s, bool *ok)
+// Facet types: 2D lines P1-P3 with 3-5 point Gauss rules; 3D P2 triangles with 12 points.
+template <int KIND, int PHYS, int D, int NEQ>
+cudaError_t dispatch_facets(const HostBC &b, const BCArgs &a, cudaStream_t s, bool *ok)
 {
   const rds_bc_group &d = b.desc;
   *ok                   = true;
-  if (D == 2 && d.nfgeo == 2)
+  if constexpr (D == 2)
   {
-#define RDS_WD(NFDOF, NFQ)                                                                         \
+    if (d.nfgeo == 2)
+    {
+#define RDS_WEAK(NFDOF, NFQ)                                                                       \
   if (d.nfdof == NFDOF && d.nfq == NFQ)                                                            \
-    return launch_wd<PHYS, D, NEQ, NFDOF, NFQ, 2>(b, a, s);
-    RDS_WD(2, 3)
-    RDS_WD(2, 4)
-    RDS_WD(3, 3)
-    RDS_WD(3, 4)
-    RDS_WD(4, 5)
-    RDS_WD(4, 4)
-#undef RDS_WD
+    return launch_weak<KIND, PHYS, D, NEQ, NFDOF, NFQ, 2>(b, a, s);
+      RDS_WEAK(2, 3)
+      RDS_WEAK(2, 4)
+      RDS_WEAK(3, 3)
+      RDS_WEAK(3, 4)
+      RDS_WEAK(4, 5)
+      RDS_WEAK(4, 4)
+#undef RDS_WEAK
+    }
+  }
+  else
+  {
+    if (d.nfgeo == 3 && d.nfdof == 6 && d.nfq == 12)
+      return launch_weak<KIND, PHYS, D, NEQ, 6, 12, 3>(b, a, s);
   }
   *ok = false;
   return cudaSuccess;
+}
+
+template <int PHYS, int D, int NEQ>
+cudaError_t dispatch_kind(const HostBC &b, const BCArgs &a, cudaStream_t s, bool *ok)
+{
+  *ok = false;
+  switch (b.desc.kind)
+  {
+  case RDS_BC_WEAK_DIRICHLET:
+    return dispatch_facets<RDS_BC_WEAK_DIRICHLET, PHYS, D, NEQ>(b, a, s, ok);
+  case RDS_BC_WEAK_WALL:
+    if constexpr (NEQ > 1)
+      return dispatch_facets<RDS_BC_WEAK_WALL, PHYS, D, NEQ>(b, a, s, ok);
+    break;
+  case RDS_BC_WEAK_SUB_INLET:
+    if constexpr (NEQ > 1)
+      return dispatch_facets<RDS_BC_WEAK_SUB_INLET, PHYS, D, NEQ>(b, a, s, ok);
+    break;
+  case RDS_BC_WEAK_SUB_OUTLET:
+    if constexpr (NEQ > 1)
+      return dispatch_facets<RDS_BC_WEAK_SUB_OUTLET, PHYS, D, NEQ>(b, a, s, ok);
+    break;
+  default:
+    break;
+  }
+  return cudaSuccess;
+}
+
+const char *bc_name(int kind)
+{
+  switch (kind)
+  {
+  case RDS_BC_WEAK_WALL:
+    return "bc_weak_wall";
+  case RDS_BC_WEAK_SUB_INLET:
+    return "bc_weak_sub_inlet";
+  case RDS_BC_WEAK_SUB_OUTLET:
+    return "bc_weak_sub_outlet";
+  default:
+    return "bc_weak_dirichlet";
+  }
 }
 
 } // namespace
@@ -252,18 +362,17 @@ cudaError_t dispatch_wd(const HostBC &b, const BCArgs &a, cudaStream_t s, bool *
 cudaError_t launch_bc(const HostBC &b, const BCArgs &a, int physics, int dim, int neq,
                       cudaStream_t s, const char **name)
 {
-  bool ok = false;
+  bool ok         = false;
   cudaError_t err = cudaSuccess;
-  *name = "bc_weak_dirichlet";
-  if (b.desc.kind == RDS_BC_WEAK_DIRICHLET)
-  {
-    if (physics == RDS_ADVECTION_CONST && dim == 2 && neq == 1)
-      err = dispatch_wd<RDS_ADVECTION_CONST, 2, 1>(b, a, s, &ok);
-    else if (physics == RDS_BURGERS2D && dim == 2 && neq == 1)
-      err = dispatch_wd<RDS_BURGERS2D, 2, 1>(b, a, s, &ok);
-    else if (physics == RDS_EULER2D && dim == 2 && neq == 4)
-      err = dispatch_wd<RDS_EULER2D, 2, 4>(b, a, s, &ok);
-  }
+  *name           = bc_name(b.desc.kind);
+  if (physics == RDS_ADVECTION_CONST && dim == 2 && neq == 1)
+    err = dispatch_kind<RDS_ADVECTION_CONST, 2, 1>(b, a, s, &ok);
+  else if (physics == RDS_BURGERS2D && dim == 2 && neq == 1)
+    err = dispatch_kind<RDS_BURGERS2D, 2, 1>(b, a, s, &ok);
+  else if (physics == RDS_EULER2D && dim == 2 && neq == 4)
+    err = dispatch_kind<RDS_EULER2D, 2, 4>(b, a, s, &ok);
+  else if (physics == RDS_EULER3D && dim == 3 && neq == 5)
+    err = dispatch_kind<RDS_EULER3D, 3, 5>(b, a, s, &ok);
   if (!ok)
     return cudaErrorNotSupported;
   return err;

@@ -1,14 +1,583 @@
-// Cell residual kernels for the 2D/3D Euler equations (added below).
+// Cell residual kernels for the 2D / 3D Euler equations (PGLDA / PGN / PGB): a group of G
+// lanes of one warp works on one cell.
+//
+// The reference's per-cell work (src/solver/rdm/cellsplitters/PGLDA.hpp:171-310,
+// PGN.hpp:154-289, PGB.hpp:314-498 with the metrics of src/interpolation/*Metric.hpp) is split
+// over the group as follows:
+//   A  stage the cell's nodal states (ndof x neq, FP64) in shared memory;
+//   B  flux nodes f = lane, lane + G, ...: S_f = Vsf u, F(S_f)            -> shared memory;
+//   C  quadrature points q = lane, lane + G, ...: u_q = V u and the flux divergence
+//      r_q = sum_d (invJ dVf F_d)_d                                       -> shared memory;
+//   D  every quadrature point, all lanes together: lane l owns nodes n = l, l + G, ...;
+//      it builds K+_n = R max(Lambda,0) L for grad phi_n (Euler2DCons.hpp:316-536 /
+//      Euler3DCons.hpp:332-560) and its part of sum K+ and sum K+ u; an xor-butterfly over the
+//      group completes the sums (bit-identical in every lane, since a + b == b + a); every lane
+//      factorises sum K+ (FP64 LU with partial pivoting) and solves for
+//      v = (sum K+)^-1 r_q and u_bar = (sum K+)^-1 sum_m K+_m u_m, then accumulates for its own
+//      nodes  lda_n += w_q |J_q| K+_n v  and  diss_n += w_q |J_q| K+_n (u_n - u_bar)
+//      (= sum_{m != n} K+_n (sum K+)^-1 K+_m (u_n - u_m), the reference's N dissipation);
+//   E  PGB blending theta = |Phi_0| / (sum_n |lda_n0 + diss_n0| + 1e-6) with a group sum,
+//      nodal residuals to the contribution slots, cell wave speed |K| max lambda.
+// T is the arithmetic type of B, C and the upwind matrices; the LU, the solves and all
+// accumulations are FP64 in both precisions.
+
 #include "rds_internal.h"
+#include "rds_physics.cuh"
+#include "rds_tables.cuh"
 
 namespace rds
 {
 
-cudaError_t launch_cells_euler(const HostCellGroup &, const CellArgs &, int, int, int,
-                               cudaStream_t, const char **name, bool *ok)
+namespace
 {
-  *name = "cells_euler";
-  *ok   = false;
+
+template <int G>
+__device__ __forceinline__ double group_sum(double v)
+{
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1)
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int G>
+__device__ __forceinline__ double group_max(double v)
+{
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1)
+    v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Solve A x = b for two right-hand sides (LU with row partial pivoting, FP64).
+template <int N>
+__device__ __forceinline__ void lu_solve2(double A[N][N], double b1[N], double b2[N])
+{
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+  {
+    int piv    = k;
+    double amx = fabs(A[k][k]);
+#pragma unroll
+    for (int i = k + 1; i < N; ++i)
+      if (fabs(A[i][k]) > amx)
+      {
+        amx = fabs(A[i][k]);
+        piv = i;
+      }
+    if (piv != k)
+    {
+#pragma unroll
+      for (int j = 0; j < N; ++j)
+      {
+        // swap rows k and piv without dynamic register indexing
+#pragma unroll
+        for (int i = k + 1; i < N; ++i)
+          if (i == piv)
+          {
+            const double t = A[k][j];
+            A[k][j]        = A[i][j];
+            A[i][j]        = t;
+          }
+      }
+#pragma unroll
+      for (int i = k + 1; i < N; ++i)
+        if (i == piv)
+        {
+          double t = b1[k];
+          b1[k]    = b1[i];
+          b1[i]    = t;
+          t        = b2[k];
+          b2[k]    = b2[i];
+          b2[i]    = t;
+        }
+    }
+    const double inv = 1.0 / A[k][k];
+#pragma unroll
+    for (int i = k + 1; i < N; ++i)
+    {
+      const double f = A[i][k] * inv;
+#pragma unroll
+      for (int j = k + 1; j < N; ++j)
+        A[i][j] -= f * A[k][j];
+      b1[i] -= f * b1[k];
+      b2[i] -= f * b2[k];
+    }
+  }
+#pragma unroll
+  for (int i = N - 1; i >= 0; --i)
+  {
+#pragma unroll
+    for (int j = i + 1; j < N; ++j)
+    {
+      b1[i] -= A[i][j] * b1[j];
+      b2[i] -= A[i][j] * b2[j];
+    }
+    b1[i] /= A[i][i];
+    b2[i] /= A[i][i];
+  }
+}
+
+// Inverse Jacobian and determinant at quadrature point q from the geometry nodes.
+template <typename T, int D, int NDOF, int NQ, int NFL, int NGEO>
+__device__ __forceinline__ T jacobian_at(const Tables<T, D, NDOF, NQ, NFL, NGEO> &tb, int q,
+                                         const T (&X)[NGEO][D], T (&ij)[D][D])
+{
+  T J[D][D];
+#pragma unroll
+  for (int xi = 0; xi < D; ++xi)
+#pragma unroll
+    for (int x = 0; x < D; ++x)
+    {
+      T s = tb.dVgeo[xi][q][0] * X[0][x];
+#pragma unroll
+      for (int g = 1; g < NGEO; ++g)
+        s = s + tb.dVgeo[xi][q][g] * X[g][x];
+      J[xi][x] = s;
+    }
+  if constexpr (D == 2)
+  {
+    const T det     = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    const T inv_det = T(1) / det;
+    ij[0][0]        = inv_det * J[1][1];
+    ij[1][1]        = inv_det * J[0][0];
+    ij[0][1]        = -inv_det * J[0][1];
+    ij[1][0]        = -inv_det * J[1][0];
+    return det;
+  }
+  else
+  {
+    const T c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const T c01 = J[1][0] * J[2][2] - J[1][2] * J[2][0];
+    const T c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const T det = J[0][0] * c00 - J[0][1] * c01 + J[0][2] * c02;
+    const T inv = T(1) / det;
+    ij[0][0]    = c00 * inv;
+    ij[0][1]    = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]) * inv;
+    ij[0][2]    = (J[0][1] * J[1][2] - J[1][1] * J[0][2]) * inv;
+    ij[1][0]    = -c01 * inv;
+    ij[1][1]    = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * inv;
+    ij[1][2]    = -(J[0][0] * J[1][2] - J[0][2] * J[1][0]) * inv;
+    ij[2][0]    = c02 * inv;
+    ij[2][1]    = -(J[0][0] * J[2][1] - J[0][1] * J[2][0]) * inv;
+    ij[2][2]    = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * inv;
+    return det;
+  }
+}
+
+// Shared-memory footprint per cell (bytes): nodal states (FP64), flux values / upwind
+// matrices (aliased: phase B-C vs D), u_q and r_q.
+// Strides are odd numbers of elements so that the lanes of a warp, which work on different
+// cells, fall on different banks.
+template <typename T, int D, int NDOF, int NQ, int NFL>
+struct EulerSmem
+{
+  static constexpr int odd(int n) { return n | 1; }
+  static constexpr int NEQ   = D + 2;
+  static constexpr int U     = odd(NDOF * NEQ);                   // doubles per cell
+  static constexpr int KS    = NEQ * NEQ + 1;                     // T per node matrix
+  static constexpr int FK_F  = NFL * NEQ * D;                     // T (phase B-C)
+  static constexpr int FK_K  = NDOF * KS;                         // T (phase D)
+  static constexpr int FK    = odd(FK_F > FK_K ? FK_F : FK_K);
+  static constexpr int QV    = NQ * NEQ;                          // T, u_q then r_q
+  static constexpr int QV2   = odd(2 * QV);
+  static constexpr int BYTES = U * 8 + FK * (int)sizeof(T) + QV2 * (int)sizeof(T);
+};
+
+template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, bool AFFINE,
+          int G>
+__global__ void __launch_bounds__(kBlock)
+    cells_euler(const CellArgs a, const Tables<T, (PHYS == RDS_EULER3D ? 3 : 2), NDOF, NQ, NFL,
+                                                NGEO> tb)
+{
+  constexpr int D   = (PHYS == RDS_EULER3D) ? 3 : 2;
+  constexpr int NEQ = D + 2;
+  constexpr int NPT = (NDOF + G - 1) / G; // nodes per lane
+  using SM          = EulerSmem<T, D, NDOF, NQ, NFL>;
+  constexpr int CPB = kBlock / G; // cells per block
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (*a.stop)
+    return;
+
+  const int lane  = threadIdx.x % G;
+  const int slot  = threadIdx.x / G; // cell within the block
+  const int c     = blockIdx.x * CPB + slot;
+  const bool live = c < a.ncells;
+  const int cc    = live ? c : a.ncells - 1; // dead groups shadow the last cell, write nothing
+
+  // per-cell shared-memory regions
+  double *su = reinterpret_cast<double *>(smem_raw) + (size_t)slot * SM::U;
+  T *sfk = reinterpret_cast<T *>(reinterpret_cast<double *>(smem_raw) + (size_t)CPB * SM::U) +
+           (size_t)slot * SM::FK;
+  T *suq = reinterpret_cast<T *>(reinterpret_cast<double *>(smem_raw) + (size_t)CPB * SM::U) +
+           (size_t)CPB * SM::FK + (size_t)slot * SM::QV2;
+  T *srq = suq + SM::QV;
+
+  // ---- A: nodal states
+  for (int i = lane; i < NDOF * NEQ; i += G)
+  {
+    const int n = i / NEQ, e = i % NEQ;
+    const int v = __ldg(a.sol_conn + (size_t)n * a.ncells + cc);
+    su[i]       = __ldg(a.u + (size_t)e * a.nnodes + v);
+  }
+  T X[NGEO][D];
+#pragma unroll
+  for (int g = 0; g < NGEO; ++g)
+  {
+    const int v = __ldg(a.geo_conn + (size_t)g * a.ncells + cc);
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+      X[g][d] = T(__ldg(a.X + (size_t)d * a.ngeo_nodes + v));
+  }
+  __syncwarp();
+
+  const T gamma = T(a.gamma);
+  bool bad      = false;
+
+  // ---- B: flux at the flux nodes
+  for (int f = lane; f < NFL; f += G)
+  {
+    T s[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+    {
+      T acc = tb.Vsf[f][0] * T(su[e]);
+#pragma unroll
+      for (int n = 1; n < NDOF; ++n)
+        acc = acc + tb.Vsf[f][n] * T(su[n * NEQ + e]);
+      s[e] = acc;
+    }
+    EulerProps<T, D> p;
+    bad |= euler_props<T, D>(s, gamma, p);
+    T F[NEQ][D];
+    euler_flux<T, D>(s, p, F);
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+        sfk[(f * NEQ + e) * D + d] = F[e][d];
+  }
+  __syncwarp();
+
+  // affine cells: one Jacobian for all points
+  T ijc[D][D];
+  T detc = T(0);
+  if (AFFINE)
+    detc = jacobian_at(tb, 0, X, ijc);
+
+  // ---- C: u_q and flux divergence r_q
+  for (int q = lane; q < NQ; q += G)
+  {
+    T ij[D][D];
+    if (AFFINE)
+    {
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j)
+          ij[i][j] = ijc[i][j];
+    }
+    else
+      jacobian_at(tb, q, X, ij);
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+    {
+      T acc = tb.V[q][0] * T(su[e]);
+#pragma unroll
+      for (int n = 1; n < NDOF; ++n)
+        acc = acc + tb.V[q][n] * T(su[n * NEQ + e]);
+      suq[q * NEQ + e] = acc;
+      T r = T(0);
+#pragma unroll
+      for (int ic = 0; ic < D; ++ic)
+      {
+        T dref[D];
+#pragma unroll
+        for (int xi = 0; xi < D; ++xi)
+        {
+          T s2 = tb.dVf[xi][q][0] * sfk[(0 * NEQ + e) * D + ic];
+#pragma unroll
+          for (int f = 1; f < NFL; ++f)
+            s2 = s2 + tb.dVf[xi][q][f] * sfk[(f * NEQ + e) * D + ic];
+          dref[xi] = s2;
+        }
+        T dphys = ij[ic][0] * dref[0];
+#pragma unroll
+        for (int xi = 1; xi < D; ++xi)
+          dphys = dphys + ij[ic][xi] * dref[xi];
+        r = r + dphys;
+      }
+      srq[q * NEQ + e] = r;
+    }
+  }
+  __syncwarp();
+
+  // ---- D: quadrature loop, nodes distributed over the lanes
+  double lda[NPT][NEQ], diss[NPT][NEQ];
+#pragma unroll
+  for (int s = 0; s < NPT; ++s)
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+    {
+      lda[s][e]  = 0.0;
+      diss[s][e] = 0.0;
+    }
+  double phi0 = 0.0, vol = 0.0;
+  T wsmax     = T(0);
+
+  for (int q = 0; q < NQ; ++q)
+  {
+    T ij[D][D];
+    T det;
+    if (AFFINE)
+    {
+      det = detc;
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j)
+          ij[i][j] = ijc[i][j];
+    }
+    else
+      det = jacobian_at(tb, q, X, ij);
+    const double wj = double(tb.w[q] * det);
+    vol += wj;
+
+    T uq[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+      uq[e] = suq[q * NEQ + e];
+    EulerProps<T, D> p;
+    bad |= euler_props<T, D>(uq, gamma, p);
+
+    double SK[NEQ][NEQ], SKu[NEQ];
+#pragma unroll
+    for (int i = 0; i < NEQ; ++i)
+    {
+      SKu[i] = 0.0;
+#pragma unroll
+      for (int j = 0; j < NEQ; ++j)
+        SK[i][j] = 0.0;
+    }
+
+#pragma unroll
+    for (int s = 0; s < NPT; ++s)
+    {
+      const int n = lane + s * G;
+      if (n < NDOF)
+      {
+        T gref[D], gphys[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+          gref[d] = tb.dV[d][q][n];
+#pragma unroll
+        for (int x = 0; x < D; ++x)
+        {
+          T acc = ij[x][0] * gref[0];
+#pragma unroll
+          for (int xi = 1; xi < D; ++xi)
+            acc = acc + ij[x][xi] * gref[xi];
+          gphys[x] = acc;
+        }
+        T K[NEQ][NEQ], lam[NEQ];
+        euler_K<+1, T, D>(p, gphys, gamma, K, lam);
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          wsmax = fmax(wsmax, fmax(T(1.e-6), fabs(lam[e])));
+        T *Kn = sfk + (size_t)n * SM::KS;
+#pragma unroll
+        for (int i = 0; i < NEQ; ++i)
+        {
+          double ku = 0.0;
+#pragma unroll
+          for (int j = 0; j < NEQ; ++j)
+          {
+            Kn[i * NEQ + j] = K[i][j];
+            SK[i][j] += double(K[i][j]);
+            ku += double(K[i][j]) * su[n * NEQ + j];
+          }
+          SKu[i] += ku;
+        }
+      }
+    }
+    // complete the sums over the group (identical in every lane)
+#pragma unroll
+    for (int i = 0; i < NEQ; ++i)
+    {
+      SKu[i] = group_sum<G>(SKu[i]);
+#pragma unroll
+      for (int j = 0; j < NEQ; ++j)
+        SK[i][j] = group_sum<G>(SK[i][j]);
+    }
+    double v[NEQ], ub[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+    {
+      v[e]  = double(srq[q * NEQ + e]);
+      ub[e] = SKu[e];
+    }
+    phi0 += wj * v[0];
+    lu_solve2<NEQ>(SK, v, ub);
+
+#pragma unroll
+    for (int s = 0; s < NPT; ++s)
+    {
+      const int n = lane + s * G;
+      if (n < NDOF)
+      {
+        const T *Kn = sfk + (size_t)n * SM::KS;
+        double du[NEQ];
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          du[e] = su[n * NEQ + e] - ub[e];
+#pragma unroll
+        for (int i = 0; i < NEQ; ++i)
+        {
+          double kv = 0.0, kd = 0.0;
+#pragma unroll
+          for (int j = 0; j < NEQ; ++j)
+          {
+            const double kij = double(Kn[i * NEQ + j]);
+            kv += kij * v[j];
+            kd += kij * du[j];
+          }
+          lda[s][i] += wj * kv;
+          if (SCHEME != RDS_PGLDA)
+            diss[s][i] += wj * kd;
+        }
+      }
+    }
+  }
+
+  // ---- E: blending, outputs
+  double theta = 1.0;
+  if (SCHEME == RDS_PGB)
+  {
+    double part = 0.0;
+#pragma unroll
+    for (int s = 0; s < NPT; ++s)
+      if (lane + s * G < NDOF)
+        part += fabs(lda[s][0] + diss[s][0]);
+    const double abs_phiN = group_sum<G>(part);
+    theta                 = fabs(phi0) / (abs_phiN + 1.e-6);
+  }
+  const double wmax = group_max<G>(double(wsmax));
+  if (live)
+  {
+#pragma unroll
+    for (int s = 0; s < NPT; ++s)
+    {
+      const int n = lane + s * G;
+      if (n < NDOF)
+      {
+        const long long slot0 = a.slot_base + (long long)n * a.ncells + c;
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+        {
+          const double r = (SCHEME == RDS_PGLDA) ? lda[s][e] : lda[s][e] + theta * diss[s][e];
+          __stcs(a.contrib + e * a.S + slot0, r);
+        }
+      }
+    }
+    if (lane == 0)
+      __stcs(a.wsc + a.ws_base + c, vol * wmax);
+    if (bad)
+      atomicOr(a.status, kFlagNegPressure);
+  }
+}
+
+template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, int G>
+cudaError_t launch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream_t s)
+{
+  constexpr int D = (PHYS == RDS_EULER3D) ? 3 : 2;
+  Tables<T, D, NDOF, NQ, NFL, NGEO> tb;
+  fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
+  constexpr int CPB  = kBlock / G;
+  const int smem     = CPB * EulerSmem<T, D, NDOF, NQ, NFL>::BYTES;
+  const int grid     = (a.ncells + CPB - 1) / CPB;
+  // the shared-memory opt-in is set once per instantiation (not a stream operation, so it
+  // also stays out of captured graphs)
+  static bool attr_set = false;
+  auto k_aff           = cells_euler<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, true, G>;
+  auto k_gen           = cells_euler<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, false, G>;
+  if (!attr_set)
+  {
+    cudaError_t e = cudaFuncSetAttribute(k_aff, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_gen, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess)
+      return e;
+    attr_set = true;
+  }
+  if (g.affine)
+    k_aff<<<grid, kBlock, smem, s>>>(a, tb);
+  else
+    k_gen<<<grid, kBlock, smem, s>>>(a, tb);
+  return cudaGetLastError();
+}
+
+template <int PHYS, int SCHEME, typename T>
+cudaError_t dispatch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream_t s, bool *ok)
+{
+  const rds_cell_group &d = g.desc;
+  *ok                     = true;
+  if constexpr (PHYS == RDS_EULER2D)
+  {
+    if (d.shape == RDS_TRIAG && d.ngeo == 3)
+    {
+      if (d.ndof == 3 && d.nq == 6 && d.nfl == 6)
+        return launch_euler<PHYS, SCHEME, T, 3, 6, 6, 3, 4>(g, a, s);
+      if (d.ndof == 6 && d.nq == 7 && d.nfl == 10)
+        return launch_euler<PHYS, SCHEME, T, 6, 7, 10, 3, 4>(g, a, s);
+      if (d.ndof == 10 && d.nq == 16 && d.nfl == 15)
+        return launch_euler<PHYS, SCHEME, T, 10, 16, 15, 3, 4>(g, a, s);
+    }
+    if (d.shape == RDS_QUAD && d.ngeo == 4)
+    {
+      if (d.ndof == 16 && d.nq == 20 && d.nfl == 25)
+        return launch_euler<PHYS, SCHEME, T, 16, 20, 25, 4, 8>(g, a, s);
+      if (d.ndof == 16 && d.nq == 25 && d.nfl == 25)
+        return launch_euler<PHYS, SCHEME, T, 16, 25, 25, 4, 8>(g, a, s);
+    }
+  }
+  else
+  {
+    if (d.shape == RDS_TETRA && d.ngeo == 4)
+    {
+      if (d.ndof == 10 && d.nq == 14 && d.nfl == 20)
+        return launch_euler<PHYS, SCHEME, T, 10, 14, 20, 4, 4>(g, a, s);
+    }
+  }
+  *ok = false;
+  return cudaSuccess;
+}
+
+const char *euler_name(int physics, int scheme)
+{
+  static const char *names[2][3] = {{"cells_euler2d_lda", "cells_euler2d_n", "cells_euler2d_b"},
+                                    {"cells_euler3d_lda", "cells_euler3d_n", "cells_euler3d_b"}};
+  return names[physics == RDS_EULER3D ? 1 : 0][scheme];
+}
+
+} // namespace
+
+cudaError_t launch_cells_euler(const HostCellGroup &g, const CellArgs &a, int physics, int scheme,
+                               int precision, cudaStream_t s, const char **name, bool *ok)
+{
+  *name = euler_name(physics, scheme);
+#define RDS_EULER_CASE(PH, SC)                                                                     \
+  if (physics == PH && scheme == SC)                                                               \
+    return precision == RDS_MIXED ? dispatch_euler<PH, SC, float>(g, a, s, ok)                     \
+                                  : dispatch_euler<PH, SC, double>(g, a, s, ok);
+  RDS_EULER_CASE(RDS_EULER2D, RDS_PGLDA)
+  RDS_EULER_CASE(RDS_EULER2D, RDS_PGN)
+  RDS_EULER_CASE(RDS_EULER2D, RDS_PGB)
+  RDS_EULER_CASE(RDS_EULER3D, RDS_PGLDA)
+  RDS_EULER_CASE(RDS_EULER3D, RDS_PGN)
+  RDS_EULER_CASE(RDS_EULER3D, RDS_PGB)
+#undef RDS_EULER_CASE
+  *ok = false;
   return cudaSuccess;
 }
 

@@ -86,6 +86,8 @@ struct BCArgs
   double *__restrict__ wsc;
   long long ws_base;
   double adv0, adv1, gamma;
+  double relax;      // WeakWall: 1 for P1 facets, 1/(3p) otherwise
+  double params[4];  // WeakSubInlet: T_tot, p_tot; WeakSubOutlet: p_out
   unsigned *status;
   const int *stop;
 };

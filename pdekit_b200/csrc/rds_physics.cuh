@@ -58,6 +58,22 @@ __device__ __forceinline__ void euler_flux(const T *u, const EulerProps<T, D> &p
   }
 }
 
+// Flux through direction n: F(u) . n (Euler2DCons::flux(p, direction, flux),
+// physics/euler/Euler2DCons.hpp:253-266; Euler3DCons.hpp:267-285).
+template <typename T, int D>
+__device__ __forceinline__ void euler_flux_n(const T *u, const EulerProps<T, D> &p, const T *n,
+                                             T *F)
+{
+  T rhoum = u[1] * n[0] + u[2] * n[1];
+  if (D == 3)
+    rhoum = u[1] * n[0] + u[2] * n[1] + u[D] * n[D - 1];
+  F[0] = rhoum;
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+    F[1 + d] = rhoum * p.V[d] + p.P * n[d];
+  F[D + 1] = rhoum * p.H;
+}
+
 // Right/left eigenvectors R, L and eigenvalues lam of the flux Jacobian in direction dir.
 template <typename T>
 __device__ __forceinline__ void euler_eigen(const EulerProps<T, 2> &p, const T *dir, T gamma,

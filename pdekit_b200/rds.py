@@ -31,7 +31,7 @@ PHYSICS = {"advconst": 0, "burgers": 1, "euler2d": 2, "euler3d": 3}
 SCHEME = {"lda": 0, "n": 1, "b": 2}
 PRECISION = {"fp64": 0, "mixed": 1}
 SHAPE = {"line": 2, "triag": 3, "quad": 4, "tetra": 10}
-BC_KIND = {"WeakDirichlet": 0}
+BC_KIND = {"WeakDirichlet": 0, "WeakWall": 1, "WeakSubInlet": 2, "WeakSubOutlet": 3}
 
 STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "NONFINITE", 4: "NEG_PRESSURE", 5: "ITER_CAP",
           6: "UNSUPPORTED", 7: "TOO_LARGE"}
@@ -70,7 +70,8 @@ class _BCGroup(C.Structure):
     _fields_ = [("kind", C.c_int), ("nfacets", C.c_int), ("nfdof", C.c_int),
                 ("nfgeo", C.c_int), ("nfq", C.c_int), ("sol_conn", C.c_void_p),
                 ("geo_conn", C.c_void_p), ("fw", C.c_void_p), ("fV", C.c_void_p),
-                ("fdVgeo", C.c_void_p), ("gq", C.c_void_p)]
+                ("fdVgeo", C.c_void_p), ("gq", C.c_void_p), ("order", C.c_int),
+                ("params", C.c_double * 4)]
 
 
 _lib = None
@@ -188,6 +189,9 @@ class PGRDMethodExplicit:
         self._keep += arrs
         cb = _BCGroup(BC_KIND[b.kind], b.nfacets, b.nfdof, b.nfgeo, b.nfq,
                       *[_ptr(a) for a in arrs])
+        cb.order = b.order
+        for k, v in enumerate(b.params[:4]):
+            cb.params[k] = v
         self._check(lib().rds_add_bc(self._ctx, C.byref(cb)))
 
     def initialize_work_data(self):
