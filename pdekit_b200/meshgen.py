@@ -390,3 +390,142 @@ def write_gmsh22_mesh(path: str, mesh: Mesh, domain_name: str = "domain") -> Non
     lines.append("$EndElements")
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
+
+
+# ---------------------------------------------------------------------------------------------
+# Continuous P_p numbering of a general mesh (vectorised)
+# ---------------------------------------------------------------------------------------------
+
+CELL_EDGES = {"triag": [(0, 1), (1, 2), (2, 0)],
+              "quad": [(0, 1), (1, 2), (2, 3), (3, 0)],
+              "tetra": [(0, 1), (1, 2), (2, 0), (3, 0), (3, 2), (3, 1)]}
+TET_FACES = [(0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3)]
+
+
+def _ref_nodes(shape, p):
+    from . import reference_element as R
+    return {"triag": lambda: equidist_triag_nodes(p), "quad": lambda: R.quad_nodes(p),
+            "tetra": lambda: R.tet_nodes(p)}[shape]()
+
+
+def _p1_map(shape, ref):
+    """Weights [nref, nvert] of the P1 geometry map at reference points."""
+    if shape == "quad":
+        from . import reference_element as R
+        V, _ = R.lagrange_quad(1, ref)
+        return V
+    lam = (ref + 1.0) * 0.5
+    return np.concatenate([1.0 - lam.sum(axis=1, keepdims=True), lam], axis=1)
+
+
+@dataclasses.dataclass
+class Clone:
+    p: int
+    conn: dict  # shape -> [nc, ndof] int32
+    nsol: int
+    coords: np.ndarray  # [nsol, dim]
+    edge_index: dict  # (min, max) vertex pair -> edge id (only via lookup arrays below)
+    edge_keys: np.ndarray  # [nedges, 2] sorted vertex pairs
+    edge_base: int  # first edge-dof id
+    face_keys: np.ndarray = None  # [nfaces, 3] sorted (tets, p = 3)
+    face_base: int = 0
+
+
+def clone_continuous(mesh: Mesh, p: int) -> Clone:
+    """Continuous P_p dofs over all cell groups of `mesh` (vertices keep their ids; then one
+    block of p-1 nodes per edge, ordered from the lower to the higher vertex id; then one node
+    per tetrahedron face for p = 3; then cell-interior nodes group by group). The local order in
+    every cell follows the reference elements: vertices, edges in local order and direction,
+    faces, interior."""
+    nv = mesh.coords.shape[0]
+    ne_int = p - 1
+    all_edges = []
+    for shape, cells in mesh.cells.items():
+        for a, b in CELL_EDGES[shape]:
+            all_edges.append(np.sort(cells[:, [a, b]], axis=1))
+    all_edges = np.concatenate(all_edges) if all_edges else np.zeros((0, 2), np.int32)
+    edge_keys, _ = np.unique(all_edges, axis=0, return_inverse=True)
+    edge_base = nv
+    next_id = nv + edge_keys.shape[0] * ne_int
+    ekey = edge_keys[:, 0].astype(np.int64) * (nv + 1) + edge_keys[:, 1]
+
+    def edge_ids(u, v):
+        lo, hi = np.minimum(u, v), np.maximum(u, v)
+        idx = np.searchsorted(ekey, lo.astype(np.int64) * (nv + 1) + hi)
+        return idx, u > v
+
+    face_keys, face_base = None, 0
+    if p == 3 and "tetra" in mesh.cells:
+        t = mesh.cells["tetra"]
+        allf = np.concatenate([np.sort(t[:, list(f)], axis=1) for f in TET_FACES])
+        face_keys = np.unique(allf, axis=0)
+        face_base = next_id
+        next_id += face_keys.shape[0]
+    if p > 3 and "tetra" in mesh.cells:
+        raise ValueError("tetrahedra up to P3")
+
+    conn, coords_parts = {}, []
+    for shape, cells in mesh.cells.items():
+        nc = cells.shape[0]
+        ref = _ref_nodes(shape, p)
+        ndof = ref.shape[0]
+        c = np.empty((nc, ndof), dtype=np.int64)
+        nvert = cells.shape[1]
+        c[:, :nvert] = cells
+        k = nvert
+        for a, b in CELL_EDGES[shape]:
+            idx, rev = edge_ids(cells[:, a], cells[:, b])
+            for i in range(ne_int):
+                j = np.where(rev, ne_int - 1 - i, i)
+                c[:, k + i] = edge_base + idx * ne_int + j
+            k += ne_int
+        if shape == "tetra" and p == 3:
+            fkey = face_keys[:, 0].astype(np.int64) * (nv + 1) ** 2 + \
+                face_keys[:, 1].astype(np.int64) * (nv + 1) + face_keys[:, 2]
+            for f in TET_FACES:
+                s = np.sort(cells[:, list(f)], axis=1).astype(np.int64)
+                key = s[:, 0] * (nv + 1) ** 2 + s[:, 1] * (nv + 1) + s[:, 2]
+                c[:, k] = face_base + np.searchsorted(fkey, key)
+                k += 1
+        n_int = ndof - k
+        if n_int > 0:
+            c[:, k:] = next_id + np.arange(nc * n_int).reshape(nc, n_int)
+            next_id += nc * n_int
+        conn[shape] = c.astype(np.int32)
+        W = _p1_map(shape, ref)  # [ndof, nvert]
+        coords_parts.append((c, np.einsum("nk,ckd->cnd", W, mesh.coords[cells])))
+    coords = np.zeros((next_id, mesh.dim))
+    for c, xy in coords_parts:
+        coords[c.ravel()] = xy.reshape(-1, mesh.dim)
+    return Clone(p=p, conn=conn, nsol=int(next_id), coords=coords, edge_index=None,
+                 edge_keys=edge_keys, edge_base=edge_base, face_keys=face_keys,
+                 face_base=face_base)
+
+
+def boundary_facets(mesh: Mesh, clone: Clone, name: str):
+    """(geometry vertices [nf, nfv], solution dofs [nf, nfdof]) of a named boundary, facets in
+    the orientation stored in the mesh (outward normals): lines [u, v, edge nodes u->v];
+    triangles [a, b, c, edges (a b), (b c), (c a)]."""
+    shape, fac = mesh.boundaries[name]
+    p = clone.p
+    nv = mesh.coords.shape[0]
+    ekey = clone.edge_keys[:, 0].astype(np.int64) * (nv + 1) + clone.edge_keys[:, 1]
+    ne_int = p - 1
+
+    def edge_nodes(u, v):
+        lo, hi = np.minimum(u, v), np.maximum(u, v)
+        idx = np.searchsorted(ekey, lo.astype(np.int64) * (nv + 1) + hi)
+        rev = u > v
+        return np.stack([clone.edge_base + idx * ne_int + np.where(rev, ne_int - 1 - i, i)
+                         for i in range(ne_int)], axis=1) if ne_int else np.zeros((len(u), 0), int)
+
+    if shape == "line":
+        sol = np.concatenate([fac, edge_nodes(fac[:, 0], fac[:, 1])], axis=1)
+    else:
+        parts = [fac]
+        for a, b in ((0, 1), (1, 2), (2, 0)):
+            parts.append(edge_nodes(fac[:, a], fac[:, b]))
+        if p == 3:
+            raise ValueError("P3 tetrahedron faces need the face node")
+        sol = np.concatenate(parts, axis=1)
+    return fac.astype(np.int32), sol.astype(np.int32)

@@ -162,3 +162,202 @@ def triag_tables(p: int, quad_order: int, geo_order: int = 1) -> dict:
     fVgeo, fdVgeo = lagrange_line(geo_order, fqp)
     return dict(qp=qp, w=w, V=V, dV=dV, dVgeo=dVgeo, dVf=dVf, Vsf=Vsf, fqp=fqp, fw=fw, fV=fV,
                 fVgeo=fVgeo, fdVgeo=fdVgeo)
+
+
+# ---------------------------------------------------------------------------------------------
+# Quadrilaterals and tetrahedra, more rules
+# ---------------------------------------------------------------------------------------------
+
+# Dunavant degree 6, 12 points (area-1 weights).
+_DUNAVANT[6] = [("s21", 0.116786275726379, 0.249286745170910),
+                ("s21", 0.050844906370207, 0.063089014491502),
+                ("s111", 0.082851075618374, 0.053145049844817, 0.310352451033784)]
+# Dunavant degree 3, 4 points (centroid weight negative), exact rational weights.
+_DUNAVANT[3] = [("s3", -27.0 / 48.0), ("s21", 25.0 / 48.0, 0.2)]
+
+
+def quad_nodes(p: int) -> np.ndarray:
+    """Equidistant nodes of the reference square [-1,1]^2 in the reference's order: the four
+    corners counter-clockwise from (-1,-1), the edge nodes of edges (v0 v1), (v1 v2), (v2 v3),
+    (v3 v0), then the interior nodes as a square of order p-2 numbered the same way."""
+    pts = []
+
+    def layer(lo: float, q: int, h: float):
+        hi = -lo
+        if q == 0:
+            pts.append((lo, lo) if lo == hi else (0.0, 0.0))
+            return
+        c = [(lo, lo), (hi, lo), (hi, hi), (lo, hi)]
+        pts.extend(c)
+        for k in range(4):
+            a, b = c[k], c[(k + 1) % 4]
+            for i in range(1, q):
+                t = i / q
+                pts.append((a[0] + t * (b[0] - a[0]), a[1] + t * (b[1] - a[1])))
+        if q >= 2:
+            layer(lo + h, q - 2, h)
+
+    layer(-1.0, p, 2.0 / p)
+    return np.asarray(pts, dtype=np.float64)
+
+
+def lagrange_quad(p: int, pts: np.ndarray):
+    """Tensor-product equidistant Lagrange basis on the square: V [npts, ndof], dV [2, npts, ndof]."""
+    pts = np.asarray(pts, dtype=np.float64)
+    nodes = quad_nodes(p)
+    g = np.linspace(-1.0, 1.0, p + 1)
+
+    def basis_1d(i, x):
+        v = np.ones_like(x)
+        dv = np.zeros_like(x)
+        for k in range(p + 1):
+            if k == i:
+                continue
+            den = g[i] - g[k]
+            dv = dv * (x - g[k]) / den + v / den
+            v = v * (x - g[k]) / den
+        return v, dv
+
+    V = np.empty((pts.shape[0], nodes.shape[0]))
+    dV = np.empty((2, pts.shape[0], nodes.shape[0]))
+    for j, (a, b) in enumerate(nodes):
+        i1 = int(round((a + 1.0) / 2.0 * p))
+        i2 = int(round((b + 1.0) / 2.0 * p))
+        vx, dvx = basis_1d(i1, pts[:, 0])
+        vy, dvy = basis_1d(i2, pts[:, 1])
+        V[:, j] = vx * vy
+        dV[0, :, j] = dvx * vy
+        dV[1, :, j] = vx * dvy
+    return V, dV
+
+
+def quad_gauss(order: int):
+    """Tensor Gauss-Legendre rule on [-1,1]^2 with n = order // 2 + 1 points per direction."""
+    x, w = line_gauss(order)
+    x = x.ravel()
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    W = np.outer(w, w)
+    return np.stack([X.ravel(), Y.ravel()], axis=1), W.ravel()
+
+
+_TET_V = np.array([[-1.0, -1.0, -1.0], [1.0, -1.0, -1.0], [-1.0, 1.0, -1.0], [-1.0, -1.0, 1.0]])
+_TET_EDGES = [(0, 1), (1, 2), (2, 0), (3, 0), (3, 2), (3, 1)]
+_TET_FACES = [(0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3)]
+
+
+def tet_nodes(p: int) -> np.ndarray:
+    """Equidistant nodes of the reference tetrahedron (-1,-1,-1),(1,-1,-1),(-1,1,-1),(-1,-1,1)
+    in the reference's order: vertices, edges (v0 v1), (v1 v2), (v2 v0), (v3 v0), (v3 v2),
+    (v3 v1), then one centroid node per face (p = 3). Orders up to 3."""
+    if p > 3:
+        raise ValueError("tetrahedra up to order 3")
+    pts = [tuple(v) for v in _TET_V]
+    for a, b in _TET_EDGES:
+        for i in range(1, p):
+            t = i / p
+            pts.append(tuple(_TET_V[a] + t * (_TET_V[b] - _TET_V[a])))
+    if p == 3:
+        for f in _TET_FACES:
+            pts.append(tuple(_TET_V[list(f)].mean(axis=0)))
+    return np.asarray(pts, dtype=np.float64)
+
+
+def lagrange_tet(p: int, pts: np.ndarray):
+    """Equidistant tetrahedron basis (Silvester's formula in 4 barycentrics):
+    V [npts, ndof], dV [3, npts, ndof]."""
+    pts = np.asarray(pts, dtype=np.float64)
+    nodes = tet_nodes(p)
+    lam = [None, (pts[:, 0] + 1) * 0.5, (pts[:, 1] + 1) * 0.5, (pts[:, 2] + 1) * 0.5]
+    lam[0] = 1.0 - lam[1] - lam[2] - lam[3]
+    V = np.empty((pts.shape[0], nodes.shape[0]))
+    dV = np.empty((3, pts.shape[0], nodes.shape[0]))
+    for j, node in enumerate(nodes):
+        idx = [int(round((node[k] + 1.0) * 0.5 * p)) for k in range(3)]
+        idx = [p - sum(idx)] + idx
+        r, dr = zip(*[_silvester(idx[k], p, lam[k]) for k in range(4)])
+        V[:, j] = r[0] * r[1] * r[2] * r[3]
+        for d in range(3):
+            # d lam_{d+1} / d xi_d = 1/2, d lam_0 / d xi_d = -1/2
+            prod_d = [r[k] for k in range(4)]
+            prod_d[d + 1] = dr[d + 1]
+            prod_0 = [r[k] for k in range(4)]
+            prod_0[0] = dr[0]
+            dV[d, :, j] = 0.5 * (np.prod(prod_d, axis=0) - np.prod(prod_0, axis=0))
+    return V, dV
+
+
+# Symmetric tetrahedron rules on the unit tetrahedron (volume-1/6 weights):
+#   ("s4", w) centroid; ("s31", w, a): (a,a,a,1-3a) x 4; ("s22", w, a): (a,a,1/2-a,1/2-a) x 6.
+_TET_RULES = {
+    1: [("s4", 1.0 / 6.0)],
+    2: [("s31", 1.0 / 24.0, (5.0 - np.sqrt(5.0)) / 20.0)],
+    # 14-point degree-5 rule (Walkington; the rule pdekit tabulates for order 5)
+    5: [("s31", 0.01224884051939366, 0.0927352503108912),
+        ("s31", 0.01878132095300264, 0.3108859192633006),
+        ("s22", 0.007091003462846911, 0.4544962958743504)],
+}
+
+
+def tet_gauss(order: int):
+    """Points [n,3] on the reference tetrahedron and weights [n] (sum 4/3)."""
+    if order not in _TET_RULES:
+        raise ValueError(f"no tetrahedron rule of order {order}")
+    bary, w = [], []
+    for orb in _TET_RULES[order]:
+        if orb[0] == "s4":
+            bary.append((0.25, 0.25, 0.25, 0.25))
+            w.append(orb[1])
+        elif orb[0] == "s31":
+            _, wt, a = orb
+            b = 1.0 - 3.0 * a
+            for k in range(4):
+                t = [a] * 4
+                t[k] = b
+                bary.append(tuple(t))
+                w.append(wt)
+        else:
+            _, wt, a = orb
+            b = 0.5 - a
+            for i in range(4):
+                for j in range(i + 1, 4):
+                    t = [b] * 4
+                    t[i] = a
+                    t[j] = a
+                    bary.append(tuple(t))
+                    w.append(wt)
+    bary = np.asarray(bary)
+    pts = -1.0 + 2.0 * bary[:, 1:4]
+    return pts, 8.0 * np.asarray(w)
+
+
+def quad_tables(p: int, quad_order: int, vol_order: int = None) -> dict:
+    """Tables for P p quadrilaterals with bilinear (P1) geometry."""
+    qp, w = quad_gauss(quad_order)
+    V, dV = lagrange_quad(p, qp)
+    _, dVgeo = lagrange_quad(1, qp)
+    _, dVf = lagrange_quad(p + 1, qp)
+    Vsf, _ = lagrange_quad(p, quad_nodes(p + 1))
+    vqp, wv = quad_gauss(p if vol_order is None else vol_order)
+    _, dVgeo_v = lagrange_quad(1, vqp)
+    fqp, fw = line_gauss(quad_order + 1)
+    fV, _ = lagrange_line(p, fqp)
+    fVgeo, fdVgeo = lagrange_line(1, fqp)
+    return dict(qp=qp, w=w, V=V, dV=dV, dVgeo=dVgeo, dVf=dVf, Vsf=Vsf, wv=wv, dVgeo_v=dVgeo_v,
+                fqp=fqp, fw=fw, fV=fV, fVgeo=fVgeo, fdVgeo=fdVgeo)
+
+
+def tet_tables(p: int, quad_order: int) -> dict:
+    """Tables for P p tetrahedra with affine geometry; boundary faces are P p triangles with the
+    triangle rule of order quad_order + 1."""
+    qp, w = tet_gauss(quad_order)
+    V, dV = lagrange_tet(p, qp)
+    _, dVgeo = lagrange_tet(1, qp)
+    _, dVf = lagrange_tet(p + 1, qp)
+    Vsf, _ = lagrange_tet(p, tet_nodes(p + 1))
+    vqp, wv = tet_gauss(2 if p >= 2 else 1)
+    _, dVgeo_v = lagrange_tet(1, vqp)
+    fqp, fw = triag_gauss(quad_order + 1)
+    fV, _ = lagrange_triag(p, fqp)
+    fVgeo, fdVgeo = lagrange_triag(1, fqp)
+    return dict(qp=qp, w=w, V=V, dV=dV, dVgeo=dVgeo, dVf=dVf, Vsf=Vsf, wv=wv, dVgeo_v=dVgeo_v,
+                fqp=fqp, fw=fw, fV=fV, fVgeo=fVgeo, fdVgeo=fdVgeo)

@@ -67,3 +67,100 @@ def sol_coords_tri(n: int, jitter: float, seed: int, p: int) -> np.ndarray:
     mesh = meshgen.unit_square_tri(n, jitter, seed=seed)
     _, _, xy = meshgen.clone_continuous_tri(mesh, p)
     return xy
+
+
+# ---------------------------------------------------------------------------------------------
+# Configurations 3 and 4 (Euler) on general meshes
+# ---------------------------------------------------------------------------------------------
+
+T_TOT, P_TOT, P_OUT = 307.6488978, 120195.4453, 101325.0
+
+
+def euler_bcs(dim: int):
+    """Weak walls, subsonic total-condition inlet and static-pressure outlet of the reference's
+    bump case (examples/testcases-rdm/Bump-RDS-2D-Explicit.cpp:137-150)."""
+    walls = [("WeakWall", "bottom_wall_bc", "bottom_wall"), ("WeakWall", "top_wall_bc", "top_wall")]
+    if dim == 3:
+        walls.append(("WeakWall", "side_walls_bc", "side_walls"))
+    return walls + [("WeakSubInlet", "inlet_bc", "inlet", (T_TOT, P_TOT, 0.0, 0.0)),
+                    ("WeakSubOutlet", "outlet_bc", "outlet", (P_OUT, 0.0, 0.0, 0.0))]
+
+
+def mesh_problem(mesh, physics: str, scheme: str, p: int, tables: dict, bcs) -> Problem:
+    """Problem on a general mesh: one cell group per element shape (tables[shape]), one weak
+    boundary condition per (kind, name, boundary[, params]) in `bcs`."""
+    clone = meshgen.clone_continuous(mesh, p)
+    dim = mesh.dim
+    neq = {"advconst": 1, "burgers": 1, "euler2d": 4, "euler3d": 5}[physics]
+    groups = []
+    for shape, conn in clone.conn.items():
+        t = tables[shape]
+        groups.append(CellGroup(sol_conn=conn, geo_conn=mesh.cells[shape], w=t["w"], V=t["V"],
+                                dV=t["dV"], dVgeo=t["dVgeo"], dVf=t["dVf"], Vsf=t["Vsf"],
+                                shape=shape, order=p, wv=t.get("wv"), dVgeo_v=t.get("dVgeo_v")))
+    prob = Problem(physics=physics, scheme=scheme, dim=dim, neq=neq, nnodes=clone.nsol,
+                   geo_coords=mesh.coords, groups=groups, bcs=[])
+    facet_tables = tables[next(iter(clone.conn))]
+    for spec in bcs:
+        kind, name, boundary = spec[:3]
+        params = spec[3] if len(spec) > 3 and not isinstance(spec[3], str) else (0.0,) * 4
+        geo, sol = meshgen.boundary_facets(mesh, clone, boundary)
+        t = facet_tables
+        b = BCGroup(kind=kind, name=name, sol_conn=sol, geo_conn=geo, fw=t["fw"], fV=t["fV"],
+                    fVgeo=t["fVgeo"], fdVgeo=t["fdVgeo"],
+                    gq=np.zeros((geo.shape[0], t["fw"].shape[0], neq)), order=p,
+                    params=tuple(params))
+        if kind == "WeakDirichlet":
+            b.gq = bcexpr.evaluate(spec[3], b.quadrature_coords(mesh.coords), neq)
+        prob.bcs.append(b)
+    prob.bcs.sort(key=lambda b: b.name)
+    prob.sol_coords = clone.coords
+    return prob
+
+
+def bump_state(xyz: np.ndarray, dim: int, mach: float) -> np.ndarray:
+    """Freestream of the bump cases (total 307.6488978 K / 120195.4453 Pa, R = 287.046) with a
+    +-1% perturbation of density and pressure that is a fixed pseudo-random function of the
+    coordinates (the same definition as the golden fixtures' harness)."""
+    gamma, R = 1.4, 287.046
+    f = 1.0 + 0.5 * (gamma - 1.0) * mach * mach
+    T = T_TOT / f
+    p0 = P_TOT / f ** (gamma / (gamma - 1.0))
+    x, y = xyz[:, 0], xyz[:, 1]
+    z = xyz[:, 2] if dim == 3 else np.zeros_like(x)
+
+    def h(a, b, c):
+        s = np.sin(12.9898 * a + 78.233 * b + 37.719 * c) * 43758.5453
+        return 2.0 * (s - np.floor(s)) - 1.0
+
+    rho = p0 / (R * T) * (1.0 + 0.01 * h(x, y, z))
+    p = p0 * (1.0 + 0.01 * h(y, z, x))
+    ux = mach * np.sqrt(gamma * R * T)
+    u = np.zeros((xyz.shape[0], dim + 2))
+    u[:, 0] = rho
+    u[:, 1] = rho * ux
+    u[:, dim + 1] = p / (gamma - 1.0) + 0.5 * rho * ux * ux
+    return u
+
+
+def config3(nx_tri=500, nx_quad=1000, ny=500, seed=3):
+    """Configuration 3: Euler 2D bump channel, P3 triangles (16-point rule) on x < 0 and P3
+    quadrilaterals (25-point rule) on x > 0, blended B scheme, Mach 0.5."""
+    from . import reference_element as R
+
+    mesh = meshgen.channel_2d(nx_tri, nx_quad, ny, jitter=0.0, seed=seed)
+    tables = {"triag": dict(R.triag_tables(3, 8), wv=R.triag_gauss(3)[1],
+                            dVgeo_v=R.lagrange_triag(1, R.triag_gauss(3)[0])[1]),
+              "quad": R.quad_tables(3, 8)}
+    prob = mesh_problem(mesh, "euler2d", "b", 3, tables, euler_bcs(2))
+    return prob, bump_state(prob.sol_coords, 2, 0.5)
+
+
+def config4(nx=128, ny=32, nz=32, seed=4):
+    """Configuration 4: Euler 3D bump box, 128 x 32 x 32 hexahedra split into 6 P2 tetrahedra
+    (786,432 cells), 14-point rule, LDA, Mach 0.6, vertices jittered by +-0.1h."""
+    from . import reference_element as R
+
+    mesh = meshgen.box_tet(nx, ny, nz, jitter=0.1, seed=seed)
+    prob = mesh_problem(mesh, "euler3d", "lda", 2, {"tetra": R.tet_tables(2, 5)}, euler_bcs(3))
+    return prob, bump_state(prob.sol_coords, 3, 0.6)

@@ -96,3 +96,27 @@ def test_mixed_precision_close_to_fp64(case):
     tol = 1e-5 if prob.neq == 1 else 1e-3
     assert rel_err(res, a["res1"]) < tol
     assert rel_err(ws, a["ws1"]) < 1e-5
+
+
+@pytest.mark.parametrize("which", ["config3_small", "config4_small"])
+def test_euler_workloads_match_oracle(which):
+    """Mixed P3 triangle + P3 quadrilateral channel (two cell groups, our own tables) and the
+    P2 tetrahedral bump box, GPU against the oracle over several iterations."""
+    from pdekit_b200 import workloads as W
+
+    prob, u0 = W.config3(6, 8, 4) if which == "config3_small" else W.config4(6, 3, 3)
+    s = _solver(prob)
+    s.set_solution(u0)
+    s.assemble_lhs_and_rhs(0.5)
+    res, dt, ws, vol = s.fields()
+    o = Oracle(prob)
+    r_ref, ws_ref, dt_ref, bad = o.assemble(u0, 0.5)
+    assert bad == 0
+    assert rel_err(vol, o.vol) < 1e-12
+    assert rel_err(res, r_ref) < 1e-11
+    assert rel_err(ws, ws_ref) < 1e-12
+    s.set_solution(u0)
+    s.iterate(0.5, 10)
+    u_ref, _ = o.iterate(u0, 0.5, 10)
+    assert rel_err(s.solution(), u_ref) < 1e-11
+    s.close()
