@@ -190,6 +190,10 @@ RDS_API rds_status rds_get_fields(rds_ctx *ctx, double *res_aos, double *dt, dou
 RDS_API rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int *it_done,
                        double *hist);
 
+/* Options: "mixed_switch" (default 1e-5): with RDS_MIXED, rds_iterate runs FP32 cell kernels
+ * until max_eq norm/norm(iter 0) <= mixed_switch and then finishes with FP64 sweeps. */
+RDS_API rds_status rds_set_option(rds_ctx *ctx, const char *key, double value);
+
 /* Enqueue n fused iterations (assemble_lhs_and_rhs(cfl) + solve()) on the context's stream and
  * return without waiting: no residual-drop test, no copies back. For timing with events on
  * rds_stream(); the norms of these iterations are not kept. */

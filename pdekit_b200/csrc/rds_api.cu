@@ -63,12 +63,17 @@ struct rds_ctx
   // pinned host scalars for the loop's stop test
   int *h_stop = nullptr;
 
-  // CUDA graph of the fused iteration
-  cudaGraphExec_t graph_exec = nullptr;
-  int graph_chunk            = 0;
-  double graph_cfl           = -1.0;
-  int graph_max_iter         = -1;
-  double graph_drop          = 0.0;
+  // CUDA graphs of a chunk of fused iterations, one per cell-kernel precision
+  cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+  int graph_chunk[2]            = {0, 0};
+  double graph_cfl[2]           = {-1.0, -1.0};
+  int graph_max_iter[2]         = {-1, -1};
+  double graph_drop[2]          = {0.0, 0.0};
+
+  // precision of the cell kernels being launched (the mixed loop finishes in FP64)
+  int active_precision = RDS_FP64;
+  // mixed form: relative residual at which the loop switches from FP32 to FP64 cell kernels
+  double mixed_switch = 1.e-5;
 
   bool timing = false;
   std::vector<TimingRec> trecs;
@@ -288,7 +293,8 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
   {
     const CellArgs a = cell_args(ctx, g, stop);
     rds_status st    = launch(ctx, [&](const char **name) {
-      return launch_cells(g, a, d.physics, d.scheme, d.precision, d.dim, d.neq, ctx->stream, name);
+      return launch_cells(g, a, d.physics, d.scheme, ctx->active_precision, d.dim, d.neq,
+                          ctx->stream, name);
     });
     if (st != RDS_OK)
       return st;
@@ -316,11 +322,12 @@ rds_status check_status(rds_ctx *ctx)
 
 void release_graph(rds_ctx *ctx)
 {
-  if (ctx->graph_exec)
-  {
-    cudaGraphExecDestroy(ctx->graph_exec);
-    ctx->graph_exec = nullptr;
-  }
+  for (int k = 0; k < 2; ++k)
+    if (ctx->graph_exec[k])
+    {
+      cudaGraphExecDestroy(ctx->graph_exec[k]);
+      ctx->graph_exec[k] = nullptr;
+    }
 }
 
 } // namespace
@@ -379,6 +386,7 @@ rds_status rds_create(rds_ctx **out, const rds_desc *desc, void *stream)
   *out         = nullptr;
   rds_ctx *ctx = new rds_ctx();
   ctx->desc    = *desc;
+  ctx->active_precision = desc->precision;
   const rds_desc &d = ctx->desc;
   if (!supported_physics(d) || d.scheme < RDS_PGLDA || d.scheme > RDS_PGB ||
       (d.precision != RDS_FP64 && d.precision != RDS_MIXED) || d.nnodes <= 0 ||
@@ -820,6 +828,74 @@ static rds_status enqueue_iteration(rds_ctx *ctx, double cfl, int max_iter, doub
   });
 }
 
+// Device loop at the active precision: chunks of `chunk` fused iterations captured once in a
+// CUDA graph and replayed until the device stop flag is raised (drop reached, iteration cap,
+// non-finite norm); the host polls the flag every 4 chunks.
+static rds_status run_loop(rds_ctx *ctx, double cfl, int max_iter, double drop)
+{
+  rds_status st;
+  const int chunk = std::min(max_iter, 16);
+  if (ctx->timing)
+  {
+    // event timing wants plain launches: run the loop without a graph
+    for (int it = 0; it < max_iter; ++it)
+      if ((st = enqueue_iteration(ctx, cfl, max_iter, drop)) != RDS_OK)
+        return st;
+    return RDS_OK;
+  }
+  const int gi = ctx->active_precision == RDS_MIXED ? 1 : 0;
+  if (!ctx->graph_exec[gi] || ctx->graph_cfl[gi] != cfl || ctx->graph_max_iter[gi] != max_iter ||
+      ctx->graph_drop[gi] != drop || ctx->graph_chunk[gi] != chunk)
+  {
+    if (ctx->graph_exec[gi])
+    {
+      cudaGraphExecDestroy(ctx->graph_exec[gi]);
+      ctx->graph_exec[gi] = nullptr;
+    }
+    cudaGraph_t graph;
+    RDS_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const long long l0 = ctx->launches;
+    for (int k = 0; k < chunk; ++k)
+    {
+      st = enqueue_iteration(ctx, cfl, max_iter, drop);
+      if (st != RDS_OK)
+      {
+        cudaStreamEndCapture(ctx->stream, &graph);
+        if (graph)
+          cudaGraphDestroy(graph);
+        return st;
+      }
+    }
+    ctx->launches = l0; // launches are counted when the graph runs
+    RDS_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(&ctx->graph_exec[gi], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess)
+      return fail(ctx, RDS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    ctx->graph_cfl[gi]      = cfl;
+    ctx->graph_max_iter[gi] = max_iter;
+    ctx->graph_drop[gi]     = drop;
+    ctx->graph_chunk[gi]    = chunk;
+  }
+  const long long per_iter = (long long)ctx->groups.size() + (long long)ctx->bcs.size() + 1;
+  const int nchunks        = (max_iter + chunk - 1) / chunk;
+  for (int k = 0; k < nchunks; ++k)
+  {
+    RDS_CUDA(cudaGraphLaunch(ctx->graph_exec[gi], ctx->stream));
+    ctx->launches += per_iter * chunk;
+    if (k + 1 < nchunks && (k % 4) == 3)
+    {
+      // poll the device stop flag now and then; chunks after a stop exit at once
+      RDS_CUDA(cudaMemcpyAsync(ctx->h_stop, ctx->d_stop, sizeof(int), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+      RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+      if (*ctx->h_stop)
+        break;
+    }
+  }
+  return RDS_OK;
+}
+
 rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int *it_done,
                        double *hist)
 {
@@ -842,62 +918,36 @@ rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int 
   RDS_CUDA(cudaMemsetAsync(ctx->d_stop, 0, sizeof(int), ctx->stream));
   RDS_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
 
-  const int chunk = std::min(max_iter, 16);
-  if (ctx->timing)
+  if (ctx->desc.precision == RDS_MIXED)
   {
-    // event timing wants plain launches: run the loop without a graph
-    for (int it = 0; it < max_iter; ++it)
-      if ((st = enqueue_iteration(ctx, cfl, max_iter, drop)) != RDS_OK)
+    // mixed form: FP32 cell kernels until the relative residual reaches mixed_switch, then a
+    // final FP64 phase of pseudo-time sweeps from that state to the requested drop; the
+    // iteration counter, the initial norm and the history continue across the switch
+    ctx->active_precision = RDS_MIXED;
+    const double drop1    = std::max(drop, ctx->mixed_switch);
+    if ((st = run_loop(ctx, cfl, max_iter, drop1)) != RDS_OK)
+      return st;
+    int done1 = 0;
+    unsigned status1 = 0;
+    RDS_CUDA(cudaMemcpyAsync(&done1, ctx->d_iter, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    RDS_CUDA(cudaMemcpyAsync(&status1, ctx->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->active_precision = RDS_FP64;
+    if (done1 < max_iter && status1 == 0)
+    {
+      RDS_CUDA(cudaMemsetAsync(ctx->d_stop, 0, sizeof(int), ctx->stream));
+      if ((st = run_loop(ctx, cfl, max_iter, drop)) != RDS_OK)
         return st;
+    }
   }
   else
   {
-    if (!ctx->graph_exec || ctx->graph_cfl != cfl || ctx->graph_max_iter != max_iter ||
-        ctx->graph_drop != drop || ctx->graph_chunk != chunk)
-    {
-      release_graph(ctx);
-      cudaGraph_t graph;
-      RDS_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-      const long long l0 = ctx->launches;
-      for (int k = 0; k < chunk; ++k)
-      {
-        st = enqueue_iteration(ctx, cfl, max_iter, drop);
-        if (st != RDS_OK)
-        {
-          cudaStreamEndCapture(ctx->stream, &graph);
-          if (graph)
-            cudaGraphDestroy(graph);
-          return st;
-        }
-      }
-      ctx->launches = l0; // launches are counted when the graph runs
-      RDS_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
-      cudaError_t e = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (e != cudaSuccess)
-        return fail(ctx, RDS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-      ctx->graph_cfl      = cfl;
-      ctx->graph_max_iter = max_iter;
-      ctx->graph_drop     = drop;
-      ctx->graph_chunk    = chunk;
-    }
-    const long long per_iter = (long long)ctx->groups.size() + (long long)ctx->bcs.size() + 1;
-    const int nchunks        = (max_iter + chunk - 1) / chunk;
-    for (int k = 0; k < nchunks; ++k)
-    {
-      RDS_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
-      ctx->launches += per_iter * chunk;
-      if (drop > 0.0 && k + 1 < nchunks && (k % 4) == 3)
-      {
-        // poll the device stop flag now and then; chunks after convergence exit at once
-        RDS_CUDA(cudaMemcpyAsync(ctx->h_stop, ctx->d_stop, sizeof(int), cudaMemcpyDeviceToHost,
-                                 ctx->stream));
-        RDS_CUDA(cudaStreamSynchronize(ctx->stream));
-        if (*ctx->h_stop)
-          break;
-      }
-    }
+    ctx->active_precision = RDS_FP64;
+    if ((st = run_loop(ctx, cfl, max_iter, drop)) != RDS_OK)
+      return st;
   }
+  ctx->active_precision = ctx->desc.precision;
   int done = 0;
   RDS_CUDA(cudaMemcpyAsync(&done, ctx->d_iter, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   RDS_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -949,6 +999,20 @@ rds_status rds_run(rds_ctx *ctx, double cfl, int n)
       return st;
   }
   return RDS_OK;
+}
+
+rds_status rds_set_option(rds_ctx *ctx, const char *key, double value)
+{
+  if (!ctx || !key)
+    return RDS_ERR_INVALID;
+  if (std::strcmp(key, "mixed_switch") == 0)
+  {
+    if (!(value > 0.0 && value < 1.0))
+      return fail(ctx, RDS_ERR_INVALID, "mixed_switch must be in (0, 1)");
+    ctx->mixed_switch = value;
+    return RDS_OK;
+  }
+  return fail(ctx, RDS_ERR_INVALID, std::string("unknown option ") + key);
 }
 
 rds_status rds_kernel_timing(rds_ctx *ctx, int enable)

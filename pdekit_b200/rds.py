@@ -41,7 +41,7 @@ EXPORTS = ["rds_create", "rds_add_cell_group", "rds_add_bc", "rds_finalize", "rd
            "rds_get_state", "rds_assemble", "rds_assemble_rhs", "rds_update",
            "rds_residual_norm", "rds_get_fields", "rds_iterate", "rds_stream",
            "rds_kernel_timing", "rds_kernel_times", "rds_launch_count", "rds_destroy",
-           "rds_last_error", "rds_version", "rds_run", "rds_measure_peak"]
+           "rds_last_error", "rds_version", "rds_run", "rds_measure_peak", "rds_set_option"]
 
 
 class RDSError(RuntimeError):
@@ -108,6 +108,7 @@ def lib():
         "rds_version": ([], C.c_char_p),
         "rds_run": ([vp, dp, ip], ip),
         "rds_measure_peak": ([ip, vp], ip),
+        "rds_set_option": ([vp, C.c_char_p, dp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -243,6 +244,9 @@ class PGRDMethodExplicit:
             return done.value, hist[:done.value]
         self._check(st)
         return done.value, hist[:done.value]
+
+    def set_option(self, key: str, value: float):
+        self._check(lib().rds_set_option(self._ctx, key.encode(), float(value)))
 
     def run(self, cfl: float, n: int):
         """Enqueue n fused iterations without waiting (for event timing on stream_handle())."""

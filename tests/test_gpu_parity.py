@@ -120,3 +120,20 @@ def test_euler_workloads_match_oracle(which):
     u_ref, _ = o.iterate(u0, 0.5, 10)
     assert rel_err(s.solution(), u_ref) < 1e-11
     s.close()
+
+
+@pytest.mark.parametrize("case,cfl", [("adv_p1_lda_zero", 0.9), ("burgers_p2_n", 0.5)])
+def test_mixed_loop_reaches_fp64_solution(case, cfl):
+    """Mixed form: FP32 cell kernels down to the switch level, then FP64 sweeps to a 1e-10
+    drop; the converged state agrees with the FP64 path's converged state to 1e-9 relative L2."""
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = _solver(prob, prec)
+        s.set_solution(a["u0"])
+        it, hist = s.iterate(cfl, 200000, 1e-10)
+        assert (hist[-1] / hist[0]).max() <= 1e-10
+        out[prec] = (s.solution(), it)
+        s.close()
+    u64, um = out["fp64"][0], out["mixed"][0]
+    assert np.linalg.norm(um - u64) / np.linalg.norm(u64) < 1e-9
