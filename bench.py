@@ -206,6 +206,57 @@ def roofline_cell_kernel(ms_per_launch, ncells, peak_fp64, hbm_gbs):
             "bytes_per_cell": 188}
 
 
+def _drop_run(prob, u0, precision, cfl, max_iter, drop=1e-10):
+    import torch
+
+    from pdekit_b200.rds import PGRDMethodExplicit
+
+    s = PGRDMethodExplicit(prob.physics, prob.scheme, precision).configure_mesh_data(prob)
+    s.initialize_work_data()
+    s.set_solution(u0)
+    s.iterate(0.1, 3, 0.0)  # builds and uploads the loop graphs outside the timed region
+    s.set_solution(u0)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    it, hist = s.iterate(cfl, max_iter, drop, raise_on_cap=False)
+    torch.cuda.synchronize()
+    sec = time.time() - t0
+    rel = float((hist[-1] / hist[0]).max()) if len(hist) else None
+    u = s.solution()
+    s.close()
+    return {"seconds": round(sec, 4), "iterations": int(it), "final_rel_norm": rel,
+            "reached": bool(rel is not None and rel <= drop),
+            "cell_updates_per_s": prob.ncells * it / sec if sec > 0 else None}, u
+
+
+def time_to_drop(args, u0_pgb):
+    """Time to a 1e-10 drop of max_eq ||res dt|| / ||res dt||(iteration 0), FP64 and mixed.
+
+    configuration 1 (advection P1 64x64, LDA, CFL 0.9) and the configuration-2 mesh with the N
+    scheme (Burgers P2 512x512, CFL 0.5) converge to 1e-10; the blended B scheme on the
+    configuration-2 mesh stalls near 1e-5 (a property of the scheme's blending on this shock
+    problem, reproduced by the reference on smaller meshes), so it is run to a capped iteration
+    count and its final drop is reported."""
+    from pdekit_b200 import workloads
+
+    out = {}
+    cases = [("configuration 1: advection P1 64x64, LDA, CFL 0.9", workloads.config1(64), 0.9,
+              args.drop_max_iter),
+             (f"configuration-2 mesh with the N scheme: Burgers P2 {args.n}x{args.n}, CFL 0.5",
+              workloads.config2(args.n, scheme="n"), 0.5, args.drop_max_iter)]
+    for name, (prob, u0), cfl, cap in cases:
+        r64, u64 = _drop_run(prob, u0, "fp64", cfl, cap)
+        rmx, umx = _drop_run(prob, u0, "mixed", cfl, cap)
+        rmx["converged_state_rel_l2_vs_fp64"] = float(np.linalg.norm(umx - u64) /
+                                                      np.linalg.norm(u64))
+        out[name] = {"cells": prob.ncells, "fp64": r64, "mixed": rmx,
+                     "speedup_mixed_vs_fp64": round(r64["seconds"] / rmx["seconds"], 3)}
+    prob, u0 = u0_pgb
+    r, _ = _drop_run(prob, u0, "fp64", CFL, 4000)
+    out[f"configuration 2 (blended B), capped at 4000 iterations"] = {"fp64": r}
+    return out
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -289,19 +340,10 @@ def run_ours(args, rank, world, local):
     ms_mixed = max_over_ranks(time_steps(mixed, args.steps, flush), world)
     mixed_value = ncells * args.steps * world / (ms_mixed * 1e-3)
 
-    # time to a 1e-10 residual drop (device loop with the device-side stop test)
+    # time to a 1e-10 residual drop, FP64 vs mixed (device loop with the device-side stop test)
     drop = None
     if not args.no_drop and world == 1:
-        drop = {}
-        for name, s in (("fp64", solver),):
-            s.set_solution(u0)
-            torch.cuda.synchronize()
-            t0 = time.time()
-            it, hist = s.iterate(CFL, args.drop_max_iter, 1e-10, raise_on_cap=False)
-            torch.cuda.synchronize()
-            rel = float((hist[-1] / hist[0]).max()) if len(hist) else None
-            drop[name] = {"seconds": round(time.time() - t0, 4), "iterations": it,
-                          "final_rel_norm": rel, "reached": bool(rel is not None and rel <= 1e-10)}
+        drop = time_to_drop(args, u0_pgb=(prob, u0))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

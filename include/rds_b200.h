@@ -190,14 +190,45 @@ RDS_API rds_status rds_get_fields(rds_ctx *ctx, double *res_aos, double *dt, dou
 RDS_API rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int *it_done,
                        double *hist);
 
-/* Options: "mixed_switch" (default 1e-5): with RDS_MIXED, rds_iterate runs FP32 cell kernels
- * until max_eq norm/norm(iter 0) <= mixed_switch and then finishes with FP64 sweeps. */
+/* Options: "mixed_switch" (default 1e-6): with RDS_MIXED, rds_iterate runs FP32 cell kernels
+ * until max_eq norm/norm(iter 0) <= mixed_switch, or until that drop has not halved for
+ * max(mixed_stall_min, mixed_stall_mult x the mean iterations per halving so far) iterations
+ * (the problem's FP32 round-off floor; defaults 1000 and 4), and then finishes with FP64 sweeps
+ * to the requested drop. */
 RDS_API rds_status rds_set_option(rds_ctx *ctx, const char *key, double value);
 
 /* Enqueue n fused iterations (assemble_lhs_and_rhs(cfl) + solve()) on the context's stream and
  * return without waiting: no residual-drop test, no copies back. For timing with events on
  * rds_stream(); the norms of these iterations are not kept. */
 RDS_API rds_status rds_run(rds_ctx *ctx, double cfl, int n);
+
+/* Batched independent problems (no counterpart in the reference, which solves one problem per
+ * solver object, src/solver/rdm/PGRDMethodExplicit.hpp:417-514). One context holds the disjoint
+ * union of P problems of scalar 2D physics: problem p owns nodes [node_offsets[p],
+ * node_offsets[p+1]) and runs at its own CFL. Call rds_set_problems right after rds_create,
+ * then add each cell group with the per-problem cell offsets (cells of problem p are rows
+ * [problem_cells[p], problem_cells[p+1]) of the group, and refer only to nodes of p) and its
+ * physics / scheme (advection and Burgers groups may share the context), and the weak
+ * conditions with their physics; then rds_finalize and rds_set_state as usual.
+ * rds_iterate_batch iterates every problem until its own max_eq norm/norm(iter 0) <= drop or
+ * max_iter: one persistent launch per group walks the tiles of the problems still iterating,
+ * the gather updates and tests each problem separately, and the whole loop is one CUDA graph.
+ * With RDS_MIXED every problem runs FP32 cell kernels down to max(drop, mixed_switch) (or to
+ * its FP32 floor, as in rds_iterate) and then FP64 ones. Every problem's iterates equal those of its own single-problem context bit for
+ * bit. iters[P] and rel[P] (may be NULL) receive the iterations done and the final
+ * max_eq norm/norm(iter 0); RDS_ERR_ITER_CAP when a problem did not reach drop > 0.
+ * rds_autotune times the persistent cell kernels for tiles of 64/128/256 cells per CTA and
+ * 1-16 CTAs per SM and keeps the fastest per group and precision; report (may be NULL)
+ * receives a JSON list of the choices. */
+RDS_API rds_status rds_set_problems(rds_ctx *ctx, int nproblems, const int32_t *node_offsets,
+                                    const double *cfl);
+RDS_API rds_status rds_add_batch_cell_group(rds_ctx *ctx, const rds_cell_group *group,
+                                            int physics, int scheme,
+                                            const int32_t *problem_cells);
+RDS_API rds_status rds_add_batch_bc(rds_ctx *ctx, const rds_bc_group *bc, int physics);
+RDS_API rds_status rds_iterate_batch(rds_ctx *ctx, int max_iter, double drop, int32_t *iters,
+                                     double *rel);
+RDS_API rds_status rds_autotune(rds_ctx *ctx, char *report, int len);
 
 /* Diagnostics. */
 /* Measured CUDA-core FMA throughput of this GPU in TFLOP/s (precision: RDS_FP64 or RDS_MIXED

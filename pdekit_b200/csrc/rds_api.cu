@@ -63,17 +63,36 @@ struct rds_ctx
   // pinned host scalars for the loop's stop test
   int *h_stop = nullptr;
 
-  // CUDA graphs of a chunk of fused iterations, one per cell-kernel precision
-  cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
-  int graph_chunk[2]            = {0, 0};
-  double graph_cfl[2]           = {-1.0, -1.0};
-  int graph_max_iter[2]         = {-1, -1};
-  double graph_drop[2]          = {0.0, 0.0};
+  // CUDA graphs of a chunk of fused iterations: FP64 cells, FP32 cells, batched problems.
+  // The loop parameters are read from d_loop, so a graph stays valid across calls.
+  static constexpr int kChunk    = 16;
+  cudaGraphExec_t graph_exec[3] = {nullptr, nullptr, nullptr};
+  LoopParams *d_loop            = nullptr;
 
   // precision of the cell kernels being launched (the mixed loop finishes in FP64)
   int active_precision = RDS_FP64;
   // mixed form: relative residual at which the loop switches from FP32 to FP64 cell kernels
-  double mixed_switch = 1.e-5;
+  // (earlier when the FP32 phase stops making progress)
+  double mixed_switch = 1.e-6;
+  int stall_min       = 1000; // FP32 phase stalled: no halving of the drop for
+  double stall_mult   = 4.0;  //   max(stall_min, stall_mult x iterations per halving so far)
+  StallRec *d_stall   = nullptr; // FP32-phase progress record of the single-problem loop
+  StallRec *d_pstall  = nullptr; // the same per batched problem
+
+  // batched independent problems (rds_set_problems): one context holds their disjoint union
+  int nprob = 0;
+  std::vector<int32_t> prob_nodes; // [P+1] node offsets
+  std::vector<double> prob_cfl;    // [P]
+  int32_t *d_node_off = nullptr, *d_nb_base = nullptr, *d_nb_prefix = nullptr;
+  int32_t *d_phase = nullptr, *d_piter = nullptr, *d_changed = nullptr;
+  int32_t *d_tile = nullptr, *d_tile_prefix = nullptr, *d_cbeg = nullptr, *d_cend = nullptr;
+  double *d_pcfl = nullptr, *d_pnorm = nullptr, *d_pnorm0 = nullptr;
+  unsigned *d_pcount = nullptr, *d_pstatus = nullptr;
+  int nsm         = 0;
+  int batch_grid  = 0; // persistent grid of the batched gather
+  bool tuned      = false;
+  std::string tune_report;
+  std::vector<void *> extra; // further device buffers, freed with the context
 
   bool timing = false;
   std::vector<TimingRec> trecs;
@@ -284,7 +303,7 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
   {
     const BCArgs a = bc_args(ctx, b, stop);
     rds_status st  = launch_on(ctx, ctx->side, [&](const char **name) {
-      return launch_bc(b, a, d.physics, d.dim, d.neq, ctx->side, name);
+      return launch_bc(b, a, b.physics, d.dim, d.neq, ctx->side, name);
     });
     if (st != RDS_OK)
       return st;
@@ -293,7 +312,7 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
   {
     const CellArgs a = cell_args(ctx, g, stop);
     rds_status st    = launch(ctx, [&](const char **name) {
-      return launch_cells(g, a, d.physics, d.scheme, ctx->active_precision, d.dim, d.neq,
+      return launch_cells(g, a, g.physics, g.scheme, ctx->active_precision, d.dim, d.neq,
                           ctx->stream, name);
     });
     if (st != RDS_OK)
@@ -322,7 +341,7 @@ rds_status check_status(rds_ctx *ctx)
 
 void release_graph(rds_ctx *ctx)
 {
-  for (int k = 0; k < 2; ++k)
+  for (int k = 0; k < 3; ++k)
     if (ctx->graph_exec[k])
     {
       cudaGraphExecDestroy(ctx->graph_exec[k]);
@@ -457,6 +476,8 @@ rds_status rds_add_cell_group(rds_ctx *ctx, const rds_cell_group *g)
     h.dVgeo_v.assign(g->dVgeo_v, g->dVgeo_v + (size_t)D * g->nqv * g->ngeo);
   }
   h.affine = (g->shape == RDS_TRIAG && g->ngeo == 3) || (g->shape == RDS_TETRA && g->ngeo == 4);
+  h.physics = ctx->desc.physics;
+  h.scheme  = ctx->desc.scheme;
   rds_status st;
   const std::vector<int32_t> sc = transpose_i32(g->sol_conn, g->ncells, g->ndof);
   const std::vector<int32_t> gc = transpose_i32(g->geo_conn, g->ncells, g->ngeo);
@@ -496,7 +517,8 @@ rds_status rds_add_bc(rds_ctx *ctx, const rds_bc_group *b)
     if (b->geo_conn[i] < 0 || b->geo_conn[i] >= ctx->desc.ngeo_nodes)
       return fail(ctx, RDS_ERR_INVALID, "boundary geometry connectivity out of range");
   HostBC h;
-  h.desc = *b;
+  h.desc    = *b;
+  h.physics = ctx->desc.physics;
   h.fw.assign(b->fw, b->fw + b->nfq);
   h.fV.assign(b->fV, b->fV + (size_t)b->nfq * b->nfdof);
   h.fdVgeo.assign(b->fdVgeo, b->fdVgeo + (size_t)(D - 1) * b->nfq * b->nfgeo);
@@ -522,6 +544,82 @@ rds_status rds_add_bc(rds_ctx *ctx, const rds_bc_group *b)
   h.desc.sol_conn = h.desc.geo_conn = nullptr;
   h.desc.fw = h.desc.fV = h.desc.fdVgeo = h.desc.gq = nullptr;
   ctx->bcs.push_back(h);
+  return RDS_OK;
+}
+
+// Batch set-up: per-problem node ranges and norm-partial slots, per-group problem cell ranges
+// and tile sizes, and the device-side phase / iteration / norm arrays of the problems.
+static rds_status finalize_batch(rds_ctx *ctx)
+{
+  const int P = ctx->nprob, NEQ = ctx->desc.neq, G = (int)ctx->groups.size();
+  for (const HostCellGroup &g : ctx->groups)
+    if (g.pcells.empty())
+      return fail(ctx, RDS_ERR_INVALID,
+                  "batched context: every cell group needs its problem ranges "
+                  "(rds_add_batch_cell_group)");
+  std::vector<int32_t> nb_base(P), cbeg((size_t)G * P), cend((size_t)G * P), tile((size_t)G * 2);
+  long long nb = 0;
+  for (int p = 0; p < P; ++p)
+  {
+    nb_base[p] = (int32_t)nb;
+    nb += (ctx->prob_nodes[p + 1] - ctx->prob_nodes[p] + kGBlock - 1) / kGBlock;
+  }
+  for (int g = 0; g < G; ++g)
+  {
+    const HostCellGroup &h = ctx->groups[g];
+    for (int p = 0; p < P; ++p)
+    {
+      cbeg[(size_t)g * P + p] = h.pcells[p];
+      cend[(size_t)g * P + p] = h.pcells[p + 1];
+    }
+    tile[g * 2]     = h.tune_tile[0];
+    tile[g * 2 + 1] = h.tune_tile[1];
+  }
+  rds_status st = RDS_OK;
+  auto track    = [&](auto **ptr, size_t n) {
+    if (st == RDS_OK && (st = dalloc(ctx, ptr, n)) == RDS_OK)
+      ctx->extra.push_back((void *)*ptr);
+  };
+  track(&ctx->d_node_off, P + 1);
+  track(&ctx->d_nb_base, P);
+  track(&ctx->d_nb_prefix, P + 1);
+  track(&ctx->d_pcfl, P);
+  track(&ctx->d_pcount, P);
+  track(&ctx->d_phase, P);
+  track(&ctx->d_piter, P);
+  track(&ctx->d_pnorm, (size_t)P * NEQ);
+  track(&ctx->d_pnorm0, (size_t)P * NEQ);
+  track(&ctx->d_pstatus, P);
+  track(&ctx->d_changed, 1);
+  track(&ctx->d_tile, (size_t)G * 2);
+  track(&ctx->d_tile_prefix, (size_t)G * 2 * (P + 1));
+  track(&ctx->d_cbeg, (size_t)G * P);
+  track(&ctx->d_cend, (size_t)G * P);
+  track(&ctx->d_pstall, P);
+  if (st != RDS_OK)
+    return st;
+  if (nb > ctx->gblocks)
+  {
+    cudaFree(ctx->d_part);
+    ctx->d_part = nullptr;
+    if ((st = dalloc(ctx, &ctx->d_part, (size_t)nb * NEQ)) != RDS_OK)
+      return st;
+  }
+  if ((st = upload(ctx, ctx->d_node_off, ctx->prob_nodes.data(), P + 1)) ||
+      (st = upload(ctx, ctx->d_nb_base, nb_base.data(), P)) ||
+      (st = upload(ctx, ctx->d_pcfl, ctx->prob_cfl.data(), P)) ||
+      (st = upload(ctx, ctx->d_tile, tile.data(), tile.size())) ||
+      (st = upload(ctx, ctx->d_cbeg, cbeg.data(), cbeg.size())) ||
+      (st = upload(ctx, ctx->d_cend, cend.data(), cend.size())))
+    return st;
+  RDS_CUDA(cudaMemsetAsync(ctx->d_pcount, 0, P * sizeof(unsigned), ctx->stream));
+  for (int g = 0; g < G; ++g)
+  {
+    ctx->groups[g].d_cbeg = ctx->d_cbeg + (size_t)g * P;
+    ctx->groups[g].d_cend = ctx->d_cend + (size_t)g * P;
+  }
+  ctx->batch_grid = ctx->nsm * 8; // 8 resident blocks of kGBlock threads per SM
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
   return RDS_OK;
 }
 
@@ -672,6 +770,13 @@ rds_status rds_finalize(rds_ctx *ctx)
   RDS_CUDA(launch_dual_volume(N, ctx->d_row, ctx->d_ent_ws, ctx->d_wsc, ctx->d_vol,
                               ctx->d_inv_vol, ctx->stream));
   RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  if ((st = dalloc(ctx, &ctx->d_loop, 1)) != RDS_OK ||
+      (st = dalloc(ctx, &ctx->d_stall, 1)) != RDS_OK)
+    return st;
+  ctx->extra.push_back(ctx->d_stall);
+  RDS_CUDA(cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+  if (ctx->nprob > 0 && (st = finalize_batch(ctx)) != RDS_OK)
+    return st;
   ctx->finalized = true;
   return RDS_OK;
 }
@@ -823,69 +928,56 @@ static rds_status enqueue_iteration(rds_ctx *ctx, double cfl, int max_iter, doub
   ga.drop       = drop;
   ga.stop_w     = ctx->d_stop;
   ga.status     = ctx->d_status;
+  ga.loop       = ctx->d_loop;
+  ga.stall      = ctx->d_stall;
   return launch(ctx, [&](const char **name) {
     return launch_gather(ga, 15, ctx->gblocks, ctx->stream, name);
   });
 }
 
-// Device loop at the active precision: chunks of `chunk` fused iterations captured once in a
-// CUDA graph and replayed until the device stop flag is raised (drop reached, iteration cap,
-// non-finite norm); the host polls the flag every 4 chunks.
-static rds_status run_loop(rds_ctx *ctx, double cfl, int max_iter, double drop)
+// Captures kChunk iterations (enqueued by `one`) into graph slot gi once; later calls reuse it.
+extern "C++" template <typename F>
+rds_status capture_chunk(rds_ctx *ctx, int gi, F &&one)
 {
-  rds_status st;
-  const int chunk = std::min(max_iter, 16);
-  if (ctx->timing)
-  {
-    // event timing wants plain launches: run the loop without a graph
-    for (int it = 0; it < max_iter; ++it)
-      if ((st = enqueue_iteration(ctx, cfl, max_iter, drop)) != RDS_OK)
-        return st;
+  if (ctx->graph_exec[gi])
     return RDS_OK;
-  }
-  const int gi = ctx->active_precision == RDS_MIXED ? 1 : 0;
-  if (!ctx->graph_exec[gi] || ctx->graph_cfl[gi] != cfl || ctx->graph_max_iter[gi] != max_iter ||
-      ctx->graph_drop[gi] != drop || ctx->graph_chunk[gi] != chunk)
+  rds_status st;
+  cudaGraph_t graph = nullptr;
+  RDS_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  const long long l0 = ctx->launches;
+  for (int k = 0; k < rds_ctx::kChunk; ++k)
   {
-    if (ctx->graph_exec[gi])
+    st = one();
+    if (st != RDS_OK)
     {
-      cudaGraphExecDestroy(ctx->graph_exec[gi]);
-      ctx->graph_exec[gi] = nullptr;
+      cudaStreamEndCapture(ctx->stream, &graph);
+      if (graph)
+        cudaGraphDestroy(graph);
+      return st;
     }
-    cudaGraph_t graph;
-    RDS_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    const long long l0 = ctx->launches;
-    for (int k = 0; k < chunk; ++k)
-    {
-      st = enqueue_iteration(ctx, cfl, max_iter, drop);
-      if (st != RDS_OK)
-      {
-        cudaStreamEndCapture(ctx->stream, &graph);
-        if (graph)
-          cudaGraphDestroy(graph);
-        return st;
-      }
-    }
-    ctx->launches = l0; // launches are counted when the graph runs
-    RDS_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
-    cudaError_t e = cudaGraphInstantiate(&ctx->graph_exec[gi], graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess)
-      return fail(ctx, RDS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-    ctx->graph_cfl[gi]      = cfl;
-    ctx->graph_max_iter[gi] = max_iter;
-    ctx->graph_drop[gi]     = drop;
-    ctx->graph_chunk[gi]    = chunk;
   }
-  const long long per_iter = (long long)ctx->groups.size() + (long long)ctx->bcs.size() + 1;
-  const int nchunks        = (max_iter + chunk - 1) / chunk;
+  ctx->launches = l0; // launches are counted when the graph runs
+  RDS_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
+  cudaError_t e = cudaGraphInstantiate(&ctx->graph_exec[gi], graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess)
+  {
+    ctx->graph_exec[gi] = nullptr;
+    return fail(ctx, RDS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  }
+  return RDS_OK;
+}
+
+// Replays graph slot gi up to nchunks times, polling the device stop flag every 4 chunks
+// (chunks enqueued after the stop exit at once).
+static rds_status replay_chunks(rds_ctx *ctx, int gi, int nchunks, long long launches_per_chunk)
+{
   for (int k = 0; k < nchunks; ++k)
   {
     RDS_CUDA(cudaGraphLaunch(ctx->graph_exec[gi], ctx->stream));
-    ctx->launches += per_iter * chunk;
+    ctx->launches += launches_per_chunk;
     if (k + 1 < nchunks && (k % 4) == 3)
     {
-      // poll the device stop flag now and then; chunks after a stop exit at once
       RDS_CUDA(cudaMemcpyAsync(ctx->h_stop, ctx->d_stop, sizeof(int), cudaMemcpyDeviceToHost,
                                ctx->stream));
       RDS_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -894,6 +986,38 @@ static rds_status run_loop(rds_ctx *ctx, double cfl, int max_iter, double drop)
     }
   }
   return RDS_OK;
+}
+
+// Device loop at the active precision: chunks of `chunk` fused iterations captured once in a
+// CUDA graph and replayed until the device stop flag is raised (drop reached, iteration cap,
+// non-finite norm); the host polls the flag every 4 chunks.
+static rds_status run_loop(rds_ctx *ctx, double cfl, int max_iter, double drop)
+{
+  rds_status st;
+  LoopParams lp{};
+  lp.cfl      = cfl;
+  lp.drop     = drop;
+  lp.sw       = ctx->mixed_switch;
+  lp.max_iter   = max_iter;
+  lp.stall      = ctx->active_precision == RDS_MIXED ? 1 : 0;
+  lp.stall_min  = ctx->stall_min;
+  lp.stall_mult = ctx->stall_mult;
+  RDS_CUDA(cudaMemcpyAsync(ctx->d_loop, &lp, sizeof(lp), cudaMemcpyHostToDevice, ctx->stream));
+  if (ctx->timing)
+  {
+    // event timing wants plain launches: run the loop without a graph
+    for (int it = 0; it < max_iter; ++it)
+      if ((st = enqueue_iteration(ctx, cfl, max_iter, drop)) != RDS_OK)
+        return st;
+    return RDS_OK;
+  }
+  const int gi    = ctx->active_precision == RDS_MIXED ? 1 : 0;
+  const int chunk = rds_ctx::kChunk;
+  if ((st = capture_chunk(ctx, gi, [&] { return enqueue_iteration(ctx, cfl, max_iter, drop); })) !=
+      RDS_OK)
+    return st;
+  const long long per_iter = (long long)ctx->groups.size() + (long long)ctx->bcs.size() + 1;
+  return replay_chunks(ctx, gi, (max_iter + chunk - 1) / chunk, per_iter * chunk);
 }
 
 rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int *it_done,
@@ -1012,6 +1136,20 @@ rds_status rds_set_option(rds_ctx *ctx, const char *key, double value)
     ctx->mixed_switch = value;
     return RDS_OK;
   }
+  if (std::strcmp(key, "mixed_stall_min") == 0)
+  {
+    if (!(value >= 1.0 && value <= 2.0e9))
+      return fail(ctx, RDS_ERR_INVALID, "mixed_stall_min must be in [1, 2e9]");
+    ctx->stall_min = (int)value;
+    return RDS_OK;
+  }
+  if (std::strcmp(key, "mixed_stall_mult") == 0)
+  {
+    if (!(value >= 0.0 && value <= 1.0e6))
+      return fail(ctx, RDS_ERR_INVALID, "mixed_stall_mult must be in [0, 1e6]");
+    ctx->stall_mult = value;
+    return RDS_OK;
+  }
   return fail(ctx, RDS_ERR_INVALID, std::string("unknown option ") + key);
 }
 
@@ -1059,6 +1197,351 @@ int rds_kernel_times(rds_ctx *ctx, char (*names)[32], double *ms, int *launches,
   return n;
 }
 
+// ---- batched independent problems -----------------------------------------------------------
+
+rds_status rds_set_problems(rds_ctx *ctx, int nproblems, const int32_t *node_offsets,
+                            const double *cfl)
+{
+  if (!ctx)
+    return RDS_ERR_INVALID;
+  if (ctx->finalized || !ctx->groups.empty() || !ctx->bcs.empty() || ctx->nprob > 0)
+    return fail(ctx, RDS_ERR_INVALID,
+                "rds_set_problems: call once, before adding cell groups and conditions");
+  if (ctx->desc.physics != RDS_ADVECTION_CONST && ctx->desc.physics != RDS_BURGERS2D)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "batched problems: scalar 2D physics only");
+  if (nproblems <= 0 || !node_offsets || !cfl || node_offsets[0] != 0 ||
+      node_offsets[nproblems] != ctx->desc.nnodes)
+    return fail(ctx, RDS_ERR_INVALID,
+                "rds_set_problems: node offsets must run from 0 to nnodes over nproblems ranges");
+  for (int p = 0; p < nproblems; ++p)
+    if (node_offsets[p + 1] <= node_offsets[p] || !(cfl[p] > 0.0) || !std::isfinite(cfl[p]))
+      return fail(ctx, RDS_ERR_INVALID, "rds_set_problems: problem " + std::to_string(p) +
+                                            " has an empty node range or a CFL <= 0");
+  ctx->nprob = nproblems;
+  ctx->prob_nodes.assign(node_offsets, node_offsets + nproblems + 1);
+  ctx->prob_cfl.assign(cfl, cfl + nproblems);
+  return RDS_OK;
+}
+
+rds_status rds_add_batch_cell_group(rds_ctx *ctx, const rds_cell_group *g, int physics,
+                                    int scheme, const int32_t *problem_cells)
+{
+  if (!ctx || !g)
+    return RDS_ERR_INVALID;
+  const int P = ctx->nprob;
+  if (P == 0)
+    return fail(ctx, RDS_ERR_INVALID, "rds_add_batch_cell_group: rds_set_problems first");
+  if (physics != RDS_ADVECTION_CONST && physics != RDS_BURGERS2D)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "batched problems: scalar 2D physics only");
+  if (scheme < RDS_PGLDA || scheme > RDS_PGB || !problem_cells || !g->sol_conn ||
+      g->ncells <= 0 || g->ndof <= 0 || problem_cells[0] != 0 || problem_cells[P] != g->ncells)
+    return fail(ctx, RDS_ERR_INVALID,
+                "rds_add_batch_cell_group: invalid scheme or problem cell offsets");
+  for (int p = 0; p < P; ++p)
+  {
+    if (problem_cells[p + 1] < problem_cells[p])
+      return fail(ctx, RDS_ERR_INVALID, "rds_add_batch_cell_group: decreasing cell offsets");
+    const int v0 = ctx->prob_nodes[p], v1 = ctx->prob_nodes[p + 1];
+    for (size_t i = (size_t)problem_cells[p] * g->ndof; i < (size_t)problem_cells[p + 1] * g->ndof;
+         ++i)
+      if (g->sol_conn[i] < v0 || g->sol_conn[i] >= v1)
+        return fail(ctx, RDS_ERR_INVALID, "rds_add_batch_cell_group: a cell of problem " +
+                                              std::to_string(p) + " has a node of another problem");
+  }
+  const rds_status st = rds_add_cell_group(ctx, g);
+  if (st != RDS_OK)
+    return st;
+  HostCellGroup &h = ctx->groups.back();
+  h.physics        = physics;
+  h.scheme         = scheme;
+  h.pcells.assign(problem_cells, problem_cells + P + 1);
+  return RDS_OK;
+}
+
+rds_status rds_add_batch_bc(rds_ctx *ctx, const rds_bc_group *b, int physics)
+{
+  if (!ctx)
+    return RDS_ERR_INVALID;
+  if (ctx->nprob == 0)
+    return fail(ctx, RDS_ERR_INVALID, "rds_add_batch_bc: rds_set_problems first");
+  if (physics != RDS_ADVECTION_CONST && physics != RDS_BURGERS2D)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "batched problems: scalar 2D physics only");
+  const rds_status st = rds_add_bc(ctx, b);
+  if (st == RDS_OK)
+    ctx->bcs.back().physics = physics;
+  return st;
+}
+
+// One batched iteration: rebuild of the active lists (only after a phase change), boundary
+// facets of all problems on the side stream, persistent cell kernels over the active tiles of
+// each group (FP32 tiles and FP64 tiles in the mixed form), persistent gather with the
+// per-problem update, norm and stop test.
+static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed)
+{
+  const rds_desc &d = ctx->desc;
+  const int P = ctx->nprob, G = (int)ctx->groups.size();
+  RebuildArgs r{};
+  r.nprob       = P;
+  r.ngroups     = G;
+  r.phase       = ctx->d_phase;
+  r.cbeg        = ctx->d_cbeg;
+  r.cend        = ctx->d_cend;
+  r.tile        = ctx->d_tile;
+  r.tile_prefix = ctx->d_tile_prefix;
+  r.node_off    = ctx->d_node_off;
+  r.nb_prefix   = ctx->d_nb_prefix;
+  r.changed     = ctx->d_changed;
+  r.stop        = ctx->d_stop;
+  rds_status st = launch(ctx, [&](const char **name) {
+    return launch_batch_rebuild(r, ctx->stream, name);
+  });
+  if (st != RDS_OK)
+    return st;
+  const bool fork = !ctx->bcs.empty();
+  if (fork)
+  {
+    RDS_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
+    RDS_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+  }
+  for (const HostBC &b : ctx->bcs)
+  {
+    const BCArgs a = bc_args(ctx, b, ctx->d_stop);
+    if ((st = launch_on(ctx, ctx->side, [&](const char **name) {
+           return launch_bc(b, a, b.physics, d.dim, d.neq, ctx->side, name);
+         })) != RDS_OK)
+      return st;
+  }
+  for (int gi = 0; gi < G; ++gi)
+  {
+    const HostCellGroup &g = ctx->groups[gi];
+    for (int ph = mixed ? 0 : 1; ph < 2; ++ph)
+    {
+      CellArgs a = cell_args(ctx, g, ctx->d_stop);
+      a.bt       = {ctx->d_tile_prefix + ((size_t)gi * 2 + ph) * (P + 1), g.d_cbeg, g.d_cend, P};
+      const int grid = g.tune_grid[ph] > 0 ? g.tune_grid[ph] : 4 * ctx->nsm;
+      if ((st = launch(ctx, [&](const char **name) {
+             bool ok = false;
+             cudaError_t e = launch_cells_scalar_batch(g, a, ph == 0 ? RDS_MIXED : RDS_FP64, grid,
+                                                       g.tune_tile[ph], ctx->stream, name, &ok);
+             return ok ? e : cudaErrorNotSupported;
+           })) != RDS_OK)
+        return st;
+    }
+  }
+  if (fork)
+  {
+    RDS_CUDA(cudaEventRecord(ctx->ev_join, ctx->side));
+    RDS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+  }
+  GatherArgs ga = gather_args(ctx, 0.0, ctx->d_stop);
+  ga.status     = ctx->d_status;
+  ga.loop       = ctx->d_loop;
+  BatchArgs b{};
+  b.nprob     = P;
+  b.node_off  = ctx->d_node_off;
+  b.nb_base   = ctx->d_nb_base;
+  b.nb_prefix = ctx->d_nb_prefix;
+  b.cfl       = ctx->d_pcfl;
+  b.pcount    = ctx->d_pcount;
+  b.phase     = ctx->d_phase;
+  b.iter      = ctx->d_piter;
+  b.norm      = ctx->d_pnorm;
+  b.norm0     = ctx->d_pnorm0;
+  b.pstatus   = ctx->d_pstatus;
+  b.changed   = ctx->d_changed;
+  b.loop      = ctx->d_loop;
+  b.stall     = ctx->d_pstall;
+  return launch(ctx, [&](const char **name) {
+    return launch_gather_batch(ga, b, ctx->batch_grid, ctx->stream, name);
+  });
+}
+
+rds_status rds_iterate_batch(rds_ctx *ctx, int max_iter, double drop, int32_t *iters,
+                             double *rel)
+{
+  if (!ctx || !ctx->finalized || ctx->nprob == 0 || max_iter <= 0)
+    return ctx ? fail(ctx, RDS_ERR_INVALID,
+                      "rds_iterate_batch: not a finalized batched context or max_iter <= 0")
+               : RDS_ERR_INVALID;
+  const int P = ctx->nprob, NEQ = ctx->desc.neq;
+  const bool mixed = ctx->desc.precision == RDS_MIXED;
+  rds_status st;
+  LoopParams lp{};
+  lp.drop     = drop;
+  lp.sw         = ctx->mixed_switch;
+  lp.max_iter   = max_iter;
+  lp.stall_min  = ctx->stall_min;
+  lp.stall_mult = ctx->stall_mult;
+  RDS_CUDA(cudaMemcpyAsync(ctx->d_loop, &lp, sizeof(lp), cudaMemcpyHostToDevice, ctx->stream));
+  const std::vector<int32_t> phase0(P, mixed ? 0 : 1);
+  const int32_t one = 1;
+  if ((st = upload(ctx, ctx->d_phase, phase0.data(), P)) ||
+      (st = upload(ctx, ctx->d_changed, &one, 1)))
+    return st;
+  RDS_CUDA(cudaMemsetAsync(ctx->d_piter, 0, P * sizeof(int32_t), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_pcount, 0, P * sizeof(unsigned), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_pstatus, 0, P * sizeof(unsigned), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_stop, 0, sizeof(int), ctx->stream));
+  RDS_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
+  // every problem is done after max_iter iterations; one more raises the stop flag
+  const int total_iter = max_iter + 1;
+  if (ctx->timing)
+  {
+    for (int it = 0; it < total_iter; ++it)
+      if ((st = enqueue_batch_iteration(ctx, mixed)) != RDS_OK)
+        return st;
+  }
+  else
+  {
+    if ((st = capture_chunk(ctx, 2, [&] { return enqueue_batch_iteration(ctx, mixed); })) !=
+        RDS_OK)
+      return st;
+    const long long per_iter =
+        2 + (long long)ctx->bcs.size() + (long long)ctx->groups.size() * (mixed ? 2 : 1);
+    if ((st = replay_chunks(ctx, 2, (total_iter + rds_ctx::kChunk - 1) / rds_ctx::kChunk,
+                            per_iter * rds_ctx::kChunk)) != RDS_OK)
+      return st;
+  }
+  std::vector<int32_t> it(P);
+  std::vector<double> nrm((size_t)P * NEQ), nrm0((size_t)P * NEQ);
+  std::vector<unsigned> pst(P);
+  RDS_CUDA(cudaMemcpyAsync(it.data(), ctx->d_piter, P * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  RDS_CUDA(cudaMemcpyAsync(nrm.data(), ctx->d_pnorm, nrm.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  RDS_CUDA(cudaMemcpyAsync(nrm0.data(), ctx->d_pnorm0, nrm0.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  RDS_CUDA(cudaMemcpyAsync(pst.data(), ctx->d_pstatus, P * sizeof(unsigned),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  int nonfinite = 0, capped = 0;
+  for (int p = 0; p < P; ++p)
+  {
+    double r = 0.0;
+    for (int e = 0; e < NEQ; ++e)
+    {
+      const double n0 = nrm0[(size_t)p * NEQ + e];
+      r = std::max(r, n0 > 0.0 ? nrm[(size_t)p * NEQ + e] / n0 : 0.0);
+    }
+    if (iters)
+      iters[p] = it[p];
+    if (rel)
+      rel[p] = r;
+    nonfinite += (pst[p] & kFlagNonFinite) != 0;
+    capped += (drop > 0.0 && !(r <= drop));
+  }
+  if (nonfinite)
+    return fail(ctx, RDS_ERR_NONFINITE,
+                std::to_string(nonfinite) + " problem(s) with a non-finite residual norm");
+  if ((st = check_status(ctx)) != RDS_OK)
+    return st;
+  if (capped)
+    return fail(ctx, RDS_ERR_ITER_CAP,
+                std::to_string(capped) + " problem(s) did not reach the drop within max_iter");
+  return RDS_OK;
+}
+
+// Autotuner: for every group and cell precision of the batch, time the persistent cell kernel
+// over all problems for tiles of 64 / 128 / 256 cells per CTA and 1..16 resident CTAs per SM,
+// and keep the fastest (tile, grid). Results per cell do not depend on the choice.
+rds_status rds_autotune(rds_ctx *ctx, char *report, int len)
+{
+  if (!ctx || !ctx->finalized || ctx->nprob == 0)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_autotune: not a finalized batched context")
+               : RDS_ERR_INVALID;
+  static const int kTiles[] = {64, 128, 256};
+  static const int kPerSm[] = {1, 2, 4, 8, 16};
+  const int P = ctx->nprob;
+  const bool mixed = ctx->desc.precision == RDS_MIXED;
+  rds_status st;
+  int32_t *d_pre = nullptr;
+  if ((st = dalloc(ctx, &d_pre, P + 1)) != RDS_OK)
+    return st;
+  ctx->extra.push_back(d_pre);
+  cudaEvent_t e0 = get_event(ctx), e1 = get_event(ctx);
+  std::string rep = "[";
+  for (size_t gi = 0; gi < ctx->groups.size(); ++gi)
+  {
+    HostCellGroup &g = ctx->groups[gi];
+    for (int ph = mixed ? 0 : 1; ph < 2; ++ph)
+    {
+      float best = 1e30f;
+      int best_tile = 128, best_grid = 4 * ctx->nsm;
+      const char *kname = "?";
+      for (int tile : kTiles)
+      {
+        std::vector<int32_t> pre(P + 1, 0);
+        for (int p = 0; p < P; ++p)
+          pre[p + 1] = pre[p] + (g.pcells[p + 1] - g.pcells[p] + tile - 1) / tile;
+        if ((st = upload(ctx, d_pre, pre.data(), P + 1)) != RDS_OK)
+          return st;
+        int last_grid = -1;
+        for (int per_sm : kPerSm)
+        {
+          const int grid = std::max(1, std::min(per_sm * ctx->nsm, pre[P]));
+          if (grid == last_grid)
+            continue;
+          last_grid  = grid;
+          CellArgs a = cell_args(ctx, g, ctx->d_zero);
+          a.bt       = {d_pre, g.d_cbeg, g.d_cend, P};
+          const int prec = ph == 0 ? RDS_MIXED : RDS_FP64;
+          bool ok        = false;
+          for (int rep_i = 0; rep_i < 4; ++rep_i)
+          {
+            if (rep_i == 1)
+              RDS_CUDA(cudaEventRecord(e0, ctx->stream));
+            RDS_CUDA(launch_cells_scalar_batch(g, a, prec, grid, tile, ctx->stream, &kname, &ok));
+            if (!ok)
+              return fail(ctx, RDS_ERR_UNSUPPORTED,
+                          "rds_autotune: no batched kernel for this cell group");
+          }
+          RDS_CUDA(cudaEventRecord(e1, ctx->stream));
+          RDS_CUDA(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          RDS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          ms /= 3.f;
+          if (ms < best)
+          {
+            best      = ms;
+            best_tile = tile;
+            best_grid = grid;
+          }
+        }
+      }
+      g.tune_tile[ph] = best_tile;
+      g.tune_grid[ph] = best_grid;
+      char buf[256];
+      snprintf(buf, sizeof buf,
+               "%s{\"group\": %zu, \"kernel\": \"%s\", \"ndof\": %d, \"nq\": %d, \"tile\": %d, "
+               "\"grid\": %d, \"ms\": %.4f}",
+               rep.size() > 1 ? ", " : "", gi, kname, g.desc.ndof, g.desc.nq, best_tile,
+               best_grid, best);
+      rep += buf;
+    }
+  }
+  rep += "]";
+  ctx->ev_pool.push_back(e0);
+  ctx->ev_pool.push_back(e1);
+  std::vector<int32_t> tile(ctx->groups.size() * 2);
+  for (size_t gi = 0; gi < ctx->groups.size(); ++gi)
+  {
+    tile[gi * 2]     = ctx->groups[gi].tune_tile[0];
+    tile[gi * 2 + 1] = ctx->groups[gi].tune_tile[1];
+  }
+  if ((st = upload(ctx, ctx->d_tile, tile.data(), tile.size())) != RDS_OK)
+    return st;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  release_graph(ctx); // the captured batch loop holds the old grids
+  ctx->tuned       = true;
+  ctx->tune_report = rep;
+  if (report && len > 0)
+  {
+    strncpy(report, rep.c_str(), (size_t)len - 1);
+    report[len - 1] = '\0';
+  }
+  return RDS_OK;
+}
+
 rds_status rds_destroy(rds_ctx *ctx)
 {
   if (!ctx)
@@ -1083,7 +1566,9 @@ rds_status rds_destroy(rds_ctx *ctx)
                   ctx->d_vol,   ctx->d_inv_vol, ctx->d_contrib, ctx->d_wsc,    ctx->d_stage,
                   ctx->d_row,   ctx->d_ent_slot, ctx->d_ent_ws, ctx->d_part,   ctx->d_norm,
                   ctx->d_norm0, ctx->d_hist,  ctx->d_iter,    ctx->d_stop,     ctx->d_zero,
-                  ctx->d_status, ctx->d_counter};
+                  ctx->d_status, ctx->d_counter, ctx->d_loop};
+  for (void *p : ctx->extra)
+    cudaFree(p);
   for (void *p : bufs)
     if (p)
       cudaFree(p);

@@ -31,15 +31,10 @@ namespace
 {
 
 template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, bool AFFINE>
-__global__ void __launch_bounds__(kBlock)
-    cells_scalar2d(const CellArgs a, const Tables<T, 2, NDOF, NQ, NFL, NGEO> tb)
+__device__ __forceinline__ void scalar_cell(const CellArgs &a,
+                                            const Tables<T, 2, NDOF, NQ, NFL, NGEO> &tb,
+                                            const int c)
 {
-  if (*a.stop)
-    return;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncells)
-    return;
-
   // ---- gather nodal state and geometry (SoA connectivity: coalesced index loads)
   double ud[NDOF];
   T un[NDOF];
@@ -59,8 +54,10 @@ __global__ void __launch_bounds__(kBlock)
     X1[g]       = T(__ldg(a.X + a.ngeo_nodes + v));
   }
 
-  // ---- physical flux at the flux nodes (order p+1 Lagrange interpolant of F)
-  T F0[NFL], F1[NFL];
+  // ---- state at the flux nodes (order p+1 Lagrange interpolant of F); the flux there is
+  // F = (s^2/2, s) for Burgers and (a0 s, a1 s) for advection, evaluated where it is used so
+  // only s is kept
+  T sf[NFL];
 #pragma unroll
   for (int f = 0; f < NFL; ++f)
   {
@@ -68,17 +65,12 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
     for (int n = 1; n < NDOF; ++n)
       s = s + tb.Vsf[f][n] * un[n];
-    if (PHYS == RDS_BURGERS2D)
-    {
-      F0[f] = T(0.5) * s * s;
-      F1[f] = s;
-    }
-    else
-    {
-      F0[f] = T(a.adv0) * s;
-      F1[f] = T(a.adv1) * s;
-    }
+    sf[f] = s;
   }
+  auto flux0 = [&](int f) -> T {
+    return PHYS == RDS_BURGERS2D ? T(0.5) * sf[f] * sf[f] : T(a.adv0) * sf[f];
+  };
+  auto flux1 = [&](int f) -> T { return PHYS == RDS_BURGERS2D ? sf[f] : T(a.adv1) * sf[f]; };
 
   T ij00 = 0, ij01 = 0, ij10 = 0, ij11 = 0, detj = 0;
   auto jacobian = [&](int q) {
@@ -122,15 +114,22 @@ __global__ void __launch_bounds__(kBlock)
     vol += wj;
 
     // flux divergence at q
-    T d00 = tb.dVf[0][q][0] * F0[0], d01 = tb.dVf[1][q][0] * F0[0];
-    T d10 = tb.dVf[0][q][0] * F1[0], d11 = tb.dVf[1][q][0] * F1[0];
+    T d00, d01, d10, d11;
+    {
+      const T f0 = flux0(0), f1 = flux1(0);
+      d00 = tb.dVf[0][q][0] * f0;
+      d01 = tb.dVf[1][q][0] * f0;
+      d10 = tb.dVf[0][q][0] * f1;
+      d11 = tb.dVf[1][q][0] * f1;
+    }
 #pragma unroll
     for (int f = 1; f < NFL; ++f)
     {
-      d00 = d00 + tb.dVf[0][q][f] * F0[f];
-      d01 = d01 + tb.dVf[1][q][f] * F0[f];
-      d10 = d10 + tb.dVf[0][q][f] * F1[f];
-      d11 = d11 + tb.dVf[1][q][f] * F1[f];
+      const T f0 = flux0(f), f1 = flux1(f);
+      d00 = d00 + tb.dVf[0][q][f] * f0;
+      d01 = d01 + tb.dVf[1][q][f] * f0;
+      d10 = d10 + tb.dVf[0][q][f] * f1;
+      d11 = d11 + tb.dVf[1][q][f] * f1;
     }
     const T rT      = (ij00 * d00 + ij01 * d01) + (ij10 * d10 + ij11 * d11);
     const double rq = double(rT);
@@ -213,6 +212,50 @@ __global__ void __launch_bounds__(kBlock)
   __stcs(a.wsc + a.ws_base + c, vol * double(wsmax));
 }
 
+template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, bool AFFINE>
+__global__ void __launch_bounds__(kBlock)
+    cells_scalar2d(const __grid_constant__ CellArgs a,
+                   const __grid_constant__ Tables<T, 2, NDOF, NQ, NFL, NGEO> tb)
+{
+  if (*a.stop)
+    return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncells)
+    return;
+  scalar_cell<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, AFFINE>(a, tb, c);
+}
+
+// Batch form: a persistent grid walks the group's active tiles (the problems still iterating
+// at this precision); a tile is blockDim.x consecutive cells of one problem, so every thread of
+// a block maps to the same problem. Results per cell are those of cells_scalar2d.
+template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO>
+__global__ void __launch_bounds__(256)
+    cells_scalar2d_batch(const __grid_constant__ CellArgs a,
+                         const __grid_constant__ Tables<T, 2, NDOF, NQ, NFL, NGEO> tb)
+{
+  if (*a.stop)
+    return;
+  const int32_t *prefix = a.bt.prefix;
+  const int np          = a.bt.nprob;
+  const int total       = prefix[np];
+  for (int t = blockIdx.x; t < total; t += gridDim.x)
+  {
+    // problem p with prefix[p] <= t < prefix[p+1] (prefix[0] = 0 <= t < prefix[np])
+    int lo = 0, hi = np;
+    while (hi - lo > 1)
+    {
+      const int mid = (lo + hi) >> 1;
+      if (prefix[mid] <= t)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const int c = a.bt.cbeg[lo] + (t - prefix[lo]) * (int)blockDim.x + (int)threadIdx.x;
+    if (c < a.bt.cend[lo])
+      scalar_cell<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, true>(a, tb, c);
+  }
+}
+
 template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO>
 cudaError_t launch_one(const HostCellGroup &g, const CellArgs &a, cudaStream_t s)
 {
@@ -249,6 +292,36 @@ cudaError_t dispatch_shape(const HostCellGroup &g, const CellArgs &a, cudaStream
   return cudaSuccess;
 }
 
+template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL>
+cudaError_t launch_batch_one(const HostCellGroup &g, const CellArgs &a, int grid, int tile,
+                             cudaStream_t s)
+{
+  Tables<T, 2, NDOF, NQ, NFL, 3> tb;
+  fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
+  cells_scalar2d_batch<PHYS, SCHEME, T, NDOF, NQ, NFL, 3><<<grid, tile, 0, s>>>(a, tb);
+  return cudaGetLastError();
+}
+
+template <int PHYS, int SCHEME, typename T>
+cudaError_t dispatch_batch(const HostCellGroup &g, const CellArgs &a, int grid, int tile,
+                           cudaStream_t s, bool *ok)
+{
+  const rds_cell_group &d = g.desc;
+  *ok                     = true;
+  if (d.shape == RDS_TRIAG && d.ngeo == 3)
+  {
+    // straight-sided triangles, P1 / P4 rule, P2 / P5 rule, P3 / P8 rule
+    if (d.ndof == 3 && d.nq == 6 && d.nfl == 6)
+      return launch_batch_one<PHYS, SCHEME, T, 3, 6, 6>(g, a, grid, tile, s);
+    if (d.ndof == 6 && d.nq == 7 && d.nfl == 10)
+      return launch_batch_one<PHYS, SCHEME, T, 6, 7, 10>(g, a, grid, tile, s);
+    if (d.ndof == 10 && d.nq == 16 && d.nfl == 15)
+      return launch_batch_one<PHYS, SCHEME, T, 10, 16, 15>(g, a, grid, tile, s);
+  }
+  *ok = false;
+  return cudaSuccess;
+}
+
 const char *kernel_name(int physics, int scheme)
 {
   static const char *names[2][3] = {{"cells_adv_lda", "cells_adv_n", "cells_adv_b"},
@@ -276,6 +349,37 @@ cudaError_t launch_cells_scalar(const HostCellGroup &g, const CellArgs &a, int p
   RDS_SCALAR_CASE(RDS_BURGERS2D, RDS_PGB)
 #undef RDS_SCALAR_CASE
   *ok = false;
+  return cudaSuccess;
+}
+
+cudaError_t launch_cells_scalar_batch(const HostCellGroup &g, const CellArgs &a, int precision,
+                                      int grid, int tile, cudaStream_t s, const char **name,
+                                      bool *ok)
+{
+  static const char *names[2][3][2] = {
+      {{"cells_adv_lda_batch", "cells_adv_lda_batch_f32"},
+       {"cells_adv_n_batch", "cells_adv_n_batch_f32"},
+       {"cells_adv_b_batch", "cells_adv_b_batch_f32"}},
+      {{"cells_burgers_lda_batch", "cells_burgers_lda_batch_f32"},
+       {"cells_burgers_n_batch", "cells_burgers_n_batch_f32"},
+       {"cells_burgers_b_batch", "cells_burgers_b_batch_f32"}}};
+  const int physics = g.physics, scheme = g.scheme;
+  *ok               = false;
+  if ((physics != RDS_ADVECTION_CONST && physics != RDS_BURGERS2D) || scheme < 0 || scheme > 2 ||
+      tile <= 0 || tile > 256 || grid <= 0)
+    return cudaSuccess;
+  *name = names[physics == RDS_BURGERS2D][scheme][precision == RDS_MIXED];
+#define RDS_BATCH_CASE(PH, SC)                                                                     \
+  if (physics == PH && scheme == SC)                                                               \
+    return precision == RDS_MIXED ? dispatch_batch<PH, SC, float>(g, a, grid, tile, s, ok)         \
+                                  : dispatch_batch<PH, SC, double>(g, a, grid, tile, s, ok);
+  RDS_BATCH_CASE(RDS_ADVECTION_CONST, RDS_PGLDA)
+  RDS_BATCH_CASE(RDS_ADVECTION_CONST, RDS_PGN)
+  RDS_BATCH_CASE(RDS_ADVECTION_CONST, RDS_PGB)
+  RDS_BATCH_CASE(RDS_BURGERS2D, RDS_PGLDA)
+  RDS_BATCH_CASE(RDS_BURGERS2D, RDS_PGN)
+  RDS_BATCH_CASE(RDS_BURGERS2D, RDS_PGB)
+#undef RDS_BATCH_CASE
   return cudaSuccess;
 }
 

@@ -41,10 +41,81 @@ __device__ __forceinline__ double block_sum(double v, double *smem)
 
 __device__ void reduce_final(const double *part, int nblocks, int neq, int nnodes, double *norm,
                              double *norm0, double *hist, int *iter, int max_iter, double drop,
-                             int *stop, unsigned *status, double *smem, double *nv);
+                             int *stop, unsigned *status, double *smem, double *nv,
+                             StallRec *stall = nullptr, const LoopParams *loop = nullptr);
+
+// Progress test of the FP32 phase of the mixed loop: a halving of the best drop so far is
+// progress; the phase has stalled (the problem's FP32 round-off floor) when no halving came for
+// max(stall_min, stall_mult x the mean number of iterations per halving so far). it = 0 starts
+// the record.
+__device__ __forceinline__ bool fp32_stalled(double rel, int it, StallRec *r, const LoopParams &L)
+{
+  if (it == 0)
+  {
+    r->best    = rel;
+    r->best_it = 0;
+    r->nhalv   = 0;
+    return false;
+  }
+  if (rel <= 0.5 * r->best)
+  {
+    r->best    = rel;
+    r->best_it = it;
+    r->nhalv += 1;
+    return false;
+  }
+  const double per    = r->nhalv > 0 ? double(r->best_it) / r->nhalv : 0.0;
+  const double window = fmax(double(L.stall_min), L.stall_mult * per);
+  return double(it - r->best_it) > window;
+}
+
+template <int NEQ, bool DT, bool UPDATE, bool NORM>
+__device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, const double cfl,
+                                            double *sq)
+{
+  double acc[NEQ];
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e)
+    acc[e] = 0.0;
+  double ws       = 0.0;
+  const double iv = a.inv_vol[v];
+  const int i0 = a.row[v], i1 = a.row[v + 1];
+  for (int i = i0; i < i1; ++i)
+  {
+    const long long s = __ldg(a.ent_slot + i);
+    const int w       = __ldg(a.ent_ws + i);
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+      acc[e] = __dadd_rn(acc[e], __dmul_rn(iv, __ldcs(a.contrib + e * a.S + s)));
+    ws = __dadd_rn(ws, __ldcs(a.wsc + w));
+  }
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e)
+    a.res[(size_t)e * a.nnodes + v] = acc[e];
+  a.ws[v] = ws;
+  if (DT)
+  {
+    const double dtv = __ddiv_rn(__dmul_rn(cfl, a.vol[v]), ws);
+    a.dt[v]          = dtv;
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+    {
+      if (UPDATE)
+      {
+        double *pu = a.u + (size_t)e * a.nnodes + v;
+        *pu        = __dsub_rn(*pu, __dmul_rn(dtv, acc[e]));
+      }
+      if (NORM)
+      {
+        const double r = __dmul_rn(acc[e], dtv);
+        sq[e]          = __dmul_rn(r, r);
+      }
+    }
+  }
+}
 
 template <int NEQ, bool DT, bool UPDATE, bool NORM, bool FINAL>
-__global__ void __launch_bounds__(kGBlock) gather_nodes(const GatherArgs a)
+__global__ void __launch_bounds__(kGBlock) gather_nodes(const __grid_constant__ GatherArgs a)
 {
   __shared__ double smem[kGBlock / 32];
   if (*a.stop)
@@ -55,47 +126,7 @@ __global__ void __launch_bounds__(kGBlock) gather_nodes(const GatherArgs a)
   for (int e = 0; e < NEQ; ++e)
     sq[e] = 0.0;
   if (v < a.nnodes)
-  {
-    double acc[NEQ];
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e)
-      acc[e] = 0.0;
-    double ws     = 0.0;
-    const double iv = a.inv_vol[v];
-    const int i0 = a.row[v], i1 = a.row[v + 1];
-    for (int i = i0; i < i1; ++i)
-    {
-      const long long s = __ldg(a.ent_slot + i);
-      const int w       = __ldg(a.ent_ws + i);
-#pragma unroll
-      for (int e = 0; e < NEQ; ++e)
-        acc[e] = __dadd_rn(acc[e], __dmul_rn(iv, __ldcs(a.contrib + e * a.S + s)));
-      ws = __dadd_rn(ws, __ldcs(a.wsc + w));
-    }
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e)
-      a.res[(size_t)e * a.nnodes + v] = acc[e];
-    a.ws[v] = ws;
-    if (DT)
-    {
-      const double dtv = __ddiv_rn(__dmul_rn(a.cfl, a.vol[v]), ws);
-      a.dt[v]          = dtv;
-#pragma unroll
-      for (int e = 0; e < NEQ; ++e)
-      {
-        if (UPDATE)
-        {
-          double *pu = a.u + (size_t)e * a.nnodes + v;
-          *pu        = __dsub_rn(*pu, __dmul_rn(dtv, acc[e]));
-        }
-        if (NORM)
-        {
-          const double r = __dmul_rn(acc[e], dtv);
-          sq[e]          = __dmul_rn(r, r);
-        }
-      }
-    }
-  }
+    gather_node<NEQ, DT, UPDATE, NORM>(a, v, a.loop ? a.loop->cfl : a.cfl, sq);
   if (NORM)
   {
 #pragma unroll
@@ -121,8 +152,10 @@ __global__ void __launch_bounds__(kGBlock) gather_nodes(const GatherArgs a)
       if (last)
       {
         __threadfence();
+        const int max_iter = a.loop ? a.loop->max_iter : a.max_iter;
+        const double drop  = a.loop ? a.loop->drop : a.drop;
         reduce_final(a.part, gridDim.x, NEQ, a.nnodes, a.norm, a.norm0, a.hist, a.iter,
-                     a.max_iter, a.drop, a.stop_w, a.status, smem, nv);
+                     max_iter, drop, a.stop_w, a.status, smem, nv, a.stall, a.loop);
         if (threadIdx.x == 0)
           *a.counter = 0u;
       }
@@ -157,7 +190,8 @@ __global__ void __launch_bounds__(kGBlock)
 // Executed by one whole block (norm_final, or the last block of a fused gather).
 __device__ void reduce_final(const double *part, int nblocks, int neq, int nnodes, double *norm,
                              double *norm0, double *hist, int *iter, int max_iter, double drop,
-                             int *stop, unsigned *status, double *smem, double *nv)
+                             int *stop, unsigned *status, double *smem, double *nv,
+                             StallRec *stall, const LoopParams *loop)
 {
   for (int e = 0; e < neq; ++e)
   {
@@ -200,6 +234,10 @@ __device__ void reduce_final(const double *part, int nblocks, int neq, int nnode
     *stop = 1;
   }
   else if ((drop > 0.0 && rel <= drop) || it + 1 >= max_iter)
+  {
+    *stop = 1;
+  }
+  else if (loop && loop->stall && fp32_stalled(rel, it, stall, *loop))
   {
     *stop = 1;
   }
@@ -281,6 +319,220 @@ __global__ void dual_volume_kernel(int nnodes, const int32_t *row, const int32_t
     s = __dadd_rn(s, cvol[ent_ws[i]]);
   vol[v]     = s;
   inv_vol[v] = 1. / s;
+}
+
+// ---- batched independent problems ---------------------------------------------------------
+
+// Largest p with prefix[p] <= t, for prefix[0] = 0 <= t < prefix[np] (non-decreasing prefix).
+__device__ __forceinline__ int find_segment(const int32_t *prefix, int np, int t)
+{
+  int lo = 0, hi = np;
+  while (hi - lo > 1)
+  {
+    const int mid = (lo + hi) >> 1;
+    if (prefix[mid] <= t)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Norm and stop test of problem p (whole block; the result is written by thread 0): the same
+// fixed-order reduction of the problem's node-block partials as the single-problem loop, then
+// the phase change FP32 -> FP64 at max(drop, sw), done at drop, or at the iteration cap.
+template <int NEQ>
+__device__ void problem_final(const GatherArgs &a, const BatchArgs &b, const int p,
+                              const int nblk, double *smem, double *nv)
+{
+  const int base = b.nb_base[p];
+  const int nn   = b.node_off[p + 1] - b.node_off[p];
+  for (int e = 0; e < NEQ; ++e)
+  {
+    double s = 0.0;
+    for (int k = threadIdx.x; k < nblk; k += blockDim.x)
+      s += __ldcg(a.part + (size_t)(base + k) * NEQ + e);
+    s = block_sum<kGBlock>(s, smem);
+    if (threadIdx.x == 0)
+      nv[e] = sqrt(s / nn);
+  }
+  if (threadIdx.x != 0)
+    return;
+  const int it = b.iter[p];
+  const int ph = b.phase[p];
+  double rel   = 0.0;
+  bool finite  = true;
+  for (int e = 0; e < NEQ; ++e)
+  {
+    const double n = nv[e];
+    b.norm[(size_t)p * NEQ + e] = n;
+    if (it == 0)
+      b.norm0[(size_t)p * NEQ + e] = n;
+    if (!isfinite(n))
+      finite = false;
+    const double n0 = (it == 0) ? n : b.norm0[(size_t)p * NEQ + e];
+    const double r  = n0 > 0.0 ? n / n0 : 0.0;
+    rel             = r > rel ? r : rel;
+  }
+  b.iter[p]              = it + 1;
+  const LoopParams &L    = *b.loop;
+  int nph                = ph;
+  const double drop1     = L.drop > L.sw ? L.drop : L.sw;
+  if (!finite)
+  {
+    atomicOr(b.pstatus + p, kFlagNonFinite);
+    atomicOr(a.status, kFlagNonFinite);
+    nph = 2;
+  }
+  else if (ph == 0 && (rel <= drop1 || fp32_stalled(rel, it, b.stall + p, L)))
+    nph = 1;
+  else if (ph == 1 && L.drop > 0.0 && rel <= L.drop)
+    nph = 2;
+  if (nph != 2 && it + 1 >= L.max_iter)
+    nph = 2;
+  if (nph != ph)
+  {
+    b.phase[p] = nph;
+    *b.changed = 1;
+  }
+  b.pcount[p] = 0u;
+}
+
+// Persistent gather over the node blocks of the problems still iterating: each problem's nodes
+// are split into blocks of kGBlock from its first node, exactly as a single-problem context
+// splits them, and the block that completes a problem's iteration reduces its norm.
+template <int NEQ>
+__global__ void __launch_bounds__(kGBlock)
+    gather_batch(const __grid_constant__ GatherArgs a, const __grid_constant__ BatchArgs b)
+{
+  __shared__ double smem[kGBlock / 32];
+  __shared__ double nv[kMaxNeq];
+  __shared__ bool last;
+  if (*a.stop)
+    return;
+  const int np    = b.nprob;
+  const int total = b.nb_prefix[np];
+  for (int t = blockIdx.x; t < total; t += gridDim.x)
+  {
+    const int p  = find_segment(b.nb_prefix, np, t);
+    const int j  = t - b.nb_prefix[p];
+    const int n0 = b.node_off[p], n1 = b.node_off[p + 1];
+    const int v  = n0 + j * kGBlock + threadIdx.x;
+    double sq[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+      sq[e] = 0.0;
+    if (v < n1)
+      gather_node<NEQ, true, true, true>(a, v, b.cfl[p], sq);
+    const int slot = b.nb_base[p] + j;
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+    {
+      const double s = block_sum<kGBlock>(sq[e], smem);
+      if (threadIdx.x == 0)
+        a.part[(size_t)slot * NEQ + e] = s;
+    }
+    const int nblk = (n1 - n0 + kGBlock - 1) / kGBlock;
+    if (threadIdx.x == 0)
+    {
+      __threadfence();
+      const unsigned done = atomicAdd(b.pcount + p, 1u);
+      last                = (done == (unsigned)nblk - 1u);
+    }
+    __syncthreads();
+    if (last)
+    {
+      __threadfence();
+      problem_final<NEQ>(a, b, p, nblk, smem, nv);
+    }
+    __syncthreads();
+  }
+}
+
+// Block-wide exclusive scan of one int per thread (blockDim.x a multiple of 32, <= 1024).
+__device__ __forceinline__ int block_exclusive_scan(int x, int *sh, int *total)
+{
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int v = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1)
+  {
+    const int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o)
+      v += y;
+  }
+  __syncthreads();
+  if (lane == 31)
+    sh[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    int acc = 0;
+    for (int w = 0; w < nw; ++w)
+    {
+      const int t = sh[w];
+      sh[w]       = acc;
+      acc += t;
+    }
+    sh[32] = acc;
+  }
+  __syncthreads();
+  *total = sh[32];
+  return sh[warp] + v - x;
+}
+
+// Exclusive prefix over p of cnt(p) into out[0..np], one block, chunked per thread.
+template <typename F>
+__device__ void prefix_over_problems(int np, F cnt, int32_t *out, int *sh)
+{
+  const int per = (np + blockDim.x - 1) / blockDim.x;
+  const int p0  = min(np, (int)threadIdx.x * per), p1 = min(np, p0 + per);
+  int local     = 0;
+  for (int p = p0; p < p1; ++p)
+    local += cnt(p);
+  int total;
+  int off = block_exclusive_scan(local, sh, &total);
+  for (int p = p0; p < p1; ++p)
+  {
+    out[p] = off;
+    off += cnt(p);
+  }
+  if (threadIdx.x == 0)
+    out[np] = total;
+}
+
+// Active lists after a phase change: per cell group and phase the tiles of the problems in
+// that phase, and the node blocks of the problems not done; raises the stop flag when every
+// problem is done. Does nothing when no problem changed phase in the last iteration.
+__global__ void __launch_bounds__(1024) batch_rebuild(const __grid_constant__ RebuildArgs r)
+{
+  __shared__ int sh[33];
+  if (*r.stop || *r.changed == 0)
+    return;
+  const int np = r.nprob;
+  for (int g = 0; g < r.ngroups; ++g)
+    for (int ph = 0; ph < 2; ++ph)
+    {
+      const int tile    = r.tile[g * 2 + ph];
+      const int32_t *cb = r.cbeg + (size_t)g * np, *ce = r.cend + (size_t)g * np;
+      prefix_over_problems(
+          np,
+          [&](int p) { return r.phase[p] == ph ? (ce[p] - cb[p] + tile - 1) / tile : 0; },
+          r.tile_prefix + ((size_t)g * 2 + ph) * (np + 1), sh);
+    }
+  prefix_over_problems(
+      np,
+      [&](int p) {
+        return r.phase[p] < 2 ? (r.node_off[p + 1] - r.node_off[p] + kGBlock - 1) / kGBlock : 0;
+      },
+      r.nb_prefix, sh);
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    *r.changed = 0;
+    if (r.nb_prefix[np] == 0)
+      *r.stop = 1;
+  }
 }
 
 template <int NEQ>
@@ -379,6 +631,34 @@ cudaError_t launch_dual_volume(int nnodes, const int32_t *row, const int32_t *en
 {
   dual_volume_kernel<<<(nnodes + kGBlock - 1) / kGBlock, kGBlock, 0, s>>>(nnodes, row, ent_ws,
                                                                           cvol, vol, inv_vol);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_batch(const GatherArgs &a, const BatchArgs &b, int grid, cudaStream_t s,
+                                const char **name)
+{
+  *name = "gather_batch";
+  switch (a.neq)
+  {
+  case 1:
+    gather_batch<1><<<grid, kGBlock, 0, s>>>(a, b);
+    break;
+  case 4:
+    gather_batch<4><<<grid, kGBlock, 0, s>>>(a, b);
+    break;
+  case 5:
+    gather_batch<5><<<grid, kGBlock, 0, s>>>(a, b);
+    break;
+  default:
+    return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_rebuild(const RebuildArgs &r, cudaStream_t s, const char **name)
+{
+  *name = "batch_rebuild";
+  batch_rebuild<<<1, 1024, 0, s>>>(r);
   return cudaGetLastError();
 }
 

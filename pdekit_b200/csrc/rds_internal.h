@@ -36,6 +36,13 @@ struct HostCellGroup
   long long slot_base = 0;       // first contribution slot of this group
   long long ws_base   = 0;       // first wave-speed slot of this group
   bool affine         = false;   // simplex with straight edges: Jacobian constant per cell
+  int physics         = 0;       // physics / scheme of this group's cells
+  int scheme          = 0;
+  // batched problems: cells of problem p are [cbeg[p], cend[p]) of this group
+  std::vector<int32_t> pcells;   // [P+1] offsets (empty outside a batch)
+  int32_t *d_cbeg = nullptr, *d_cend = nullptr;
+  int tune_tile[2] = {128, 128}; // cells per CTA tile (phase 0 FP32, phase 1 FP64)
+  int tune_grid[2] = {0, 0};     // persistent grid (CTAs), 0: 4 per SM
 };
 
 struct HostBC
@@ -47,6 +54,73 @@ struct HostBC
   double *d_gq        = nullptr; // [neq][nfq][nfacets]
   long long slot_base = 0;
   long long ws_base   = 0;
+  int physics         = 0;
+};
+
+// Loop parameters read by the device from memory, so a captured loop graph stays valid when
+// they change between calls.
+struct LoopParams
+{
+  double cfl;
+  double drop;     // stop at max_eq norm/norm0 <= drop (0: never)
+  double sw;       // batched mixed form: switch from FP32 to FP64 cells at this drop
+  double stall_mult; // FP32 phase stalled: no halving of the drop for
+  int stall_min;     //   max(stall_min, stall_mult x iterations per halving so far)
+  int max_iter;
+  int stall;       // nonzero: FP32 phase, also stop when progress stalls
+};
+
+// Progress record of the FP32 phase of the mixed loop.
+struct StallRec
+{
+  double best; // best drop (a halving of the previous best)
+  int best_it; // iteration it was reached
+  int nhalv;   // halvings so far
+};
+
+// Active-tile map of one cell group in a batch (persistent cell kernels): tile t of the
+// active list belongs to the problem p with prefix[p] <= t < prefix[p+1], and covers cells
+// cbeg[p] + (t - prefix[p]) * blockDim.x + [0, blockDim.x) clipped to cend[p].
+struct BatchTileMap
+{
+  const int32_t *prefix; // [P+1], rebuilt on the device when a problem changes phase
+  const int32_t *cbeg;   // [P]
+  const int32_t *cend;   // [P]
+  int nprob;
+};
+
+// Per-problem state of a batch (one context holding the disjoint union of the problems).
+struct BatchArgs
+{
+  int nprob;
+  const int32_t *node_off;  // [P+1] node range of each problem
+  const int32_t *nb_base;   // [P] first norm-partial slot (node block) of each problem
+  const int32_t *nb_prefix; // [P+1] active node blocks, exclusive prefix
+  const double *cfl;        // [P]
+  unsigned *pcount;         // [P] node blocks of the problem done in this iteration
+  int32_t *phase;           // [P] 0: FP32 cells, 1: FP64 cells, 2: done
+  int32_t *iter;            // [P] iterations done
+  double *norm, *norm0;     // [P][neq]
+  unsigned *pstatus;        // [P] status bits of each problem
+  int32_t *changed;         // a problem changed phase in this iteration
+  const LoopParams *loop;
+  StallRec *stall;          // [P] FP32-phase progress records
+};
+
+// Rebuild of the active lists after a phase change (one block).
+struct RebuildArgs
+{
+  int nprob;
+  int ngroups;
+  const int32_t *phase;     // [P]
+  const int32_t *cbeg;      // [ngroups][P]
+  const int32_t *cend;      // [ngroups][P]
+  const int32_t *tile;      // [ngroups][2] cells per tile of each phase
+  int32_t *tile_prefix;     // [ngroups][2][P+1]
+  const int32_t *node_off;  // [P+1]
+  int32_t *nb_prefix;       // [P+1]
+  int32_t *changed;
+  int *stop;
 };
 
 // Arguments common to every cell kernel.
@@ -67,6 +141,7 @@ struct CellArgs
   double adv0, adv1, adv2, gamma;
   unsigned *status;
   const int *stop; // nonzero: skip the work (converged loop)
+  BatchTileMap bt; // batch mode only
 };
 
 struct BCArgs
@@ -119,6 +194,8 @@ struct GatherArgs
   double drop;
   int *stop_w;
   unsigned *status;
+  const LoopParams *loop; // non-null: cfl, drop, max_iter are read from here
+  StallRec *stall;        // FP32-phase progress record (mixed loop)
 };
 
 // ---- launchers (return cudaError_t of the launch) --------------------------------------
@@ -147,6 +224,15 @@ cudaError_t launch_cells_euler(const HostCellGroup &g, const CellArgs &a, int ph
                                bool *ok);
 cudaError_t launch_dual_volume(int nnodes, const int32_t *row, const int32_t *ent_ws,
                                const double *cvol, double *vol, double *inv_vol, cudaStream_t s);
+// Batch mode: persistent cell kernel of a scalar group over its active tiles (block = tile).
+cudaError_t launch_cells_scalar_batch(const HostCellGroup &g, const CellArgs &a, int precision,
+                                      int grid, int tile, cudaStream_t s, const char **name,
+                                      bool *ok);
+// Batch mode: persistent gather over the active problems' node blocks with per-problem dt,
+// update, norm and stop test; then the rebuild of the active lists after phase changes.
+cudaError_t launch_gather_batch(const GatherArgs &a, const BatchArgs &b, int grid, cudaStream_t s,
+                                const char **name);
+cudaError_t launch_batch_rebuild(const RebuildArgs &r, cudaStream_t s, const char **name);
 cudaError_t launch_update(int nnodes, int neq, const double *dt, const double *res, double *u,
                           cudaStream_t s, const char **name);
 

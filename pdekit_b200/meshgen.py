@@ -116,30 +116,35 @@ def clone_continuous_tri(mesh: Mesh2D, p: int):
     if p == 1:
         return mesh.cells.copy(), nv, mesh.coords.copy()
     ne_int = p - 1
-    edge_ids = {}
-    next_id = nv
     ndof = tri_dof_layout(p)
     n_int = ndof - 3 - 3 * ne_int
-    conn = np.empty((nc, ndof), dtype=np.int32)
     ref = equidist_triag_nodes(p)  # on (-1,-1),(1,-1),(-1,1)
-    coords_out = {}
-    for c in range(nc):
-        v = mesh.cells[c]
-        conn[c, :3] = v
-        k = 3
-        for (a, b) in ((v[0], v[1]), (v[1], v[2]), (v[2], v[0])):
-            key = (min(a, b), max(a, b))
-            if key not in edge_ids:
-                edge_ids[key] = np.arange(next_id, next_id + ne_int, dtype=np.int32)
-                next_id += ne_int
-            ids = edge_ids[key]
-            if a > b:
-                ids = ids[::-1]
-            conn[c, k:k + ne_int] = ids
-            k += ne_int
-        if n_int > 0:
-            conn[c, k:] = np.arange(next_id, next_id + n_int, dtype=np.int32)
-            next_id += n_int
+    cells = mesh.cells.astype(np.int64)
+    # directed cell edges v0->v1, v1->v2, v2->v0, cell-major
+    a = cells[:, [0, 1, 2]].reshape(-1)
+    b = cells[:, [1, 2, 0]].reshape(-1)
+    key = np.minimum(a, b) * nv + np.maximum(a, b)
+    _, first, inv = np.unique(key, return_index=True, return_inverse=True)
+    first_slot = first[inv]  # slot of the edge's first appearance
+    is_new = first_slot == np.arange(key.shape[0])
+    # ids are handed out while walking the cells in order: new edges of the cell (local edge
+    # order), then its interior dofs
+    sizes = np.zeros((nc, 4), dtype=np.int64)
+    sizes[:, :3] = is_new.reshape(nc, 3) * ne_int
+    sizes[:, 3] = n_int
+    start = nv + np.concatenate([[0], np.cumsum(sizes.reshape(-1))[:-1]]).reshape(nc, 4)
+    conn = np.empty((nc, ndof), dtype=np.int64)
+    conn[:, :3] = cells
+    slot_start = start[:, :3].reshape(-1)[first_slot]  # [3 nc] first id of each edge's block
+    steps = np.arange(ne_int)
+    ids = slot_start[:, None] + steps[None, :]
+    rev = a > b
+    ids[rev] = ids[rev][:, ::-1]
+    conn[:, 3:3 + 3 * ne_int] = ids.reshape(nc, 3 * ne_int)
+    if n_int > 0:
+        conn[:, 3 + 3 * ne_int:] = start[:, 3:4] + np.arange(n_int)[None, :]
+    next_id = int(nv + sizes.sum())
+    conn = conn.astype(np.int32)
     nsol = next_id
     # physical coordinates of every dof (P1 map)
     xi = (ref[:, 0] + 1.0) * 0.5
@@ -185,22 +190,27 @@ def boundary_facets_tri(mesh: Mesh2D, sol_conn: np.ndarray, p: int, name: str):
     """Facet (edge) connectivity of a named boundary: geometry vertices [nf, 2] and solution
     dofs [nf, p+1] in the line element's order (two end vertices, then interior edge nodes
     from the first vertex to the second), oriented like the parent cell's edge."""
-    edges = mesh.boundaries[name]
-    # map each directed cell edge to (cell, local edge)
-    lookup = {}
-    for c, (a, b, cc) in enumerate(mesh.cells):
-        for le, (u, v) in enumerate(((a, b), (b, cc), (cc, a))):
-            lookup[(min(u, v), max(u, v))] = (c, le, u, v)
-    geo = np.empty((len(edges), 2), dtype=np.int32)
-    sol = np.empty((len(edges), p + 1), dtype=np.int32)
-    for k, (a, b) in enumerate(edges):
-        c, le, u, v = lookup[(min(a, b), max(a, b))]
-        geo[k] = (u, v)
-        dofs = [u, v]
-        if p > 1:
-            start = 3 + le * (p - 1)
-            dofs += list(sol_conn[c, start:start + p - 1])
-        sol[k] = dofs
+    edges = np.asarray(mesh.boundaries[name], dtype=np.int64).reshape(-1, 2)
+    nv = mesh.coords.shape[0]
+    cells = mesh.cells.astype(np.int64)
+    a = cells[:, [0, 1, 2]].reshape(-1)
+    b = cells[:, [1, 2, 0]].reshape(-1)
+    key = np.minimum(a, b) * nv + np.maximum(a, b)
+    order = np.argsort(key, kind="stable")
+    bkey = np.minimum(edges[:, 0], edges[:, 1]) * nv + np.maximum(edges[:, 0], edges[:, 1])
+    pos = np.searchsorted(key[order], bkey)
+    if np.any(pos >= key.shape[0]) or np.any(key[order][np.minimum(pos, key.shape[0] - 1)] != bkey):
+        raise ValueError(f"boundary {name}: an edge belongs to no cell")
+    # a boundary edge has one cell; with several matches the last one in cell order wins
+    last = np.searchsorted(key[order], bkey, side="right") - 1
+    slot = order[last]
+    c, le = slot // 3, slot % 3
+    geo = np.stack([a[slot], b[slot]], axis=1).astype(np.int32)
+    sol = np.empty((edges.shape[0], p + 1), dtype=np.int32)
+    sol[:, :2] = geo
+    if p > 1:
+        start = 3 + le * (p - 1)
+        sol[:, 2:] = sol_conn[c[:, None], start[:, None] + np.arange(p - 1)[None, :]]
     return geo, sol
 
 

@@ -41,7 +41,9 @@ EXPORTS = ["rds_create", "rds_add_cell_group", "rds_add_bc", "rds_finalize", "rd
            "rds_get_state", "rds_assemble", "rds_assemble_rhs", "rds_update",
            "rds_residual_norm", "rds_get_fields", "rds_iterate", "rds_stream",
            "rds_kernel_timing", "rds_kernel_times", "rds_launch_count", "rds_destroy",
-           "rds_last_error", "rds_version", "rds_run", "rds_measure_peak", "rds_set_option"]
+           "rds_last_error", "rds_version", "rds_run", "rds_measure_peak", "rds_set_option",
+           "rds_set_problems", "rds_add_batch_cell_group", "rds_add_batch_bc",
+           "rds_iterate_batch", "rds_autotune", "rds_residual_norm_noalloc"]
 
 
 class RDSError(RuntimeError):
@@ -109,6 +111,11 @@ def lib():
         "rds_run": ([vp, dp, ip], ip),
         "rds_measure_peak": ([ip, vp], ip),
         "rds_set_option": ([vp, C.c_char_p, dp], ip),
+        "rds_set_problems": ([vp, ip, vp, vp], ip),
+        "rds_add_batch_cell_group": ([vp, vp, ip, ip, vp], ip),
+        "rds_add_batch_bc": ([vp, vp, ip], ip),
+        "rds_iterate_batch": ([vp, ip, dp, vp, vp], ip),
+        "rds_autotune": ([vp, C.c_char_p, ip], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -29,7 +29,7 @@ def tri_problem(physics: str, scheme: str, p: int, n: int, jitter: float, seed: 
     """Unit-square triangle problem of order p with the reference-element tables `tables`
     (keys w, V, dV, dVgeo, dVf, Vsf for cells; fw, fV, fVgeo, fdVgeo for facets)."""
     mesh = meshgen.unit_square_tri(n, jitter, seed=seed)
-    conn, nsol, _ = meshgen.clone_continuous_tri(mesh, p)
+    conn, nsol, xy = meshgen.clone_continuous_tri(mesh, p)
     g = CellGroup(sol_conn=conn, geo_conn=mesh.cells, w=tables["w"], V=tables["V"],
                   dV=tables["dV"], dVgeo=tables["dVgeo"], dVf=tables["dVf"], Vsf=tables["Vsf"],
                   shape="triag", order=p)
@@ -45,6 +45,7 @@ def tri_problem(physics: str, scheme: str, p: int, n: int, jitter: float, seed: 
         b.gq = bcexpr.evaluate(expr, b.quadrature_coords(mesh.coords), neq)
         prob.bcs.append(b)
     prob.bcs.sort(key=lambda b: b.name)  # the reference applies BCs in name order
+    prob.sol_coords = xy
     return prob
 
 
@@ -67,6 +68,24 @@ def sol_coords_tri(n: int, jitter: float, seed: int, p: int) -> np.ndarray:
     mesh = meshgen.unit_square_tri(n, jitter, seed=seed)
     _, _, xy = meshgen.clone_continuous_tri(mesh, p)
     return xy
+
+
+def config1(n=64, seed=1, scheme="lda"):
+    """Configuration 1: constant advection, P1 triangles on an n x n grid (jitter 0.2h), 6-point
+    rule, inflow sin(2 pi x) / 0, initial u = 0 (run at CFL 0.9)."""
+    from . import reference_element as R
+
+    prob = tri_problem("advconst", scheme, 1, n, 0.2, seed, ADV_BCS, R.triag_tables(1, 4))
+    return prob, initial_state(prob, "zero", prob.sol_coords)
+
+
+def config2(n=512, seed=7, scheme="b"):
+    """Configuration 2: Burgers, P2 triangles on an n x n grid (jitter 0.15h), 7-point rule,
+    inflow 1.5 - 2x, initial 1.5 - 2x + 0.1 sin(7x + 3y) y (run at CFL 0.5)."""
+    from . import reference_element as R
+
+    prob = tri_problem("burgers", scheme, 2, n, 0.15, seed, BURGERS_BCS, R.triag_tables(2, 5))
+    return prob, initial_state(prob, "burgers", prob.sol_coords)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -164,3 +183,36 @@ def config4(nx=128, ny=32, nz=32, seed=4):
     mesh = meshgen.box_tet(nx, ny, nz, jitter=0.1, seed=seed)
     prob = mesh_problem(mesh, "euler3d", "lda", 2, {"tetra": R.tet_tables(2, 5)}, euler_bcs(3))
     return prob, bump_state(prob.sol_coords, 3, 0.6)
+
+
+def config5(nprob=256, seed=5, min_cells=1000, max_cells=200000):
+    """Configuration 5: `nprob` independent unit-square problems drawn from `seed`: advection
+    (LDA, CFL U[0.5, 0.9], initial 0) or Burgers (N scheme, CFL U[0.3, 0.6], initial
+    1.5 - 2x + 0.1 sin(7x + 3y) y), order P1 / P2 / P3 (6 / 7 / 16-point rules), cell count
+    log-uniform in [min_cells, max_cells] (n x n squares, n = round(sqrt(cells / 2))), jitter
+    0.2h. Returns (problems, initial states, CFLs, descriptions)."""
+    from . import reference_element as R
+
+    rng = np.random.default_rng(seed)
+    rules = {1: 4, 2: 5, 3: 8}
+    tables = {p: R.triag_tables(p, rules[p]) for p in (1, 2, 3)}
+    probs, states, cfls, info = [], [], [], []
+    for i in range(nprob):
+        kind = "advconst" if rng.random() < 0.5 else "burgers"
+        p = int(rng.integers(1, 4))
+        cells = float(np.exp(rng.uniform(np.log(min_cells), np.log(max_cells))))
+        n = max(2, int(round(np.sqrt(cells / 2.0))))
+        pseed = int(rng.integers(0, 2**31 - 1))
+        if kind == "advconst":
+            prob = tri_problem(kind, "lda", p, n, 0.2, pseed, ADV_BCS, tables[p])
+            u0 = initial_state(prob, "zero", prob.sol_coords)
+            cfl = float(rng.uniform(0.5, 0.9))
+        else:
+            prob = tri_problem(kind, "n", p, n, 0.2, pseed, BURGERS_BCS, tables[p])
+            u0 = initial_state(prob, "burgers", prob.sol_coords)
+            cfl = float(rng.uniform(0.3, 0.6))
+        probs.append(prob)
+        states.append(u0)
+        cfls.append(cfl)
+        info.append({"physics": kind, "order": p, "n": n, "cells": prob.ncells, "cfl": cfl})
+    return probs, states, np.array(cfls), info
