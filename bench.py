@@ -47,7 +47,7 @@ BURGERS_BCS_SPEC = ("WeakDirichlet:inlet:bottom:burgers_inlet,WeakDirichlet:left
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=512, help="squares per side (512 = configuration 2)")

@@ -191,10 +191,10 @@ RDS_API rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double dr
                        double *hist);
 
 /* Options: "mixed_switch" (default 1e-6): with RDS_MIXED, rds_iterate runs FP32 cell kernels
- * until max_eq norm/norm(iter 0) <= mixed_switch, or until that drop has not halved for
- * max(mixed_stall_min, mixed_stall_mult x the mean iterations per halving so far) iterations
- * (the problem's FP32 round-off floor; defaults 1000 and 4), and then finishes with FP64 sweeps
- * to the requested drop. */
+ * until max_eq norm/norm(iter 0) <= mixed_switch, or, once that drop has halved at least
+ * once, until it has not halved for max(mixed_stall_min, mixed_stall_mult x the last interval
+ * between halvings) iterations (the problem's FP32 round-off floor; defaults 200 and 3), and
+ * then finishes with FP64 sweeps to the requested drop. */
 RDS_API rds_status rds_set_option(rds_ctx *ctx, const char *key, double value);
 
 /* Enqueue n fused iterations (assemble_lhs_and_rhs(cfl) + solve()) on the context's stream and

@@ -74,8 +74,8 @@ struct rds_ctx
   // mixed form: relative residual at which the loop switches from FP32 to FP64 cell kernels
   // (earlier when the FP32 phase stops making progress)
   double mixed_switch = 1.e-6;
-  int stall_min       = 1000; // FP32 phase stalled: no halving of the drop for
-  double stall_mult   = 4.0;  //   max(stall_min, stall_mult x iterations per halving so far)
+  int stall_min       = 200; // FP32 phase stalled: no halving of the drop for
+  double stall_mult   = 3.0; //   max(stall_min, stall_mult x the last interval between halvings)
   StallRec *d_stall   = nullptr; // FP32-phase progress record of the single-problem loop
   StallRec *d_pstall  = nullptr; // the same per batched problem
 

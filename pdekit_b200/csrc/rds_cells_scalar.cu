@@ -35,6 +35,13 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
                                             const Tables<T, 2, NDOF, NQ, NFL, NGEO> &tb,
                                             const int c)
 {
+  // FP32 form: states and coordinates enter as deviations from the cell's first node, taken in
+  // FP64 (u_n - u_0, X_g - X_0); interpolants and fluxes are written in those deviations
+  // (the bases sum to one and their derivatives to zero), so FP32 round-off acts on terms of the
+  // size of the variation across the cell instead of the size of the state, which keeps the
+  // FP32 residual floor low. The FP64 form evaluates the reference's expressions as they are.
+  constexpr bool DEV = sizeof(T) == 4;
+
   // ---- gather nodal state and geometry (SoA connectivity: coalesced index loads)
   double ud[NDOF];
   T un[NDOF];
@@ -43,32 +50,44 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
   {
     const int v = __ldg(a.sol_conn + (size_t)n * a.ncells + c);
     ud[n]       = __ldg(a.u + v);
-    un[n]       = T(ud[n]);
+    un[n]       = DEV ? T(ud[n] - ud[0]) : T(ud[n]);
   }
+  const T u0 = T(ud[0]);
   T X0[NGEO], X1[NGEO];
-#pragma unroll
-  for (int g = 0; g < NGEO; ++g)
   {
-    const int v = __ldg(a.geo_conn + (size_t)g * a.ncells + c);
-    X0[g]       = T(__ldg(a.X + v));
-    X1[g]       = T(__ldg(a.X + a.ngeo_nodes + v));
+    double xg0 = 0.0, yg0 = 0.0;
+#pragma unroll
+    for (int g = 0; g < NGEO; ++g)
+    {
+      const int v     = __ldg(a.geo_conn + (size_t)g * a.ncells + c);
+      const double xg = __ldg(a.X + v), yg = __ldg(a.X + a.ngeo_nodes + v);
+      if (g == 0)
+      {
+        xg0 = xg;
+        yg0 = yg;
+      }
+      X0[g] = DEV ? T(xg - xg0) : T(xg);
+      X1[g] = DEV ? T(yg - yg0) : T(yg);
+    }
   }
 
   // ---- state at the flux nodes (order p+1 Lagrange interpolant of F); the flux there is
   // F = (s^2/2, s) for Burgers and (a0 s, a1 s) for advection, evaluated where it is used so
-  // only s is kept
+  // only s is kept (FP32 form: s - u_0 and F(s) - F(u_0))
   T sf[NFL];
 #pragma unroll
   for (int f = 0; f < NFL; ++f)
   {
-    T s = tb.Vsf[f][0] * un[0];
+    T s = DEV ? T(0) : tb.Vsf[f][0] * un[0];
 #pragma unroll
     for (int n = 1; n < NDOF; ++n)
       s = s + tb.Vsf[f][n] * un[n];
     sf[f] = s;
   }
   auto flux0 = [&](int f) -> T {
-    return PHYS == RDS_BURGERS2D ? T(0.5) * sf[f] * sf[f] : T(a.adv0) * sf[f];
+    if (PHYS == RDS_BURGERS2D)
+      return DEV ? sf[f] * (u0 + T(0.5) * sf[f]) : T(0.5) * sf[f] * sf[f];
+    return T(a.adv0) * sf[f];
   };
   auto flux1 = [&](int f) -> T { return PHYS == RDS_BURGERS2D ? sf[f] : T(a.adv1) * sf[f]; };
 
@@ -138,10 +157,12 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
     T ax, ay;
     if (PHYS == RDS_BURGERS2D)
     {
-      T uq = tb.V[q][0] * un[0];
+      T uq = DEV ? T(0) : tb.V[q][0] * un[0];
 #pragma unroll
       for (int n = 1; n < NDOF; ++n)
         uq = uq + tb.V[q][n] * un[n];
+      if (DEV)
+        uq = u0 + uq;
       ax = uq;
       ay = T(1);
     }

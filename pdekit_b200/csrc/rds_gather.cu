@@ -45,27 +45,28 @@ __device__ void reduce_final(const double *part, int nblocks, int neq, int nnode
                              StallRec *stall = nullptr, const LoopParams *loop = nullptr);
 
 // Progress test of the FP32 phase of the mixed loop: a halving of the best drop so far is
-// progress; the phase has stalled (the problem's FP32 round-off floor) when no halving came for
-// max(stall_min, stall_mult x the mean number of iterations per halving so far). it = 0 starts
-// the record.
+// progress; once the drop has halved at least once, the phase has stalled (the problem's FP32
+// round-off floor) when no halving came for max(stall_min, stall_mult x the last interval
+// between halvings) iterations. it = 0 starts the record.
 __device__ __forceinline__ bool fp32_stalled(double rel, int it, StallRec *r, const LoopParams &L)
 {
   if (it == 0)
   {
     r->best    = rel;
     r->best_it = 0;
-    r->nhalv   = 0;
+    r->gap     = 0;
     return false;
   }
   if (rel <= 0.5 * r->best)
   {
+    r->gap     = it - r->best_it;
     r->best    = rel;
     r->best_it = it;
-    r->nhalv += 1;
     return false;
   }
-  const double per    = r->nhalv > 0 ? double(r->best_it) / r->nhalv : 0.0;
-  const double window = fmax(double(L.stall_min), L.stall_mult * per);
+  if (r->gap == 0)
+    return false; // initial transient: no rate known yet
+  const double window = fmax(double(L.stall_min), L.stall_mult * double(r->gap));
   return double(it - r->best_it) > window;
 }
 

@@ -65,7 +65,7 @@ struct LoopParams
   double drop;     // stop at max_eq norm/norm0 <= drop (0: never)
   double sw;       // batched mixed form: switch from FP32 to FP64 cells at this drop
   double stall_mult; // FP32 phase stalled: no halving of the drop for
-  int stall_min;     //   max(stall_min, stall_mult x iterations per halving so far)
+  int stall_min;     //   max(stall_min, stall_mult x the last interval between halvings)
   int max_iter;
   int stall;       // nonzero: FP32 phase, also stop when progress stalls
 };
@@ -75,7 +75,7 @@ struct StallRec
 {
   double best; // best drop (a halving of the previous best)
   int best_it; // iteration it was reached
-  int nhalv;   // halvings so far
+  int gap;     // iterations between the last two halvings (0: no halving yet)
 };
 
 // Active-tile map of one cell group in a batch (persistent cell kernels): tile t of the
