@@ -528,6 +528,8 @@ cudaError_t dispatch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream
     {
       if (d.ndof == 3 && d.nq == 6 && d.nfl == 6)
         return launch_euler<PHYS, SCHEME, T, 3, 6, 6, 3, 4>(g, a, s);
+      if (d.ndof == 6 && d.nq == 6 && d.nfl == 10)
+        return launch_euler<PHYS, SCHEME, T, 6, 6, 10, 3, 4>(g, a, s);
       if (d.ndof == 6 && d.nq == 7 && d.nfl == 10)
         return launch_euler<PHYS, SCHEME, T, 6, 7, 10, 3, 4>(g, a, s);
       if (d.ndof == 10 && d.nq == 16 && d.nfl == 15)
@@ -535,6 +537,16 @@ cudaError_t dispatch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream
     }
     if (d.shape == RDS_QUAD && d.ngeo == 4)
     {
+      // P1 and P2 with the reference's 8-point rule of orders 4-5 or a 3x3 Gauss rule, P3 with
+      // the reference's 20-point rule of order 8 or a 5x5 Gauss rule
+      if (d.ndof == 4 && d.nq == 8 && d.nfl == 9)
+        return launch_euler<PHYS, SCHEME, T, 4, 8, 9, 4, 4>(g, a, s);
+      if (d.ndof == 4 && d.nq == 9 && d.nfl == 9)
+        return launch_euler<PHYS, SCHEME, T, 4, 9, 9, 4, 4>(g, a, s);
+      if (d.ndof == 9 && d.nq == 8 && d.nfl == 16)
+        return launch_euler<PHYS, SCHEME, T, 9, 8, 16, 4, 4>(g, a, s);
+      if (d.ndof == 9 && d.nq == 9 && d.nfl == 16)
+        return launch_euler<PHYS, SCHEME, T, 9, 9, 16, 4, 4>(g, a, s);
       if (d.ndof == 16 && d.nq == 20 && d.nfl == 25)
         return launch_euler<PHYS, SCHEME, T, 16, 20, 25, 4, 8>(g, a, s);
       if (d.ndof == 16 && d.nq == 25 && d.nfl == 25)
