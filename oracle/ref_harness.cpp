@@ -200,7 +200,16 @@ int run(const Args &a)
   const Uint ngeo_nodes = (*geo).nb_nodes();
   std::vector<Real> geo_coords(ngeo_nodes * D, 0.0);
   std::vector<int> geo_conn(ncells * ngeo), sol_conn(ncells * ndof);
+  bool single_type = true;
   for (Uint c = 0; c < ncells; ++c)
+    if ((*sol).active_cell(ActiveIdx(c)).pt_set_id() != cell0.pt_set_id())
+      single_type = false;
+  if (!single_type && a.mode == "dump")
+  {
+    std::cerr << "dump mode needs a mesh of one element type" << std::endl;
+    return 2;
+  }
+  for (Uint c = 0; c < ncells && single_type; ++c)
   {
     const MeshEntity gc = (*geo).active_cell(ActiveIdx(c));
     const MeshEntity sc = (*sol).active_cell(ActiveIdx(c));
@@ -266,28 +275,9 @@ int run(const Args &a)
                     sf::SFTag(fshape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
   fe_fgeo.fill_Vandermonde(fqp, fqw);
 
-  // ---- initial state from coordinates of solution dofs (geometry basis at sol nodes)
-  interpolation::FEValues fe_geo_at_sol;
-  math::DenseDVec<Real> dummy_ws(ndof);
-  dummy_ws.fill(1.0);
-  fe_geo_at_sol.configure(PointSetTag(shape, geo_order, PointSetID::Equidist),
-                          sf::SFTag(shape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
-  fe_geo_at_sol.fill_Vandermonde(sol_nodes, dummy_ws);
-  const math::DenseDMat<Real> &Vgs = fe_geo_at_sol.Vandermonde();
-
-  std::vector<Real> sol_coords(nsol * D, 0.0);
-  for (Uint c = 0; c < ncells; ++c)
-  {
-    for (Uint n = 0; n < ndof; ++n)
-    {
-      Real x[3] = {0.0, 0.0, 0.0};
-      for (Uint g = 0; g < ngeo; ++g)
-        for (Uint d = 0; d < D; ++d)
-          x[d] += Vgs(n, g) * geo_coords[geo_conn[c * ngeo + g] * D + d];
-      for (Uint d = 0; d < D; ++d)
-        sol_coords[sol_conn[c * ndof + n] * D + d] = x[d];
-    }
-  }
+  // ---- initial state from coordinates of solution dofs (geometry basis at the solution nodes
+  // of each cell, so mixed meshes work too)
+  const std::vector<Real> sol_coords = solution_node_coords(*mesh, *geo, *sol, D);
   std::vector<Real> u0(nsol * NEQ);
   for (Uint i = 0; i < nsol; ++i)
   {
