@@ -63,10 +63,12 @@ struct rds_ctx
   // pinned host scalars for the loop's stop test
   int *h_stop = nullptr;
 
-  // CUDA graphs of a chunk of fused iterations: FP64 cells, FP32 cells, batched problems.
+  // CUDA graphs: a chunk of fused iterations with FP64 cells (0), FP32 cells (1), batched
+  // problems (2); one iteration without stop test for rds_run, FP64 (3) / FP32 (4) cells.
   // The loop parameters are read from d_loop, so a graph stays valid across calls.
   static constexpr int kChunk    = 16;
-  cudaGraphExec_t graph_exec[3] = {nullptr, nullptr, nullptr};
+  static constexpr int kGraphs   = 5;
+  cudaGraphExec_t graph_exec[kGraphs] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   LoopParams *d_loop            = nullptr;
 
   // precision of the cell kernels being launched (the mixed loop finishes in FP64)
@@ -341,7 +343,7 @@ rds_status check_status(rds_ctx *ctx)
 
 void release_graph(rds_ctx *ctx)
 {
-  for (int k = 0; k < 3; ++k)
+  for (int k = 0; k < rds_ctx::kGraphs; ++k)
     if (ctx->graph_exec[k])
     {
       cudaGraphExecDestroy(ctx->graph_exec[k]);
@@ -935,9 +937,10 @@ static rds_status enqueue_iteration(rds_ctx *ctx, double cfl, int max_iter, doub
   });
 }
 
-// Captures kChunk iterations (enqueued by `one`) into graph slot gi once; later calls reuse it.
+// Captures `count` iterations (enqueued by `one`) into graph slot gi once; later calls reuse
+// it.
 extern "C++" template <typename F>
-rds_status capture_chunk(rds_ctx *ctx, int gi, F &&one)
+rds_status capture_graph(rds_ctx *ctx, int gi, int count, F &&one)
 {
   if (ctx->graph_exec[gi])
     return RDS_OK;
@@ -945,7 +948,7 @@ rds_status capture_chunk(rds_ctx *ctx, int gi, F &&one)
   cudaGraph_t graph = nullptr;
   RDS_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   const long long l0 = ctx->launches;
-  for (int k = 0; k < rds_ctx::kChunk; ++k)
+  for (int k = 0; k < count; ++k)
   {
     st = one();
     if (st != RDS_OK)
@@ -966,6 +969,12 @@ rds_status capture_chunk(rds_ctx *ctx, int gi, F &&one)
     return fail(ctx, RDS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
   }
   return RDS_OK;
+}
+
+extern "C++" template <typename F>
+rds_status capture_chunk(rds_ctx *ctx, int gi, F &&one)
+{
+  return capture_graph(ctx, gi, rds_ctx::kChunk, one);
 }
 
 // Replays graph slot gi up to nchunks times, polling the device stop flag every 4 chunks
@@ -1111,16 +1120,36 @@ rds_status rds_run(rds_ctx *ctx, double cfl, int n)
       return st;
     ctx->hist_cap = 1;
   }
-  for (int i = 0; i < n; ++i)
-  {
-    if ((st = launch_residual_kernels(ctx, ctx->d_zero)) != RDS_OK)
-      return st;
-    const GatherArgs ga = gather_args(ctx, cfl, ctx->d_zero);
-    st = launch(ctx, [&](const char **name) {
+  auto one = [&]() -> rds_status {
+    rds_status s2 = launch_residual_kernels(ctx, ctx->d_zero);
+    if (s2 != RDS_OK)
+      return s2;
+    GatherArgs ga = gather_args(ctx, cfl, ctx->d_zero);
+    ga.loop       = ctx->d_loop;
+    return launch(ctx, [&](const char **name) {
       return launch_gather(ga, 7, ctx->gblocks, ctx->stream, name);
     });
-    if (st != RDS_OK)
-      return st;
+  };
+  LoopParams lp{};
+  lp.cfl = cfl;
+  RDS_CUDA(cudaMemcpyAsync(ctx->d_loop, &lp, sizeof(lp), cudaMemcpyHostToDevice, ctx->stream));
+  if (ctx->timing)
+  {
+    for (int i = 0; i < n; ++i)
+      if ((st = one()) != RDS_OK)
+        return st;
+    return RDS_OK;
+  }
+  // one iteration captured once (graph slot 3) and replayed n times: the launch sequence of an
+  // iteration costs one graph launch
+  const int gi = ctx->active_precision == RDS_MIXED ? 4 : 3;
+  if ((st = capture_graph(ctx, gi, 1, one)) != RDS_OK)
+    return st;
+  const long long per_iter = (long long)ctx->groups.size() + (long long)ctx->bcs.size() + 1;
+  for (int i = 0; i < n; ++i)
+  {
+    RDS_CUDA(cudaGraphLaunch(ctx->graph_exec[gi], ctx->stream));
+    ctx->launches += per_iter;
   }
   return RDS_OK;
 }

@@ -476,12 +476,12 @@ __global__ void __launch_bounds__(kBlock)
         for (int e = 0; e < NEQ; ++e)
         {
           const double r = (SCHEME == RDS_PGLDA) ? lda[s][e] : lda[s][e] + theta * diss[s][e];
-          __stcs(a.contrib + e * a.S + slot0, r);
+          a.contrib[e * a.S + slot0] = r; // write-back: the gather reads it from L2
         }
       }
     }
     if (lane == 0)
-      __stcs(a.wsc + a.ws_base + c, vol * wmax);
+      a.wsc[a.ws_base + c] = vol * wmax;
     if (bad)
       atomicOr(a.status, kFlagNegPressure);
   }

@@ -228,9 +228,9 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
   for (int n = 0; n < NDOF; ++n)
   {
     const double r = (SCHEME == RDS_PGLDA) ? lda[n] : lda[n] + theta * diss[n];
-    __stcs(out + (size_t)n * a.ncells, r);
+    out[(size_t)n * a.ncells] = r; // write-back: the gather reads it from L2
   }
-  __stcs(a.wsc + a.ws_base + c, vol * double(wsmax));
+  a.wsc[a.ws_base + c] = vol * double(wsmax);
 }
 
 template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, bool AFFINE>

@@ -81,7 +81,39 @@ __device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, co
   double ws       = 0.0;
   const double iv = a.inv_vol[v];
   const int i0 = a.row[v], i1 = a.row[v + 1];
-  for (int i = i0; i < i1; ++i)
+  int i        = i0;
+  // four entries at a time: all their loads are issued before the ordered sums consume them
+  // (same summation order as the one-by-one loop below)
+  constexpr int B = 4;
+  for (; i + B <= i1; i += B)
+  {
+    long long s[B];
+    int w[B];
+#pragma unroll
+    for (int k = 0; k < B; ++k)
+    {
+      s[k] = __ldg(a.ent_slot + i + k);
+      w[k] = __ldg(a.ent_ws + i + k);
+    }
+    double cv[B][NEQ], wv[B];
+#pragma unroll
+    for (int k = 0; k < B; ++k)
+    {
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+        cv[k][e] = __ldcs(a.contrib + e * a.S + s[k]);
+      wv[k] = __ldcs(a.wsc + w[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < B; ++k)
+    {
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+        acc[e] = __dadd_rn(acc[e], __dmul_rn(iv, cv[k][e]));
+      ws = __dadd_rn(ws, wv[k]);
+    }
+  }
+  for (; i < i1; ++i)
   {
     const long long s = __ldg(a.ent_slot + i);
     const int w       = __ldg(a.ent_ws + i);
