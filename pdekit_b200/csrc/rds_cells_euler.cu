@@ -185,8 +185,8 @@ struct EulerSmem
 };
 
 template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, bool AFFINE,
-          int G>
-__global__ void __launch_bounds__(kBlock)
+          int G, int NT>
+__global__ void __launch_bounds__(NT)
     cells_euler(const CellArgs a, const Tables<T, (PHYS == RDS_EULER3D ? 3 : 2), NDOF, NQ, NFL,
                                                 NGEO> tb)
 {
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(kBlock)
   constexpr int NEQ = D + 2;
   constexpr int NPT = (NDOF + G - 1) / G; // nodes per lane
   using SM          = EulerSmem<T, D, NDOF, NQ, NFL>;
-  constexpr int CPB = kBlock / G; // cells per block
+  constexpr int CPB = NT / G; // cells per block
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (*a.stop)
@@ -487,20 +487,26 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, int G>
+// NT: threads per block. kBlock unless the per-cell shared memory would then leave the SM
+// with fewer warps than its registers allow (Euler 3D FP64: 3.9 KB per cell, so 56 cells in
+// one block of 224 threads use the SM's 227 KB instead of one block of 32 cells).
+template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, int G,
+          int NT = kBlock>
 cudaError_t launch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream_t s)
 {
   constexpr int D = (PHYS == RDS_EULER3D) ? 3 : 2;
   Tables<T, D, NDOF, NQ, NFL, NGEO> tb;
   fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
-  constexpr int CPB  = kBlock / G;
+  constexpr int CPB  = NT / G;
+  static_assert(CPB * EulerSmem<T, D, NDOF, NQ, NFL>::BYTES <= 227 * 1024,
+                "per-block shared memory above the sm_100 limit");
   const int smem     = CPB * EulerSmem<T, D, NDOF, NQ, NFL>::BYTES;
   const int grid     = (a.ncells + CPB - 1) / CPB;
   // the shared-memory opt-in is set once per instantiation (not a stream operation, so it
   // also stays out of captured graphs)
   static bool attr_set = false;
-  auto k_aff           = cells_euler<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, true, G>;
-  auto k_gen           = cells_euler<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, false, G>;
+  auto k_aff           = cells_euler<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, true, G, NT>;
+  auto k_gen           = cells_euler<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, false, G, NT>;
   if (!attr_set)
   {
     cudaError_t e = cudaFuncSetAttribute(k_aff, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -511,9 +517,9 @@ cudaError_t launch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream_t
     attr_set = true;
   }
   if (g.affine)
-    k_aff<<<grid, kBlock, smem, s>>>(a, tb);
+    k_aff<<<grid, NT, smem, s>>>(a, tb);
   else
-    k_gen<<<grid, kBlock, smem, s>>>(a, tb);
+    k_gen<<<grid, NT, smem, s>>>(a, tb);
   return cudaGetLastError();
 }
 
@@ -558,7 +564,8 @@ cudaError_t dispatch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream
     if (d.shape == RDS_TETRA && d.ngeo == 4)
     {
       if (d.ndof == 10 && d.nq == 14 && d.nfl == 20)
-        return launch_euler<PHYS, SCHEME, T, 10, 14, 20, 4, 4>(g, a, s);
+        return launch_euler<PHYS, SCHEME, T, 10, 14, 20, 4, 4, (sizeof(T) == 8 ? 224 : kBlock)>(
+            g, a, s);
     }
   }
   *ok = false;
