@@ -75,6 +75,10 @@ def parse():
     ap.add_argument("--drop-max-iter", type=int, default=400000)
     ap.add_argument("--quick", action="store_true",
                     help="only warm-up + timed steps (profiling runs): no e2e, mixed, drop, CPU")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="--quick: precision of the timed steps")
+    ap.add_argument("--tensor-cores", action="store_true",
+                    help="mixed cells with the basis contractions on the tensor cores")
     return ap.parse_args()
 
 
@@ -393,8 +397,11 @@ def run_ours(args, rank, world, local):
     steps = args.steps or default_steps
     ncells = prob.ncells
 
-    solver = PGRDMethodExplicit(prob.physics, prob.scheme, "fp64").configure_mesh_data(prob)
+    prec0 = args.precision if args.quick else "fp64"
+    solver = PGRDMethodExplicit(prob.physics, prob.scheme, prec0).configure_mesh_data(prob)
     solver.initialize_work_data()
+    if args.tensor_cores:
+        solver.set_option("tensor_cores", 1)
     solver.set_solution(u0)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
 
@@ -419,7 +426,8 @@ def run_ours(args, rank, world, local):
     if args.quick:
         line = {"metric": "cell-residual updates/s", "value": value, "steps": steps,
                 "ms_per_step": ms / steps, "gpu_launches": int(launches), "quick": True,
-                "workload": args.workload}
+                "workload": args.workload, "precision": prec0,
+                "tensor_cores": bool(args.tensor_cores)}
         solver.close()
         return line
 
@@ -462,6 +470,8 @@ def run_ours(args, rank, world, local):
     # mixed precision form
     mixed = PGRDMethodExplicit(prob.physics, prob.scheme, "mixed").configure_mesh_data(prob)
     mixed.initialize_work_data()
+    if args.tensor_cores:
+        mixed.set_option("tensor_cores", 1)
     mixed.set_solution(u0)
     mixed.run(cfl, max(args.warmup, 3))
     mixed.set_solution(u0)

@@ -194,7 +194,10 @@ RDS_API rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double dr
  * until max_eq norm/norm(iter 0) <= mixed_switch, or, once that drop has halved at least
  * once, until it has not halved for max(mixed_stall_min, mixed_stall_mult x the last interval
  * between halvings) iterations (the problem's FP32 round-off floor; defaults 200 and 3), and
- * then finishes with FP64 sweeps to the requested drop. */
+ * then finishes with FP64 sweeps to the requested drop.
+ * "tensor_cores" (default 0): with RDS_MIXED, scalar physics on straight-sided P1-P3 triangles,
+ * 1 runs the FP32 cell kernel with its basis contractions on the tensor cores (tcgen05,
+ * 3xTF32); results agree with the CUDA-core FP32 kernel to FP32 accuracy. */
 RDS_API rds_status rds_set_option(rds_ctx *ctx, const char *key, double value);
 
 /* Enqueue n fused iterations (assemble_lhs_and_rhs(cfl) + solve()) on the context's stream and
@@ -217,7 +220,7 @@ RDS_API rds_status rds_run(rds_ctx *ctx, double cfl, int n);
  * its FP32 floor, as in rds_iterate) and then FP64 ones. Every problem's iterates equal those of its own single-problem context bit for
  * bit. iters[P] and rel[P] (may be NULL) receive the iterations done and the final
  * max_eq norm/norm(iter 0); RDS_ERR_ITER_CAP when a problem did not reach drop > 0.
- * rds_autotune times the persistent cell kernels for tiles of 64/128/256 cells per CTA and
+ * rds_autotune times the persistent cell kernels for tiles of 64/128 cells per CTA and
  * 1-16 CTAs per SM and keeps the fastest per group and precision; report (may be NULL)
  * receives a JSON list of the choices. */
 RDS_API rds_status rds_set_problems(rds_ctx *ctx, int nproblems, const int32_t *node_offsets,

@@ -76,6 +76,9 @@ struct rds_ctx
   // mixed form: relative residual at which the loop switches from FP32 to FP64 cell kernels
   // (earlier when the FP32 phase stops making progress)
   double mixed_switch = 1.e-6;
+  // mixed form: basis contractions on the tensor cores where built (option "tensor_cores";
+  // off by default: slower than the CUDA-core FP32 kernel at these contraction sizes)
+  bool use_tc         = false;
   int stall_min       = 200; // FP32 phase stalled: no halving of the drop for
   double stall_mult   = 3.0; //   max(stall_min, stall_mult x the last interval between halvings)
   StallRec *d_stall   = nullptr; // FP32-phase progress record of the single-problem loop
@@ -314,6 +317,16 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
   {
     const CellArgs a = cell_args(ctx, g, stop);
     rds_status st    = launch(ctx, [&](const char **name) {
+      if (ctx->active_precision == RDS_MIXED && ctx->use_tc && g.d_tc)
+      {
+        // FP32 cells with the basis contractions on the tensor cores, persistent CTAs
+        const int ntiles = (g.desc.ncells + 127) / 128;
+        const int grid   = std::max(1, std::min(ntiles, 4 * ctx->nsm));
+        bool ok          = false;
+        const cudaError_t e =
+            launch_cells_scalar_tc(g, a, false, grid, ntiles, ctx->stream, name, &ok);
+        return ok ? e : cudaErrorNotSupported;
+      }
       return launch_cells(g, a, g.physics, g.scheme, ctx->active_precision, d.dim, d.neq,
                           ctx->stream, name);
     });
@@ -338,6 +351,8 @@ rds_status check_status(rds_ctx *ctx)
     return fail(ctx, RDS_ERR_NONFINITE, "non-finite residual norm");
   if (st & kFlagNegPressure)
     return fail(ctx, RDS_ERR_NEG_PRESSURE, "non-positive pressure met");
+  if (st & kFlagTimeout)
+    return fail(ctx, RDS_ERR_CUDA, "a bounded device wait (tensor-core commit) gave up");
   return RDS_OK;
 }
 
@@ -776,6 +791,21 @@ rds_status rds_finalize(rds_ctx *ctx)
       (st = dalloc(ctx, &ctx->d_stall, 1)) != RDS_OK)
     return st;
   ctx->extra.push_back(ctx->d_stall);
+  // mixed form: operand tables of the tensor-core cell kernel (scalar physics, triangles)
+  if (d.precision == RDS_MIXED)
+    for (HostCellGroup &g : ctx->groups)
+    {
+      std::vector<float> tct;
+      tc_tables(g, tct);
+      if (tct.empty())
+        continue;
+      if ((st = dalloc(ctx, &g.d_tc, tct.size())) != RDS_OK ||
+          (st = upload(ctx, g.d_tc, tct.data(), tct.size())) != RDS_OK)
+        return st;
+      ctx->extra.push_back(g.d_tc);
+      g.tune_tile[0] = 128; // one cell per TMEM lane
+    }
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
   RDS_CUDA(cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device));
   if (ctx->nprob > 0 && (st = finalize_batch(ctx)) != RDS_OK)
     return st;
@@ -1165,6 +1195,12 @@ rds_status rds_set_option(rds_ctx *ctx, const char *key, double value)
     ctx->mixed_switch = value;
     return RDS_OK;
   }
+  if (std::strcmp(key, "tensor_cores") == 0)
+  {
+    ctx->use_tc = value != 0.0;
+    release_graph(ctx); // captured loops hold the previous choice
+    return RDS_OK;
+  }
   if (std::strcmp(key, "mixed_stall_min") == 0)
   {
     if (!(value >= 1.0 && value <= 2.0e9))
@@ -1348,10 +1384,13 @@ static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed)
       CellArgs a = cell_args(ctx, g, ctx->d_stop);
       a.bt       = {ctx->d_tile_prefix + ((size_t)gi * 2 + ph) * (P + 1), g.d_cbeg, g.d_cend, P};
       const int grid = g.tune_grid[ph] > 0 ? g.tune_grid[ph] : 4 * ctx->nsm;
+      const bool tc  = ph == 0 && ctx->use_tc && g.d_tc;
       if ((st = launch(ctx, [&](const char **name) {
              bool ok = false;
-             cudaError_t e = launch_cells_scalar_batch(g, a, ph == 0 ? RDS_MIXED : RDS_FP64, grid,
-                                                       g.tune_tile[ph], ctx->stream, name, &ok);
+             cudaError_t e =
+                 tc ? launch_cells_scalar_tc(g, a, true, grid, 0, ctx->stream, name, &ok)
+                    : launch_cells_scalar_batch(g, a, ph == 0 ? RDS_MIXED : RDS_FP64, grid,
+                                                g.tune_tile[ph], ctx->stream, name, &ok);
              return ok ? e : cudaErrorNotSupported;
            })) != RDS_OK)
         return st;
@@ -1471,14 +1510,14 @@ rds_status rds_iterate_batch(rds_ctx *ctx, int max_iter, double drop, int32_t *i
 }
 
 // Autotuner: for every group and cell precision of the batch, time the persistent cell kernel
-// over all problems for tiles of 64 / 128 / 256 cells per CTA and 1..16 resident CTAs per SM,
+// over all problems for tiles of 64 / 128 cells per CTA and 1..16 resident CTAs per SM,
 // and keep the fastest (tile, grid). Results per cell do not depend on the choice.
 rds_status rds_autotune(rds_ctx *ctx, char *report, int len)
 {
   if (!ctx || !ctx->finalized || ctx->nprob == 0)
     return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_autotune: not a finalized batched context")
                : RDS_ERR_INVALID;
-  static const int kTiles[] = {64, 128, 256};
+  static const int kTiles[] = {64, 128};
   static const int kPerSm[] = {1, 2, 4, 8, 16};
   const int P = ctx->nprob;
   const bool mixed = ctx->desc.precision == RDS_MIXED;
@@ -1497,8 +1536,11 @@ rds_status rds_autotune(rds_ctx *ctx, char *report, int len)
       float best = 1e30f;
       int best_tile = 128, best_grid = 4 * ctx->nsm;
       const char *kname = "?";
+      const bool tc     = ph == 0 && ctx->use_tc && g.d_tc; // tensor-core kernel: 128-cell tiles
       for (int tile : kTiles)
       {
+        if (tc && tile != 128)
+          continue;
         std::vector<int32_t> pre(P + 1, 0);
         for (int p = 0; p < P; ++p)
           pre[p + 1] = pre[p] + (g.pcells[p + 1] - g.pcells[p] + tile - 1) / tile;
@@ -1519,7 +1561,11 @@ rds_status rds_autotune(rds_ctx *ctx, char *report, int len)
           {
             if (rep_i == 1)
               RDS_CUDA(cudaEventRecord(e0, ctx->stream));
-            RDS_CUDA(launch_cells_scalar_batch(g, a, prec, grid, tile, ctx->stream, &kname, &ok));
+            if (tc)
+              RDS_CUDA(launch_cells_scalar_tc(g, a, true, grid, 0, ctx->stream, &kname, &ok));
+            else
+              RDS_CUDA(
+                  launch_cells_scalar_batch(g, a, prec, grid, tile, ctx->stream, &kname, &ok));
             if (!ok)
               return fail(ctx, RDS_ERR_UNSUPPORTED,
                           "rds_autotune: no batched kernel for this cell group");

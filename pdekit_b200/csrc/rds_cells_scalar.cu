@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(kBlock)
 // at this precision); a tile is blockDim.x consecutive cells of one problem, so every thread of
 // a block maps to the same problem. Results per cell are those of cells_scalar2d.
 template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(128)
     cells_scalar2d_batch(const __grid_constant__ CellArgs a,
                          const __grid_constant__ Tables<T, 2, NDOF, NQ, NFL, NGEO> tb)
 {
@@ -390,7 +390,7 @@ cudaError_t launch_cells_scalar_batch(const HostCellGroup &g, const CellArgs &a,
   const int physics = g.physics, scheme = g.scheme;
   *ok               = false;
   if ((physics != RDS_ADVECTION_CONST && physics != RDS_BURGERS2D) || scheme < 0 || scheme > 2 ||
-      tile <= 0 || tile > 256 || grid <= 0)
+      tile <= 0 || tile > 128 || grid <= 0)
     return cudaSuccess;
   *name = names[physics == RDS_BURGERS2D][scheme][precision == RDS_MIXED];
 #define RDS_BATCH_CASE(PH, SC)                                                                     \

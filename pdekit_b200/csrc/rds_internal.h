@@ -21,7 +21,8 @@ constexpr int kGBlock  = 256; // threads per block of the node gather kernel
 enum : unsigned
 {
   kFlagNonFinite   = 1u,
-  kFlagNegPressure = 2u
+  kFlagNegPressure = 2u,
+  kFlagTimeout     = 4u // a bounded device wait gave up
 };
 
 // Host copy of one element type's tables; passed to kernels by value through the parameter
@@ -43,6 +44,7 @@ struct HostCellGroup
   int32_t *d_cbeg = nullptr, *d_cend = nullptr;
   int tune_tile[2] = {128, 128}; // cells per CTA tile (phase 0 FP32, phase 1 FP64)
   int tune_grid[2] = {0, 0};     // persistent grid (CTAs), 0: 4 per SM
+  float *d_tc      = nullptr;    // tensor-core tables of the FP32 kernel (rds_cells_scalar_tc.cu)
 };
 
 struct HostBC
@@ -233,6 +235,12 @@ cudaError_t launch_cells_scalar_batch(const HostCellGroup &g, const CellArgs &a,
 cudaError_t launch_gather_batch(const GatherArgs &a, const BatchArgs &b, int grid, cudaStream_t s,
                                 const char **name);
 cudaError_t launch_batch_rebuild(const RebuildArgs &r, cudaStream_t s, const char **name);
+// Mixed form, scalar physics on straight-sided triangles: the cell kernel with the basis
+// contractions on the tensor cores (persistent over 128-cell tiles; batch: active tiles).
+bool tc_supported(const HostCellGroup &g);
+void tc_tables(const HostCellGroup &g, std::vector<float> &out);
+cudaError_t launch_cells_scalar_tc(const HostCellGroup &g, const CellArgs &a, bool batch, int grid,
+                                   int ntiles, cudaStream_t s, const char **name, bool *ok);
 cudaError_t launch_update(int nnodes, int neq, const double *dt, const double *res, double *u,
                           cudaStream_t s, const char **name);
 

@@ -91,3 +91,23 @@ def test_batch_iteration_cap(batch_case):
     for i in (0, len(probs) - 1):
         it, u, r = _single(probs[i], states[i], cfls[i], "fp64", max_iter=25)
         assert it == 25 and np.array_equal(u, us[i])
+
+
+def test_batch_tensor_core_cells(batch_case):
+    """Batched mixed form with the FP32 cells on the tensor cores: every problem reaches the drop
+    and its state agrees with the CUDA-core mixed batch to 1e-9 relative L2 (both finish with
+    FP64 sweeps)."""
+    from pdekit_b200.batch import BatchedRDS
+
+    probs, states, cfls, info = batch_case
+    us = {}
+    for tc in (0, 1):
+        b = BatchedRDS(probs, cfls, "mixed")
+        b.set_option("tensor_cores", tc)
+        b.set_solutions(states)
+        iters, rel = b.iterate(CAP, DROP)
+        assert np.all(rel <= DROP)
+        us[tc] = b.solutions()
+        b.close()
+    for u0, u1 in zip(us[0], us[1]):
+        assert np.linalg.norm(u1 - u0) <= 1e-9 * np.linalg.norm(u0)

@@ -137,3 +137,29 @@ def test_mixed_loop_reaches_fp64_solution(case, cfl):
         s.close()
     u64, um = out["fp64"][0], out["mixed"][0]
     assert np.linalg.norm(um - u64) / np.linalg.norm(u64) < 1e-9
+
+
+@pytest.mark.parametrize("case", [c for c in golden_cases() if not c.startswith("euler")])
+def test_tensor_core_contraction_matches_fp32_path(case):
+    """Mixed form: the cell kernel with the basis contractions on the tensor cores (tcgen05,
+    3xTF32 split operands, FP32 accumulation) against the CUDA-core FP32 kernel, on the first
+    residual and after 40 iterations (both FP32-level: 2e-6 of the largest magnitude)."""
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    out = {}
+    for tc in (0, 1):
+        s = _solver(prob, "mixed")
+        s.set_option("tensor_cores", tc)
+        s.set_solution(a["u0"])
+        s.assemble_lhs_and_rhs(meta["cfl"])
+        res, dt, ws, vol = s.fields()
+        s.set_solution(a["u0"])
+        s.kernel_timing(True)
+        s.run(meta["cfl"], 40)
+        names = set(s.kernel_times())
+        s.kernel_timing(False)
+        assert any(n.endswith("_tc") for n in names) == bool(tc), names
+        out[tc] = (res, ws, s.solution())
+        s.close()
+    for i in range(3):
+        ref, got = out[0][i], out[1][i]
+        assert np.abs(got - ref).max() <= 2e-6 * np.abs(ref).max(), (case, i)
