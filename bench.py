@@ -26,8 +26,9 @@ Metric: cell-residual updates/s = cells x steps / time. Reported:
             on a bounded sample of the same workload, all host cores.
 
   python bench.py [--workload c1..c5] [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-With N > 1 (torchrun), every rank runs its own independent copy of the workload (replicas; the
-path has no data exchange between independent problems), timing is the max over ranks.
+With N > 1 (torchrun), every rank runs its own independent copy of c1-c4 (replicas, weak
+scaling; the path has no data exchange between independent problems); c5's problems are split
+over the ranks by estimated work (strong scaling). Timing is the max over ranks.
 """
 
 from __future__ import annotations
@@ -105,6 +106,17 @@ def max_over_ranks(x, world):
 
     t = torch.tensor([x], dtype=torch.float64, device="cuda")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -527,7 +539,17 @@ def run_batched(args, rank, world, local):
     from pdekit_b200.batch import BatchedRDS
     from pdekit_b200.rds import PGRDMethodExplicit, measure_peak
 
-    probs, states, cfls, info = workloads.config5(nprob=args.c5_nprob, seed=5 + rank)
+    probs, states, cfls, info = workloads.config5(nprob=args.c5_nprob, seed=5)
+    total_cells = sum(p.ncells for p in probs)
+    if world > 1:
+        # one problem set, split over the ranks by estimated work (no exchange between problems)
+        from pdekit_b200.batch import shard_problems
+
+        mine = shard_problems(probs, world)[rank]
+        probs = [probs[i] for i in mine]
+        states = [states[i] for i in mine]
+        cfls = cfls[mine]
+        info = [info[i] for i in mine]
     cells = sum(p.ncells for p in probs)
     u_host = [torch.from_numpy(np.ascontiguousarray(s)).pin_memory() for s in states]
     res = {}
@@ -550,18 +572,20 @@ def run_batched(args, rank, world, local):
             torch.cuda.synchronize()
             sec = time.time() - t0
         sec = max_over_ranks(sec, world)
-        cu = float(sum(p.ncells * int(i) for p, i in zip(probs, iters)))
-        res[prec] = {"seconds": round(sec, 3), "iterations_max": int(iters.max()),
+        cu = sum_over_ranks(float(sum(p.ncells * int(i) for p, i in zip(probs, iters))), world)
+        res[prec] = {"seconds": round(sec, 3),
+                     "iterations_max": int(max_over_ranks(float(iters.max()), world)),
                      "iterations_mean": float(iters.mean()), "cell_updates": cu,
-                     "cell_updates_per_s": cu * world / sec,
-                     "problems_reached": int((rel <= 1e-10).sum()), "autotune": tune}
+                     "cell_updates_per_s": cu / sec,
+                     "problems_reached": int(sum_over_ranks(float((rel <= 1e-10).sum()), world)),
+                     "autotune": tune}
         res[prec + "_states"] = out
         if prec == "fp64":
             launches = b.launch_count() - l0
             clocks = clk.summary()
         b.close()
-    rel_l2 = max(float(np.linalg.norm(a - c) / np.linalg.norm(a))
-                 for a, c in zip(res["fp64_states"], res["mixed_states"]))
+    rel_l2 = max_over_ranks(max(float(np.linalg.norm(a - c) / np.linalg.norm(a))
+                                for a, c in zip(res["fp64_states"], res["mixed_states"])), world)
     del res["fp64_states"], res["mixed_states"]
     seq = None
     if args.c5_sequential and world == 1:
@@ -587,14 +611,16 @@ def run_batched(args, rank, world, local):
         "metric": "cell-residual updates/s", "value": f64["cell_updates_per_s"],
         "unit": "cell-residual updates/s", "n_gpus": world, "steps": f64["iterations_max"],
         "warmup": 3, "ms_per_step": f64["seconds"] * 1e3 / f64["iterations_max"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
-        "config": {"workload": f"configuration 5: {len(probs)} independent problems "
+        "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"configuration 5: {args.c5_nprob} independent problems "
                                f"(advection LDA / Burgers N, P1-P3 triangles, log-uniform "
-                               f"1k-200k cells, own CFL), {cells:,} cells in total, each to its "
-                               f"own 1e-10 drop, batched persistent launches in one CUDA graph",
-                   "cells": cells, "l2": "inputs larger than L2 (state and contributions)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                               f"1k-200k cells, own CFL), {total_cells:,} cells in total, each "
+                               f"to its own 1e-10 drop, batched persistent launches in one CUDA "
+                               f"graph",
+                   "cells": total_cells, "l2": "inputs larger than L2 (state and contributions)",
+                   "parallelism": (f"problems split over {world} GPUs by estimated work, no "
+                                   f"exchange") if world > 1 else "single GPU"},
         "e2e": {"value": f64["cell_updates_per_s"], "unit": "cell-residual updates/s",
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                 "note": "the timed region of value already copies every problem's state in from "

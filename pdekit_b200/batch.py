@@ -133,6 +133,28 @@ def merge_problems(problems: list) -> MergedBatch:
                        groups=groups, bcs=bcs, adv=adv or (0.0, 0.0, 0.0))
 
 
+def problem_work(p: Problem) -> float:
+    """Relative cost estimate of iterating one problem to its drop: cells x points x dofs (one
+    cell kernel step) x order (pseudo-time iterations grow with the order)."""
+    return float(sum(g.ncells * g.nq * g.ndof * g.order for g in p.groups))
+
+
+def shard_problems(problems: list, nranks: int) -> list:
+    """Split independent problems over ranks (one GPU each): largest estimated work first, each
+    to the least loaded rank. Returns the sorted problem indices of every rank; the problems need
+    no exchange between ranks."""
+    if nranks < 1:
+        raise ValueError("nranks must be >= 1")
+    load = [0.0] * nranks
+    shards = [[] for _ in range(nranks)]
+    order = sorted(range(len(problems)), key=lambda i: (-problem_work(problems[i]), i))
+    for i in order:
+        r = min(range(nranks), key=lambda k: (load[k], k))
+        shards[r].append(i)
+        load[r] += problem_work(problems[i])
+    return [sorted(sh) for sh in shards]
+
+
 class BatchedRDS:
     """P independent problems iterated together: persistent cell launches over the active
     problems, one per-problem gather / update / norm / stop test, the loop in one CUDA graph."""
