@@ -133,23 +133,24 @@ def barrier(world):
 
 
 def scalar_flops(physics, scheme, ndof, nq, nfl):
-    """Scalar 2D kernel on straight-sided triangles (affine geometry):
-      flux nodes  nfl x (2 ndof - 1 + 2)            state at the node, flux
+    """Scalar 2D kernel on straight-sided triangles (affine geometry), in the form the kernel
+    evaluates (flux contracted with invJ once per flux node, k_n = dV0 A + dV1 B):
+      flux nodes  nfl x (2 ndof - 1 + 2 + 6)        state at the node, flux, G0/G1 = invJ^T F
       geometry    28                                Jacobian, determinant, inverse
-      per point   2 + 4 (2 nfl - 1) + 7             weight, flux divergence
+      per point   4 nfl - 1 + 4                     flux divergence, weight, volume, Phi
                   + (2 ndof - 1 for Burgers)        advection speed u_q
-                  + 10 ndof + 1                     upwind coefficients, their sum, 1/sum
-                  + 2 + 4 ndof                      Phi and LDA part
-                  + (2 ndof + 6 ndof for N / B)     N dissipation (O(ndof) form)
+                  + 6 + 6 ndof + 3                  A, B; k_n, K+, max |k|, sum K+; 1/sum, e
+                  + 2 ndof                          LDA part
+                  + (7 ndof for N / B)              N dissipation (O(ndof) form)
       end         27 for B (blending), 5 otherwise
-    Configuration 2 (Burgers P2 B, ndof 6, nq 7, nfl 10): 1,802 flop; configuration 1
-    (advection P1 LDA, ndof 3, nq 6, nfl 6): 663 flop."""
-    fl = nfl * (2 * ndof - 1 + 2) + 28
-    per_q = 2 + 4 * (2 * nfl - 1) + 7 + 10 * ndof + 1 + 2 + 4 * ndof
+    Configuration 2 (Burgers P2 B, ndof 6, nq 7, nfl 10): 1,316 flop; configuration 1
+    (advection P1 LDA, ndof 3, nq 6, nfl 6): 471 flop."""
+    fl = nfl * (2 * ndof - 1 + 2 + 6) + 28
+    per_q = 4 * nfl - 1 + 4 + 6 + 6 * ndof + 3 + 2 * ndof
     if physics == "burgers":
         per_q += 2 * ndof - 1
     if scheme != "lda":
-        per_q += 8 * ndof
+        per_q += 7 * ndof
     return fl + nq * per_q + (27 if scheme == "b" else 5)
 
 

@@ -1518,7 +1518,7 @@ rds_status rds_autotune(rds_ctx *ctx, char *report, int len)
     return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_autotune: not a finalized batched context")
                : RDS_ERR_INVALID;
   static const int kTiles[] = {64, 128};
-  static const int kPerSm[] = {1, 2, 4, 8, 16};
+  static const int kPerSm[] = {1, 2, 3, 4, 5, 6, 8, 12, 16}; // capped at the kernel's occupancy
   const int P = ctx->nprob;
   const bool mixed = ctx->desc.precision == RDS_MIXED;
   rds_status st;

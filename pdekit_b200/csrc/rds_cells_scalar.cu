@@ -30,7 +30,7 @@ namespace rds
 namespace
 {
 
-template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, bool AFFINE>
+template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO>
 __device__ __forceinline__ void scalar_cell(const CellArgs &a,
                                             const Tables<T, 2, NDOF, NQ, NFL, NGEO> &tb,
                                             const int c)
@@ -53,8 +53,11 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
     un[n]       = DEV ? T(ud[n] - ud[0]) : T(ud[n]);
   }
   const T u0 = T(ud[0]);
-  T X0[NGEO], X1[NGEO];
+
+  // ---- straight-sided triangle: one Jacobian for all points
+  T ij00, ij01, ij10, ij11, detj;
   {
+    T X0[NGEO], X1[NGEO];
     double xg0 = 0.0, yg0 = 0.0;
 #pragma unroll
     for (int g = 0; g < NGEO; ++g)
@@ -69,49 +72,76 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
       X0[g] = DEV ? T(xg - xg0) : T(xg);
       X1[g] = DEV ? T(yg - yg0) : T(yg);
     }
-  }
-
-  // ---- state at the flux nodes (order p+1 Lagrange interpolant of F); the flux there is
-  // F = (s^2/2, s) for Burgers and (a0 s, a1 s) for advection, evaluated where it is used so
-  // only s is kept (FP32 form: s - u_0 and F(s) - F(u_0))
-  T sf[NFL];
-#pragma unroll
-  for (int f = 0; f < NFL; ++f)
-  {
-    T s = DEV ? T(0) : tb.Vsf[f][0] * un[0];
-#pragma unroll
-    for (int n = 1; n < NDOF; ++n)
-      s = s + tb.Vsf[f][n] * un[n];
-    sf[f] = s;
-  }
-  auto flux0 = [&](int f) -> T {
-    if (PHYS == RDS_BURGERS2D)
-      return DEV ? sf[f] * (u0 + T(0.5) * sf[f]) : T(0.5) * sf[f] * sf[f];
-    return T(a.adv0) * sf[f];
-  };
-  auto flux1 = [&](int f) -> T { return PHYS == RDS_BURGERS2D ? sf[f] : T(a.adv1) * sf[f]; };
-
-  T ij00 = 0, ij01 = 0, ij10 = 0, ij11 = 0, detj = 0;
-  auto jacobian = [&](int q) {
-    T J00 = tb.dVgeo[0][q][0] * X0[0], J01 = tb.dVgeo[0][q][0] * X1[0];
-    T J10 = tb.dVgeo[1][q][0] * X0[0], J11 = tb.dVgeo[1][q][0] * X1[0];
+    T J00 = tb.dVgeo[0][0][0] * X0[0], J01 = tb.dVgeo[0][0][0] * X1[0];
+    T J10 = tb.dVgeo[1][0][0] * X0[0], J11 = tb.dVgeo[1][0][0] * X1[0];
 #pragma unroll
     for (int g = 1; g < NGEO; ++g)
     {
-      J00 = J00 + tb.dVgeo[0][q][g] * X0[g];
-      J01 = J01 + tb.dVgeo[0][q][g] * X1[g];
-      J10 = J10 + tb.dVgeo[1][q][g] * X0[g];
-      J11 = J11 + tb.dVgeo[1][q][g] * X1[g];
+      J00 = J00 + tb.dVgeo[0][0][g] * X0[g];
+      J01 = J01 + tb.dVgeo[0][0][g] * X1[g];
+      J10 = J10 + tb.dVgeo[1][0][g] * X0[g];
+      J11 = J11 + tb.dVgeo[1][0][g] * X1[g];
     }
-    detj           = J00 * J11 - J01 * J10;
+    detj            = J00 * J11 - J01 * J10;
     const T inv_det = T(1) / detj;
     ij00            = inv_det * J11;
     ij11            = inv_det * J00;
     ij01            = -inv_det * J01;
     ij10            = -inv_det * J10;
-  };
-  if (AFFINE)
-    jacobian(0);
+  }
+
+  // ---- flux divergence at the points. F is the order p+1 Lagrange interpolant through the
+  // flux nodes, F = (s^2/2, s) for Burgers and (a0 s, a1 s) for advection with s the state at
+  // the node (FP32 form: s - u_0 and F(s) - F(u_0)). With invJ constant over the cell,
+  //   r_q = sum_f dVf[0][q][f] G0_f + dVf[1][q][f] G1_f,
+  //   G0_f = invJ00 F0_f + invJ10 F1_f,  G1_f = invJ01 F0_f + invJ11 F1_f,
+  // i.e. the flux is contracted with invJ once per node instead of once per node and point.
+  // The values r_q (and Phi = sum_q w_q detJ r_q) are formed first, so the contracted flux is
+  // dead before the upwind loop; the rolled FP64 loop keeps them in shared memory.
+  constexpr int QUNROLL = sizeof(T) == 8 ? 1 : NQ;
+  constexpr bool RQ_SHARED = QUNROLL == 1;
+  __shared__ T s_rq[RQ_SHARED ? NQ * kBlock : 1];
+  T rq_reg[RQ_SHARED ? 1 : NQ];
+  double phi = 0.0, vol = 0.0;
+  {
+    T G0[NFL], G1[NFL];
+#pragma unroll
+    for (int f = 0; f < NFL; ++f)
+    {
+      T s = DEV ? T(0) : tb.Vsf[f][0] * un[0];
+#pragma unroll
+      for (int n = 1; n < NDOF; ++n)
+        s = s + tb.Vsf[f][n] * un[n];
+      T F0, F1;
+      if (PHYS == RDS_BURGERS2D)
+      {
+        F0 = DEV ? s * (u0 + T(0.5) * s) : T(0.5) * s * s;
+        F1 = s;
+      }
+      else
+      {
+        F0 = T(a.adv0) * s;
+        F1 = T(a.adv1) * s;
+      }
+      G0[f] = ij00 * F0 + ij10 * F1;
+      G1[f] = ij01 * F0 + ij11 * F1;
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+    {
+      T r = tb.dVf[0][q][0] * G0[0] + tb.dVf[1][q][0] * G1[0];
+#pragma unroll
+      for (int f = 1; f < NFL; ++f)
+        r = r + tb.dVf[0][q][f] * G0[f] + tb.dVf[1][q][f] * G1[f];
+      const double wj = double(tb.w[q] * detj);
+      vol += wj;
+      phi += wj * double(r);
+      if constexpr (RQ_SHARED)
+        s_rq[q * kBlock + threadIdx.x] = r;
+      else
+        rq_reg[q] = r;
+    }
+  }
 
   double lda[NDOF], diss[NDOF];
 #pragma unroll
@@ -120,41 +150,19 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
     lda[n]  = 0.0;
     diss[n] = 0.0;
   }
-  double phi = 0.0, vol = 0.0;
-  T wsmax    = T(0);
+  T kmax = T(0);
 
   // FP64: the quadrature loop stays rolled (the unrolled P3 body overflows the instruction
-  // cache: 1.7x slower); table entries are then indexed constant-bank loads. FP32: unrolled.
-  constexpr int QUNROLL = sizeof(T) == 8 ? 1 : NQ;
+  // cache); table entries are then indexed constant-bank loads. FP32: unrolled.
 #pragma unroll QUNROLL
   for (int q = 0; q < NQ; ++q)
   {
-    if (!AFFINE)
-      jacobian(q);
-    const T wjT     = tb.w[q] * detj;
-    const double wj = double(wjT);
-    vol += wj;
-
-    // flux divergence at q
-    T d00, d01, d10, d11;
-    {
-      const T f0 = flux0(0), f1 = flux1(0);
-      d00 = tb.dVf[0][q][0] * f0;
-      d01 = tb.dVf[1][q][0] * f0;
-      d10 = tb.dVf[0][q][0] * f1;
-      d11 = tb.dVf[1][q][0] * f1;
-    }
-#pragma unroll
-    for (int f = 1; f < NFL; ++f)
-    {
-      const T f0 = flux0(f), f1 = flux1(f);
-      d00 = d00 + tb.dVf[0][q][f] * f0;
-      d01 = d01 + tb.dVf[1][q][f] * f0;
-      d10 = d10 + tb.dVf[0][q][f] * f1;
-      d11 = d11 + tb.dVf[1][q][f] * f1;
-    }
-    const T rT      = (ij00 * d00 + ij01 * d01) + (ij10 * d10 + ij11 * d11);
-    const double rq = double(rT);
+    const double wj = double(tb.w[q] * detj);
+    double rq;
+    if constexpr (RQ_SHARED)
+      rq = double(s_rq[q * kBlock + threadIdx.x]);
+    else
+      rq = double(rq_reg[q]);
 
     // advection speed at q
     T ax, ay;
@@ -175,29 +183,26 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
       ay = T(a.adv1);
     }
 
-    // upwind coefficients k+_n and their sum
+    // upwind coefficients k_n = a . invJ^T grad_xi phi_n = dV[0][q][n] A + dV[1][q][n] B
+    const T A = ax * ij00 + ay * ij10;
+    const T B = ax * ij01 + ay * ij11;
     T kp[NDOF];
     T sumkp = T(0);
 #pragma unroll
     for (int n = 0; n < NDOF; ++n)
     {
-      const T gx = ij00 * tb.dV[0][q][n] + ij01 * tb.dV[1][q][n];
-      const T gy = ij10 * tb.dV[0][q][n] + ij11 * tb.dV[1][q][n];
-      const T k  = ax * gx + ay * gy;
-      kp[n]      = k > T(0) ? k : T(0);
-      const T ak = fabs(k);
-      wsmax      = fmax(wsmax, fmax(T(1.e-6), ak));
-      sumkp      = sumkp + kp[n];
+      const T k = tb.dV[0][q][n] * A + tb.dV[1][q][n] * B;
+      kp[n]     = k > T(0) ? k : T(0);
+      kmax      = fmax(kmax, fabs(k));
+      sumkp     = sumkp + kp[n];
     }
-    const double inv = 1.0 / double(sumkp); // FP64 inverse in both precisions
+    // beta_n = K+_n / sum K+ (FP64 inverse in both precisions); w_q detJ beta_n is e K+_n
+    const double e = wj * (1.0 / double(sumkp));
 
-    phi += wj * rq;
+    const double erq = e * rq;
 #pragma unroll
     for (int n = 0; n < NDOF; ++n)
-    {
-      const double beta = double(kp[n]) * inv;
-      lda[n] += wj * (beta * rq);
-    }
+      lda[n] += erq * double(kp[n]);
     if (SCHEME != RDS_PGLDA)
     {
       // sum_{m != n} K+_m (u_n - u_m) = u_n sum_m K+_m - sum_m K+_m u_m (the m = n terms
@@ -209,12 +214,11 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
       const double sk = double(sumkp);
 #pragma unroll
       for (int n = 0; n < NDOF; ++n)
-      {
-        const double s = ud[n] * sk - tku;
-        diss[n] += wj * ((double(kp[n]) * inv) * s);
-      }
+        diss[n] += (e * double(kp[n])) * (ud[n] * sk - tku);
     }
   }
+  // wave speed |K| max_{q,n} max(1e-6, |k_n|)
+  const T wsmax = fmax(T(1.e-6), kmax);
 
   double theta = 1.0;
   if (SCHEME == RDS_PGB)
@@ -236,7 +240,7 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
   a.wsc[a.ws_base + c] = vol * double(wsmax);
 }
 
-template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, bool AFFINE>
+template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO>
 __global__ void __launch_bounds__(kBlock)
     cells_scalar2d(const __grid_constant__ CellArgs a,
                    const __grid_constant__ Tables<T, 2, NDOF, NQ, NFL, NGEO> tb)
@@ -246,7 +250,7 @@ __global__ void __launch_bounds__(kBlock)
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.ncells)
     return;
-  scalar_cell<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, AFFINE>(a, tb, c);
+  scalar_cell<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO>(a, tb, c);
 }
 
 // Batch form: a persistent grid walks the group's active tiles (the problems still iterating
@@ -276,7 +280,7 @@ __global__ void __launch_bounds__(128)
     }
     const int c = a.bt.cbeg[lo] + (t - prefix[lo]) * (int)blockDim.x + (int)threadIdx.x;
     if (c < a.bt.cend[lo])
-      scalar_cell<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, true>(a, tb, c);
+      scalar_cell<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO>(a, tb, c);
   }
 }
 
@@ -286,10 +290,7 @@ cudaError_t launch_one(const HostCellGroup &g, const CellArgs &a, cudaStream_t s
   Tables<T, 2, NDOF, NQ, NFL, NGEO> tb;
   fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
   const int grid = (a.ncells + kBlock - 1) / kBlock;
-  if (g.affine)
-    cells_scalar2d<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, true><<<grid, kBlock, 0, s>>>(a, tb);
-  else
-    cells_scalar2d<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, false><<<grid, kBlock, 0, s>>>(a, tb);
+  cells_scalar2d<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO><<<grid, kBlock, 0, s>>>(a, tb);
   return cudaGetLastError();
 }
 
@@ -322,7 +323,22 @@ cudaError_t launch_batch_one(const HostCellGroup &g, const CellArgs &a, int grid
 {
   Tables<T, 2, NDOF, NQ, NFL, 3> tb;
   fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
-  cells_scalar2d_batch<PHYS, SCHEME, T, NDOF, NQ, NFL, 3><<<grid, tile, 0, s>>>(a, tb);
+  auto k = cells_scalar2d_batch<PHYS, SCHEME, T, NDOF, NQ, NFL, 3>;
+  // a persistent grid only balances if all its CTAs are resident at once: cap it at the
+  // occupancy of this kernel and tile (computed once per tile size)
+  static int per_sm[2] = {0, 0}, nsm = 0;
+  const int ti = tile > 64 ? 1 : 0;
+  if (per_sm[ti] == 0)
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[ti], k, tile, 0);
+    if (per_sm[ti] < 1)
+      per_sm[ti] = 1;
+  }
+  const int cap = per_sm[ti] * nsm;
+  k<<<grid < cap ? grid : cap, tile, 0, s>>>(a, tb);
   return cudaGetLastError();
 }
 
