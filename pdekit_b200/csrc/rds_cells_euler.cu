@@ -10,9 +10,10 @@
 //      r_q = sum_d (invJ dVf F_d)_d                                       -> shared memory;
 //   D  every quadrature point, all lanes together: lane l owns nodes n = l, l + G, ...;
 //      it builds K+_n = R max(Lambda,0) L for grad phi_n (Euler2DCons.hpp:316-536 /
-//      Euler3DCons.hpp:332-560) and its part of sum K+ and sum K+ u; an xor-butterfly over the
-//      group completes the sums (bit-identical in every lane, since a + b == b + a); every lane
-//      factorises sum K+ (FP64 LU with partial pivoting) and solves for
+//      Euler3DCons.hpp:332-560; in the split form of euler_K_split) and its part of sum K+ and
+//      sum K+ u; an xor-butterfly over the group completes the sums (bit-identical in every
+//      lane, since a + b == b + a); every lane solves with sum K+ (2D: closed-form adjugate, as
+//      the reference's 4 x 4 inverse; 3D: FP64 LU with partial pivoting) for
 //      v = (sum K+)^-1 r_q and u_bar = (sum K+)^-1 sum_m K+_m u_m, then accumulates for its own
 //      nodes  lda_n += w_q |J_q| K+_n v  and  diss_n += w_q |J_q| K+_n (u_n - u_bar)
 //      (= sum_{m != n} K+_n (sum K+)^-1 K+_m (u_n - u_m), the reference's N dissipation);
@@ -54,6 +55,8 @@ template <int N>
 __device__ __forceinline__ void lu_solve2(double A[N][N], double b1[N], double b2[N])
 {
 #pragma unroll
+  double rdiag[N]; // 1 / U_kk, reused by the back substitution
+#pragma unroll
   for (int k = 0; k < N; ++k)
   {
     int piv    = k;
@@ -93,6 +96,7 @@ __device__ __forceinline__ void lu_solve2(double A[N][N], double b1[N], double b
         }
     }
     const double inv = 1.0 / A[k][k];
+    rdiag[k]         = inv;
 #pragma unroll
     for (int i = k + 1; i < N; ++i)
     {
@@ -113,8 +117,52 @@ __device__ __forceinline__ void lu_solve2(double A[N][N], double b1[N], double b
       b1[i] -= A[i][j] * b1[j];
       b2[i] -= A[i][j] * b2[j];
     }
-    b1[i] /= A[i][i];
-    b2[i] /= A[i][i];
+    b1[i] *= rdiag[i];
+    b2[i] *= rdiag[i];
+  }
+}
+
+// Solve A x = b for two right-hand sides, 4 x 4: x = adj(A) b / det(A), the adjugate from the
+// 2 x 2 minors of rows (0, 1) and of rows (2, 3) (Laplace expansion by complementary minors).
+// The reference inverts these matrices by a closed-form adjugate too
+// (src/math/unary_ops/matrix_unary_ops/MatrixInverse.hpp:187-290).
+__device__ __forceinline__ void adj_solve4(const double A[4][4], double b1[4], double b2[4])
+{
+  const double s0 = A[0][0] * A[1][1] - A[1][0] * A[0][1];
+  const double s1 = A[0][0] * A[1][2] - A[1][0] * A[0][2];
+  const double s2 = A[0][0] * A[1][3] - A[1][0] * A[0][3];
+  const double s3 = A[0][1] * A[1][2] - A[1][1] * A[0][2];
+  const double s4 = A[0][1] * A[1][3] - A[1][1] * A[0][3];
+  const double s5 = A[0][2] * A[1][3] - A[1][2] * A[0][3];
+  const double c5 = A[2][2] * A[3][3] - A[3][2] * A[2][3];
+  const double c4 = A[2][1] * A[3][3] - A[3][1] * A[2][3];
+  const double c3 = A[2][1] * A[3][2] - A[3][1] * A[2][2];
+  const double c2 = A[2][0] * A[3][3] - A[3][0] * A[2][3];
+  const double c1 = A[2][0] * A[3][2] - A[3][0] * A[2][2];
+  const double c0 = A[2][0] * A[3][1] - A[3][0] * A[2][1];
+  const double det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+  const double id  = 1.0 / det;
+  const double B[4][4] = {
+      {A[1][1] * c5 - A[1][2] * c4 + A[1][3] * c3, -A[0][1] * c5 + A[0][2] * c4 - A[0][3] * c3,
+       A[3][1] * s5 - A[3][2] * s4 + A[3][3] * s3, -A[2][1] * s5 + A[2][2] * s4 - A[2][3] * s3},
+      {-A[1][0] * c5 + A[1][2] * c2 - A[1][3] * c1, A[0][0] * c5 - A[0][2] * c2 + A[0][3] * c1,
+       -A[3][0] * s5 + A[3][2] * s2 - A[3][3] * s1, A[2][0] * s5 - A[2][2] * s2 + A[2][3] * s1},
+      {A[1][0] * c4 - A[1][1] * c2 + A[1][3] * c0, -A[0][0] * c4 + A[0][1] * c2 - A[0][3] * c0,
+       A[3][0] * s4 - A[3][1] * s2 + A[3][3] * s0, -A[2][0] * s4 + A[2][1] * s2 - A[2][3] * s0},
+      {-A[1][0] * c3 + A[1][1] * c1 - A[1][2] * c0, A[0][0] * c3 - A[0][1] * c1 + A[0][2] * c0,
+       -A[3][0] * s3 + A[3][1] * s1 - A[3][2] * s0, A[2][0] * s3 - A[2][1] * s1 + A[2][2] * s0}};
+  double x1[4], x2[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+  {
+    x1[i] = (B[i][0] * b1[0] + B[i][1] * b1[1] + B[i][2] * b1[2] + B[i][3] * b1[3]) * id;
+    x2[i] = (B[i][0] * b2[0] + B[i][1] * b2[1] + B[i][2] * b2[2] + B[i][3] * b2[3]) * id;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+  {
+    b1[i] = x1[i];
+    b2[i] = x2[i];
   }
 }
 
@@ -350,6 +398,8 @@ __global__ void __launch_bounds__(NT)
       uq[e] = suq[q * NEQ + e];
     EulerProps<T, D> p;
     bad |= euler_props<T, D>(uq, gamma, p);
+    EulerAcoustic<T, D> ac;
+    euler_acoustic<T, D>(p, gamma, ac);
 
     double SK[NEQ][NEQ], SKu[NEQ];
 #pragma unroll
@@ -380,11 +430,8 @@ __global__ void __launch_bounds__(NT)
             acc = acc + ij[x][xi] * gref[xi];
           gphys[x] = acc;
         }
-        T K[NEQ][NEQ], lam[NEQ];
-        euler_K<+1, T, D>(p, gphys, gamma, K, lam);
-#pragma unroll
-        for (int e = 0; e < NEQ; ++e)
-          wsmax = fmax(wsmax, fmax(T(1.e-6), fabs(lam[e])));
+        T K[NEQ][NEQ];
+        wsmax = fmax(wsmax, euler_K_split<+1, T, D>(p, ac, gphys, K));
         T *Kn = sfk + (size_t)n * SM::KS;
 #pragma unroll
         for (int i = 0; i < NEQ; ++i)
@@ -418,7 +465,10 @@ __global__ void __launch_bounds__(NT)
       ub[e] = SKu[e];
     }
     phi0 += wj * v[0];
-    lu_solve2<NEQ>(SK, v, ub);
+    if constexpr (NEQ == 4)
+      adj_solve4(SK, v, ub);
+    else
+      lu_solve2<NEQ>(SK, v, ub);
 
 #pragma unroll
     for (int s = 0; s < NPT; ++s)

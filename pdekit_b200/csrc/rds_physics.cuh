@@ -233,4 +233,90 @@ __device__ __forceinline__ void euler_K(const EulerProps<T, D> &p, const T *dir,
     }
 }
 
+// Direction-independent factors of the acoustic eigenvectors at one state: computed once per
+// point and shared by the upwind matrices of all nodes there.
+template <typename T, int D>
+struct EulerAcoustic
+{
+  T inv_a;  // 1 / a
+  T ra;     // rho / (2 a)
+  T kin;    // (gamma - 1) |V|^2 / (2 a^2)
+  T gV[D];  // (gamma - 1) V_d / a
+  T g_rhoa; // (gamma - 1) / (rho a)
+};
+
+template <typename T, int D>
+__device__ __forceinline__ void euler_acoustic(const EulerProps<T, D> &p, T gamma,
+                                               EulerAcoustic<T, D> &c)
+{
+  const T gm1 = gamma - T(1);
+  c.inv_a     = T(1) / p.a;
+  c.ra        = T(0.5) * p.rho * c.inv_a;
+  c.kin       = (T(0.5) * gm1 * p.v2) * (c.inv_a * c.inv_a);
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+    c.gV[d] = gm1 * p.V[d] * c.inv_a;
+  c.g_rhoa = gm1 / (p.rho * p.a);
+}
+
+// K = R op(Lambda) L for direction dir (op = max(0, .) for SIGN > 0, min(0, .) otherwise), in
+// split form. The convective eigenvalue lam_c = |dir| u.n has multiplicity D and the eigenvector
+// pairs satisfy sum_k r_k l_k^T = I, so
+//   K = op(lam_c) I + (op(lam_+) - op(lam_c)) r_+ l_+^T + (op(lam_-) - op(lam_c)) r_- l_-^T
+// where r_+- = rho/(2a) (1, V +- a n, H +- a u.n) and l_+- are the acoustic eigenvector pairs
+// (columns / rows D and D + 1 of R and L in euler_eigen): two rank-one updates instead of the
+// product of three N x N matrices. Returns max_k max(1e-6, |lam_k|).
+template <int SIGN, typename T, int D>
+__device__ __forceinline__ T euler_K_split(const EulerProps<T, D> &p,
+                                           const EulerAcoustic<T, D> &c, const T *dir,
+                                           T K[D + 2][D + 2])
+{
+  constexpr int N = D + 2;
+  T n2            = dir[0] * dir[0] + dir[1] * dir[1];
+  if (D == 3)
+    n2 = n2 + dir[D - 1] * dir[D - 1];
+  const T norm = sqrt(n2);
+  // the reference keeps dir unnormalised below |dir| = 1e-9 (2D) or at |dir| = 0 (3D)
+  const bool keep = (D == 2) ? (norm < T(1.e-9)) : (norm == T(0));
+  const T inv_n   = keep ? T(1) : T(1) / norm;
+  T n[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+    n[d] = dir[d] * inv_n;
+  T um = p.V[0] * n[0] + p.V[1] * n[1];
+  if (D == 3)
+    um = um + p.V[D - 1] * n[D - 1];
+  const T a  = p.a;
+  const T lc = norm * um, lp = norm * (um + a), lm = norm * (um - a);
+  auto op    = [](T x) -> T { return SIGN > 0 ? (x > T(0) ? x : T(0)) : (x < T(0) ? x : T(0)); };
+  const T oc = op(lc);
+  const T ap = (op(lp) - oc) * c.ra, am = (op(lm) - oc) * c.ra;
+  T rp[N], rm[N], lpv[N], lmv[N];
+  rp[0] = ap;
+  rm[0] = am;
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+  {
+    rp[1 + d]  = ap * (p.V[d] + a * n[d]);
+    rm[1 + d]  = am * (p.V[d] - a * n[d]);
+    lpv[1 + d] = p.inv_rho * (n[d] - c.gV[d]);
+    lmv[1 + d] = -p.inv_rho * (n[d] + c.gV[d]);
+  }
+  rp[N - 1]  = ap * (p.H + a * um);
+  rm[N - 1]  = am * (p.H - a * um);
+  lpv[0]     = a * p.inv_rho * (c.kin - um * c.inv_a);
+  lmv[0]     = a * p.inv_rho * (c.kin + um * c.inv_a);
+  lpv[N - 1] = c.g_rhoa;
+  lmv[N - 1] = c.g_rhoa;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j)
+    {
+      const T s = rp[i] * lpv[j] + rm[i] * lmv[j];
+      K[i][j]   = (i == j) ? oc + s : s;
+    }
+  return fmax(fmax(T(1.e-6), fabs(lc)), fmax(fabs(lp), fabs(lm)));
+}
+
 } // namespace rds
