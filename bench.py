@@ -155,23 +155,33 @@ def scalar_flops(physics, scheme, ndof, nq, nfl):
 
 
 def euler_flops(dim, neq, ndof, nq, nfl, ngeo, scheme):
-    """Efficient-form count of one Euler cell (the algorithm the reference runs per cell):
-      geometry    nq (2 D^2 ngeo + c_invJ)                      c_invJ 10 (2D) / 60 (3D)
-      contraction 2 NEQ ndof (nq + nfl) + 2 NEQ D^2 nq nfl       u_q, flux-node states, div F
-      flux nodes  nfl (c_props + c_flux)                         30 + 20 (2D) / 40 + 20 (3D)
-      per point   c_props + ndof (2 D^2 + c_K) + c_inv + (D + 3) NEQ^2 + 2 ndof NEQ^2
-                  (+ ndof (4 NEQ^2 + 2 NEQ) for N / B)           c_K 250 / 450, c_inv 200 / 350
-    Configuration 3: 74,334 (P3 triangle, 16 points) and 181,250 (P3 quadrilateral, 25
-    points); configuration 4: 111,728 (P2 tetrahedron, 14 points, LDA)."""
-    c_invj, c_props, c_flux, c_k, c_inv = (10, 30, 20, 250, 200) if dim == 2 else \
-        (60, 40, 20, 450, 350)
-    f = nq * (2 * dim * dim * ngeo + c_invj)
-    f += 2 * neq * ndof * (nq + nfl) + 2 * neq * dim * dim * nq * nfl
-    f += nfl * (c_props + c_flux)
-    per_q = c_props + ndof * (2 * dim * dim + c_k) + c_inv + (dim + 3) * neq * neq \
-        + 2 * ndof * neq * neq
+    """Count of one Euler cell in the form the kernel evaluates (affine = straight-sided
+    triangle / tetrahedron):
+      geometry    (1 if affine else nq) (2 D^2 ngeo + c_invJ)        c_invJ 10 (2D) / 60 (3D)
+      flux nodes  nfl (2 NEQ ndof + c_props + c_flux                 state, properties, flux
+                       + 2 NEQ D^2 if affine)                        flux contracted with invJ
+      points      nq (2 NEQ ndof                                     u_q
+                      + 2 NEQ D nfl (affine) or 2 NEQ D (D nfl + D)  flux divergence
+                      + c_props + c_ac + c_solve                     state, acoustic factors,
+                                                                     (sum K+)^-1 [r, sum K+ u]
+                      + ndof (2 D^2 + c_K + 5 NEQ^2 + 2 NEQ)         grad phi, K+ (split form),
+                                                                     sum K+, sum K+ u, LDA part
+                      + ndof (2 NEQ^2 + 3 NEQ) for N / B)            N dissipation
+      c_props 20 / 22, c_flux 12 / 24, c_ac 15 / 17, c_K 110 / 150, c_solve 190 (adjugate) /
+      165 (LU) for 2D / 3D.
+    Configuration 3: 50,914 (P3 triangle, 16 points) and 134,675 (P3 quadrilateral, 25
+    points); configuration 4: 59,928 (P2 tetrahedron, 14 points, LDA)."""
+    affine = (dim == 2 and ngeo == 3) or (dim == 3 and ngeo == 4)
+    c_invj, c_props, c_flux, c_ac, c_k, c_solve = (10, 20, 12, 15, 110, 190) if dim == 2 else \
+        (60, 22, 24, 17, 150, 165)
+    f = (1 if affine else nq) * (2 * dim * dim * ngeo + c_invj)
+    f += nfl * (2 * neq * ndof + c_props + c_flux + (2 * neq * dim * dim if affine else 0))
+    per_q = 2 * neq * ndof
+    per_q += 2 * neq * dim * nfl if affine else 2 * neq * dim * (dim * nfl + dim)
+    per_q += c_props + c_ac + c_solve
+    per_q += ndof * (2 * dim * dim + c_k + 5 * neq * neq + 2 * neq)
     if scheme != "lda":
-        per_q += ndof * (4 * neq * neq + 2 * neq)
+        per_q += ndof * (2 * neq * neq + 3 * neq)
     return f + nq * per_q
 
 

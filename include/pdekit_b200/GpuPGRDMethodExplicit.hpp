@@ -205,9 +205,16 @@ class GpuRDMBC : public RDMBCBase<MeshConfig, Physics, Physics::DIM - 1>
   {
     m_params[param_name] = value;
   }
+  /* WeakFarfield: the reference state in conservative variables */
+  void set_reference_state(const math::DenseDVec<Real> &state) override
+  {
+    m_state.assign(state.size(), 0.0);
+    for (Uint i = 0; i < state.size(); ++i)
+      m_state[i] = state[i];
+  }
   RDMBCType bc_type() const override
   {
-    return BC_TYPE_WEAK;
+    return m_type == "StrongDirichlet" ? BC_TYPE_STRONG : BC_TYPE_WEAK;
   }
   void apply(RDTimeUpdate &) override
   {
@@ -226,6 +233,10 @@ class GpuRDMBC : public RDMBCBase<MeshConfig, Physics, Physics::DIM - 1>
   {
     return m_expr;
   }
+  const std::vector<Real> &reference_state() const
+  {
+    return m_state;
+  }
   Real parameter(const std::string &n) const
   {
     const auto it = m_params.find(n);
@@ -238,6 +249,7 @@ class GpuRDMBC : public RDMBCBase<MeshConfig, Physics, Physics::DIM - 1>
   private:
   std::string m_type, m_boundary;
   expr_type m_expr = nullptr;
+  std::vector<Real> m_state;
   std::map<std::string, Real> m_params;
 };
 
@@ -290,7 +302,8 @@ class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>
                                                        const std::string &boundary_name) override
   {
     if (bc_type_name != "WeakDirichlet" && bc_type_name != "WeakWall" &&
-        bc_type_name != "WeakSubInlet" && bc_type_name != "WeakSubOutlet")
+        bc_type_name != "WeakSubInlet" && bc_type_name != "WeakSubOutlet" &&
+        bc_type_name != "WeakFarfield" && bc_type_name != "StrongDirichlet")
       throw std::runtime_error("GpuPGRDMethodExplicit: boundary condition '" + bc_type_name +
                                "' not supported on the GPU");
     auto bc             = std::make_shared<bc_type>(bc_type_name, condition_name, boundary_name);
@@ -591,6 +604,58 @@ class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>
             t.gq[(size_t(f) * nfq + q) * NEQ + e] = bc.expression()(xv, zero.const_value(0), e);
         }
       b.kind = RDS_BC_WEAK_DIRICHLET;
+    }
+    else if (bc.type() == "WeakFarfield")
+    {
+      if (bc.reference_state().size() != NEQ)
+        throw std::runtime_error("boundary condition '" + bc.name() +
+                                 "': set_reference_state with " + std::to_string(NEQ) +
+                                 " values first");
+      t.gq.assign(bc.reference_state().begin(), bc.reference_state().end());
+      b.kind = RDS_BC_WEAK_FARFIELD;
+    }
+    else if (bc.type() == "StrongDirichlet")
+    {
+      if (!bc.expression())
+        throw std::runtime_error("boundary condition '" + bc.name() + "': no expression set");
+      // values at the facet dofs (StrongDirichletBC::compute_Dirichlet_data): the expression
+      // at the dof's coordinates, with the current state as its state argument. The reference
+      // takes the coordinates from the facet geometry's nodes; for the dofs past the geometry
+      // nodes of P2 / P3 facets it reads beyond them, here they are the dof coordinates (the
+      // facet geometry at the dof's reference point).
+      const vec_fn::ptr u = this->vec_function(SolverVecFn::solution);
+      if (!u)
+        throw std::runtime_error("GpuPGRDMethodExplicit: solution function not set");
+      for (const int32_t v : fsol)
+        if (Uint(v) >= u->nb_entries())
+          throw std::runtime_error("GpuPGRDMethodExplicit: solution function too short");
+      mesh::StdRegion fsol_region;
+      Uint f0 = 0;
+      t.gq.assign(size_t(nf) * nfdof * NEQ, 0.0);
+      for (Uint r = 0; r < sranges.size(); ++r)
+        for (auto it = sranges[r].begin(); it != sranges[r].end(); ++it, ++f0)
+        {
+          const mesh::MeshEntity se = it->mesh_entity();
+          fsol_region.change_type(se.pt_set_id());
+          const math::DenseDMat<Real> &rc = fsol_region.get().coordinates();
+          math::DenseDVec<Real> ones(rc.rows());
+          ones.fill(1.0);
+          interpolation::FEValues fe_at_dofs;
+          fill_fe(fe_at_dofs, fshape, pgf, rc, ones);
+          const math::DenseDMat<Real> &Vd = fe_at_dofs.Vandermonde();
+          for (Uint n = 0; n < nfdof; ++n)
+          {
+            Real x[3] = {0.0, 0.0, 0.0};
+            for (Uint g = 0; g < nfgeo; ++g)
+              for (Uint d = 0; d < D; ++d)
+                x[d] += Vd(n, g) * m_coords[size_t(fgeo[f0 * nfgeo + g]) * D + d];
+            const math::DenseConstVecView<Real> xv(x, D);
+            for (Uint e = 0; e < NEQ; ++e)
+              t.gq[(size_t(f0) * nfdof + n) * NEQ + e] =
+                  bc.expression()(xv, u->const_value(fsol[f0 * nfdof + n]), e);
+          }
+        }
+      b.kind = RDS_BC_STRONG_DIRICHLET;
     }
     else if (bc.type() == "WeakWall")
       b.kind = RDS_BC_WEAK_WALL;

@@ -92,7 +92,16 @@ typedef enum
   RDS_BC_WEAK_DIRICHLET  = 0, /* bc/WeakDirichletBC.hpp: gq = boundary state */
   RDS_BC_WEAK_WALL       = 1, /* bc/WeakWall.hpp (Euler) */
   RDS_BC_WEAK_SUB_INLET  = 2, /* bc/WeakSubInlet.hpp (Euler): params = total temperature, pressure */
-  RDS_BC_WEAK_SUB_OUTLET = 3  /* bc/WeakSubOutlet.hpp (Euler): params[0] = outlet pressure */
+  RDS_BC_WEAK_SUB_OUTLET = 3, /* bc/WeakSubOutlet.hpp (Euler): params[0] = outlet pressure */
+  RDS_BC_WEAK_FARFIELD   = 4, /* bc/WeakFarfield.hpp:125-240 (Euler): gq = [neq] reference state
+                               * (conservative variables, set_reference_state) */
+  RDS_BC_STRONG_DIRICHLET = 5 /* bc/StrongDirichletBC.hpp:202-233: gq = [nfacets][nfdof][neq]
+                               * values the facet dofs take, facet by facet (a dof on two facets
+                               * keeps the later value); only sol_conn / nfacets / nfdof are
+                               * read besides. Applied in condition order after the cells (the
+                               * conditions added after it see the new state); the update then
+                               * moves these dofs by -dt res like every other dof. Not in
+                               * batched contexts. */
 } rds_bc_kind;
 
 typedef struct
@@ -154,7 +163,9 @@ typedef struct
   const double *fw;        /* [nfq] */
   const double *fV;        /* [nfq][nfdof] */
   const double *fdVgeo;    /* [dim-1][nfq][nfgeo] */
-  const double *gq;        /* [nfacets][nfq][neq] (RDS_BC_WEAK_DIRICHLET; NULL otherwise) */
+  const double *gq;        /* RDS_BC_WEAK_DIRICHLET: [nfacets][nfq][neq]; RDS_BC_WEAK_FARFIELD:
+                            [neq]; RDS_BC_STRONG_DIRICHLET: [nfacets][nfdof][neq]; NULL
+                            otherwise */
   int order;               /* polynomial order of the facet basis (WeakWall relaxation) */
   double params[4];        /* kind-specific parameters (set_parameter of the reference) */
 } rds_bc_group;

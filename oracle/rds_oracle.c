@@ -706,10 +706,10 @@ static void euler_flux_normal(const rdso_model *m, const props_t *p, const doubl
 }
 
 /* Weak boundary-facet residuals: WeakDirichlet (WeakDirichletBC.hpp:159-265), WeakWall,
- * WeakSubInlet, WeakSubOutlet, plus the rescaling to the facet total (WeakBC.hpp:786-832) and
+ * WeakSubInlet, WeakSubOutlet, WeakFarfield, plus the rescaling to the facet total (WeakBC.hpp:786-832) and
  * the nodal accumulation (WeakBC.hpp:315-352). */
 static int apply_weak_bc(const rdso_model *m, const rdso_bc *b, const double *geo_coords,
-                                const double *vol, const double *u, double *res, double *ws)
+                         const double *vol, const double *u, double *res, double *ws)
 {
   const int D = m->dim, NEQ = m->neq;
   int bad = 0;
@@ -787,7 +787,9 @@ static int apply_weak_bc(const rdso_model *m, const rdso_bc *b, const double *ge
       double eig[NEQ_MAX], Km[NEQ_MAX][NEQ_MAX];
       build_K(m, &p, nrm, -1, eig, Km);
 
-      double eig_max = 1.e-9, ghost[NEQ_MAX], gflux[NEQ_MAX];
+      /* lambda floor 1e-9 (WeakDirichletBC.hpp), 1e-8 for WeakFarfield (WeakFarfield.hpp:149) */
+      double eig_max = (b->kind == RDSO_BC_WEAK_FARFIELD) ? 1.e-8 : 1.e-9;
+      double ghost[NEQ_MAX], gflux[NEQ_MAX];
       for (int e = 0; e < NEQ; ++e)
       {
         const double ae = fabs(eig[e]);
@@ -829,6 +831,12 @@ static int apply_weak_bc(const rdso_model *m, const rdso_bc *b, const double *ge
           const double *gq = b->gq + ((size_t)f * b->nfq + q) * NEQ;
           for (int e = 0; e < NEQ; ++e)
             ghost[e] = gq[e];
+        }
+        else if (b->kind == RDSO_BC_WEAK_FARFIELD)
+        {
+          /* WeakFarfield.hpp:125-240 (active branch): the reference state, K-(n) (u_ref - u) */
+          for (int e = 0; e < NEQ; ++e)
+            ghost[e] = b->gq[e];
         }
         else if (b->kind == RDSO_BC_WEAK_SUB_INLET)
         {
@@ -901,9 +909,23 @@ static int apply_weak_bc(const rdso_model *m, const rdso_bc *b, const double *ge
   return bad;
 }
 
+/* StrongDirichletBC::apply (StrongDirichletBC.hpp:202-233): the facet dofs take the condition's
+ * values, facet by facet in order (a dof shared by two facets keeps the later value). */
+static void apply_strong_bc(const rdso_model *m, const rdso_bc *b, double *u)
+{
+  const int NEQ = m->neq;
+  for (int f = 0; f < b->nfacets; ++f)
+    for (int n = 0; n < b->nfdof; ++n)
+    {
+      const int v = b->sol_conn[(size_t)f * b->nfdof + n];
+      for (int e = 0; e < NEQ; ++e)
+        u[(size_t)v * NEQ + e] = b->gq[((size_t)f * b->nfdof + n) * NEQ + e];
+    }
+}
+
 int rdso_assemble(const rdso_model *m, const rdso_cells *groups, int ngroups, const rdso_bc *bcs,
                   int nbcs, int nnodes, const double *geo_coords, const double *vol,
-                  const double *u, double cfl, double *res, double *ws, double *dt)
+                  double *u, double cfl, double *res, double *ws, double *dt)
 {
   const int D = m->dim, NEQ = m->neq;
   int bad = 0;
@@ -939,9 +961,14 @@ int rdso_assemble(const rdso_model *m, const rdso_cells *groups, int ngroups, co
     }
   }
 
+  /* conditions in their (name) order: weak ones add facet residuals, strong ones overwrite
+   * the state that the later conditions and the update see */
   for (int ib = 0; ib < nbcs; ++ib)
   {
-    bad += apply_weak_bc(m, &bcs[ib], geo_coords, vol, u, res, ws);
+    if (bcs[ib].kind == RDSO_BC_STRONG_DIRICHLET)
+      apply_strong_bc(m, &bcs[ib], u);
+    else
+      bad += apply_weak_bc(m, &bcs[ib], geo_coords, vol, u, res, ws);
   }
 
   /* RDTimeUpdate::compute_local_time_step (RDTimeUpdate.cpp:41-53) */

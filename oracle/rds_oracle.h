@@ -49,7 +49,9 @@ enum
   RDSO_BC_WEAK_DIRICHLET  = 0, /* bc/WeakDirichletBC.hpp */
   RDSO_BC_WEAK_WALL       = 1, /* bc/WeakWall.hpp */
   RDSO_BC_WEAK_SUB_INLET  = 2, /* bc/WeakSubInlet.hpp, params: total temperature, pressure */
-  RDSO_BC_WEAK_SUB_OUTLET = 3  /* bc/WeakSubOutlet.hpp, params: outlet pressure */
+  RDSO_BC_WEAK_SUB_OUTLET = 3, /* bc/WeakSubOutlet.hpp, params: outlet pressure */
+  RDSO_BC_WEAK_FARFIELD   = 4, /* bc/WeakFarfield.hpp, gq: [neq] reference state */
+  RDSO_BC_STRONG_DIRICHLET = 5 /* bc/StrongDirichletBC.hpp, gq: [nfacets][nfdof][neq] values */
 };
 
 typedef struct
@@ -88,7 +90,9 @@ typedef struct
   const double *fw;     /* [nfq] */
   const double *fV;     /* [nfq][nfdof] */
   const double *fdVgeo; /* [dim-1][nfq][nfgeo] */
-  const double *gq;     /* [nfacets][nfq][neq] boundary state at facet quadrature points */
+  const double *gq;     /* WeakDirichlet: [nfacets][nfq][neq] boundary state at the facet
+                         * quadrature points; WeakFarfield: [neq]; StrongDirichlet:
+                         * [nfacets][nfdof][neq] values at the facet dofs */
   int order;            /* polynomial order of the facet's solution basis */
   double params[4];     /* kind-specific parameters */
 } rdso_bc;
@@ -97,11 +101,12 @@ typedef struct
 void rdso_dual_volume(const rdso_model *m, const rdso_cells *groups, int ngroups, int nnodes,
                       const double *geo_coords, double *vol);
 
-/* One assemble_lhs_and_rhs(CFL): res, ws and dt from u. Returns the number of
- * non-positive-pressure evaluations seen (Euler), 0 otherwise. */
+/* One assemble_lhs_and_rhs(CFL): res, ws and dt from u; StrongDirichlet conditions overwrite
+ * their dofs of u in place. Returns the number of non-positive-pressure evaluations seen
+ * (Euler), 0 otherwise. */
 int rdso_assemble(const rdso_model *m, const rdso_cells *groups, int ngroups, const rdso_bc *bcs,
                   int nbcs, int nnodes, const double *geo_coords, const double *vol,
-                  const double *u, double cfl, double *res, double *ws, double *dt);
+                  double *u, double cfl, double *res, double *ws, double *dt);
 
 /* solve(): u -= dt * res */
 void rdso_update(int nnodes, int neq, const double *dt, const double *res, double *u);

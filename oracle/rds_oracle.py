@@ -19,7 +19,8 @@ HARNESS_PATH = os.path.join(_HERE, "_ref", "rds_ref_harness")
 
 PHYSICS = {"advconst": 0, "burgers": 1, "euler2d": 2, "euler3d": 3}
 SCHEME = {"lda": 0, "n": 1, "b": 2}
-BC_KIND = {"WeakDirichlet": 0, "WeakWall": 1, "WeakSubInlet": 2, "WeakSubOutlet": 3}
+BC_KIND = {"WeakDirichlet": 0, "WeakWall": 1, "WeakSubInlet": 2, "WeakSubOutlet": 3,
+           "WeakFarfield": 4, "StrongDirichlet": 5}
 
 
 class _Model(C.Structure):
@@ -119,10 +120,8 @@ class Oracle:
         lib().rdso_dual_volume(C.byref(self.model), self.groups, len(prob.groups), prob.nnodes,
                                _p(self.coords), _p(self.vol))
 
-    def assemble(self, u, cfl):
-        """Returns (res [n,neq], ws [n], dt [n], nbad)."""
+    def _assemble_inplace(self, u, cfl):
         prob = self.prob
-        u = np.ascontiguousarray(u, dtype=np.float64).reshape(prob.nnodes, prob.neq)
         res = np.zeros_like(u)
         ws = np.zeros(prob.nnodes)
         dt = np.zeros(prob.nnodes)
@@ -131,13 +130,22 @@ class Oracle:
                                   _p(u), float(cfl), _p(res), _p(ws), _p(dt))
         return res, ws, dt, bad
 
+    def assemble(self, u, cfl):
+        """Returns (res [n,neq], ws [n], dt [n], nbad); `u` is not modified (the state after
+        the strong conditions is `self.last_state`)."""
+        prob = self.prob
+        u = np.array(u, dtype=np.float64).reshape(prob.nnodes, prob.neq)
+        out = self._assemble_inplace(u, cfl)
+        self.last_state = u
+        return out
+
     def iterate(self, u, cfl, iters):
         """iters x (assemble + solve). Returns (u, norms [iters, neq])."""
         prob = self.prob
         u = np.array(u, dtype=np.float64).reshape(prob.nnodes, prob.neq)
         norms = np.zeros((iters, prob.neq))
         for it in range(iters):
-            res, ws, dt, _ = self.assemble(u, cfl)
+            res, ws, dt, _ = self._assemble_inplace(u, cfl)
             nrm = np.zeros(prob.neq)
             lib().rdso_residual_norm(prob.nnodes, prob.neq, _p(res), _p(dt), _p(nrm))
             norms[it] = nrm

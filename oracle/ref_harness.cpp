@@ -173,7 +173,20 @@ int run(const Args &a)
   for (const BCDesc &b : bcs)
   {
     auto bc = solver->add_boundary_condition(b.type, b.name, b.boundary);
-    if (b.expr.find('=') != std::string::npos)
+    if (b.expr.rfind("state=", 0) == 0)
+    {
+      // "state=v0|v1|..." : the reference state of WeakFarfield (set_reference_state)
+      std::vector<Real> vals;
+      std::stringstream vs(b.expr.substr(6));
+      std::string v;
+      while (std::getline(vs, v, '|'))
+        vals.push_back(std::atof(v.c_str()));
+      math::DenseDVec<Real> st(vals.size());
+      for (Uint i = 0; i < vals.size(); ++i)
+        st[i] = vals[i];
+      bc->set_reference_state(st);
+    }
+    else if (b.expr.find('=') != std::string::npos)
     {
       // parameters "name=value;name=value" (WeakSubInlet / WeakSubOutlet)
       std::stringstream ps(b.expr);
@@ -425,6 +438,9 @@ int run(const Args &a)
   // first iteration: residual, wave speed, dt, dual volume at u0
   solver->assemble_lhs_and_rhs(a.cfl);
   out.put("res1", grab(*res), {nsol, NEQ});
+  // the state the update starts from: StrongDirichlet conditions overwrite their facet dofs
+  // during assemble (bc/StrongDirichletBC.hpp:202-233)
+  out.put("ua1", grab(*u), {nsol, NEQ});
   out.put("ws1", grab_scalar(solver->time_update().nodal_wave_speed()), {nsol});
   out.put("dt1", grab_scalar(*solver->scal_function(SolverScalFn::time_step)), {nsol});
   out.put("dual_volume", grab_scalar(solver->time_update().nodal_dual_volume()), {nsol});

@@ -265,6 +265,11 @@ BCArgs bc_args(rds_ctx *ctx, const HostBC &b, const int *stop)
     a.params[k] = b.desc.params[k];
   a.status     = ctx->d_status;
   a.stop       = stop;
+  if (b.desc.kind == RDS_BC_STRONG_DIRICHLET)
+  {
+    a.nfacets  = b.nstrong;
+    a.u_strong = ctx->d_u;
+  }
   return a;
 }
 
@@ -298,18 +303,29 @@ GatherArgs gather_args(rds_ctx *ctx, double cfl, const int *stop)
 rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
 {
   const rds_desc &d = ctx->desc;
-  const bool fork   = !ctx->bcs.empty();
+  // A strong Dirichlet condition writes the state that the cells read and that the conditions
+  // after it read: then the conditions run after the cells, in order, on the main stream.
+  bool strong = false;
+  for (const HostBC &b : ctx->bcs)
+    strong |= b.desc.kind == RDS_BC_STRONG_DIRICHLET;
+  const bool fork = !ctx->bcs.empty() && !strong;
+  auto launch_bcs = [&](cudaStream_t s) -> rds_status {
+    for (const HostBC &b : ctx->bcs)
+    {
+      const BCArgs a = bc_args(ctx, b, stop);
+      rds_status st  = launch_on(ctx, s, [&](const char **name) {
+        return launch_bc(b, a, b.physics, d.dim, d.neq, s, name);
+      });
+      if (st != RDS_OK)
+        return st;
+    }
+    return RDS_OK;
+  };
   if (fork)
   {
     RDS_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
     RDS_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
-  }
-  for (const HostBC &b : ctx->bcs)
-  {
-    const BCArgs a = bc_args(ctx, b, stop);
-    rds_status st  = launch_on(ctx, ctx->side, [&](const char **name) {
-      return launch_bc(b, a, b.physics, d.dim, d.neq, ctx->side, name);
-    });
+    const rds_status st = launch_bcs(ctx->side);
     if (st != RDS_OK)
       return st;
   }
@@ -338,6 +354,8 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
     RDS_CUDA(cudaEventRecord(ctx->ev_join, ctx->side));
     RDS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
   }
+  else if (!ctx->bcs.empty())
+    return launch_bcs(ctx->stream);
   return RDS_OK;
 }
 
@@ -522,32 +540,63 @@ rds_status rds_add_bc(rds_ctx *ctx, const rds_bc_group *b)
     return fail(ctx, RDS_ERR_INVALID, "rds_add_bc after rds_finalize");
   const int D = ctx->desc.dim, NEQ = ctx->desc.neq;
   const bool dirichlet = b->kind == RDS_BC_WEAK_DIRICHLET;
-  if (b->kind < RDS_BC_WEAK_DIRICHLET || b->kind > RDS_BC_WEAK_SUB_OUTLET ||
-      (!dirichlet && NEQ == 1) || b->nfacets <= 0 || b->nfdof <= 0 || b->nfdof > 16 ||
-      b->nfgeo <= 0 || b->nfgeo > 16 || b->nfq <= 0 || b->nfq > 32 || !b->sol_conn ||
-      !b->geo_conn || !b->fw || !b->fV || !b->fdVgeo || (dirichlet && !b->gq))
+  const bool farfield  = b->kind == RDS_BC_WEAK_FARFIELD;
+  const bool strong    = b->kind == RDS_BC_STRONG_DIRICHLET;
+  if (b->kind < RDS_BC_WEAK_DIRICHLET || b->kind > RDS_BC_STRONG_DIRICHLET || b->nfacets <= 0 ||
+      b->nfdof <= 0 || b->nfdof > 16 || !b->sol_conn || ((dirichlet || farfield || strong) && !b->gq))
     return fail(ctx, RDS_ERR_INVALID, "invalid boundary group");
+  if (!strong && (b->nfgeo <= 0 || b->nfgeo > 16 || b->nfq <= 0 || b->nfq > 32 || !b->geo_conn ||
+                  !b->fw || !b->fV || !b->fdVgeo))
+    return fail(ctx, RDS_ERR_INVALID, "invalid boundary group");
+  if (NEQ == 1 && !(dirichlet || strong))
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "this boundary condition needs Euler physics");
   for (size_t i = 0; i < (size_t)b->nfacets * b->nfdof; ++i)
     if (b->sol_conn[i] < 0 || b->sol_conn[i] >= ctx->desc.nnodes)
       return fail(ctx, RDS_ERR_INVALID, "boundary solution connectivity out of range");
-  for (size_t i = 0; i < (size_t)b->nfacets * b->nfgeo; ++i)
-    if (b->geo_conn[i] < 0 || b->geo_conn[i] >= ctx->desc.ngeo_nodes)
-      return fail(ctx, RDS_ERR_INVALID, "boundary geometry connectivity out of range");
+  if (!strong)
+    for (size_t i = 0; i < (size_t)b->nfacets * b->nfgeo; ++i)
+      if (b->geo_conn[i] < 0 || b->geo_conn[i] >= ctx->desc.ngeo_nodes)
+        return fail(ctx, RDS_ERR_INVALID, "boundary geometry connectivity out of range");
   HostBC h;
   h.desc    = *b;
   h.physics = ctx->desc.physics;
-  h.fw.assign(b->fw, b->fw + b->nfq);
-  h.fV.assign(b->fV, b->fV + (size_t)b->nfq * b->nfdof);
-  h.fdVgeo.assign(b->fdVgeo, b->fdVgeo + (size_t)(D - 1) * b->nfq * b->nfgeo);
-  const std::vector<int32_t> sc = transpose_i32(b->sol_conn, b->nfacets, b->nfdof);
-  const std::vector<int32_t> gc = transpose_i32(b->geo_conn, b->nfacets, b->nfgeo);
-  std::vector<double> gq(dirichlet ? (size_t)NEQ * b->nfq * b->nfacets : 1, 0.0);
-  if (dirichlet)
-    for (int f = 0; f < b->nfacets; ++f)
-      for (int q = 0; q < b->nfq; ++q)
-        for (int e = 0; e < NEQ; ++e)
-          gq[((size_t)e * b->nfq + q) * b->nfacets + f] =
-              b->gq[((size_t)f * b->nfq + q) * NEQ + e];
+  std::vector<int32_t> sc, gc(1, 0);
+  std::vector<double> gq(1, 0.0);
+  if (strong)
+  {
+    // the value each dof ends with (the last facet that names it) for the distinct dofs in
+    // ascending order, so that the kernel writes every dof once
+    std::vector<long long> last(ctx->desc.nnodes, -1);
+    for (size_t i = 0; i < (size_t)b->nfacets * b->nfdof; ++i)
+      last[b->sol_conn[i]] = (long long)i;
+    for (int v = 0; v < ctx->desc.nnodes; ++v)
+      if (last[v] >= 0)
+        sc.push_back(v);
+    h.nstrong = (int)sc.size();
+    gq.assign((size_t)NEQ * sc.size(), 0.0);
+    for (size_t k = 0; k < sc.size(); ++k)
+      for (int e = 0; e < NEQ; ++e)
+        gq[(size_t)e * sc.size() + k] = b->gq[(size_t)last[sc[k]] * NEQ + e];
+  }
+  else
+  {
+    h.fw.assign(b->fw, b->fw + b->nfq);
+    h.fV.assign(b->fV, b->fV + (size_t)b->nfq * b->nfdof);
+    h.fdVgeo.assign(b->fdVgeo, b->fdVgeo + (size_t)(D - 1) * b->nfq * b->nfgeo);
+    sc = transpose_i32(b->sol_conn, b->nfacets, b->nfdof);
+    gc = transpose_i32(b->geo_conn, b->nfacets, b->nfgeo);
+    if (dirichlet)
+    {
+      gq.assign((size_t)NEQ * b->nfq * b->nfacets, 0.0);
+      for (int f = 0; f < b->nfacets; ++f)
+        for (int q = 0; q < b->nfq; ++q)
+          for (int e = 0; e < NEQ; ++e)
+            gq[((size_t)e * b->nfq + q) * b->nfacets + f] =
+                b->gq[((size_t)f * b->nfq + q) * NEQ + e];
+    }
+    else if (farfield)
+      gq.assign(b->gq, b->gq + NEQ);
+  }
   rds_status st;
   if ((st = dalloc(ctx, &h.d_sol_conn, sc.size())) != RDS_OK ||
       (st = dalloc(ctx, &h.d_geo_conn, gc.size())) != RDS_OK ||
@@ -662,6 +711,8 @@ rds_status rds_finalize(rds_ctx *ctx)
   }
   for (HostBC &b : ctx->bcs)
   {
+    if (b.desc.kind == RDS_BC_STRONG_DIRICHLET)
+      continue; // writes the state, no residual contributions
     b.slot_base = S;
     b.ws_base   = W;
     S += (long long)b.desc.nfdof * b.desc.nfacets;
@@ -689,6 +740,8 @@ rds_status rds_finalize(rds_ctx *ctx)
   for (size_t ib = 0; ib < ctx->bcs.size(); ++ib)
   {
     const HostBC &b = ctx->bcs[ib];
+    if (b.desc.kind == RDS_BC_STRONG_DIRICHLET)
+      continue;
     bconn[ib].resize((size_t)b.desc.nfacets * b.desc.nfdof);
     RDS_CUDA(cudaMemcpy(bconn[ib].data(), b.d_sol_conn, bconn[ib].size() * 4,
                         cudaMemcpyDeviceToHost));
@@ -717,6 +770,8 @@ rds_status rds_finalize(rds_ctx *ctx)
   for (size_t ib = 0; ib < ctx->bcs.size(); ++ib)
   {
     const HostBC &b = ctx->bcs[ib];
+    if (b.desc.kind == RDS_BC_STRONG_DIRICHLET)
+      continue;
     const int nf = b.desc.nfacets, nd = b.desc.nfdof;
     for (int f = 0; f < nf; ++f)
       for (int n = 0; n < nd; ++n)
@@ -1331,6 +1386,8 @@ rds_status rds_add_batch_bc(rds_ctx *ctx, const rds_bc_group *b, int physics)
     return fail(ctx, RDS_ERR_INVALID, "rds_add_batch_bc: rds_set_problems first");
   if (physics != RDS_ADVECTION_CONST && physics != RDS_BURGERS2D)
     return fail(ctx, RDS_ERR_UNSUPPORTED, "batched problems: scalar 2D physics only");
+  if (b && b->kind == RDS_BC_STRONG_DIRICHLET)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "batched problems: weak boundary conditions only");
   const rds_status st = rds_add_bc(ctx, b);
   if (st == RDS_OK)
     ctx->bcs.back().physics = physics;

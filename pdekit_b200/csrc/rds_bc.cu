@@ -12,6 +12,10 @@
 //     temperature and pressure at the local Mach number (gas constant 287.046 as there).
 //   WeakSubOutlet (bc/WeakSubOutlet.hpp:105-190): K-(n) (u_out - u_q), u_out = u_q with the
 //     energy of the outlet pressure.
+//   WeakFarfield (bc/WeakFarfield.hpp:125-240, the active branch): K-(n) (u_ref - u_q) with the
+//     reference state u_ref, lambda floor 1e-8.
+// StrongDirichletBC::apply (bc/StrongDirichletBC.hpp:202-233) has its own kernel: the listed
+// dofs take their values (one thread per distinct dof, the value of the last facet naming it).
 // Facet normals are (dy/dxi, -dx/dxi)/|.| in 2D and the normalised cross product of the two
 // tangents in 3D, with |J| the length / area factor (src/interpolation/GeometryMetric.hpp:560-660).
 
@@ -130,7 +134,7 @@ __global__ void __launch_bounds__(kBlock)
       uq[e] = s;
     }
 
-    double eig_max = 1.e-9;
+    double eig_max = (KIND == RDS_BC_WEAK_FARFIELD) ? 1.e-8 : 1.e-9;
     double gflux[NEQ];
     if constexpr (NEQ == 1)
     {
@@ -206,6 +210,12 @@ __global__ void __launch_bounds__(kBlock)
           for (int d = 0; d < D; ++d)
             rho2u2 += uq[d + 1] * uq[d + 1];
           ghost[NEQ - 1] = a.params[0] / gm1 + 0.5 * rho2u2 / uq[0];
+        }
+        else if constexpr (KIND == RDS_BC_WEAK_FARFIELD)
+        {
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e)
+            ghost[e] = a.gq[e];
         }
         else
         {
@@ -336,6 +346,10 @@ cudaError_t dispatch_kind(const HostBC &b, const BCArgs &a, cudaStream_t s, bool
     if constexpr (NEQ > 1)
       return dispatch_facets<RDS_BC_WEAK_SUB_OUTLET, PHYS, D, NEQ>(b, a, s, ok);
     break;
+  case RDS_BC_WEAK_FARFIELD:
+    if constexpr (NEQ > 1)
+      return dispatch_facets<RDS_BC_WEAK_FARFIELD, PHYS, D, NEQ>(b, a, s, ok);
+    break;
   default:
     break;
   }
@@ -352,9 +366,28 @@ const char *bc_name(int kind)
     return "bc_weak_sub_inlet";
   case RDS_BC_WEAK_SUB_OUTLET:
     return "bc_weak_sub_outlet";
+  case RDS_BC_WEAK_FARFIELD:
+    return "bc_weak_farfield";
+  case RDS_BC_STRONG_DIRICHLET:
+    return "bc_strong_dirichlet";
   default:
     return "bc_weak_dirichlet";
   }
+}
+
+// Strong Dirichlet: ndofs distinct dofs, their values SoA [neq][ndofs].
+__global__ void __launch_bounds__(kBlock)
+    bc_strong(int ndofs, int neq, int nnodes, const int32_t *__restrict__ dofs,
+              const double *__restrict__ vals, double *__restrict__ u, const int *stop)
+{
+  if (*stop)
+    return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ndofs)
+    return;
+  const int v = dofs[i];
+  for (int e = 0; e < neq; ++e)
+    u[(size_t)e * nnodes + v] = vals[(size_t)e * ndofs + i];
 }
 
 } // namespace
@@ -365,6 +398,13 @@ cudaError_t launch_bc(const HostBC &b, const BCArgs &a, int physics, int dim, in
   bool ok         = false;
   cudaError_t err = cudaSuccess;
   *name           = bc_name(b.desc.kind);
+  if (b.desc.kind == RDS_BC_STRONG_DIRICHLET)
+  {
+    if (a.nfacets > 0)
+      bc_strong<<<(a.nfacets + kBlock - 1) / kBlock, kBlock, 0, s>>>(
+          a.nfacets, neq, a.nnodes, a.sol_conn, a.gq, a.u_strong, a.stop);
+    return cudaGetLastError();
+  }
   if (physics == RDS_ADVECTION_CONST && dim == 2 && neq == 1)
     err = dispatch_kind<RDS_ADVECTION_CONST, 2, 1>(b, a, s, &ok);
   else if (physics == RDS_BURGERS2D && dim == 2 && neq == 1)

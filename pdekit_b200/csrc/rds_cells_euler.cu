@@ -283,7 +283,15 @@ __global__ void __launch_bounds__(NT)
   const T gamma = T(a.gamma);
   bool bad      = false;
 
-  // ---- B: flux at the flux nodes
+  // affine cells: one Jacobian for all points
+  T ijc[D][D];
+  T detc = T(0);
+  if (AFFINE)
+    detc = jacobian_at(tb, 0, X, ijc);
+
+  // ---- B: flux at the flux nodes; affine cells store it contracted with invJ,
+  // G[f][e][xi] = sum_x invJ[x][xi] F[f][e][x], so that C needs D instead of D^2 products per
+  // flux node and point
   for (int f = lane; f < NFL; f += G)
   {
     T s[NEQ];
@@ -304,29 +312,25 @@ __global__ void __launch_bounds__(NT)
     for (int e = 0; e < NEQ; ++e)
 #pragma unroll
       for (int d = 0; d < D; ++d)
-        sfk[(f * NEQ + e) * D + d] = F[e][d];
+      {
+        T v = F[e][d];
+        if (AFFINE)
+        {
+          v = ijc[0][d] * F[e][0];
+#pragma unroll
+          for (int x = 1; x < D; ++x)
+            v = v + ijc[x][d] * F[e][x];
+        }
+        sfk[(f * NEQ + e) * D + d] = v;
+      }
   }
   __syncwarp();
-
-  // affine cells: one Jacobian for all points
-  T ijc[D][D];
-  T detc = T(0);
-  if (AFFINE)
-    detc = jacobian_at(tb, 0, X, ijc);
 
   // ---- C: u_q and flux divergence r_q
   for (int q = lane; q < NQ; q += G)
   {
     T ij[D][D];
-    if (AFFINE)
-    {
-#pragma unroll
-      for (int i = 0; i < D; ++i)
-#pragma unroll
-        for (int j = 0; j < D; ++j)
-          ij[i][j] = ijc[i][j];
-    }
-    else
+    if (!AFFINE)
       jacobian_at(tb, q, X, ij);
 #pragma unroll
     for (int e = 0; e < NEQ; ++e)
@@ -337,24 +341,35 @@ __global__ void __launch_bounds__(NT)
         acc = acc + tb.V[q][n] * T(su[n * NEQ + e]);
       suq[q * NEQ + e] = acc;
       T r = T(0);
-#pragma unroll
-      for (int ic = 0; ic < D; ++ic)
+      if (AFFINE)
       {
-        T dref[D];
 #pragma unroll
         for (int xi = 0; xi < D; ++xi)
+#pragma unroll
+          for (int f = 0; f < NFL; ++f)
+            r = r + tb.dVf[xi][q][f] * sfk[(f * NEQ + e) * D + xi];
+      }
+      else
+      {
+#pragma unroll
+        for (int ic = 0; ic < D; ++ic)
         {
-          T s2 = tb.dVf[xi][q][0] * sfk[(0 * NEQ + e) * D + ic];
+          T dref[D];
 #pragma unroll
-          for (int f = 1; f < NFL; ++f)
-            s2 = s2 + tb.dVf[xi][q][f] * sfk[(f * NEQ + e) * D + ic];
-          dref[xi] = s2;
+          for (int xi = 0; xi < D; ++xi)
+          {
+            T s2 = tb.dVf[xi][q][0] * sfk[(0 * NEQ + e) * D + ic];
+#pragma unroll
+            for (int f = 1; f < NFL; ++f)
+              s2 = s2 + tb.dVf[xi][q][f] * sfk[(f * NEQ + e) * D + ic];
+            dref[xi] = s2;
+          }
+          T dphys = ij[ic][0] * dref[0];
+#pragma unroll
+          for (int xi = 1; xi < D; ++xi)
+            dphys = dphys + ij[ic][xi] * dref[xi];
+          r = r + dphys;
         }
-        T dphys = ij[ic][0] * dref[0];
-#pragma unroll
-        for (int xi = 1; xi < D; ++xi)
-          dphys = dphys + ij[ic][xi] * dref[xi];
-        r = r + dphys;
       }
       srq[q * NEQ + e] = r;
     }

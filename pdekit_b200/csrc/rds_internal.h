@@ -53,7 +53,8 @@ struct HostBC
   std::vector<double> fw, fV, fdVgeo;
   int32_t *d_sol_conn = nullptr; // SoA [nfdof][nfacets]
   int32_t *d_geo_conn = nullptr; // SoA [nfgeo][nfacets]
-  double *d_gq        = nullptr; // [neq][nfq][nfacets]
+  double *d_gq        = nullptr; // [neq][nfq][nfacets]; farfield [neq]; strong [neq][nstrong]
+  int nstrong         = 0;       // strong Dirichlet: distinct dofs (d_sol_conn holds them)
   long long slot_base = 0;
   long long ws_base   = 0;
   int physics         = 0;
@@ -167,6 +168,7 @@ struct BCArgs
   double params[4];  // WeakSubInlet: T_tot, p_tot; WeakSubOutlet: p_out
   unsigned *status;
   const int *stop;
+  double *u_strong; // strong Dirichlet: the state it overwrites (the same buffer as u)
 };
 
 struct GatherArgs

@@ -256,7 +256,7 @@ __device__ __forceinline__ void euler_acoustic(const EulerProps<T, D> &p, T gamm
 #pragma unroll
   for (int d = 0; d < D; ++d)
     c.gV[d] = gm1 * p.V[d] * c.inv_a;
-  c.g_rhoa = gm1 / (p.rho * p.a);
+  c.g_rhoa = gm1 * p.inv_rho * c.inv_a;
 }
 
 // K = R op(Lambda) L for direction dir (op = max(0, .) for SIGN > 0, min(0, .) otherwise), in
@@ -275,10 +275,12 @@ __device__ __forceinline__ T euler_K_split(const EulerProps<T, D> &p,
   T n2            = dir[0] * dir[0] + dir[1] * dir[1];
   if (D == 3)
     n2 = n2 + dir[D - 1] * dir[D - 1];
-  const T norm = sqrt(n2);
+  // |dir| and 1/|dir| from one reciprocal square root
+  const T rn   = n2 > T(0) ? rsqrt(n2) : T(0);
+  const T norm = n2 * rn;
   // the reference keeps dir unnormalised below |dir| = 1e-9 (2D) or at |dir| = 0 (3D)
   const bool keep = (D == 2) ? (norm < T(1.e-9)) : (norm == T(0));
-  const T inv_n   = keep ? T(1) : T(1) / norm;
+  const T inv_n   = keep ? T(1) : rn;
   T n[D];
 #pragma unroll
   for (int d = 0; d < D; ++d)

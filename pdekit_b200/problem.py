@@ -58,7 +58,8 @@ class CellGroup:
 
 @dataclasses.dataclass
 class BCGroup:
-    kind: str  # WeakDirichlet | WeakWall | WeakSubInlet | WeakSubOutlet
+    kind: str  # WeakDirichlet | WeakWall | WeakSubInlet | WeakSubOutlet | WeakFarfield |
+    # StrongDirichlet
     name: str
     sol_conn: np.ndarray  # [nfacets, nfdof] int32
     geo_conn: np.ndarray  # [nfacets, nfgeo] int32
@@ -66,7 +67,10 @@ class BCGroup:
     fV: np.ndarray  # [nfq, nfdof]
     fVgeo: np.ndarray  # [nfq, nfgeo]
     fdVgeo: np.ndarray  # [dim-1, nfq, nfgeo]
-    gq: np.ndarray  # [nfacets, nfq, neq] boundary state at facet quadrature points
+    # WeakDirichlet: [nfacets, nfq, neq] boundary state at the facet quadrature points;
+    # WeakFarfield: [neq] reference state (conservative); StrongDirichlet: [nfacets, nfdof, neq]
+    # values the facet dofs take (facet by facet, a shared dof keeps the later value)
+    gq: np.ndarray
     order: int = 1  # polynomial order of the facet's solution basis
     params: tuple = (0.0, 0.0, 0.0, 0.0)  # WeakSubInlet: (T_tot, p_tot); WeakSubOutlet: (p,)
 
@@ -148,12 +152,20 @@ def load_golden(path: str):
                     gq=np.zeros((arrs[f"bc{ib}_sol"].shape[0], arrs["fw"].shape[0], meta["neq"])))
         b.order = meta["p"]
         expr = bc["expr"]
-        if "=" in expr:  # parameters of WeakSubInlet / WeakSubOutlet
+        if bc["type"] == "WeakFarfield":  # "state=v0|v1|...", set_reference_state
+            b.gq = np.array([float(v) for v in expr.split("=", 1)[1].split("|")])
+        elif "=" in expr:  # parameters of WeakSubInlet / WeakSubOutlet
             kv = dict(item.split("=") for item in expr.split(";"))
             if bc["type"] == "WeakSubInlet":
                 b.params = (float(kv["total_temperature"]), float(kv["total_pressure"]), 0.0, 0.0)
             else:
                 b.params = (float(kv["total_pressure"]), 0.0, 0.0, 0.0)
+        elif bc["type"] == "StrongDirichlet":
+            # the values the reference's StrongDirichletBC applied (state after its first
+            # assemble at the facet dofs): for P2 / P3 facets the reference evaluates its
+            # expression at the facet's geometry-node coordinates, also for the dofs past the
+            # geometry nodes, so these are not the expression at the dof coordinates there
+            b.gq = np.ascontiguousarray(arrs["ua1"][b.sol_conn])
         elif bc["type"] == "WeakDirichlet":
             xq = b.quadrature_coords(prob.geo_coords)
             b.gq = bcexpr.evaluate(expr, xq, meta["neq"])

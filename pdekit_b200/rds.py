@@ -31,7 +31,8 @@ PHYSICS = {"advconst": 0, "burgers": 1, "euler2d": 2, "euler3d": 3}
 SCHEME = {"lda": 0, "n": 1, "b": 2}
 PRECISION = {"fp64": 0, "mixed": 1}
 SHAPE = {"line": 2, "triag": 3, "quad": 4, "tetra": 10}
-BC_KIND = {"WeakDirichlet": 0, "WeakWall": 1, "WeakSubInlet": 2, "WeakSubOutlet": 3}
+BC_KIND = {"WeakDirichlet": 0, "WeakWall": 1, "WeakSubInlet": 2, "WeakSubOutlet": 3,
+           "WeakFarfield": 4, "StrongDirichlet": 5}
 
 STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "NONFINITE", 4: "NEG_PRESSURE", 5: "ITER_CAP",
           6: "UNSUPPORTED", 7: "TOO_LARGE"}
@@ -190,7 +191,9 @@ class PGRDMethodExplicit:
         return self
 
     def add_boundary_condition(self, b):
-        """RDMethod::add_boundary_condition for a weak condition with its boundary data."""
+        """RDMethod::add_boundary_condition with its boundary data (`b.gq`: the boundary state
+        at the facet quadrature points for WeakDirichlet, the reference state for WeakFarfield,
+        the values of the facet dofs for StrongDirichlet)."""
         arrs = [np.ascontiguousarray(b.sol_conn, dtype=np.int32),
                 np.ascontiguousarray(b.geo_conn, dtype=np.int32)] + \
                [np.ascontiguousarray(x, dtype=np.float64) for x in (b.fw, b.fV, b.fdVgeo, b.gq)]

@@ -58,7 +58,20 @@ void add_bcs(Solver &s, const std::string &spec)
     std::getline(is, boundary, ':');
     std::getline(is, expr, ':');
     auto bc = s.add_boundary_condition(type, name, boundary);
-    if (expr.find('=') != std::string::npos)
+    if (expr.rfind("state=", 0) == 0)
+    {
+      // WeakFarfield reference state "state=v0|v1|..."
+      std::vector<double> vals;
+      std::stringstream vs(expr.substr(6));
+      std::string v;
+      while (std::getline(vs, v, '|'))
+        vals.push_back(std::atof(v.c_str()));
+      math::DenseDVec<Real> st(vals.size());
+      for (Uint i = 0; i < vals.size(); ++i)
+        st[i] = vals[i];
+      bc->set_reference_state(st);
+    }
+    else if (expr.find('=') != std::string::npos)
     {
       std::stringstream ps(expr);
       std::string kv;

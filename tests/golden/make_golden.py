@@ -40,6 +40,24 @@ EULER3D_BCS = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakWall:top_wall_bc:top_w
                "total_pressure=120195.4453,"
                "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
 
+# WeakFarfield with the bump freestream as reference state (conservative variables), and
+# StrongDirichlet inflow (the strong condition precedes the weak left inflow in name order, so
+# the weak condition sees the overwritten corner state)
+FAR2D = "state=1.204780419|206.7048679|0|271049.8994"
+FAR3D = "state=1.143916132|233.0856257|0|0|259331.1534"
+EULER2D_FAR_BCS = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakFarfield:farfield_bc:top_wall:" + FAR2D
+                   + ",WeakSubInlet:inlet_bc:inlet:total_temperature=307.6488978;"
+                   "total_pressure=120195.4453,"
+                   "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
+EULER3D_FAR_BCS = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakFarfield:farfield_bc:top_wall:" + FAR3D
+                   + ",WeakFarfield:side_bc:side_walls:" + FAR3D
+                   + ",WeakSubInlet:inlet_bc:inlet:total_temperature=307.6488978;"
+                   "total_pressure=120195.4453,"
+                   "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
+ADV_STRONG_BCS = "StrongDirichlet:inlet_bottom:bottom:sin2pix,WeakDirichlet:inlet_left:left:zero"
+BURG_STRONG_BCS = ("WeakDirichlet:inlet:bottom:burgers_inlet,StrongDirichlet:left:left:c1.5,"
+                   "WeakDirichlet:right:right:c-0.5")
+
 # name: (physics, scheme, p, quad order, n, jitter, seed, init, bcs, cfl, iters)
 # n is the squares per side of the unit square, or a tuple naming another mesh:
 #   ("channel_tri", nx, ny) / ("channel_quad", nx, ny): bump channel [-1.5,1.5] x [0,1]
@@ -69,6 +87,15 @@ CASES = {
     # configuration 4 (Euler 3D bump box, P2 tetrahedra, LDA)
     "euler3d_tet_p2_lda": ("euler3d", "lda", 2, 5, ("box_tet", 3, 2, 2), 0.1, 41, "bump3d",
                            EULER3D_BCS, 0.5, 3),
+    # the other two conditions of the reference's registry (bc/RDMBCManager.hpp:57-89);
+    # WeakFarfield only with Euler (the reference's scalar instantiation crashes in the harness)
+    "adv_p2_strong": ("advconst", "lda", 2, 5, 5, 0.2, 16, "smooth", ADV_STRONG_BCS, 0.9, 3),
+    "adv_p1_strong": ("advconst", "n", 1, 4, 6, 0.2, 18, "smooth", ADV_STRONG_BCS, 0.9, 3),
+    "burgers_p2_strong": ("burgers", "b", 2, 5, 5, 0.15, 26, "burgers", BURG_STRONG_BCS, 0.5, 3),
+    "euler2d_tri_p2_farfield": ("euler2d", "n", 2, 5, ("channel_tri", 4, 3), 0.15, 35, "bump2d",
+                                EULER2D_FAR_BCS, 0.5, 3),
+    "euler3d_tet_p2_farfield": ("euler3d", "lda", 2, 5, ("box_tet", 3, 2, 2), 0.1, 42, "bump3d",
+                                EULER3D_FAR_BCS, 0.5, 3),
 }
 
 

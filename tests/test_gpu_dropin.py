@@ -31,9 +31,21 @@ E3D = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakWall:top_wall_bc:top_wall:-,"
        "WeakSubInlet:inlet_bc:inlet:total_temperature=307.6488978;total_pressure=120195.4453,"
        "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
 
+E2D_FAR = ("WeakWall:bottom_wall_bc:bottom_wall:-,"
+           "WeakFarfield:farfield_bc:top_wall:state=1.204780419|206.7048679|0|271049.8994,"
+           "WeakSubInlet:inlet_bc:inlet:total_temperature=307.6488978;total_pressure=120195.4453,"
+           "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
+ADV_STRONG = "StrongDirichlet:inlet_bottom:bottom:sin2pix,WeakDirichlet:inlet_left:left:zero"
+
 # (physics, scheme, p, quad order, mesh, init, conditions, CFL, iterations)
 CASES = {
     "adv_p1_lda": ("advconst", "lda", 1, 4, ("square", 8, 0.2, 1), "zero", ADV, 0.9, 20),
+    # StrongDirichlet on P1 facets (for P2 / P3 facets the reference evaluates the expression
+    # past the facet geometry's nodes)
+    "adv_p1_n_strong": ("advconst", "n", 1, 4, ("square", 8, 0.2, 6), "smooth", ADV_STRONG, 0.9,
+                        10),
+    "euler2d_tri_p2_farfield": ("euler2d", "n", 2, 5, ("channel", 4, 0, 3, 7), "bump2d", E2D_FAR,
+                                0.5, 5),
     "adv_p2_b": ("advconst", "b", 2, 5, ("square", 6, 0.2, 2), "smooth", ADV, 0.9, 10),
     "burgers_p2_b": ("burgers", "b", 2, 5, ("square", 6, 0.15, 3), "burgers", BURG, 0.5, 10),
     "burgers_p3_n": ("burgers", "n", 3, 8, ("square", 4, 0.2, 4), "burgers", BURG, 0.5, 10),

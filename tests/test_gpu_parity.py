@@ -70,7 +70,8 @@ def test_bitwise_repeatable(case):
 
 @pytest.mark.parametrize("case", ["burgers_p2_b", "adv_p1_lda", "adv_p2_b", "burgers_p3_b",
                                   "euler2d_tri_p3_b", "euler2d_quad_p3_b",
-                                  "euler3d_tet_p2_lda"])
+                                  "euler3d_tet_p2_lda", "adv_p2_strong", "burgers_p2_strong",
+                                  "euler2d_tri_p2_farfield", "euler3d_tet_p2_farfield"])
 def test_gpu_matches_oracle_many_iterations(case):
     prob, a, meta = load_golden(os.path.join(GOLDEN, case))
     s = _solver(prob)
