@@ -80,6 +80,9 @@ def parse():
                     help="--quick: precision of the timed steps")
     ap.add_argument("--tensor-cores", action="store_true",
                     help="mixed cells with the basis contractions on the tensor cores")
+    ap.add_argument("--partition", action="store_true",
+                    help="c1-c4: split the one mesh over the ranks (interface sums all-reduced "
+                         "every iteration, strong scaling) instead of one replica per rank")
     return ap.parse_args()
 
 
@@ -416,6 +419,8 @@ def run_ours(args, rank, world, local):
     torch.cuda.set_device(local)
     if args.workload == "c5":
         return run_batched(args, rank, world, local)
+    if args.partition:
+        return run_partitioned(args, rank, world, local)
     prob, u0, cfl, desc, default_steps, cpu_spec = workload(args.workload, args)
     steps = args.steps or default_steps
     ncells = prob.ncells
@@ -539,6 +544,58 @@ def run_ours(args, rank, world, local):
         "wall_s_timed_region": round(wall, 3),
     }
     solver.close()
+    return line
+
+
+def run_partitioned(args, rank, world, local):
+    """c1-c4 with the one mesh split over the ranks (pdekit_b200.partition): per step every rank
+    assembles its cells, the interface sums are all-reduced, every rank updates its nodes and the
+    norm parts are all-reduced. Strong scaling: value = the whole mesh's cells x steps / the
+    slowest rank's time."""
+    import torch
+
+    from pdekit_b200.partition import PartitionedRDS
+
+    prob, u0, cfl, desc, default_steps, _ = workload(args.workload, args)
+    steps = args.steps or default_steps
+    pr = PartitionedRDS(prob, rank, world)
+    pr.set_solution(u0)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+    for _ in range(max(args.warmup, 3)):
+        pr.step(cfl)
+    torch.cuda.synchronize()
+    pr.set_solution(u0)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = pr.rank.solver.launch_count()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(pr.rank.stream):
+            for k in range(steps):
+                flush.zero_()
+                ev[k][0].record(pr.rank.stream)
+                pr.step(cfl)
+                ev[k][1].record(pr.rank.stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    launches = pr.rank.solver.launch_count() - launches0
+    ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world)
+    norm = pr.norm()
+    part = pr.partition.parts[rank]
+    line = {"metric": "cell-residual updates/s", "value": prob.ncells * steps / (ms * 1e-3),
+            "unit": "cell-residual updates/s", "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "cells": prob.ncells,
+                       "l2": "L2 flushed (256 MB write) before every timed step",
+                       "parallelism": f"one mesh split over {world} ranks along x "
+                                      f"({pr.partition.nslots:,} interface nodes), interface "
+                                      "sums all-reduced per step"},
+            "final_norm": [float(x) for x in norm], "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+            "cells_rank0": int(sum(len(c) for c in part.cells))}
+    pr.close()
     return line
 
 

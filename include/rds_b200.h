@@ -189,6 +189,31 @@ RDS_API rds_status rds_assemble_rhs(rds_ctx *ctx);
 RDS_API rds_status rds_update(rds_ctx *ctx);
 /* compute_residual_norm(): sqrt(sum_n (res_n dt_n)^2 / N) per equation, into norm[neq]. */
 RDS_API rds_status rds_residual_norm(rds_ctx *ctx, double *norm);
+/* Partitioned single mesh (no counterpart call in the reference, whose explicit solver runs
+ * one mesh per process): one context per rank holds a part of the cells and the nodes they
+ * touch, renumbered; the ranks add their partial nodal sums at the nodes they share.
+ * Per iteration: rds_assemble_rhs, rds_pack_interface, a sum of the buffers over the ranks
+ * (e.g. an NCCL all-reduce on the context's stream), rds_unpack_interface, rds_finish, a sum
+ * of 'sq' over the ranks; norm = sqrt(sum / total node count).
+ *   rds_set_dual_volume: replaces the dual volumes [nnodes] (host) after rds_finalize, with the
+ *     sums over all ranks' cells at the shared nodes.
+ *   rds_set_interface: the n shared nodes (local numbers) and their slots in an exchange
+ *     buffer of nslots x (neq + 1) doubles, and owned [nnodes] (host, 1 where this rank counts
+ *     the node in the norm: every node is owned by exactly one rank).
+ *   rds_pack_interface: zeroes the device buffer, then writes residual and wave speed of the
+ *     shared nodes at their slots.
+ *   rds_unpack_interface: the summed residual and wave speed back from the device buffer.
+ *   rds_finish: dt = CFL V / ws, u -= dt res when update != 0, and sq[neq] (device) = sum over
+ *     the owned nodes of (res dt)^2. Asynchronous; rds_check reports the status flags
+ *     (non-finite values, non-positive pressure) raised by the work done so far. */
+RDS_API rds_status rds_set_dual_volume(rds_ctx *ctx, const double *vol);
+RDS_API rds_status rds_set_interface(rds_ctx *ctx, int n, const int32_t *nodes,
+                                     const int32_t *slots, int nslots, const uint8_t *owned);
+RDS_API rds_status rds_pack_interface(rds_ctx *ctx, double *buf);
+RDS_API rds_status rds_unpack_interface(rds_ctx *ctx, const double *buf);
+RDS_API rds_status rds_finish(rds_ctx *ctx, double cfl, int update, double *sq);
+RDS_API rds_status rds_check(rds_ctx *ctx);
+
 /* Copy out any of: residual [node][neq], dt [node], nodal wave speed [node], dual volume [node]
  * (NULL skips). */
 RDS_API rds_status rds_get_fields(rds_ctx *ctx, double *res_aos, double *dt, double *ws, double *vol);

@@ -60,6 +60,12 @@ struct rds_ctx
   int gblocks   = 0;
   int hist_cap  = 0;
 
+  // partitioned single mesh: the nodes this rank shares with others, their slots in the
+  // exchange buffer, and the nodes whose (res dt)^2 this rank counts in the norm
+  int32_t *d_if_nodes = nullptr, *d_if_slots = nullptr;
+  uint8_t *d_owned    = nullptr;
+  int n_if = 0, n_slots = 0;
+
   // pinned host scalars for the loop's stop test
   int *h_stop = nullptr;
 
@@ -979,6 +985,105 @@ rds_status rds_residual_norm(rds_ctx *ctx, double *norm)
   return RDS_OK;
 }
 
+// ---- partitioned single mesh ------------------------------------------------------------
+
+rds_status rds_set_dual_volume(rds_ctx *ctx, const double *vol)
+{
+  if (!ctx || !vol || !ctx->finalized)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_set_dual_volume: not finalized or null")
+               : RDS_ERR_INVALID;
+  const int N = ctx->desc.nnodes;
+  std::vector<double> v(vol, vol + N), iv(N);
+  for (int i = 0; i < N; ++i)
+  {
+    if (!(v[i] > 0.0))
+      return fail(ctx, RDS_ERR_INVALID, "rds_set_dual_volume: non-positive volume");
+    iv[i] = 1. / v[i];
+  }
+  rds_status st;
+  if ((st = upload(ctx, ctx->d_vol, v.data(), N)) != RDS_OK ||
+      (st = upload(ctx, ctx->d_inv_vol, iv.data(), N)) != RDS_OK)
+    return st;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RDS_OK;
+}
+
+rds_status rds_set_interface(rds_ctx *ctx, int n, const int32_t *nodes, const int32_t *slots,
+                             int nslots, const uint8_t *owned)
+{
+  if (!ctx || !ctx->finalized || n < 0 || nslots < 0 || (n > 0 && (!nodes || !slots)) || !owned)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_set_interface: invalid arguments")
+               : RDS_ERR_INVALID;
+  const int N = ctx->desc.nnodes;
+  for (int i = 0; i < n; ++i)
+    if (nodes[i] < 0 || nodes[i] >= N || slots[i] < 0 || slots[i] >= nslots)
+      return fail(ctx, RDS_ERR_INVALID, "rds_set_interface: node or slot out of range");
+  cudaFree(ctx->d_if_nodes);
+  cudaFree(ctx->d_if_slots);
+  cudaFree(ctx->d_owned);
+  ctx->d_if_nodes = ctx->d_if_slots = nullptr;
+  ctx->d_owned                      = nullptr;
+  rds_status st;
+  if ((st = dalloc(ctx, &ctx->d_if_nodes, n)) != RDS_OK ||
+      (st = dalloc(ctx, &ctx->d_if_slots, n)) != RDS_OK ||
+      (st = dalloc(ctx, &ctx->d_owned, N)) != RDS_OK)
+    return st;
+  if ((n > 0 && ((st = upload(ctx, ctx->d_if_nodes, nodes, n)) != RDS_OK ||
+                 (st = upload(ctx, ctx->d_if_slots, slots, n)) != RDS_OK)) ||
+      (st = upload(ctx, ctx->d_owned, owned, N)) != RDS_OK)
+    return st;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->n_if    = n;
+  ctx->n_slots = nslots;
+  return RDS_OK;
+}
+
+rds_status rds_pack_interface(rds_ctx *ctx, double *buf)
+{
+  if (!ctx || !buf || !ctx->d_owned)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_pack_interface: rds_set_interface first")
+               : RDS_ERR_INVALID;
+  const int NEQ = ctx->desc.neq;
+  return launch(ctx, [&](const char **name) {
+    *name = "pack_interface";
+    return launch_pack_interface(ctx->n_if, NEQ, ctx->desc.nnodes, ctx->d_if_nodes,
+                                 ctx->d_if_slots, ctx->d_res, ctx->d_ws, buf,
+                                 (size_t)ctx->n_slots * (NEQ + 1), ctx->stream);
+  });
+}
+
+rds_status rds_unpack_interface(rds_ctx *ctx, const double *buf)
+{
+  if (!ctx || !buf || !ctx->d_owned)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_unpack_interface: rds_set_interface first")
+               : RDS_ERR_INVALID;
+  return launch(ctx, [&](const char **name) {
+    *name = "unpack_interface";
+    return launch_unpack_interface(ctx->n_if, ctx->desc.neq, ctx->desc.nnodes, ctx->d_if_nodes,
+                                   ctx->d_if_slots, buf, ctx->d_res, ctx->d_ws, ctx->stream);
+  });
+}
+
+rds_status rds_finish(rds_ctx *ctx, double cfl, int update, double *sq)
+{
+  if (!ctx || !sq || !ctx->d_owned)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_finish: rds_set_interface first")
+               : RDS_ERR_INVALID;
+  return launch(ctx, [&](const char **name) {
+    *name = "finish_nodes";
+    return launch_finish(ctx->desc.nnodes, ctx->desc.neq, cfl, update, ctx->d_vol, ctx->d_ws,
+                         ctx->d_res, ctx->d_dt, ctx->d_u, ctx->d_owned, ctx->d_part, sq,
+                         ctx->stream);
+  });
+}
+
+rds_status rds_check(rds_ctx *ctx)
+{
+  if (!ctx)
+    return RDS_ERR_INVALID;
+  return check_status(ctx);
+}
+
 rds_status rds_get_fields(rds_ctx *ctx, double *res, double *dt, double *ws, double *vol)
 {
   if (!ctx || !ctx->finalized)
@@ -1694,6 +1799,9 @@ rds_status rds_destroy(rds_ctx *ctx)
     cudaFree(b.d_geo_conn);
     cudaFree(b.d_gq);
   }
+  cudaFree(ctx->d_if_nodes);
+  cudaFree(ctx->d_if_slots);
+  cudaFree(ctx->d_owned);
   void *bufs[] = {ctx->d_X,     ctx->d_u,     ctx->d_res,     ctx->d_ws,       ctx->d_dt,
                   ctx->d_vol,   ctx->d_inv_vol, ctx->d_contrib, ctx->d_wsc,    ctx->d_stage,
                   ctx->d_row,   ctx->d_ent_slot, ctx->d_ent_ws, ctx->d_part,   ctx->d_norm,

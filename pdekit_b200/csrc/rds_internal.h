@@ -245,5 +245,15 @@ cudaError_t launch_cells_scalar_tc(const HostCellGroup &g, const CellArgs &a, bo
                                    int ntiles, cudaStream_t s, const char **name, bool *ok);
 cudaError_t launch_update(int nnodes, int neq, const double *dt, const double *res, double *u,
                           cudaStream_t s, const char **name);
+// partitioned single mesh (rds_partition.cu)
+cudaError_t launch_pack_interface(int n, int neq, int nnodes, const int32_t *nodes,
+                                  const int32_t *slots, const double *res, const double *ws,
+                                  double *buf, size_t buf_len, cudaStream_t s);
+cudaError_t launch_unpack_interface(int n, int neq, int nnodes, const int32_t *nodes,
+                                    const int32_t *slots, const double *buf, double *res,
+                                    double *ws, cudaStream_t s);
+cudaError_t launch_finish(int nnodes, int neq, double cfl, int update, const double *vol,
+                          const double *ws, const double *res, double *dt, double *u,
+                          const uint8_t *owned, double *part, double *sq, cudaStream_t s);
 
 } // namespace rds

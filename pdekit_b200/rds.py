@@ -117,6 +117,12 @@ def lib():
         "rds_add_batch_bc": ([vp, vp, ip], ip),
         "rds_iterate_batch": ([vp, ip, dp, vp, vp], ip),
         "rds_autotune": ([vp, C.c_char_p, ip], ip),
+        "rds_set_dual_volume": ([vp, vp], ip),
+        "rds_set_interface": ([vp, ip, vp, vp, ip, vp], ip),
+        "rds_pack_interface": ([vp, vp], ip),
+        "rds_unpack_interface": ([vp, vp], ip),
+        "rds_finish": ([vp, dp, ip, vp], ip),
+        "rds_check": ([vp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

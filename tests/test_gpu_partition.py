@@ -1,0 +1,48 @@
+"""Partitioned single mesh on the GPU: two to four ranks emulated in one process on one GPU
+(pdekit_b200.partition.emulate: every rank's phases in turn, the sums over the ranks between
+them, so no rank waits for another on the device), against the single-context solver."""
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from helpers import rel_err
+from pdekit_b200.partition import emulate
+from pdekit_b200.problem import load_golden
+from pdekit_b200.rds import PGRDMethodExplicit
+
+pytestmark = pytest.mark.gpu
+
+
+def _single(prob, u0, cfl, iters):
+    s = PGRDMethodExplicit(prob.physics, prob.scheme, "fp64").configure_mesh_data(prob)
+    s.initialize_work_data()
+    s.set_solution(u0)
+    _, hist = s.iterate(cfl, iters)
+    u = s.solution()
+    s.close()
+    return u, hist
+
+
+@pytest.mark.parametrize("case", ["burgers_p2_b", "adv_p2_b", "euler2d_tri_p3_b",
+                                  "euler2d_quad_p3_b", "euler3d_tet_p2_lda",
+                                  "euler2d_tri_p2_farfield"])
+@pytest.mark.parametrize("nparts", [2, 3])
+def test_partitioned_matches_single_context(case, nparts):
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    u, norms = emulate(prob, nparts, a["u0"], meta["cfl"], 5)
+    u1, hist = _single(prob, a["u0"], meta["cfl"], 5)
+    assert rel_err(u, u1) < 1e-12
+    np.testing.assert_allclose(norms, hist, rtol=1e-11)
+
+
+def test_partitioned_larger_mesh_four_ranks():
+    from pdekit_b200 import workloads as W
+
+    prob, u0 = W.config2(n=48)
+    u, norms = emulate(prob, 4, u0, 0.5, 30)
+    u1, hist = _single(prob, u0, 0.5, 30)
+    assert rel_err(u, u1) < 1e-11
+    np.testing.assert_allclose(norms, hist, rtol=1e-10)
