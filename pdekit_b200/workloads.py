@@ -106,8 +106,10 @@ def euler_bcs(dim: int):
 
 
 def mesh_problem(mesh, physics: str, scheme: str, p: int, tables: dict, bcs) -> Problem:
-    """Problem on a general mesh: one cell group per element shape (tables[shape]), one weak
-    boundary condition per (kind, name, boundary[, params]) in `bcs`."""
+    """Problem on a general mesh: one cell group per element shape (tables[shape]), one boundary
+    condition per (kind, name, boundary[, data]) in `bcs`; data: the expression name
+    (WeakDirichlet, at the facet quadrature points; StrongDirichlet, at the facet dofs), the
+    parameters (WeakSubInlet / WeakSubOutlet) or the reference state (WeakFarfield)."""
     clone = meshgen.clone_continuous(mesh, p)
     dim = mesh.dim
     neq = {"advconst": 1, "burgers": 1, "euler2d": 4, "euler3d": 5}[physics]
@@ -118,7 +120,8 @@ def mesh_problem(mesh, physics: str, scheme: str, p: int, tables: dict, bcs) -> 
                                 dV=t["dV"], dVgeo=t["dVgeo"], dVf=t["dVf"], Vsf=t["Vsf"],
                                 shape=shape, order=p, wv=t.get("wv"), dVgeo_v=t.get("dVgeo_v")))
     prob = Problem(physics=physics, scheme=scheme, dim=dim, neq=neq, nnodes=clone.nsol,
-                   geo_coords=mesh.coords, groups=groups, bcs=[])
+                   geo_coords=mesh.coords, groups=groups, bcs=[],
+                   adv=ADV_CONST_DIR if physics == "advconst" else (0.0, 0.0, 0.0))
     facet_tables = tables[next(iter(clone.conn))]
     for spec in bcs:
         kind, name, boundary = spec[:3]
@@ -131,6 +134,11 @@ def mesh_problem(mesh, physics: str, scheme: str, p: int, tables: dict, bcs) -> 
                     params=tuple(params))
         if kind == "WeakDirichlet":
             b.gq = bcexpr.evaluate(spec[3], b.quadrature_coords(mesh.coords), neq)
+        elif kind == "StrongDirichlet":
+            b.gq = bcexpr.evaluate(spec[3], clone.coords[sol], neq)
+        elif kind == "WeakFarfield":
+            b.gq = np.asarray(spec[3], dtype=np.float64)
+            b.params = (0.0,) * 4
         prob.bcs.append(b)
     prob.bcs.sort(key=lambda b: b.name)
     prob.sol_coords = clone.coords
