@@ -27,8 +27,9 @@ Metric: cell-residual updates/s = cells x steps / time. Reported:
 
   python bench.py [--workload c1..c5] [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 With N > 1 (torchrun), every rank runs its own independent copy of c1-c4 (replicas, weak
-scaling; the path has no data exchange between independent problems); c5's problems are split
-over the ranks by estimated work (strong scaling). Timing is the max over ranks.
+scaling), or with --partition the one mesh split over the ranks with the interface sums
+all-reduced every iteration (strong scaling); c5's problems are split over the ranks by
+estimated work (strong scaling). Timing is the max over ranks.
 """
 
 from __future__ import annotations
@@ -204,6 +205,17 @@ def group_work(prob):
         flop += f * g.ncells
         byts += cell_bytes(prob.dim, prob.neq, g.ndof, g.ngeo) * g.ncells
     return flop, byts
+
+
+# DRAM bytes (read + write) per launch of the dominant cell kernel(s) of a workload, from one ncu
+# capture of the same kernel (cold caches between replays); the summary files give the command.
+PROFILED_TRAFFIC = {
+    "c1": (0.30771e6, "profiles/dram_traffic_cell_kernels.md"),
+    "c2": (31.508736e6 + 0.380416e6, "profiles/cells_burgers_b_p2_512.md"),
+    "c3": ((102.85 + 118.34 + 193.39 + 220.73) * 1e6,  # both groups, per iteration
+           "profiles/dram_traffic_cell_kernels.md"),
+    "c4": ((91.59 + 271.63) * 1e6, "profiles/dram_traffic_cell_kernels.md"),
+}
 
 
 def roofline(kernel, ms_per_launch, flop, byts, peak_fp64, hbm_gbs):
@@ -473,6 +485,8 @@ def run_ours(args, rank, world, local):
     peak64 = measure_peak("fp64")
     roof = roofline(kname, cell_ms, flop, byts, peak64, hbm_peak())
     roof["launches_per_iteration"] = len(prob.groups)
+    if args.workload in PROFILED_TRAFFIC and (args.workload != "c2" or args.n == 512):
+        roof["traffic"], roof["traffic_source"] = PROFILED_TRAFFIC[args.workload]
 
     # e2e through the C ABI with host buffers (pinned)
     u_host = torch.from_numpy(np.ascontiguousarray(u0)).pin_memory()
