@@ -27,3 +27,21 @@ def test_library_exports_every_declared_symbol():
 
 def test_version_string():
     assert b"sm_100a" in rds.lib().rds_version()
+
+
+def test_invalid_descriptor_rejected_before_any_device_call():
+    """rds_create validates the descriptor first (no GPU needed to see the error)."""
+    import numpy as np
+
+    L = rds.lib()
+    coords = np.zeros((3, 2))
+    for physics, dim, neq, scheme, nnodes in [(9, 2, 1, 0, 3), (1, 3, 1, 0, 3), (2, 2, 1, 0, 3),
+                                              (1, 2, 1, 7, 3), (1, 2, 1, 0, 0)]:
+        d = rds._Desc()
+        d.physics, d.dim, d.neq, d.scheme, d.precision = physics, dim, neq, scheme, 0
+        d.nnodes, d.ngeo_nodes, d.geo_coords = nnodes, 3, coords.ctypes.data_as(ctypes.c_void_p)
+        ctx = ctypes.c_void_p()
+        assert L.rds_create(ctypes.byref(ctx), ctypes.byref(d), None) == 1  # RDS_ERR_INVALID
+        assert b"invalid descriptor" in L.rds_last_error(ctx)
+        L.rds_destroy(ctx)
+    assert L.rds_create(None, None, None) == 1
