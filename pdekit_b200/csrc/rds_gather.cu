@@ -79,7 +79,10 @@ __device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, co
   for (int e = 0; e < NEQ; ++e)
     acc[e] = 0.0;
   double ws       = 0.0;
-  const double iv = a.inv_vol[v];
+  // 1 / V formed here (correctly rounded, the same value as the stored inverse) instead of
+  // loaded: one 8-byte read less per node; V itself is read once for both uses
+  const double vv = a.vol[v];
+  const double iv = __drcp_rn(vv);
   const int i0 = a.row[v], i1 = a.row[v + 1];
   int i        = i0;
   // four entries at a time: all their loads are issued before the ordered sums consume them
@@ -128,7 +131,7 @@ __device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, co
   a.ws[v] = ws;
   if (DT)
   {
-    const double dtv = __ddiv_rn(__dmul_rn(cfl, a.vol[v]), ws);
+    const double dtv = __ddiv_rn(__dmul_rn(cfl, vv), ws);
     a.dt[v]          = dtv;
 #pragma unroll
     for (int e = 0; e < NEQ; ++e)
