@@ -269,7 +269,8 @@ static void build_K(const rdso_model *m, const props_t *p, const double *dir, in
   eigen_structure(m, p, dir, R, L, eig);
   double lo[NEQ_MAX];
   for (int k = 0; k < n; ++k)
-    lo[k] = sign > 0 ? (eig[k] > 0.0 ? eig[k] : 0.0) : (eig[k] < 0.0 ? eig[k] : 0.0);
+    lo[k] = sign > 0 ? (eig[k] > 0.0 ? eig[k] : 0.0)
+                     : sign < 0 ? (eig[k] < 0.0 ? eig[k] : 0.0) : eig[k];
   if (n == 1)
   {
     /* scalar build_K_mat: 1. * op(lambda) * 1. */
@@ -655,6 +656,78 @@ void rdso_cell_residual(const rdso_model *m, const rdso_cells *g, const double *
                         const double *un, double *elem_res, double *elem_ws)
 {
   cell_residual(m, g, X, un, elem_res, elem_ws);
+}
+
+/* PGLDA element Jacobian of the Picard linearisation (PGLDA.hpp:316-536):
+ * J_mn += w_q |J_q| (Kp_m (sum Kp)^-1) K_n with Kp from build_K_mat(op = max(0,.)) and K_n
+ * from build_K_mat(op = identity), accumulated point by point in the reference's order. */
+void rdso_element_jacobian(const rdso_model *m, const rdso_cells *g, const double *X,
+                           const double *un, double *jac)
+{
+  const int D = m->dim, NEQ = m->neq;
+  const int ndof = g->ndof, nq = g->nq, ngeo = g->ngeo, NR = ndof * NEQ;
+  for (int i = 0; i < NR * NR; ++i)
+    jac[i] = 0.0;
+  static double Kp[NDOF_MAX][NEQ_MAX][NEQ_MAX], Kn[NDOF_MAX][NEQ_MAX][NEQ_MAX];
+  for (int q = 0; q < nq; ++q)
+  {
+    double invJ[DIM_MAX][DIM_MAX];
+    const double jd = jacobian(D, g->dVgeo, nq, ngeo, q, X, invJ);
+    const double wj = g->w[q] * jd;
+    double uq[NEQ_MAX];
+    for (int e = 0; e < NEQ; ++e)
+    {
+      const double *row = g->V + (size_t)q * ndof;
+      double s          = row[0] * un[0 * NEQ + e];
+      for (int n = 1; n < ndof; ++n)
+        s = s + row[n] * un[n * NEQ + e];
+      uq[e] = s;
+    }
+    props_t pq;
+    props(m, uq, &pq);
+    double sumKp[NEQ_MAX][NEQ_MAX], inv[NEQ_MAX][NEQ_MAX];
+    memset(sumKp, 0, sizeof(sumKp));
+    for (int n = 0; n < ndof; ++n)
+    {
+      double gref[DIM_MAX], gphys[DIM_MAX], eig[NEQ_MAX];
+      for (int d = 0; d < D; ++d)
+        gref[d] = g->dV[((size_t)d * nq + q) * ndof + n];
+      for (int x = 0; x < D; ++x)
+      {
+        double s = invJ[x][0] * gref[0];
+        for (int xi = 1; xi < D; ++xi)
+          s = s + invJ[x][xi] * gref[xi];
+        gphys[x] = s;
+      }
+      build_K(m, &pq, gphys, +1, eig, Kp[n]);
+      build_K(m, &pq, gphys, 0, eig, Kn[n]);
+      for (int i = 0; i < NEQ; ++i)
+        for (int j = 0; j < NEQ; ++j)
+          sumKp[i][j] += Kp[n][i][j];
+    }
+    inverse(NEQ, sumKp, inv);
+    for (int mm = 0; mm < ndof; ++mm)
+    {
+      double B[NEQ_MAX][NEQ_MAX];
+      for (int i = 0; i < NEQ; ++i)
+        for (int j = 0; j < NEQ; ++j)
+        {
+          double s = Kp[mm][i][0] * inv[0][j];
+          for (int k = 1; k < NEQ; ++k)
+            s = s + Kp[mm][i][k] * inv[k][j];
+          B[i][j] = s;
+        }
+      for (int n = 0; n < ndof; ++n)
+        for (int i = 0; i < NEQ; ++i)
+          for (int j = 0; j < NEQ; ++j)
+          {
+            double s = B[i][0] * Kn[n][0][j];
+            for (int k = 1; k < NEQ; ++k)
+              s = s + B[i][k] * Kn[n][k][j];
+            jac[(size_t)(mm * NEQ + i) * NR + n * NEQ + j] += wj * s;
+          }
+    }
+  }
 }
 
 /* ------------------------------------------------------------------------------------------ */

@@ -65,6 +65,7 @@ def lib():
         L.rdso_update.argtypes = [C.c_int, C.c_int, vp, vp, vp]
         L.rdso_residual_norm.argtypes = [C.c_int, C.c_int, vp, vp, vp]
         L.rdso_cell_residual.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.rdso_element_jacobian.argtypes = [vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -151,3 +152,25 @@ class Oracle:
             norms[it] = nrm
             lib().rdso_update(prob.nnodes, prob.neq, _p(dt), _p(res), _p(u))
         return u, norms
+
+    def cell_residual(self, group, cell, u):
+        """Scheme residual [ndof, neq] and wave speed [ndof] of one cell from the state u."""
+        prob, g = self.prob, self.prob.groups[group]
+        X = np.ascontiguousarray(prob.geo_coords[g.geo_conn[cell]], dtype=np.float64)
+        un = np.ascontiguousarray(np.asarray(u).reshape(-1, prob.neq)[g.sol_conn[cell]])
+        res = np.zeros((g.ndof, prob.neq))
+        ws = np.zeros(g.ndof)
+        lib().rdso_cell_residual(C.byref(self.model), C.byref(self.groups[group]), _p(X), _p(un),
+                                 _p(res), _p(ws))
+        return res, ws
+
+    def element_jacobian(self, group, cell, u):
+        """PGLDA element Jacobian [ndof * neq, ndof * neq] of one cell at the state u."""
+        prob, g = self.prob, self.prob.groups[group]
+        X = np.ascontiguousarray(prob.geo_coords[g.geo_conn[cell]], dtype=np.float64)
+        un = np.ascontiguousarray(np.asarray(u).reshape(-1, prob.neq)[g.sol_conn[cell]])
+        nr = g.ndof * prob.neq
+        jac = np.zeros((nr, nr))
+        lib().rdso_element_jacobian(C.byref(self.model), C.byref(self.groups[group]), _p(X),
+                                    _p(un), _p(jac))
+        return jac

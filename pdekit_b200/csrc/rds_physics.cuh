@@ -259,8 +259,8 @@ __device__ __forceinline__ void euler_acoustic(const EulerProps<T, D> &p, T gamm
   c.g_rhoa = gm1 * p.inv_rho * c.inv_a;
 }
 
-// K = R op(Lambda) L for direction dir (op = max(0, .) for SIGN > 0, min(0, .) otherwise), in
-// split form. The convective eigenvalue lam_c = |dir| u.n has multiplicity D and the eigenvector
+// K = R op(Lambda) L for direction dir (op = max(0, .) for SIGN > 0, min(0, .) for SIGN < 0,
+// the identity for SIGN == 0: the flux Jacobian in direction dir), in split form. The convective eigenvalue lam_c = |dir| u.n has multiplicity D and the eigenvector
 // pairs satisfy sum_k r_k l_k^T = I, so
 //   K = op(lam_c) I + (op(lam_+) - op(lam_c)) r_+ l_+^T + (op(lam_-) - op(lam_c)) r_- l_-^T
 // where r_+- = rho/(2a) (1, V +- a n, H +- a u.n) and l_+- are the acoustic eigenvector pairs
@@ -290,7 +290,9 @@ __device__ __forceinline__ T euler_K_split(const EulerProps<T, D> &p,
     um = um + p.V[D - 1] * n[D - 1];
   const T a  = p.a;
   const T lc = norm * um, lp = norm * (um + a), lm = norm * (um - a);
-  auto op    = [](T x) -> T { return SIGN > 0 ? (x > T(0) ? x : T(0)) : (x < T(0) ? x : T(0)); };
+  auto op    = [](T x) -> T {
+    return SIGN > 0 ? (x > T(0) ? x : T(0)) : SIGN < 0 ? (x < T(0) ? x : T(0)) : x;
+  };
   const T oc = op(lc);
   const T ap = (op(lp) - oc) * c.ra, am = (op(lm) - oc) * c.ra;
   T rp[N], rm[N], lpv[N], lmv[N];

@@ -123,6 +123,7 @@ def lib():
         "rds_unpack_interface": ([vp, vp], ip),
         "rds_finish": ([vp, dp, ip, vp], ip),
         "rds_check": ([vp], ip),
+        "rds_element_jacobians": ([vp, ip, vp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -260,6 +261,20 @@ class PGRDMethodExplicit:
             return done.value, hist[:done.value]
         self._check(st)
         return done.value, hist[:done.value]
+
+    def element_jacobians(self, group: int = 0):
+        """PGLDA element Jacobians [ncells, ndof * neq, ndof * neq] of a cell group at the
+        current state (computed on the GPU, copied to the host)."""
+        import torch
+
+        g = self.problem.groups[group]
+        nr = g.ndof * self.problem.neq
+        jac = torch.empty((g.ncells, nr, nr), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        self._check(lib().rds_element_jacobians(self._ctx, int(group), C.c_void_p(jac.data_ptr())))
+        torch.cuda.ExternalStream(self.stream_handle()).synchronize()
+        self._check(lib().rds_check(self._ctx))
+        return jac.cpu().numpy()
 
     def set_option(self, key: str, value: float):
         self._check(lib().rds_set_option(self._ctx, key.encode(), float(value)))

@@ -1,0 +1,45 @@
+"""PGLDA element Jacobians of the oracle (oracle/rds_oracle.c rdso_element_jacobian, the
+restatement of PGLDA.hpp:316-536), pinned through the reference's residual: for constant
+advection the flux interpolant is exact, so J u equals the cell's scheme residual, which the
+golden cases pin to the reference itself."""
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle.rds_oracle import Oracle
+from pdekit_b200.problem import load_golden
+
+
+@pytest.mark.parametrize("case", ["adv_p1_lda", "adv_p1_lda_zero", "adv_p3_lda", "adv_p2_b"])
+def test_linear_advection_jacobian_reproduces_residual(case):
+    prob, a, _ = load_golden(os.path.join(GOLDEN, case))
+    prob.scheme = "lda"
+    o = Oracle(prob)
+    o.model.scheme = 0  # PGLDA residual for the comparison
+    g = prob.groups[0]
+    rng = np.random.default_rng(5)
+    for u in (np.asarray(a["u0"]), rng.standard_normal((prob.nnodes, 1))):
+        worst = 0.0
+        for c in range(g.ncells):
+            jac = o.element_jacobian(0, c, u)
+            res, _ = o.cell_residual(0, c, u)
+            un = u.reshape(-1, 1)[g.sol_conn[c]].ravel()
+            scale = max(np.abs(res).max(), np.abs(jac).max() * np.abs(un).max())
+            diff = np.abs(jac @ un - res.ravel()).max()
+            worst = max(worst, diff / scale if scale > 0 else diff)
+        assert worst < 1e-13
+
+
+def test_jacobian_annihilates_constant_states():
+    """sum_n grad phi_n = 0, so J maps a constant state to zero (Burgers, Euler)."""
+    for case in ("burgers_p2_lda", "euler2d_tri_p1_lda", "euler3d_tet_p2_lda"):
+        prob, a, _ = load_golden(os.path.join(GOLDEN, case))
+        o = Oracle(prob)
+        g = prob.groups[0]
+        u = np.asarray(a["u0"]).reshape(-1, prob.neq)
+        const = np.tile(u[0], g.ndof)
+        jac = o.element_jacobian(0, 0, np.tile(u[0], (prob.nnodes, 1)))
+        assert np.abs(jac @ const).max() <= 1e-10 * np.abs(jac).max() * np.abs(const).max()
