@@ -189,13 +189,15 @@ RDS_API rds_status rds_assemble_rhs(rds_ctx *ctx);
 RDS_API rds_status rds_update(rds_ctx *ctx);
 /* compute_residual_norm(): sqrt(sum_n (res_n dt_n)^2 / N) per equation, into norm[neq]. */
 RDS_API rds_status rds_residual_norm(rds_ctx *ctx, double *norm);
-/* Element Jacobians of the PGLDA scheme at the current state, as the reference's Picard-
- * linearised implicit solver assembles them (solver/rdm/cellsplitters/PGLDA.hpp:316-536,
- * called from solver/rdm/assembly/PGRDMPicardJacCellAssemblyWorker.hpp:370):
- * J_mn = sum_q w_q |J_q| K+_m (sum_k K+_k)^-1 K_n with K_n the unclipped upwind matrix.
+/* Element Jacobians of the PGLDA and PGN schemes at the current state, as the reference's
+ * Picard-linearised implicit solver assembles them (solver/rdm/cellsplitters/PGLDA.hpp:316-536,
+ * PGN.hpp:296-440, called from solver/rdm/assembly/PGRDMPicardJacCellAssemblyWorker.hpp:370):
+ * PGLDA J_mn = sum_q w_q |J_q| K+_m (sum_k K+_k)^-1 K_n (K_n the unclipped upwind matrix);
+ * PGN   J_mn = sum_q w_q |J_q| (delta_mn K+_m - K+_m (sum_k K-_k)^-1 K-_n) (the reference's
+ * implicit PGN is the plain N scheme).
  * jac: device array [ncells][ndof*neq][ndof*neq] of cell group 'group' (row m*neq + i, column
  * n*neq + j), before the division by the dual volumes. Asynchronous on the context's stream;
- * PGLDA contexts only (RDS_ERR_UNSUPPORTED otherwise). */
+ * RDS_ERR_UNSUPPORTED for PGB contexts. */
 RDS_API rds_status rds_element_jacobians(rds_ctx *ctx, int group, double *jac);
 
 /* Partitioned single mesh (no counterpart call in the reference, whose explicit solver runs

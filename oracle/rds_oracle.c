@@ -658,9 +658,11 @@ void rdso_cell_residual(const rdso_model *m, const rdso_cells *g, const double *
   cell_residual(m, g, X, un, elem_res, elem_ws);
 }
 
-/* PGLDA element Jacobian of the Picard linearisation (PGLDA.hpp:316-536):
- * J_mn += w_q |J_q| (Kp_m (sum Kp)^-1) K_n with Kp from build_K_mat(op = max(0,.)) and K_n
- * from build_K_mat(op = identity), accumulated point by point in the reference's order. */
+/* Element Jacobian of the Picard linearisation, accumulated point by point in the reference's
+ * order. PGLDA (PGLDA.hpp:316-536): J_mn += w_q |J_q| (Kp_m (sum Kp)^-1) K_n with Kp from
+ * build_K_mat(op = max(0,.)) and K_n from build_K_mat(op = identity). PGN (PGN.hpp:296-440,
+ * the plain N scheme): J_mn += w_q |J_q| (delta_mn Kp_m - Kp_m (sum Km)^-1 Km_n) with Kp, Km
+ * = R max/min(Lambda, 0) L. */
 void rdso_element_jacobian(const rdso_model *m, const rdso_cells *g, const double *X,
                            const double *un, double *jac)
 {
@@ -700,10 +702,10 @@ void rdso_element_jacobian(const rdso_model *m, const rdso_cells *g, const doubl
         gphys[x] = s;
       }
       build_K(m, &pq, gphys, +1, eig, Kp[n]);
-      build_K(m, &pq, gphys, 0, eig, Kn[n]);
+      build_K(m, &pq, gphys, m->scheme == RDSO_N ? -1 : 0, eig, Kn[n]);
       for (int i = 0; i < NEQ; ++i)
         for (int j = 0; j < NEQ; ++j)
-          sumKp[i][j] += Kp[n][i][j];
+          sumKp[i][j] += (m->scheme == RDSO_N) ? Kn[n][i][j] : Kp[n][i][j];
     }
     inverse(NEQ, sumKp, inv);
     for (int mm = 0; mm < ndof; ++mm)
@@ -724,6 +726,8 @@ void rdso_element_jacobian(const rdso_model *m, const rdso_cells *g, const doubl
             double s = B[i][0] * Kn[n][0][j];
             for (int k = 1; k < NEQ; ++k)
               s = s + B[i][k] * Kn[n][k][j];
+            if (m->scheme == RDSO_N)
+              s = (n == mm ? Kp[mm][i][j] : 0.0) - s;
             jac[(size_t)(mm * NEQ + i) * NR + n * NEQ + j] += wj * s;
           }
     }

@@ -165,7 +165,8 @@ class Oracle:
         return res, ws
 
     def element_jacobian(self, group, cell, u):
-        """PGLDA element Jacobian [ndof * neq, ndof * neq] of one cell at the state u."""
+        """Element Jacobian [ndof * neq, ndof * neq] of one cell at the state u (PGLDA, or PGN
+        when the problem's scheme is "n")."""
         prob, g = self.prob, self.prob.groups[group]
         X = np.ascontiguousarray(prob.geo_coords[g.geo_conn[cell]], dtype=np.float64)
         un = np.ascontiguousarray(np.asarray(u).reshape(-1, prob.neq)[g.sol_conn[cell]])

@@ -992,15 +992,16 @@ rds_status rds_element_jacobians(rds_ctx *ctx, int group, double *jac)
   if (!ctx || !jac || !ctx->finalized || group < 0 || group >= (int)ctx->groups.size())
     return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_element_jacobians: invalid group or not finalized")
                : RDS_ERR_INVALID;
-  if (ctx->desc.scheme != RDS_PGLDA)
-    return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_element_jacobians: PGLDA contexts only");
+  if (ctx->desc.scheme == RDS_PGB)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_element_jacobians: PGLDA and PGN contexts only");
   if (ctx->nprob > 0)
     return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_element_jacobians: not in batched contexts");
   const HostCellGroup &g = ctx->groups[group];
   const CellArgs a       = cell_args(ctx, g, ctx->d_zero);
   return launch(ctx, [&](const char **name) {
     *name = "cells_jacobian";
-    return launch_jacobians(g, a, g.physics, ctx->desc.dim, ctx->desc.neq, jac, ctx->stream);
+    return launch_jacobians(g, a, g.physics, ctx->desc.scheme, ctx->desc.dim, ctx->desc.neq, jac,
+                            ctx->stream);
   });
 }
 

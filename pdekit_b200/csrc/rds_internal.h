@@ -245,9 +245,9 @@ cudaError_t launch_cells_scalar_tc(const HostCellGroup &g, const CellArgs &a, bo
                                    int ntiles, cudaStream_t s, const char **name, bool *ok);
 cudaError_t launch_update(int nnodes, int neq, const double *dt, const double *res, double *u,
                           cudaStream_t s, const char **name);
-// PGLDA element Jacobians (rds_jacobian.cu): jac [ncells][ndof*neq][ndof*neq]
-cudaError_t launch_jacobians(const HostCellGroup &g, const CellArgs &a, int physics, int dim,
-                             int neq, double *jac, cudaStream_t s);
+// PGLDA / PGN element Jacobians (rds_jacobian.cu): jac [ncells][ndof*neq][ndof*neq]
+cudaError_t launch_jacobians(const HostCellGroup &g, const CellArgs &a, int physics, int scheme,
+                             int dim, int neq, double *jac, cudaStream_t s);
 
 // partitioned single mesh (rds_partition.cu)
 cudaError_t launch_pack_interface(int n, int neq, int nnodes, const int32_t *nodes,

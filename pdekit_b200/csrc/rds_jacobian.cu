@@ -1,13 +1,15 @@
-// Element Jacobians of the PGLDA scheme, the matrices the reference's Picard-linearised implicit
-// solver assembles (src/solver/rdm/cellsplitters/PGLDA.hpp:316-536, called from
-// src/solver/rdm/assembly/PGRDMPicardJacCellAssemblyWorker.hpp:370):
+// Element Jacobians of the PGLDA and PGN schemes, the matrices the reference's Picard-linearised
+// implicit solver assembles (src/solver/rdm/cellsplitters/PGLDA.hpp:316-536, PGN.hpp:296-440,
+// called from src/solver/rdm/assembly/PGRDMPicardJacCellAssemblyWorker.hpp:370):
 //
-//   J_mn = sum_q w_q |J_q| (K+_m (sum_k K+_k)^-1) K_n,     K_n = A(u_q) . grad phi_n(x_q),
+//   PGLDA  J_mn = sum_q w_q |J_q| (K+_m (sum_k K+_k)^-1) K_n
+//   PGN    J_mn = sum_q w_q |J_q| (delta_mn K+_m - K+_m (sum_k K-_k)^-1 K-_n)
 //
-// with K+_n = R max(Lambda, 0) L as in the residual and K_n the unclipped upwind matrix (the flux
-// Jacobian in direction grad phi_n). One thread per (cell, row node m). Scalar physics keep the
-// row in registers; Euler rows (NEQ x NDOF NEQ) are accumulated in the thread's own rows of the
-// output, point by point. The output is [cell][ndof * neq][ndof * neq], row-major per cell, the
+// with K+- = R max/min(Lambda, 0) L as in the residual and K_n the unclipped upwind matrix (the
+// flux Jacobian in direction grad phi_n); the implicit PGN of the reference is the plain N
+// scheme (its explicit PGN adds the N dissipation to LDA instead). One thread per (cell, row
+// node m). Scalar physics keep the row in registers; Euler rows (NEQ x NDOF NEQ) are accumulated
+// in the thread's own rows of the output, point by point. The output is [cell][ndof * neq][ndof * neq], row-major per cell, the
 // element matrix before the division by the dual volumes that the reference applies when it
 // assembles the global matrix.
 
@@ -127,7 +129,7 @@ __device__ __forceinline__ double inv_jacobian(const Tables<double, D, NDOF, NQ,
   }
 }
 
-template <int PHYS, int D, int NEQ, int NDOF, int NQ, int NFL, int NGEO, bool AFFINE>
+template <int PHYS, int SCHEME, int D, int NEQ, int NDOF, int NQ, int NFL, int NGEO, bool AFFINE>
 __global__ void __launch_bounds__(kBlock)
     cells_jacobian(const CellArgs a, const __grid_constant__ Tables<double, D, NDOF, NQ, NFL, NGEO> tb,
                    double *__restrict__ jac)
@@ -180,7 +182,7 @@ __global__ void __launch_bounds__(kBlock)
         ax = uq;
         ay = 1.0;
       }
-      double k[NDOF], sumkp = 0.0, kpm = 0.0;
+      double k[NDOF], sumk = 0.0, kpm = 0.0;
 #pragma unroll
       for (int n = 0; n < NDOF; ++n)
       {
@@ -188,14 +190,25 @@ __global__ void __launch_bounds__(kBlock)
         const double gy = ij[1][0] * tb.dV[0][q][n] + ij[1][1] * tb.dV[1][q][n];
         k[n]            = ax * gx + ay * gy;
         const double kp = k[n] > 0.0 ? k[n] : 0.0;
-        sumkp += kp;
+        if (SCHEME == RDS_PGN)
+          sumk += k[n] < 0.0 ? k[n] : 0.0; // sum of K-
+        else
+          sumk += kp; // sum of K+
         if (n == m)
           kpm = kp;
       }
-      const double beta = kpm * (1.0 / sumkp);
+      const double beta = kpm * (1.0 / sumk);
 #pragma unroll
       for (int n = 0; n < NDOF; ++n)
-        row[n] += wj * (beta * k[n]);
+      {
+        if (SCHEME == RDS_PGN)
+        {
+          const double km = k[n] < 0.0 ? k[n] : 0.0;
+          row[n] += wj * ((n == m ? kpm : 0.0) - beta * km);
+        }
+        else
+          row[n] += wj * (beta * k[n]);
+      }
     }
 #pragma unroll
     for (int n = 0; n < NDOF; ++n)
@@ -250,19 +263,25 @@ __global__ void __launch_bounds__(kBlock)
         double g[D], K[NEQ][NEQ];
         grad(n, g);
         euler_K_split<+1, double, D>(p, ac, g, K);
+        if (n == m)
+        {
+#pragma unroll
+          for (int i = 0; i < NEQ; ++i)
+#pragma unroll
+            for (int j = 0; j < NEQ; ++j)
+              Km[i][j] = K[i][j];
+        }
+        if (SCHEME == RDS_PGN)
+          euler_K_split<-1, double, D>(p, ac, g, K);
 #pragma unroll
         for (int i = 0; i < NEQ; ++i)
 #pragma unroll
           for (int j = 0; j < NEQ; ++j)
-          {
             SK[i][j] += K[i][j];
-            if (n == m)
-              Km[i][j] = K[i][j];
-          }
       }
       double inv[NEQ][NEQ];
       gj_inverse<NEQ>(SK, inv);
-      double B[NEQ][NEQ]; // K+_m (sum K+)^-1
+      double B[NEQ][NEQ]; // K+_m (sum K+)^-1, PGN: K+_m (sum K-)^-1
 #pragma unroll
       for (int i = 0; i < NEQ; ++i)
 #pragma unroll
@@ -278,7 +297,10 @@ __global__ void __launch_bounds__(kBlock)
       {
         double g[D], K[NEQ][NEQ];
         grad(n, g);
-        euler_K_split<0, double, D>(p, ac, g, K);
+        if (SCHEME == RDS_PGN)
+          euler_K_split<-1, double, D>(p, ac, g, K);
+        else
+          euler_K_split<0, double, D>(p, ac, g, K);
 #pragma unroll
         for (int i = 0; i < NEQ; ++i)
 #pragma unroll
@@ -288,14 +310,15 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
             for (int k = 0; k < NEQ; ++k)
               s += B[i][k] * K[k][j];
-            rows[(size_t)i * NR + n * NEQ + j] += wj * s;
+            const double v = (SCHEME == RDS_PGN) ? ((n == m ? Km[i][j] : 0.0) - s) : s;
+            rows[(size_t)i * NR + n * NEQ + j] += wj * v;
           }
       }
     }
   }
 }
 
-template <int PHYS, int D, int NEQ, int NDOF, int NQ, int NFL, int NGEO>
+template <int PHYS, int SCHEME, int D, int NEQ, int NDOF, int NQ, int NFL, int NGEO>
 cudaError_t launch_jac(const HostCellGroup &g, const CellArgs &a, double *jac, cudaStream_t s)
 {
   Tables<double, D, NDOF, NQ, NFL, NGEO> tb;
@@ -303,13 +326,13 @@ cudaError_t launch_jac(const HostCellGroup &g, const CellArgs &a, double *jac, c
   const long long nt = (long long)a.ncells * NDOF;
   const unsigned grid = (unsigned)((nt + kBlock - 1) / kBlock);
   if (g.affine)
-    cells_jacobian<PHYS, D, NEQ, NDOF, NQ, NFL, NGEO, true><<<grid, kBlock, 0, s>>>(a, tb, jac);
+    cells_jacobian<PHYS, SCHEME, D, NEQ, NDOF, NQ, NFL, NGEO, true><<<grid, kBlock, 0, s>>>(a, tb, jac);
   else
-    cells_jacobian<PHYS, D, NEQ, NDOF, NQ, NFL, NGEO, false><<<grid, kBlock, 0, s>>>(a, tb, jac);
+    cells_jacobian<PHYS, SCHEME, D, NEQ, NDOF, NQ, NFL, NGEO, false><<<grid, kBlock, 0, s>>>(a, tb, jac);
   return cudaGetLastError();
 }
 
-template <int PHYS, int D, int NEQ>
+template <int PHYS, int SCHEME, int D, int NEQ>
 cudaError_t dispatch_jac(const HostCellGroup &g, const CellArgs &a, double *jac, cudaStream_t s,
                          bool *ok)
 {
@@ -317,7 +340,7 @@ cudaError_t dispatch_jac(const HostCellGroup &g, const CellArgs &a, double *jac,
   *ok                     = true;
 #define RDS_JAC(SHAPE, NGEO, NDOF, NQ, NFL)                                                        \
   if (d.shape == SHAPE && d.ngeo == NGEO && d.ndof == NDOF && d.nq == NQ && d.nfl == NFL)         \
-    return launch_jac<PHYS, D, NEQ, NDOF, NQ, NFL, NGEO>(g, a, jac, s);
+    return launch_jac<PHYS, SCHEME, D, NEQ, NDOF, NQ, NFL, NGEO>(g, a, jac, s);
   if constexpr (D == 2)
   {
     RDS_JAC(RDS_TRIAG, 3, 3, 6, 6)
@@ -343,19 +366,24 @@ cudaError_t dispatch_jac(const HostCellGroup &g, const CellArgs &a, double *jac,
 
 } // namespace
 
-cudaError_t launch_jacobians(const HostCellGroup &g, const CellArgs &a, int physics, int dim,
-                             int neq, double *jac, cudaStream_t s)
+cudaError_t launch_jacobians(const HostCellGroup &g, const CellArgs &a, int physics, int scheme,
+                             int dim, int neq, double *jac, cudaStream_t s)
 {
   bool ok         = false;
   cudaError_t err = cudaSuccess;
+  const bool n    = scheme == RDS_PGN;
   if (physics == RDS_ADVECTION_CONST && dim == 2 && neq == 1)
-    err = dispatch_jac<RDS_ADVECTION_CONST, 2, 1>(g, a, jac, s, &ok);
+    err = n ? dispatch_jac<RDS_ADVECTION_CONST, RDS_PGN, 2, 1>(g, a, jac, s, &ok)
+            : dispatch_jac<RDS_ADVECTION_CONST, RDS_PGLDA, 2, 1>(g, a, jac, s, &ok);
   else if (physics == RDS_BURGERS2D && dim == 2 && neq == 1)
-    err = dispatch_jac<RDS_BURGERS2D, 2, 1>(g, a, jac, s, &ok);
+    err = n ? dispatch_jac<RDS_BURGERS2D, RDS_PGN, 2, 1>(g, a, jac, s, &ok)
+            : dispatch_jac<RDS_BURGERS2D, RDS_PGLDA, 2, 1>(g, a, jac, s, &ok);
   else if (physics == RDS_EULER2D && dim == 2 && neq == 4)
-    err = dispatch_jac<RDS_EULER2D, 2, 4>(g, a, jac, s, &ok);
+    err = n ? dispatch_jac<RDS_EULER2D, RDS_PGN, 2, 4>(g, a, jac, s, &ok)
+            : dispatch_jac<RDS_EULER2D, RDS_PGLDA, 2, 4>(g, a, jac, s, &ok);
   else if (physics == RDS_EULER3D && dim == 3 && neq == 5)
-    err = dispatch_jac<RDS_EULER3D, 3, 5>(g, a, jac, s, &ok);
+    err = n ? dispatch_jac<RDS_EULER3D, RDS_PGN, 3, 5>(g, a, jac, s, &ok)
+            : dispatch_jac<RDS_EULER3D, RDS_PGLDA, 3, 5>(g, a, jac, s, &ok);
   if (!ok)
     return cudaErrorNotSupported;
   return err;

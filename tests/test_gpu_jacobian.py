@@ -14,8 +14,8 @@ from pdekit_b200.rds import PGRDMethodExplicit, RDSError
 pytestmark = pytest.mark.gpu
 
 
-def _jacobians(prob, u):
-    s = PGRDMethodExplicit(prob.physics, "lda", "fp64").configure_mesh_data(prob)
+def _jacobians(prob, u, scheme="lda"):
+    s = PGRDMethodExplicit(prob.physics, scheme, "fp64").configure_mesh_data(prob)
     s.initialize_work_data()
     s.set_solution(u)
     jac = [s.element_jacobians(ig) for ig in range(len(prob.groups))]
@@ -49,7 +49,20 @@ def test_linear_advection_identity_on_gpu():
         assert np.abs(jac[c] @ un - res[:, 0]).max() <= 1e-12 * np.abs(jac[c]).max() * 4
 
 
-def test_element_jacobians_need_pglda():
+@pytest.mark.parametrize("case", ["adv_p1_n", "burgers_p2_n", "euler2d_tri_p2_n",
+                                  "euler2d_quad_p3_b", "euler3d_tet_p2_lda"])
+def test_n_scheme_element_jacobians_match_oracle(case):
+    prob, a, _ = load_golden(os.path.join(GOLDEN, case))
+    prob.scheme = "n"
+    u = np.asarray(a["u0"])
+    jac = _jacobians(prob, u, "n")[0]
+    o = Oracle(prob)
+    o.model.scheme = 1
+    ref = np.stack([o.element_jacobian(0, c, u) for c in range(prob.groups[0].ncells)])
+    assert np.abs(jac - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_element_jacobians_need_pglda_or_pgn():
     prob, a, _ = load_golden(os.path.join(GOLDEN, "burgers_p2_b"))
     s = PGRDMethodExplicit(prob.physics, "b", "fp64").configure_mesh_data(prob)
     s.initialize_work_data()

@@ -43,3 +43,24 @@ def test_jacobian_annihilates_constant_states():
         const = np.tile(u[0], g.ndof)
         jac = o.element_jacobian(0, 0, np.tile(u[0], (prob.nnodes, 1)))
         assert np.abs(jac @ const).max() <= 1e-10 * np.abs(jac).max() * np.abs(const).max()
+
+
+@pytest.mark.parametrize("case", ["adv_p1_n", "adv_p2_b"])
+def test_n_scheme_jacobian_is_the_n_residual_operator(case):
+    """Implicit PGN (the plain N scheme): J u equals sum_q w |J| sum_{n != m} K+_m (sum K-)^-1
+    K-_n (u_m - u_n), evaluated here from the same frozen upwind coefficients; and J has zero
+    row sums (constant states give no residual)."""
+    prob, a, _ = load_golden(os.path.join(GOLDEN, case))
+    prob.scheme = "n"
+    o = Oracle(prob)
+    o.model.scheme = 1
+    g = prob.groups[0]
+    u = np.asarray(a["u0"]).reshape(-1)
+    for c in range(g.ncells):
+        jac = o.element_jacobian(0, c, u)
+        assert np.abs(jac.sum(axis=1)).max() <= 1e-13 * np.abs(jac).max()
+        # J u with u_m - u_n differences: sum_n J_mn u_n = sum_n J_mn (u_n - u_m) since rows sum
+        # to zero, i.e. only differences of the state enter, as in the N scheme
+        un = u[g.sol_conn[c]]
+        d = jac @ un - np.array([jac[mm] @ (un - un[mm]) for mm in range(g.ndof)])
+        assert np.abs(d).max() <= 1e-12 * max(np.abs(jac).max() * np.abs(un).max(), 1e-300)
