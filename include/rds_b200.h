@@ -200,6 +200,19 @@ RDS_API rds_status rds_residual_norm(rds_ctx *ctx, double *norm);
  * RDS_ERR_UNSUPPORTED for PGB contexts. */
 RDS_API rds_status rds_element_jacobians(rds_ctx *ctx, int group, double *jac);
 
+/* The same Jacobians assembled into a block-CSR matrix over the solution nodes, as the
+ * reference's Picard worker hands them to its sparse matrix (PGRDMPicardJacCellAssemblyWorker.hpp:
+ * 392-412): block (v, w) (neq x neq) = sum over the cells holding nodes v and w of the (v, w)
+ * block of their element matrix, each entry divided by the dual volume of v. No Dirichlet rows
+ * are removed and no boundary terms are added.
+ *   rds_jacobian_pattern: nnzb (number of blocks) and, when not NULL, row_ptr [nnodes + 1] and
+ *     col_idx [nnzb] (host arrays; columns ascending within a row). Built on the first call.
+ *   rds_assemble_jacobian: values (device array [nnzb][neq][neq], row-major blocks) at the
+ *     current state. Asynchronous on the context's stream; PGLDA / PGN contexts. */
+RDS_API rds_status rds_jacobian_pattern(rds_ctx *ctx, int64_t *nnzb, int32_t *row_ptr,
+                                        int32_t *col_idx);
+RDS_API rds_status rds_assemble_jacobian(rds_ctx *ctx, double *values);
+
 /* Partitioned single mesh (no counterpart call in the reference, whose explicit solver runs
  * one mesh per process): one context per rank holds a part of the cells and the nodes they
  * touch, renumbered; the ranks add their partial nodal sums at the nodes they share.

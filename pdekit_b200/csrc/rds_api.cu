@@ -60,6 +60,16 @@ struct rds_ctx
   int gblocks   = 0;
   int hist_cap  = 0;
 
+  // sparse (block CSR) Jacobian: pattern over node pairs, per-block contribution lists into
+  // the element-Jacobian buffer (built on first use)
+  bool jp_built = false;
+  long long jp_nnzb = 0, jp_njac = 0;
+  std::vector<int32_t> jp_row_ptr, jp_col_idx;
+  std::vector<long long> jp_gbase;
+  int32_t *d_jp_brow = nullptr, *d_jp_cnr = nullptr;
+  int64_t *d_jp_cptr = nullptr, *d_jp_coff = nullptr;
+  double *d_jp_jac = nullptr;
+
   // partitioned single mesh: the nodes this rank shares with others, their slots in the
   // exchange buffer, and the nodes whose (res dt)^2 this rank counts in the norm
   int32_t *d_if_nodes = nullptr, *d_if_slots = nullptr;
@@ -1005,6 +1015,132 @@ rds_status rds_element_jacobians(rds_ctx *ctx, int group, double *jac)
   });
 }
 
+// ---- sparse Jacobian ---------------------------------------------------------------------
+
+// Block pattern of the assembled Jacobian: block (v, w) exists when a cell holds both nodes;
+// its contributions are the (m(v), n(w)) blocks of those cells' element matrices, in ascending
+// group and cell order.
+static rds_status build_jac_pattern(rds_ctx *ctx)
+{
+  if (ctx->jp_built)
+    return RDS_OK;
+  const long long N = ctx->desc.nnodes;
+  const int NEQ     = ctx->desc.neq;
+  struct Contrib
+  {
+    long long key, off;
+    int32_t nr;
+  };
+  std::vector<Contrib> t;
+  long long total = 0, base = 0;
+  for (const HostCellGroup &g : ctx->groups)
+    total += (long long)g.desc.ncells * g.desc.ndof * g.desc.ndof;
+  t.reserve((size_t)total);
+  ctx->jp_gbase.clear();
+  for (const HostCellGroup &g : ctx->groups)
+  {
+    const int nc = g.desc.ncells, nd = g.desc.ndof, NR = nd * NEQ;
+    std::vector<int32_t> conn((size_t)nc * nd);
+    RDS_CUDA(cudaMemcpy(conn.data(), g.d_sol_conn, conn.size() * 4, cudaMemcpyDeviceToHost));
+    ctx->jp_gbase.push_back(base);
+    for (int c = 0; c < nc; ++c)
+      for (int m = 0; m < nd; ++m)
+        for (int n = 0; n < nd; ++n)
+        {
+          const long long v = conn[(size_t)m * nc + c], w = conn[(size_t)n * nc + c];
+          t.push_back({v * N + w,
+                       base + (long long)c * NR * NR + (long long)m * NEQ * NR + (long long)n * NEQ,
+                       NR});
+        }
+    base += (long long)nc * NR * NR;
+  }
+  ctx->jp_njac = base;
+  std::stable_sort(t.begin(), t.end(),
+                   [](const Contrib &a, const Contrib &b) { return a.key < b.key; });
+  std::vector<int32_t> brow, cnr(t.size());
+  std::vector<int64_t> cptr, coff(t.size());
+  ctx->jp_row_ptr.assign((size_t)N + 1, 0);
+  ctx->jp_col_idx.clear();
+  for (size_t k = 0; k < t.size(); ++k)
+  {
+    if (k == 0 || t[k].key != t[k - 1].key)
+    {
+      const long long v = t[k].key / N, w = t[k].key % N;
+      brow.push_back((int32_t)v);
+      ctx->jp_col_idx.push_back((int32_t)w);
+      ctx->jp_row_ptr[(size_t)v + 1]++;
+      cptr.push_back((int64_t)k);
+    }
+    coff[k] = t[k].off;
+    cnr[k]  = t[k].nr;
+  }
+  cptr.push_back((int64_t)t.size());
+  for (long long v = 0; v < N; ++v)
+    ctx->jp_row_ptr[(size_t)v + 1] += ctx->jp_row_ptr[(size_t)v];
+  ctx->jp_nnzb = (long long)brow.size();
+  rds_status st;
+  if ((st = dalloc(ctx, &ctx->d_jp_brow, brow.size())) != RDS_OK ||
+      (st = dalloc(ctx, &ctx->d_jp_cptr, cptr.size())) != RDS_OK ||
+      (st = dalloc(ctx, &ctx->d_jp_coff, coff.size())) != RDS_OK ||
+      (st = dalloc(ctx, &ctx->d_jp_cnr, cnr.size())) != RDS_OK ||
+      (st = dalloc(ctx, &ctx->d_jp_jac, (size_t)ctx->jp_njac)) != RDS_OK)
+    return st;
+  if ((st = upload(ctx, ctx->d_jp_brow, brow.data(), brow.size())) != RDS_OK ||
+      (st = upload(ctx, ctx->d_jp_cptr, cptr.data(), cptr.size())) != RDS_OK ||
+      (st = upload(ctx, ctx->d_jp_coff, coff.data(), coff.size())) != RDS_OK ||
+      (st = upload(ctx, ctx->d_jp_cnr, cnr.data(), cnr.size())) != RDS_OK)
+    return st;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->jp_built = true;
+  return RDS_OK;
+}
+
+rds_status rds_jacobian_pattern(rds_ctx *ctx, int64_t *nnzb, int32_t *row_ptr, int32_t *col_idx)
+{
+  if (!ctx || !nnzb || !ctx->finalized || ctx->nprob > 0)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_jacobian_pattern: not a finalized single context")
+               : RDS_ERR_INVALID;
+  rds_status st = build_jac_pattern(ctx);
+  if (st != RDS_OK)
+    return st;
+  *nnzb = ctx->jp_nnzb;
+  if (row_ptr)
+    std::copy(ctx->jp_row_ptr.begin(), ctx->jp_row_ptr.end(), row_ptr);
+  if (col_idx)
+    std::copy(ctx->jp_col_idx.begin(), ctx->jp_col_idx.end(), col_idx);
+  return RDS_OK;
+}
+
+rds_status rds_assemble_jacobian(rds_ctx *ctx, double *values)
+{
+  if (!ctx || !values || !ctx->finalized || ctx->nprob > 0)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_assemble_jacobian: not a finalized single context")
+               : RDS_ERR_INVALID;
+  if (ctx->desc.scheme == RDS_PGB)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_assemble_jacobian: PGLDA and PGN contexts only");
+  rds_status st = build_jac_pattern(ctx);
+  if (st != RDS_OK)
+    return st;
+  for (size_t ig = 0; ig < ctx->groups.size(); ++ig)
+  {
+    const HostCellGroup &g = ctx->groups[ig];
+    const CellArgs a       = cell_args(ctx, g, ctx->d_zero);
+    st = launch(ctx, [&](const char **name) {
+      *name = "cells_jacobian";
+      return launch_jacobians(g, a, g.physics, ctx->desc.scheme, ctx->desc.dim, ctx->desc.neq,
+                              ctx->d_jp_jac + ctx->jp_gbase[ig], ctx->stream);
+    });
+    if (st != RDS_OK)
+      return st;
+  }
+  return launch(ctx, [&](const char **name) {
+    *name = "assemble_bsr";
+    return launch_assemble_bsr(ctx->jp_nnzb, ctx->desc.neq, ctx->d_jp_brow, ctx->d_jp_cptr,
+                               ctx->d_jp_coff, ctx->d_jp_cnr, ctx->d_jp_jac, ctx->d_vol, values,
+                               ctx->stream);
+  });
+}
+
 // ---- partitioned single mesh ------------------------------------------------------------
 
 rds_status rds_set_dual_volume(rds_ctx *ctx, const double *vol)
@@ -1822,6 +1958,11 @@ rds_status rds_destroy(rds_ctx *ctx)
   cudaFree(ctx->d_if_nodes);
   cudaFree(ctx->d_if_slots);
   cudaFree(ctx->d_owned);
+  cudaFree(ctx->d_jp_brow);
+  cudaFree(ctx->d_jp_cnr);
+  cudaFree(ctx->d_jp_cptr);
+  cudaFree(ctx->d_jp_coff);
+  cudaFree(ctx->d_jp_jac);
   void *bufs[] = {ctx->d_X,     ctx->d_u,     ctx->d_res,     ctx->d_ws,       ctx->d_dt,
                   ctx->d_vol,   ctx->d_inv_vol, ctx->d_contrib, ctx->d_wsc,    ctx->d_stage,
                   ctx->d_row,   ctx->d_ent_slot, ctx->d_ent_ws, ctx->d_part,   ctx->d_norm,

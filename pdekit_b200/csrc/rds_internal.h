@@ -249,6 +249,10 @@ cudaError_t launch_update(int nnodes, int neq, const double *dt, const double *r
 cudaError_t launch_jacobians(const HostCellGroup &g, const CellArgs &a, int physics, int scheme,
                              int dim, int neq, double *jac, cudaStream_t s);
 
+cudaError_t launch_assemble_bsr(long long nnzb, int neq, const int32_t *brow, const int64_t *cptr,
+                                const int64_t *coff, const int32_t *cnr, const double *jac,
+                                const double *vol, double *values, cudaStream_t s);
+
 // partitioned single mesh (rds_partition.cu)
 cudaError_t launch_pack_interface(int n, int neq, int nnodes, const int32_t *nodes,
                                   const int32_t *slots, const double *res, const double *ws,

@@ -364,7 +364,43 @@ cudaError_t dispatch_jac(const HostCellGroup &g, const CellArgs &a, double *jac,
   return cudaSuccess;
 }
 
+// Block-CSR assembly: entry (i, j) of block b (row node v) = sum over the block's contributions
+// k (in ascending group and cell order) of jac[off_k + i * nr_k + j] / V_v, each element entry
+// scaled by the row node's inverse dual volume before the sum, as the reference hands them to its
+// sparse matrix (PGRDMPicardJacCellAssemblyWorker.hpp:392-412).
+__global__ void __launch_bounds__(kBlock)
+    assemble_bsr(long long nvals, int neq, const int32_t *__restrict__ brow,
+                 const int64_t *__restrict__ cptr, const int64_t *__restrict__ coff,
+                 const int32_t *__restrict__ cnr, const double *__restrict__ jac,
+                 const double *__restrict__ vol, double *__restrict__ values)
+{
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nvals)
+    return;
+  const int bs         = neq * neq;
+  const long long b    = t / bs;
+  const int r          = (int)(t % bs);
+  const int ei = r / neq, ej = r % neq;
+  const double iv      = 1. / vol[brow[b]];
+  double s             = 0.0;
+  for (long long k = cptr[b]; k < cptr[b + 1]; ++k)
+    s += iv * jac[coff[k] + (long long)ei * cnr[k] + ej];
+  values[t] = s;
+}
+
 } // namespace
+
+cudaError_t launch_assemble_bsr(long long nnzb, int neq, const int32_t *brow, const int64_t *cptr,
+                                const int64_t *coff, const int32_t *cnr, const double *jac,
+                                const double *vol, double *values, cudaStream_t s)
+{
+  const long long nvals = nnzb * neq * neq;
+  if (nvals == 0)
+    return cudaSuccess;
+  assemble_bsr<<<(unsigned)((nvals + kBlock - 1) / kBlock), kBlock, 0, s>>>(
+      nvals, neq, brow, cptr, coff, cnr, jac, vol, values);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_jacobians(const HostCellGroup &g, const CellArgs &a, int physics, int scheme,
                              int dim, int neq, double *jac, cudaStream_t s)

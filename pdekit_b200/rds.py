@@ -124,6 +124,8 @@ def lib():
         "rds_finish": ([vp, dp, ip, vp], ip),
         "rds_check": ([vp], ip),
         "rds_element_jacobians": ([vp, ip, vp], ip),
+        "rds_jacobian_pattern": ([vp, vp, vp, vp], ip),
+        "rds_assemble_jacobian": ([vp, vp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -275,6 +277,25 @@ class PGRDMethodExplicit:
         torch.cuda.ExternalStream(self.stream_handle()).synchronize()
         self._check(lib().rds_check(self._ctx))
         return jac.cpu().numpy()
+
+    def assemble_jacobian(self):
+        """Block-CSR Jacobian at the current state: (row_ptr [n + 1], col_idx [nnzb],
+        values [nnzb, neq, neq]), block (v, w) divided by the dual volume of v."""
+        import torch
+
+        nnzb = C.c_int64(0)
+        self._check(lib().rds_jacobian_pattern(self._ctx, C.byref(nnzb), None, None))
+        row_ptr = np.zeros(self.problem.nnodes + 1, dtype=np.int32)
+        col_idx = np.zeros(nnzb.value, dtype=np.int32)
+        self._check(lib().rds_jacobian_pattern(self._ctx, C.byref(nnzb), _ptr(row_ptr),
+                                               _ptr(col_idx)))
+        neq = self.problem.neq
+        vals = torch.empty((nnzb.value, neq, neq), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        self._check(lib().rds_assemble_jacobian(self._ctx, C.c_void_p(vals.data_ptr())))
+        torch.cuda.ExternalStream(self.stream_handle()).synchronize()
+        self._check(lib().rds_check(self._ctx))
+        return row_ptr, col_idx, vals.cpu().numpy()
 
     def set_option(self, key: str, value: float):
         self._check(lib().rds_set_option(self._ctx, key.encode(), float(value)))

@@ -1,6 +1,8 @@
-"""PGLDA element Jacobians on the GPU (rds_element_jacobians) against the oracle, and the linear
-advection identity J u = cell residual (pinned to the reference by the golden cases)."""
+"""PGLDA / PGN element Jacobians on the GPU (rds_element_jacobians) and their block-CSR assembly
+(rds_jacobian_pattern, rds_assemble_jacobian) against the oracle, and the linear advection
+identity J u = cell residual (pinned to the reference by the golden cases)."""
 
+import dataclasses
 import os
 
 import numpy as np
@@ -70,3 +72,61 @@ def test_element_jacobians_need_pglda_or_pgn():
         s.element_jacobians(0)
     assert e.value.status == 6
     s.close()
+
+
+def _dense(row_ptr, col_idx, vals, n, neq):
+    A = np.zeros((n * neq, n * neq))
+    for v in range(n):
+        for k in range(row_ptr[v], row_ptr[v + 1]):
+            w = col_idx[k]
+            A[v * neq:(v + 1) * neq, w * neq:(w + 1) * neq] = vals[k]
+    return A
+
+
+def _assembled(prob, u, scheme):
+    s = PGRDMethodExplicit(prob.physics, scheme, "fp64").configure_mesh_data(prob)
+    s.initialize_work_data()
+    s.set_solution(u)
+    out = s.assemble_jacobian()
+    s.close()
+    return out
+
+
+@pytest.mark.parametrize("case,scheme", [("adv_p2_b", "lda"), ("burgers_p2_n", "n"),
+                                         ("euler2d_tri_p1_lda", "lda"),
+                                         ("euler3d_tet_p2_lda", "n")])
+def test_assembled_jacobian_matches_oracle_elements(case, scheme):
+    prob, a, _ = load_golden(os.path.join(GOLDEN, case))
+    prob.scheme = scheme
+    u = np.asarray(a["u0"])
+    row_ptr, col_idx, vals = _assembled(prob, u, scheme)
+    n, neq = prob.nnodes, prob.neq
+    assert row_ptr[0] == 0 and row_ptr[-1] == len(col_idx)
+    for v in range(n):
+        cols = col_idx[row_ptr[v]:row_ptr[v + 1]]
+        assert np.all(np.diff(cols) > 0) and v in cols
+    o = Oracle(prob)
+    o.model.scheme = {"lda": 0, "n": 1}[scheme]
+    g = prob.groups[0]
+    ref = np.zeros((n * neq, n * neq))
+    for c in range(g.ncells):
+        jac = o.element_jacobian(0, c, u)
+        d = g.sol_conn[c]
+        for m in range(g.ndof):
+            for k in range(g.ndof):
+                ref[d[m] * neq:(d[m] + 1) * neq, d[k] * neq:(d[k] + 1) * neq] += \
+                    jac[m * neq:(m + 1) * neq, k * neq:(k + 1) * neq] / o.vol[d[m]]
+    A = _dense(row_ptr, col_idx, vals, n, neq)
+    assert np.abs(A - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_assembled_advection_jacobian_applies_the_cell_residual():
+    """For constant advection (PGLDA) the assembled operator times the state is the nodal
+    residual of the cells (the golden cases pin that residual to the reference)."""
+    prob, a, meta = load_golden(os.path.join(GOLDEN, "adv_p3_lda"))
+    u = np.random.default_rng(4).standard_normal((prob.nnodes, 1))
+    row_ptr, col_idx, vals = _assembled(prob, u, "lda")
+    A = _dense(row_ptr, col_idx, vals, prob.nnodes, 1)
+    cells_only = dataclasses.replace(prob, bcs=[])
+    res, _, _, _ = Oracle(cells_only).assemble(u, meta["cfl"])
+    assert np.abs(A @ u[:, 0] - res[:, 0]).max() <= 1e-12 * np.abs(A).max() * np.abs(u).max() * 8
