@@ -20,9 +20,10 @@
  * GPU sees exactly the reference's tables. nb_threads and nb_blocks are accepted and ignored.
  *
  * Scope: physics Burgers2D, Euler2DCons, Euler3DCons and RotationAdvection2D with a constant
- * direction; schemes PGLDA, PGN, PGB; weak boundary conditions WeakDirichlet (expression of the
+ * direction; schemes PGLDA, PGN, PGB; boundary conditions WeakDirichlet (expression of the
  * coordinates, evaluated once at the facet quadrature points), WeakWall, WeakSubInlet,
- * WeakSubOutlet. Anything else throws std::runtime_error at set-up.
+ * WeakSubOutlet, WeakFarfield (Euler; set_reference_state) and StrongDirichlet (expression at
+ * the facet dofs' coordinates). Anything else throws std::runtime_error at set-up.
  *
  * Host fields stay the source of truth between calls: assemble_lhs_and_rhs uploads the
  * solution function, and downloads the residual and time-step functions; solve() downloads
