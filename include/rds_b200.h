@@ -189,15 +189,18 @@ RDS_API rds_status rds_assemble_rhs(rds_ctx *ctx);
 RDS_API rds_status rds_update(rds_ctx *ctx);
 /* compute_residual_norm(): sqrt(sum_n (res_n dt_n)^2 / N) per equation, into norm[neq]. */
 RDS_API rds_status rds_residual_norm(rds_ctx *ctx, double *norm);
-/* Element Jacobians of the PGLDA and PGN schemes at the current state, as the reference's
+/* Element Jacobians of the PGLDA, PGN and PGB schemes at the current state, as the reference's
  * Picard-linearised implicit solver assembles them (solver/rdm/cellsplitters/PGLDA.hpp:316-536,
- * PGN.hpp:296-440, called from solver/rdm/assembly/PGRDMPicardJacCellAssemblyWorker.hpp:370):
+ * PGN.hpp:296-440, PGB.hpp:505-690, called from
+ * solver/rdm/assembly/PGRDMPicardJacCellAssemblyWorker.hpp:370):
  * PGLDA J_mn = sum_q w_q |J_q| K+_m (sum_k K+_k)^-1 K_n (K_n the unclipped upwind matrix);
  * PGN   J_mn = sum_q w_q |J_q| (delta_mn K+_m - K+_m (sum_k K-_k)^-1 K-_n) (the reference's
- * implicit PGN is the plain N scheme).
+ *       implicit PGN is the plain N scheme);
+ * PGB   J_mn = PGLDA + theta sum_q w_q |J_q| (delta_mn K+_m - K+_m (sum_k K+_k)^-1 K+_n), theta
+ *       the cell's blending coefficient of the residual at the same state.
  * jac: device array [ncells][ndof*neq][ndof*neq] of cell group 'group' (row m*neq + i, column
- * n*neq + j), before the division by the dual volumes. Asynchronous on the context's stream;
- * RDS_ERR_UNSUPPORTED for PGB contexts. */
+ * n*neq + j), before the division by the dual volumes. Asynchronous on the context's stream
+ * (for PGB the residual kernel runs first to get theta; the residual fields are not touched). */
 RDS_API rds_status rds_element_jacobians(rds_ctx *ctx, int group, double *jac);
 
 /* The same Jacobians assembled into a block-CSR matrix over the solution nodes, as the
@@ -208,7 +211,7 @@ RDS_API rds_status rds_element_jacobians(rds_ctx *ctx, int group, double *jac);
  *   rds_jacobian_pattern: nnzb (number of blocks) and, when not NULL, row_ptr [nnodes + 1] and
  *     col_idx [nnzb] (host arrays; columns ascending within a row). Built on the first call.
  *   rds_assemble_jacobian: values (device array [nnzb][neq][neq], row-major blocks) at the
- *     current state. Asynchronous on the context's stream; PGLDA / PGN contexts. */
+ *     current state. Asynchronous on the context's stream. */
 RDS_API rds_status rds_jacobian_pattern(rds_ctx *ctx, int64_t *nnzb, int32_t *row_ptr,
                                         int32_t *col_idx);
 RDS_API rds_status rds_assemble_jacobian(rds_ctx *ctx, double *values);

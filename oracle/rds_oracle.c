@@ -11,6 +11,7 @@
 #define NEQ_MAX 5
 #define DIM_MAX 3
 #define NDOF_MAX 32
+#define NR_MAX (NDOF_MAX * NEQ_MAX)
 #define NQ_MAX 64
 #define NFL_MAX 40
 #define NGEO_MAX 32
@@ -402,8 +403,20 @@ static double jacobian(int D, const double *dVgeo, int nq, int ngeo, int q, cons
  * One cell: metrics + scheme
  * ------------------------------------------------------------------------------------------ */
 
+static int cell_residual_theta(const rdso_model *m, const rdso_cells *g, const double *X,
+                               const double *un, double *elem_res, double *elem_ws,
+                               double *theta_out);
+
 static int cell_residual(const rdso_model *m, const rdso_cells *g, const double *X,
                          const double *un, double *elem_res, double *elem_ws)
+{
+  return cell_residual_theta(m, g, X, un, elem_res, elem_ws, NULL);
+}
+
+/* The cell's scheme residual; for PGB also its blending coefficient (theta_out, may be NULL). */
+static int cell_residual_theta(const rdso_model *m, const rdso_cells *g, const double *X,
+                               const double *un, double *elem_res, double *elem_ws,
+                               double *theta_out)
 {
   const int D = m->dim, NEQ = m->neq;
   const int ndof = g->ndof, nq = g->nq, nfl = g->nfl, ngeo = g->ngeo;
@@ -639,6 +652,8 @@ static int cell_residual(const rdso_model *m, const rdso_cells *g, const double 
     for (int n = 0; n < ndof; ++n)
       abs_phiN += fabs(lda[n][0] + diss[n][0]);
     const double theta = fabs(phi[0]) / (abs_phiN + 1.e-6);
+    if (theta_out)
+      *theta_out = theta;
     for (int n = 0; n < ndof; ++n)
       for (int e = 0; e < NEQ; ++e)
         elem_res[n * NEQ + e] = lda[n][e] + theta * diss[n][e];
@@ -670,6 +685,18 @@ void rdso_element_jacobian(const rdso_model *m, const rdso_cells *g, const doubl
   const int ndof = g->ndof, nq = g->nq, ngeo = g->ngeo, NR = ndof * NEQ;
   for (int i = 0; i < NR * NR; ++i)
     jac[i] = 0.0;
+  /* PGB (PGB.hpp:505-690): the LDA Jacobian plus theta times the stabilisation Jacobian
+   * stab_mn = sum_q w_q |J_q| (delta_mn Kp_m - Kp_m (sum Kp)^-1 Kp_n), theta from the residual */
+  const int pgb = m->scheme == RDSO_B;
+  static double stab[NR_MAX * NR_MAX];
+  double theta = 0.0;
+  if (pgb)
+  {
+    double er[NDOF_MAX * NEQ_MAX], ew[NDOF_MAX];
+    cell_residual_theta(m, g, X, un, er, ew, &theta);
+    for (int i = 0; i < NR * NR; ++i)
+      stab[i] = 0.0;
+  }
   static double Kp[NDOF_MAX][NEQ_MAX][NEQ_MAX], Kn[NDOF_MAX][NEQ_MAX][NEQ_MAX];
   for (int q = 0; q < nq; ++q)
   {
@@ -729,9 +756,20 @@ void rdso_element_jacobian(const rdso_model *m, const rdso_cells *g, const doubl
             if (m->scheme == RDSO_N)
               s = (n == mm ? Kp[mm][i][j] : 0.0) - s;
             jac[(size_t)(mm * NEQ + i) * NR + n * NEQ + j] += wj * s;
+            if (pgb)
+            {
+              double sp = B[i][0] * Kp[n][0][j];
+              for (int k = 1; k < NEQ; ++k)
+                sp = sp + B[i][k] * Kp[n][k][j];
+              stab[(size_t)(mm * NEQ + i) * NR + n * NEQ + j] +=
+                  (n == mm) ? wj * (Kp[mm][i][j] - sp) : -(wj * sp);
+            }
           }
     }
   }
+  if (pgb)
+    for (int i = 0; i < NR * NR; ++i)
+      jac[i] += theta * stab[i];
 }
 
 /* ------------------------------------------------------------------------------------------ */

@@ -119,7 +119,8 @@ void rdso_residual_norm(int nnodes, int neq, const double *res, const double *dt
 void rdso_cell_residual(const rdso_model *m, const rdso_cells *g, const double *X /* [ngeo][dim] */,
                         const double *un /* [ndof][neq] */, double *elem_res, double *elem_ws);
 
-/* Element Jacobian of ONE cell, PGLDA (PGLDA.hpp:316-536) or PGN (PGN.hpp:296-440) after
+/* Element Jacobian of ONE cell, PGLDA (PGLDA.hpp:316-536), PGN (PGN.hpp:296-440) or PGB
+ * (PGB.hpp:505-690) after
  * the model's scheme, [ndof*neq][ndof*neq] row-major. */
 void rdso_element_jacobian(const rdso_model *m, const rdso_cells *g, const double *X,
                            const double *un, double *jac);

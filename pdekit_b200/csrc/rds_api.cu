@@ -69,6 +69,8 @@ struct rds_ctx
   int32_t *d_jp_brow = nullptr, *d_jp_cnr = nullptr;
   int64_t *d_jp_cptr = nullptr, *d_jp_coff = nullptr;
   double *d_jp_jac = nullptr;
+  double *d_theta   = nullptr; // PGB Jacobians: per-cell blending coefficients of one group
+  long long theta_cap = 0;
 
   // partitioned single mesh: the nodes this rank shares with others, their slots in the
   // exchange buffer, and the nodes whose (res dt)^2 this rank counts in the norm
@@ -997,17 +999,48 @@ rds_status rds_residual_norm(rds_ctx *ctx, double *norm)
 
 // ---- element Jacobians ------------------------------------------------------------------
 
+// Cell arguments of a Jacobian launch; for PGB the cells' blending coefficients are computed
+// first by the FP64 residual kernel at the current state (its contributions are scratch).
+static rds_status jacobian_args(rds_ctx *ctx, size_t ig, CellArgs *out)
+{
+  const HostCellGroup &g = ctx->groups[ig];
+  CellArgs a             = cell_args(ctx, g, ctx->d_zero);
+  if (ctx->desc.scheme == RDS_PGB)
+  {
+    if (ctx->theta_cap < g.desc.ncells)
+    {
+      cudaFree(ctx->d_theta);
+      ctx->d_theta   = nullptr;
+      ctx->theta_cap = 0;
+      rds_status st  = dalloc(ctx, &ctx->d_theta, (size_t)g.desc.ncells);
+      if (st != RDS_OK)
+        return st;
+      ctx->theta_cap = g.desc.ncells;
+    }
+    a.theta       = ctx->d_theta;
+    rds_status st = launch(ctx, [&](const char **name) {
+      return launch_cells(g, a, g.physics, g.scheme, RDS_FP64, ctx->desc.dim, ctx->desc.neq,
+                          ctx->stream, name);
+    });
+    if (st != RDS_OK)
+      return st;
+  }
+  *out = a;
+  return RDS_OK;
+}
+
 rds_status rds_element_jacobians(rds_ctx *ctx, int group, double *jac)
 {
   if (!ctx || !jac || !ctx->finalized || group < 0 || group >= (int)ctx->groups.size())
     return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_element_jacobians: invalid group or not finalized")
                : RDS_ERR_INVALID;
-  if (ctx->desc.scheme == RDS_PGB)
-    return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_element_jacobians: PGLDA and PGN contexts only");
   if (ctx->nprob > 0)
     return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_element_jacobians: not in batched contexts");
   const HostCellGroup &g = ctx->groups[group];
-  const CellArgs a       = cell_args(ctx, g, ctx->d_zero);
+  CellArgs a;
+  rds_status st = jacobian_args(ctx, (size_t)group, &a);
+  if (st != RDS_OK)
+    return st;
   return launch(ctx, [&](const char **name) {
     *name = "cells_jacobian";
     return launch_jacobians(g, a, g.physics, ctx->desc.scheme, ctx->desc.dim, ctx->desc.neq, jac,
@@ -1116,15 +1149,15 @@ rds_status rds_assemble_jacobian(rds_ctx *ctx, double *values)
   if (!ctx || !values || !ctx->finalized || ctx->nprob > 0)
     return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_assemble_jacobian: not a finalized single context")
                : RDS_ERR_INVALID;
-  if (ctx->desc.scheme == RDS_PGB)
-    return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_assemble_jacobian: PGLDA and PGN contexts only");
   rds_status st = build_jac_pattern(ctx);
   if (st != RDS_OK)
     return st;
   for (size_t ig = 0; ig < ctx->groups.size(); ++ig)
   {
     const HostCellGroup &g = ctx->groups[ig];
-    const CellArgs a       = cell_args(ctx, g, ctx->d_zero);
+    CellArgs a;
+    if ((st = jacobian_args(ctx, ig, &a)) != RDS_OK)
+      return st;
     st = launch(ctx, [&](const char **name) {
       *name = "cells_jacobian";
       return launch_jacobians(g, a, g.physics, ctx->desc.scheme, ctx->desc.dim, ctx->desc.neq,
@@ -1963,6 +1996,7 @@ rds_status rds_destroy(rds_ctx *ctx)
   cudaFree(ctx->d_jp_cptr);
   cudaFree(ctx->d_jp_coff);
   cudaFree(ctx->d_jp_jac);
+  cudaFree(ctx->d_theta);
   void *bufs[] = {ctx->d_X,     ctx->d_u,     ctx->d_res,     ctx->d_ws,       ctx->d_dt,
                   ctx->d_vol,   ctx->d_inv_vol, ctx->d_contrib, ctx->d_wsc,    ctx->d_stage,
                   ctx->d_row,   ctx->d_ent_slot, ctx->d_ent_ws, ctx->d_part,   ctx->d_norm,

@@ -546,7 +546,11 @@ __global__ void __launch_bounds__(NT)
       }
     }
     if (lane == 0)
+    {
       a.wsc[a.ws_base + c] = vol * wmax;
+      if (SCHEME == RDS_PGB && a.theta)
+        a.theta[c] = theta;
+    }
     if (bad)
       atomicOr(a.status, kFlagNegPressure);
   }

@@ -228,6 +228,8 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
     for (int n = 0; n < NDOF; ++n)
       abs_phiN += fabs(lda[n] + diss[n]);
     theta = fabs(phi) / (abs_phiN + 1.e-6);
+    if (a.theta)
+      a.theta[c] = theta;
   }
 
   double *out = a.contrib + a.slot_base + c;

@@ -145,6 +145,7 @@ struct CellArgs
   unsigned *status;
   const int *stop; // nonzero: skip the work (converged loop)
   BatchTileMap bt; // batch mode only
+  double *theta;   // PGB: the cell's blending coefficient [ncells] when not null (Jacobians)
 };
 
 struct BCArgs

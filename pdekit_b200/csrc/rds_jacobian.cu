@@ -1,9 +1,12 @@
-// Element Jacobians of the PGLDA and PGN schemes, the matrices the reference's Picard-linearised
-// implicit solver assembles (src/solver/rdm/cellsplitters/PGLDA.hpp:316-536, PGN.hpp:296-440,
+// Element Jacobians of the PGLDA, PGN and PGB schemes, the matrices the reference's
+// Picard-linearised implicit solver assembles (src/solver/rdm/cellsplitters/PGLDA.hpp:316-536,
+// PGN.hpp:296-440, PGB.hpp:505-690,
 // called from src/solver/rdm/assembly/PGRDMPicardJacCellAssemblyWorker.hpp:370):
 //
 //   PGLDA  J_mn = sum_q w_q |J_q| (K+_m (sum_k K+_k)^-1) K_n
 //   PGN    J_mn = sum_q w_q |J_q| (delta_mn K+_m - K+_m (sum_k K-_k)^-1 K-_n)
+//   PGB    J_mn = PGLDA + theta sum_q w_q |J_q| (delta_mn K+_m - K+_m (sum_k K+_k)^-1 K+_n)
+//          (PGB.hpp:505-690), theta the cell's blending coefficient of the residual (a.theta)
 //
 // with K+- = R max/min(Lambda, 0) L as in the residual and K_n the unclipped upwind matrix (the
 // flux Jacobian in direction grad phi_n); the implicit PGN of the reference is the plain N
@@ -163,10 +166,10 @@ __global__ void __launch_bounds__(kBlock)
 
   if constexpr (NEQ == 1)
   {
-    double row[NDOF];
+    double row[NDOF], stab[NDOF];
 #pragma unroll
     for (int n = 0; n < NDOF; ++n)
-      row[n] = 0.0;
+      row[n] = stab[n] = 0.0;
     for (int q = 0; q < NQ; ++q)
     {
       if (!AFFINE)
@@ -207,12 +210,20 @@ __global__ void __launch_bounds__(kBlock)
           row[n] += wj * ((n == m ? kpm : 0.0) - beta * km);
         }
         else
+        {
           row[n] += wj * (beta * k[n]);
+          if (SCHEME == RDS_PGB)
+          {
+            const double kp = k[n] > 0.0 ? k[n] : 0.0;
+            stab[n] += (n == m) ? wj * (kpm - beta * kp) : -(wj * (beta * kp));
+          }
+        }
       }
     }
+    const double theta = (SCHEME == RDS_PGB) ? a.theta[c] : 0.0;
 #pragma unroll
     for (int n = 0; n < NDOF; ++n)
-      rows[n] = row[n];
+      rows[n] = (SCHEME == RDS_PGB) ? row[n] + theta * stab[n] : row[n];
   }
   else
   {
@@ -220,6 +231,7 @@ __global__ void __launch_bounds__(kBlock)
       for (int j = 0; j < NR; ++j)
         rows[(size_t)i * NR + j] = 0.0;
     const double gamma = a.gamma;
+    const double theta = (SCHEME == RDS_PGB) ? a.theta[c] : 0.0;
     for (int q = 0; q < NQ; ++q)
     {
       if (!AFFINE)
@@ -301,6 +313,9 @@ __global__ void __launch_bounds__(kBlock)
           euler_K_split<-1, double, D>(p, ac, g, K);
         else
           euler_K_split<0, double, D>(p, ac, g, K);
+        double Kp[NEQ][NEQ]; // PGB: K+_n for the stabilisation part
+        if (SCHEME == RDS_PGB)
+          euler_K_split<+1, double, D>(p, ac, g, Kp);
 #pragma unroll
         for (int i = 0; i < NEQ; ++i)
 #pragma unroll
@@ -310,7 +325,15 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
             for (int k = 0; k < NEQ; ++k)
               s += B[i][k] * K[k][j];
-            const double v = (SCHEME == RDS_PGN) ? ((n == m ? Km[i][j] : 0.0) - s) : s;
+            double v = (SCHEME == RDS_PGN) ? ((n == m ? Km[i][j] : 0.0) - s) : s;
+            if (SCHEME == RDS_PGB)
+            {
+              double sp = 0.0;
+#pragma unroll
+              for (int k = 0; k < NEQ; ++k)
+                sp += B[i][k] * Kp[k][j];
+              v += theta * ((n == m ? Km[i][j] : 0.0) - sp);
+            }
             rows[(size_t)i * NR + n * NEQ + j] += wj * v;
           }
       }
@@ -407,19 +430,22 @@ cudaError_t launch_jacobians(const HostCellGroup &g, const CellArgs &a, int phys
 {
   bool ok         = false;
   cudaError_t err = cudaSuccess;
-  const bool n    = scheme == RDS_PGN;
+  auto by_scheme = [&](auto lda, auto n, auto b) {
+    return scheme == RDS_PGN ? n() : scheme == RDS_PGB ? b() : lda();
+  };
+#define RDS_JAC_PHYS(P, D, NEQ)                                                                    \
+  by_scheme([&] { return dispatch_jac<P, RDS_PGLDA, D, NEQ>(g, a, jac, s, &ok); },                \
+            [&] { return dispatch_jac<P, RDS_PGN, D, NEQ>(g, a, jac, s, &ok); },                  \
+            [&] { return dispatch_jac<P, RDS_PGB, D, NEQ>(g, a, jac, s, &ok); })
   if (physics == RDS_ADVECTION_CONST && dim == 2 && neq == 1)
-    err = n ? dispatch_jac<RDS_ADVECTION_CONST, RDS_PGN, 2, 1>(g, a, jac, s, &ok)
-            : dispatch_jac<RDS_ADVECTION_CONST, RDS_PGLDA, 2, 1>(g, a, jac, s, &ok);
+    err = RDS_JAC_PHYS(RDS_ADVECTION_CONST, 2, 1);
   else if (physics == RDS_BURGERS2D && dim == 2 && neq == 1)
-    err = n ? dispatch_jac<RDS_BURGERS2D, RDS_PGN, 2, 1>(g, a, jac, s, &ok)
-            : dispatch_jac<RDS_BURGERS2D, RDS_PGLDA, 2, 1>(g, a, jac, s, &ok);
+    err = RDS_JAC_PHYS(RDS_BURGERS2D, 2, 1);
   else if (physics == RDS_EULER2D && dim == 2 && neq == 4)
-    err = n ? dispatch_jac<RDS_EULER2D, RDS_PGN, 2, 4>(g, a, jac, s, &ok)
-            : dispatch_jac<RDS_EULER2D, RDS_PGLDA, 2, 4>(g, a, jac, s, &ok);
+    err = RDS_JAC_PHYS(RDS_EULER2D, 2, 4);
   else if (physics == RDS_EULER3D && dim == 3 && neq == 5)
-    err = n ? dispatch_jac<RDS_EULER3D, RDS_PGN, 3, 5>(g, a, jac, s, &ok)
-            : dispatch_jac<RDS_EULER3D, RDS_PGLDA, 3, 5>(g, a, jac, s, &ok);
+    err = RDS_JAC_PHYS(RDS_EULER3D, 3, 5);
+#undef RDS_JAC_PHYS
   if (!ok)
     return cudaErrorNotSupported;
   return err;

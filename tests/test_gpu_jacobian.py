@@ -1,7 +1,8 @@
-"""PGLDA / PGN element Jacobians on the GPU (rds_element_jacobians) and their block-CSR assembly
+"""PGLDA / PGN / PGB element Jacobians on the GPU (rds_element_jacobians) and their block-CSR assembly
 (rds_jacobian_pattern, rds_assemble_jacobian) against the oracle, and the linear advection
 identity J u = cell residual (pinned to the reference by the golden cases)."""
 
+import ctypes as C
 import dataclasses
 import os
 
@@ -11,7 +12,7 @@ import pytest
 from conftest import GOLDEN
 from oracle.rds_oracle import Oracle
 from pdekit_b200.problem import load_golden
-from pdekit_b200.rds import PGRDMethodExplicit, RDSError
+from pdekit_b200.rds import PGRDMethodExplicit, RDSError, lib
 
 pytestmark = pytest.mark.gpu
 
@@ -64,14 +65,34 @@ def test_n_scheme_element_jacobians_match_oracle(case):
     assert np.abs(jac - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
-def test_element_jacobians_need_pglda_or_pgn():
-    prob, a, _ = load_golden(os.path.join(GOLDEN, "burgers_p2_b"))
-    s = PGRDMethodExplicit(prob.physics, "b", "fp64").configure_mesh_data(prob)
-    s.initialize_work_data()
-    with pytest.raises(RDSError) as e:
-        s.element_jacobians(0)
-    assert e.value.status == 6
-    s.close()
+@pytest.mark.parametrize("case", ["adv_p2_b", "burgers_p2_b", "euler2d_tri_p3_b",
+                                  "euler2d_quad_p3_b", "euler3d_tet_p2_lda"])
+def test_pgb_element_jacobians_match_oracle(case):
+    prob, a, _ = load_golden(os.path.join(GOLDEN, case))
+    prob.scheme = "b"
+    u = np.asarray(a["u0"])
+    jac = _jacobians(prob, u, "b")[0]
+    o = Oracle(prob)
+    o.model.scheme = 2
+    ref = np.stack([o.element_jacobian(0, c, u) for c in range(prob.groups[0].ncells)])
+    assert np.abs(jac - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_element_jacobians_not_in_batched_contexts():
+    from pdekit_b200.batch import BatchedRDS
+
+    prob, a, _ = load_golden(os.path.join(GOLDEN, "adv_p1_lda"))
+    b = BatchedRDS([prob, prob], np.array([0.9, 0.9]))
+    jac = torch_empty(prob.groups[0].ncells * 2 * 9)
+    st = lib().rds_element_jacobians(b._ctx, 0, C.c_void_p(jac.data_ptr()))
+    assert st == 6
+    b.close()
+
+
+def torch_empty(n):
+    import torch
+
+    return torch.empty(n, dtype=torch.float64, device="cuda")
 
 
 def _dense(row_ptr, col_idx, vals, n, neq):
@@ -94,7 +115,7 @@ def _assembled(prob, u, scheme):
 
 @pytest.mark.parametrize("case,scheme", [("adv_p2_b", "lda"), ("burgers_p2_n", "n"),
                                          ("euler2d_tri_p1_lda", "lda"),
-                                         ("euler3d_tet_p2_lda", "n")])
+                                         ("euler3d_tet_p2_lda", "n"), ("burgers_p2_b", "b")])
 def test_assembled_jacobian_matches_oracle_elements(case, scheme):
     prob, a, _ = load_golden(os.path.join(GOLDEN, case))
     prob.scheme = scheme
@@ -106,7 +127,7 @@ def test_assembled_jacobian_matches_oracle_elements(case, scheme):
         cols = col_idx[row_ptr[v]:row_ptr[v + 1]]
         assert np.all(np.diff(cols) > 0) and v in cols
     o = Oracle(prob)
-    o.model.scheme = {"lda": 0, "n": 1}[scheme]
+    o.model.scheme = {"lda": 0, "n": 1, "b": 2}[scheme]
     g = prob.groups[0]
     ref = np.zeros((n * neq, n * neq))
     for c in range(g.ncells):

@@ -64,3 +64,22 @@ def test_n_scheme_jacobian_is_the_n_residual_operator(case):
         un = u[g.sol_conn[c]]
         d = jac @ un - np.array([jac[mm] @ (un - un[mm]) for mm in range(g.ndof)])
         assert np.abs(d).max() <= 1e-12 * max(np.abs(jac).max() * np.abs(un).max(), 1e-300)
+
+
+@pytest.mark.parametrize("case", ["adv_p2_b", "adv_p1_lda"])
+def test_pgb_jacobian_reproduces_the_pgb_residual(case):
+    """PGB for constant advection: J(u) u = the blended residual (LDA part plus theta times the
+    N part, theta frozen at u); the golden case adv_p2_b pins that residual to the reference."""
+    prob, a, _ = load_golden(os.path.join(GOLDEN, case))
+    prob.scheme = "b"
+    o = Oracle(prob)
+    o.model.scheme = 2
+    g = prob.groups[0]
+    rng = np.random.default_rng(7)
+    for u in (np.asarray(a["u0"]).reshape(-1), rng.standard_normal(prob.nnodes)):
+        for c in range(g.ncells):
+            jac = o.element_jacobian(0, c, u)
+            res, _ = o.cell_residual(0, c, u)
+            un = u[g.sol_conn[c]]
+            scale = max(np.abs(res).max(), np.abs(jac).max() * np.abs(un).max(), 1e-300)
+            assert np.abs(jac @ un - res[:, 0]).max() <= 1e-12 * scale
