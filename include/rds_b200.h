@@ -216,6 +216,19 @@ RDS_API rds_status rds_jacobian_pattern(rds_ctx *ctx, int64_t *nnzb, int32_t *ro
                                         int32_t *col_idx);
 RDS_API rds_status rds_assemble_jacobian(rds_ctx *ctx, double *values);
 
+/* One step on host buffers, pipelined: upload u_in ([nnodes][neq], pinned host memory for the
+ * copies to overlap), one assemble_lhs_and_rhs + solve, residual norm into norm[neq] (may be
+ * NULL) and the new state into u_out ([nnodes][neq], pinned). Returns without waiting; the
+ * upload of the next call and the download of this one overlap the compute (two staging
+ * buffers, separate copy streams), so consecutive calls keep both copy directions and the GPU
+ * busy. u_in must stay unchanged and u_out / norm unread until rds_step_sync returns. The same
+ * sequence as rds_set_state, rds_assemble, rds_update, rds_residual_norm, rds_get_state
+ * (solver/rdm/PGRDMethodExplicit.hpp:417-514). */
+RDS_API rds_status rds_step_host(rds_ctx *ctx, const double *u_in, double *u_out, double cfl,
+                                 double *norm);
+/* Waits for every issued rds_step_host and reports the status flags. */
+RDS_API rds_status rds_step_sync(rds_ctx *ctx);
+
 /* Partitioned single mesh (no counterpart call in the reference, whose explicit solver runs
  * one mesh per process): one context per rank holds a part of the cells and the nodes they
  * touch, renumbered; the ranks add their partial nodal sums at the nodes they share.

@@ -72,6 +72,14 @@ struct rds_ctx
   double *d_theta   = nullptr; // PGB Jacobians: per-cell blending coefficients of one group
   long long theta_cap = 0;
 
+  // pipelined host-buffer steps (rds_step_host): copy streams, double-buffered staging
+  cudaStream_t h_in = nullptr, h_out = nullptr;
+  cudaEvent_t ev_in_ready[2] = {nullptr, nullptr}, ev_in_free[2] = {nullptr, nullptr};
+  cudaEvent_t ev_out_ready[2] = {nullptr, nullptr}, ev_out_free[2] = {nullptr, nullptr};
+  double *d_hin[2] = {nullptr, nullptr}, *d_hout[2] = {nullptr, nullptr};
+  double *d_hnorm[2] = {nullptr, nullptr};
+  long long hstep = 0;
+
   // partitioned single mesh: the nodes this rank shares with others, their slots in the
   // exchange buffer, and the nodes whose (res dt)^2 this rank counts in the norm
   int32_t *d_if_nodes = nullptr, *d_if_slots = nullptr;
@@ -1174,6 +1182,101 @@ rds_status rds_assemble_jacobian(rds_ctx *ctx, double *values)
   });
 }
 
+// ---- pipelined host-buffer steps --------------------------------------------------------
+
+// Per call: upload (stream h_in) into staging buffer k, compute stream: layout conversion into
+// the state, one fused iteration, the norm, the state into output buffer k; download (stream
+// h_out). Buffers alternate between calls, so the upload of the next call and the download of
+// the previous one overlap this call's compute; events keep a buffer from being overwritten
+// while a copy still reads it.
+static rds_status step_host_init(rds_ctx *ctx)
+{
+  if (ctx->h_in)
+    return RDS_OK;
+  const size_t n = (size_t)ctx->desc.nnodes * ctx->desc.neq;
+  RDS_CUDA(cudaStreamCreateWithFlags(&ctx->h_in, cudaStreamNonBlocking));
+  RDS_CUDA(cudaStreamCreateWithFlags(&ctx->h_out, cudaStreamNonBlocking));
+  for (int k = 0; k < 2; ++k)
+  {
+    RDS_CUDA(cudaEventCreateWithFlags(&ctx->ev_in_ready[k], cudaEventDisableTiming));
+    RDS_CUDA(cudaEventCreateWithFlags(&ctx->ev_in_free[k], cudaEventDisableTiming));
+    RDS_CUDA(cudaEventCreateWithFlags(&ctx->ev_out_ready[k], cudaEventDisableTiming));
+    RDS_CUDA(cudaEventCreateWithFlags(&ctx->ev_out_free[k], cudaEventDisableTiming));
+    rds_status st;
+    if ((st = dalloc(ctx, &ctx->d_hin[k], n)) != RDS_OK ||
+        (st = dalloc(ctx, &ctx->d_hout[k], n)) != RDS_OK ||
+        (st = dalloc(ctx, &ctx->d_hnorm[k], (size_t)ctx->desc.neq)) != RDS_OK)
+      return st;
+  }
+  return RDS_OK;
+}
+
+rds_status rds_step_host(rds_ctx *ctx, const double *u_in, double *u_out, double cfl, double *norm)
+{
+  if (!ctx || !u_in || !u_out || !ctx->finalized || ctx->nprob > 0)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_step_host: not a finalized single context")
+               : RDS_ERR_INVALID;
+  rds_status st = step_host_init(ctx);
+  if (st != RDS_OK)
+    return st;
+  const int N = ctx->desc.nnodes, NEQ = ctx->desc.neq;
+  const size_t bytes = (size_t)N * NEQ * sizeof(double);
+  const int k        = (int)(ctx->hstep++ & 1);
+  cudaStream_t s     = ctx->stream;
+
+  // upload
+  RDS_CUDA(cudaStreamWaitEvent(ctx->h_in, ctx->ev_in_free[k], 0));
+  RDS_CUDA(cudaMemcpyAsync(ctx->d_hin[k], u_in, bytes, cudaMemcpyHostToDevice, ctx->h_in));
+  RDS_CUDA(cudaEventRecord(ctx->ev_in_ready[k], ctx->h_in));
+
+  // compute: AoS staging -> SoA state, one iteration (assemble + update + norm partials)
+  RDS_CUDA(cudaStreamWaitEvent(s, ctx->ev_in_ready[k], 0));
+  if (NEQ == 1)
+    RDS_CUDA(cudaMemcpyAsync(ctx->d_u, ctx->d_hin[k], bytes, cudaMemcpyDeviceToDevice, s));
+  else
+    for (int e = 0; e < NEQ; ++e)
+      RDS_CUDA(cudaMemcpy2DAsync(ctx->d_u + (size_t)e * N, sizeof(double), ctx->d_hin[k] + e,
+                                 NEQ * sizeof(double), sizeof(double), N,
+                                 cudaMemcpyDeviceToDevice, s));
+  RDS_CUDA(cudaEventRecord(ctx->ev_in_free[k], s));
+  if ((st = rds_run(ctx, cfl, 1)) != RDS_OK)
+    return st;
+  st = launch(ctx, [&](const char **name) {
+    return launch_norm_final(ctx->d_part, ctx->gblocks, NEQ, N, ctx->d_hnorm[k], nullptr,
+                             nullptr, nullptr, 0, 0.0, nullptr, nullptr, s, name);
+  });
+  if (st != RDS_OK)
+    return st;
+  RDS_CUDA(cudaStreamWaitEvent(s, ctx->ev_out_free[k], 0));
+  if (NEQ == 1)
+    RDS_CUDA(cudaMemcpyAsync(ctx->d_hout[k], ctx->d_u, bytes, cudaMemcpyDeviceToDevice, s));
+  else
+    for (int e = 0; e < NEQ; ++e)
+      RDS_CUDA(cudaMemcpy2DAsync(ctx->d_hout[k] + e, NEQ * sizeof(double),
+                                 ctx->d_u + (size_t)e * N, sizeof(double), sizeof(double), N,
+                                 cudaMemcpyDeviceToDevice, s));
+  RDS_CUDA(cudaEventRecord(ctx->ev_out_ready[k], s));
+
+  // download
+  RDS_CUDA(cudaStreamWaitEvent(ctx->h_out, ctx->ev_out_ready[k], 0));
+  RDS_CUDA(cudaMemcpyAsync(u_out, ctx->d_hout[k], bytes, cudaMemcpyDeviceToHost, ctx->h_out));
+  if (norm)
+    RDS_CUDA(cudaMemcpyAsync(norm, ctx->d_hnorm[k], NEQ * sizeof(double), cudaMemcpyDeviceToHost,
+                             ctx->h_out));
+  RDS_CUDA(cudaEventRecord(ctx->ev_out_free[k], ctx->h_out));
+  return RDS_OK;
+}
+
+rds_status rds_step_sync(rds_ctx *ctx)
+{
+  if (!ctx)
+    return RDS_ERR_INVALID;
+  if (ctx->h_out)
+    RDS_CUDA(cudaStreamSynchronize(ctx->h_out));
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return check_status(ctx);
+}
+
 // ---- partitioned single mesh ------------------------------------------------------------
 
 rds_status rds_set_dual_volume(rds_ctx *ctx, const double *vol)
@@ -1997,6 +2100,24 @@ rds_status rds_destroy(rds_ctx *ctx)
   cudaFree(ctx->d_jp_coff);
   cudaFree(ctx->d_jp_jac);
   cudaFree(ctx->d_theta);
+  if (ctx->h_out)
+    cudaStreamSynchronize(ctx->h_out);
+  if (ctx->h_in)
+    cudaStreamSynchronize(ctx->h_in);
+  for (int k = 0; k < 2; ++k)
+  {
+    cudaFree(ctx->d_hin[k]);
+    cudaFree(ctx->d_hout[k]);
+    cudaFree(ctx->d_hnorm[k]);
+    for (cudaEvent_t e : {ctx->ev_in_ready[k], ctx->ev_in_free[k], ctx->ev_out_ready[k],
+                          ctx->ev_out_free[k]})
+      if (e)
+        cudaEventDestroy(e);
+  }
+  if (ctx->h_in)
+    cudaStreamDestroy(ctx->h_in);
+  if (ctx->h_out)
+    cudaStreamDestroy(ctx->h_out);
   void *bufs[] = {ctx->d_X,     ctx->d_u,     ctx->d_res,     ctx->d_ws,       ctx->d_dt,
                   ctx->d_vol,   ctx->d_inv_vol, ctx->d_contrib, ctx->d_wsc,    ctx->d_stage,
                   ctx->d_row,   ctx->d_ent_slot, ctx->d_ent_ws, ctx->d_part,   ctx->d_norm,

@@ -126,6 +126,8 @@ def lib():
         "rds_element_jacobians": ([vp, ip, vp], ip),
         "rds_jacobian_pattern": ([vp, vp, vp, vp], ip),
         "rds_assemble_jacobian": ([vp, vp], ip),
+        "rds_step_host": ([vp, vp, vp, dp, vp], ip),
+        "rds_step_sync": ([vp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -296,6 +298,25 @@ class PGRDMethodExplicit:
         torch.cuda.ExternalStream(self.stream_handle()).synchronize()
         self._check(lib().rds_check(self._ctx))
         return row_ptr, col_idx, vals.cpu().numpy()
+
+    def step_host(self, u_in, u_out, cfl: float, norm=None):
+        """One pipelined step on host arrays (pinned for overlap): returns without waiting;
+        call step_sync() before reading u_out / norm or reusing u_in. The arrays are used in
+        place (no copies): float64, C-contiguous, nnodes x neq values (norm: neq)."""
+        p = self.problem
+        for nm, a, n in (("u_in", u_in, p.nnodes * p.neq), ("u_out", u_out, p.nnodes * p.neq),
+                         ("norm", norm, p.neq)):
+            if a is None and nm == "norm":
+                continue
+            if (not isinstance(a, np.ndarray) or a.dtype != np.float64
+                    or not a.flags.c_contiguous or a.size != n):
+                raise ValueError(f"step_host: {nm} must be a C-contiguous float64 array of "
+                                 f"{n} values")
+        self._check(lib().rds_step_host(self._ctx, _ptr(u_in), _ptr(u_out), float(cfl),
+                                        None if norm is None else _ptr(norm)))
+
+    def step_sync(self):
+        self._check(lib().rds_step_sync(self._ctx))
 
     def set_option(self, key: str, value: float):
         self._check(lib().rds_set_option(self._ctx, key.encode(), float(value)))
