@@ -82,6 +82,11 @@ def parse():
                     help="--quick: precision of the timed steps")
     ap.add_argument("--tensor-cores", action="store_true",
                     help="mixed cells with the basis contractions on the tensor cores")
+    ap.add_argument("--stab", default=None, choices=["av", "lf", "wj", "visc"],
+                    help="also time the steps with a stabilisation field computed on the device "
+                         "(av: artificial viscosity, read by PGLDA; lf / wj / visc: LF_Blend / "
+                         "WongJansen / ViscosityIndicator blending coefficient, read by PGB) and "
+                         "the operator that computes it")
     ap.add_argument("--partition", action="store_true",
                     help="c1-c4: split the one mesh over the ranks (interface sums all-reduced "
                          "every iteration, strong scaling) instead of one replica per rank")
@@ -559,6 +564,8 @@ def run_ours(args, rank, world, local):
                              f"{cpu_spec['sample']}, {r['iters']} iterations after one warm-up "
                              f"assemble, nb_threads={threads} ({r['cells']} cells)"}
 
+    stab = measure_stab(args, solver, prob, u0, cfl, steps, flush, world) if args.stab else None
+
     line = {
         "metric": "cell-residual updates/s", "value": value, "unit": "cell-residual updates/s",
         "n_gpus": world, "steps": steps, "warmup": args.warmup,
@@ -578,8 +585,48 @@ def run_ours(args, rank, world, local):
         "gpu_launches": int(launches),
         "wall_s_timed_region": round(wall, 3),
     }
+    if stab:
+        line["stabilised"] = stab
     solver.close()
     return line
+
+
+def measure_stab(args, solver, prob, u0, cfl, steps, flush, world):
+    """The step with a stabilisation field: the operator computes the nodal field from the
+    state on the device and installs it (no host copy), then the same timed steps as `value`.
+    The operator is timed with CUDA events on the solver's stream (mean of 5 calls after one
+    warm-up call)."""
+    import torch
+
+    from pdekit_b200 import stabilisation as st
+
+    op, p0, name = {"av": (st.ART_VISC, 5.0, "artificial viscosity (kappa 5, factor 1)"),
+                    "lf": (st.BLEND_LF, 0.0, "LF_Blend"),
+                    "wj": (st.BLEND_WONG_JANSEN, 1.0, "WongJansen (u_inf 1)"),
+                    "visc": (st.BLEND_VISC, 5.0, "ViscosityIndicator (kappa 5)")}[args.stab]
+    solver.set_solution(u0)
+    stream = torch.cuda.ExternalStream(solver.stream_handle())
+    solver.compute_stabilisation(op, p0, 1.0, install=True, cells=False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(5):
+        solver.compute_stabilisation(op, p0, 1.0, install=True, cells=False)
+    e1.record(stream)
+    e1.synchronize()
+    op_ms = max_over_ranks(e0.elapsed_time(e1) / 5, world)
+    solver.run(cfl, max(args.warmup, 3))
+    torch.cuda.synchronize()
+    solver.set_solution(u0)
+    solver.compute_stabilisation(op, p0, 1.0, install=True, cells=False)
+    launches0 = solver.launch_count()
+    ms = max_over_ranks(time_steps(solver, steps, flush, cfl), world)
+    launches = solver.launch_count() - launches0
+    reads = {"av": "PGLDA", "lf": "PGB", "wj": "PGB", "visc": "PGB"}[args.stab]
+    return {"field": name, "read_by": reads,
+            "applies": (prob.scheme == "lda") == (reads == "PGLDA"),
+            "value": prob.ncells * steps * world / (ms * 1e-3), "ms_per_step": ms / steps,
+            "operator_ms": op_ms, "gpu_launches": int(launches)}
 
 
 def run_partitioned(args, rank, world, local):

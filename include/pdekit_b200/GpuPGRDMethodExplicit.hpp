@@ -681,12 +681,34 @@ class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>
     ctx.add_bc(b);
   }
 
+  /* The state, and the stabilisation fields handed over through the reference's
+   * set_blending_coeff / set_artificial_viscosity (RDMethod.hpp:79-85): the reference's cell
+   * worker reads their current values at every assembly (PGRDMExplicitCellWorker.hpp:505-533),
+   * so they travel with the state. */
   void upload_solution()
   {
     const vec_fn::ptr u = this->vec_function(SolverVecFn::solution);
     if (!u || u->nb_entries() != Uint(m_ctx->nnodes()))
       throw std::runtime_error("GpuPGRDMethodExplicit: solution function not set or wrong size");
     m_ctx->set_state(&u->value(0)[0]);
+    upload_field(base::m_blending_coeff, m_blend_sent, &rds_b200::Context::set_blending_coeff);
+    upload_field(base::m_art_viscosity, m_av_sent, &rds_b200::Context::set_artificial_viscosity);
+  }
+  void upload_field(const interpolation::ScalarMeshFunction<Real>::ptr &f, bool &sent,
+                    void (rds_b200::Context::*set)(const double *))
+  {
+    if (f)
+    {
+      if (f->nb_entries() != Uint(m_ctx->nnodes()))
+        throw std::runtime_error("GpuPGRDMethodExplicit: stabilisation field of wrong size");
+      ((*m_ctx).*set)(&(*f)[0]);
+      sent = true;
+    }
+    else if (sent)
+    {
+      ((*m_ctx).*set)(nullptr);
+      sent = false;
+    }
   }
   void download_solution()
   {
@@ -712,6 +734,7 @@ class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>
 
   int m_precision;
   bool m_cfl_set = false;
+  bool m_blend_sent = false, m_av_sent = false;
   std::map<std::string, std::shared_ptr<bc_type>> m_bcs;
   std::vector<double> m_coords;
   std::unique_ptr<rds_b200::Context> m_ctx;

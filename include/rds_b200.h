@@ -216,6 +216,52 @@ RDS_API rds_status rds_jacobian_pattern(rds_ctx *ctx, int64_t *nnzb, int32_t *ro
                                         int32_t *col_idx);
 RDS_API rds_status rds_assemble_jacobian(rds_ctx *ctx, double *values);
 
+/* Stabilisation fields (solver/rdm/RDMethod.hpp:79-85, read by the cell worker at
+ * solver/rdm/assembly/PGRDMExplicitCellWorker.hpp:505-533). Both are nodal [nnodes] host
+ * arrays, copied; NULL removes the field.
+ *   rds_set_blending_coeff       (set_blending_coeff): PGB cells use theta_n = theta[dof(c,n)]
+ *     instead of their own blending coefficient, res_n = lda_n + theta_n diss_n, and drop the
+ *     N part when every theta_n < 1e-6 (solver/rdm/cellsplitters/PGB.hpp:141-148,467-477).
+ *     Other schemes ignore it. rds_element_jacobians refuses PGB contexts that have one.
+ *   rds_set_artificial_viscosity (set_artificial_viscosity): PGLDA cells add
+ *     w_q detJ_q eps_q grad phi_n . grad u(q), eps_q = sum_n V(q,n) eps[dof(c,n)]
+ *     (cellsplitters/PGLDA.hpp:245-256). Other schemes ignore it.
+ * Not in batched contexts. */
+RDS_API rds_status rds_set_blending_coeff(rds_ctx *ctx, const double *theta);
+RDS_API rds_status rds_set_artificial_viscosity(rds_ctx *ctx, const double *eps);
+
+/* Stabilisation operators on the current state (its first component), the producers of those
+ * fields: solver/art_visc/ArtificialViscosity.hpp and solver/rdm/blending_coeff/ (the
+ * RDBlendingCoeff types LF_Blend, ViscosityIndicator, WongJansen).
+ *   rds_set_stab_tables (after rds_finalize), per cell group:
+ *     nq, w [nq], Vn [nq][ndof], R [nq][ndof]: the smoothness sensor's rule (exact to degree
+ *       2p on the reference element), the nodal basis there, and the map from nodal values to
+ *       u - u_{p-1} there, u_{p-1} the reference's modal truncation (the L2 projection onto
+ *       degree p - 1; at p = 1 the reference truncates to 0, R = Vn). nq = 0: no sensor.
+ *     nvert, P1 [ndof][nvert]: the vertex interpolant at the cell's nodes (cell-to-node
+ *       transfer).
+ *   rds_compute_stabilisation: cell values of operator op (rds_stab_op), into cells_out
+ *     [total cells, groups in order] when not NULL; their nodal field (every vertex the max of
+ *     0 and its cells' values, every other node the vertex interpolant of the last cell holding
+ *     it; interpolation/mesh_function/MeshFunctionTools.hpp:52-397) into nodes_out [nnodes]
+ *     when not NULL; install != 0 makes the nodal field the context's artificial viscosity
+ *     (RDS_STAB_ART_VISC) or blending coefficient (the blend operators), as
+ *     rds_set_artificial_viscosity / rds_set_blending_coeff would, without a host copy.
+ *     The sensor operators need affine simplex groups with sensor tables. */
+typedef enum
+{
+  RDS_STAB_ART_VISC          = 0, /* compute_artificial_viscosity; p0 = kappa, p1 = factor */
+  RDS_STAB_INDICATOR         = 1, /* compute_indicator_normalized (cells only); p0 = kappa */
+  RDS_STAB_BLEND_LF          = 2, /* "LF_Blend" */
+  RDS_STAB_BLEND_VISC        = 3, /* "ViscosityIndicator"; p0 = kappa */
+  RDS_STAB_BLEND_WONG_JANSEN = 4  /* "WongJansen"; p0 = u_inf */
+} rds_stab_op;
+RDS_API rds_status rds_set_stab_tables(rds_ctx *ctx, int group, int nq, const double *w,
+                                       const double *Vn, const double *R, int nvert,
+                                       const double *P1);
+RDS_API rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
+                                             int install, double *cells_out, double *nodes_out);
+
 /* One step on host buffers, pipelined: upload u_in ([nnodes][neq], pinned host memory for the
  * copies to overlap), one assemble_lhs_and_rhs + solve, residual norm into norm[neq] (may be
  * NULL) and the new state into u_out ([nnodes][neq], pinned). Returns without waiting; the

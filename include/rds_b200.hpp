@@ -132,6 +132,17 @@ class Context
   {
     check(m_ctx, rds_set_state(m_ctx, u_aos), "rds_set_state");
   }
+
+  /* Nodal stabilisation fields [nnodes] (nullptr removes one): the external blending
+   * coefficient read by PGB cells, the artificial viscosity added by PGLDA cells. */
+  void set_blending_coeff(const double *theta)
+  {
+    check(m_ctx, rds_set_blending_coeff(m_ctx, theta), "rds_set_blending_coeff");
+  }
+  void set_artificial_viscosity(const double *eps)
+  {
+    check(m_ctx, rds_set_artificial_viscosity(m_ctx, eps), "rds_set_artificial_viscosity");
+  }
   void get_state(double *u_aos) const
   {
     check(m_ctx, rds_get_state(m_ctx, u_aos), "rds_get_state");

@@ -106,14 +106,22 @@ inline void init_state(const std::string &name, const Real *x, Uint dim, Uint ne
     // inflow profile 1.5 - 2x with a smooth perturbation
     u[0] = 1.5 - 2.0 * x[0] + 0.1 * std::sin(7.0 * x[0] + 3.0 * x[1]) * x[1];
   }
-  else if (name == "bump2d" || name == "bump3d")
+  else if (name == "steep")
+  {
+    // scalar: a steep front (width 0.04) from 1.5 to -0.5 across x = 0.5 + 0.15 y, the
+    // profile the Burgers inflow/outflow values build up to
+    u[0] = 0.5 - std::tanh((x[0] - 0.5 - 0.15 * x[1]) / 0.04);
+  }
+  else if (name == "bump2d" || name == "bump3d" || name == "bump2d_jump" ||
+           name == "bump3d_jump")
   {
     // Freestream of the reference's bump case (examples/testcases-rdm/Bump-RDS-2D-Explicit.cpp:
     // 100-131): total temperature / pressure 307.6488978 K / 120195.4453 Pa, R = 287.046,
     // Mach 0.5 (2D) or 0.6 (3D) along x, with a +-1% perturbation of density and pressure that
     // is a fixed pseudo-random function of the coordinates.
     const Real gamma = 1.4, R = 287.046, Ttot = 307.6488978, Ptot = 120195.4453;
-    const Real M  = (name == "bump2d") ? 0.5 : 0.6;
+    const bool d2 = name == "bump2d" || name == "bump2d_jump";
+    const Real M  = d2 ? 0.5 : 0.6;
     const Real f  = 1. + 0.5 * (gamma - 1.) * M * M;
     const Real T  = Ttot / f, p0 = Ptot / std::pow(f, gamma / (gamma - 1.));
     const Real z  = dim == 3 ? x[2] : 0.0;
@@ -121,8 +129,12 @@ inline void init_state(const std::string &name, const Real *x, Uint dim, Uint ne
       const Real s = std::sin(12.9898 * a + 78.233 * b + 37.719 * c) * 43758.5453;
       return 2.0 * (s - std::floor(s)) - 1.0;
     };
-    const Real rho = p0 / (R * T) * (1. + 0.01 * hash(x[0], x[1], z));
-    const Real p   = p0 * (1. + 0.01 * hash(x[1], z, x[0]));
+    // "_jump": density and pressure raised by up to 30% across a steep front (width 0.05) at
+    // x = 0.2 + 0.1 y
+    const Real jump = name.size() > 6 ? 1. + 0.15 * (1. + std::tanh((x[0] - 0.2 - 0.1 * x[1]) / 0.05))
+                                      : 1.;
+    const Real rho = jump * p0 / (R * T) * (1. + 0.01 * hash(x[0], x[1], z));
+    const Real p   = jump * p0 * (1. + 0.01 * hash(x[1], z, x[0]));
     const Real ux  = M * std::sqrt(gamma * R * T);
     u[0]           = rho;
     u[1]           = rho * ux;

@@ -15,11 +15,21 @@
 //
 // Usage:
 //   rds_ref_harness dump|time <physics> <scheme> <p> <quad> <mesh.msh> <outdir|-> <iters> <cfl>
-//                   <init> <bcspec> [threads]
+//                   <init> <bcspec> [threads] [stab]
 //     physics: advconst (a = (0.5,1)/|(0.5,1)|) | burgers | euler2d | euler3d
 //     scheme : lda | n | b
 //     init   : name of an initial-state function of the node coordinates (see init_state)
 //     bcspec : comma-separated Type:condition_name:boundary:expr, or "none"
+//     stab   : "none" | "av:<kappa>:<factor>" | "blend:<type>:<param>" -- a stabilisation field
+//              computed at the initial state by the reference's own operators and handed to the
+//              solver the way examples/testcases-rdm/Burgers-RDS-2D.cpp:121-176 does:
+//              ArtificialViscosity (solver/art_visc/ArtificialViscosity.hpp) ->
+//              set_artificial_viscosity, or RDBlendingCoeff of <type> (LF_Blend,
+//              ViscosityIndicator, WongJansen; <param> = kappa or u_inf) -> set_blending_coeff.
+//              "avcells:<kappa>:<factor>" / "blendcells:<type>:<param>": the cellwise values
+//              only (the reference's cell-to-node transfer crashes on tetrahedral meshes);
+//              "avfield:<file>" / "blendfield:<file>": a nodal field read from a raw array of
+//              nsol doubles, handed to the solver.
 //
 // The only addition to the reference is the constant-direction advection policy below: the
 // reference's ConstAdvection2D is hard-wired to a = (0,1) (physics/scalar/RotationAdvection2D.hpp:17-30),
@@ -47,7 +57,9 @@
 #include "physics/euler/Euler3DCons.hpp"
 #include "physics/scalar/Burgers2D.hpp"
 #include "physics/scalar/RotationAdvection2D.hpp"
+#include "solver/art_visc/ArtificialViscosity.hpp"
 #include "solver/rdm/PGRDMethodExplicit.hpp"
+#include "solver/rdm/blending_coeff/RDBlendingCoeff.hpp"
 #include "solver/rdm/cellsplitters/CellSplitters.hpp"
 
 #include "ref_common.hpp"
@@ -108,7 +120,7 @@ class ProbeSolver : public rdm::PGRDMethodExplicit<MC, Phys, Scheme>
 
 struct Args
 {
-  std::string mode, physics, scheme, mesh, outdir, init, bcspec;
+  std::string mode, physics, scheme, mesh, outdir, init, bcspec, stab = "none";
   Uint p = 1, quad = 1, iters = 1, threads = 1;
   Real cfl = 0.5;
 };
@@ -317,6 +329,90 @@ int run(const Args &a)
     return v;
   };
 
+  // ---- stabilisation field at u0 (optional)
+  using scal_fn = interpolation::ScalarMeshFunction<Real>;
+  std::vector<std::pair<std::string, std::vector<Real>>> stab_arrays;
+  std::shared_ptr<scal_fn> stab_nodal;
+  auto cells_of = [&](const scal_fn &f) {
+    std::vector<Real> v(ncells);
+    for (Uint c = 0; c < ncells; ++c)
+      v[c] = f[c];
+    return v;
+  };
+  if (a.stab != "none")
+  {
+    std::vector<std::string> tok;
+    std::stringstream ts(a.stab);
+    std::string t;
+    while (std::getline(ts, t, ':'))
+      tok.push_back(t);
+    const bool field = tok.size() == 2 && (tok[0] == "avfield" || tok[0] == "blendfield");
+    const bool ok3   = tok.size() == 3 && (tok[0] == "av" || tok[0] == "blend" ||
+                                         tok[0] == "avcells" || tok[0] == "blendcells");
+    if (!field && !ok3)
+    {
+      std::cerr << "bad stab spec " << a.stab << std::endl;
+      return 2;
+    }
+    stab_nodal = std::make_shared<scal_fn>("", "stab_nodal");
+    stab_nodal->resize(nsol);
+    scal_fn cellwise("", "cellwise");
+    cellwise.resize(ncells);
+    if (field)
+    {
+      std::ifstream fin(tok[1], std::ios::binary);
+      std::vector<Real> vals(nsol);
+      fin.read(reinterpret_cast<char *>(vals.data()), nsol * sizeof(Real));
+      if (!fin)
+      {
+        std::cerr << "cannot read " << nsol << " values from " << tok[1] << std::endl;
+        return 2;
+      }
+      for (Uint i = 0; i < nsol; ++i)
+        (*stab_nodal)[i] = vals[i];
+      if (tok[0] == "avfield")
+      {
+        stab_arrays.push_back({"av_nodal", vals});
+        solver->set_artificial_viscosity(stab_nodal);
+      }
+      else
+      {
+        stab_arrays.push_back({"blend_nodal", vals});
+        solver->set_blending_coeff(stab_nodal);
+      }
+    }
+    else if (tok[0] == "av" || tok[0] == "avcells")
+    {
+      const Real kappa = std::atof(tok[1].c_str()), factor = std::atof(tok[2].c_str());
+      solver::ArtificialViscosity<MC> op;
+      op.prepare_indicator_operators(*sol);
+      op.compute_artificial_viscosity(*sol, *u, cellwise, kappa, factor);
+      stab_arrays.push_back({"av_cell", cells_of(cellwise)});
+      op.compute_indicator_normalized(*sol, *u, cellwise, kappa);
+      stab_arrays.push_back({"indicator", cells_of(cellwise)});
+      if (tok[0] == "av")
+      {
+          op.compute_artificial_viscosity_nodal(*mesh, *sol, *u, *stab_nodal, kappa, factor);
+        stab_arrays.push_back({"av_nodal", grab_scalar(*stab_nodal)});
+        solver->set_artificial_viscosity(stab_nodal);
+      }
+    }
+    else
+    {
+      solver::rdm::RDBlendingCoeff<MC> op;
+      op.setup(*sol, tok[1]);
+      op.set_param(tok[1] == "WongJansen" ? "u_inf" : "kappa", std::atof(tok[2].c_str()));
+      op.calculate_in_cells(*mesh, *sol, *u, cellwise);
+      stab_arrays.push_back({"blend_cell", cells_of(cellwise)});
+      if (tok[0] == "blend")
+      {
+        op.calculate(*mesh, *sol, *u, *stab_nodal);
+        stab_arrays.push_back({"blend_nodal", grab_scalar(*stab_nodal)});
+        solver->set_blending_coeff(stab_nodal);
+      }
+    }
+  }
+
   if (a.mode == "time")
   {
     solver->assemble_lhs_and_rhs(a.cfl); // warm-up
@@ -434,6 +530,8 @@ int run(const Args &a)
   }
 
   out.put("u0", u0, {nsol, NEQ});
+  for (const auto &sa : stab_arrays)
+    out.put(sa.first, sa.second, {Uint(sa.second.size())});
 
   // first iteration: residual, wave speed, dt, dual volume at u0
   solver->assemble_lhs_and_rhs(a.cfl);
@@ -475,7 +573,8 @@ int run(const Args &a)
        << ", \"nsol\": " << nsol << ", \"ngeo_nodes\": " << ngeo_nodes << ", \"ndof\": " << ndof
        << ", \"ngeo\": " << ngeo << ", \"nq\": " << nq << ", \"nfl\": " << nfl
        << ", \"nfq\": " << nfq << ",\n \"iters\": " << a.iters << ", \"cfl\": " << a.cfl
-       << ", \"init\": \"" << a.init << "\",\n \"bcs\": [" << bcmeta.str()
+       << ", \"init\": \"" << a.init << "\", \"stab\": \"" << a.stab
+       << "\",\n \"bcs\": [" << bcmeta.str()
        << "],\n \"arrays\": {\n"
        << out.manifest.str() << "\n }\n}\n";
   return 0;
@@ -486,7 +585,7 @@ int main(int argc, char **argv)
   if (argc < 12)
   {
     std::fprintf(stderr, "usage: %s dump|time physics scheme p quad mesh outdir iters cfl init "
-                         "bcspec [threads]\n",
+                         "bcspec [threads] [stab]\n",
                  argv[0]);
     return 2;
   }
@@ -503,6 +602,8 @@ int main(int argc, char **argv)
   a.init    = argv[10];
   a.bcspec  = argv[11];
   a.threads = argc > 12 ? std::atoi(argv[12]) : 1;
+  if (argc > 13)
+    a.stab = argv[13];
 
   using Adv   = physics::RotationAdvection2D<ConstDirection2D>;
   using Burg  = physics::Burgers2D;

@@ -1,0 +1,180 @@
+"""Test oracle (test infrastructure only; the product never imports it): a numpy restatement of
+the reference's stabilisation operators that sit either side of the cell residual.
+
+* `sensor_cells`: the Persson-Peraire smoothness sensor per cell
+  (src/solver/art_visc/ArtificialViscosity.hpp:300-455, and the same sensor as a blending
+  coefficient in src/solver/rdm/blending_coeff/ArtViscIndicatorCoeffImpl.hpp:261-425): the
+  first state component is projected in L2 onto the cell's modal basis of order p, the modes
+  of total degree p are dropped (at p = 1 all modes), Se = int (u - u_{p-1})^2 / int u^2 (0 when the denominator
+  is <= 1e-10), se = log10 Se, s0 = 1/p^4, and the value is 0 below s0 - kappa, eps0 above
+  s0 + kappa, 0.5 eps0 (1 + sin(pi (se - s0) / (2 kappa))) between; eps0 = factor h / p with
+  h = |K|^(1/D) for the viscosity, eps0 = 1 for the blending coefficient.
+  Restated with an explicit orthogonal (Dubiner) basis in collapsed coordinates
+  (M. Dubiner, J. Sci. Comput. 6, 1991; the basis the reference registers as the modal basis
+  of triangles and tetrahedra, mesh/shape_function/ModalBasisFactory.cpp:36-46) and
+  collapsed-coordinate Gauss-Legendre quadrature exact to degree 2p (the reference integrates
+  with its Gauss rule of order max(2p, geometry order); on affine cells both are exact).
+* `nodal_from_cells`: the cell-to-node transfer
+  (src/interpolation/mesh_function/MeshFunctionTools.hpp:52-397 without adaptation): every
+  vertex takes max(0, max over its cells), every other node the P1 interpolant of the vertex
+  values of the last cell (in cell order) that holds it.
+* `blend_cells`: LF_Blend (blending_coeff/LFBlendingCoeffImpl.hpp:76-126), WongJansen
+  (WongJansenBlendingCoeffImpl.hpp:80-116), ViscosityIndicator (the sensor with eps0 = 1).
+
+Pinned against the reference's own outputs (tests/golden/*_av, *_lf, *_wj, *_visc, dumped by
+oracle/ref_harness.cpp through the reference's classes).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+from scipy.special import eval_jacobi
+
+
+# ---- quadrature: collapsed-coordinate Gauss-Legendre (Duffy) rules on the reference simplex
+def _simplex_rule(dim: int, n: int):
+    x, w = np.polynomial.legendre.leggauss(n)
+    if dim == 2:
+        a, b = np.meshgrid(x, x, indexing="ij")
+        wa, wb = np.meshgrid(w, w, indexing="ij")
+        a, b, wt = a.ravel(), b.ravel(), (wa * wb).ravel() * (1 - b.ravel()) / 2
+        xi = (1 + a) * (1 - b) / 2 - 1
+        return np.stack([xi, b], 1), wt
+    a, b, c = np.meshgrid(x, x, x, indexing="ij")
+    wa, wb, wc = np.meshgrid(w, w, w, indexing="ij")
+    a, b, c = a.ravel(), b.ravel(), c.ravel()
+    wt = (wa * wb * wc).ravel() * (1 - b) / 2 * ((1 - c) / 2) ** 2
+    zeta = c
+    eta = (1 + b) * (1 - c) / 2 - 1
+    xi = (1 + a) * (1 - b) / 2 * (1 - c) / 2 - 1
+    return np.stack([xi, eta, zeta], 1), wt
+
+
+# ---- Dubiner basis of total degree <= p at points of the reference simplex
+def _dubiner(dim: int, p: int, pts: np.ndarray):
+    """[npts, nmodes] values and the degree of each mode."""
+    cols, deg = [], []
+    if dim == 2:
+        xi, eta = pts[:, 0], pts[:, 1]
+        den = np.where(np.abs(1 - eta) < 1e-15, 1e-15, 1 - eta)
+        a = 2 * (1 + xi) / den - 1
+        for i in range(p + 1):
+            for j in range(p + 1 - i):
+                cols.append(eval_jacobi(i, 0, 0, a) * ((1 - eta) / 2) ** i *
+                            eval_jacobi(j, 2 * i + 1, 0, eta))
+                deg.append(i + j)
+    else:
+        xi, eta, zeta = pts[:, 0], pts[:, 1], pts[:, 2]
+        d1 = np.where(np.abs(-eta - zeta) < 1e-15, 1e-15, -eta - zeta)
+        d2 = np.where(np.abs(1 - zeta) < 1e-15, 1e-15, 1 - zeta)
+        a = 2 * (1 + xi) / d1 - 1
+        b = 2 * (1 + eta) / d2 - 1
+        for i in range(p + 1):
+            for j in range(p + 1 - i):
+                for k in range(p + 1 - i - j):
+                    cols.append(eval_jacobi(i, 0, 0, a) * ((1 - b) / 2) ** i *
+                                eval_jacobi(j, 2 * i + 1, 0, b) * ((1 - zeta) / 2) ** (i + j) *
+                                eval_jacobi(k, 2 * i + 2 * j + 2, 0, zeta))
+                    deg.append(i + j + k)
+    return np.stack(cols, 1), np.asarray(deg)
+
+
+def _monomials(dim: int, p: int, pts: np.ndarray):
+    cols = []
+    if dim == 2:
+        for i in range(p + 1):
+            for j in range(p + 1 - i):
+                cols.append(pts[:, 0] ** i * pts[:, 1] ** j)
+    else:
+        for i in range(p + 1):
+            for j in range(p + 1 - i):
+                for k in range(p + 1 - i - j):
+                    cols.append(pts[:, 0] ** i * pts[:, 1] ** j * pts[:, 2] ** k)
+    return np.stack(cols, 1)
+
+
+def lagrange_at(dim: int, p: int, nodes: np.ndarray, pts: np.ndarray):
+    """Nodal Lagrange basis through `nodes` (reference coordinates) evaluated at `pts`."""
+    return _monomials(dim, p, pts) @ np.linalg.inv(_monomials(dim, p, nodes))
+
+
+def p1_at(dim: int, nodes: np.ndarray):
+    """[ndof, dim+1] P1 (barycentric) values of the vertices at the solution nodes."""
+    lam = [-(np.sum(nodes, 1) + (dim - 2)) / 2] + [(1 + nodes[:, d]) / 2 for d in range(dim)]
+    return np.stack(lam, 1)
+
+
+def _ramp(se, s0, kappa, eps0):
+    return np.where(se < s0 - kappa, 0.0,
+                    np.where(se > s0 + kappa, eps0,
+                             0.5 * eps0 * (1 + np.sin(np.pi * (se - s0) / (2 * kappa)))))
+
+
+def sensor_cells(dim, p, sol_nodes, geo_coords, geo_conn, sol_conn, u0, kappa=5.0, factor=1.0,
+                 blend=False):
+    """Cellwise artificial viscosity (blend=False) or ViscosityIndicator blending coefficient
+    (blend=True) of the first state component u0 [nnodes] on affine simplices."""
+    qp, qw = _simplex_rule(dim, p + 2)
+    Vn = lagrange_at(dim, p, sol_nodes, qp)
+    Vm, deg = _dubiner(dim, p, qp)
+    # the modes of degree p switched off; at p = 1 the reference marks every mode, the
+    # constant included, as leading (mesh/shape_function/DubinerExpansionTriag.cpp:460-467,
+    # DubinerExpansionTetra.cpp:715-723), so u_{p-1} = 0 there
+    Vl = Vm * (deg < p) if p > 1 else 0.0 * Vm
+    X = geo_coords[geo_conn[:, :dim + 1]]     # [nc, dim+1, dim] vertex coordinates
+    J = np.stack([X[:, k + 1] - X[:, 0] for k in range(dim)], 2) / 2  # dx/dxi
+    jdet = np.linalg.det(J)
+    out = np.empty(len(sol_conn))
+    s0 = 1.0 / p ** 4
+    for c in range(len(sol_conn)):
+        wj = jdet[c] * qw
+        uq = Vn @ u0[sol_conn[c]]
+        M = (Vm * wj[:, None]).T @ Vm
+        cm = np.linalg.solve(M, (Vm * (wj * uq)[:, None]).sum(0))
+        uq = Vm @ cm
+        ul = Vl @ cm
+        nom = np.sum(wj * (uq - ul) ** 2)
+        den = np.sum(wj * uq * uq)
+        Se = 0.0 if den <= 1e-10 else nom / den
+        with np.errstate(divide="ignore"):
+            se = np.log(Se) / np.log(10.0)
+        if blend:
+            out[c] = _ramp(se, s0, kappa, 1.0)
+        else:
+            h = np.sum(wj) ** (1.0 / dim)
+            out[c] = factor * _ramp(se, s0, kappa, h / p)
+    return out
+
+
+def nodal_from_cells(f_cells, sol_conn, nnodes, P1):
+    """Cell values -> nodal values (see the module docstring). P1 [ndof, nvert]."""
+    nvert = P1.shape[1]
+    f = np.zeros(nnodes)
+    vert = sol_conn[:, :nvert]
+    np.maximum.at(f, vert.ravel(), np.repeat(f_cells, nvert))
+    for c in range(len(sol_conn)):
+        fv = f[vert[c]]
+        for n in range(nvert, sol_conn.shape[1]):
+            f[sol_conn[c, n]] = sum(P1[n, i] * fv[i] for i in range(nvert))
+    return f
+
+
+def blend_cells(kind, sol_conn, u0, param=None):
+    """LF_Blend / WongJansen cellwise blending coefficients of the first state component."""
+    uc = u0[sol_conn]
+    uavg = uc.sum(1) / sol_conn.shape[1]
+    if kind == "LF_Blend":
+        ksi = np.max(np.abs(uc - uavg[:, None]) / (np.abs(uc) + np.abs(uavg)[:, None] + 1e-12), 1)
+        th = np.zeros(int(sol_conn.max()) + 1)
+        np.maximum.at(th, sol_conn.ravel(), np.repeat(ksi, sol_conn.shape[1]))
+        return 1.0 - th[sol_conn].max(1)
+    if kind == "WongJansen":
+        u_inf = 1e-14 if param is None else param
+        t = (uc * uc - (uavg * uavg)[:, None]) ** 2
+        nom = np.zeros(len(uc))
+        den = np.full(len(uc), 1.0 * u_inf ** 4)
+        for n in range(uc.shape[1]):
+            nom += t[:, n]
+            den += t[:, n]
+        return nom / den
+    raise ValueError(kind)

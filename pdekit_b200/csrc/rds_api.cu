@@ -72,6 +72,20 @@ struct rds_ctx
   double *d_theta   = nullptr; // PGB Jacobians: per-cell blending coefficients of one group
   long long theta_cap = 0;
 
+  // stabilisation (rds_stab.cu): external nodal blending coefficient read by PGB cells, nodal
+  // artificial viscosity added by PGLDA cells, scratch cell / node values; per group the
+  // sensor tables (w, Vn, R), the vertex interpolant P1 and device copies of the tables of the
+  // viscous term. All in 'extra'.
+  double *d_blend = nullptr, *d_av = nullptr, *d_cellf = nullptr, *d_nodef = nullptr;
+  bool blend_on = false, av_on = false;
+  struct StabTab
+  {
+    int nq = 0, nvert = 0;
+    double *w = nullptr, *Vn = nullptr, *R = nullptr, *P1 = nullptr;
+    double *vw = nullptr, *vV = nullptr, *vdV = nullptr, *vdVgeo = nullptr;
+  };
+  std::vector<StabTab> stab;
+
   // pipelined host-buffer steps (rds_step_host): copy streams, double-buffered staging
   cudaStream_t h_in = nullptr, h_out = nullptr;
   cudaEvent_t ev_in_ready[2] = {nullptr, nullptr}, ev_in_free[2] = {nullptr, nullptr};
@@ -262,6 +276,35 @@ CellArgs cell_args(rds_ctx *ctx, const HostCellGroup &g, const int *stop)
   a.gamma      = ctx->desc.gamma;
   a.status     = ctx->d_status;
   a.stop       = stop;
+  a.blend      = ctx->blend_on ? ctx->d_blend : nullptr;
+  return a;
+}
+
+ViscArgs visc_args(rds_ctx *ctx, size_t ig, const int *stop)
+{
+  const HostCellGroup &g   = ctx->groups[ig];
+  const rds_ctx::StabTab &t = ctx->stab[ig];
+  ViscArgs a{};
+  a.ncells     = g.desc.ncells;
+  a.ndof       = g.desc.ndof;
+  a.nq         = (int)g.w.size();
+  a.ngeo       = g.desc.ngeo;
+  a.nnodes     = ctx->desc.nnodes;
+  a.ngeo_nodes = ctx->desc.ngeo_nodes;
+  a.affine     = g.affine ? 1 : 0;
+  a.sol_conn   = g.d_sol_conn;
+  a.geo_conn   = g.d_geo_conn;
+  a.X          = ctx->d_X;
+  a.u          = ctx->d_u;
+  a.eps        = ctx->d_av;
+  a.w          = t.vw;
+  a.V          = t.vV;
+  a.dV         = t.vdV;
+  a.dVgeo      = t.vdVgeo;
+  a.contrib    = ctx->d_contrib;
+  a.S          = ctx->S;
+  a.slot_base  = g.slot_base;
+  a.stop       = stop;
   return a;
 }
 
@@ -355,11 +398,12 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
     if (st != RDS_OK)
       return st;
   }
-  for (const HostCellGroup &g : ctx->groups)
+  for (size_t ig = 0; ig < ctx->groups.size(); ++ig)
   {
-    const CellArgs a = cell_args(ctx, g, stop);
-    rds_status st    = launch(ctx, [&](const char **name) {
-      if (ctx->active_precision == RDS_MIXED && ctx->use_tc && g.d_tc)
+    const HostCellGroup &g = ctx->groups[ig];
+    const CellArgs a       = cell_args(ctx, g, stop);
+    rds_status st          = launch(ctx, [&](const char **name) {
+      if (ctx->active_precision == RDS_MIXED && ctx->use_tc && g.d_tc && !ctx->blend_on)
       {
         // FP32 cells with the basis contractions on the tensor cores, persistent CTAs
         const int ntiles = (g.desc.ncells + 127) / 128;
@@ -374,6 +418,16 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
     });
     if (st != RDS_OK)
       return st;
+    // PGLDA with a nodal artificial viscosity: the viscous term added to the group's slots
+    if (ctx->av_on && g.scheme == RDS_PGLDA)
+    {
+      const ViscArgs va = visc_args(ctx, ig, stop);
+      st                = launch(ctx, [&](const char **name) {
+        return launch_viscous(va, d.dim, d.neq, ctx->stream, name);
+      });
+      if (st != RDS_OK)
+        return st;
+    }
   }
   if (fork)
   {
@@ -1045,6 +1099,9 @@ rds_status rds_element_jacobians(rds_ctx *ctx, int group, double *jac)
   if (ctx->nprob > 0)
     return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_element_jacobians: not in batched contexts");
   const HostCellGroup &g = ctx->groups[group];
+  if (ctx->blend_on && ctx->desc.scheme == RDS_PGB)
+    return fail(ctx, RDS_ERR_UNSUPPORTED,
+                "rds_element_jacobians: PGB with an external blending coefficient");
   CellArgs a;
   rds_status st = jacobian_args(ctx, (size_t)group, &a);
   if (st != RDS_OK)
@@ -1189,6 +1246,238 @@ rds_status rds_assemble_jacobian(rds_ctx *ctx, double *values)
 // h_out). Buffers alternate between calls, so the upload of the next call and the download of
 // the previous one overlap this call's compute; events keep a buffer from being overwritten
 // while a copy still reads it.
+// ---- stabilisation fields and operators --------------------------------------------------
+
+static rds_status stab_alloc(rds_ctx *ctx, double **p, size_t n)
+{
+  const rds_status st = dalloc(ctx, p, n);
+  if (st == RDS_OK)
+    ctx->extra.push_back(*p);
+  return st;
+}
+
+static rds_status stab_upload(rds_ctx *ctx, double **p, const double *h, size_t n)
+{
+  rds_status st;
+  if ((st = stab_alloc(ctx, p, n)) != RDS_OK || (st = upload(ctx, *p, h, n)) != RDS_OK)
+    return st;
+  return RDS_OK;
+}
+
+static rds_status stab_check(rds_ctx *ctx, const char *fn)
+{
+  if (!ctx)
+    return RDS_ERR_INVALID;
+  if (!ctx->finalized)
+    return fail(ctx, RDS_ERR_INVALID, std::string(fn) + ": not finalized");
+  if (ctx->nprob > 0)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, std::string(fn) + ": not in batched contexts");
+  ctx->stab.resize(ctx->groups.size());
+  return RDS_OK;
+}
+
+// device copies of the residual tables each group's viscous term reads
+static rds_status ensure_visc_tables(rds_ctx *ctx)
+{
+  for (size_t ig = 0; ig < ctx->groups.size(); ++ig)
+  {
+    const HostCellGroup &g = ctx->groups[ig];
+    rds_ctx::StabTab &t    = ctx->stab[ig];
+    if (t.vw)
+      continue;
+    rds_status st;
+    if ((st = stab_upload(ctx, &t.vw, g.w.data(), g.w.size())) ||
+        (st = stab_upload(ctx, &t.vV, g.V.data(), g.V.size())) ||
+        (st = stab_upload(ctx, &t.vdV, g.dV.data(), g.dV.size())) ||
+        (st = stab_upload(ctx, &t.vdVgeo, g.dVgeo.data(), g.dVgeo.size())))
+      return st;
+  }
+  return RDS_OK;
+}
+
+static rds_status set_field(rds_ctx *ctx, const double *h, double **d, bool *on)
+{
+  release_graph(ctx); // captured iterations change with the field's presence
+  if (!h)
+  {
+    *on = false;
+    return RDS_OK;
+  }
+  rds_status st;
+  if (!*d && (st = stab_alloc(ctx, d, ctx->desc.nnodes)) != RDS_OK)
+    return st;
+  if ((st = upload(ctx, *d, h, ctx->desc.nnodes)) != RDS_OK)
+    return st;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  *on = true;
+  return RDS_OK;
+}
+
+rds_status rds_set_blending_coeff(rds_ctx *ctx, const double *theta)
+{
+  const rds_status st = stab_check(ctx, "rds_set_blending_coeff");
+  if (st != RDS_OK)
+    return st;
+  return set_field(ctx, theta, &ctx->d_blend, &ctx->blend_on);
+}
+
+rds_status rds_set_artificial_viscosity(rds_ctx *ctx, const double *eps)
+{
+  rds_status st = stab_check(ctx, "rds_set_artificial_viscosity");
+  if (st != RDS_OK || (eps && (st = ensure_visc_tables(ctx)) != RDS_OK))
+    return st;
+  return set_field(ctx, eps, &ctx->d_av, &ctx->av_on);
+}
+
+rds_status rds_set_stab_tables(rds_ctx *ctx, int group, int nq, const double *w, const double *Vn,
+                               const double *R, int nvert, const double *P1)
+{
+  rds_status st = stab_check(ctx, "rds_set_stab_tables");
+  if (st != RDS_OK)
+    return st;
+  if (group < 0 || group >= (int)ctx->groups.size())
+    return fail(ctx, RDS_ERR_INVALID, "rds_set_stab_tables: invalid group");
+  const int ndof      = ctx->groups[group].desc.ndof;
+  rds_ctx::StabTab &t = ctx->stab[group];
+  if (nq < 0 || nvert < 1 || nvert > ndof || !P1 || (nq > 0 && (!w || !Vn || !R)))
+    return fail(ctx, RDS_ERR_INVALID, "rds_set_stab_tables: invalid sizes or missing tables");
+  if ((t.P1 && t.nvert != nvert) || (t.w && t.nq != nq))
+    return fail(ctx, RDS_ERR_INVALID, "rds_set_stab_tables: table sizes differ from the first call");
+  if ((!t.P1 && (st = stab_alloc(ctx, &t.P1, (size_t)ndof * nvert))) ||
+      (st = upload(ctx, t.P1, P1, (size_t)ndof * nvert)))
+    return st;
+  t.nvert = nvert;
+  if (nq > 0)
+  {
+    if ((!t.w && ((st = stab_alloc(ctx, &t.w, nq)) || (st = stab_alloc(ctx, &t.Vn, (size_t)nq * ndof)) ||
+                  (st = stab_alloc(ctx, &t.R, (size_t)nq * ndof)))) ||
+        (st = upload(ctx, t.w, w, nq)) || (st = upload(ctx, t.Vn, Vn, (size_t)nq * ndof)) ||
+        (st = upload(ctx, t.R, R, (size_t)nq * ndof)))
+      return st;
+    t.nq = nq;
+  }
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RDS_OK;
+}
+
+rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1, int install,
+                                     double *cells_out, double *nodes_out)
+{
+  rds_status st = stab_check(ctx, "rds_compute_stabilisation");
+  if (st != RDS_OK)
+    return st;
+  const int G = (int)ctx->groups.size(), N = ctx->desc.nnodes;
+  const bool sensor = op == RDS_STAB_ART_VISC || op == RDS_STAB_INDICATOR || op == RDS_STAB_BLEND_VISC;
+  const bool nodal  = install || nodes_out;
+  if (op < RDS_STAB_ART_VISC || op > RDS_STAB_BLEND_WONG_JANSEN ||
+      (op == RDS_STAB_INDICATOR && nodal))
+    return fail(ctx, RDS_ERR_INVALID, "rds_compute_stabilisation: unknown operator, or a nodal "
+                                      "field of the normalised indicator");
+  if (G > kStabMaxGroups)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_compute_stabilisation: more than 8 cell groups");
+  if (sensor && !(p0 > 0.0))
+    return fail(ctx, RDS_ERR_INVALID, "rds_compute_stabilisation: kappa must be positive");
+  long long wc = 0, sc = 0;
+  for (int k = 0; k < G; ++k)
+  {
+    const rds_ctx::StabTab &t = ctx->stab[k];
+    if (sensor && (t.nq == 0 || !ctx->groups[k].affine))
+      return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_compute_stabilisation: the smoothness sensor "
+                                            "needs affine simplex cells with sensor tables");
+    if (nodal && t.nvert == 0)
+      return fail(ctx, RDS_ERR_INVALID, "rds_compute_stabilisation: no vertex interpolant "
+                                        "(rds_set_stab_tables) for a group");
+    wc += ctx->groups[k].desc.ncells;
+    sc += (long long)ctx->groups[k].desc.ncells * ctx->groups[k].desc.ndof;
+  }
+  if ((!ctx->d_cellf && (st = stab_alloc(ctx, &ctx->d_cellf, wc))) ||
+      (!ctx->d_nodef && (st = stab_alloc(ctx, &ctx->d_nodef, N))))
+    return st;
+  cudaStream_t s = ctx->stream;
+  for (int k = 0; k < G; ++k)
+  {
+    const HostCellGroup &g    = ctx->groups[k];
+    const rds_ctx::StabTab &t = ctx->stab[k];
+    double *out               = ctx->d_cellf + g.ws_base;
+    if (sensor)
+    {
+      SensorArgs a{};
+      a.ncells     = g.desc.ncells;
+      a.ndof       = g.desc.ndof;
+      a.nq         = t.nq;
+      a.order      = g.desc.order;
+      a.ngeo_nodes = ctx->desc.ngeo_nodes;
+      a.blend      = op == RDS_STAB_BLEND_VISC;
+      a.sol_conn   = g.d_sol_conn;
+      a.geo_conn   = g.d_geo_conn;
+      a.X          = ctx->d_X;
+      a.u          = ctx->d_u;
+      a.w          = t.w;
+      a.Vn         = t.Vn;
+      a.R          = t.R;
+      a.kappa      = p0;
+      a.factor     = op == RDS_STAB_ART_VISC ? p1 : 1.0;
+      a.out        = out;
+      RDS_CUDA(launch_sensor(a, ctx->desc.dim, s));
+    }
+    else
+      RDS_CUDA(launch_blend_cells(op == RDS_STAB_BLEND_LF ? 0 : 1, g.desc.ncells, g.desc.ndof,
+                                  g.d_sol_conn, ctx->d_u, p0, out, s));
+  }
+  if (op == RDS_STAB_INDICATOR)
+    RDS_CUDA(launch_normalise_max((int)wc, ctx->d_cellf, s));
+  if (op == RDS_STAB_BLEND_LF)
+  {
+    RDS_CUDA(launch_node_max(N, ctx->d_row, ctx->d_ent_ws, wc, ctx->d_cellf, ctx->d_nodef, s));
+    for (int k = 0; k < G; ++k)
+    {
+      const HostCellGroup &g = ctx->groups[k];
+      RDS_CUDA(launch_lf_finish(g.desc.ncells, g.desc.ndof, g.d_sol_conn, ctx->d_nodef,
+                                ctx->d_cellf + g.ws_base, s));
+    }
+  }
+  if (cells_out)
+    RDS_CUDA(cudaMemcpyAsync(cells_out, ctx->d_cellf, wc * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+  if (nodal)
+  {
+    double *target = ctx->d_nodef;
+    if (install)
+    {
+      double **d = op == RDS_STAB_ART_VISC ? &ctx->d_av : &ctx->d_blend;
+      if ((!*d && (st = stab_alloc(ctx, d, N))) ||
+          (op == RDS_STAB_ART_VISC && (st = ensure_visc_tables(ctx))))
+        return st;
+      target = *d;
+    }
+    StabGroups sg{};
+    sg.n = G;
+    for (int k = 0; k < G; ++k)
+    {
+      const HostCellGroup &g = ctx->groups[k];
+      sg.slot_base[k]        = g.slot_base;
+      sg.ws_base[k]          = g.ws_base;
+      sg.ncells[k]           = g.desc.ncells;
+      sg.ndof[k]             = g.desc.ndof;
+      sg.nvert[k]            = ctx->stab[k].nvert;
+      sg.sol_conn[k]         = g.d_sol_conn;
+      sg.P1[k]               = ctx->stab[k].P1;
+    }
+    RDS_CUDA(launch_cells_to_nodes(N, ctx->d_row, ctx->d_ent_slot, sc, sg, ctx->d_cellf, target,
+                                   s));
+    if (nodes_out)
+      RDS_CUDA(cudaMemcpyAsync(nodes_out, target, (size_t)N * sizeof(double),
+                               cudaMemcpyDeviceToHost, s));
+    if (install)
+    {
+      release_graph(ctx);
+      (op == RDS_STAB_ART_VISC ? ctx->av_on : ctx->blend_on) = true;
+    }
+  }
+  RDS_CUDA(cudaStreamSynchronize(s));
+  return RDS_OK;
+}
+
 static rds_status step_host_init(rds_ctx *ctx)
 {
   if (ctx->h_in)

@@ -528,6 +528,24 @@ __global__ void __launch_bounds__(NT)
     theta                 = fabs(phi0) / (abs_phiN + 1.e-6);
   }
   const double wmax = group_max<G>(double(wsmax));
+  // external nodal blending coefficient: theta_n of the lane's nodes, the N part dropped when
+  // all of the cell's are below 1e-6 (PGRDMExplicitCellWorker.hpp:508-517,
+  // PGB.hpp:141-148,467-477); the group max runs in every lane of the warp
+  double tn[NPT];
+  bool skip = false;
+  if (SCHEME == RDS_PGB && a.blend)
+  {
+    double tmax = 0.0;
+#pragma unroll
+    for (int s = 0; s < NPT; ++s)
+    {
+      const int n = lane + s * G;
+      tn[s]       = (live && n < NDOF) ? __ldg(a.blend + __ldg(a.sol_conn + (size_t)n * a.ncells + c))
+                                       : 0.0;
+      tmax        = fmax(tmax, tn[s]);
+    }
+    skip = group_max<G>(tmax) < 1.e-6;
+  }
   if (live)
   {
 #pragma unroll
@@ -540,7 +558,9 @@ __global__ void __launch_bounds__(NT)
 #pragma unroll
         for (int e = 0; e < NEQ; ++e)
         {
-          const double r = (SCHEME == RDS_PGLDA) ? lda[s][e] : lda[s][e] + theta * diss[s][e];
+          double r = (SCHEME == RDS_PGLDA) ? lda[s][e] : lda[s][e] + theta * diss[s][e];
+          if (SCHEME == RDS_PGB && a.blend)
+            r = skip ? lda[s][e] : lda[s][e] + tn[s] * diss[s][e];
           a.contrib[e * a.S + slot0] = r; // write-back: the gather reads it from L2
         }
       }

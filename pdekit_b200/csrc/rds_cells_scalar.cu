@@ -30,7 +30,9 @@ namespace rds
 namespace
 {
 
-template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO>
+// EXT: the external nodal blending coefficient may be set (single contexts; batched contexts
+// never hold one, and the branch costs their kernels registers)
+template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, bool EXT = true>
 __device__ __forceinline__ void scalar_cell(const CellArgs &a,
                                             const Tables<T, 2, NDOF, NQ, NFL, NGEO> &tb,
                                             const int c)
@@ -233,11 +235,30 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
   }
 
   double *out = a.contrib + a.slot_base + c;
-#pragma unroll
-  for (int n = 0; n < NDOF; ++n)
+  if (EXT && SCHEME == RDS_PGB && a.blend)
   {
-    const double r = (SCHEME == RDS_PGLDA) ? lda[n] : lda[n] + theta * diss[n];
-    out[(size_t)n * a.ncells] = r; // write-back: the gather reads it from L2
+    // external nodal blending coefficient: theta_n of the cell's nodes, the N part dropped
+    // when all are below 1e-6 (PGRDMExplicitCellWorker.hpp:508-517, PGB.hpp:141-148,467-477)
+    double tn[NDOF], tmax = 0.0;
+#pragma unroll
+    for (int n = 0; n < NDOF; ++n)
+    {
+      tn[n] = __ldg(a.blend + __ldg(a.sol_conn + (size_t)n * a.ncells + c));
+      tmax  = fmax(tmax, tn[n]);
+    }
+    const bool skip = tmax < 1.e-6;
+#pragma unroll
+    for (int n = 0; n < NDOF; ++n)
+      out[(size_t)n * a.ncells] = skip ? lda[n] : lda[n] + tn[n] * diss[n];
+  }
+  else
+  {
+#pragma unroll
+    for (int n = 0; n < NDOF; ++n)
+    {
+      const double r = (SCHEME == RDS_PGLDA) ? lda[n] : lda[n] + theta * diss[n];
+      out[(size_t)n * a.ncells] = r; // write-back: the gather reads it from L2
+    }
   }
   a.wsc[a.ws_base + c] = vol * double(wsmax);
 }
@@ -287,7 +308,7 @@ __global__ void __launch_bounds__(128, kMinBlocks<PHYS, T, NDOF>)
     }
     const int c = a.bt.cbeg[lo] + (t - prefix[lo]) * (int)blockDim.x + (int)threadIdx.x;
     if (c < a.bt.cend[lo])
-      scalar_cell<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO>(a, tb, c);
+      scalar_cell<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, false>(a, tb, c);
   }
 }
 

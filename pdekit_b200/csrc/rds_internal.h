@@ -146,6 +146,7 @@ struct CellArgs
   const int *stop; // nonzero: skip the work (converged loop)
   BatchTileMap bt; // batch mode only
   double *theta;   // PGB: the cell's blending coefficient [ncells] when not null (Jacobians)
+  const double *blend; // PGB: external nodal blending coefficient [nnodes] when not null
 };
 
 struct BCArgs
@@ -264,5 +265,52 @@ cudaError_t launch_unpack_interface(int n, int neq, int nnodes, const int32_t *n
 cudaError_t launch_finish(int nnodes, int neq, double cfl, int update, const double *vol,
                           const double *ws, const double *res, double *dt, double *u,
                           const uint8_t *owned, double *part, double *sq, cudaStream_t s);
+
+// stabilisation operators (rds_stab.cu)
+constexpr int kStabMaxGroups = 8;
+// cell groups as the node-parallel kernels decode them from the gather lists
+struct StabGroups
+{
+  int n;
+  long long slot_base[kStabMaxGroups];
+  long long ws_base[kStabMaxGroups];
+  int ncells[kStabMaxGroups], ndof[kStabMaxGroups], nvert[kStabMaxGroups];
+  const int32_t *sol_conn[kStabMaxGroups];
+  const double *P1[kStabMaxGroups]; // [ndof][nvert] vertex interpolant at the nodes
+};
+struct ViscArgs
+{
+  int ncells, ndof, nq, ngeo, nnodes, ngeo_nodes, affine;
+  const int32_t *sol_conn, *geo_conn;
+  const double *X, *u, *eps;
+  const double *w, *V, *dV, *dVgeo; // [nq], [nq][ndof], [D][nq][ndof], [D][nq][ngeo]
+  double *contrib;
+  long long S, slot_base;
+  const int *stop;
+};
+struct SensorArgs
+{
+  int ncells, ndof, nq, order, ngeo_nodes, blend;
+  const int32_t *sol_conn, *geo_conn;
+  const double *X, *u;           // u: the first state component [nnodes]
+  const double *w, *Vn, *R;      // [nq], [nq][ndof], [nq][ndof]
+  double kappa, factor;
+  double *out;                   // [ncells]
+};
+cudaError_t launch_viscous(const ViscArgs &a, int dim, int neq, cudaStream_t s, const char **name);
+cudaError_t launch_sensor(const SensorArgs &a, int dim, cudaStream_t s);
+cudaError_t launch_normalise_max(int n, double *v, cudaStream_t s);
+// kind 0: LF_Blend cell values ksi (pass 1), 1: Wong-Jansen (u_inf)
+cudaError_t launch_blend_cells(int kind, int ncells, int ndof, const int32_t *sol_conn,
+                               const double *u, double param, double *out, cudaStream_t s);
+// LF_Blend pass 2 / 3: nodal max of the cells' values; 1 - max over each cell's nodes
+cudaError_t launch_node_max(int nnodes, const int32_t *row, const int32_t *ent_ws, long long wcells,
+                            const double *cellf, double *nodef, cudaStream_t s);
+cudaError_t launch_lf_finish(int ncells, int ndof, const int32_t *sol_conn, const double *nodef,
+                             double *out, cudaStream_t s);
+// cell values -> nodal field: vertex max, then the vertex interpolant at the other nodes
+cudaError_t launch_cells_to_nodes(int nnodes, const int32_t *row, const int32_t *ent_slot,
+                                  long long scells, const StabGroups &g, const double *cellf,
+                                  double *nodef, cudaStream_t s);
 
 } // namespace rds

@@ -1,0 +1,532 @@
+// Stabilisation operators either side of the cell residual: the shock sensor and blending
+// coefficients that produce nodal fields, the cell-to-node transfer, and the artificial
+// viscosity term that PGLDA adds to its nodal residuals.
+//
+//   viscous    PGLDA cells with a nodal artificial viscosity eps: at every quadrature point
+//              eps_q = sum_n V(q,n) eps_n and, when eps_q != 0,
+//              res_n += w_q detJ_q eps_q grad phi_n . grad u_e(q)  for every equation e
+//              (src/solver/rdm/cellsplitters/PGLDA.hpp:245-256, the viscosity interpolated as
+//              in assembly/PGRDMExplicitCellWorker.hpp:519-533). Runs after the cell kernel of
+//              the group and adds to its contribution slots; a group of G lanes per cell, a
+//              lane per node, the sums over the nodes (eps_q, grad u) as group shuffles.
+//   sensor     the Persson-Peraire smoothness sensor of the first state component
+//              (src/solver/art_visc/ArtificialViscosity.hpp:300-455,
+//              blending_coeff/ArtViscIndicatorCoeffImpl.hpp:261-425), one thread per affine
+//              simplex: Se = sum_q wj (R u)_q^2 / sum_q wj (Vn u)_q^2 (0 if the denominator is
+//              <= 1e-10), R mapping nodal values to u - u_{p-1} at the points (u_{p-1} the
+//              modal truncation of the reference, an L2 projection because its simplex bases
+//              are orthogonal; the host builds R), se = log10 Se, s0 = 1/p^4, value 0 / eps0 /
+//              0.5 eps0 (1 + sin(pi (se - s0) / (2 kappa))) below / above / within
+//              s0 -+ kappa, eps0 = factor h / p (h = |K|^(1/D)) or 1 for the blending form.
+//   blend      LF_Blend (blending_coeff/LFBlendingCoeffImpl.hpp:76-126): per cell
+//              ksi = max_n |u_n - u_avg| / (|u_n| + |u_avg| + 1e-12), per node the max over its
+//              cells (node-parallel over the gather lists), per cell 1 - max over its nodes;
+//              Wong-Jansen (WongJansenBlendingCoeffImpl.hpp:80-116): per cell
+//              sum_n t_n / (u_inf^4 + sum_n t_n), t_n = (u_n^2 - u_avg^2)^2.
+//   transfer   cell values -> nodal field (interpolation/mesh_function/MeshFunctionTools.hpp:
+//              52-397, no adaptation): every vertex node max(0, max over its cells), every
+//              other node the vertex interpolant of the last cell (in cell order) holding it.
+//              Node-parallel over the gather lists, which hold each node's cells in ascending
+//              order, so the result does not depend on scheduling.
+
+#include "rds_internal.h"
+
+namespace rds
+{
+
+namespace
+{
+
+constexpr double kPi = 3.14159265358979323846;
+
+template <int G>
+__device__ __forceinline__ double group_add(double v)
+{
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1)
+    v += __shfl_xor_sync(0xffffffffu, v, o, G);
+  return v;
+}
+
+template <int D>
+__device__ __forceinline__ double invert(const double J[D][D], double iJ[D][D])
+{
+  if constexpr (D == 2)
+  {
+    const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    const double r   = 1.0 / det;
+    iJ[0][0]         = r * J[1][1];
+    iJ[1][1]         = r * J[0][0];
+    iJ[0][1]         = -r * J[0][1];
+    iJ[1][0]         = -r * J[1][0];
+    return det;
+  }
+  else
+  {
+    const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+    const double r   = 1.0 / det;
+    iJ[0][0]         = r * c00;
+    iJ[1][0]         = r * c01;
+    iJ[2][0]         = r * c02;
+    iJ[0][1]         = r * (J[0][2] * J[2][1] - J[0][1] * J[2][2]);
+    iJ[1][1]         = r * (J[0][0] * J[2][2] - J[0][2] * J[2][0]);
+    iJ[2][1]         = r * (J[0][1] * J[2][0] - J[0][0] * J[2][1]);
+    iJ[0][2]         = r * (J[0][1] * J[1][2] - J[0][2] * J[1][1]);
+    iJ[1][2]         = r * (J[0][2] * J[1][0] - J[0][0] * J[1][2]);
+    iJ[2][2]         = r * (J[0][0] * J[1][1] - J[0][1] * J[1][0]);
+    return det;
+  }
+}
+
+// J[k][i] = d x_i / d xi_k at point q of cell c (every lane of the group computes it)
+template <int D>
+__device__ __forceinline__ void jacobian_at(const ViscArgs &a, int c, int q, double J[D][D])
+{
+#pragma unroll
+  for (int k = 0; k < D; ++k)
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      J[k][i] = 0.0;
+  for (int g = 0; g < a.ngeo; ++g)
+  {
+    const int v = __ldg(a.geo_conn + (size_t)g * a.ncells + c);
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+    {
+      const double d = __ldg(a.dVgeo + ((size_t)k * a.nq + q) * a.ngeo + g);
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+        J[k][i] += d * __ldg(a.X + (size_t)i * a.ngeo_nodes + v);
+    }
+  }
+}
+
+template <int D, int NEQ, int G>
+__global__ void __launch_bounds__(kBlock) viscous_cells(const ViscArgs a)
+{
+  if (a.stop && *a.stop)
+    return; // uniform over the grid
+  const int t     = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c     = t / G, n = t % G;
+  const bool live = c < a.ncells;
+  const bool mine = live && n < a.ndof;
+  double un[NEQ], en = 0.0;
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e)
+    un[e] = 0.0;
+  if (mine)
+  {
+    const int v = __ldg(a.sol_conn + (size_t)n * a.ncells + c);
+    en          = __ldg(a.eps + v);
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+      un[e] = __ldg(a.u + (size_t)e * a.nnodes + v);
+  }
+  double acc[NEQ];
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e)
+    acc[e] = 0.0;
+  double iJ[D][D], det = 0.0;
+  if (a.affine && live)
+  {
+    double J[D][D];
+    jacobian_at<D>(a, c, 0, J);
+    det = invert<D>(J, iJ);
+  }
+  for (int q = 0; q < a.nq; ++q)
+  {
+    if (!a.affine && live)
+    {
+      double J[D][D];
+      jacobian_at<D>(a, c, q, J);
+      det = invert<D>(J, iJ);
+    }
+    // eps at the point and the node's physical shape-function gradient
+    const double eq = group_add<G>(mine ? __ldg(a.V + (size_t)q * a.ndof + n) * en : 0.0);
+    double gp[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      gp[i] = 0.0;
+    if (mine)
+    {
+      double gr[D];
+#pragma unroll
+      for (int k = 0; k < D; ++k)
+        gr[k] = __ldg(a.dV + ((size_t)k * a.nq + q) * a.ndof + n);
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+      {
+        double s = iJ[i][0] * gr[0];
+#pragma unroll
+        for (int k = 1; k < D; ++k)
+          s += iJ[i][k] * gr[k];
+        gp[i] = s;
+      }
+    }
+    // grad u_e at the point (sum over the group's nodes), taken in every lane
+    double gu[NEQ][D];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+        gu[e][i] = group_add<G>(gp[i] * un[e]);
+    if (mine && eq != 0.0)
+    {
+      const double wj = __ldg(a.w + q) * det;
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+#pragma unroll
+        for (int i = 0; i < D; ++i)
+          acc[e] += (wj * eq * gp[i]) * gu[e][i];
+    }
+  }
+  if (mine)
+  {
+    const long long slot = a.slot_base + (long long)n * a.ncells + c;
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+      a.contrib[e * a.S + slot] += acc[e];
+  }
+}
+
+template <int D, int NEQ>
+cudaError_t launch_viscous_g(const ViscArgs &a, cudaStream_t s, const char **name)
+{
+  auto go = [&](auto kern, int G) {
+    const long long threads = (long long)a.ncells * G;
+    const int grid          = (int)((threads + kBlock - 1) / kBlock);
+    kern<<<grid, kBlock, 0, s>>>(a);
+    return cudaGetLastError();
+  };
+  if (name)
+    *name = "viscous_cells";
+  if (a.ndof <= 4)
+    return go(viscous_cells<D, NEQ, 4>, 4);
+  if (a.ndof <= 8)
+    return go(viscous_cells<D, NEQ, 8>, 8);
+  if (a.ndof <= 16)
+    return go(viscous_cells<D, NEQ, 16>, 16);
+  if (a.ndof <= 32)
+    return go(viscous_cells<D, NEQ, 32>, 32);
+  return cudaErrorInvalidValue;
+}
+
+__global__ void __launch_bounds__(kBlock) sensor_cells_2d(const SensorArgs a);
+__global__ void __launch_bounds__(kBlock) sensor_cells_3d(const SensorArgs a);
+
+template <int D>
+__device__ __forceinline__ void sensor_cell(const SensorArgs &a)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncells)
+    return;
+  // affine simplex on the reference element with vertices (-1,..,-1) and -1 + 2 e_k:
+  // d x / d xi_k = (X_{k+1} - X_0) / 2
+  double X0[D], J[D][D];
+  {
+    const int v0 = __ldg(a.geo_conn + c);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      X0[i] = __ldg(a.X + (size_t)i * a.ngeo_nodes + v0);
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+    {
+      const int v = __ldg(a.geo_conn + (size_t)(k + 1) * a.ncells + c);
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+        J[k][i] = 0.5 * (__ldg(a.X + (size_t)i * a.ngeo_nodes + v) - X0[i]);
+    }
+  }
+  double det;
+  if constexpr (D == 2)
+    det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+  else
+    det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) +
+          J[0][1] * (J[1][2] * J[2][0] - J[1][0] * J[2][2]) +
+          J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+
+  double nom = 0.0, den = 0.0, vol = 0.0;
+  for (int q = 0; q < a.nq; ++q)
+  {
+    double s = 0.0, r = 0.0;
+    for (int n = 0; n < a.ndof; ++n)
+    {
+      const double un = __ldg(a.u + __ldg(a.sol_conn + (size_t)n * a.ncells + c));
+      s += __ldg(a.Vn + (size_t)q * a.ndof + n) * un;
+      r += __ldg(a.R + (size_t)q * a.ndof + n) * un;
+    }
+    const double wj = det * __ldg(a.w + q);
+    vol += wj;
+    nom += wj * r * r;
+    den += wj * s * s;
+  }
+  const double Se = (den <= 1.e-10) ? 0.0 : nom / den;
+  const double se = log(Se) / log(10.0);
+  const double p  = (double)a.order;
+  const double s0 = 1.0 / (p * p * p * p);
+  const double e0 = a.blend ? 1.0 : a.factor * (pow(vol, 1.0 / D) / p);
+  double val;
+  if (se < s0 - a.kappa)
+    val = 0.0;
+  else if (se > s0 + a.kappa)
+    val = e0;
+  else
+    val = 0.5 * e0 * (1.0 + sin(kPi * (se - s0) / (2.0 * a.kappa)));
+  a.out[c] = val;
+}
+
+__global__ void __launch_bounds__(kBlock) sensor_cells_2d(const SensorArgs a)
+{
+  sensor_cell<2>(a);
+}
+__global__ void __launch_bounds__(kBlock) sensor_cells_3d(const SensorArgs a)
+{
+  sensor_cell<3>(a);
+}
+
+// one block: v /= max(v) unless max(v) < 1e-14 (ArtificialViscosity.hpp:257-279)
+__global__ void __launch_bounds__(kGBlock) normalise_max(int n, double *v)
+{
+  __shared__ double sm[kGBlock / 32];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    m = fmax(m, v[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0)
+    sm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  m = 0.0;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k)
+    m = fmax(m, sm[k]);
+  if (m < 1.e-14)
+    return;
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    v[i] /= m;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    blend_cells(int kind, int ncells, int ndof, const int32_t *__restrict__ conn,
+                const double *__restrict__ u, double param, double *__restrict__ out)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells)
+    return;
+  double avg = 0.0;
+  for (int n = 0; n < ndof; ++n)
+    avg += __ldg(u + __ldg(conn + (size_t)n * ncells + c));
+  avg /= ndof;
+  if (kind == 0)
+  {
+    double ksi = 0.0;
+    for (int n = 0; n < ndof; ++n)
+    {
+      const double un = __ldg(u + __ldg(conn + (size_t)n * ncells + c));
+      ksi             = fmax(ksi, fabs(un - avg) / (fabs(un) + fabs(avg) + 1.e-12));
+    }
+    out[c] = ksi;
+  }
+  else
+  {
+    const double ui2 = param * param;
+    double nom = 0.0, den = 1.0 * (ui2 * ui2);
+    for (int n = 0; n < ndof; ++n)
+    {
+      const double un = __ldg(u + __ldg(conn + (size_t)n * ncells + c));
+      const double d  = un * un - avg * avg;
+      const double t  = d * d;
+      nom += t;
+      den += t;
+    }
+    out[c] = nom / den;
+  }
+}
+
+__global__ void __launch_bounds__(kGBlock)
+    node_max(int nnodes, const int32_t *__restrict__ row, const int32_t *__restrict__ ent_ws,
+             long long wcells, const double *__restrict__ cellf, double *__restrict__ nodef)
+{
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nnodes)
+    return;
+  double m = 0.0;
+  for (int p = row[v]; p < row[v + 1]; ++p)
+  {
+    const int w = ent_ws[p];
+    if (w < wcells)
+      m = fmax(m, cellf[w]);
+  }
+  nodef[v] = m;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    lf_finish(int ncells, int ndof, const int32_t *__restrict__ conn,
+              const double *__restrict__ nodef, double *__restrict__ out)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells)
+    return;
+  double m = 0.0;
+  for (int n = 0; n < ndof; ++n)
+    m = fmax(m, nodef[__ldg(conn + (size_t)n * ncells + c)]);
+  out[c] = 1.0 - m;
+}
+
+// (group, cell, local node) of a cell contribution slot
+__device__ __forceinline__ int decode(const StabGroups &g, long long slot, int *c, int *n)
+{
+  for (int k = 0; k < g.n; ++k)
+  {
+    const long long off = slot - g.slot_base[k];
+    if (off >= 0 && off < (long long)g.ndof[k] * g.ncells[k])
+    {
+      *n = (int)(off / g.ncells[k]);
+      *c = (int)(off % g.ncells[k]);
+      return k;
+    }
+  }
+  return -1;
+}
+
+// pass 1: vertex nodes take max(0, max over their cells)
+__global__ void __launch_bounds__(kGBlock)
+    vertex_max(int nnodes, const int32_t *__restrict__ row, const int32_t *__restrict__ ent_slot,
+               long long scells, const StabGroups g, const double *__restrict__ cellf,
+               double *__restrict__ nodef)
+{
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nnodes)
+    return;
+  double m    = 0.0;
+  bool vertex = false;
+  for (int p = row[v]; p < row[v + 1]; ++p)
+  {
+    const long long slot = ent_slot[p];
+    if (slot >= scells)
+      break; // boundary-facet entries follow the cells
+    int c, n;
+    const int k = decode(g, slot, &c, &n);
+    if (k < 0 || n >= g.nvert[k])
+      break; // a node that is not a vertex of its cells
+    vertex = true;
+    m      = fmax(m, cellf[g.ws_base[k] + c]);
+  }
+  if (vertex)
+    nodef[v] = m;
+}
+
+// pass 2: other nodes take the vertex interpolant of the last cell holding them
+__global__ void __launch_bounds__(kGBlock)
+    interior_interp(int nnodes, const int32_t *__restrict__ row,
+                    const int32_t *__restrict__ ent_slot, long long scells, const StabGroups g,
+                    double *__restrict__ nodef)
+{
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nnodes)
+    return;
+  int k = -1, c = 0, n = 0;
+  for (int p = row[v]; p < row[v + 1]; ++p)
+  {
+    const long long slot = ent_slot[p];
+    if (slot >= scells)
+      break;
+    int cc, nn;
+    const int kk = decode(g, slot, &cc, &nn);
+    if (kk < 0 || nn < g.nvert[kk])
+      return; // a vertex (pass 1), or not a cell node
+    k = kk;
+    c = cc;
+    n = nn;
+  }
+  if (k < 0)
+    return;
+  const int nv     = g.nvert[k];
+  const double *P1 = g.P1[k] + (size_t)n * nv;
+  double f         = 0.0;
+  for (int i = 0; i < nv; ++i)
+    f += P1[i] * nodef[g.sol_conn[k][(size_t)i * g.ncells[k] + c]];
+  nodef[v] = f;
+}
+
+} // namespace
+
+cudaError_t launch_viscous(const ViscArgs &a, int dim, int neq, cudaStream_t s, const char **name)
+{
+  if (a.ncells == 0)
+    return cudaSuccess;
+  if (dim == 2 && neq == 1)
+    return launch_viscous_g<2, 1>(a, s, name);
+  if (dim == 2 && neq == 4)
+    return launch_viscous_g<2, 4>(a, s, name);
+  if (dim == 3 && neq == 5)
+    return launch_viscous_g<3, 5>(a, s, name);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_sensor(const SensorArgs &a, int dim, cudaStream_t s)
+{
+  if (a.ncells == 0)
+    return cudaSuccess;
+  const int grid = (a.ncells + kBlock - 1) / kBlock;
+  if (dim == 2)
+    sensor_cells_2d<<<grid, kBlock, 0, s>>>(a);
+  else
+    sensor_cells_3d<<<grid, kBlock, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_normalise_max(int n, double *v, cudaStream_t s)
+{
+  if (n == 0)
+    return cudaSuccess;
+  normalise_max<<<1, kGBlock, 0, s>>>(n, v);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_blend_cells(int kind, int ncells, int ndof, const int32_t *sol_conn,
+                               const double *u, double param, double *out, cudaStream_t s)
+{
+  if (ncells == 0)
+    return cudaSuccess;
+  blend_cells<<<(ncells + kBlock - 1) / kBlock, kBlock, 0, s>>>(kind, ncells, ndof, sol_conn, u,
+                                                                param, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_node_max(int nnodes, const int32_t *row, const int32_t *ent_ws, long long wcells,
+                            const double *cellf, double *nodef, cudaStream_t s)
+{
+  node_max<<<(nnodes + kGBlock - 1) / kGBlock, kGBlock, 0, s>>>(nnodes, row, ent_ws, wcells,
+                                                                 cellf, nodef);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lf_finish(int ncells, int ndof, const int32_t *sol_conn, const double *nodef,
+                             double *out, cudaStream_t s)
+{
+  if (ncells == 0)
+    return cudaSuccess;
+  lf_finish<<<(ncells + kBlock - 1) / kBlock, kBlock, 0, s>>>(ncells, ndof, sol_conn, nodef, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cells_to_nodes(int nnodes, const int32_t *row, const int32_t *ent_slot,
+                                  long long scells, const StabGroups &g, const double *cellf,
+                                  double *nodef, cudaStream_t s)
+{
+  const int grid = (nnodes + kGBlock - 1) / kGBlock;
+  cudaError_t e  = cudaMemsetAsync(nodef, 0, (size_t)nnodes * sizeof(double), s);
+  if (e != cudaSuccess)
+    return e;
+  vertex_max<<<grid, kGBlock, 0, s>>>(nnodes, row, ent_slot, scells, g, cellf, nodef);
+  if ((e = cudaGetLastError()) != cudaSuccess)
+    return e;
+  interior_interp<<<grid, kGBlock, 0, s>>>(nnodes, row, ent_slot, scells, g, nodef);
+  return cudaGetLastError();
+}
+
+} // namespace rds

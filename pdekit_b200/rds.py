@@ -44,7 +44,9 @@ EXPORTS = ["rds_create", "rds_add_cell_group", "rds_add_bc", "rds_finalize", "rd
            "rds_kernel_timing", "rds_kernel_times", "rds_launch_count", "rds_destroy",
            "rds_last_error", "rds_version", "rds_run", "rds_measure_peak", "rds_set_option",
            "rds_set_problems", "rds_add_batch_cell_group", "rds_add_batch_bc",
-           "rds_iterate_batch", "rds_autotune", "rds_residual_norm_noalloc"]
+           "rds_iterate_batch", "rds_autotune", "rds_residual_norm_noalloc",
+           "rds_set_blending_coeff", "rds_set_artificial_viscosity", "rds_set_stab_tables",
+           "rds_compute_stabilisation"]
 
 
 class RDSError(RuntimeError):
@@ -128,6 +130,10 @@ def lib():
         "rds_assemble_jacobian": ([vp, vp], ip),
         "rds_step_host": ([vp, vp, vp, dp, vp], ip),
         "rds_step_sync": ([vp], ip),
+        "rds_set_blending_coeff": ([vp, vp], ip),
+        "rds_set_artificial_viscosity": ([vp, vp], ip),
+        "rds_set_stab_tables": ([vp, ip, ip, vp, vp, vp, ip, vp], ip),
+        "rds_compute_stabilisation": ([vp, ip, dp, dp, ip, vp, vp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -218,7 +224,46 @@ class PGRDMethodExplicit:
 
     def initialize_work_data(self):
         self._check(lib().rds_finalize(self._ctx))
+        # tables of the stabilisation operators: the vertex interpolant of every group, the
+        # smoothness sensor's where it is defined (affine simplices)
+        from .reference_element import stab_tables
+        for ig, g in enumerate(self.problem.groups):
+            t = stab_tables(g.shape, g.order, g.ngeo)
+            arrs = [t[k] for k in ("w", "Vn", "R", "P1")]
+            self._keep += arrs
+            self._check(lib().rds_set_stab_tables(self._ctx, ig, t["nq"], *[_ptr(a) for a in arrs[:3]],
+                                                  t["P1"].shape[1], _ptr(arrs[3])))
         return self
+
+    # ---- stabilisation fields (RDMethod::set_blending_coeff / set_artificial_viscosity) -------
+    def set_blending_coeff(self, theta):
+        """External nodal blending coefficient [nnodes] read by PGB cells (None removes it)."""
+        self._check(lib().rds_set_blending_coeff(self._ctx, None if theta is None else
+                                                 _ptr(self._nodal(theta, "theta"))))
+
+    def set_artificial_viscosity(self, eps):
+        """Nodal artificial viscosity [nnodes] added by PGLDA cells (None removes it)."""
+        self._check(lib().rds_set_artificial_viscosity(self._ctx, None if eps is None else
+                                                       _ptr(self._nodal(eps, "eps"))))
+
+    def compute_stabilisation(self, op: int, p0: float = 0.0, p1: float = 1.0,
+                              install: bool = False, cells: bool = True, nodes: bool = False):
+        """Operator `op` (RDS_STAB_*) on the current state: (cell values [total cells] or None,
+        nodal field [nnodes] or None); install=True makes the nodal field the solver's
+        artificial viscosity / blending coefficient."""
+        nc = sum(g.ncells for g in self.problem.groups)
+        cv = np.empty(nc) if cells else None
+        nv = np.empty(self.problem.nnodes) if nodes else None
+        self._check(lib().rds_compute_stabilisation(
+            self._ctx, int(op), float(p0), float(p1), int(bool(install)),
+            None if cv is None else _ptr(cv), None if nv is None else _ptr(nv)))
+        return cv, nv
+
+    def _nodal(self, a, name):
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        if a.size != self.problem.nnodes:
+            raise ValueError(f"{name} must hold {self.problem.nnodes} nodal values")
+        return a
 
     # ---- fields -------------------------------------------------------------------------------
     def set_solution(self, u):

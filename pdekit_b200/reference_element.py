@@ -361,3 +361,62 @@ def tet_tables(p: int, quad_order: int) -> dict:
     fVgeo, fdVgeo = lagrange_triag(1, fqp)
     return dict(qp=qp, w=w, V=V, dV=dV, dVgeo=dVgeo, dVf=dVf, Vsf=Vsf, wv=wv, dVgeo_v=dVgeo_v,
                 fqp=fqp, fw=fw, fV=fV, fVgeo=fVgeo, fdVgeo=fdVgeo)
+
+
+# ---------------------------------------------------------------------------------------------
+# Stabilisation operators
+# ---------------------------------------------------------------------------------------------
+
+_STAB_CACHE = {}
+
+
+def stab_tables(shape: str, p: int, ngeo: int) -> dict:
+    """Tables of the stabilisation operators for cells of `shape` and order p.
+
+    * P1 [ndof, nvert]: the vertex interpolant (P1 on simplices, Q1 on quadrilaterals) at the
+      cell's nodes, for the cell-to-node transfer
+      (src/interpolation/mesh_function/MeshFunctionTools.hpp:328-397);
+    * on affine simplices, the smoothness sensor (src/solver/art_visc/ArtificialViscosity.hpp:
+      174-300, 388-455): w [nq] and points of a rule exact to degree 2p, Vn [nq, ndof] the nodal
+      basis there and R [nq, ndof] the map from nodal values to u - u_{p-1} at the points.
+      The reference projects u on its modal basis and switches off the modes of degree p; its
+      simplex bases (Dubiner) are orthogonal, so u_{p-1} is the L2 projection of u onto the
+      polynomials of degree p - 1, built here with the nodal basis of order p - 1:
+      R = Vn - Vl (Vl^T W Vl)^-1 Vl^T W Vn. At p = 1 the reference switches off every mode
+      (mesh/shape_function/DubinerExpansionTriag.cpp:460-467), u_{p-1} = 0 and R = Vn.
+      On affine cells detJ is constant, so any rule exact to degree 2p gives the reference's
+      integrals. nq = 0 elsewhere (no sensor).
+    """
+    key = (shape, p, ngeo)
+    if key in _STAB_CACHE:
+        return _STAB_CACHE[key]
+    empty = np.zeros(1)
+    if shape == "triag":
+        P1, _ = lagrange_triag(1, meshgen.equidist_triag_nodes(p))
+        rule = (lambda o: triag_gauss(o)) if 2 * p in _DUNAVANT and ngeo == 3 else None
+        basis = lagrange_triag
+        order = 2 * p
+    elif shape == "tetra":
+        P1, _ = lagrange_tet(1, tet_nodes(p))
+        order = min([o for o in _TET_RULES if o >= 2 * p], default=None)
+        rule = tet_gauss if order is not None and ngeo == 4 else None
+        basis = lagrange_tet
+    elif shape == "quad":
+        P1, _ = lagrange_quad(1, quad_nodes(p))
+        rule = None
+    else:
+        raise ValueError(f"no stabilisation tables for {shape}")
+    out = dict(nq=0, w=empty, Vn=empty, R=empty, P1=np.ascontiguousarray(P1))
+    if rule is not None:
+        qp, w = rule(order)
+        Vn, _ = basis(p, qp)
+        if p == 1:
+            R = Vn.copy()
+        else:
+            Vl, _ = basis(p - 1, qp)
+            G = Vl.T @ (w[:, None] * Vl)
+            R = Vn - Vl @ np.linalg.solve(G, Vl.T @ (w[:, None] * Vn))
+        out.update(nq=len(w), w=np.ascontiguousarray(w), Vn=np.ascontiguousarray(Vn),
+                   R=np.ascontiguousarray(R))
+    _STAB_CACHE[key] = out
+    return out

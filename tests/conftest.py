@@ -10,9 +10,21 @@ if ROOT not in sys.path:
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
+def _stab(d):
+    import json
+    return json.load(open(os.path.join(GOLDEN, d, "meta.json"))).get("stab", "none")
+
+
 def golden_cases():
+    """Cases without a stabilisation field (the plain residual path)."""
     return sorted(d for d in os.listdir(GOLDEN)
-                  if os.path.exists(os.path.join(GOLDEN, d, "meta.json")))
+                  if os.path.exists(os.path.join(GOLDEN, d, "meta.json")) and _stab(d) == "none")
+
+
+def stab_cases():
+    """Cases whose solver had a stabilisation field computed by the reference's operators."""
+    return sorted(d for d in os.listdir(GOLDEN)
+                  if os.path.exists(os.path.join(GOLDEN, d, "meta.json")) and _stab(d) != "none")
 
 
 def pytest_configure(config):

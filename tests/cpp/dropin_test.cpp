@@ -11,19 +11,27 @@
 // (iterate), and the residual norms.
 //
 // usage: dropin_test <advconst|burgers|euler2d|euler3d> <lda|n|b> <p> <quad> <mesh.msh> <iters>
-//                    <cfl> <init> <bcspec>
+//                    <cfl> <init> <bcspec> [stab]
+//   stab: "av:<kappa>:<factor>" / "blend:<type>:<param>" -- each solver gets a nodal
+//   stabilisation field (set_artificial_viscosity / set_blending_coeff) that the reference's own
+//   operator recomputes in place from that solver's state before the first and every second
+//   iteration, as examples/testcases-rdm/Burgers-RDS-2D.cpp:224-229 does (the device loop is
+//   then not compared: its field stays fixed).
 // Test infrastructure: linked with the reference sources compiled in place (oracle/Makefile).
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <functional>
 #include <memory>
 #include <sstream>
 #include <string>
 #include <vector>
 
 #include "mesh/io/gmsh/GmshReader.hpp"
+#include "solver/art_visc/ArtificialViscosity.hpp"
 #include "solver/rdm/PGRDMethodExplicit.hpp"
+#include "solver/rdm/blending_coeff/RDBlendingCoeff.hpp"
 
 #include "pdekit_b200/GpuPGRDMethodExplicit.hpp"
 #include "ref_common.hpp"
@@ -37,7 +45,7 @@ using vec_fn = interpolation::VectorMeshFunction<Real>;
 
 struct Args
 {
-  std::string physics, scheme, mesh, init, bcspec;
+  std::string physics, scheme, mesh, init, bcspec, stab = "none";
   Uint p = 1, quad = 1, iters = 1;
   Real cfl = 0.5;
 };
@@ -157,6 +165,48 @@ int run(const Args &a)
   add_bcs(ref, a.bcspec);
   add_bcs(gpu, a.bcspec);
 
+  // stabilisation field per solver, recomputed in place by the reference's operator
+  using scal_fn = interpolation::ScalarMeshFunction<Real>;
+  auto f_ref    = std::make_shared<scal_fn>("", "stab");
+  auto f_gpu    = std::make_shared<scal_fn>("", "stab");
+  f_ref->resize(nsol);
+  f_gpu->resize(nsol);
+  std::function<void(const vec_fn &, scal_fn &)> compute;
+  std::shared_ptr<solver::ArtificialViscosity<MC>> av_op;
+  std::shared_ptr<solver::rdm::RDBlendingCoeff<MC>> bl_op;
+  if (a.stab != "none")
+  {
+    std::vector<std::string> tok;
+    std::stringstream ts(a.stab);
+    std::string t;
+    while (std::getline(ts, t, ':'))
+      tok.push_back(t);
+    if (tok.size() != 3)
+      return 2;
+    const Real p0 = std::atof(tok[1].c_str()), p1 = std::atof(tok[2].c_str());
+    if (tok[0] == "av")
+    {
+      av_op = std::make_shared<solver::ArtificialViscosity<MC>>();
+      av_op->prepare_indicator_operators(*sol);
+      compute = [&, p0, p1](const vec_fn &u, scal_fn &f) {
+        av_op->compute_artificial_viscosity_nodal(*mesh, *sol, u, f, p0, p1);
+      };
+      ref.set_artificial_viscosity(f_ref);
+      gpu.set_artificial_viscosity(f_gpu);
+    }
+    else
+    {
+      bl_op = std::make_shared<solver::rdm::RDBlendingCoeff<MC>>();
+      bl_op->setup(*sol, tok[1]);
+      bl_op->set_param(tok[1] == "WongJansen" ? "u_inf" : "kappa", std::atof(tok[2].c_str()));
+      compute = [&](const vec_fn &u, scal_fn &f) { bl_op->calculate(*mesh, *sol, u, f); };
+      ref.set_blending_coeff(f_ref);
+      gpu.set_blending_coeff(f_gpu);
+    }
+    compute(*u_ref, *f_ref);
+    compute(*u_gpu, *f_gpu);
+  }
+
   // first assembly
   ref.assemble_lhs_and_rhs(a.cfl);
   gpu.assemble_lhs_and_rhs(a.cfl);
@@ -177,6 +227,11 @@ int run(const Args &a)
   gpu.solve({});
   for (Uint it = 1; it < a.iters; ++it)
   {
+    if (compute && it % 2 == 0)
+    {
+      compute(*u_ref, *f_ref);
+      compute(*u_gpu, *f_gpu);
+    }
     ref.assemble_lhs_and_rhs(a.cfl);
     ref.solve({});
     gpu.assemble_lhs_and_rhs(a.cfl);
@@ -184,10 +239,14 @@ int run(const Args &a)
   }
   const std::vector<double> uK_r = grab(*u_ref), uK_g = grab(*u_gpu);
 
-  // the drop-in's device loop from the same initial state
-  load(*u_gpu);
-  gpu.iterate(a.cfl, a.iters, 0.0);
-  const std::vector<double> uL_g = grab(*u_gpu);
+  // the drop-in's device loop from the same initial state (without a recomputed field)
+  std::vector<double> uL_g = uK_r;
+  if (!compute)
+  {
+    load(*u_gpu);
+    gpu.iterate(a.cfl, a.iters, 0.0);
+    uL_g = grab(*u_gpu);
+  }
 
   const double su = std::max(max_abs(uK_r), 1e-300);
   std::printf("{\"nodes\": %u, \"cells\": %u, \"iters\": %u, \"res1\": %.3e, \"dt1\": %.3e, "
@@ -216,6 +275,8 @@ int main(int argc, char **argv)
   a.cfl     = std::atof(argv[7]);
   a.init    = argv[8];
   a.bcspec  = argv[9];
+  if (argc > 10)
+    a.stab = argv[10];
 
   using Adv   = physics::RotationAdvection2D<ConstDirection2D>;
   using Burg  = physics::Burgers2D;

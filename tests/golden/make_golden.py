@@ -96,11 +96,35 @@ CASES = {
                                 EULER2D_FAR_BCS, 0.5, 3),
     "euler3d_tet_p2_farfield": ("euler3d", "lda", 2, 5, ("box_tet", 3, 2, 2), 0.1, 42, "bump3d",
                                 EULER3D_FAR_BCS, 0.5, 3),
+    # stabilisation fields computed at u0 by the reference's own operators (a steep front, so
+    # that the sensor is zero in some cells and on its ramp in others): nodal artificial
+    # viscosity into PGLDA, nodal blending coefficients into PGB; optional 12th entry
+    "burgers_p2_lda_av": ("burgers", "lda", 2, 5, 8, 0.15, 51, "steep", BURG_BCS, 0.5, 3,
+                          "av:2.0:1.0"),
+    "adv_p1_lda_av": ("advconst", "lda", 1, 4, 8, 0.2, 52, "steep", ADV_BCS, 0.9, 3,
+                      "av:3.0:0.5"),
+    "burgers_p3_lda_av": ("burgers", "lda", 3, 8, 5, 0.15, 53, "steep", BURG_BCS, 0.5, 3,
+                          "av:2.0:1.0"),
+    "burgers_p2_b_lf": ("burgers", "b", 2, 5, 8, 0.15, 54, "steep", BURG_BCS, 0.5, 3,
+                        "blend:LF_Blend:0"),
+    "burgers_p2_b_wj": ("burgers", "b", 2, 5, 8, 0.15, 55, "steep", BURG_BCS, 0.5, 3,
+                        "blend:WongJansen:1.0"),
+    "adv_p2_b_visc": ("advconst", "b", 2, 5, 8, 0.2, 56, "steep", ADV_BCS, 0.9, 3,
+                      "blend:ViscosityIndicator:2.0"),
+    "euler2d_tri_p2_lda_av": ("euler2d", "lda", 2, 5, ("channel_tri", 6, 3), 0.15, 57,
+                              "bump2d_jump", EULER2D_BCS, 0.5, 3, "av:4.0:1.0"),
+    "euler2d_tri_p3_b_lf": ("euler2d", "b", 3, 8, ("channel_tri", 5, 3), 0.15, 58, "bump2d_jump",
+                            EULER2D_BCS, 0.5, 3, "blend:LF_Blend:0"),
+    # the reference's cell-to-node transfer crashes on tetrahedral meshes: the cellwise values
+    # come from the reference, the nodal field handed to its solver from the oracle's transfer
+    "euler3d_tet_p2_lda_av": ("euler3d", "lda", 2, 5, ("box_tet", 4, 2, 2), 0.1, 59,
+                              "bump3d_jump", EULER3D_BCS, 0.5, 3, "av3d:4.0:1.0"),
 }
 
 
 def make(name, spec):
-    physics, scheme, p, quad, n, jit, seed, init, bcs, cfl, iters = spec
+    physics, scheme, p, quad, n, jit, seed, init, bcs, cfl, iters = spec[:11]
+    stab = spec[11] if len(spec) > 11 else "none"
     out = os.path.join(HERE, name)
     if os.path.isdir(out):
         shutil.rmtree(out)
@@ -119,8 +143,36 @@ def make(name, spec):
     else:
         meshgen.write_gmsh22(msh, meshgen.unit_square_tri(n, jit, seed=seed))
     cmd = [HARNESS, "dump", physics, scheme, str(p), str(quad), msh, out, str(iters), str(cfl),
-           init, bcs]
-    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+           init, bcs, "1"]
+    if not stab.startswith("av3d:"):
+        subprocess.run(cmd + [stab], check=True, stdout=subprocess.DEVNULL)
+        return
+    # two passes: the reference's cellwise viscosity, then the solver with the nodal field
+    import json
+    import numpy as np
+    from oracle import stab_oracle
+    _, kappa, factor = stab.split(":")
+    tmp = out + "_cells"
+    os.makedirs(tmp, exist_ok=True)
+    subprocess.run(cmd[:7] + [tmp] + cmd[8:] + [f"avcells:{kappa}:{factor}"], check=True,
+                   stdout=subprocess.DEVNULL)
+    meta = json.load(open(os.path.join(tmp, "meta.json")))
+    shp = meta["arrays"]
+    rd = lambda n, t: np.fromfile(os.path.join(tmp, f"{n}.{t}"),
+                                  dtype=np.float64 if t == "f64" else np.int32).reshape(shp[n])
+    sol_conn, sol_nodes = rd("sol_conn", "i32"), rd("sol_nodes", "f64")
+    av = stab_oracle.nodal_from_cells(rd("av_cell", "f64"), sol_conn, meta["nsol"],
+                                      stab_oracle.p1_at(meta["dim"], sol_nodes))
+    field = os.path.join(tmp, "field.f64")
+    av.tofile(field)
+    subprocess.run(cmd + [f"avfield:{field}"], check=True, stdout=subprocess.DEVNULL)
+    meta2 = json.load(open(os.path.join(out, "meta.json")))
+    for n in ("av_cell", "indicator"):
+        shutil.copy(os.path.join(tmp, f"{n}.f64"), os.path.join(out, f"{n}.f64"))
+        meta2["arrays"][n] = shp[n]
+    meta2["stab"] = stab
+    json.dump(meta2, open(os.path.join(out, "meta.json"), "w"), indent=1)
+    shutil.rmtree(tmp)
 
 
 def main(argv):

@@ -52,6 +52,16 @@ CASES = {
     "euler2d_tri_p3_b": ("euler2d", "b", 3, 8, ("channel", 4, 0, 3, 5), "bump2d", E2D, 0.5, 5),
     "euler2d_mixed_p2_n": ("euler2d", "n", 2, 5, ("channel", 3, 6, 3, 6), "bump2d", E2D, 0.5, 5),
     "euler3d_tet_p2_lda": ("euler3d", "lda", 2, 5, ("box", 3, 2, 2, 7), "bump3d", E3D, 0.5, 5),
+    # stabilisation fields handed over with set_artificial_viscosity / set_blending_coeff and
+    # recomputed in place by the reference's operators every second iteration (10th entry)
+    "burgers_p2_lda_av": ("burgers", "lda", 2, 5, ("square", 8, 0.15, 8), "steep", BURG, 0.5, 8,
+                          "av:2.0:1.0"),
+    "burgers_p2_b_lf": ("burgers", "b", 2, 5, ("square", 8, 0.15, 9), "steep", BURG, 0.5, 8,
+                        "blend:LF_Blend:0"),
+    "adv_p2_b_visc": ("advconst", "b", 2, 5, ("square", 8, 0.2, 10), "steep", ADV, 0.9, 8,
+                      "blend:ViscosityIndicator:2.0"),
+    "euler2d_tri_p2_lda_av": ("euler2d", "lda", 2, 5, ("channel", 6, 0, 3, 11), "bump2d_jump", E2D,
+                              0.5, 6, "av:4.0:1.0"),
 }
 
 
@@ -71,11 +81,12 @@ def _mesh(spec, path):
 def test_dropin_matches_reference_solver(name, tmp_path):
     if not os.path.exists(BIN):
         pytest.skip("oracle/_ref/dropin_test not built (needs the reference sources)")
-    physics, scheme, p, quad, mesh, init, bcs, cfl, iters = CASES[name]
+    physics, scheme, p, quad, mesh, init, bcs, cfl, iters = CASES[name][:9]
+    stab = CASES[name][9] if len(CASES[name]) > 9 else "none"
     msh = str(tmp_path / "mesh.msh")
     _mesh(mesh, msh)
     out = subprocess.run([BIN, physics, scheme, str(p), str(quad), msh, str(iters), str(cfl),
-                          init, bcs], capture_output=True, text=True, timeout=600)
+                          init, bcs, stab], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr
     r = json.loads(out.stdout.strip().splitlines()[-1])
     assert r["max_res"] > 0.0

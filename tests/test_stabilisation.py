@@ -1,0 +1,125 @@
+"""Stabilisation operators on the CPU: the oracle restatement against the reference's own
+outputs (tests/golden/*: the sensor, the normalised indicator, the blending coefficients and
+their nodal fields, dumped through ArtificialViscosity / RDBlendingCoeff), and the host tables
+the GPU sensor uses (reference_element.stab_tables) evaluated in numpy with the kernel's
+formula against the same outputs."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, stab_cases
+from oracle import stab_oracle as so
+from pdekit_b200.problem import load_golden
+from pdekit_b200.reference_element import stab_tables
+
+# FP64 restatement: rounding only; the reference's tetrahedron rule of order 4 is tabulated to
+# about 10 digits (its results differ from exact integration by ~1e-9 relative)
+TOL = {2: 1e-12, 3: 1e-8}
+
+
+def _case(c):
+    prob, a, meta = load_golden(os.path.join(GOLDEN, c))
+    kind, *par = meta["stab"].split(":")
+    return prob, a, meta, kind, par
+
+
+def _rel(got, ref):
+    scale = max(np.abs(ref).max(), 1e-300)
+    return np.abs(got - ref).max() / scale
+
+
+@pytest.mark.parametrize("case", stab_cases())
+def test_oracle_matches_reference(case):
+    prob, a, meta, kind, par = _case(case)
+    dim, p = meta["dim"], meta["p"]
+    u0 = a["u0"][:, 0]
+    P1 = so.p1_at(dim, a["sol_nodes"])
+    tol = TOL[dim]
+    if kind.startswith("av"):
+        kappa, factor = float(par[0]), float(par[1])
+        av = so.sensor_cells(dim, p, a["sol_nodes"], a["geo_coords"], a["geo_conn"],
+                             a["sol_conn"], u0, kappa, factor)
+        assert _rel(av, a["av_cell"]) < tol
+        ind = so.sensor_cells(dim, p, a["sol_nodes"], a["geo_coords"], a["geo_conn"],
+                              a["sol_conn"], u0, kappa, 1.0)
+        if ind.max() >= 1e-14:
+            ind = ind / ind.max()
+        assert _rel(ind, a["indicator"]) < max(tol, 1e-12) * 100
+        if kind == "av":  # the reference's own transfer (2D; it crashes on tetrahedra)
+            nod = so.nodal_from_cells(a["av_cell"], a["sol_conn"], meta["nsol"], P1)
+            assert _rel(nod, a["av_nodal"]) < 1e-14
+    else:
+        typ, prm = par[0], float(par[1])
+        if typ == "ViscosityIndicator":
+            bc = so.sensor_cells(dim, p, a["sol_nodes"], a["geo_coords"], a["geo_conn"],
+                                 a["sol_conn"], u0, prm, blend=True)
+        else:
+            bc = so.blend_cells(typ, a["sol_conn"], u0, prm)
+        assert _rel(bc, a["blend_cell"]) < tol
+        nod = so.nodal_from_cells(a["blend_cell"], a["sol_conn"], meta["nsol"], P1)
+        assert _rel(nod, a["blend_nodal"]) < 1e-14
+
+
+def test_cases_exercise_every_branch():
+    """The fixtures hold cells on both sides of the sensor's switch-off and nonzero nodal
+    fields, for every operator."""
+    seen = set()
+    for c in stab_cases():
+        _, a, meta, kind, par = _case(c)
+        key = "av_cell" if kind.startswith("av") else "blend_cell"
+        v = a[key]
+        assert v.max() > 0.0, c
+        seen.add(kind if kind.startswith("av") else par[0])
+        if kind.startswith("av"):
+            assert (v == 0.0).any() or meta["p"] == 1, c
+    assert {"av", "av3d", "LF_Blend", "WongJansen", "ViscosityIndicator"} <= seen
+
+
+@pytest.mark.parametrize("case", [c for c in stab_cases()
+                                  if c.endswith("_av") or c.endswith("_visc")])
+def test_host_sensor_tables_give_reference_values(case):
+    """stab_tables + the kernel's formula (Se from R and Vn, the ramp) in numpy."""
+    prob, a, meta, kind, par = _case(case)
+    dim, p = meta["dim"], meta["p"]
+    g = prob.groups[0]
+    t = stab_tables(g.shape, g.order, g.ngeo)
+    assert t["nq"] > 0
+    u = a["u0"][:, 0][a["sol_conn"]]  # [nc, ndof]
+    X = a["geo_coords"][a["geo_conn"][:, :dim + 1]]
+    J = np.stack([X[:, k + 1] - X[:, 0] for k in range(dim)], 2) / 2
+    det = np.linalg.det(J)
+    s = u @ t["Vn"].T
+    r = u @ t["R"].T
+    wj = det[:, None] * t["w"][None, :]
+    nom, den, vol = (wj * r * r).sum(1), (wj * s * s).sum(1), wj.sum(1)
+    Se = np.where(den <= 1e-10, 0.0, nom / np.where(den <= 1e-10, 1.0, den))
+    with np.errstate(divide="ignore"):
+        se = np.log(Se) / np.log(10.0)
+    kappa = float(par[0] if kind != "blend" else par[1])
+    blend = kind == "blend"
+    factor = 1.0 if blend else float(par[1])
+    s0 = 1.0 / p ** 4
+    e0 = 1.0 if blend else factor * vol ** (1.0 / dim) / p
+    val = np.where(se < s0 - kappa, 0.0, np.where(se > s0 + kappa, e0,
+                   0.5 * e0 * (1 + np.sin(np.pi * (se - s0) / (2 * kappa)))))
+    ref = a["blend_cell"] if blend else a["av_cell"]
+    assert _rel(val, ref) < TOL[dim]
+
+
+@pytest.mark.parametrize("shape,p", [("triag", 1), ("triag", 2), ("triag", 3), ("tetra", 2)])
+def test_vertex_interpolant_matches_oracle(shape, p):
+    from pdekit_b200 import meshgen
+    from pdekit_b200.reference_element import tet_nodes
+    dim = 2 if shape == "triag" else 3
+    nodes = meshgen.equidist_triag_nodes(p) if dim == 2 else tet_nodes(p)
+    t = stab_tables(shape, p, dim + 1)
+    np.testing.assert_allclose(t["P1"], so.p1_at(dim, nodes), atol=1e-15)
+
+
+def test_fixture_meta_names_its_operator():
+    for c in stab_cases():
+        meta = json.load(open(os.path.join(GOLDEN, c, "meta.json")))
+        assert meta["stab"].split(":")[0] in ("av", "av3d", "blend")
