@@ -7,8 +7,8 @@
 //              res_n += w_q detJ_q eps_q grad phi_n . grad u_e(q)  for every equation e
 //              (src/solver/rdm/cellsplitters/PGLDA.hpp:245-256, the viscosity interpolated as
 //              in assembly/PGRDMExplicitCellWorker.hpp:519-533). Runs after the cell kernel of
-//              the group and adds to its contribution slots; a group of G lanes per cell, a
-//              lane per node, the sums over the nodes (eps_q, grad u) as group shuffles.
+//              the group and adds to its contribution slots; G lanes per cell, on the points
+//              to form the gradient terms, then on the nodes to contract them (shared memory).
 //   sensor     the Persson-Peraire smoothness sensor of the first state component
 //              (src/solver/art_visc/ArtificialViscosity.hpp:300-455,
 //              blending_coeff/ArtViscIndicatorCoeffImpl.hpp:261-425), one thread per affine
@@ -38,15 +38,6 @@ namespace
 {
 
 constexpr double kPi = 3.14159265358979323846;
-
-template <int G>
-__device__ __forceinline__ double group_add(double v)
-{
-#pragma unroll
-  for (int o = G / 2; o > 0; o >>= 1)
-    v += __shfl_xor_sync(0xffffffffu, v, o, G);
-  return v;
-}
 
 template <int D>
 __device__ __forceinline__ double invert(const double J[D][D], double iJ[D][D])
@@ -104,114 +95,176 @@ __device__ __forceinline__ void jacobian_at(const ViscArgs &a, int c, int q, dou
   }
 }
 
+// Shared memory of viscous_cells: the tables (V, dV) once per block, then per cell the nodal
+// values (eps, u) and the point values S'_q[e][a] = sum_i invJ_q[i][a] w_q detJ_q eps_q du_e/dx_i.
+template <int D, int NEQ>
+struct ViscSmem
+{
+  __host__ __device__ static size_t tables(int nq, int ndof) { return (size_t)nq * ndof * (1 + D); }
+  __host__ __device__ static size_t cell(int nq, int ndof)
+  {
+    return (size_t)ndof * (NEQ + 1) + (size_t)nq * NEQ * D;
+  }
+  static size_t bytes(int nq, int ndof, int cpb)
+  {
+    return sizeof(double) * (tables(nq, ndof) + (size_t)cpb * cell(nq, ndof));
+  }
+};
+
+// Two phases per cell, through shared memory: lanes on points form S' (the physical gradient
+// of u, the viscosity at the point and the test function's invJ folded in, so the same form
+// holds on curved cells), then lanes on nodes contract it with the reference gradients:
+//   res_n,e += sum_q sum_a dV[a][q][n] S'_q[e][a]
+//            = sum_q w_q detJ_q eps_q grad phi_n(q) . grad u_e(q).
+// The sum over the points runs in a different order than the reference's (rounding only).
 template <int D, int NEQ, int G>
 __global__ void __launch_bounds__(kBlock) viscous_cells(const ViscArgs a)
 {
   if (a.stop && *a.stop)
     return; // uniform over the grid
-  const int t     = blockIdx.x * blockDim.x + threadIdx.x;
-  const int c     = t / G, n = t % G;
+  extern __shared__ double smem[];
+  const int nq = a.nq, ndof = a.ndof;
+  double *sV   = smem;                            // [nq][ndof]
+  double *sdV  = sV + (size_t)nq * ndof;          // [D][nq][ndof]
+  const int cl = threadIdx.x / G, lane = threadIdx.x % G;
+  double *cell = smem + ViscSmem<D, NEQ>::tables(nq, ndof) + (size_t)cl * ViscSmem<D, NEQ>::cell(nq, ndof);
+  double *seps = cell;                            // [ndof]
+  double *su   = seps + ndof;                     // [ndof][NEQ]
+  double *sS   = su + (size_t)ndof * NEQ;         // [nq][NEQ][D]
+  const int c     = blockIdx.x * (blockDim.x / G) + cl;
   const bool live = c < a.ncells;
-  const bool mine = live && n < a.ndof;
-  double un[NEQ], en = 0.0;
-#pragma unroll
-  for (int e = 0; e < NEQ; ++e)
-    un[e] = 0.0;
-  if (mine)
-  {
-    const int v = __ldg(a.sol_conn + (size_t)n * a.ncells + c);
-    en          = __ldg(a.eps + v);
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e)
-      un[e] = __ldg(a.u + (size_t)e * a.nnodes + v);
-  }
-  double acc[NEQ];
-#pragma unroll
-  for (int e = 0; e < NEQ; ++e)
-    acc[e] = 0.0;
-  double iJ[D][D], det = 0.0;
-  if (a.affine && live)
-  {
-    double J[D][D];
-    jacobian_at<D>(a, c, 0, J);
-    det = invert<D>(J, iJ);
-  }
-  for (int q = 0; q < a.nq; ++q)
-  {
-    if (!a.affine && live)
+
+  for (int i = threadIdx.x; i < nq * ndof; i += blockDim.x)
+    sV[i] = __ldg(a.V + i);
+  for (int i = threadIdx.x; i < D * nq * ndof; i += blockDim.x)
+    sdV[i] = __ldg(a.dV + i);
+  if (live)
+    for (int n = lane; n < ndof; n += G)
     {
-      double J[D][D];
-      jacobian_at<D>(a, c, q, J);
-      det = invert<D>(J, iJ);
+      const int v = __ldg(a.sol_conn + (size_t)n * a.ncells + c);
+      seps[n]     = __ldg(a.eps + v);
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+        su[n * NEQ + e] = __ldg(a.u + (size_t)e * a.nnodes + v);
     }
-    // eps at the point and the node's physical shape-function gradient
-    const double eq = group_add<G>(mine ? __ldg(a.V + (size_t)q * a.ndof + n) * en : 0.0);
-    double gp[D];
-#pragma unroll
-    for (int i = 0; i < D; ++i)
-      gp[i] = 0.0;
-    if (mine)
+  __syncthreads();
+
+  // phase 1: lanes on points
+  if (live)
+    for (int q = lane; q < nq; q += G)
     {
-      double gr[D];
-#pragma unroll
-      for (int k = 0; k < D; ++k)
-        gr[k] = __ldg(a.dV + ((size_t)k * a.nq + q) * a.ndof + n);
-#pragma unroll
-      for (int i = 0; i < D; ++i)
-      {
-        double s = iJ[i][0] * gr[0];
-#pragma unroll
-        for (int k = 1; k < D; ++k)
-          s += iJ[i][k] * gr[k];
-        gp[i] = s;
-      }
-    }
-    // grad u_e at the point (sum over the group's nodes), taken in every lane
-    double gu[NEQ][D];
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e)
-#pragma unroll
-      for (int i = 0; i < D; ++i)
-        gu[e][i] = group_add<G>(gp[i] * un[e]);
-    if (mine && eq != 0.0)
-    {
-      const double wj = __ldg(a.w + q) * det;
+      double J[D][D], iJ[D][D];
+      jacobian_at<D>(a, c, a.affine ? 0 : q, J);
+      const double det = invert<D>(J, iJ);
+      double eq = 0.0, gx[NEQ][D];
 #pragma unroll
       for (int e = 0; e < NEQ; ++e)
 #pragma unroll
-        for (int i = 0; i < D; ++i)
-          acc[e] += (wj * eq * gp[i]) * gu[e][i];
-    }
-  }
-  if (mine)
-  {
-    const long long slot = a.slot_base + (long long)n * a.ncells + c;
+        for (int k = 0; k < D; ++k)
+          gx[e][k] = 0.0;
+      for (int n = 0; n < ndof; ++n)
+      {
+        eq += sV[q * ndof + n] * seps[n];
+        double gr[D];
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e)
-      a.contrib[e * a.S + slot] += acc[e];
-  }
+        for (int k = 0; k < D; ++k)
+          gr[k] = sdV[((size_t)k * nq + q) * ndof + n];
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+        {
+          const double un = su[n * NEQ + e];
+#pragma unroll
+          for (int k = 0; k < D; ++k)
+            gx[e][k] += gr[k] * un;
+        }
+      }
+      const double f = __ldg(a.w + q) * det * eq;
+      double *S      = sS + (size_t)q * NEQ * D;
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+      {
+        double gp[D]; // f du_e/dx_i
+#pragma unroll
+        for (int i = 0; i < D; ++i)
+        {
+          double t = iJ[i][0] * gx[e][0];
+#pragma unroll
+          for (int k = 1; k < D; ++k)
+            t += iJ[i][k] * gx[e][k];
+          gp[i] = f * t;
+        }
+#pragma unroll
+        for (int k = 0; k < D; ++k)
+        {
+          double t = iJ[0][k] * gp[0];
+#pragma unroll
+          for (int i = 1; i < D; ++i)
+            t += iJ[i][k] * gp[i];
+          S[e * D + k] = t;
+        }
+      }
+    }
+  __syncthreads();
+
+  // phase 2: lanes on nodes
+  if (live)
+    for (int n = lane; n < ndof; n += G)
+    {
+      double acc[NEQ];
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+        acc[e] = 0.0;
+      for (int q = 0; q < nq; ++q)
+      {
+        double gr[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k)
+          gr[k] = sdV[((size_t)k * nq + q) * ndof + n];
+        const double *S = sS + (size_t)q * NEQ * D;
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+#pragma unroll
+          for (int k = 0; k < D; ++k)
+            acc[e] += gr[k] * S[e * D + k];
+      }
+      const long long slot = a.slot_base + (long long)n * a.ncells + c;
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+        a.contrib[e * a.S + slot] += acc[e];
+    }
 }
 
 template <int D, int NEQ>
 cudaError_t launch_viscous_g(const ViscArgs &a, cudaStream_t s, const char **name)
 {
-  auto go = [&](auto kern, int G) {
-    const long long threads = (long long)a.ncells * G;
-    const int grid          = (int)((threads + kBlock - 1) / kBlock);
-    kern<<<grid, kBlock, 0, s>>>(a);
-    return cudaGetLastError();
-  };
   if (name)
     *name = "viscous_cells";
-  if (a.ndof <= 4)
-    return go(viscous_cells<D, NEQ, 4>, 4);
-  if (a.ndof <= 8)
-    return go(viscous_cells<D, NEQ, 8>, 8);
-  if (a.ndof <= 16)
-    return go(viscous_cells<D, NEQ, 16>, 16);
-  if (a.ndof <= 32)
-    return go(viscous_cells<D, NEQ, 32>, 32);
-  return cudaErrorInvalidValue;
+  // lanes per cell: the smallest power of two >= the nodes (phase 2) and >= 4
+  int G = 4;
+  while (G < a.ndof)
+    G *= 2;
+  if (G > 32)
+    return cudaErrorInvalidValue;
+  const int cpb       = kBlock / G;
+  const size_t smem   = ViscSmem<D, NEQ>::bytes(a.nq, a.ndof, cpb);
+  if (smem > 48 * 1024)
+    return cudaErrorInvalidValue;
+  const int grid = (a.ncells + cpb - 1) / cpb;
+  switch (G)
+  {
+  case 4:
+    viscous_cells<D, NEQ, 4><<<grid, kBlock, smem, s>>>(a);
+    break;
+  case 8:
+    viscous_cells<D, NEQ, 8><<<grid, kBlock, smem, s>>>(a);
+    break;
+  case 16:
+    viscous_cells<D, NEQ, 16><<<grid, kBlock, smem, s>>>(a);
+    break;
+  default:
+    viscous_cells<D, NEQ, 32><<<grid, kBlock, smem, s>>>(a);
+  }
+  return cudaGetLastError();
 }
 
 __global__ void __launch_bounds__(kBlock) sensor_cells_2d(const SensorArgs a);
