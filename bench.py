@@ -356,8 +356,9 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def time_steps(solver, steps, flush, cfl):
-    """Per-step device time (ms) of `steps` fused iterations, L2 flushed before each step."""
+def time_steps(solver, steps, flush, cfl, step=None):
+    """Per-step device time (ms) of `steps` fused iterations (or calls of `step`), L2 flushed
+    before each step."""
     import torch
 
     stream = torch.cuda.ExternalStream(solver.stream_handle())
@@ -367,7 +368,10 @@ def time_steps(solver, steps, flush, cfl):
         for k in range(steps):
             flush.zero_()
             ev[k][0].record(stream)
-            solver.run(cfl, 1)
+            if step is None:
+                solver.run(cfl, 1)
+            else:
+                step()
             ev[k][1].record(stream)
     stream.synchronize()
     return sum(a.elapsed_time(b) for a, b in ev)
@@ -547,6 +551,17 @@ def run_ours(args, rank, world, local):
     mixed_value = ncells * steps * world / (ms_mixed * 1e-3)
     mixed.close()
 
+    # third-order TVD Runge-Kutta steps (three residual passes each, one graph launch)
+    solver.set_solution(u0)
+    solver.advance_rk3tvd(cfl, max(args.warmup, 3))
+    solver.set_solution(u0)
+    ms_rk3 = max_over_ranks(time_steps(solver, steps, flush, cfl,
+                                       lambda: solver.advance_rk3tvd(cfl, 1)), world)
+    solver.set_solution(u0)
+    rk3 = {"ms_per_step": ms_rk3 / steps,
+           "cell_residual_updates_per_s": 3 * ncells * steps * world / (ms_rk3 * 1e-3),
+           "api": "rds_advance_rk3tvd (RK3TVD::advance_in_time), CUDA events"}
+
     # time to a 1e-10 residual drop, FP64 vs mixed (device loop with the device-side stop test)
     drop = None
     if not args.no_drop and world == 1 and args.workload in ("c1", "c2"):
@@ -577,6 +592,7 @@ def run_ours(args, rank, world, local):
         "e2e": e2e,
         "mixed": {"value": mixed_value, "ms_per_step": ms_mixed / steps,
                   "dtype": "f32 interpolation/flux/upwind, f64 accumulation/inverse/norms"},
+        "rk3tvd": rk3,
         "time_to_drop_1e-10": drop,
         "roofline": roof,
         "kernels_ms_per_launch": {k: round(v[0] / v[1], 5) for k, v in ktimes.items()},

@@ -376,6 +376,20 @@ class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>
     return r;
   }
 
+  /* nsteps of the reference's RK3TVD::advance_in_time(*this, CFL) (solver/time/
+   * ExplicitTimeStepper.cpp:66-100) with the stages on the device: one upload before, the
+   * solution, residual and time-step functions refreshed after (the residual and dt of the
+   * last step's first stage, as the reference's stepper leaves them). */
+  void advance_rk3tvd(const Real CFL, const Uint nsteps = 1)
+  {
+    ensure_context();
+    upload_solution();
+    m_ctx->advance_rk3tvd(CFL, int(nsteps));
+    m_cfl_set = true;
+    download_solution();
+    download_fields();
+  }
+
   rds_b200::Context &context()
   {
     ensure_context();

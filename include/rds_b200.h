@@ -327,6 +327,17 @@ RDS_API rds_status rds_set_option(rds_ctx *ctx, const char *key, double value);
  * rds_stream(); the norms of these iterations are not kept. */
 RDS_API rds_status rds_run(rds_ctx *ctx, double cfl, int n);
 
+/* nsteps x RK3TVD::advance_in_time(scheme, cfl) (src/solver/time/ExplicitTimeStepper.cpp:66-100):
+ * per step the residual, wave speed and dt at u_n (assemble_lhs_and_rhs), u_1 = u_n - dt r,
+ * the residual at u_1 (assemble_rhs; cells and conditions read u_1), u_2 = 3/4 u_n + 1/4 u_1 -
+ * 1/4 dt r(u_1), the residual at u_2, u_n+1 = 1/3 u_n + 2/3 u_2 - 2/3 dt r(u_2). Afterwards the
+ * context's residual and dt are those of the last step's first stage, as the reference's solver
+ * holds them, so rds_residual_norm / rds_get_fields give what compute_residual_norm and the
+ * solver's functions give after advance_in_time. One step is captured in a CUDA graph and
+ * replayed; enqueued without waiting. Single-mesh FP64 contexts only (RDS_ERR_UNSUPPORTED
+ * otherwise); the three stage buffers are allocated on the first call. */
+RDS_API rds_status rds_advance_rk3tvd(rds_ctx *ctx, double cfl, int nsteps);
+
 /* Batched independent problems (no counterpart in the reference, which solves one problem per
  * solver object, src/solver/rdm/PGRDMethodExplicit.hpp:417-514). One context holds the disjoint
  * union of P problems of scalar 2D physics: problem p owns nodes [node_offsets[p],

@@ -161,6 +161,11 @@ class Context
   {
     check(m_ctx, rds_update(m_ctx), "rds_update");
   }
+  /* nsteps RK3TVD steps on the device (see rds_advance_rk3tvd). */
+  void advance_rk3tvd(double cfl, int nsteps = 1)
+  {
+    check(m_ctx, rds_advance_rk3tvd(m_ctx, cfl, nsteps), "rds_advance_rk3tvd");
+  }
   std::vector<double> residual_norm()
   {
     std::vector<double> n((size_t)m_neq);

@@ -153,6 +153,25 @@ class Oracle:
             lib().rdso_update(prob.nnodes, prob.neq, _p(dt), _p(res), _p(u))
         return u, norms
 
+    def rk3tvd(self, u, cfl, steps):
+        """`steps` x RK3TVD::advance_in_time (solver/time/ExplicitTimeStepper.cpp:66-100).
+        Every stage assembles at its own state (cells and conditions read it; strong conditions
+        overwrite it) and the later stages reuse the first stage's dt. Returns (u, residual and
+        dt of the last step's first stage, norms [steps, neq] after each step)."""
+        prob = self.prob
+        un = np.array(u, dtype=np.float64).reshape(prob.nnodes, prob.neq)
+        norms = np.zeros((steps, prob.neq))
+        for k in range(steps):
+            res_n, _, dt, _ = self._assemble_inplace(un, cfl)
+            d = dt[:, None]
+            u1 = un - d * res_n
+            r, _, _, _ = self._assemble_inplace(u1, cfl)
+            u2 = 3. / 4. * un + 1. / 4. * u1 - 1. / 4. * (d * r)
+            r, _, _, _ = self._assemble_inplace(u2, cfl)
+            un = 1. / 3. * un + 2. / 3 * u2 - 2. / 3. * (d * r)
+            lib().rdso_residual_norm(prob.nnodes, prob.neq, _p(res_n), _p(dt), _p(norms[k]))
+        return un, res_n, dt, norms
+
     def cell_residual(self, group, cell, u):
         """Scheme residual [ndof, neq] and wave speed [ndof] of one cell from the state u."""
         prob, g = self.prob, self.prob.groups[group]

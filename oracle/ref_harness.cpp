@@ -61,6 +61,7 @@
 #include "solver/rdm/PGRDMethodExplicit.hpp"
 #include "solver/rdm/blending_coeff/RDBlendingCoeff.hpp"
 #include "solver/rdm/cellsplitters/CellSplitters.hpp"
+#include "solver/time/ExplicitTimeStepper.hpp"
 
 #include "ref_common.hpp"
 
@@ -560,6 +561,32 @@ int run(const Args &a)
   }
   out.put("uK", grab(*u), {nsol, NEQ});
   out.put("norms", norms, {Uint(norms.size() / NEQ), NEQ});
+
+  // two steps of the reference's third-order TVD Runge-Kutta stepper from u0
+  // (solver/time/ExplicitTimeStepper.cpp:66-100): the state, the residual of the last step's
+  // first stage, the time step of that stage and the residual norm after each step
+  for (Uint i = 0; i < nsol; ++i)
+  {
+    auto e = u->value(i);
+    for (Uint k = 0; k < NEQ; ++k)
+      e[k] = u0[i * NEQ + k];
+  }
+  {
+    time::RK3TVD rk3;
+    rk3.setup(NEQ, nsol);
+    std::vector<Real> rk_norms;
+    for (Uint step = 0; step < 2; ++step)
+    {
+      rk3.advance_in_time(*solver, a.cfl);
+      solver->compute_residual_norm(nrm);
+      for (Uint k = 0; k < NEQ; ++k)
+        rk_norms.push_back(nrm[k]);
+    }
+    out.put("u_rk3", grab(*u), {nsol, NEQ});
+    out.put("res_rk3", grab(*res), {nsol, NEQ});
+    out.put("dt_rk3", grab_scalar(*solver->scal_function(SolverScalFn::time_step)), {nsol});
+    out.put("norms_rk3", rk_norms, {2, NEQ});
+  }
 
   const char *shape_name = shape == ElemShape::Triag   ? "triag"
                            : shape == ElemShape::Quad  ? "quad"

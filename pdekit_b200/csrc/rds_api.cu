@@ -104,12 +104,17 @@ struct rds_ctx
   int *h_stop = nullptr;
 
   // CUDA graphs: a chunk of fused iterations with FP64 cells (0), FP32 cells (1), batched
-  // problems (2); one iteration without stop test for rds_run, FP64 (3) / FP32 (4) cells.
+  // problems (2); one iteration without stop test for rds_run, FP64 (3) / FP32 (4) cells;
+  // one third-order TVD Runge-Kutta step (5).
   // The loop parameters are read from d_loop, so a graph stays valid across calls.
   static constexpr int kChunk    = 16;
-  static constexpr int kGraphs   = 5;
-  cudaGraphExec_t graph_exec[kGraphs] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  static constexpr int kGraphs   = 6;
+  cudaGraphExec_t graph_exec[kGraphs] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   LoopParams *d_loop            = nullptr;
+  double rk_cfl                 = 0.0; // CFL the Runge-Kutta graph was captured with
+
+  // Runge-Kutta stage states u_1, u_2 and the later stages' residual (SoA [neq][nnodes])
+  double *d_rk_u1 = nullptr, *d_rk_u2 = nullptr, *d_rk_res = nullptr;
 
   // precision of the cell kernels being launched (the mixed loop finishes in FP64)
   int active_precision = RDS_FP64;
@@ -1925,6 +1930,90 @@ rds_status rds_run(rds_ctx *ctx, double cfl, int n)
   return RDS_OK;
 }
 
+// One step of the third-order TVD Runge-Kutta stepper (solver/time/ExplicitTimeStepper.cpp:
+// 66-100): the residual, wave speed and dt at u_n, then two more residual passes at the stage
+// states u_1 and u_2 with the dt of the first. Each gather ends in the stage combination, so a
+// stage costs one pass over the nodes. The later stages run the cell and boundary kernels on
+// the stage state and write their residual to a separate buffer, the way the reference's
+// stepper points the solver's solution and residuals at u_1 / u_2 and res_tmp; the first
+// stage's residual and dt stay in the context for the norm.
+static rds_status enqueue_rk3tvd(rds_ctx *ctx, double cfl)
+{
+  double *const u = ctx->d_u, *const res = ctx->d_res;
+  auto stage = [&](int k) -> rds_status {
+    rds_status st = launch_residual_kernels(ctx, ctx->d_zero);
+    if (st != RDS_OK)
+      return st;
+    GatherArgs ga = gather_args(ctx, k == 1 ? cfl : 0.0, ctx->d_zero);
+    ga.rk_first   = k == 1;
+    ga.rk_un      = u;
+    ga.rk_us      = ctx->d_u;
+    ga.rk_out     = k == 1 ? ctx->d_rk_u1 : k == 2 ? ctx->d_rk_u2 : u;
+    ga.rk_ca      = k == 2 ? 3. / 4. : 1. / 3.;
+    ga.rk_cb      = k == 2 ? 1. / 4. : 2. / 3;
+    ga.rk_cc      = k == 2 ? 1. / 4. : 2. / 3.;
+    return launch(ctx, [&](const char **name) {
+      return launch_gather(ga, k == 1 ? 17 : 16, ctx->gblocks, ctx->stream, name);
+    });
+  };
+  rds_status st = stage(1);
+  if (st == RDS_OK)
+  {
+    ctx->d_u   = ctx->d_rk_u1;
+    ctx->d_res = ctx->d_rk_res;
+    st         = stage(2);
+  }
+  if (st == RDS_OK)
+  {
+    ctx->d_u = ctx->d_rk_u2;
+    st       = stage(3);
+  }
+  ctx->d_u   = u;
+  ctx->d_res = res;
+  return st;
+}
+
+rds_status rds_advance_rk3tvd(rds_ctx *ctx, double cfl, int nsteps)
+{
+  if (!ctx || !ctx->finalized || nsteps <= 0)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_advance_rk3tvd: not finalized or nsteps <= 0")
+               : RDS_ERR_INVALID;
+  if (ctx->nprob > 0 || ctx->d_if_nodes)
+    return fail(ctx, RDS_ERR_UNSUPPORTED,
+                "rds_advance_rk3tvd: single-mesh contexts only (not batched or partitioned)");
+  if (ctx->active_precision != RDS_FP64)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_advance_rk3tvd: FP64 contexts only");
+  rds_status st;
+  const size_t n = (size_t)ctx->desc.nnodes * ctx->desc.neq;
+  for (double **p : {&ctx->d_rk_u1, &ctx->d_rk_u2, &ctx->d_rk_res})
+    if (!*p && (st = dalloc(ctx, p, n)) != RDS_OK)
+      return st;
+  if (ctx->timing)
+  {
+    for (int i = 0; i < nsteps; ++i)
+      if ((st = enqueue_rk3tvd(ctx, cfl)) != RDS_OK)
+        return st;
+    return RDS_OK;
+  }
+  // one step captured once (graph slot 5, recaptured when the CFL changes) and replayed
+  const int gi = 5;
+  if (ctx->graph_exec[gi] && ctx->rk_cfl != cfl)
+  {
+    cudaGraphExecDestroy(ctx->graph_exec[gi]);
+    ctx->graph_exec[gi] = nullptr;
+  }
+  ctx->rk_cfl = cfl;
+  if ((st = capture_graph(ctx, gi, 1, [&] { return enqueue_rk3tvd(ctx, cfl); })) != RDS_OK)
+    return st;
+  const long long per_step = 3 * ((long long)ctx->groups.size() + (long long)ctx->bcs.size() + 1);
+  for (int i = 0; i < nsteps; ++i)
+  {
+    RDS_CUDA(cudaGraphLaunch(ctx->graph_exec[gi], ctx->stream));
+    ctx->launches += per_step;
+  }
+  return RDS_OK;
+}
+
 rds_status rds_set_option(rds_ctx *ctx, const char *key, double value)
 {
   if (!ctx || !key)
@@ -2411,7 +2500,8 @@ rds_status rds_destroy(rds_ctx *ctx)
                   ctx->d_vol,   ctx->d_inv_vol, ctx->d_contrib, ctx->d_wsc,    ctx->d_stage,
                   ctx->d_row,   ctx->d_ent_slot, ctx->d_ent_ws, ctx->d_part,   ctx->d_norm,
                   ctx->d_norm0, ctx->d_hist,  ctx->d_iter,    ctx->d_stop,     ctx->d_zero,
-                  ctx->d_status, ctx->d_counter, ctx->d_loop};
+                  ctx->d_status, ctx->d_counter, ctx->d_loop, ctx->d_rk_u1, ctx->d_rk_u2,
+                  ctx->d_rk_res};
   for (void *p : ctx->extra)
     cudaFree(p);
   for (void *p : bufs)

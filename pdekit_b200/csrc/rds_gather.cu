@@ -70,7 +70,7 @@ __device__ __forceinline__ bool fp32_stalled(double rel, int it, StallRec *r, co
   return double(it - r->best_it) > window;
 }
 
-template <int NEQ, bool DT, bool UPDATE, bool NORM>
+template <int NEQ, bool DT, bool UPDATE, bool NORM, bool RK = false>
 __device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, const double cfl,
                                             double *sq)
 {
@@ -129,6 +129,29 @@ __device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, co
   for (int e = 0; e < NEQ; ++e)
     a.res[(size_t)e * a.nnodes + v] = acc[e];
   a.ws[v] = ws;
+  if (RK)
+  {
+    // Runge-Kutta stage combination of solver/time/ExplicitTimeStepper.cpp:66-100, evaluated
+    // left to right without contraction like the reference's expression templates:
+    //   first stage   u_1 = u_n - dt * r
+    //   later stages  u_k = (ca * u_n + cb * u_s) - cc * (dt * r)
+    // dt is this stage's (first) or the first stage's (later stages; assemble_rhs keeps it)
+    const double d = DT ? __ddiv_rn(__dmul_rn(cfl, vv), ws) : a.dt[v];
+    if (DT)
+      a.dt[v] = d;
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+    {
+      const size_t k   = (size_t)e * a.nnodes + v;
+      const double r   = __dmul_rn(d, acc[e]);
+      const double un  = a.rk_un[k];
+      a.rk_out[k]      = a.rk_first ? __dsub_rn(un, r)
+                                    : __dsub_rn(__dadd_rn(__dmul_rn(a.rk_ca, un),
+                                                          __dmul_rn(a.rk_cb, a.rk_us[k])),
+                                                __dmul_rn(a.rk_cc, r));
+    }
+    return;
+  }
   if (DT)
   {
     const double dtv = __ddiv_rn(__dmul_rn(cfl, vv), ws);
@@ -150,7 +173,7 @@ __device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, co
   }
 }
 
-template <int NEQ, bool DT, bool UPDATE, bool NORM, bool FINAL>
+template <int NEQ, bool DT, bool UPDATE, bool NORM, bool FINAL, bool RK = false>
 __global__ void __launch_bounds__(kGBlock) gather_nodes(const __grid_constant__ GatherArgs a)
 {
   __shared__ double smem[kGBlock / 32];
@@ -162,7 +185,7 @@ __global__ void __launch_bounds__(kGBlock) gather_nodes(const __grid_constant__ 
   for (int e = 0; e < NEQ; ++e)
     sq[e] = 0.0;
   if (v < a.nnodes)
-    gather_node<NEQ, DT, UPDATE, NORM>(a, v, a.loop ? a.loop->cfl : a.cfl, sq);
+    gather_node<NEQ, DT, UPDATE, NORM, RK>(a, v, a.loop ? a.loop->cfl : a.cfl, sq);
   if (NORM)
   {
 #pragma unroll
@@ -588,6 +611,12 @@ cudaError_t launch_gather_neq(const GatherArgs &a, int mode, int nblocks, cudaSt
   case 15:
     gather_nodes<NEQ, true, true, true, true><<<nblocks, kGBlock, 0, s>>>(a);
     break;
+  case 16:
+    gather_nodes<NEQ, false, false, false, false, true><<<nblocks, kGBlock, 0, s>>>(a);
+    break;
+  case 17:
+    gather_nodes<NEQ, true, false, false, false, true><<<nblocks, kGBlock, 0, s>>>(a);
+    break;
   default:
     return cudaErrorInvalidValue;
   }
@@ -599,8 +628,10 @@ cudaError_t launch_gather_neq(const GatherArgs &a, int mode, int nblocks, cudaSt
 cudaError_t launch_gather(const GatherArgs &a, int mode, int nblocks, cudaStream_t s,
                           const char **name)
 {
-  *name = (mode == 15) ? "gather_update_norm_final" : (mode == 7) ? "gather_update_norm"
-                                                                   : "gather_nodes";
+  *name = (mode == 15)  ? "gather_update_norm_final"
+          : (mode == 7) ? "gather_update_norm"
+          : (mode >= 16) ? "gather_rk_stage"
+                        : "gather_nodes";
   switch (a.neq)
   {
   case 1:

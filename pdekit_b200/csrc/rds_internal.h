@@ -202,6 +202,13 @@ struct GatherArgs
   unsigned *status;
   const LoopParams *loop; // non-null: cfl, drop, max_iter are read from here
   StallRec *stall;        // FP32-phase progress record (mixed loop)
+  // Runge-Kutta stage combination (modes 16 / 17): rk_out = ca * rk_un + cb * rk_us
+  // - cc * (dt * res), or rk_out = rk_un - dt * res when rk_first
+  int rk_first;
+  double rk_ca, rk_cb, rk_cc;
+  const double *rk_un; // SoA [neq][nnodes]
+  const double *rk_us;
+  double *rk_out;
 };
 
 // ---- launchers (return cudaError_t of the launch) --------------------------------------
@@ -210,7 +217,8 @@ cudaError_t launch_cells(const HostCellGroup &g, const CellArgs &a, int physics,
                          int precision, int dim, int neq, cudaStream_t s, const char **name);
 cudaError_t launch_bc(const HostBC &b, const BCArgs &a, int physics, int dim, int neq,
                       cudaStream_t s, const char **name);
-// Node gather: mode bit 0 = compute dt, bit 1 = update u, bit 2 = norm partials.
+// Node gather: mode bit 0 = compute dt, bit 1 = update u, bit 2 = norm partials, bit 3 = final
+// reduction; 16 / 17 = residual (17: and dt) followed by a Runge-Kutta stage combination.
 cudaError_t launch_gather(const GatherArgs &a, int mode, int nblocks, cudaStream_t s,
                           const char **name);
 cudaError_t launch_norm_final(const double *part, int nblocks, int neq, int nnodes,

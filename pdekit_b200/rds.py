@@ -46,7 +46,7 @@ EXPORTS = ["rds_create", "rds_add_cell_group", "rds_add_bc", "rds_finalize", "rd
            "rds_set_problems", "rds_add_batch_cell_group", "rds_add_batch_bc",
            "rds_iterate_batch", "rds_autotune", "rds_residual_norm_noalloc",
            "rds_set_blending_coeff", "rds_set_artificial_viscosity", "rds_set_stab_tables",
-           "rds_compute_stabilisation"]
+           "rds_compute_stabilisation", "rds_advance_rk3tvd"]
 
 
 class RDSError(RuntimeError):
@@ -112,6 +112,7 @@ def lib():
         "rds_last_error": ([vp], C.c_char_p),
         "rds_version": ([], C.c_char_p),
         "rds_run": ([vp, dp, ip], ip),
+        "rds_advance_rk3tvd": ([vp, dp, ip], ip),
         "rds_measure_peak": ([ip, vp], ip),
         "rds_set_option": ([vp, C.c_char_p, dp], ip),
         "rds_set_problems": ([vp, ip, vp, vp], ip),
@@ -370,6 +371,11 @@ class PGRDMethodExplicit:
         """Enqueue n fused iterations without waiting (for event timing on stream_handle())."""
         self._check(lib().rds_run(self._ctx, float(cfl), int(n)))
 
+    def advance_rk3tvd(self, cfl: float, nsteps: int = 1):
+        """nsteps third-order TVD Runge-Kutta steps on the device (enqueued without waiting);
+        afterwards residual and dt are those of the last step's first stage."""
+        self._check(lib().rds_advance_rk3tvd(self._ctx, float(cfl), int(nsteps)))
+
     # ---- diagnostics --------------------------------------------------------------------------
     def stream_handle(self) -> int:
         return lib().rds_stream(self._ctx) or 0
@@ -402,3 +408,27 @@ class PGRDMethodExplicit:
             self.close()
         except Exception:
             pass
+
+
+class ExplicitEuler:
+    """Forward-Euler pseudo-time stepper over a solver (solver/time/ExplicitTimeStepper.cpp:
+    36-40): assemble_lhs_and_rhs(CFL) then solve()."""
+
+    def setup(self, nb_fields: int, nb_entries: int):
+        pass
+
+    def advance_in_time(self, scheme: PGRDMethodExplicit, CFL: float):
+        scheme.assemble_lhs_and_rhs(CFL)
+        scheme.solve()
+
+
+class RK3TVD:
+    """Third-order TVD Runge-Kutta stepper (solver/time/ExplicitTimeStepper.cpp:46-100). The
+    three stages run on the device in one graph launch (rds_advance_rk3tvd); the stage states
+    live in the solver's context, so setup() has nothing to allocate."""
+
+    def setup(self, nb_fields: int, nb_entries: int):
+        pass
+
+    def advance_in_time(self, scheme: PGRDMethodExplicit, CFL: float):
+        scheme.advance_rk3tvd(CFL, 1)

@@ -37,6 +37,19 @@ def test_oracle_iterations(case):
     np.testing.assert_allclose(norms, a["norms"], rtol=1e-11, atol=0)
 
 
+@pytest.mark.parametrize("case", golden_cases())
+def test_oracle_rk3tvd(case):
+    """Two steps of the third-order TVD Runge-Kutta stepper against the reference's own
+    RK3TVD class run on the same solver (state, first-stage residual and dt, norms)."""
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    o = Oracle(prob)
+    u, res, dt, norms = o.rk3tvd(a["u0"], meta["cfl"], 2)
+    assert rel_err(u, a["u_rk3"]) < TOL
+    assert rel_err(res, a["res_rk3"]) < TOL
+    assert rel_err(dt, a["dt_rk3"]) < TOL
+    np.testing.assert_allclose(norms, a["norms_rk3"], rtol=1e-11, atol=0)
+
+
 def test_oracle_detects_planted_error():
     """A mistake planted in the oracle's inputs (one wrong table entry) must be caught."""
     prob, a, meta = load_golden(os.path.join(GOLDEN, "burgers_p2_b"))
