@@ -337,6 +337,7 @@ class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>
     m_ctx->assemble(CFL);
     m_cfl_set = true;
     download_fields();
+    download_strong_state();
   }
   void assemble_rhs() override
   {
@@ -346,6 +347,7 @@ class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>
     upload_solution();
     m_ctx->assemble_rhs();
     download_fields();
+    download_strong_state();
   }
   /* u -= dt * res (PGRDMethodExplicit.hpp:468-477). */
   void solve(std::vector<SolverOption> const & = {}) override
@@ -729,6 +731,18 @@ class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>
     const vec_fn::ptr u = this->vec_function(SolverVecFn::solution);
     if (u && u->nb_entries() == Uint(m_ctx->nnodes()))
       m_ctx->get_state(&u->value(0)[0]);
+  }
+  /* StrongDirichlet conditions overwrite their dofs in the solution function during the
+   * assembly (StrongDirichletBC::apply, bc/StrongDirichletBC.hpp:202-233); a caller that combines
+   * states on the host (a Runge-Kutta stepper) reads them there. */
+  void download_strong_state()
+  {
+    for (const auto &kv : m_bcs)
+      if (kv.second->type() == "StrongDirichlet")
+      {
+        download_solution();
+        return;
+      }
   }
   void download_fields()
   {

@@ -8,7 +8,8 @@
 // compute_residual_norm), runs K iterations of each and prints one JSON line with the largest
 // differences: residual and time step after the first assembly (normalised by the reference's
 // largest magnitude), the state after K iterations, the state after the drop-in's device loop
-// (iterate), and the residual norms.
+// (iterate), the residual norms, and the state after two RK3TVD steps (device stages, and the
+// reference's own stepper class driving the drop-in).
 //
 // usage: dropin_test <advconst|burgers|euler2d|euler3d> <lda|n|b> <p> <quad> <mesh.msh> <iters>
 //                    <cfl> <init> <bcspec> [stab]
@@ -32,6 +33,7 @@
 #include "solver/art_visc/ArtificialViscosity.hpp"
 #include "solver/rdm/PGRDMethodExplicit.hpp"
 #include "solver/rdm/blending_coeff/RDBlendingCoeff.hpp"
+#include "solver/time/ExplicitTimeStepper.hpp"
 
 #include "pdekit_b200/GpuPGRDMethodExplicit.hpp"
 #include "ref_common.hpp"
@@ -248,13 +250,41 @@ int run(const Args &a)
     uL_g = grab(*u_gpu);
   }
 
+  // two RK3TVD steps from the initial state (solver/time/ExplicitTimeStepper.cpp:66-100): the
+  // reference's stepper on the reference solver, the drop-in's device stages, and the
+  // reference's stepper driving the drop-in through the solver interface
+  double rk3 = 0.0, rk3_class = 0.0;
+  if (!compute)
+  {
+    load(*u_ref);
+    time::RK3TVD rk_ref;
+    rk_ref.setup(NEQ, nsol);
+    rk_ref.advance_in_time(ref, a.cfl);
+    rk_ref.advance_in_time(ref, a.cfl);
+    const std::vector<double> uR = grab(*u_ref);
+    load(*u_gpu);
+    gpu.advance_rk3tvd(a.cfl, 2);
+    const std::vector<double> uG = grab(*u_gpu);
+    load(*u_gpu);
+    time::RK3TVD rk_gpu;
+    rk_gpu.setup(NEQ, nsol);
+    rk_gpu.advance_in_time(gpu, a.cfl);
+    rk_gpu.advance_in_time(gpu, a.cfl);
+    const std::vector<double> uC = grab(*u_gpu);
+    const double sr = std::max(max_abs(uR), 1e-300);
+    rk3             = max_diff(uR, uG) / sr;
+    rk3_class       = max_diff(uR, uC) / sr;
+  }
+
   const double su = std::max(max_abs(uK_r), 1e-300);
   std::printf("{\"nodes\": %u, \"cells\": %u, \"iters\": %u, \"res1\": %.3e, \"dt1\": %.3e, "
-              "\"norm1\": %.3e, \"uK\": %.3e, \"uK_loop\": %.3e, \"max_res\": %.6e}\n",
+              "\"norm1\": %.3e, \"uK\": %.3e, \"uK_loop\": %.3e, \"rk3\": %.3e, "
+              "\"rk3_class\": %.3e, \"max_res\": %.6e}\n",
               nsol, (*sol).nb_active_cells(), a.iters,
               max_diff(res_r, res_g) / std::max(max_abs(res_r), 1e-300),
               max_diff(dt_r, dt_g) / std::max(max_abs(dt_r), 1e-300), norm_diff,
-              max_diff(uK_r, uK_g) / su, max_diff(uK_r, uL_g) / su, max_abs(res_r));
+              max_diff(uK_r, uK_g) / su, max_diff(uK_r, uL_g) / su, rk3, rk3_class,
+              max_abs(res_r));
   return 0;
 }
 

@@ -92,3 +92,4 @@ def test_dropin_matches_reference_solver(name, tmp_path):
     assert r["max_res"] > 0.0
     assert r["res1"] <= 1e-12 and r["dt1"] <= 1e-12 and r["norm1"] <= 1e-12, r
     assert r["uK"] <= 1e-11 and r["uK_loop"] <= 1e-11, r
+    assert r["rk3"] <= 1e-11 and r["rk3_class"] <= 1e-11, r
