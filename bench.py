@@ -572,12 +572,19 @@ def run_ours(args, rank, world, local):
         threads = os.cpu_count() or 1
         with tempfile.TemporaryDirectory() as td:
             r = cpu_reference(prob, cpu_spec, threads, td)
+            # the deterministic one-thread run (the parity reference) beside it; the
+            # multi-thread scatter is unsynchronised, so its final norm is compared
+            r1 = cpu_reference(prob, cpu_spec, 1, td) if (r and threads > 1) else r
         if r:
             cpu = {"value": r["cell_updates_per_s"], "unit": "cell-residual updates/s",
                    "cores": threads, "kind": "reference",
                    "sample": f"reference PGRDMethodExplicit ({prob.physics}, {prob.scheme}) on "
                              f"{cpu_spec['sample']}, {r['iters']} iterations after one warm-up "
-                             f"assemble, nb_threads={threads} ({r['cells']} cells)"}
+                             f"assemble, nb_threads={threads} ({r['cells']} cells)",
+                   "single_thread": {
+                       "value": r1["cell_updates_per_s"], "cores": 1,
+                       "final_norm_rel_diff_vs_threads":
+                           abs(r["norm0"] - r1["norm0"]) / max(abs(r1["norm0"]), 1e-300)}}
 
     stab = measure_stab(args, solver, prob, u0, cfl, steps, flush, world) if args.stab else None
 
