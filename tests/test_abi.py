@@ -45,3 +45,10 @@ def test_invalid_descriptor_rejected_before_any_device_call():
         assert b"invalid descriptor" in L.rds_last_error(ctx)
         L.rds_destroy(ctx)
     assert L.rds_create(None, None, None) == 1
+
+
+def test_steppers_reject_missing_context():
+    """The stepping entry points check their context before touching the device."""
+    L = rds.lib()
+    assert L.rds_advance_rk3tvd(None, 0.5, 1) == 1  # RDS_ERR_INVALID
+    assert L.rds_run(None, 0.5, 1) == 1
