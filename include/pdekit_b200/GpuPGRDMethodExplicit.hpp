@@ -66,6 +66,14 @@ namespace solver
 namespace rdm
 {
 
+/* Solvers that run RK3TVD steps on the device (GpuRK3TVD dispatches to them). */
+class DeviceRK3TVDSolver
+{
+  public:
+  virtual ~DeviceRK3TVDSolver() = default;
+  virtual void advance_rk3tvd(const Real CFL, const Uint nsteps) = 0;
+};
+
 namespace gpu_detail
 {
 
@@ -255,7 +263,7 @@ class GpuRDMBC : public RDMBCBase<MeshConfig, Physics, Physics::DIM - 1>
 };
 
 template <typename MeshConfig, typename Physics, typename SchemeTag>
-class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>
+class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>, public DeviceRK3TVDSolver
 {
   using base           = RDMethod<MeshConfig, Physics>;
   using mesh_type      = typename base::mesh_type;
@@ -382,7 +390,7 @@ class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>
    * ExplicitTimeStepper.cpp:66-100) with the stages on the device: one upload before, the
    * solution, residual and time-step functions refreshed after (the residual and dt of the
    * last step's first stage, as the reference's stepper leaves them). */
-  void advance_rk3tvd(const Real CFL, const Uint nsteps = 1)
+  void advance_rk3tvd(const Real CFL, const Uint nsteps = 1) override
   {
     ensure_context();
     upload_solution();

@@ -9,7 +9,7 @@
 // differences: residual and time step after the first assembly (normalised by the reference's
 // largest magnitude), the state after K iterations, the state after the drop-in's device loop
 // (iterate), the residual norms, and the state after two RK3TVD steps (device stages, and the
-// reference's own stepper class driving the drop-in).
+// reference's own stepper class driving the drop-in, and the drop-in stepper GpuRK3TVD).
 //
 // usage: dropin_test <advconst|burgers|euler2d|euler3d> <lda|n|b> <p> <quad> <mesh.msh> <iters>
 //                    <cfl> <init> <bcspec> [stab]
@@ -34,6 +34,8 @@
 #include "solver/rdm/PGRDMethodExplicit.hpp"
 #include "solver/rdm/blending_coeff/RDBlendingCoeff.hpp"
 #include "solver/time/ExplicitTimeStepper.hpp"
+
+#include "pdekit_b200/GpuRK3TVD.hpp"
 
 #include "pdekit_b200/GpuPGRDMethodExplicit.hpp"
 #include "ref_common.hpp"
@@ -271,8 +273,15 @@ int run(const Args &a)
     rk_gpu.advance_in_time(gpu, a.cfl);
     rk_gpu.advance_in_time(gpu, a.cfl);
     const std::vector<double> uC = grab(*u_gpu);
+    // the drop-in stepper class, through the stepper base class
+    load(*u_gpu);
+    std::unique_ptr<time::ExplicitTimeStepperBase> stepper(new time::GpuRK3TVD());
+    stepper->setup(NEQ, nsol);
+    stepper->advance_in_time(gpu, a.cfl);
+    stepper->advance_in_time(gpu, a.cfl);
+    const std::vector<double> uS = grab(*u_gpu);
     const double sr = std::max(max_abs(uR), 1e-300);
-    rk3             = max_diff(uR, uG) / sr;
+    rk3             = std::max(max_diff(uR, uG), max_diff(uR, uS)) / sr;
     rk3_class       = max_diff(uR, uC) / sr;
   }
 
