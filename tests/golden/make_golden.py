@@ -4,8 +4,9 @@ Each case writes a seeded synthetic P1 triangle mesh (Gmsh 2.2, pdekit_b200.mesh
 reference's own PGRDMethodExplicit through oracle/_ref/rds_ref_harness (the reference sources
 compiled in place by oracle/Makefile) and keeps what the harness dumps: the reference's
 connectivity, reference-element tables, boundary facets, initial state, and its outputs after
-one assemble_lhs_and_rhs (residual, wave speed, dt, dual volume), after one solve, and after
-`iters` iterations (state and residual norms).
+one assemble_lhs_and_rhs (residual, wave speed, dt, dual volume), after one solve, after
+`iters` iterations (state and residual norms), and after two steps of its RK3TVD stepper (state,
+first-stage residual and dt, norms).
 
 Needs the reference tree (it runs only where the reference is mounted):
     make -C oracle && python tests/golden/make_golden.py
