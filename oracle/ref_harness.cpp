@@ -10,7 +10,8 @@
 // Two jobs:
 //   dump  -- write golden inputs (mesh arrays, reference-element tables, boundary facets,
 //            initial state) and outputs (nodal residual, wave speed, dt, dual volume, states
-//            after k iterations, residual norms) as raw little-endian arrays + meta.json.
+//            after k iterations, residual norms, two steps of the reference's RK3TVD stepper)
+//            as raw little-endian arrays + meta.json.
 //   time  -- time K explicit iterations (the CPU baseline), print one JSON line.
 //
 // Usage:
