@@ -388,8 +388,10 @@ RDS_API long long rds_launch_count(rds_ctx *ctx);
  * Scratch is a fixed device array inside this library, sized for RDS_NOALLOC_MAX_NODES nodes
  * and 5 equations (1.25 MiB per GPU, held until the process exits); larger inputs get
  * RDS_ERR_TOO_LARGE. Its address is looked up in the first call on each device, so make that
- * first call before any stream capture. All calls share the array: calls that overlap on the
- * GPU race and must be serialised by the caller. */
+ * first call before any stream capture. The address stays cached for the life of the process:
+ * cudaDeviceReset invalidates it (as it invalidates every context of this library), so a process
+ * that resets a device does not call this entry point on that device again. All calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the caller. */
 #define RDS_NOALLOC_MAX_NODES (32768 * 256)
 RDS_API rds_status rds_residual_norm_noalloc(const double *res, const double *dt, int nnodes,
                                              int neq, double *norm, void *stream);

@@ -215,81 +215,53 @@ int run(const Args &a)
       bc->set_expression(find_expr(b.expr));
   }
 
-  // ---- element types (this harness drives single-type meshes)
-  const MeshEntity cell0     = (*sol).active_cell(ActiveIdx(0));
-  const MeshEntity geo_cell0 = (*geo).active_cell(ActiveIdx(0));
-  const ElemShape shape      = cell0.pt_set_id().elem_shape();
-  const Uint ndof            = cell0.nb_vert();
-  const Uint ngeo            = geo_cell0.nb_vert();
-  const Uint geo_order       = geo_cell0.pt_set_id().poly_order();
+  // ---- element types: (solution point set, geometry point set) pairs in order of first
+  // appearance among the active cells; every type keeps its cells in ascending active-cell
+  // order (mixed meshes, e.g. triangles + quadrilaterals, dump one table set per type)
+  struct CellType
+  {
+    PointSetTag sol_tag, geo_tag;
+    std::vector<Uint> cells;
+  };
+  std::vector<CellType> types;
+  for (Uint c = 0; c < ncells; ++c)
+  {
+    const PointSetTag st = (*sol).active_cell(ActiveIdx(c)).pt_set_id();
+    const PointSetTag gt = (*geo).active_cell(ActiveIdx(c)).pt_set_id();
+    Uint k               = 0;
+    while (k < types.size() && (types[k].sol_tag != st || types[k].geo_tag != gt))
+      ++k;
+    if (k == types.size())
+      types.push_back({st, gt, {}});
+    types[k].cells.push_back(c);
+  }
+  const ElemShape shape  = types[0].sol_tag.elem_shape();
+  const Uint geo_order   = types[0].geo_tag.poly_order();
+  const ElemShape fshape = facet_shape_of(shape);
+  for (const CellType &t : types)
+    if (facet_shape_of(t.sol_tag.elem_shape()) != fshape || t.geo_tag.poly_order() != geo_order)
+    {
+      std::cerr << "dump mode needs one facet shape and one geometry order" << std::endl;
+      return 2;
+    }
 
   // ---- geometry nodes (coordinates indexed by geometry dof id)
   const Uint ngeo_nodes = (*geo).nb_nodes();
   std::vector<Real> geo_coords(ngeo_nodes * D, 0.0);
-  std::vector<int> geo_conn(ncells * ngeo), sol_conn(ncells * ndof);
-  bool single_type = true;
   for (Uint c = 0; c < ncells; ++c)
-    if ((*sol).active_cell(ActiveIdx(c)).pt_set_id() != cell0.pt_set_id())
-      single_type = false;
-  if (!single_type && a.mode == "dump")
-  {
-    std::cerr << "dump mode needs a mesh of one element type" << std::endl;
-    return 2;
-  }
-  for (Uint c = 0; c < ncells && single_type; ++c)
   {
     const MeshEntity gc = (*geo).active_cell(ActiveIdx(c));
-    const MeshEntity sc = (*sol).active_cell(ActiveIdx(c));
     const auto coords   = mesh->active_cell(ActiveIdx(c)).coordinates();
-    for (Uint v = 0; v < ngeo; ++v)
+    for (Uint v = 0; v < gc.nb_vert(); ++v)
     {
-      geo_conn[c * ngeo + v] = gc.vertex(v);
-      const auto node        = coords.const_node_view(v);
+      const auto node = coords.const_node_view(v);
       for (Uint d = 0; d < D; ++d)
         geo_coords[gc.vertex(v) * D + d] = node[d];
     }
-    for (Uint n = 0; n < ndof; ++n)
-      sol_conn[c * ndof + n] = sc.vertex(n);
   }
-
-  // ---- reference-element tables, built through the reference's own classes
-  StdPointSet quad;
-  quad.change_type(shape, a.quad, PointSetID::Gauss);
-  const math::DenseDMat<Real> &qp = quad.get().coordinates();
-  const math::DenseDVec<Real> &qw = quad.get().weights();
-  const Uint nq                   = qp.rows();
-
-  interpolation::FEValues fe_sol, fe_geo, fe_flux, fe_sol_at_flux, fe_geo_at_flux;
-  fe_sol.configure(PointSetTag(shape, a.p, PointSetID::Equidist),
-                   sf::SFTag(shape, SFunc::Lagrange, a.p, ModalBasis::Modal));
-  fe_sol.fill_Vandermonde(qp, qw);
-  fe_geo.configure(PointSetTag(shape, geo_order, PointSetID::Equidist),
-                   sf::SFTag(shape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
-  fe_geo.fill_Vandermonde(qp, qw);
-  fe_flux.configure(PointSetTag(shape, a.p + 1, PointSetID::Equidist),
-                    sf::SFTag(shape, SFunc::Lagrange, a.p + 1, ModalBasis::Modal));
-  fe_flux.fill_Vandermonde(qp, qw);
-
-  StdRegion flux_region;
-  flux_region.change_type(PointSetTag(shape, a.p + 1, PointSetID::Equidist));
-  const math::DenseDMat<Real> &flux_nodes = flux_region.get().coordinates();
-  const Uint nfl                          = flux_nodes.rows();
-  math::DenseDVec<Real> dummy_w(nfl);
-  dummy_w.fill(1.0);
-  fe_sol_at_flux.configure(PointSetTag(shape, a.p, PointSetID::Equidist),
-                           sf::SFTag(shape, SFunc::Lagrange, a.p, ModalBasis::Modal));
-  fe_sol_at_flux.fill_Vandermonde(flux_nodes, dummy_w);
-  fe_geo_at_flux.configure(PointSetTag(shape, geo_order, PointSetID::Equidist),
-                           sf::SFTag(shape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
-  fe_geo_at_flux.fill_Vandermonde(flux_nodes, dummy_w);
-
-  StdRegion sol_region;
-  sol_region.change_type(PointSetTag(shape, a.p, PointSetID::Equidist));
-  const math::DenseDMat<Real> &sol_nodes = sol_region.get().coordinates();
 
   // Facet tables (boundary quadrature order = cell quadrature order + 1,
   // solver/rdm/bc/RDMBCBase.hpp:261-263)
-  const ElemShape fshape = facet_shape_of(shape);
   StdPointSet fquad;
   fquad.change_type(fshape, a.quad + 1, PointSetID::Gauss);
   const math::DenseDMat<Real> &fqp = fquad.get().coordinates();
@@ -440,49 +412,122 @@ int run(const Args &a)
   out.dir = a.outdir;
 
   out.put("geo_coords", geo_coords, {ngeo_nodes, D});
-  out.put("geo_conn", geo_conn, {ncells, ngeo});
-  out.put("sol_conn", sol_conn, {ncells, ndof});
   out.put("sol_coords", sol_coords, {nsol, D});
-  out.put("qp", mat_to_vec(qp), {nq, qp.cols()});
-  std::vector<Real> w(nq);
-  for (Uint q = 0; q < nq; ++q)
-    w[q] = qw[q];
-  out.put("w", w, {nq});
-  out.put("V", mat_to_vec(fe_sol.Vandermonde()), {nq, ndof});
-  out.put("Vgeo", mat_to_vec(fe_geo.Vandermonde()), {nq, ngeo});
-  out.put("Vf", mat_to_vec(fe_flux.Vandermonde()), {nq, nfl});
-  out.put("Vsf", mat_to_vec(fe_sol_at_flux.Vandermonde()), {nfl, ndof});
-  out.put("Vgf", mat_to_vec(fe_geo_at_flux.Vandermonde()), {nfl, ngeo});
-  for (Uint d = 0; d < D; ++d)
-  {
-    const std::string s = std::to_string(d);
-    out.put("dV" + s, mat_to_vec(fe_sol.deriv_Vandermonde(d)), {nq, ndof});
-    out.put("dVgeo" + s, mat_to_vec(fe_geo.deriv_Vandermonde(d)), {nq, ngeo});
-    out.put("dVf" + s, mat_to_vec(fe_flux.deriv_Vandermonde(d)), {nq, nfl});
-    out.put("dVgf" + s, mat_to_vec(fe_geo_at_flux.deriv_Vandermonde(d)), {nfl, ngeo});
-    out.put("dVsf" + s, mat_to_vec(fe_sol_at_flux.deriv_Vandermonde(d)), {nfl, ndof});
-  }
-  out.put("flux_nodes", mat_to_vec(flux_nodes), {nfl, flux_nodes.cols()});
-  out.put("sol_nodes", mat_to_vec(sol_nodes), {ndof, sol_nodes.cols()});
 
-  // dual-volume rule: Gauss rule of the cell's own order (RDTimeUpdate.hpp:85-150)
+  // ---- per element type: connectivity (reference dof order) and the reference-element tables,
+  // built through the reference's own classes. A single-type mesh keeps the plain array names;
+  // the types of a mixed mesh get the suffix _t<k> and are listed under "groups" in meta.json.
+  std::ostringstream groupmeta;
+  Uint nq = 0, nfl = 0, ndof = 0, ngeo = 0;
+  for (Uint k = 0; k < types.size(); ++k)
   {
+    const CellType &t       = types[k];
+    const std::string sfx   = types.size() > 1 ? "_t" + std::to_string(k) : "";
+    const ElemShape tshape  = t.sol_tag.elem_shape();
+    const Uint tcells       = t.cells.size();
+    const Uint tndof        = (*sol).active_cell(ActiveIdx(t.cells[0])).nb_vert();
+    const Uint tngeo        = (*geo).active_cell(ActiveIdx(t.cells[0])).nb_vert();
+    std::vector<int> gconn(tcells * tngeo), sconn(tcells * tndof);
+    for (Uint i = 0; i < tcells; ++i)
+    {
+      const MeshEntity gc = (*geo).active_cell(ActiveIdx(t.cells[i]));
+      const MeshEntity sc = (*sol).active_cell(ActiveIdx(t.cells[i]));
+      for (Uint v = 0; v < tngeo; ++v)
+        gconn[i * tngeo + v] = gc.vertex(v);
+      for (Uint n = 0; n < tndof; ++n)
+        sconn[i * tndof + n] = sc.vertex(n);
+    }
+    out.put("geo_conn" + sfx, gconn, {tcells, tngeo});
+    out.put("sol_conn" + sfx, sconn, {tcells, tndof});
+
+    StdPointSet quad;
+    quad.change_type(tshape, a.quad, PointSetID::Gauss);
+    const math::DenseDMat<Real> &qp = quad.get().coordinates();
+    const math::DenseDVec<Real> &qw = quad.get().weights();
+    const Uint tnq                  = qp.rows();
+
+    interpolation::FEValues fe_sol, fe_geo, fe_flux, fe_sol_at_flux, fe_geo_at_flux;
+    fe_sol.configure(PointSetTag(tshape, a.p, PointSetID::Equidist),
+                     sf::SFTag(tshape, SFunc::Lagrange, a.p, ModalBasis::Modal));
+    fe_sol.fill_Vandermonde(qp, qw);
+    fe_geo.configure(PointSetTag(tshape, geo_order, PointSetID::Equidist),
+                     sf::SFTag(tshape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
+    fe_geo.fill_Vandermonde(qp, qw);
+    fe_flux.configure(PointSetTag(tshape, a.p + 1, PointSetID::Equidist),
+                      sf::SFTag(tshape, SFunc::Lagrange, a.p + 1, ModalBasis::Modal));
+    fe_flux.fill_Vandermonde(qp, qw);
+
+    StdRegion flux_region;
+    flux_region.change_type(PointSetTag(tshape, a.p + 1, PointSetID::Equidist));
+    const math::DenseDMat<Real> &flux_nodes = flux_region.get().coordinates();
+    const Uint tnfl                         = flux_nodes.rows();
+    math::DenseDVec<Real> dummy_w(tnfl);
+    dummy_w.fill(1.0);
+    fe_sol_at_flux.configure(PointSetTag(tshape, a.p, PointSetID::Equidist),
+                             sf::SFTag(tshape, SFunc::Lagrange, a.p, ModalBasis::Modal));
+    fe_sol_at_flux.fill_Vandermonde(flux_nodes, dummy_w);
+    fe_geo_at_flux.configure(PointSetTag(tshape, geo_order, PointSetID::Equidist),
+                             sf::SFTag(tshape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
+    fe_geo_at_flux.fill_Vandermonde(flux_nodes, dummy_w);
+
+    StdRegion sol_region;
+    sol_region.change_type(PointSetTag(tshape, a.p, PointSetID::Equidist));
+    const math::DenseDMat<Real> &sol_nodes = sol_region.get().coordinates();
+
+    out.put("qp" + sfx, mat_to_vec(qp), {tnq, qp.cols()});
+    std::vector<Real> w(tnq);
+    for (Uint q = 0; q < tnq; ++q)
+      w[q] = qw[q];
+    out.put("w" + sfx, w, {tnq});
+    out.put("V" + sfx, mat_to_vec(fe_sol.Vandermonde()), {tnq, tndof});
+    out.put("Vgeo" + sfx, mat_to_vec(fe_geo.Vandermonde()), {tnq, tngeo});
+    out.put("Vf" + sfx, mat_to_vec(fe_flux.Vandermonde()), {tnq, tnfl});
+    out.put("Vsf" + sfx, mat_to_vec(fe_sol_at_flux.Vandermonde()), {tnfl, tndof});
+    out.put("Vgf" + sfx, mat_to_vec(fe_geo_at_flux.Vandermonde()), {tnfl, tngeo});
+    for (Uint d = 0; d < D; ++d)
+    {
+      const std::string s = std::to_string(d);
+      out.put("dV" + s + sfx, mat_to_vec(fe_sol.deriv_Vandermonde(d)), {tnq, tndof});
+      out.put("dVgeo" + s + sfx, mat_to_vec(fe_geo.deriv_Vandermonde(d)), {tnq, tngeo});
+      out.put("dVf" + s + sfx, mat_to_vec(fe_flux.deriv_Vandermonde(d)), {tnq, tnfl});
+      out.put("dVgf" + s + sfx, mat_to_vec(fe_geo_at_flux.deriv_Vandermonde(d)), {tnfl, tngeo});
+      out.put("dVsf" + s + sfx, mat_to_vec(fe_sol_at_flux.deriv_Vandermonde(d)), {tnfl, tndof});
+    }
+    out.put("flux_nodes" + sfx, mat_to_vec(flux_nodes), {tnfl, flux_nodes.cols()});
+    out.put("sol_nodes" + sfx, mat_to_vec(sol_nodes), {tndof, sol_nodes.cols()});
+
+    // dual-volume rule: Gauss rule of the cell's own order (RDTimeUpdate.hpp:85-150)
     StdPointSet vquad;
-    vquad.change_type(shape, a.p, PointSetID::Gauss);
+    vquad.change_type(tshape, a.p, PointSetID::Gauss);
     const math::DenseDMat<Real> &vqp = vquad.get().coordinates();
     const math::DenseDVec<Real> &vqw = vquad.get().weights();
     interpolation::FEValues fe_vgeo;
-    fe_vgeo.configure(PointSetTag(shape, geo_order, PointSetID::Equidist),
-                      sf::SFTag(shape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
+    fe_vgeo.configure(PointSetTag(tshape, geo_order, PointSetID::Equidist),
+                      sf::SFTag(tshape, SFunc::Lagrange, geo_order, ModalBasis::Modal));
     fe_vgeo.fill_Vandermonde(vqp, vqw);
     std::vector<Real> vw(vqp.rows());
     for (Uint q = 0; q < vqp.rows(); ++q)
       vw[q] = vqw[q];
-    out.put("vqp", mat_to_vec(vqp), {vqp.rows(), vqp.cols()});
-    out.put("vw", vw, {vqp.rows()});
+    out.put("vqp" + sfx, mat_to_vec(vqp), {vqp.rows(), vqp.cols()});
+    out.put("vw" + sfx, vw, {vqp.rows()});
     for (Uint d = 0; d < D; ++d)
-      out.put("vdVgeo" + std::to_string(d), mat_to_vec(fe_vgeo.deriv_Vandermonde(d)),
-              {vqp.rows(), ngeo});
+      out.put("vdVgeo" + std::to_string(d) + sfx, mat_to_vec(fe_vgeo.deriv_Vandermonde(d)),
+              {vqp.rows(), tngeo});
+
+    const char *tname = tshape == ElemShape::Triag   ? "triag"
+                        : tshape == ElemShape::Quad  ? "quad"
+                        : tshape == ElemShape::Tetra ? "tetra"
+                                                     : "other";
+    groupmeta << (k ? ", " : "") << "{\"shape\": \"" << tname << "\", \"suffix\": \"" << sfx
+              << "\", \"ncells\": " << tcells << ", \"ndof\": " << tndof << ", \"ngeo\": "
+              << tngeo << ", \"nq\": " << tnq << ", \"nfl\": " << tnfl << "}";
+    if (k == 0)
+    {
+      nq   = tnq;
+      nfl  = tnfl;
+      ndof = tndof;
+      ngeo = tngeo;
+    }
   }
 
   const Uint nfq = fqp.rows();
@@ -566,12 +611,15 @@ int run(const Args &a)
   // two steps of the reference's third-order TVD Runge-Kutta stepper from u0
   // (solver/time/ExplicitTimeStepper.cpp:66-100): the state, the residual of the last step's
   // first stage, the time step of that stage and the residual norm after each step
-  for (Uint i = 0; i < nsol; ++i)
+  // (left out when RDS_HARNESS_NO_RK3 is set: six more assemblies on large meshes)
+  const bool with_rk3 = std::getenv("RDS_HARNESS_NO_RK3") == nullptr;
+  for (Uint i = 0; i < nsol && with_rk3; ++i)
   {
     auto e = u->value(i);
     for (Uint k = 0; k < NEQ; ++k)
       e[k] = u0[i * NEQ + k];
   }
+  if (with_rk3)
   {
     time::RK3TVD rk3;
     rk3.setup(NEQ, nsol);
@@ -602,7 +650,8 @@ int run(const Args &a)
        << ", \"ngeo\": " << ngeo << ", \"nq\": " << nq << ", \"nfl\": " << nfl
        << ", \"nfq\": " << nfq << ",\n \"iters\": " << a.iters << ", \"cfl\": " << a.cfl
        << ", \"init\": \"" << a.init << "\", \"stab\": \"" << a.stab
-       << "\",\n \"bcs\": [" << bcmeta.str()
+       << "\",\n \"groups\": [" << groupmeta.str() << "]"
+       << ",\n \"bcs\": [" << bcmeta.str()
        << "],\n \"arrays\": {\n"
        << out.manifest.str() << "\n }\n}\n";
   return 0;

@@ -11,9 +11,11 @@
 // The array's address is taken once per device with cudaGetSymbolAddress (host code cannot use
 // the symbol itself: in host code it names a host-side stand-in, not device memory). That
 // set-up happens in the first call on each device, so the first call on a device must come
-// before any stream capture. All calls share the array: calls that overlap on the GPU (two
-// streams, two host threads) race on it. Every partial that a call reads was written by the
-// same call, so nothing has to start at zero.
+// before any stream capture. The cached address is not looked up again: a cudaDeviceReset
+// (which unloads the module) makes it stale, so a process that resets a device does not call
+// this entry point on that device afterwards. All calls share the array: calls that overlap on
+// the GPU (two streams, two host threads) race on it. Every partial that a call reads was
+// written by the same call, so nothing has to start at zero.
 
 #include <mutex>
 

@@ -16,7 +16,7 @@ from conftest import GOLDEN
 from helpers import rel_err
 from oracle.rds_oracle import Oracle
 from pdekit_b200 import gmsh, meshgen
-from pdekit_b200.problem import load_golden
+from golden_io import load_golden
 from pdekit_b200.workloads import mesh_problem
 
 CASES = ["adv_p1_lda", "adv_p2_b", "adv_p3_lda", "burgers_p2_b", "burgers_p3_b",

@@ -13,7 +13,7 @@ import pytest
 from conftest import GOLDEN
 from helpers import rel_err
 from oracle.rds_oracle import Oracle
-from pdekit_b200.problem import load_golden
+from golden_io import load_golden
 from pdekit_b200.rds import PGRDMethodExplicit, RDSError, lib
 
 pytestmark = pytest.mark.gpu

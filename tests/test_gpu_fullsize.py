@@ -1,0 +1,205 @@
+"""FP64 parity at the benchmark configurations' own sizes, against the reference itself.
+
+A module fixture writes each configuration's mesh (pdekit_b200.meshgen with the bench's seeds)
+as Gmsh 2.2 and runs the reference's own PGRDMethodExplicit on it through
+oracle/_ref/rds_ref_harness (the reference sources compiled in place), all cases concurrently on
+the host cores, one solver thread each (the reference's deterministic mode). The dumps stay in
+a temporary directory; they are 10-160 MB each and are not fixtures of the repository.
+
+  c1   advection P1, LDA, 6-point rule, 64x64 squares (8,192 cells), CFL 0.9: the full mesh
+  c2   Burgers P2, blended B, 7-point rule, 512x512 squares (524,288 cells, 1,050,625 nodes),
+       CFL 0.5: the full mesh
+  c3s  Euler 2D bump channel, P3 triangles (16-point rule) + P3 quadrilaterals (the reference's
+       20-point rule), blended B: the bench's CPU sample, 125x125 + 250x125 squares (62,500
+       cells), two iterations
+  c4s  Euler 3D bump box, P2 tetrahedra (14-point rule), LDA: the bench's CPU sample, 32x8x8
+       hexahedra (12,288 cells)
+
+Checks (max |got - ref| / max |ref| per equation, tests/helpers.py):
+  * the CUDA path on the reference's own connectivity and tables (golden_io.load_golden):
+    dual volume, residual, wave speed, dt, norm, state after one update (1e-12), and the device
+    loop's state and norm history after the harness's iterations;
+  * the bench's own workload builders (pdekit_b200.workloads: own tables and node numbering),
+    nodes matched to the reference's by coordinates, from the reference's initial state: c1 and
+    c2 at 1e-12; c4 at 5e-9, because the reference tabulates the 14-point tetrahedron rule to
+    about ten digits (its weights sum to 4/3 - 3.3e-10) where the bench's tables carry the
+    published rule to full precision;
+  * configuration 3 as benched (5x5 = 25-point quadrilateral rule, which the reference does
+    not have) on the c3 sample mesh against the C restatement (oracle/rds_oracle.c).
+
+The reference forms its dual volumes from each cell's coordinates transferred to the cell's
+solution-order points (solver/rdm/RDTimeUpdate.hpp:118-160), so its rounding error there grows
+with |x| / h; on the c3 sample it is 2e-13 of the largest volume, which the tolerance covers.
+"""
+
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from golden_io import load_golden
+from helpers import rel_err
+from pdekit_b200 import meshgen
+from pdekit_b200.rds import PGRDMethodExplicit
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "rds_ref_harness")
+TOL = 1e-12
+
+ADV = "WeakDirichlet:inlet_bottom:bottom:sin2pix,WeakDirichlet:inlet_left:left:zero"
+BURG = ("WeakDirichlet:inlet:bottom:burgers_inlet,WeakDirichlet:left:left:c1.5,"
+        "WeakDirichlet:right:right:c-0.5")
+E2D = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakWall:top_wall_bc:top_wall:-,"
+       "WeakSubInlet:inlet_bc:inlet:total_temperature=307.6488978;total_pressure=120195.4453,"
+       "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
+E3D = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakWall:top_wall_bc:top_wall:-,"
+       "WeakWall:side_walls_bc:side_walls:-,"
+       "WeakSubInlet:inlet_bc:inlet:total_temperature=307.6488978;total_pressure=120195.4453,"
+       "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
+
+# name: (physics, scheme, p, quad order, mesh, init, conditions, CFL, iterations, with RK3TVD)
+CASES = {
+    "c1": ("advconst", "lda", 1, 4, ("square", 64, 0.2, 1), "zero", ADV, 0.9, 5, True),
+    "c2": ("burgers", "b", 2, 5, ("square", 512, 0.15, 7), "burgers", BURG, 0.5, 3, False),
+    "c3s": ("euler2d", "b", 3, 8, ("channel", 125, 250, 125, 3), "bump2d", E2D, 0.5, 2, False),
+    "c4s": ("euler3d", "lda", 2, 5, ("box", 32, 8, 8, 4), "bump3d", E3D, 0.5, 3, False),
+}
+
+
+def _write_mesh(spec, path):
+    if spec[0] == "square":
+        meshgen.write_gmsh22(path, meshgen.unit_square_tri(spec[1], spec[2], seed=spec[3]))
+    elif spec[0] == "channel":
+        meshgen.write_gmsh22_mesh(path, meshgen.channel_2d(spec[1], spec[2], spec[3],
+                                                           jitter=0.0, seed=spec[4]))
+    else:
+        meshgen.write_gmsh22_mesh(path, meshgen.box_tet(spec[1], spec[2], spec[3], jitter=0.1,
+                                                        seed=spec[4]))
+
+
+@pytest.fixture(scope="module")
+def dumps():
+    """Reference dumps of every case, made concurrently: {name: directory}."""
+    if not os.path.exists(HARNESS):
+        pytest.skip("oracle/_ref/rds_ref_harness not built (make -C oracle needs the reference "
+                    "sources)")
+    tmp = tempfile.TemporaryDirectory(prefix="rds_fullsize_")
+    procs, out = {}, {}
+    for name, (phys, scheme, p, quad, mesh, init, bcs, cfl, iters, rk3) in CASES.items():
+        d = os.path.join(tmp.name, name)
+        os.makedirs(d)
+        msh = os.path.join(d, "mesh.msh")
+        _write_mesh(mesh, msh)
+        env = dict(os.environ)
+        if not rk3:
+            env["RDS_HARNESS_NO_RK3"] = "1"
+        procs[name] = subprocess.Popen(
+            [HARNESS, "dump", phys, scheme, str(p), str(quad), msh, d, str(iters), str(cfl), init,
+             bcs, "1"], stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, env=env)
+        out[name] = d
+    for name, pr in procs.items():
+        _, err = pr.communicate(timeout=900)
+        assert pr.returncode == 0, (name, err.decode()[-2000:])
+    yield out
+    tmp.cleanup()
+
+
+def _solver(prob):
+    s = PGRDMethodExplicit(prob.physics, prob.scheme, "fp64")
+    s.configure_mesh_data(prob)
+    s.initialize_work_data()
+    return s
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_reference_tables_match_reference_at_size(dumps, name):
+    prob, a, meta = load_golden(dumps[name])
+    assert prob.ncells == meta["ncells"]
+    s = _solver(prob)
+    s.set_solution(a["u0"])
+    s.assemble_lhs_and_rhs(meta["cfl"])
+    res, dt, ws, vol = s.fields()
+    errs = {"vol": rel_err(vol, a["dual_volume"]), "res": rel_err(res, a["res1"]),
+            "ws": rel_err(ws, a["ws1"]), "dt": rel_err(dt, a["dt1"])}
+    assert max(errs.values()) < TOL, errs
+    np.testing.assert_allclose(s.compute_residual_norm(), a["norms"][0], rtol=1e-11)
+    s.solve()
+    assert rel_err(s.solution(), a["u1"]) < TOL
+    # the device loop (graph-replayed fused iterations) from u0 for the harness's iterations
+    s.set_solution(a["u0"])
+    it, hist = s.iterate(meta["cfl"], meta["iters"])
+    assert it == meta["iters"]
+    assert rel_err(s.solution(), a["uK"]) < TOL
+    np.testing.assert_allclose(hist, a["norms"], rtol=1e-11)
+    s.close()
+
+
+def _node_map(ours_xy, ref_xy):
+    """Index into ours for every reference node, matched by coordinates."""
+    from scipy.spatial import cKDTree
+
+    dist, idx = cKDTree(ours_xy).query(ref_xy)
+    assert dist.max() < 1e-9, dist.max()
+    assert np.unique(idx).size == idx.size
+    return idx
+
+
+@pytest.mark.parametrize("name,tol", [("c1", TOL), ("c2", TOL), ("c4s", 5e-9)])
+def test_bench_workload_matches_reference_at_size(dumps, name, tol):
+    """The problem the bench times (own tables, own numbering) against the reference run."""
+    from pdekit_b200 import workloads as W
+
+    _, a, meta = load_golden(dumps[name])
+    prob, u0 = {"c1": lambda: W.config1(64), "c2": lambda: W.config2(512),
+                "c4s": lambda: W.config4(32, 8, 8)}[name]()
+    assert prob.ncells == meta["ncells"] and prob.nnodes == meta["nsol"]
+    m = _node_map(prob.sol_coords, a["sol_coords"])
+    # the bump state's +-1% perturbation is a sine hash of the coordinates, which magnifies
+    # last-bit differences of the node coordinates to ~1e-11; both runs start from the
+    # reference's state
+    assert rel_err(u0[m], a["u0"]) < 1e-9
+    u0 = u0.copy()
+    u0[m] = a["u0"]
+    s = _solver(prob)
+    s.set_solution(u0)
+    s.assemble_lhs_and_rhs(meta["cfl"])
+    res, dt, ws, vol = s.fields()
+    errs = {"vol": rel_err(vol[m], a["dual_volume"]), "res": rel_err(res[m], a["res1"]),
+            "ws": rel_err(ws[m], a["ws1"]), "dt": rel_err(dt[m], a["dt1"])}
+    assert max(errs.values()) < tol, errs
+    s.solve()
+    assert rel_err(s.solution()[m], a["u1"]) < tol
+    s.set_solution(u0)
+    s.iterate(meta["cfl"], meta["iters"])
+    assert rel_err(s.solution()[m], a["uK"]) < tol
+    s.close()
+
+
+def test_c3_as_benched_matches_oracle_on_sample():
+    """Configuration 3 with the 25-point quadrilateral rule (own tables) on the c3 sample mesh
+    (62,500 cells, 423,376 nodes): first residual, wave speed, dt, dual volume and the state
+    after one update against the C restatement, which the golden cases pin to the reference."""
+    from oracle.rds_oracle import Oracle
+    from pdekit_b200 import workloads as W
+
+    prob, u0 = W.config3(125, 250, 125)
+    assert [g.nq for g in prob.groups] == [16, 25]
+    s = _solver(prob)
+    s.set_solution(u0)
+    s.assemble_lhs_and_rhs(0.5)
+    res, dt, ws, vol = s.fields()
+    s.solve()
+    u1 = s.solution()
+    s.close()
+    o = Oracle(prob)
+    r_ref, ws_ref, dt_ref, bad = o.assemble(u0, 0.5)
+    assert bad == 0
+    errs = {"vol": rel_err(vol, o.vol), "res": rel_err(res, r_ref), "ws": rel_err(ws, ws_ref),
+            "dt": rel_err(dt, dt_ref)}
+    assert max(errs.values()) < TOL, errs
+    u1_ref = u0 - dt_ref[:, None] * r_ref
+    assert rel_err(u1, u1_ref) < TOL

@@ -9,7 +9,7 @@ import pytest
 from conftest import GOLDEN, golden_cases
 from helpers import rel_err
 from oracle.rds_oracle import Oracle
-from pdekit_b200.problem import load_golden
+from golden_io import load_golden
 from pdekit_b200.rds import PGRDMethodExplicit
 
 pytestmark = pytest.mark.gpu

@@ -10,7 +10,7 @@ import pytest
 from conftest import GOLDEN
 from helpers import rel_err
 from pdekit_b200.partition import emulate
-from pdekit_b200.problem import load_golden
+from golden_io import load_golden
 from pdekit_b200.rds import PGRDMethodExplicit
 
 pytestmark = pytest.mark.gpu

@@ -20,7 +20,7 @@ def _rank(rank, world, port, case, iters, out):
     import torch.distributed as dist
 
     from pdekit_b200.partition import PartitionedRDS
-    from pdekit_b200.problem import load_golden
+    from golden_io import load_golden
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     torch.cuda.set_device(0)
@@ -44,7 +44,7 @@ def test_two_rank_driver_matches_single_context(case, tmp_path):
     import torch.multiprocessing as mp
 
     from helpers import rel_err
-    from pdekit_b200.problem import load_golden
+    from golden_io import load_golden
     from pdekit_b200.rds import PGRDMethodExplicit
 
     with socket.socket() as s:

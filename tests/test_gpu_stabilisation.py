@@ -12,7 +12,7 @@ import pytest
 
 from conftest import GOLDEN, stab_cases
 from helpers import rel_err
-from pdekit_b200.problem import load_golden
+from golden_io import load_golden
 from pdekit_b200.rds import PGRDMethodExplicit, RDSError
 from pdekit_b200.stabilisation import ArtificialViscosity, RDBlendingCoeff
 

@@ -10,7 +10,7 @@ import pytest
 
 from conftest import GOLDEN
 from oracle.rds_oracle import Oracle
-from pdekit_b200.problem import load_golden
+from golden_io import load_golden
 
 
 @pytest.mark.parametrize("case", ["adv_p1_lda", "adv_p1_lda_zero", "adv_p3_lda", "adv_p2_b"])

@@ -7,7 +7,7 @@ import pytest
 
 from conftest import GOLDEN
 from pdekit_b200 import meshgen
-from pdekit_b200.problem import load_golden
+from golden_io import load_golden
 
 
 @pytest.mark.parametrize("p", [1, 2, 3, 4])

@@ -12,7 +12,7 @@ from conftest import GOLDEN
 from helpers import rel_err
 from oracle.rds_oracle import Oracle
 from pdekit_b200.partition import partition
-from pdekit_b200.problem import load_golden
+from golden_io import load_golden
 
 CASES = ["burgers_p2_b", "adv_p2_b", "euler2d_tri_p3_b", "euler2d_quad_p3_b",
          "euler3d_tet_p2_lda", "euler2d_tri_p2_farfield"]

@@ -8,7 +8,7 @@ import pytest
 
 from conftest import GOLDEN
 from pdekit_b200 import reference_element as re_
-from pdekit_b200.problem import load_golden
+from golden_io import load_golden
 
 CASES = {(1, 4): "adv_p1_lda", (2, 5): "burgers_p2_b", (3, 8): "burgers_p3_b"}
 

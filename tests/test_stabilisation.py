@@ -12,7 +12,7 @@ import pytest
 
 from conftest import GOLDEN, stab_cases
 from oracle import stab_oracle as so
-from pdekit_b200.problem import load_golden
+from golden_io import load_golden
 from pdekit_b200.reference_element import stab_tables
 
 # FP64 restatement: rounding only; the reference's tetrahedron rule of order 4 is tabulated to

@@ -14,7 +14,7 @@ import pytest
 
 from conftest import GOLDEN
 from pdekit_b200 import reference_element, workloads
-from pdekit_b200.problem import load_golden
+from golden_io import load_golden
 from pdekit_b200.rds import PGRDMethodExplicit, lib
 
 pytestmark = pytest.mark.gpu
@@ -44,19 +44,24 @@ def _device_norm(res, dt):
     return d_norm.cpu().numpy()
 
 
-def _problems():
-    prob, a, meta = load_golden(os.path.join(GOLDEN, "burgers_p2_b"))
-    yield prob, a["u0"], meta["cfl"]
-    t = reference_element.triag_tables(2, 5)
-    n = 64  # 16,641 nodes: 66 blocks of partial sums
-    big = workloads.tri_problem("burgers", "b", 2, n, 0.15, 7, workloads.BURGERS_BCS, t)
-    u0 = workloads.initial_state(big, "burgers", workloads.sol_coords_tri(n, 0.15, 7, 2))
-    yield big, u0, 0.5
+def _problem(which):
+    """Scalar (one equation) small and 66-block cases, Euler 2D (4) and Euler 3D (5)."""
+    if which == "burgers_64":
+        t = reference_element.triag_tables(2, 5)
+        n = 64  # 16,641 nodes: 66 blocks of partial sums
+        big = workloads.tri_problem("burgers", "b", 2, n, 0.15, 7, workloads.BURGERS_BCS, t)
+        u0 = workloads.initial_state(big, "burgers", workloads.sol_coords_tri(n, 0.15, 7, 2))
+        return big, u0, 0.5
+    prob, a, meta = load_golden(os.path.join(GOLDEN, which))
+    return prob, a["u0"], meta["cfl"]
 
 
-@pytest.mark.parametrize("which", [0, 1])
+@pytest.mark.parametrize("which", ["burgers_p2_b", "burgers_64", "euler2d_quad_p3_b",
+                                   "euler3d_tet_p2_lda"])
 def test_noalloc_norm_matches_existing_entry_two_calls(which):
-    prob, u0, cfl = list(_problems())[which]
+    """Two calls in a row on different residuals; the block split and the summation order are
+    those of rds_residual_norm, so the results are equal bit for bit."""
+    prob, u0, cfl = _problem(which)
     s = PGRDMethodExplicit(prob.physics, prob.scheme).configure_mesh_data(prob)
     s.initialize_work_data()
     s.set_solution(u0)
@@ -65,7 +70,8 @@ def test_noalloc_norm_matches_existing_entry_two_calls(which):
         ref = s.compute_residual_norm()
         res, dt, _, _ = s.fields()
         got = _device_norm(res, dt)
-        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=0)
+        assert got.shape == (prob.neq,)
+        np.testing.assert_array_equal(got, ref)
         s.solve()
     s.close()
 
