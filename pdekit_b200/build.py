@@ -14,7 +14,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["rds_api.cu", "rds_cells_scalar.cu", "rds_cells_scalar_tc.cu", "rds_cells_euler.cu",
            "rds_bc.cu",
-           "rds_gather.cu", "rds_peak.cu", "rds_noalloc.cu", "rds_partition.cu", "rds_jacobian.cu", "rds_stab.cu"]
+           "rds_gather.cu", "rds_peak.cu", "rds_noalloc.cu", "rds_partition.cu", "rds_jacobian.cu", "rds_stab.cu",
+           "rds_cells_scalar_dc.cu"]
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
          "-cudart", "static", f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]

@@ -33,6 +33,11 @@ struct rds_ctx
   cudaStream_t stream    = nullptr;
   cudaStream_t side      = nullptr; // boundary kernels, concurrent with the cell kernels
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // one more side stream per further weak condition (they write disjoint slots, so they run
+  // concurrently with each other as well), with its join event
+  static constexpr int kMaxSides = 8;
+  cudaStream_t sides[kMaxSides] = {};
+  cudaEvent_t ev_joins[kMaxSides] = {};
   bool own_stream        = false;
   bool finalized         = false;
   std::string err;
@@ -105,11 +110,12 @@ struct rds_ctx
 
   // CUDA graphs: a chunk of fused iterations with FP64 cells (0), FP32 cells (1), batched
   // problems (2); one iteration without stop test for rds_run, FP64 (3) / FP32 (4) cells;
-  // one third-order TVD Runge-Kutta step (5).
+  // one third-order TVD Runge-Kutta step (5); cycles of the defect-correction loop (6).
   // The loop parameters are read from d_loop, so a graph stays valid across calls.
   static constexpr int kChunk    = 16;
-  static constexpr int kGraphs   = 6;
-  cudaGraphExec_t graph_exec[kGraphs] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  static constexpr int kGraphs   = 7;
+  cudaGraphExec_t graph_exec[kGraphs] = {nullptr, nullptr, nullptr, nullptr,
+                                         nullptr, nullptr, nullptr};
   LoopParams *d_loop            = nullptr;
   double rk_cfl                 = 0.0; // CFL the Runge-Kutta graph was captured with
 
@@ -127,6 +133,18 @@ struct rds_ctx
   int stall_min       = 200; // FP32 phase stalled: no halving of the drop for
   double stall_mult   = 3.0; //   max(stall_min, stall_mult x the last interval between halvings)
   StallRec *d_stall   = nullptr; // FP32-phase progress record of the single-problem loop
+
+  // mixed form, scalar physics on triangles: defect-correction loop (run_loop_dc). An exact
+  // FP64 sweep every dc_m sweeps keeps its update dt res (d_dres), dt / V (d_dtv) and the state
+  // it started from (d_ur); the sweeps in between add the FP32 changes of every cell and facet
+  // contribution since then (d_c32, one value per slot), the cells' with the blending
+  // coefficients of PGB frozen at d_ur (d_dc_theta, one per cell)
+  bool dc_ok         = false;
+  int dc_m           = 8;
+  int dc_phase       = 0; // launch_residual_kernels: 0 plain, 1 exact DC sweep, 2 correction
+  double *d_ur = nullptr, *d_dres = nullptr, *d_dc_theta = nullptr;
+  float *d_c32 = nullptr, *d_dtv = nullptr;
+  std::vector<long long> dc_cell_base; // first cell of each group in d_dc_theta
   StallRec *d_pstall  = nullptr; // the same per batched problem
 
   // batched independent problems (rds_set_problems): one context holds their disjoint union
@@ -370,6 +388,38 @@ GatherArgs gather_args(rds_ctx *ctx, double cfl, const int *stop)
   return a;
 }
 
+// Side stream of the k-th weak condition (the first one is ctx->side).
+cudaStream_t side_stream(rds_ctx *ctx, int k)
+{
+  const int n = std::min((int)ctx->bcs.size(), rds_ctx::kMaxSides);
+  k           = k % std::max(1, n);
+  return k == 0 ? ctx->side : ctx->sides[k];
+}
+
+// Forks the side streams of the conditions from the main stream (a parallel graph branch each
+// when captured).
+rds_status fork_sides(rds_ctx *ctx)
+{
+  const int n = std::min((int)ctx->bcs.size(), rds_ctx::kMaxSides);
+  RDS_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
+  for (int k = 0; k < n; ++k)
+    RDS_CUDA(cudaStreamWaitEvent(side_stream(ctx, k), ctx->ev_fork, 0));
+  return RDS_OK;
+}
+
+// Joins the side streams into the main stream.
+rds_status join_sides(rds_ctx *ctx)
+{
+  const int n = std::min((int)ctx->bcs.size(), rds_ctx::kMaxSides);
+  for (int k = 0; k < n; ++k)
+  {
+    cudaEvent_t e = k == 0 ? ctx->ev_join : ctx->ev_joins[k];
+    RDS_CUDA(cudaEventRecord(e, side_stream(ctx, k)));
+    RDS_CUDA(cudaStreamWaitEvent(ctx->stream, e, 0));
+  }
+  return RDS_OK;
+}
+
 // Residual contributions of all cells and boundary facets (assemble_rhs without the gather).
 // The boundary-facet kernels only touch their own contribution slots, so they run on a side
 // stream concurrently with the cell kernels (a parallel branch when captured in a graph) and
@@ -383,12 +433,17 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
   for (const HostBC &b : ctx->bcs)
     strong |= b.desc.kind == RDS_BC_STRONG_DIRICHLET;
   const bool fork = !ctx->bcs.empty() && !strong;
-  auto launch_bcs = [&](cudaStream_t s) -> rds_status {
-    for (const HostBC &b : ctx->bcs)
+  // stream of the k-th condition: all on s (in order), or one side stream each when forked
+  auto launch_bcs = [&](cudaStream_t s, bool spread) -> rds_status {
+    for (size_t k = 0; k < ctx->bcs.size(); ++k)
     {
-      const BCArgs a = bc_args(ctx, b, stop);
-      rds_status st  = launch_on(ctx, s, [&](const char **name) {
-        return launch_bc(b, a, b.physics, d.dim, d.neq, s, name);
+      const HostBC &b    = ctx->bcs[k];
+      const cudaStream_t sk = spread ? side_stream(ctx, (int)k) : s;
+      BCArgs a = bc_args(ctx, b, stop);
+      if (ctx->dc_phase == 2)
+        a.c32 = ctx->d_c32; // the change since the exact sweep, in FP32
+      rds_status st  = launch_on(ctx, sk, [&](const char **name) {
+        return launch_bc(b, a, b.physics, d.dim, d.neq, sk, name);
       });
       if (st != RDS_OK)
         return st;
@@ -397,17 +452,40 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
   };
   if (fork)
   {
-    RDS_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
-    RDS_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
-    const rds_status st = launch_bcs(ctx->side);
+    rds_status st = fork_sides(ctx);
+    if (st == RDS_OK)
+      st = launch_bcs(ctx->side, true);
     if (st != RDS_OK)
       return st;
   }
   for (size_t ig = 0; ig < ctx->groups.size(); ++ig)
   {
     const HostCellGroup &g = ctx->groups[ig];
-    const CellArgs a       = cell_args(ctx, g, stop);
+    CellArgs a             = cell_args(ctx, g, stop);
+    if (ctx->dc_phase == 1 && g.scheme == RDS_PGB)
+      a.theta = ctx->d_dc_theta + ctx->dc_cell_base[ig]; // blending coefficients at u_r
     rds_status st          = launch(ctx, [&](const char **name) {
+      if (ctx->dc_phase == 2)
+      {
+        // correction sweep: the FP32 change of the cell residual since the exact sweep
+        DcCellArgs da{};
+        da.ncells     = g.desc.ncells;
+        da.sol_conn   = g.d_sol_conn;
+        da.geo_conn   = g.d_geo_conn;
+        da.X          = ctx->d_X;
+        da.ngeo_nodes = ctx->desc.ngeo_nodes;
+        da.u          = ctx->d_u;
+        da.ur         = ctx->d_ur;
+        da.c32        = ctx->d_c32;
+        da.slot_base  = g.slot_base;
+        da.theta      = ctx->d_dc_theta + ctx->dc_cell_base[ig];
+        da.adv0       = ctx->desc.adv[0];
+        da.adv1       = ctx->desc.adv[1];
+        da.stop       = stop;
+        bool ok       = false;
+        const cudaError_t e = launch_cells_scalar_dc(g, da, 0, 0, ctx->stream, name, &ok);
+        return ok ? e : cudaErrorNotSupported;
+      }
       if (ctx->active_precision == RDS_MIXED && ctx->use_tc && g.d_tc && !ctx->blend_on)
       {
         // FP32 cells with the basis contractions on the tensor cores, persistent CTAs
@@ -435,12 +513,9 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
     }
   }
   if (fork)
-  {
-    RDS_CUDA(cudaEventRecord(ctx->ev_join, ctx->side));
-    RDS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
-  }
-  else if (!ctx->bcs.empty())
-    return launch_bcs(ctx->stream);
+    return join_sides(ctx);
+  if (!ctx->bcs.empty())
+    return launch_bcs(ctx->stream, false);
   return RDS_OK;
 }
 
@@ -945,6 +1020,42 @@ rds_status rds_finalize(rds_ctx *ctx)
       ctx->extra.push_back(g.d_tc);
       g.tune_tile[0] = 128; // one cell per TMEM lane
     }
+  // side streams of the weak conditions after the first (rds_ctx::sides)
+  for (int k = 1; k < std::min((int)ctx->bcs.size(), rds_ctx::kMaxSides); ++k)
+  {
+    RDS_CUDA(cudaStreamCreateWithFlags(&ctx->sides[k], cudaStreamNonBlocking));
+    RDS_CUDA(cudaEventCreateWithFlags(&ctx->ev_joins[k], cudaEventDisableTiming));
+  }
+  // mixed form, scalar physics: buffers of the defect-correction loop
+  if (d.precision == RDS_MIXED && NEQ == 1)
+  {
+    bool ok = true;
+    for (const HostCellGroup &g : ctx->groups)
+      ok = ok && dc_supported(g);
+    if (ok)
+    {
+      long long nc = 0;
+      ctx->dc_cell_base.clear();
+      for (const HostCellGroup &g : ctx->groups)
+      {
+        ctx->dc_cell_base.push_back(nc);
+        nc += g.desc.ncells;
+      }
+      if ((st = dalloc(ctx, &ctx->d_ur, N)) != RDS_OK ||
+          (st = dalloc(ctx, &ctx->d_dres, N)) != RDS_OK ||
+          (st = dalloc(ctx, &ctx->d_dtv, N)) != RDS_OK ||
+          (st = dalloc(ctx, &ctx->d_c32, (size_t)S)) != RDS_OK ||
+          (st = dalloc(ctx, &ctx->d_dc_theta, (size_t)nc)) != RDS_OK)
+        return st;
+      ctx->extra.push_back(ctx->d_ur);
+      ctx->extra.push_back(ctx->d_dres);
+      ctx->extra.push_back(ctx->d_dtv);
+      ctx->extra.push_back(ctx->d_c32);
+      ctx->extra.push_back(ctx->d_dc_theta);
+      RDS_CUDA(cudaMemsetAsync(ctx->d_dc_theta, 0, (size_t)nc * sizeof(double), ctx->stream));
+      ctx->dc_ok = true;
+    }
+  }
   RDS_CUDA(cudaStreamSynchronize(ctx->stream));
   RDS_CUDA(cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device));
   if (ctx->nprob > 0 && (st = finalize_batch(ctx)) != RDS_OK)
@@ -1805,6 +1916,82 @@ static rds_status run_loop(rds_ctx *ctx, double cfl, int max_iter, double drop)
   return replay_chunks(ctx, gi, (max_iter + chunk - 1) / chunk, per_iter * chunk);
 }
 
+// One sweep of the defect-correction loop (mixed form, scalar physics): exact = the fused FP64
+// iteration whose gather also keeps its update dt res, dt / V and the state it started from,
+// with its norm and stop test; otherwise a correction sweep: the FP32 change of each cell's
+// contribution since then (rds_cells_scalar_dc.cu), each facet's FP64 contribution at the
+// current state minus its exact-sweep value, written as FP32, and u -= dt res + (dt / V) sum.
+static rds_status enqueue_dc_sweep(rds_ctx *ctx, bool exact, double cfl, int max_iter,
+                                   double drop)
+{
+  ctx->dc_phase = exact ? 1 : 2;
+  rds_status st = launch_residual_kernels(ctx, ctx->d_stop);
+  ctx->dc_phase = 0;
+  if (st != RDS_OK)
+    return st;
+  GatherArgs ga = gather_args(ctx, cfl, ctx->d_stop);
+  ga.c32        = ctx->d_c32;
+  ga.dres       = ctx->d_dres;
+  ga.dtv        = ctx->d_dtv;
+  ga.ur         = ctx->d_ur;
+  ga.loop       = ctx->d_loop;
+  if (exact)
+  {
+    ga.counter  = ctx->d_counter;
+    ga.norm     = ctx->d_norm;
+    ga.norm0    = ctx->d_norm0;
+    ga.hist     = ctx->d_hist;
+    ga.iter     = ctx->d_iter;
+    ga.max_iter = max_iter;
+    ga.drop     = drop;
+    ga.stop_w   = ctx->d_stop;
+    ga.status   = ctx->d_status;
+    ga.stall    = ctx->d_stall;
+  }
+  return launch(ctx, [&](const char **name) {
+    return launch_gather(ga, exact ? 18 : 19, ctx->gblocks, ctx->stream, name);
+  });
+}
+
+// Defect-correction loop of the mixed form: cycles of one exact FP64 sweep and dc_m - 1 FP32
+// correction sweeps, captured once (graph slot 6, several cycles per graph) and replayed until
+// an exact sweep raises the stop flag. The stop test sees only exact FP64 norms, and the fixed
+// point is the FP64 scheme's: at convergence the correction is zero and R64 = 0.
+static rds_status run_loop_dc(rds_ctx *ctx, double cfl, int max_iter, double drop)
+{
+  rds_status st;
+  const int m = ctx->dc_m;
+  LoopParams lp{};
+  lp.cfl      = cfl;
+  lp.drop     = drop;
+  lp.max_iter = max_iter;
+  lp.dc_m     = m;
+  RDS_CUDA(cudaMemcpyAsync(ctx->d_loop, &lp, sizeof(lp), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->active_precision = RDS_FP64;
+  if (ctx->timing)
+  {
+    for (int it = 0; it < max_iter; ++it)
+      if ((st = enqueue_dc_sweep(ctx, it % m == 0, cfl, max_iter, drop)) != RDS_OK)
+        return st;
+    return RDS_OK;
+  }
+  const int cycles = std::max(1, 32 / m); // sweeps per graph launch: cycles x m
+  auto cycle       = [&]() -> rds_status {
+    for (int j = 0; j < m; ++j)
+    {
+      const rds_status s2 = enqueue_dc_sweep(ctx, j == 0, cfl, max_iter, drop);
+      if (s2 != RDS_OK)
+        return s2;
+    }
+    return RDS_OK;
+  };
+  if ((st = capture_graph(ctx, 6, cycles, cycle)) != RDS_OK)
+    return st;
+  const long long per_sweep = (long long)ctx->groups.size() + (long long)ctx->bcs.size() + 1;
+  const int per_graph       = cycles * m;
+  return replay_chunks(ctx, 6, (max_iter + per_graph - 1) / per_graph, per_sweep * per_graph);
+}
+
 rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int *it_done,
                        double *hist)
 {
@@ -1827,7 +2014,13 @@ rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int 
   RDS_CUDA(cudaMemsetAsync(ctx->d_stop, 0, sizeof(int), ctx->stream));
   RDS_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
 
-  if (ctx->desc.precision == RDS_MIXED)
+  if (ctx->desc.precision == RDS_MIXED && ctx->dc_ok && !ctx->blend_on && !ctx->av_on)
+  {
+    // mixed form, scalar physics: defect-correction loop (exact FP64 sweep every dc_m sweeps)
+    if ((st = run_loop_dc(ctx, cfl, max_iter, drop)) != RDS_OK)
+      return st;
+  }
+  else if (ctx->desc.precision == RDS_MIXED)
   {
     // mixed form: FP32 cell kernels until the relative residual reaches mixed_switch, then a
     // final FP64 phase of pseudo-time sweeps from that state to the requested drop; the
@@ -2031,6 +2224,21 @@ rds_status rds_set_option(rds_ctx *ctx, const char *key, double value)
     release_graph(ctx); // captured loops hold the previous choice
     return RDS_OK;
   }
+  if (std::strcmp(key, "mixed_refresh") == 0)
+  {
+    // defect-correction loop: an exact FP64 sweep every `value` sweeps
+    if (!(value >= 1.0 && value <= 1024.0))
+      return fail(ctx, RDS_ERR_INVALID, "mixed_refresh must be in [1, 1024]");
+    if ((int)value != ctx->dc_m)
+      for (int gi : {2, 6}) // the captured cycles hold the previous period
+        if (ctx->graph_exec[gi])
+        {
+          cudaGraphExecDestroy(ctx->graph_exec[gi]);
+          ctx->graph_exec[gi] = nullptr;
+        }
+    ctx->dc_m = (int)value;
+    return RDS_OK;
+  }
   if (std::strcmp(key, "mixed_stall_min") == 0)
   {
     if (!(value >= 1.0 && value <= 2.0e9))
@@ -2173,7 +2381,10 @@ rds_status rds_add_batch_bc(rds_ctx *ctx, const rds_bc_group *b, int physics)
 // facets of all problems on the side stream, persistent cell kernels over the active tiles of
 // each group (FP32 tiles and FP64 tiles in the mixed form), persistent gather with the
 // per-problem update, norm and stop test.
-static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed)
+// dc: 0 plain iteration (FP32 tiles of the problems in phase 0 when mixed, FP64 tiles of those
+// in phase 1); 1 exact sweep of the defect-correction loop (FP64 cells of every active problem,
+// blending coefficients kept for the corrections); 2 correction sweep (FP32 cell changes).
+static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed, int dc = 0)
 {
   const rds_desc &d = ctx->desc;
   const int P = ctx->nprob, G = (int)ctx->groups.size();
@@ -2195,26 +2406,57 @@ static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed)
   if (st != RDS_OK)
     return st;
   const bool fork = !ctx->bcs.empty();
-  if (fork)
+  if (fork && (st = fork_sides(ctx)) != RDS_OK)
+    return st;
+  for (size_t k = 0; k < ctx->bcs.size(); ++k)
   {
-    RDS_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
-    RDS_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
-  }
-  for (const HostBC &b : ctx->bcs)
-  {
-    const BCArgs a = bc_args(ctx, b, ctx->d_stop);
-    if ((st = launch_on(ctx, ctx->side, [&](const char **name) {
-           return launch_bc(b, a, b.physics, d.dim, d.neq, ctx->side, name);
+    const HostBC &b       = ctx->bcs[k];
+    const cudaStream_t sk = side_stream(ctx, (int)k);
+    BCArgs a              = bc_args(ctx, b, ctx->d_stop);
+    if (dc == 2)
+      a.c32 = ctx->d_c32; // the change since the exact sweep, in FP32
+    if ((st = launch_on(ctx, sk, [&](const char **name) {
+           return launch_bc(b, a, b.physics, d.dim, d.neq, sk, name);
          })) != RDS_OK)
       return st;
   }
   for (int gi = 0; gi < G; ++gi)
   {
     const HostCellGroup &g = ctx->groups[gi];
-    for (int ph = mixed ? 0 : 1; ph < 2; ++ph)
+    if (dc == 2)
+    {
+      // correction sweep over the same active tiles as the exact sweep (phase 1)
+      DcCellArgs da{};
+      da.ncells     = g.desc.ncells;
+      da.sol_conn   = g.d_sol_conn;
+      da.geo_conn   = g.d_geo_conn;
+      da.X          = ctx->d_X;
+      da.ngeo_nodes = d.ngeo_nodes;
+      da.u          = ctx->d_u;
+      da.ur         = ctx->d_ur;
+      da.c32        = ctx->d_c32;
+      da.slot_base  = g.slot_base;
+      da.theta      = ctx->d_dc_theta + ctx->dc_cell_base[gi];
+      da.adv0       = d.adv[0];
+      da.adv1       = d.adv[1];
+      da.stop       = ctx->d_stop;
+      da.bt         = {ctx->d_tile_prefix + ((size_t)gi * 2 + 1) * (P + 1), g.d_cbeg, g.d_cend, P};
+      const int grid = g.tune_grid[1] > 0 ? g.tune_grid[1] : 4 * ctx->nsm;
+      if ((st = launch(ctx, [&](const char **name) {
+             bool ok             = false;
+             const cudaError_t e = launch_cells_scalar_dc(g, da, grid, g.tune_tile[1],
+                                                          ctx->stream, name, &ok);
+             return ok ? e : cudaErrorNotSupported;
+           })) != RDS_OK)
+        return st;
+      continue;
+    }
+    for (int ph = (mixed && dc == 0) ? 0 : 1; ph < 2; ++ph)
     {
       CellArgs a = cell_args(ctx, g, ctx->d_stop);
       a.bt       = {ctx->d_tile_prefix + ((size_t)gi * 2 + ph) * (P + 1), g.d_cbeg, g.d_cend, P};
+      if (dc == 1 && g.scheme == RDS_PGB)
+        a.theta = ctx->d_dc_theta + ctx->dc_cell_base[gi];
       const int grid = g.tune_grid[ph] > 0 ? g.tune_grid[ph] : 4 * ctx->nsm;
       const bool tc  = ph == 0 && ctx->use_tc && g.d_tc;
       if ((st = launch(ctx, [&](const char **name) {
@@ -2228,14 +2470,15 @@ static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed)
         return st;
     }
   }
-  if (fork)
-  {
-    RDS_CUDA(cudaEventRecord(ctx->ev_join, ctx->side));
-    RDS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
-  }
+  if (fork && (st = join_sides(ctx)) != RDS_OK)
+    return st;
   GatherArgs ga = gather_args(ctx, 0.0, ctx->d_stop);
   ga.status     = ctx->d_status;
   ga.loop       = ctx->d_loop;
+  ga.c32        = ctx->d_c32;
+  ga.dres       = ctx->d_dres;
+  ga.dtv        = ctx->d_dtv;
+  ga.ur         = ctx->d_ur;
   BatchArgs b{};
   b.nprob     = P;
   b.node_off  = ctx->d_node_off;
@@ -2252,7 +2495,7 @@ static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed)
   b.loop      = ctx->d_loop;
   b.stall     = ctx->d_pstall;
   return launch(ctx, [&](const char **name) {
-    return launch_gather_batch(ga, b, ctx->batch_grid, ctx->stream, name);
+    return launch_gather_batch(ga, b, ctx->batch_grid, ctx->stream, name, dc);
   });
 }
 
@@ -2265,6 +2508,10 @@ rds_status rds_iterate_batch(rds_ctx *ctx, int max_iter, double drop, int32_t *i
                : RDS_ERR_INVALID;
   const int P = ctx->nprob, NEQ = ctx->desc.neq;
   const bool mixed = ctx->desc.precision == RDS_MIXED;
+  // mixed form, scalar physics: the defect-correction loop, every problem in step with the
+  // single-problem loop (exact FP64 sweep at sweeps 0, m, 2m, ..., FP32 corrections between)
+  const bool dc    = mixed && ctx->dc_ok;
+  const int m      = dc ? ctx->dc_m : 1;
   rds_status st;
   LoopParams lp{};
   lp.drop     = drop;
@@ -2272,8 +2519,9 @@ rds_status rds_iterate_batch(rds_ctx *ctx, int max_iter, double drop, int32_t *i
   lp.max_iter   = max_iter;
   lp.stall_min  = ctx->stall_min;
   lp.stall_mult = ctx->stall_mult;
+  lp.dc_m       = dc ? m : 0;
   RDS_CUDA(cudaMemcpyAsync(ctx->d_loop, &lp, sizeof(lp), cudaMemcpyHostToDevice, ctx->stream));
-  const std::vector<int32_t> phase0(P, mixed ? 0 : 1);
+  const std::vector<int32_t> phase0(P, (mixed && !dc) ? 0 : 1);
   const int32_t one = 1;
   if ((st = upload(ctx, ctx->d_phase, phase0.data(), P)) ||
       (st = upload(ctx, ctx->d_changed, &one, 1)))
@@ -2285,7 +2533,36 @@ rds_status rds_iterate_batch(rds_ctx *ctx, int max_iter, double drop, int32_t *i
   RDS_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
   // every problem is done after max_iter iterations; one more raises the stop flag
   const int total_iter = max_iter + 1;
-  if (ctx->timing)
+  if (dc)
+  {
+    const long long per_sweep = 2 + (long long)ctx->bcs.size() + (long long)ctx->groups.size();
+    if (ctx->timing)
+    {
+      for (int it = 0; it < total_iter; ++it)
+        if ((st = enqueue_batch_iteration(ctx, mixed, it % m == 0 ? 1 : 2)) != RDS_OK)
+          return st;
+    }
+    else
+    {
+      const int cycles = std::max(1, 32 / m);
+      auto cycle       = [&]() -> rds_status {
+        for (int j = 0; j < m; ++j)
+        {
+          const rds_status s2 = enqueue_batch_iteration(ctx, mixed, j == 0 ? 1 : 2);
+          if (s2 != RDS_OK)
+            return s2;
+        }
+        return RDS_OK;
+      };
+      if ((st = capture_graph(ctx, 2, cycles, cycle)) != RDS_OK)
+        return st;
+      const int per_graph = cycles * m;
+      if ((st = replay_chunks(ctx, 2, (total_iter + per_graph - 1) / per_graph,
+                              per_sweep * per_graph)) != RDS_OK)
+        return st;
+    }
+  }
+  else if (ctx->timing)
   {
     for (int it = 0; it < total_iter; ++it)
       if ((st = enqueue_batch_iteration(ctx, mixed)) != RDS_OK)
@@ -2457,6 +2734,9 @@ rds_status rds_destroy(rds_ctx *ctx)
     cudaStreamSynchronize(ctx->stream);
   if (ctx->side)
     cudaStreamSynchronize(ctx->side);
+  for (int k = 1; k < rds_ctx::kMaxSides; ++k)
+    if (ctx->sides[k])
+      cudaStreamSynchronize(ctx->sides[k]);
   release_graph(ctx);
   for (HostCellGroup &g : ctx->groups)
   {
@@ -2522,6 +2802,13 @@ rds_status rds_destroy(rds_ctx *ctx)
     cudaEventDestroy(ctx->ev_join);
   if (ctx->side)
     cudaStreamDestroy(ctx->side);
+  for (int k = 1; k < rds_ctx::kMaxSides; ++k)
+  {
+    if (ctx->sides[k])
+      cudaStreamDestroy(ctx->sides[k]);
+    if (ctx->ev_joins[k])
+      cudaEventDestroy(ctx->ev_joins[k]);
+  }
   if (ctx->own_stream && ctx->stream)
     cudaStreamDestroy(ctx->stream);
   delete ctx;

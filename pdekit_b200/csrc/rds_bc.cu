@@ -264,14 +264,28 @@ __global__ void __launch_bounds__(kBlock)
     }
   }
 
-#pragma unroll
-  for (int n = 0; n < NFDOF; ++n)
+  if (NEQ == 1 && a.c32)
   {
-    const long long slot = a.slot_base + (long long)n * a.nfacets + f;
+    // correction sweep of the defect-correction loop: the change since the exact sweep, whose
+    // contribution is still in contrib (FP64 difference, then FP32: relative to the change)
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e)
-      a.contrib[e * a.S + slot] = bres[n][e];
-    a.wsc[a.ws_base + (long long)n * a.nfacets + f] = a.vol[dof[n]] * coeff;
+    for (int n = 0; n < NFDOF; ++n)
+    {
+      const long long slot = a.slot_base + (long long)n * a.nfacets + f;
+      a.c32[slot]          = float(bres[n][0] - a.contrib[slot]);
+    }
+  }
+  else
+  {
+#pragma unroll
+    for (int n = 0; n < NFDOF; ++n)
+    {
+      const long long slot = a.slot_base + (long long)n * a.nfacets + f;
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+        a.contrib[e * a.S + slot] = bres[n][e];
+      a.wsc[a.ws_base + (long long)n * a.nfacets + f] = a.vol[dof[n]] * coeff;
+    }
   }
   if (bad)
     atomicOr(a.status, kFlagNegPressure);

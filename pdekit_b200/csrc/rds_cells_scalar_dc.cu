@@ -1,0 +1,348 @@
+// Mixed form, scalar physics: cell kernels of the FP32 correction sweeps of the defect-correction
+// loop (rds_api.cu, run_loop_dc).
+//
+// Every m sweeps the loop evaluates the exact FP64 residual R64(u_r) at the current state u_r
+// (the plain cell kernels, rds_cells_scalar.cu) and keeps its update dt R64(u_r). The m - 1
+// sweeps in between advance u = u_r + d with the increment
+//     R64(u_r) + dR_cells(d) + [R64_bc(u) - R64_bc(u_r)],
+// where the boundary part is evaluated in FP64 at u (facets are few; rds_bc.cu writes the
+// difference) and dR_cells(d) is the change of the cell residual computed HERE, in FP32, from
+// d = u - u_r directly:
+//   * the flux change is exact in d: Burgers F(s_r + ds) - F(s_r) = (ds (s_r + ds/2), ds),
+//     advection a ds, at the p+1 flux nodes, contracted like the plain kernel;
+//   * the distribution coefficients (K+_n, beta_n = K+_n / sum K+, the blending coefficient
+//     theta of PGB) are those of u_r (Picard linearisation; for advection they do not depend
+//     on u, so dR is then exact);
+//   * LDA part  sum_q w_q detJ beta_n dr_q,
+//     N part    sum_q w_q detJ beta_n sum_m K+_m (d_n - d_m).
+// Every term is a product of a coefficient and a d-sized quantity, so FP32 round-off is relative
+// to the correction itself and shrinks with it: the loop keeps converging past the FP32 floor
+// of a plain FP32 residual, to the FP64 scheme's own fixed point (at a fixed point d = 0 and
+// R64(u_r) = 0). No FP64 arithmetic is left in the cell loop; the changes are stored as FP32
+// and summed by the node gather in FP64.
+//
+// Schemes follow src/solver/rdm/cellsplitters/PGLDA.hpp:171-310, PGN.hpp:154-289 and
+// PGB.hpp:314-498 (the plain kernels restate them; this is their linearisation at u_r).
+
+#include "rds_internal.h"
+#include "rds_tables.cuh"
+
+namespace rds
+{
+
+namespace
+{
+
+template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL, int NGEO>
+__device__ __forceinline__ void dc_cell(const DcCellArgs &a,
+                                        const Tables<float, 2, NDOF, NQ, NFL, NGEO> &tb,
+                                        const int c)
+{
+  using T = float;
+  // reference state in deviation form (coefficients) and the correction d = u - u_r
+  double ur0 = 0.0;
+  T ut[NDOF], dn[NDOF];
+#pragma unroll
+  for (int n = 0; n < NDOF; ++n)
+  {
+    const int v     = __ldg(a.sol_conn + (size_t)n * a.ncells + c);
+    const double r  = __ldg(a.ur + v);
+    const double uu = __ldg(a.u + v);
+    if (n == 0)
+      ur0 = r;
+    ut[n] = T(r - ur0);
+    dn[n] = T(uu - r);
+  }
+  const T u0 = T(ur0);
+
+  // straight-sided triangle (deviation form of the vertex coordinates)
+  T ij00, ij01, ij10, ij11, detj;
+  {
+    T X0[NGEO], X1[NGEO];
+    double xg0 = 0.0, yg0 = 0.0;
+#pragma unroll
+    for (int g = 0; g < NGEO; ++g)
+    {
+      const int v     = __ldg(a.geo_conn + (size_t)g * a.ncells + c);
+      const double xg = __ldg(a.X + v), yg = __ldg(a.X + a.ngeo_nodes + v);
+      if (g == 0)
+      {
+        xg0 = xg;
+        yg0 = yg;
+      }
+      X0[g] = T(xg - xg0);
+      X1[g] = T(yg - yg0);
+    }
+    T J00 = tb.dVgeo[0][0][0] * X0[0], J01 = tb.dVgeo[0][0][0] * X1[0];
+    T J10 = tb.dVgeo[1][0][0] * X0[0], J11 = tb.dVgeo[1][0][0] * X1[0];
+#pragma unroll
+    for (int g = 1; g < NGEO; ++g)
+    {
+      J00 = J00 + tb.dVgeo[0][0][g] * X0[g];
+      J01 = J01 + tb.dVgeo[0][0][g] * X1[g];
+      J10 = J10 + tb.dVgeo[1][0][g] * X0[g];
+      J11 = J11 + tb.dVgeo[1][0][g] * X1[g];
+    }
+    detj            = J00 * J11 - J01 * J10;
+    const T inv_det = T(1) / detj;
+    ij00            = inv_det * J11;
+    ij11            = inv_det * J00;
+    ij01            = -inv_det * J01;
+    ij10            = -inv_det * J10;
+  }
+
+  // change of the flux divergence at the points, dr_q = sum_f dVf[.][q][f] dG_f, with the flux
+  // change at each flux node contracted with invJ once (constant over the cell)
+  T dr[NQ];
+  {
+    T G0[NFL], G1[NFL];
+#pragma unroll
+    for (int f = 0; f < NFL; ++f)
+    {
+      T ds = tb.Vsf[f][0] * dn[0];
+#pragma unroll
+      for (int n = 1; n < NDOF; ++n)
+        ds = ds + tb.Vsf[f][n] * dn[n];
+      T F0, F1;
+      if (PHYS == RDS_BURGERS2D)
+      {
+        T sr = T(0); // s_r - u_r0 (the node-0 deviation basis sums to one)
+#pragma unroll
+        for (int n = 1; n < NDOF; ++n)
+          sr = sr + tb.Vsf[f][n] * ut[n];
+        F0 = ds * ((u0 + sr) + T(0.5) * ds);
+        F1 = ds;
+      }
+      else
+      {
+        F0 = T(a.adv0) * ds;
+        F1 = T(a.adv1) * ds;
+      }
+      G0[f] = ij00 * F0 + ij10 * F1;
+      G1[f] = ij01 * F0 + ij11 * F1;
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+    {
+      T r = tb.dVf[0][q][0] * G0[0] + tb.dVf[1][q][0] * G1[0];
+#pragma unroll
+      for (int f = 1; f < NFL; ++f)
+        r = r + tb.dVf[0][q][f] * G0[f] + tb.dVf[1][q][f] * G1[f];
+      dr[q] = r;
+    }
+  }
+
+  // d in deviation form for the N dissipation (sum_m K+_m (d_n - d_m) is invariant to a shift)
+  T dd[NDOF];
+#pragma unroll
+  for (int n = 0; n < NDOF; ++n)
+    dd[n] = dn[n] - dn[0];
+
+  // With e = w_q detJ / sum K+ (so e sum K+ = w_q detJ), the LDA and blended N parts are
+  //   sum_q e K+_n dr_q + theta sum_q e K+_n (d_n sum K+ - sum_m K+_m d_m)
+  //   = sum_q K+_n [e (dr_q - theta sum_m K+_m d_m)] + theta d_n sum_q w_q detJ K+_n,
+  // two FMAs per point and node (theta = 1 for PGN, the N part absent for PGLDA).
+  const T theta = (SCHEME == RDS_PGB) ? T(__ldg(a.theta + c)) : T(1);
+  T racc[NDOF], wacc[NDOF];
+#pragma unroll
+  for (int n = 0; n < NDOF; ++n)
+  {
+    racc[n] = T(0);
+    wacc[n] = T(0);
+  }
+
+#pragma unroll
+  for (int q = 0; q < NQ; ++q)
+  {
+    const T wj = tb.w[q] * detj;
+    T ax, ay;
+    if (PHYS == RDS_BURGERS2D)
+    {
+      T uq = T(0);
+#pragma unroll
+      for (int n = 1; n < NDOF; ++n)
+        uq = uq + tb.V[q][n] * ut[n];
+      ax = u0 + uq;
+      ay = T(1);
+    }
+    else
+    {
+      ax = T(a.adv0);
+      ay = T(a.adv1);
+    }
+    const T A = ax * ij00 + ay * ij10;
+    const T B = ax * ij01 + ay * ij11;
+    T kp[NDOF];
+    T sumkp = T(0);
+#pragma unroll
+    for (int n = 0; n < NDOF; ++n)
+    {
+      const T k = tb.dV[0][q][n] * A + tb.dV[1][q][n] * B;
+      kp[n]     = k > T(0) ? k : T(0);
+      sumkp     = sumkp + kp[n];
+    }
+    const T e = __fdividef(wj, sumkp); // a coefficient: 2-ulp division is enough
+    T ec;
+    if (SCHEME == RDS_PGLDA)
+      ec = e * dr[q];
+    else
+    {
+      T tkd = T(0);
+#pragma unroll
+      for (int m = 1; m < NDOF; ++m)
+        tkd = tkd + kp[m] * dd[m];
+      ec = e * (dr[q] - theta * tkd);
+    }
+#pragma unroll
+    for (int n = 0; n < NDOF; ++n)
+    {
+      racc[n] = racc[n] + kp[n] * ec;
+      if (SCHEME != RDS_PGLDA)
+        wacc[n] = wacc[n] + wj * kp[n];
+    }
+  }
+
+  float *out = a.c32 + a.slot_base + c;
+#pragma unroll
+  for (int n = 0; n < NDOF; ++n)
+    out[(size_t)n * a.ncells] =
+        (SCHEME == RDS_PGLDA) ? racc[n] : racc[n] + (theta * dd[n]) * wacc[n];
+}
+
+template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL, int NGEO>
+__global__ void __launch_bounds__(kBlock)
+    cells_scalar2d_dc(const __grid_constant__ DcCellArgs a,
+                      const __grid_constant__ Tables<float, 2, NDOF, NQ, NFL, NGEO> tb)
+{
+  if (*a.stop)
+    return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncells)
+    return;
+  dc_cell<PHYS, SCHEME, NDOF, NQ, NFL, NGEO>(a, tb, c);
+}
+
+// Batch form: a persistent grid walks the group's active tiles (the problems still iterating);
+// a tile is blockDim.x consecutive cells of one problem. Results per cell are those of
+// cells_scalar2d_dc.
+template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL, int NGEO>
+__global__ void __launch_bounds__(128)
+    cells_scalar2d_dc_batch(const __grid_constant__ DcCellArgs a,
+                            const __grid_constant__ Tables<float, 2, NDOF, NQ, NFL, NGEO> tb)
+{
+  if (*a.stop)
+    return;
+  const int32_t *prefix = a.bt.prefix;
+  const int np          = a.bt.nprob;
+  const int total       = prefix[np];
+  for (int t = blockIdx.x; t < total; t += gridDim.x)
+  {
+    // problem p with prefix[p] <= t < prefix[p+1]
+    int lo = 0, hi = np;
+    while (hi - lo > 1)
+    {
+      const int mid = (lo + hi) >> 1;
+      if (prefix[mid] <= t)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const int c = a.bt.cbeg[lo] + (t - prefix[lo]) * (int)blockDim.x + (int)threadIdx.x;
+    if (c < a.bt.cend[lo])
+      dc_cell<PHYS, SCHEME, NDOF, NQ, NFL, NGEO>(a, tb, c);
+  }
+}
+
+template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL>
+cudaError_t launch_batch_one(const HostCellGroup &g, const DcCellArgs &a, int grid, int tile,
+                             cudaStream_t s)
+{
+  Tables<float, 2, NDOF, NQ, NFL, 3> tb;
+  fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
+  auto k = cells_scalar2d_dc_batch<PHYS, SCHEME, NDOF, NQ, NFL, 3>;
+  // a persistent grid only balances if all its CTAs are resident at once: cap it at the
+  // occupancy of this kernel and tile
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, tile, 0);
+  const int cap = (per_sm < 1 ? 1 : per_sm) * nsm;
+  k<<<grid < cap ? grid : cap, tile, 0, s>>>(a, tb);
+  return cudaGetLastError();
+}
+
+template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL>
+cudaError_t launch_one(const HostCellGroup &g, const DcCellArgs &a, cudaStream_t s)
+{
+  Tables<float, 2, NDOF, NQ, NFL, 3> tb;
+  fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
+  const int grid = (a.ncells + kBlock - 1) / kBlock;
+  cells_scalar2d_dc<PHYS, SCHEME, NDOF, NQ, NFL, 3><<<grid, kBlock, 0, s>>>(a, tb);
+  return cudaGetLastError();
+}
+
+// grid > 0: the batch form (persistent over the active tiles, `tile` cells per CTA)
+template <int PHYS, int SCHEME>
+cudaError_t dispatch_shape(const HostCellGroup &g, const DcCellArgs &a, int grid, int tile,
+                           cudaStream_t s, bool *ok)
+{
+  const rds_cell_group &d = g.desc;
+  *ok                     = true;
+#define RDS_DC_SHAPE(ND, NQ_, NF)                                                                  \
+  if (d.ndof == ND && d.nq == NQ_ && d.nfl == NF)                                                  \
+    return grid > 0 ? launch_batch_one<PHYS, SCHEME, ND, NQ_, NF>(g, a, grid, tile, s)             \
+                    : launch_one<PHYS, SCHEME, ND, NQ_, NF>(g, a, s);
+  if (d.shape == RDS_TRIAG && d.ngeo == 3)
+  {
+    // (order, quadrature points, flux nodes): P1/P4-rule, P1/P5, P2/P4, P2/P5, P3/P8
+    RDS_DC_SHAPE(3, 6, 6)
+    RDS_DC_SHAPE(3, 7, 6)
+    RDS_DC_SHAPE(6, 6, 10)
+    RDS_DC_SHAPE(6, 7, 10)
+    RDS_DC_SHAPE(10, 16, 15)
+  }
+#undef RDS_DC_SHAPE
+  *ok = false;
+  return cudaSuccess;
+}
+
+} // namespace
+
+bool dc_supported(const HostCellGroup &g)
+{
+  const rds_cell_group &d = g.desc;
+  if ((g.physics != RDS_ADVECTION_CONST && g.physics != RDS_BURGERS2D) || d.shape != RDS_TRIAG ||
+      d.ngeo != 3)
+    return false;
+  return (d.ndof == 3 && (d.nq == 6 || d.nq == 7) && d.nfl == 6) ||
+         (d.ndof == 6 && (d.nq == 6 || d.nq == 7) && d.nfl == 10) ||
+         (d.ndof == 10 && d.nq == 16 && d.nfl == 15);
+}
+
+cudaError_t launch_cells_scalar_dc(const HostCellGroup &g, const DcCellArgs &a, int grid,
+                                   int tile, cudaStream_t s, const char **name, bool *ok)
+{
+  static const char *names[2][2][3] = {
+      {{"cells_adv_lda_dc", "cells_adv_n_dc", "cells_adv_b_dc"},
+       {"cells_burgers_lda_dc", "cells_burgers_n_dc", "cells_burgers_b_dc"}},
+      {{"cells_adv_lda_dc_batch", "cells_adv_n_dc_batch", "cells_adv_b_dc_batch"},
+       {"cells_burgers_lda_dc_batch", "cells_burgers_n_dc_batch", "cells_burgers_b_dc_batch"}}};
+  *ok = false;
+  if (!dc_supported(g) || g.scheme < 0 || g.scheme > 2 ||
+      (grid > 0 && (tile <= 0 || tile > 128 || tile % 32 != 0)))
+    return cudaSuccess;
+  *name = names[grid > 0][g.physics == RDS_BURGERS2D][g.scheme];
+#define RDS_DC_CASE(PH, SC)                                                                        \
+  if (g.physics == PH && g.scheme == SC)                                                           \
+    return dispatch_shape<PH, SC>(g, a, grid, tile, s, ok);
+  RDS_DC_CASE(RDS_ADVECTION_CONST, RDS_PGLDA)
+  RDS_DC_CASE(RDS_ADVECTION_CONST, RDS_PGN)
+  RDS_DC_CASE(RDS_ADVECTION_CONST, RDS_PGB)
+  RDS_DC_CASE(RDS_BURGERS2D, RDS_PGLDA)
+  RDS_DC_CASE(RDS_BURGERS2D, RDS_PGN)
+  RDS_DC_CASE(RDS_BURGERS2D, RDS_PGB)
+#undef RDS_DC_CASE
+  return cudaSuccess;
+}
+
+} // namespace rds

@@ -70,10 +70,37 @@ __device__ __forceinline__ bool fp32_stalled(double rel, int it, StallRec *r, co
   return double(it - r->best_it) > window;
 }
 
-template <int NEQ, bool DT, bool UPDATE, bool NORM, bool RK = false>
+// DC (defect-correction loop, one equation): 1 = exact sweep that also keeps its update
+// dt res, dt / V and the state the sweep starts from; 2 = correction sweep: every slot holds
+// the FP32 change of its contribution since the exact sweep, u -= dt res + (dt / V) sum
+// (nothing else is written).
+template <int NEQ, bool DT, bool UPDATE, bool NORM, bool RK = false, int DC = 0>
 __device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, const double cfl,
                                             double *sq)
 {
+  static_assert(DC == 0 || NEQ == 1, "the defect-correction gather is scalar");
+  if (DC == 2)
+  {
+    const int i0 = a.row[v], i1 = a.row[v + 1];
+    double sum   = 0.0;
+    int i        = i0;
+    constexpr int B = 4;
+    for (; i + B <= i1; i += B)
+    {
+      float c[B];
+#pragma unroll
+      for (int k = 0; k < B; ++k)
+        c[k] = __ldcs(a.c32 + __ldg(a.ent_slot + i + k));
+#pragma unroll
+      for (int k = 0; k < B; ++k)
+        sum += double(c[k]);
+    }
+    for (; i < i1; ++i)
+      sum += double(__ldcs(a.c32 + __ldg(a.ent_slot + i)));
+    double *pu = a.u + v;
+    *pu        = *pu - (a.dres[v] + double(a.dtv[v]) * sum);
+    return;
+  }
   double acc[NEQ];
 #pragma unroll
   for (int e = 0; e < NEQ; ++e)
@@ -125,6 +152,8 @@ __device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, co
       acc[e] = __dadd_rn(acc[e], __dmul_rn(iv, __ldcs(a.contrib + e * a.S + s)));
     ws = __dadd_rn(ws, __ldcs(a.wsc + w));
   }
+  if (DC == 1)
+    a.ur[v] = a.u[v];
 #pragma unroll
   for (int e = 0; e < NEQ; ++e)
     a.res[(size_t)e * a.nnodes + v] = acc[e];
@@ -156,6 +185,11 @@ __device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, co
   {
     const double dtv = __ddiv_rn(__dmul_rn(cfl, vv), ws);
     a.dt[v]          = dtv;
+    if (DC == 1)
+    {
+      a.dres[v] = __dmul_rn(dtv, acc[0]); // this sweep's update, u_new = u - dres
+      a.dtv[v]  = float(dtv * iv);
+    }
 #pragma unroll
     for (int e = 0; e < NEQ; ++e)
     {
@@ -173,7 +207,7 @@ __device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, co
   }
 }
 
-template <int NEQ, bool DT, bool UPDATE, bool NORM, bool FINAL, bool RK = false>
+template <int NEQ, bool DT, bool UPDATE, bool NORM, bool FINAL, bool RK = false, int DC = 0>
 __global__ void __launch_bounds__(kGBlock) gather_nodes(const __grid_constant__ GatherArgs a)
 {
   __shared__ double smem[kGBlock / 32];
@@ -185,7 +219,7 @@ __global__ void __launch_bounds__(kGBlock) gather_nodes(const __grid_constant__ 
   for (int e = 0; e < NEQ; ++e)
     sq[e] = 0.0;
   if (v < a.nnodes)
-    gather_node<NEQ, DT, UPDATE, NORM, RK>(a, v, a.loop ? a.loop->cfl : a.cfl, sq);
+    gather_node<NEQ, DT, UPDATE, NORM, RK, DC>(a, v, a.loop ? a.loop->cfl : a.cfl, sq);
   if (NORM)
   {
 #pragma unroll
@@ -286,19 +320,30 @@ __device__ void reduce_final(const double *part, int nblocks, int neq, int nnode
     const double r  = n0 > 0.0 ? n / n0 : 0.0;
     rel             = r > rel ? r : rel;
   }
-  *iter = it + 1;
+  // defect-correction loop: this exact sweep is followed by m - 1 correction sweeps, which
+  // count as iterations and repeat this norm in the history; the loop stops only here, so it
+  // also stops when the next exact sweep would fall past max_iter
+  const int m = (loop && loop->dc_m > 1) ? loop->dc_m : 1;
+  *iter       = it + 1;
   if (!finite)
   {
     atomicOr(status, kFlagNonFinite);
     *stop = 1;
   }
-  else if ((drop > 0.0 && rel <= drop) || it + 1 >= max_iter)
+  else if ((drop > 0.0 && rel <= drop) || it + m >= max_iter)
   {
     *stop = 1;
   }
   else if (loop && loop->stall && fp32_stalled(rel, it, stall, *loop))
   {
     *stop = 1;
+  }
+  else if (m > 1)
+  {
+    for (int j = 1; j < m; ++j)
+      for (int e = 0; e < neq; ++e)
+        hist[(size_t)(it + j) * neq + e] = nv[e];
+    *iter = it + m;
   }
 }
 
@@ -433,8 +478,10 @@ __device__ void problem_final(const GatherArgs &a, const BatchArgs &b, const int
     const double r  = n0 > 0.0 ? n / n0 : 0.0;
     rel             = r > rel ? r : rel;
   }
-  b.iter[p]              = it + 1;
   const LoopParams &L    = *b.loop;
+  // defect-correction loop: m - 1 correction sweeps follow this exact sweep and count as
+  // iterations; the problem stops here when the next exact sweep would fall past max_iter
+  const int m            = L.dc_m > 1 ? L.dc_m : 1;
   int nph                = ph;
   const double drop1     = L.drop > L.sw ? L.drop : L.sw;
   if (!finite)
@@ -447,8 +494,9 @@ __device__ void problem_final(const GatherArgs &a, const BatchArgs &b, const int
     nph = 1;
   else if (ph == 1 && L.drop > 0.0 && rel <= L.drop)
     nph = 2;
-  if (nph != 2 && it + 1 >= L.max_iter)
+  if (nph != 2 && it + m >= L.max_iter)
     nph = 2;
+  b.iter[p] = (nph == 2) ? it + 1 : it + m;
   if (nph != ph)
   {
     b.phase[p] = nph;
@@ -460,7 +508,9 @@ __device__ void problem_final(const GatherArgs &a, const BatchArgs &b, const int
 // Persistent gather over the node blocks of the problems still iterating: each problem's nodes
 // are split into blocks of kGBlock from its first node, exactly as a single-problem context
 // splits them, and the block that completes a problem's iteration reduces its norm.
-template <int NEQ>
+// DC: 0 plain; 1 exact sweep of the defect-correction loop (also keeps dres / dtv / ur);
+// 2 correction sweep (FP32 changes of every slot, no norm or stop test).
+template <int NEQ, int DC = 0>
 __global__ void __launch_bounds__(kGBlock)
     gather_batch(const __grid_constant__ GatherArgs a, const __grid_constant__ BatchArgs b)
 {
@@ -482,7 +532,9 @@ __global__ void __launch_bounds__(kGBlock)
     for (int e = 0; e < NEQ; ++e)
       sq[e] = 0.0;
     if (v < n1)
-      gather_node<NEQ, true, true, true>(a, v, b.cfl[p], sq);
+      gather_node<NEQ, DC != 2, DC != 2, DC != 2, false, DC>(a, v, b.cfl[p], sq);
+    if (DC == 2)
+      continue; // uniform over the block: no barrier is skipped by part of it
     const int slot = b.nb_base[p] + j;
 #pragma unroll
     for (int e = 0; e < NEQ; ++e)
@@ -623,6 +675,19 @@ cudaError_t launch_gather_neq(const GatherArgs &a, int mode, int nblocks, cudaSt
   return cudaGetLastError();
 }
 
+// defect-correction loop (one equation): 18 exact fused sweep keeping dres / dtv / ur, 19
+// correction sweep
+cudaError_t launch_gather_dc(const GatherArgs &a, int mode, int nblocks, cudaStream_t s)
+{
+  if (mode == 18)
+    gather_nodes<1, true, true, true, true, false, 1><<<nblocks, kGBlock, 0, s>>>(a);
+  else if (mode == 19)
+    gather_nodes<1, false, false, false, false, false, 2><<<nblocks, kGBlock, 0, s>>>(a);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
 } // namespace
 
 cudaError_t launch_gather(const GatherArgs &a, int mode, int nblocks, cudaStream_t s,
@@ -630,8 +695,12 @@ cudaError_t launch_gather(const GatherArgs &a, int mode, int nblocks, cudaStream
 {
   *name = (mode == 15)  ? "gather_update_norm_final"
           : (mode == 7) ? "gather_update_norm"
+          : (mode == 18) ? "gather_dc_exact"
+          : (mode == 19) ? "gather_dc_correction"
           : (mode >= 16) ? "gather_rk_stage"
                         : "gather_nodes";
+  if (mode == 18 || mode == 19)
+    return a.neq == 1 ? launch_gather_dc(a, mode, nblocks, s) : cudaErrorInvalidValue;
   switch (a.neq)
   {
   case 1:
@@ -702,8 +771,19 @@ cudaError_t launch_dual_volume(int nnodes, const int32_t *row, const int32_t *en
 }
 
 cudaError_t launch_gather_batch(const GatherArgs &a, const BatchArgs &b, int grid, cudaStream_t s,
-                                const char **name)
+                                const char **name, int dc)
 {
+  if (dc == 1 || dc == 2)
+  {
+    if (a.neq != 1)
+      return cudaErrorInvalidValue;
+    *name = dc == 1 ? "gather_batch_dc_exact" : "gather_batch_dc_correction";
+    if (dc == 1)
+      gather_batch<1, 1><<<grid, kGBlock, 0, s>>>(a, b);
+    else
+      gather_batch<1, 2><<<grid, kGBlock, 0, s>>>(a, b);
+    return cudaGetLastError();
+  }
   *name = "gather_batch";
   switch (a.neq)
   {

@@ -71,6 +71,7 @@ struct LoopParams
   int stall_min;     //   max(stall_min, stall_mult x the last interval between halvings)
   int max_iter;
   int stall;       // nonzero: FP32 phase, also stop when progress stalls
+  int dc_m;        // defect-correction loop: an exact FP64 sweep every dc_m sweeps (0, 1: off)
 };
 
 // Progress record of the FP32 phase of the mixed loop.
@@ -149,6 +150,25 @@ struct CellArgs
   const double *blend; // PGB: external nodal blending coefficient [nnodes] when not null
 };
 
+// FP32 correction sweep of the defect-correction loop (rds_cells_scalar_dc.cu): the change of
+// the cell residual from u_r to u, written as FP32 values to the cell slots of c32.
+struct DcCellArgs
+{
+  int ncells;
+  const int32_t *__restrict__ sol_conn; // SoA [ndof][ncells]
+  const int32_t *__restrict__ geo_conn; // SoA [ngeo][ncells]
+  const double *__restrict__ X;
+  int ngeo_nodes;
+  const double *__restrict__ u;  // current state [nnodes]
+  const double *__restrict__ ur; // reference state of the cycle [nnodes]
+  float *__restrict__ c32;       // [slots]
+  long long slot_base;
+  const double *__restrict__ theta; // PGB: the cell's blending coefficient at u_r [ncells]
+  double adv0, adv1;
+  const int *stop;
+  BatchTileMap bt; // batch form only
+};
+
 struct BCArgs
 {
   int nfacets;
@@ -171,6 +191,10 @@ struct BCArgs
   unsigned *status;
   const int *stop;
   double *u_strong; // strong Dirichlet: the state it overwrites (the same buffer as u)
+  // correction sweep of the defect-correction loop (one equation): when set, the facet writes
+  // the change of its contribution since the exact sweep (still in contrib) to c32[slot]
+  // instead of contrib, and no wave speed
+  float *c32;
 };
 
 struct GatherArgs
@@ -209,6 +233,15 @@ struct GatherArgs
   const double *rk_un; // SoA [neq][nnodes]
   const double *rk_us;
   double *rk_out;
+  // defect-correction loop (modes 18 / 19, one equation):
+  // 18: the fused FP64 sweep that also keeps dres = dt res (its update), dtv = dt / V and the
+  //     state it started from (ur);
+  // 19: a correction sweep, u -= dres + dtv sum(c32 entries): c32 holds, per slot, the FP32
+  //     change of the cell or facet contribution since the exact sweep
+  const float *c32;
+  double *dres;
+  float *dtv;
+  double *ur;
 };
 
 // ---- launchers (return cudaError_t of the launch) --------------------------------------
@@ -244,8 +277,10 @@ cudaError_t launch_cells_scalar_batch(const HostCellGroup &g, const CellArgs &a,
                                       bool *ok);
 // Batch mode: persistent gather over the active problems' node blocks with per-problem dt,
 // update, norm and stop test; then the rebuild of the active lists after phase changes.
+// dc: 0 plain, 1 exact sweep of the defect-correction loop (keeps rcell / ur), 2 correction
+// sweep (no norm, no stop test).
 cudaError_t launch_gather_batch(const GatherArgs &a, const BatchArgs &b, int grid, cudaStream_t s,
-                                const char **name);
+                                const char **name, int dc = 0);
 cudaError_t launch_batch_rebuild(const RebuildArgs &r, cudaStream_t s, const char **name);
 // Mixed form, scalar physics on straight-sided triangles: the cell kernel with the basis
 // contractions on the tensor cores (persistent over 128-cell tiles; batch: active tiles).
@@ -255,6 +290,11 @@ cudaError_t launch_cells_scalar_tc(const HostCellGroup &g, const CellArgs &a, bo
                                    int ntiles, cudaStream_t s, const char **name, bool *ok);
 cudaError_t launch_update(int nnodes, int neq, const double *dt, const double *res, double *u,
                           cudaStream_t s, const char **name);
+// Mixed form, scalar physics: FP32 correction-sweep cell kernels of the defect-correction loop;
+// grid > 0 launches the batch form (persistent over a.bt's active tiles of `tile` cells).
+bool dc_supported(const HostCellGroup &g);
+cudaError_t launch_cells_scalar_dc(const HostCellGroup &g, const DcCellArgs &a, int grid,
+                                   int tile, cudaStream_t s, const char **name, bool *ok);
 // PGLDA / PGN element Jacobians (rds_jacobian.cu): jac [ncells][ndof*neq][ndof*neq]
 cudaError_t launch_jacobians(const HostCellGroup &g, const CellArgs &a, int physics, int scheme,
                              int dim, int neq, double *jac, cudaStream_t s);
