@@ -60,6 +60,7 @@
 #include "physics/scalar/RotationAdvection2D.hpp"
 #include "solver/art_visc/ArtificialViscosity.hpp"
 #include "solver/rdm/PGRDMethodExplicit.hpp"
+#include "solver/rdm/assembly/PGRDMPicardJacCellAssemblyWorker.hpp"
 #include "solver/rdm/blending_coeff/RDBlendingCoeff.hpp"
 #include "solver/rdm/cellsplitters/CellSplitters.hpp"
 #include "solver/time/ExplicitTimeStepper.hpp"
@@ -579,6 +580,38 @@ int run(const Args &a)
   out.put("u0", u0, {nsol, NEQ});
   for (const auto &sa : stab_arrays)
     out.put(sa.first, sa.second, {Uint(sa.second.size())});
+
+  // ---- (RDS_HARNESS_JACOBIAN set) the reference's Picard-linearised implicit assembly at u0:
+  // its cell worker (solver/rdm/assembly/PGRDMPicardJacCellAssemblyWorker.hpp:120-490) computes
+  // every cell's residual and element Jacobian with the scheme's compute_adv_res_and_jacobian
+  // (PGLDA.hpp:316-536, PGN.hpp:296, PGB.hpp:503-819) and adds J(m, n) / V(m) to the system
+  // matrix and -res(m) / V(m) to the right-hand side; the recording classes of
+  // oracle/shim_jac/linear_system/TpetraFwd.hpp keep the summed entries. No Dirichlet rows.
+  if (std::getenv("RDS_HARNESS_JACOBIAN"))
+  {
+    rdm::RDTimeUpdate tu;
+    tu.setup(*mesh, *sol);
+    rdm::detail::PGRDMPicardJacCellAssemblyWorker<MC, Phys, Scheme> worker(0);
+    worker.configure_cell_spaces(*mesh, *sol, 0, ncells - 1, 100, SFunc::Lagrange,
+                                 PointSetID::Gauss, a.quad);
+    const std::vector<bool> no_dirichlet(nsol * NEQ, false);
+    ls::TpetraCrsMatrix<Real> mat;
+    ls::TpetraMultiVector<Real> rhs;
+    rhs.values.assign(nsol * NEQ, 0.0);
+    worker.assemble_mat_and_rhs_part(*mesh, *sol, *u, tu, no_dirichlet, mat, rhs);
+    std::vector<int> jrow, jcol;
+    std::vector<Real> jval;
+    for (const auto &e : mat.entries)
+    {
+      jrow.push_back(int(e.first.first));
+      jcol.push_back(int(e.first.second));
+      jval.push_back(e.second);
+    }
+    out.put("jac_row", jrow, {Uint(jrow.size())});
+    out.put("jac_col", jcol, {Uint(jcol.size())});
+    out.put("jac_val", jval, {Uint(jval.size())});
+    out.put("jac_rhs", rhs.values, {nsol, NEQ});
+  }
 
   // first iteration: residual, wave speed, dt, dual volume at u0
   solver->assemble_lhs_and_rhs(a.cfl);

@@ -6,7 +6,9 @@ compiled in place by oracle/Makefile) and keeps what the harness dumps: the refe
 connectivity, reference-element tables, boundary facets, initial state, and its outputs after
 one assemble_lhs_and_rhs (residual, wave speed, dt, dual volume), after one solve, after
 `iters` iterations (state and residual norms), and after two steps of its RK3TVD stepper (state,
-first-stage residual and dt, norms).
+first-stage residual and dt, norms). The cases in JACOBIAN_CASES also hold the reference's
+Picard-linearised implicit assembly at u0 (jac_row / jac_col / jac_val: the summed J(m, n) / V(m)
+entries of its PGRDMPicardJacCellAssemblyWorker; jac_rhs: -res / V).
 
 Needs the reference tree (it runs only where the reference is mounted):
     make -C oracle && python tests/golden/make_golden.py
@@ -123,6 +125,12 @@ CASES = {
 }
 
 
+# cases that also dump the reference's assembled element Jacobians (RDS_HARNESS_JACOBIAN)
+JACOBIAN_CASES = {"burgers_p2_lda", "burgers_p2_n", "burgers_p2_b", "burgers_p3_b", "adv_p2_b",
+                  "euler2d_tri_p1_lda", "euler2d_tri_p2_n", "euler2d_tri_p3_b",
+                  "euler2d_quad_p3_b", "euler3d_tet_p2_lda"}
+
+
 def make(name, spec):
     physics, scheme, p, quad, n, jit, seed, init, bcs, cfl, iters = spec[:11]
     stab = spec[11] if len(spec) > 11 else "none"
@@ -145,8 +153,14 @@ def make(name, spec):
         meshgen.write_gmsh22(msh, meshgen.unit_square_tri(n, jit, seed=seed))
     cmd = [HARNESS, "dump", physics, scheme, str(p), str(quad), msh, out, str(iters), str(cfl),
            init, bcs, "1"]
+    env = dict(os.environ)
+    env.pop("RDS_HARNESS_NO_RK3", None)
+    if name in JACOBIAN_CASES:
+        env["RDS_HARNESS_JACOBIAN"] = "1"
+    else:
+        env.pop("RDS_HARNESS_JACOBIAN", None)
     if not stab.startswith("av3d:"):
-        subprocess.run(cmd + [stab], check=True, stdout=subprocess.DEVNULL)
+        subprocess.run(cmd + [stab], check=True, stdout=subprocess.DEVNULL, env=env)
         return
     # two passes: the reference's cellwise viscosity, then the solver with the nodal field
     import json

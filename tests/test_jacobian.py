@@ -83,3 +83,28 @@ def test_pgb_jacobian_reproduces_the_pgb_residual(case):
             un = u[g.sol_conn[c]]
             scale = max(np.abs(res).max(), np.abs(jac).max() * np.abs(un).max(), 1e-300)
             assert np.abs(jac @ un - res[:, 0]).max() <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("case", ["burgers_p2_lda", "burgers_p2_n", "burgers_p2_b",
+                                  "burgers_p3_b", "adv_p2_b", "euler2d_tri_p1_lda",
+                                  "euler2d_tri_p2_n", "euler2d_tri_p3_b", "euler2d_quad_p3_b",
+                                  "euler3d_tet_p2_lda"])
+def test_element_jacobians_assemble_to_the_reference(case):
+    """The oracle's element Jacobians (PGLDA / PGN / PGB), assembled as J(m, n) / V(m), against
+    the reference's own Picard-Jacobian cell worker (PGRDMPicardJacCellAssemblyWorker with
+    compute_adv_res_and_jacobian, PGLDA.hpp:316-536, PGN.hpp:296, PGB.hpp:503-819) dumped with
+    the golden case at u0."""
+    prob, a, _ = load_golden(os.path.join(GOLDEN, case))
+    o = Oracle(prob)
+    n, neq = prob.nnodes, prob.neq
+    ref = np.zeros((n * neq, n * neq))
+    ref[a["jac_row"], a["jac_col"]] = a["jac_val"]
+    got = np.zeros_like(ref)
+    u = np.asarray(a["u0"])
+    for gi, g in enumerate(prob.groups):
+        for c in range(g.ncells):
+            jac = o.element_jacobian(gi, c, u)
+            d = g.sol_conn[c]
+            rows = (d[:, None] * neq + np.arange(neq)[None, :]).ravel()
+            got[np.ix_(rows, rows)] += jac / np.repeat(o.vol[d], neq)[:, None]
+    assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
