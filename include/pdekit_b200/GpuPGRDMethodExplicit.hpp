@@ -22,8 +22,9 @@
  * Scope: physics Burgers2D, Euler2DCons, Euler3DCons and RotationAdvection2D with a constant
  * direction; schemes PGLDA, PGN, PGB; boundary conditions WeakDirichlet (expression of the
  * coordinates, evaluated once at the facet quadrature points), WeakWall, WeakSubInlet,
- * WeakSubOutlet, WeakFarfield (Euler; set_reference_state) and StrongDirichlet (expression at
- * the facet dofs' coordinates). Anything else throws std::runtime_error at set-up.
+ * WeakSubOutlet, WeakFarfield (Euler; set_reference_state), WeakSuperInlet, WeakSymmetry
+ * (Euler) and StrongDirichlet (expression at the facet dofs' coordinates). Anything else throws
+ * std::runtime_error at set-up.
  *
  * Host fields stay the source of truth between calls: assemble_lhs_and_rhs uploads the
  * solution function, and downloads the residual and time-step functions; solve() downloads
@@ -312,7 +313,8 @@ class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>, public Devic
   {
     if (bc_type_name != "WeakDirichlet" && bc_type_name != "WeakWall" &&
         bc_type_name != "WeakSubInlet" && bc_type_name != "WeakSubOutlet" &&
-        bc_type_name != "WeakFarfield" && bc_type_name != "StrongDirichlet")
+        bc_type_name != "WeakFarfield" && bc_type_name != "StrongDirichlet" &&
+        bc_type_name != "WeakSuperInlet" && bc_type_name != "WeakSymmetry")
       throw std::runtime_error("GpuPGRDMethodExplicit: boundary condition '" + bc_type_name +
                                "' not supported on the GPU");
     auto bc             = std::make_shared<bc_type>(bc_type_name, condition_name, boundary_name);
@@ -684,6 +686,10 @@ class GpuPGRDMethodExplicit : public RDMethod<MeshConfig, Physics>, public Devic
     }
     else if (bc.type() == "WeakWall")
       b.kind = RDS_BC_WEAK_WALL;
+    else if (bc.type() == "WeakSuperInlet")
+      b.kind = RDS_BC_WEAK_SUPER_INLET;
+    else if (bc.type() == "WeakSymmetry")
+      b.kind = RDS_BC_WEAK_SYMMETRY;
     else if (bc.type() == "WeakSubInlet")
     {
       b.kind      = RDS_BC_WEAK_SUB_INLET;

@@ -101,7 +101,11 @@ typedef enum
                                * read besides. Applied in condition order after the cells (the
                                * conditions added after it see the new state); the update then
                                * moves these dofs by -dt res like every other dof. Not in
-                               * batched contexts. */
+                               * batched contexts. */,
+  RDS_BC_WEAK_SUPER_INLET = 6, /* bc/WeakSuperInlet.hpp:62-160 (Euler): no residual, only the
+                                * facet's wave speed (max eigenvalue magnitude on the facet) */
+  RDS_BC_WEAK_SYMMETRY    = 7  /* bc/WeakSymmetry.hpp:100-190 (Euler): K-(n) (u_mirror - u), the
+                                * mirror state with the momentum reflected about the facet */
 } rds_bc_kind;
 
 typedef struct

@@ -821,8 +821,9 @@ static void euler_flux_normal(const rdso_model *m, const props_t *p, const doubl
 }
 
 /* Weak boundary-facet residuals: WeakDirichlet (WeakDirichletBC.hpp:159-265), WeakWall,
- * WeakSubInlet, WeakSubOutlet, WeakFarfield, plus the rescaling to the facet total (WeakBC.hpp:786-832) and
- * the nodal accumulation (WeakBC.hpp:315-352). */
+ * WeakSubInlet, WeakSubOutlet, WeakFarfield, WeakSuperInlet (WeakSuperInlet.hpp:62-160: no
+ * residual, only the wave speed), WeakSymmetry (WeakSymmetry.hpp:100-190), plus the rescaling to
+ * the facet total (WeakBC.hpp:786-832) and the nodal accumulation (WeakBC.hpp:315-352). */
 static int apply_weak_bc(const rdso_model *m, const rdso_bc *b, const double *geo_coords,
                          const double *vol, const double *u, double *res, double *ws)
 {
@@ -914,7 +915,12 @@ static int apply_weak_bc(const rdso_model *m, const rdso_bc *b, const double *ge
         coeff[n] = coeff[n] > eig_max ? coeff[n] : eig_max;
 
       double relax = 1.0;
-      if (b->kind == RDSO_BC_WEAK_WALL)
+      if (b->kind == RDSO_BC_WEAK_SUPER_INLET)
+      {
+        for (int e = 0; e < NEQ; ++e)
+          gflux[e] = 0.0;
+      }
+      else if (b->kind == RDSO_BC_WEAK_WALL)
       {
         /* WeakWall.hpp:93-250 (active branch): mirror state with the normal velocity removed,
          * same density and pressure; residual = relax V w (F(u_ghost).n - F(u).n), relax = 1
@@ -952,6 +958,17 @@ static int apply_weak_bc(const rdso_model *m, const rdso_bc *b, const double *ge
           /* WeakFarfield.hpp:125-240 (active branch): the reference state, K-(n) (u_ref - u) */
           for (int e = 0; e < NEQ; ++e)
             ghost[e] = b->gq[e];
+        }
+        else if (b->kind == RDSO_BC_WEAK_SYMMETRY)
+        {
+          /* WeakSymmetry.hpp:120-160: density and energy kept, momentum rho (V - 2 (V.n) n) */
+          double vn = 0.0;
+          for (int d = 0; d < D; ++d)
+            vn += nrm[d] * p.V[d];
+          ghost[0]       = uqf[0];
+          ghost[NEQ - 1] = uqf[NEQ - 1];
+          for (int d = 0; d < D; ++d)
+            ghost[d + 1] = uqf[0] * (p.V[d] - 2. * vn * nrm[d]);
         }
         else if (b->kind == RDSO_BC_WEAK_SUB_INLET)
         {

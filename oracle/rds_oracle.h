@@ -51,7 +51,9 @@ enum
   RDSO_BC_WEAK_SUB_INLET  = 2, /* bc/WeakSubInlet.hpp, params: total temperature, pressure */
   RDSO_BC_WEAK_SUB_OUTLET = 3, /* bc/WeakSubOutlet.hpp, params: outlet pressure */
   RDSO_BC_WEAK_FARFIELD   = 4, /* bc/WeakFarfield.hpp, gq: [neq] reference state */
-  RDSO_BC_STRONG_DIRICHLET = 5 /* bc/StrongDirichletBC.hpp, gq: [nfacets][nfdof][neq] values */
+  RDSO_BC_STRONG_DIRICHLET = 5, /* bc/StrongDirichletBC.hpp, gq: [nfacets][nfdof][neq] values */
+  RDSO_BC_WEAK_SUPER_INLET = 6, /* bc/WeakSuperInlet.hpp: wave speed only */
+  RDSO_BC_WEAK_SYMMETRY    = 7  /* bc/WeakSymmetry.hpp: mirrored momentum */
 };
 
 typedef struct

@@ -20,7 +20,8 @@ HARNESS_PATH = os.path.join(_HERE, "_ref", "rds_ref_harness")
 PHYSICS = {"advconst": 0, "burgers": 1, "euler2d": 2, "euler3d": 3}
 SCHEME = {"lda": 0, "n": 1, "b": 2}
 BC_KIND = {"WeakDirichlet": 0, "WeakWall": 1, "WeakSubInlet": 2, "WeakSubOutlet": 3,
-           "WeakFarfield": 4, "StrongDirichlet": 5}
+           "WeakFarfield": 4, "StrongDirichlet": 5,
+           "WeakSuperInlet": 6, "WeakSymmetry": 7}
 
 
 class _Model(C.Structure):

@@ -140,7 +140,7 @@ struct rds_ctx
   // contribution since then (d_c32, one value per slot), the cells' with the blending
   // coefficients of PGB frozen at d_ur (d_dc_theta, one per cell)
   bool dc_ok         = false;
-  int dc_m           = 8;
+  int dc_m           = 16;
   int dc_phase       = 0; // launch_residual_kernels: 0 plain, 1 exact DC sweep, 2 correction
   double *d_ur = nullptr, *d_dres = nullptr, *d_dc_theta = nullptr;
   float *d_c32 = nullptr, *d_dtv = nullptr;
@@ -702,7 +702,7 @@ rds_status rds_add_bc(rds_ctx *ctx, const rds_bc_group *b)
   const bool dirichlet = b->kind == RDS_BC_WEAK_DIRICHLET;
   const bool farfield  = b->kind == RDS_BC_WEAK_FARFIELD;
   const bool strong    = b->kind == RDS_BC_STRONG_DIRICHLET;
-  if (b->kind < RDS_BC_WEAK_DIRICHLET || b->kind > RDS_BC_STRONG_DIRICHLET || b->nfacets <= 0 ||
+  if (b->kind < RDS_BC_WEAK_DIRICHLET || b->kind > RDS_BC_WEAK_SYMMETRY || b->nfacets <= 0 ||
       b->nfdof <= 0 || b->nfdof > 16 || !b->sol_conn || ((dirichlet || farfield || strong) && !b->gq))
     return fail(ctx, RDS_ERR_INVALID, "invalid boundary group");
   if (!strong && (b->nfgeo <= 0 || b->nfgeo > 16 || b->nfq <= 0 || b->nfq > 32 || !b->geo_conn ||

@@ -14,6 +14,9 @@
 //     energy of the outlet pressure.
 //   WeakFarfield (bc/WeakFarfield.hpp:125-240, the active branch): K-(n) (u_ref - u_q) with the
 //     reference state u_ref, lambda floor 1e-8.
+//   WeakSuperInlet (bc/WeakSuperInlet.hpp:62-160): no residual; only the facet's wave speed.
+//   WeakSymmetry (bc/WeakSymmetry.hpp:100-190): K-(n) (u_mirror - u_q), u_mirror with the same
+//     density and energy and the momentum rho (V - 2 (V.n) n).
 // StrongDirichletBC::apply (bc/StrongDirichletBC.hpp:202-233) has its own kernel: the listed
 // dofs take their values (one thread per distinct dof, the value of the last facet naming it).
 // Facet normals are (dy/dxi, -dx/dxi)/|.| in 2D and the normalised cross product of the two
@@ -155,7 +158,13 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
       for (int e = 0; e < NEQ; ++e)
         eig_max = fmax(eig_max, fabs(lam[e]));
-      if constexpr (KIND == RDS_BC_WEAK_WALL)
+      if constexpr (KIND == RDS_BC_WEAK_SUPER_INLET)
+      {
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          gflux[e] = 0.0;
+      }
+      else if constexpr (KIND == RDS_BC_WEAK_WALL)
       {
         double Fn[NEQ], Fg[NEQ], ug[NEQ];
         euler_flux_n<double, D>(uq, p, nrm, Fn);
@@ -216,6 +225,18 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
           for (int e = 0; e < NEQ; ++e)
             ghost[e] = a.gq[e];
+        }
+        else if constexpr (KIND == RDS_BC_WEAK_SYMMETRY)
+        {
+          double vn = 0.0;
+#pragma unroll
+          for (int d = 0; d < D; ++d)
+            vn += nrm[d] * p.V[d];
+          ghost[0]       = uq[0];
+          ghost[NEQ - 1] = uq[NEQ - 1];
+#pragma unroll
+          for (int d = 0; d < D; ++d)
+            ghost[d + 1] = uq[0] * (p.V[d] - 2. * vn * nrm[d]);
         }
         else
         {
@@ -364,6 +385,14 @@ cudaError_t dispatch_kind(const HostBC &b, const BCArgs &a, cudaStream_t s, bool
     if constexpr (NEQ > 1)
       return dispatch_facets<RDS_BC_WEAK_FARFIELD, PHYS, D, NEQ>(b, a, s, ok);
     break;
+  case RDS_BC_WEAK_SUPER_INLET:
+    if constexpr (NEQ > 1)
+      return dispatch_facets<RDS_BC_WEAK_SUPER_INLET, PHYS, D, NEQ>(b, a, s, ok);
+    break;
+  case RDS_BC_WEAK_SYMMETRY:
+    if constexpr (NEQ > 1)
+      return dispatch_facets<RDS_BC_WEAK_SYMMETRY, PHYS, D, NEQ>(b, a, s, ok);
+    break;
   default:
     break;
   }
@@ -382,6 +411,10 @@ const char *bc_name(int kind)
     return "bc_weak_sub_outlet";
   case RDS_BC_WEAK_FARFIELD:
     return "bc_weak_farfield";
+  case RDS_BC_WEAK_SUPER_INLET:
+    return "bc_weak_super_inlet";
+  case RDS_BC_WEAK_SYMMETRY:
+    return "bc_weak_symmetry";
   case RDS_BC_STRONG_DIRICHLET:
     return "bc_strong_dirichlet";
   default:

@@ -57,6 +57,7 @@ class CellGroup:
 @dataclasses.dataclass
 class BCGroup:
     kind: str  # WeakDirichlet | WeakWall | WeakSubInlet | WeakSubOutlet | WeakFarfield |
+    # WeakSuperInlet | WeakSymmetry |
     # StrongDirichlet
     name: str
     sol_conn: np.ndarray  # [nfacets, nfdof] int32

@@ -32,7 +32,8 @@ SCHEME = {"lda": 0, "n": 1, "b": 2}
 PRECISION = {"fp64": 0, "mixed": 1}
 SHAPE = {"line": 2, "triag": 3, "quad": 4, "tetra": 10}
 BC_KIND = {"WeakDirichlet": 0, "WeakWall": 1, "WeakSubInlet": 2, "WeakSubOutlet": 3,
-           "WeakFarfield": 4, "StrongDirichlet": 5}
+           "WeakFarfield": 4, "StrongDirichlet": 5,
+           "WeakSuperInlet": 6, "WeakSymmetry": 7}
 
 STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "NONFINITE", 4: "NEG_PRESSURE", 5: "ITER_CAP",
           6: "UNSUPPORTED", 7: "TOO_LARGE"}

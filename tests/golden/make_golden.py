@@ -57,6 +57,14 @@ EULER3D_FAR_BCS = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakFarfield:farfield_
                    + ",WeakSubInlet:inlet_bc:inlet:total_temperature=307.6488978;"
                    "total_pressure=120195.4453,"
                    "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
+# WeakSymmetry (reflected momentum) and WeakSuperInlet (wave speed only) of the Euler registry
+EULER2D_SYM_BCS = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakSymmetry:symmetry_bc:top_wall:-,"
+                   "WeakSuperInlet:inlet_bc:inlet:-,"
+                   "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
+EULER3D_SYM_BCS = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakSymmetry:symmetry_top_bc:top_wall:-,"
+                   "WeakSymmetry:symmetry_side_bc:side_walls:-,"
+                   "WeakSubInlet:inlet_bc:inlet:total_temperature=307.6488978;"
+                   "total_pressure=120195.4453,WeakSuperInlet:outlet_bc:outlet:-")
 ADV_STRONG_BCS = "StrongDirichlet:inlet_bottom:bottom:sin2pix,WeakDirichlet:inlet_left:left:zero"
 BURG_STRONG_BCS = ("WeakDirichlet:inlet:bottom:burgers_inlet,StrongDirichlet:left:left:c1.5,"
                    "WeakDirichlet:right:right:c-0.5")
@@ -99,6 +107,10 @@ CASES = {
                                 EULER2D_FAR_BCS, 0.5, 3),
     "euler3d_tet_p2_farfield": ("euler3d", "lda", 2, 5, ("box_tet", 3, 2, 2), 0.1, 42, "bump3d",
                                 EULER3D_FAR_BCS, 0.5, 3),
+    "euler2d_tri_p2_symmetry": ("euler2d", "b", 2, 5, ("channel_tri", 4, 3), 0.15, 36, "bump2d",
+                                EULER2D_SYM_BCS, 0.5, 3),
+    "euler3d_tet_p2_symmetry": ("euler3d", "n", 2, 5, ("box_tet", 3, 2, 2), 0.1, 43, "bump3d",
+                                EULER3D_SYM_BCS, 0.5, 3),
     # stabilisation fields computed at u0 by the reference's own operators (a steep front, so
     # that the sensor is zero in some cells and on its ramp in others): nodal artificial
     # viscosity into PGLDA, nodal blending coefficients into PGB; optional 12th entry

@@ -36,6 +36,8 @@ E2D_FAR = ("WeakWall:bottom_wall_bc:bottom_wall:-,"
            "WeakSubInlet:inlet_bc:inlet:total_temperature=307.6488978;total_pressure=120195.4453,"
            "WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
 ADV_STRONG = "StrongDirichlet:inlet_bottom:bottom:sin2pix,WeakDirichlet:inlet_left:left:zero"
+E2D_SYM = ("WeakWall:bottom_wall_bc:bottom_wall:-,WeakSymmetry:symmetry_bc:top_wall:-,"
+           "WeakSuperInlet:inlet_bc:inlet:-,WeakSubOutlet:outlet_bc:outlet:total_pressure=101325.0")
 
 # (physics, scheme, p, quad order, mesh, init, conditions, CFL, iterations)
 CASES = {
@@ -45,6 +47,8 @@ CASES = {
     "adv_p1_n_strong": ("advconst", "n", 1, 4, ("square", 8, 0.2, 6), "smooth", ADV_STRONG, 0.9,
                         10),
     "euler2d_tri_p2_farfield": ("euler2d", "n", 2, 5, ("channel", 4, 0, 3, 7), "bump2d", E2D_FAR,
+                                0.5, 5),
+    "euler2d_tri_p2_symmetry": ("euler2d", "b", 2, 5, ("channel", 4, 0, 3, 9), "bump2d", E2D_SYM,
                                 0.5, 5),
     "adv_p2_b": ("advconst", "b", 2, 5, ("square", 6, 0.2, 2), "smooth", ADV, 0.9, 10),
     "burgers_p2_b": ("burgers", "b", 2, 5, ("square", 6, 0.15, 3), "burgers", BURG, 0.5, 10),
