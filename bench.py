@@ -75,6 +75,8 @@ def parse():
                     help="c5: also time every problem alone through the plain FP64 path")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-drop", action="store_true", help="skip the time-to-drop runs")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="c2: skip the compact records of configurations 1, 3, 4 and 5")
     ap.add_argument("--drop-max-iter", type=int, default=400000)
     ap.add_argument("--quick", action="store_true",
                     help="only warm-up + timed steps (profiling runs): no e2e, mixed, drop, CPU")
@@ -193,6 +195,31 @@ def euler_flops(dim, neq, ndof, nq, nfl, ngeo, scheme):
     if scheme != "lda":
         per_q += ndof * (2 * neq * neq + 3 * neq)
     return f + nq * per_q
+
+
+def dc_flops(physics, scheme, ndof, nq, nfl):
+    """FP32 correction-sweep kernel of the mixed form's defect-correction loop
+    (rds_cells_scalar_dc.cu), per straight-sided triangle:
+      geometry    28
+      flux nodes  nfl x (2 ndof - 1 + 6 + (2 (ndof - 1) + 4 for Burgers, 2 for advection))
+                                                  change of the state and flux, contracted
+      points      nq (4 nfl - 1)                  change of the flux divergence
+                  + nq (1 + 6 + 3 ndof + ndof + 1 + 2 ndof)    w detJ, A, B, k_n, sum K+, e,
+                                                               the K+_n e c accumulation
+                  + nq (2 (ndof - 1) + 1) for Burgers           u_q of the reference state
+                  + nq (1) for LDA, nq (2 (ndof - 1) + 3 + 2 ndof) + 3 ndof for N / B
+    Configuration-2 mesh with the N scheme (ndof 6, nq 7, nfl 10): 1,189 flop."""
+    fl = 28
+    per_f = 2 * ndof - 1 + 6 + (2 * (ndof - 1) + 4 if physics == "burgers" else 2)
+    fl += nfl * per_f + nq * (4 * nfl - 1)
+    per_q = 1 + 6 + 3 * ndof + ndof + 1 + 2 * ndof
+    if physics == "burgers":
+        per_q += 2 * (ndof - 1) + 1
+    per_q += 1 if scheme == "lda" else 2 * (ndof - 1) + 3 + 2 * ndof
+    fl += nq * per_q
+    if scheme != "lda":
+        fl += 3 * ndof
+    return fl
 
 
 def cell_bytes(dim, neq, ndof, ngeo):
@@ -385,7 +412,9 @@ def _drop_run(prob, u0, precision, cfl, max_iter, drop=1e-10):
     s = PGRDMethodExplicit(prob.physics, prob.scheme, precision).configure_mesh_data(prob)
     s.initialize_work_data()
     s.set_solution(u0)
-    s.iterate(0.1, 3, 0.0)  # builds and uploads the loop graphs outside the timed region
+    # the history buffer for max_iter rows and the loop graphs are made outside the timed
+    # region (a drop of 1 stops at the first exact sweep)
+    s.iterate(cfl, max_iter, 1.0, raise_on_cap=False)
     s.set_solution(u0)
     torch.cuda.synchronize()
     t0 = time.time()
@@ -428,9 +457,134 @@ def time_to_drop(args, c2_pgb):
                      "speedup_mixed_vs_fp64": round(r64["seconds"] / rmx["seconds"], 3)}
     if c2_pgb is not None:
         prob, u0 = c2_pgb
-        r, _ = _drop_run(prob, u0, "fp64", 0.5, 4000)
-        out["configuration 2 (blended B), capped at 4000 iterations"] = {"fp64": r}
+        r, u64 = _drop_run(prob, u0, "fp64", 0.5, 4000)
+        rm, um = _drop_run(prob, u0, "mixed", 0.5, 4000)
+        rm["state_rel_l2_vs_fp64"] = float(np.linalg.norm(um - u64) / np.linalg.norm(u64))
+        out["configuration 2 (blended B), capped at 4000 iterations"] = {"fp64": r, "mixed": rm}
     return out
+
+
+def loop_rates(prob, u0, cfl, sweeps, world):
+    """Sweep rate of the FP64 loop and of the mixed form's loop over the same number of sweeps
+    through rds_iterate (one CUDA graph per chunk, no stop test), CUDA events on each solver's
+    stream. Scalar physics: the defect-correction loop (an exact FP64 sweep every m sweeps,
+    FP32 correction sweeps between); Euler: the FP32 cell kernels. Also the per-kernel device
+    times of two cycles of the mixed loop (event timing, separate pass)."""
+    import torch
+
+    from pdekit_b200.rds import PGRDMethodExplicit
+
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = PGRDMethodExplicit(prob.physics, prob.scheme, prec).configure_mesh_data(prob)
+        s.initialize_work_data()
+        s.set_solution(u0)
+        s.iterate(cfl, 64, 0.0)  # graph capture
+        s.set_solution(u0)
+        st = torch.cuda.ExternalStream(s.stream_handle())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        s.iterate(cfl, sweeps, 0.0)
+        e1.record(st)
+        e1.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
+        out[prec] = {"value": prob.ncells * sweeps * world / (ms * 1e-3),
+                     "ms_per_sweep": ms / sweeps}
+        if prec == "mixed":
+            s.set_solution(u0)
+            s.kernel_timing(True)
+            s.iterate(cfl, 33, 0.0)
+            out["mixed_kernels_ms_per_launch"] = {k: round(v[0] / v[1], 5)
+                                                  for k, v in s.kernel_times().items()}
+            s.kernel_timing(False)
+        s.close()
+    return out
+
+
+def dc_roofline(prob, kernels):
+    """Roofline of the mixed loop's FP32 correction-sweep cell kernel (scalar physics): its
+    algorithmic flop per launch (dc_flops) over its event-timed duration, against the FP32 FMA
+    peak measured on this GPU."""
+    from pdekit_b200.rds import measure_peak
+
+    dc = {k: v for k, v in kernels.items() if k.startswith("cells_") and k.endswith("_dc")}
+    if not dc or prob.physics not in ("advconst", "burgers"):
+        return None
+    ms = sum(dc.values())
+    flop = sum(dc_flops(prob.physics, prob.scheme, g.ndof, g.nq, g.nfl) * g.ncells
+               for g in prob.groups)
+    peak32 = measure_peak("mixed")
+    achieved = flop / (ms * 1e-3) / 1e12
+    return {"bound": "fp32", "kernel": max(dc, key=dc.get), "achieved": round(achieved, 3),
+            "peak": round(peak32, 3), "unit": "TFLOP/s", "frac": round(achieved / peak32, 4),
+            "peak_source": "measured in this run: rds_measure_peak (FP32 FMA micro-kernel)",
+            "flop_per_launch": flop}
+
+
+def compact_config(name, args, world):
+    """One more configuration in fewer steps than the headline run: value (FP64, L2 flushed
+    before every step, CUDA events), e2e (pipelined host-buffer steps), the FP64 and mixed loop
+    rates, the roofline of the dominant kernel and the reference's CPU path on its sample."""
+    import torch
+
+    from pdekit_b200.rds import PGRDMethodExplicit, measure_peak
+
+    prob, u0, cfl, desc, _, cpu_spec = workload(name, args)
+    steps = {"c1": 2000, "c3": 20, "c4": 20}[name]
+    s = PGRDMethodExplicit(prob.physics, prob.scheme, "fp64").configure_mesh_data(prob)
+    s.initialize_work_data()
+    s.set_solution(u0)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+    s.run(cfl, 3)
+    s.set_solution(u0)
+    ms = max_over_ranks(time_steps(s, steps, flush, cfl), world)
+    s.set_solution(u0)
+    s.kernel_timing(True)
+    nt = min(20, steps)
+    s.run(cfl, nt)
+    kt = s.kernel_times()
+    s.kernel_timing(False)
+    cells = {k: v for k, v in kt.items() if k.startswith("cells_")}
+    cell_ms = sum(v[0] for v in cells.values()) / nt
+    flop, byts = group_work(prob)
+    roof = roofline(max(cells, key=lambda k: cells[k][0]), cell_ms, flop, byts,
+                    measure_peak("fp64"), hbm_peak())
+    if name in PROFILED_TRAFFIC:
+        roof["traffic"], roof["traffic_source"] = PROFILED_TRAFFIC[name]
+    # e2e: host buffers every step, pipelined (rds_step_host), host clock
+    u_host = torch.from_numpy(np.ascontiguousarray(u0)).pin_memory()
+    outs = [torch.empty_like(u_host).pin_memory() for _ in range(2)]
+    nrms = [torch.empty(prob.neq, dtype=torch.float64).pin_memory() for _ in range(2)]
+    ke = {"c1": 500, "c3": 10, "c4": 10}[name]
+    s.step_host(u_host.numpy(), outs[0].numpy(), cfl, nrms[0].numpy())
+    s.step_sync()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(ke):
+        s.step_host(u_host.numpy(), outs[i % 2].numpy(), cfl, nrms[i % 2].numpy())
+    s.step_sync()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3, world)
+    s.close()
+    rates = loop_rates(prob, u0, cfl, {"c1": 4096, "c3": 64, "c4": 64}[name], world)
+    rec = {"workload": desc, "cells": prob.ncells, "nodes": prob.nnodes, "steps": steps,
+           "value": prob.ncells * steps * world / (ms * 1e-3), "ms_per_step": ms / steps,
+           "e2e": {"value": prob.ncells * ke * world / (e2e_ms * 1e-3), "steps": ke,
+                   "h2d_bytes_per_step": int(u_host.numel() * 8),
+                   "d2h_bytes_per_step": int(u_host.numel() * 8 + 8 * prob.neq)},
+           "loop_fp64": rates["fp64"], "mixed": rates["mixed"],
+           "mixed_kernels_ms_per_launch": rates["mixed_kernels_ms_per_launch"],
+           "roofline": roof, "mixed_roofline": dc_roofline(prob, rates["mixed_kernels_ms_per_launch"])}
+    if not args.no_cpu:
+        threads = os.cpu_count() or 1
+        with tempfile.TemporaryDirectory() as td:
+            r = cpu_reference(prob, cpu_spec, threads, td)
+        if r:
+            rec["cpu_baseline"] = {"value": r["cell_updates_per_s"], "cores": threads,
+                                   "kind": "reference",
+                                   "sample": f"{r['iters']} iterations of {cpu_spec['sample']} "
+                                             f"({r['cells']} cells), nb_threads={threads}"}
+    return rec
 
 
 def run_ours(args, rank, world, local):
@@ -539,17 +693,8 @@ def run_ours(args, rank, world, local):
            "synchronous_api": "rds_set_state + rds_assemble + rds_update + rds_residual_norm + "
                               "rds_get_state per step, CUDA events"}
 
-    # mixed precision form
-    mixed = PGRDMethodExplicit(prob.physics, prob.scheme, "mixed").configure_mesh_data(prob)
-    mixed.initialize_work_data()
-    if args.tensor_cores:
-        mixed.set_option("tensor_cores", 1)
-    mixed.set_solution(u0)
-    mixed.run(cfl, max(args.warmup, 3))
-    mixed.set_solution(u0)
-    ms_mixed = max_over_ranks(time_steps(mixed, steps, flush, cfl), world)
-    mixed_value = ncells * steps * world / (ms_mixed * 1e-3)
-    mixed.close()
+    # mixed precision form: the defect-correction loop's sweep rate beside the FP64 loop's
+    rates = loop_rates(prob, u0, cfl, min(steps, 4096), world)
 
     # third-order TVD Runge-Kutta steps (three residual passes each, one graph launch)
     solver.set_solution(u0)
@@ -597,8 +742,14 @@ def run_ours(args, rank, world, local):
                    "l2": "flushed (256 MB write) before every timed step",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "e2e": e2e,
-        "mixed": {"value": mixed_value, "ms_per_step": ms_mixed / steps,
-                  "dtype": "f32 interpolation/flux/upwind, f64 accumulation/inverse/norms"},
+        "mixed": dict(rates["mixed"], loop_fp64=rates["fp64"],
+                      speedup_per_sweep_vs_fp64_loop=round(rates["mixed"]["value"] /
+                                                           rates["fp64"]["value"], 3),
+                      form="defect correction: an exact FP64 sweep every 16 sweeps, FP32 "
+                           "correction sweeps between (the cell and facet changes computed from "
+                           "the correction itself); rds_iterate, no stop test, CUDA events",
+                      kernels_ms_per_launch=rates["mixed_kernels_ms_per_launch"],
+                      roofline=dc_roofline(prob, rates["mixed_kernels_ms_per_launch"])),
         "rk3tvd": rk3,
         "time_to_drop_1e-10": drop,
         "roofline": roof,
@@ -611,6 +762,13 @@ def run_ours(args, rank, world, local):
     if stab:
         line["stabilised"] = stab
     solver.close()
+    if args.workload == "c2" and world == 1 and not args.no_configs:
+        # the other configurations, compact (the driver records this one line)
+        line["configs"] = {k: compact_config(k, args, world) for k in ("c1", "c3", "c4")}
+        c5 = run_batched(args, rank, world, local)
+        line["configs"]["c5"] = {"workload": c5["config"]["workload"], "cells": c5["config"]["cells"],
+                                 "value": c5["value"], "gpu_launches": c5["gpu_launches"],
+                                 "time_to_drop_1e-10": c5["time_to_drop_1e-10"]}
     return line
 
 
@@ -759,6 +917,7 @@ def run_batched(args, rank, world, local):
         b.close()
     rel_l2 = max_over_ranks(max(float(np.linalg.norm(a - c) / np.linalg.norm(a))
                                 for a, c in zip(res["fp64_states"], res["mixed_states"])), world)
+    res["speedup_mixed_vs_fp64"] = round(res["fp64"]["seconds"] / res["mixed"]["seconds"], 3)
     del res["fp64_states"], res["mixed_states"]
     seq = None
     if args.c5_sequential and world == 1:
@@ -799,6 +958,7 @@ def run_batched(args, rank, world, local):
                 "note": "the timed region of value already copies every problem's state in from "
                         "pinned host memory and back out"},
         "time_to_drop_1e-10": {"batched_fp64": res["fp64"], "batched_mixed": res["mixed"],
+                               "speedup_mixed_vs_fp64": res["speedup_mixed_vs_fp64"],
                                "mixed_vs_fp64_converged_rel_l2_max": rel_l2,
                                "sequential_plain_fp64": seq},
         "roofline": {"bound": "fp64", "peak": round(peak64, 3), "unit": "TFLOP/s",
@@ -822,7 +982,7 @@ def run_reference(args, rank, world):
     threads = os.cpu_count() or 1
     spec = dict(spec)
     if args.workload == "c2":
-        spec["iters"] = max(1, (args.steps or 500) // 50)
+        spec["iters"] = max(5, (args.steps or 500) // 50)
     with tempfile.TemporaryDirectory() as td:
         t0 = time.time()
         r = cpu_reference(prob, spec, threads, td)

@@ -51,7 +51,9 @@ __device__ __forceinline__ double group_max(double v)
 }
 
 // Solve A x = b for two right-hand sides (LU with row partial pivoting, FP64).
-template <int N>
+// TWO = false: b2 is left alone (PGLDA needs only the first right-hand side; the first is
+// computed with the same operations either way).
+template <int N, bool TWO = true>
 __device__ __forceinline__ void lu_solve2(double A[N][N], double b1[N], double b2[N])
 {
 #pragma unroll
@@ -90,9 +92,12 @@ __device__ __forceinline__ void lu_solve2(double A[N][N], double b1[N], double b
           double t = b1[k];
           b1[k]    = b1[i];
           b1[i]    = t;
-          t        = b2[k];
-          b2[k]    = b2[i];
-          b2[i]    = t;
+          if (TWO)
+          {
+            t     = b2[k];
+            b2[k] = b2[i];
+            b2[i] = t;
+          }
         }
     }
     const double inv = 1.0 / A[k][k];
@@ -105,7 +110,8 @@ __device__ __forceinline__ void lu_solve2(double A[N][N], double b1[N], double b
       for (int j = k + 1; j < N; ++j)
         A[i][j] -= f * A[k][j];
       b1[i] -= f * b1[k];
-      b2[i] -= f * b2[k];
+      if (TWO)
+        b2[i] -= f * b2[k];
     }
   }
 #pragma unroll
@@ -115,10 +121,12 @@ __device__ __forceinline__ void lu_solve2(double A[N][N], double b1[N], double b
     for (int j = i + 1; j < N; ++j)
     {
       b1[i] -= A[i][j] * b1[j];
-      b2[i] -= A[i][j] * b2[j];
+      if (TWO)
+        b2[i] -= A[i][j] * b2[j];
     }
     b1[i] *= rdiag[i];
-    b2[i] *= rdiag[i];
+    if (TWO)
+      b2[i] *= rdiag[i];
   }
 }
 
@@ -126,6 +134,7 @@ __device__ __forceinline__ void lu_solve2(double A[N][N], double b1[N], double b
 // 2 x 2 minors of rows (0, 1) and of rows (2, 3) (Laplace expansion by complementary minors).
 // The reference inverts these matrices by a closed-form adjugate too
 // (src/math/unary_ops/matrix_unary_ops/MatrixInverse.hpp:187-290).
+template <bool TWO = true>
 __device__ __forceinline__ void adj_solve4(const double A[4][4], double b1[4], double b2[4])
 {
   const double s0 = A[0][0] * A[1][1] - A[1][0] * A[0][1];
@@ -156,13 +165,15 @@ __device__ __forceinline__ void adj_solve4(const double A[4][4], double b1[4], d
   for (int i = 0; i < 4; ++i)
   {
     x1[i] = (B[i][0] * b1[0] + B[i][1] * b1[1] + B[i][2] * b1[2] + B[i][3] * b1[3]) * id;
-    x2[i] = (B[i][0] * b2[0] + B[i][1] * b2[1] + B[i][2] * b2[2] + B[i][3] * b2[3]) * id;
+    if (TWO)
+      x2[i] = (B[i][0] * b2[0] + B[i][1] * b2[1] + B[i][2] * b2[2] + B[i][3] * b2[3]) * id;
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i)
   {
     b1[i] = x1[i];
-    b2[i] = x2[i];
+    if (TWO)
+      b2[i] = x2[i];
   }
 }
 
@@ -457,9 +468,11 @@ __global__ void __launch_bounds__(NT)
           {
             Kn[i * NEQ + j] = K[i][j];
             SK[i][j] += double(K[i][j]);
-            ku += double(K[i][j]) * su[n * NEQ + j];
+            if (SCHEME != RDS_PGLDA) // sum K+ u feeds only the N dissipation
+              ku += double(K[i][j]) * su[n * NEQ + j];
           }
-          SKu[i] += ku;
+          if (SCHEME != RDS_PGLDA)
+            SKu[i] += ku;
         }
       }
     }
@@ -467,7 +480,8 @@ __global__ void __launch_bounds__(NT)
 #pragma unroll
     for (int i = 0; i < NEQ; ++i)
     {
-      SKu[i] = group_sum<G>(SKu[i]);
+      if (SCHEME != RDS_PGLDA)
+        SKu[i] = group_sum<G>(SKu[i]);
 #pragma unroll
       for (int j = 0; j < NEQ; ++j)
         SK[i][j] = group_sum<G>(SK[i][j]);
@@ -481,9 +495,9 @@ __global__ void __launch_bounds__(NT)
     }
     phi0 += wj * v[0];
     if constexpr (NEQ == 4)
-      adj_solve4(SK, v, ub);
+      adj_solve4<SCHEME != RDS_PGLDA>(SK, v, ub);
     else
-      lu_solve2<NEQ>(SK, v, ub);
+      lu_solve2<NEQ, SCHEME != RDS_PGLDA>(SK, v, ub);
 
 #pragma unroll
     for (int s = 0; s < NPT; ++s)
