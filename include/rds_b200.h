@@ -316,7 +316,13 @@ RDS_API rds_status rds_get_fields(rds_ctx *ctx, double *res_aos, double *dt, dou
 RDS_API rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int *it_done,
                        double *hist);
 
-/* Options: "mixed_switch" (default 1e-6): with RDS_MIXED, rds_iterate runs FP32 cell kernels
+/* Options: "mixed_refresh" (default 32): with RDS_MIXED and scalar physics, rds_iterate and
+ * rds_iterate_batch run the defect-correction loop: an exact FP64 sweep every mixed_refresh
+ * sweeps, FP32 correction sweeps between (the change of every contribution computed from the
+ * correction itself, the coefficients of the exact sweep's state); the loop stops only at an
+ * exact sweep and converges to the FP64 scheme's fixed point.
+ * "mixed_switch" (default 1e-6): with RDS_MIXED and Euler physics (or a stabilisation field
+ * installed), rds_iterate runs FP32 cell kernels
  * until max_eq norm/norm(iter 0) <= mixed_switch, or, once that drop has halved at least
  * once, until it has not halved for max(mixed_stall_min, mixed_stall_mult x the last interval
  * between halvings) iterations (the problem's FP32 round-off floor; defaults 200 and 3), and

@@ -140,8 +140,12 @@ struct rds_ctx
   // contribution since then (d_c32, one value per slot), the cells' with the blending
   // coefficients of PGB frozen at d_ur (d_dc_theta, one per cell)
   bool dc_ok         = false;
-  int dc_m           = 16;
+  int dc_m           = 32;
   int dc_phase       = 0; // launch_residual_kernels: 0 plain, 1 exact DC sweep, 2 correction
+  // loop graphs: the main-stream kernels of an iteration (first cell group, gather) with
+  // programmatic dependent launch (option "loop_pdl", default off: measured no gain on the
+  // configurations, whose critical path runs through the side-stream boundary kernels)
+  int loop_pdl       = 0;
   double *d_ur = nullptr, *d_dres = nullptr, *d_dc_theta = nullptr;
   float *d_c32 = nullptr, *d_dtv = nullptr;
   std::vector<long long> dc_cell_base; // first cell of each group in d_dc_theta
@@ -462,6 +466,9 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
   {
     const HostCellGroup &g = ctx->groups[ig];
     CellArgs a             = cell_args(ctx, g, stop);
+    // programmatic dependent launch for the first cell group of a loop iteration (the kernel
+    // before it on the stream is the previous iteration's gather)
+    a.pdl = (ctx->loop_pdl && !ctx->timing && ig == 0) ? 1 : 0;
     if (ctx->dc_phase == 1 && g.scheme == RDS_PGB)
       a.theta = ctx->d_dc_theta + ctx->dc_cell_base[ig]; // blending coefficients at u_r
     rds_status st          = launch(ctx, [&](const char **name) {
@@ -482,6 +489,7 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
         da.adv0       = ctx->desc.adv[0];
         da.adv1       = ctx->desc.adv[1];
         da.stop       = stop;
+        da.pdl        = (ctx->loop_pdl && !ctx->timing && ig == 0) ? 1 : 0;
         bool ok       = false;
         const cudaError_t e = launch_cells_scalar_dc(g, da, 0, 0, ctx->stream, name, &ok);
         return ok ? e : cudaErrorNotSupported;
@@ -1808,6 +1816,7 @@ static rds_status enqueue_iteration(rds_ctx *ctx, double cfl, int max_iter, doub
     return st;
   // gather + dt + update + norm, with the final reduction and stop test done by the last block
   GatherArgs ga = gather_args(ctx, cfl, ctx->d_stop);
+  ga.pdl        = (ctx->loop_pdl && !ctx->timing) ? 1 : 0;
   ga.counter    = ctx->d_counter;
   ga.norm       = ctx->d_norm;
   ga.norm0      = ctx->d_norm0;
@@ -1935,6 +1944,7 @@ static rds_status enqueue_dc_sweep(rds_ctx *ctx, bool exact, double cfl, int max
   ga.dtv        = ctx->d_dtv;
   ga.ur         = ctx->d_ur;
   ga.loop       = ctx->d_loop;
+  ga.pdl        = (ctx->loop_pdl && !ctx->timing) ? 1 : 0;
   if (exact)
   {
     ga.counter  = ctx->d_counter;
@@ -2222,6 +2232,13 @@ rds_status rds_set_option(rds_ctx *ctx, const char *key, double value)
   {
     ctx->use_tc = value != 0.0;
     release_graph(ctx); // captured loops hold the previous choice
+    return RDS_OK;
+  }
+  if (std::strcmp(key, "loop_pdl") == 0)
+  {
+    // programmatic dependent launch of the iteration's main-stream kernels (0 / 1)
+    ctx->loop_pdl = value != 0.0 ? 1 : 0;
+    release_graph(ctx);
     return RDS_OK;
   }
   if (std::strcmp(key, "mixed_refresh") == 0)

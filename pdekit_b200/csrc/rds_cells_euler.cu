@@ -14,8 +14,8 @@
 //      sum K+ u; an xor-butterfly over the group completes the sums (bit-identical in every
 //      lane, since a + b == b + a); every lane solves with sum K+ (2D: closed-form adjugate, as
 //      the reference's 4 x 4 inverse; 3D: FP64 LU with partial pivoting) for
-//      v = (sum K+)^-1 r_q and u_bar = (sum K+)^-1 sum_m K+_m u_m, then accumulates for its own
-//      nodes  lda_n += w_q |J_q| K+_n v  and  diss_n += w_q |J_q| K+_n (u_n - u_bar)
+//      v = (sum K+)^-1 r_q and u_bar - u_0 = (sum K+)^-1 sum_m K+_m (u_m - u_0), then accumulates
+//      for its own nodes  lda_n += w_q |J_q| K+_n v  and  diss_n += w_q |J_q| K+_n (u_n - u_bar)
 //      (= sum_{m != n} K+_n (sum K+)^-1 K+_m (u_n - u_m), the reference's N dissipation);
 //   E  PGB blending theta = |Phi_0| / (sum_n |lda_n0 + diss_n0| + 1e-6) with a group sum,
 //      nodal residuals to the contribution slots, cell wave speed |K| max lambda.
@@ -468,8 +468,11 @@ __global__ void __launch_bounds__(NT)
           {
             Kn[i * NEQ + j] = K[i][j];
             SK[i][j] += double(K[i][j]);
-            if (SCHEME != RDS_PGLDA) // sum K+ u feeds only the N dissipation
-              ku += double(K[i][j]) * su[n * NEQ + j];
+            // sum K+ (u - u_0) feeds only the N dissipation. Taken from node 0's state: the
+            // solve then acts on the differences of the states (a nearly uniform flow has
+            // them 100x smaller than the states), as the reference's K+_m (u_n - u_m)
+            if (SCHEME != RDS_PGLDA)
+              ku += double(K[i][j]) * (su[n * NEQ + j] - su[j]);
           }
           if (SCHEME != RDS_PGLDA)
             SKu[i] += ku;
@@ -506,10 +509,10 @@ __global__ void __launch_bounds__(NT)
       if (n < NDOF)
       {
         const T *Kn = sfk + (size_t)n * SM::KS;
-        double du[NEQ];
+        double du[NEQ]; // u_n - u_bar = (u_n - u_0) - (u_bar - u_0)
 #pragma unroll
         for (int e = 0; e < NEQ; ++e)
-          du[e] = su[n * NEQ + e] - ub[e];
+          du[e] = (su[n * NEQ + e] - su[e]) - ub[e];
 #pragma unroll
         for (int i = 0; i < NEQ; ++i)
         {

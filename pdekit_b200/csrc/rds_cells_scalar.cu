@@ -273,6 +273,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks<PHYS, T, NDOF>)
     cells_scalar2d(const __grid_constant__ CellArgs a,
                    const __grid_constant__ Tables<T, 2, NDOF, NQ, NFL, NGEO> tb)
 {
+  pdl_wait_and_release();
   if (*a.stop)
     return;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -318,8 +319,8 @@ cudaError_t launch_one(const HostCellGroup &g, const CellArgs &a, cudaStream_t s
   Tables<T, 2, NDOF, NQ, NFL, NGEO> tb;
   fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
   const int grid = (a.ncells + kBlock - 1) / kBlock;
-  cells_scalar2d<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO><<<grid, kBlock, 0, s>>>(a, tb);
-  return cudaGetLastError();
+  return launch_kernel(cells_scalar2d<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO>, dim3(grid),
+                       dim3(kBlock), 0, s, a.pdl != 0, a, tb);
 }
 
 template <int PHYS, int SCHEME, typename T>

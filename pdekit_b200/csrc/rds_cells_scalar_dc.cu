@@ -214,6 +214,7 @@ __global__ void __launch_bounds__(kBlock)
     cells_scalar2d_dc(const __grid_constant__ DcCellArgs a,
                       const __grid_constant__ Tables<float, 2, NDOF, NQ, NFL, NGEO> tb)
 {
+  pdl_wait_and_release();
   if (*a.stop)
     return;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -277,8 +278,8 @@ cudaError_t launch_one(const HostCellGroup &g, const DcCellArgs &a, cudaStream_t
   Tables<float, 2, NDOF, NQ, NFL, 3> tb;
   fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
   const int grid = (a.ncells + kBlock - 1) / kBlock;
-  cells_scalar2d_dc<PHYS, SCHEME, NDOF, NQ, NFL, 3><<<grid, kBlock, 0, s>>>(a, tb);
-  return cudaGetLastError();
+  return launch_kernel(cells_scalar2d_dc<PHYS, SCHEME, NDOF, NQ, NFL, 3>, dim3(grid),
+                       dim3(kBlock), 0, s, a.pdl != 0, a, tb);
 }
 
 // grid > 0: the batch form (persistent over the active tiles, `tile` cells per CTA)

@@ -211,6 +211,7 @@ template <int NEQ, bool DT, bool UPDATE, bool NORM, bool FINAL, bool RK = false,
 __global__ void __launch_bounds__(kGBlock) gather_nodes(const __grid_constant__ GatherArgs a)
 {
   __shared__ double smem[kGBlock / 32];
+  pdl_wait_and_release();
   if (*a.stop)
     return;
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -661,8 +662,8 @@ cudaError_t launch_gather_neq(const GatherArgs &a, int mode, int nblocks, cudaSt
     gather_nodes<NEQ, true, true, true, false><<<nblocks, kGBlock, 0, s>>>(a);
     break;
   case 15:
-    gather_nodes<NEQ, true, true, true, true><<<nblocks, kGBlock, 0, s>>>(a);
-    break;
+    return launch_kernel(gather_nodes<NEQ, true, true, true, true>, dim3(nblocks), dim3(kGBlock),
+                         0, s, a.pdl != 0, a);
   case 16:
     gather_nodes<NEQ, false, false, false, false, true><<<nblocks, kGBlock, 0, s>>>(a);
     break;
@@ -680,12 +681,12 @@ cudaError_t launch_gather_neq(const GatherArgs &a, int mode, int nblocks, cudaSt
 cudaError_t launch_gather_dc(const GatherArgs &a, int mode, int nblocks, cudaStream_t s)
 {
   if (mode == 18)
-    gather_nodes<1, true, true, true, true, false, 1><<<nblocks, kGBlock, 0, s>>>(a);
-  else if (mode == 19)
-    gather_nodes<1, false, false, false, false, false, 2><<<nblocks, kGBlock, 0, s>>>(a);
-  else
-    return cudaErrorInvalidValue;
-  return cudaGetLastError();
+    return launch_kernel(gather_nodes<1, true, true, true, true, false, 1>, dim3(nblocks),
+                         dim3(kGBlock), 0, s, a.pdl != 0, a);
+  if (mode == 19)
+    return launch_kernel(gather_nodes<1, false, false, false, false, false, 2>, dim3(nblocks),
+                         dim3(kGBlock), 0, s, a.pdl != 0, a);
+  return cudaErrorInvalidValue;
 }
 
 } // namespace

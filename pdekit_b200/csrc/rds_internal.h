@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "rds_b200.h"
@@ -16,6 +17,43 @@ constexpr int kMaxNeq  = 5;
 constexpr int kMaxDim  = 3;
 constexpr int kBlock   = 128; // threads per block of the cell/facet kernels
 constexpr int kGBlock  = 256; // threads per block of the node gather kernel
+
+// Programmatic dependent launch (sm_90+): a kernel launched with launch_kernel(pdl = true) may
+// start while the kernel before it on the stream finishes; it waits here, before touching
+// anything that kernel wrote, and lets the kernel after it start early in turn. Both are no-ops
+// for a kernel launched without the attribute.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_wait_and_release()
+{
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+
+// Launches kernel k, with the programmatic-dependent-launch attribute when pdl is set.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_kernel(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                 cudaStream_t s, bool pdl, Args &&...args)
+{
+  if (!pdl)
+  {
+    k<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim          = grid;
+  cfg.blockDim         = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream           = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id                                         = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs                                          = attr;
+  cfg.numAttrs                                       = 1;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+#endif
 
 // Device-side status word bits (ORed by kernels, read by the host).
 enum : unsigned
@@ -148,6 +186,7 @@ struct CellArgs
   BatchTileMap bt; // batch mode only
   double *theta;   // PGB: the cell's blending coefficient [ncells] when not null (Jacobians)
   const double *blend; // PGB: external nodal blending coefficient [nnodes] when not null
+  int pdl;         // launch with programmatic dependent launch (loop graphs)
 };
 
 // FP32 correction sweep of the defect-correction loop (rds_cells_scalar_dc.cu): the change of
@@ -167,6 +206,7 @@ struct DcCellArgs
   double adv0, adv1;
   const int *stop;
   BatchTileMap bt; // batch form only
+  int pdl;         // launch with programmatic dependent launch (loop graphs)
 };
 
 struct BCArgs
@@ -242,6 +282,7 @@ struct GatherArgs
   double *dres;
   float *dtv;
   double *ur;
+  int pdl; // launch with programmatic dependent launch (loop graphs)
 };
 
 // ---- launchers (return cudaError_t of the launch) --------------------------------------
