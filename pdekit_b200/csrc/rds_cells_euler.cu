@@ -8,14 +8,14 @@
 //   B  flux nodes f = lane, lane + G, ...: S_f = Vsf u, F(S_f)            -> shared memory;
 //   C  quadrature points q = lane, lane + G, ...: u_q = V u and the flux divergence
 //      r_q = sum_d (invJ dVf F_d)_d                                       -> shared memory;
-//   D  every quadrature point, all lanes together: lane l owns nodes n = l, l + G, ...;
-//      it builds K+_n = R max(Lambda,0) L for grad phi_n (Euler2DCons.hpp:316-536 /
-//      Euler3DCons.hpp:332-560; in the split form of euler_K_split) and its part of sum K+ and
-//      sum K+ u; an xor-butterfly over the group completes the sums (bit-identical in every
-//      lane, since a + b == b + a); every lane solves with sum K+ (2D: closed-form adjugate, as
-//      the reference's 4 x 4 inverse; 3D: FP64 LU with partial pivoting) for
-//      v = (sum K+)^-1 r_q and u_bar - u_0 = (sum K+)^-1 sum_m K+_m (u_m - u_0), then accumulates
-//      for its own nodes  lda_n += w_q |J_q| K+_n v  and  diss_n += w_q |J_q| K+_n (u_n - u_bar)
+//   D1 quadrature points q = lane, lane + G, ...: the upwind matrices of all nodes in the split
+//      form K+_n = oc I + rp lp^T + rm lm^T (Euler2DCons.hpp:316-536 / Euler3DCons.hpp:332-560;
+//      euler_K_factors), summed into sum K+ (and sum K+ (u - u_0) for N / B) without storing
+//      any K+_n; one solve per point with sum K+ (2D: closed-form adjugate, as the reference's
+//      4 x 4 inverse; 3D: FP64 LU with partial pivoting) for v = (sum K+)^-1 r_q and
+//      u_bar - u_0 = (sum K+)^-1 sum_m K+_m (u_m - u_0)                   -> shared memory;
+//   D2 nodes n = lane, lane + G, ...: for every point the factors of K+_n again, applied in
+//      factored form:  lda_n += w_q |J_q| K+_n v  and  diss_n += w_q |J_q| K+_n (u_n - u_bar)
 //      (= sum_{m != n} K+_n (sum K+)^-1 K+_m (u_n - u_m), the reference's N dissipation);
 //   E  PGB blending theta = |Phi_0| / (sum_n |lda_n0 + diss_n0| + 1e-6) with a group sum,
 //      nodal residuals to the contribution slots, cell wave speed |K| max lambda.
@@ -56,7 +56,6 @@ __device__ __forceinline__ double group_max(double v)
 template <int N, bool TWO = true>
 __device__ __forceinline__ void lu_solve2(double A[N][N], double b1[N], double b2[N])
 {
-#pragma unroll
   double rdiag[N]; // 1 / U_kk, reused by the back substitution
 #pragma unroll
   for (int k = 0; k < N; ++k)
@@ -224,35 +223,36 @@ __device__ __forceinline__ T jacobian_at(const Tables<T, D, NDOF, NQ, NFL, NGEO>
   }
 }
 
-// Shared-memory footprint per cell (bytes): nodal states (FP64), flux values / upwind
-// matrices (aliased: phase B-C vs D), u_q and r_q.
+// Shared-memory footprint per cell (bytes): nodal states (FP64), the flux values of one chunk of
+// NFC flux nodes in phases B-C aliased with the per-point solutions of D1 (FP64, 8-byte
+// aligned: u_bar - u_0, and for T = float also v, which otherwise overwrites r_q), u_q and r_q.
 // Strides are odd numbers of elements so that the lanes of a warp, which work on different
 // cells, fall on different banks.
-template <typename T, int D, int NDOF, int NQ, int NFL>
+template <typename T, int D, int NDOF, int NQ, int NFL, int NFC>
 struct EulerSmem
 {
   static constexpr int odd(int n) { return n | 1; }
   static constexpr int NEQ   = D + 2;
-  static constexpr int U     = odd(NDOF * NEQ);                   // doubles per cell
-  static constexpr int KS    = NEQ * NEQ + 1;                     // T per node matrix
-  static constexpr int FK_F  = NFL * NEQ * D;                     // T (phase B-C)
-  static constexpr int FK_K  = NDOF * KS;                         // T (phase D)
-  static constexpr int FK    = odd(FK_F > FK_K ? FK_F : FK_K);
-  static constexpr int QV    = NQ * NEQ;                          // T, u_q then r_q
+  static constexpr int U     = odd(NDOF * NEQ); // doubles per cell
+  static constexpr int FK_F  = NFC * NEQ * D;   // T (phases B-C)
+  static constexpr int FK_S  = sizeof(T) == 8 ? NQ * NEQ : (2 * NQ * NEQ + 1) * 2; // T (D1-D2)
+  static constexpr int FK    = odd(FK_F > FK_S ? FK_F : FK_S);
+  static constexpr int QV    = NQ * NEQ;        // T, u_q then r_q
   static constexpr int QV2   = odd(2 * QV);
   static constexpr int BYTES = U * 8 + FK * (int)sizeof(T) + QV2 * (int)sizeof(T);
 };
 
 template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, bool AFFINE,
-          int G, int NT>
-__global__ void __launch_bounds__(NT)
+          int G, int NT, int NCH, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
     cells_euler(const CellArgs a, const Tables<T, (PHYS == RDS_EULER3D ? 3 : 2), NDOF, NQ, NFL,
                                                 NGEO> tb)
 {
   constexpr int D   = (PHYS == RDS_EULER3D) ? 3 : 2;
   constexpr int NEQ = D + 2;
   constexpr int NPT = (NDOF + G - 1) / G; // nodes per lane
-  using SM          = EulerSmem<T, D, NDOF, NQ, NFL>;
+  constexpr int NFC = (NFL + NCH - 1) / NCH; // flux nodes per chunk
+  using SM          = EulerSmem<T, D, NDOF, NQ, NFL, NFC>;
   constexpr int CPB = NT / G; // cells per block
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -300,107 +300,295 @@ __global__ void __launch_bounds__(NT)
   if (AFFINE)
     detc = jacobian_at(tb, 0, X, ijc);
 
-  // ---- B: flux at the flux nodes; affine cells store it contracted with invJ,
-  // G[f][e][xi] = sum_x invJ[x][xi] F[f][e][x], so that C needs D instead of D^2 products per
-  // flux node and point
-  for (int f = lane; f < NFL; f += G)
+  if constexpr (NCH == 1)
   {
-    T s[NEQ];
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e)
+    // ---- B: flux at the flux nodes; affine cells store it contracted with invJ,
+    // G[f][e][xi] = sum_x invJ[x][xi] F[f][e][x], so that C needs D instead of D^2 products
+    // per flux node and point. Table entries are read once each and applied to all equations
+    // (every sum keeps its order over the nodes).
+    for (int f = lane; f < NFL; f += G)
     {
-      T acc = tb.Vsf[f][0] * T(su[e]);
-#pragma unroll
-      for (int n = 1; n < NDOF; ++n)
-        acc = acc + tb.Vsf[f][n] * T(su[n * NEQ + e]);
-      s[e] = acc;
-    }
-    EulerProps<T, D> p;
-    bad |= euler_props<T, D>(s, gamma, p);
-    T F[NEQ][D];
-    euler_flux<T, D>(s, p, F);
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e)
-#pragma unroll
-      for (int d = 0; d < D; ++d)
+      T s[NEQ];
       {
-        T v = F[e][d];
-        if (AFFINE)
-        {
-          v = ijc[0][d] * F[e][0];
+        const T c = tb.Vsf[f][0];
 #pragma unroll
-          for (int x = 1; x < D; ++x)
-            v = v + ijc[x][d] * F[e][x];
-        }
-        sfk[(f * NEQ + e) * D + d] = v;
+        for (int e = 0; e < NEQ; ++e)
+          s[e] = c * T(su[e]);
       }
-  }
-  __syncwarp();
-
-  // ---- C: u_q and flux divergence r_q
-  for (int q = lane; q < NQ; q += G)
-  {
-    T ij[D][D];
-    if (!AFFINE)
-      jacobian_at(tb, q, X, ij);
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e)
-    {
-      T acc = tb.V[q][0] * T(su[e]);
 #pragma unroll
       for (int n = 1; n < NDOF; ++n)
-        acc = acc + tb.V[q][n] * T(su[n * NEQ + e]);
-      suq[q * NEQ + e] = acc;
-      T r = T(0);
+      {
+        const T c = tb.Vsf[f][n];
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          s[e] = s[e] + c * T(su[n * NEQ + e]);
+      }
+      EulerProps<T, D> p;
+      bad |= euler_props<T, D>(s, gamma, p);
+      T F[NEQ][D];
+      euler_flux<T, D>(s, p, F);
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+        {
+          T v = F[e][d];
+          if (AFFINE)
+          {
+            v = ijc[0][d] * F[e][0];
+#pragma unroll
+            for (int x = 1; x < D; ++x)
+              v = v + ijc[x][d] * F[e][x];
+          }
+          sfk[(f * NEQ + e) * D + d] = v;
+        }
+    }
+    __syncwarp();
+
+    // ---- C: u_q and flux divergence r_q (table entries read once each, as in B)
+    for (int q = lane; q < NQ; q += G)
+    {
+      T uq[NEQ];
+      {
+        const T c = tb.V[q][0];
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          uq[e] = c * T(su[e]);
+      }
+#pragma unroll
+      for (int n = 1; n < NDOF; ++n)
+      {
+        const T c = tb.V[q][n];
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          uq[e] = uq[e] + c * T(su[n * NEQ + e]);
+      }
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+        suq[q * NEQ + e] = uq[e];
       if (AFFINE)
       {
+        // r_e = sum_xi sum_f dVf[xi][q][f] G[f][e][xi]
+        T r[NEQ];
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          r[e] = T(0);
 #pragma unroll
         for (int xi = 0; xi < D; ++xi)
 #pragma unroll
           for (int f = 0; f < NFL; ++f)
-            r = r + tb.dVf[xi][q][f] * sfk[(f * NEQ + e) * D + xi];
+          {
+            const T c = tb.dVf[xi][q][f];
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e)
+              r[e] = r[e] + c * sfk[(f * NEQ + e) * D + xi];
+          }
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          srq[q * NEQ + e] = r[e];
       }
       else
       {
+        // r_e = sum_ic sum_xi invJ[ic][xi] (sum_f dVf[xi][q][f] F[f][e][ic])
+        T ij[D][D];
+        jacobian_at(tb, q, X, ij);
+        T dref[NEQ][D][D]; // [e][ic][xi]
 #pragma unroll
-        for (int ic = 0; ic < D; ++ic)
+        for (int xi = 0; xi < D; ++xi)
         {
-          T dref[D];
+          {
+            const T c = tb.dVf[xi][q][0];
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e)
+#pragma unroll
+              for (int ic = 0; ic < D; ++ic)
+                dref[e][ic][xi] = c * sfk[(0 * NEQ + e) * D + ic];
+          }
+#pragma unroll
+          for (int f = 1; f < NFL; ++f)
+          {
+            const T c = tb.dVf[xi][q][f];
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e)
+#pragma unroll
+              for (int ic = 0; ic < D; ++ic)
+                dref[e][ic][xi] = dref[e][ic][xi] + c * sfk[(f * NEQ + e) * D + ic];
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+        {
+          T r = T(0);
+#pragma unroll
+          for (int ic = 0; ic < D; ++ic)
+          {
+            T dphys = ij[ic][0] * dref[e][ic][0];
+#pragma unroll
+            for (int xi = 1; xi < D; ++xi)
+              dphys = dphys + ij[ic][xi] * dref[e][ic][xi];
+            r = r + dphys;
+          }
+          srq[q * NEQ + e] = r;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  else
+  {
+    // ---- B and C, NCH chunks of NFC flux nodes (the flux region holds one chunk): the flux at
+    // the chunk's nodes, then its part of every point's flux divergence r_q (and with the first
+    // chunk u_q = V u). Affine cells store the flux contracted with invJ,
+    // G[f][e][xi] = sum_x invJ[x][xi] F[f][e][x], so that C needs D instead of D^2 products per
+    // flux node and point. Table entries are read once each and applied to all equations (every
+    // sum keeps its order over the nodes).
+#pragma unroll 1
+    for (int ch = 0; ch < NCH; ++ch)
+    {
+      const int c0 = ch * NFC;
+      for (int fl = lane; fl < NFC && c0 + fl < NFL; fl += G)
+      {
+        const int f = c0 + fl;
+        T s[NEQ];
+        {
+          const T c = tb.Vsf[f][0];
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e)
+            s[e] = c * T(su[e]);
+        }
+#pragma unroll
+        for (int n = 1; n < NDOF; ++n)
+        {
+          const T c = tb.Vsf[f][n];
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e)
+            s[e] = s[e] + c * T(su[n * NEQ + e]);
+        }
+        EulerProps<T, D> p;
+        bad |= euler_props<T, D>(s, gamma, p);
+        T F[NEQ][D];
+        euler_flux<T, D>(s, p, F);
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+#pragma unroll
+          for (int d = 0; d < D; ++d)
+          {
+            T v = F[e][d];
+            if (AFFINE)
+            {
+              v = ijc[0][d] * F[e][0];
+#pragma unroll
+              for (int x = 1; x < D; ++x)
+                v = v + ijc[x][d] * F[e][x];
+            }
+            sfk[(fl * NEQ + e) * D + d] = v;
+          }
+      }
+      __syncwarp();
+
+      for (int q = lane; q < NQ; q += G)
+      {
+        if (ch == 0)
+        {
+          T uq[NEQ];
+          {
+            const T c = tb.V[q][0];
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e)
+              uq[e] = c * T(su[e]);
+          }
+#pragma unroll
+          for (int n = 1; n < NDOF; ++n)
+          {
+            const T c = tb.V[q][n];
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e)
+              uq[e] = uq[e] + c * T(su[n * NEQ + e]);
+          }
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e)
+            suq[q * NEQ + e] = uq[e];
+        }
+        T r[NEQ];
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          r[e] = ch == 0 ? T(0) : srq[q * NEQ + e];
+        if (AFFINE)
+        {
+          // r_e += sum_xi sum_f dVf[xi][q][f] G[f][e][xi]
+#pragma unroll
+          for (int xi = 0; xi < D; ++xi)
+#pragma unroll
+            for (int fl = 0; fl < NFC; ++fl)
+              if (c0 + fl < NFL)
+              {
+                const T c = tb.dVf[xi][q][c0 + fl];
+#pragma unroll
+                for (int e = 0; e < NEQ; ++e)
+                  r[e] = r[e] + c * sfk[(fl * NEQ + e) * D + xi];
+              }
+        }
+        else
+        {
+          // r_e += sum_ic sum_xi invJ[ic][xi] (sum_f dVf[xi][q][f] F[f][e][ic])
+          T ij[D][D];
+          jacobian_at(tb, q, X, ij);
+          T dref[NEQ][D][D]; // [e][ic][xi]
 #pragma unroll
           for (int xi = 0; xi < D; ++xi)
           {
-            T s2 = tb.dVf[xi][q][0] * sfk[(0 * NEQ + e) * D + ic];
+            {
+              const T c = tb.dVf[xi][q][c0];
 #pragma unroll
-            for (int f = 1; f < NFL; ++f)
-              s2 = s2 + tb.dVf[xi][q][f] * sfk[(f * NEQ + e) * D + ic];
-            dref[xi] = s2;
+              for (int e = 0; e < NEQ; ++e)
+#pragma unroll
+                for (int ic = 0; ic < D; ++ic)
+                  dref[e][ic][xi] = c * sfk[(0 * NEQ + e) * D + ic];
+            }
+#pragma unroll
+            for (int fl = 1; fl < NFC; ++fl)
+              if (c0 + fl < NFL)
+              {
+                const T c = tb.dVf[xi][q][c0 + fl];
+#pragma unroll
+                for (int e = 0; e < NEQ; ++e)
+#pragma unroll
+                  for (int ic = 0; ic < D; ++ic)
+                    dref[e][ic][xi] = dref[e][ic][xi] + c * sfk[(fl * NEQ + e) * D + ic];
+              }
           }
-          T dphys = ij[ic][0] * dref[0];
 #pragma unroll
-          for (int xi = 1; xi < D; ++xi)
-            dphys = dphys + ij[ic][xi] * dref[xi];
-          r = r + dphys;
+          for (int e = 0; e < NEQ; ++e)
+          {
+            T rr = T(0);
+#pragma unroll
+            for (int ic = 0; ic < D; ++ic)
+            {
+              T dphys = ij[ic][0] * dref[e][ic][0];
+#pragma unroll
+              for (int xi = 1; xi < D; ++xi)
+                dphys = dphys + ij[ic][xi] * dref[e][ic][xi];
+              rr = rr + dphys;
+            }
+            r[e] = ch == 0 ? rr : r[e] + rr;
+          }
         }
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          srq[q * NEQ + e] = r[e];
       }
-      srq[q * NEQ + e] = r;
+      __syncwarp();
     }
   }
-  __syncwarp();
 
-  // ---- D: quadrature loop, nodes distributed over the lanes
-  double lda[NPT][NEQ], diss[NPT][NEQ];
-#pragma unroll
-  for (int s = 0; s < NPT; ++s)
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e)
-    {
-      lda[s][e]  = 0.0;
-      diss[s][e] = 0.0;
-    }
-  double phi0 = 0.0, vol = 0.0;
-  T wsmax     = T(0);
-
-  for (int q = 0; q < NQ; ++q)
+  // ---- D1: quadrature points over the lanes; per point v = (sum K+)^-1 r_q and, for N / B,
+  // u_bar - u_0 = (sum K+)^-1 sum_m K+_m (u_m - u_0), both FP64 in the flux region
+  double *sfd = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(sfk) + 7) & ~uintptr_t(7));
+  double *sv  = sizeof(T) == 8 ? reinterpret_cast<double *>(srq) : sfd + NQ * NEQ;
+  double *sub = sfd;
+  double phi0_l = 0.0; // this lane's points' part of Phi_0 = sum_q w_q |J_q| r_q0
+  T wsmax       = T(0);
+  for (int q = lane; q < NQ; q += G)
   {
     T ij[D][D];
     T det;
@@ -415,9 +603,6 @@ __global__ void __launch_bounds__(NT)
     }
     else
       det = jacobian_at(tb, q, X, ij);
-    const double wj = double(tb.w[q] * det);
-    vol += wj;
-
     T uq[NEQ];
 #pragma unroll
     for (int e = 0; e < NEQ; ++e)
@@ -436,58 +621,55 @@ __global__ void __launch_bounds__(NT)
       for (int j = 0; j < NEQ; ++j)
         SK[i][j] = 0.0;
     }
-
-#pragma unroll
-    for (int s = 0; s < NPT; ++s)
+#pragma unroll 1
+    for (int n = 0; n < NDOF; ++n)
     {
-      const int n = lane + s * G;
-      if (n < NDOF)
+      T gphys[D];
+#pragma unroll
+      for (int x = 0; x < D; ++x)
       {
-        T gref[D], gphys[D];
+        T acc = ij[x][0] * tb.dV[0][q][n];
 #pragma unroll
-        for (int d = 0; d < D; ++d)
-          gref[d] = tb.dV[d][q][n];
+        for (int xi = 1; xi < D; ++xi)
+          acc = acc + ij[x][xi] * tb.dV[xi][q][n];
+        gphys[x] = acc;
+      }
+      EulerKFactors<T, D> f;
+      wsmax = fmax(wsmax, euler_K_factors<+1, T, D>(p, ac, gphys, f));
+      double rp[NEQ], rm[NEQ], lp[NEQ], lm[NEQ];
 #pragma unroll
-        for (int x = 0; x < D; ++x)
+      for (int i = 0; i < NEQ; ++i)
+      {
+        rp[i] = double(f.rp[i]);
+        rm[i] = double(f.rm[i]);
+        lp[i] = double(f.lp[i]);
+        lm[i] = double(f.lm[i]);
+      }
+#pragma unroll
+      for (int i = 0; i < NEQ; ++i)
+      {
+#pragma unroll
+        for (int j = 0; j < NEQ; ++j)
+          SK[i][j] += rp[i] * lp[j] + rm[i] * lm[j];
+        SK[i][i] += double(f.oc);
+      }
+      if (SCHEME != RDS_PGLDA)
+      {
+        // sum K+ (u - u_0): the solve then acts on the differences of the states (a nearly
+        // uniform flow has them 100x smaller than the states), as the reference's
+        // K+_m (u_n - u_m)
+        double du[NEQ], pd = 0.0, md = 0.0;
+#pragma unroll
+        for (int j = 0; j < NEQ; ++j)
         {
-          T acc = ij[x][0] * gref[0];
-#pragma unroll
-          for (int xi = 1; xi < D; ++xi)
-            acc = acc + ij[x][xi] * gref[xi];
-          gphys[x] = acc;
+          du[j] = su[n * NEQ + j] - su[j];
+          pd += lp[j] * du[j];
+          md += lm[j] * du[j];
         }
-        T K[NEQ][NEQ];
-        wsmax = fmax(wsmax, euler_K_split<+1, T, D>(p, ac, gphys, K));
-        T *Kn = sfk + (size_t)n * SM::KS;
 #pragma unroll
         for (int i = 0; i < NEQ; ++i)
-        {
-          double ku = 0.0;
-#pragma unroll
-          for (int j = 0; j < NEQ; ++j)
-          {
-            Kn[i * NEQ + j] = K[i][j];
-            SK[i][j] += double(K[i][j]);
-            // sum K+ (u - u_0) feeds only the N dissipation. Taken from node 0's state: the
-            // solve then acts on the differences of the states (a nearly uniform flow has
-            // them 100x smaller than the states), as the reference's K+_m (u_n - u_m)
-            if (SCHEME != RDS_PGLDA)
-              ku += double(K[i][j]) * (su[n * NEQ + j] - su[j]);
-          }
-          if (SCHEME != RDS_PGLDA)
-            SKu[i] += ku;
-        }
+          SKu[i] += double(f.oc) * du[i] + rp[i] * pd + rm[i] * md;
       }
-    }
-    // complete the sums over the group (identical in every lane)
-#pragma unroll
-    for (int i = 0; i < NEQ; ++i)
-    {
-      if (SCHEME != RDS_PGLDA)
-        SKu[i] = group_sum<G>(SKu[i]);
-#pragma unroll
-      for (int j = 0; j < NEQ; ++j)
-        SK[i][j] = group_sum<G>(SK[i][j]);
     }
     double v[NEQ], ub[NEQ];
 #pragma unroll
@@ -496,41 +678,112 @@ __global__ void __launch_bounds__(NT)
       v[e]  = double(srq[q * NEQ + e]);
       ub[e] = SKu[e];
     }
-    phi0 += wj * v[0];
+    phi0_l += double(tb.w[q] * det) * v[0];
     if constexpr (NEQ == 4)
       adj_solve4<SCHEME != RDS_PGLDA>(SK, v, ub);
     else
       lu_solve2<NEQ, SCHEME != RDS_PGLDA>(SK, v, ub);
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+    {
+      sv[q * NEQ + e] = v[e];
+      if (SCHEME != RDS_PGLDA)
+        sub[q * NEQ + e] = ub[e];
+    }
+  }
+  __syncwarp();
 
+  // ---- D2: nodes over the lanes, every point: K+_n v and K+_n (u_n - u_bar) in factored form
+  double lda[NPT][NEQ], diss[NPT][NEQ];
+#pragma unroll
+  for (int s = 0; s < NPT; ++s)
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+    {
+      lda[s][e]  = 0.0;
+      diss[s][e] = 0.0;
+    }
+  double vol = 0.0;
+#pragma unroll 1
+  for (int q = 0; q < NQ; ++q)
+  {
+    T ij[D][D];
+    T det;
+    if (AFFINE)
+    {
+      det = detc;
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j)
+          ij[i][j] = ijc[i][j];
+    }
+    else
+      det = jacobian_at(tb, q, X, ij);
+    const double wj = double(tb.w[q] * det);
+    vol += wj;
+    T uq[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+      uq[e] = suq[q * NEQ + e];
+    EulerProps<T, D> p;
+    euler_props<T, D>(uq, gamma, p);
+    EulerAcoustic<T, D> ac;
+    euler_acoustic<T, D>(p, gamma, ac);
+    double v[NEQ], ub[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+    {
+      v[e]  = sv[q * NEQ + e];
+      ub[e] = (SCHEME != RDS_PGLDA) ? sub[q * NEQ + e] : 0.0;
+    }
 #pragma unroll
     for (int s = 0; s < NPT; ++s)
     {
       const int n = lane + s * G;
       if (n < NDOF)
       {
-        const T *Kn = sfk + (size_t)n * SM::KS;
-        double du[NEQ]; // u_n - u_bar = (u_n - u_0) - (u_bar - u_0)
+        T gphys[D];
 #pragma unroll
-        for (int e = 0; e < NEQ; ++e)
-          du[e] = (su[n * NEQ + e] - su[e]) - ub[e];
+        for (int x = 0; x < D; ++x)
+        {
+          T acc = ij[x][0] * tb.dV[0][q][n];
+#pragma unroll
+          for (int xi = 1; xi < D; ++xi)
+            acc = acc + ij[x][xi] * tb.dV[xi][q][n];
+          gphys[x] = acc;
+        }
+        EulerKFactors<T, D> f;
+        euler_K_factors<+1, T, D>(p, ac, gphys, f);
+        const double oc = double(f.oc);
+        double pv = 0.0, mv = 0.0;
+#pragma unroll
+        for (int j = 0; j < NEQ; ++j)
+        {
+          pv += double(f.lp[j]) * v[j];
+          mv += double(f.lm[j]) * v[j];
+        }
 #pragma unroll
         for (int i = 0; i < NEQ; ++i)
+          lda[s][i] += wj * (oc * v[i] + double(f.rp[i]) * pv + double(f.rm[i]) * mv);
+        if (SCHEME != RDS_PGLDA)
         {
-          double kv = 0.0, kd = 0.0;
+          double du[NEQ], pd = 0.0, md = 0.0; // u_n - u_bar = (u_n - u_0) - (u_bar - u_0)
 #pragma unroll
           for (int j = 0; j < NEQ; ++j)
           {
-            const double kij = double(Kn[i * NEQ + j]);
-            kv += kij * v[j];
-            kd += kij * du[j];
+            du[j] = (su[n * NEQ + j] - su[j]) - ub[j];
+            pd += double(f.lp[j]) * du[j];
+            md += double(f.lm[j]) * du[j];
           }
-          lda[s][i] += wj * kv;
-          if (SCHEME != RDS_PGLDA)
-            diss[s][i] += wj * kd;
+#pragma unroll
+          for (int i = 0; i < NEQ; ++i)
+            diss[s][i] += wj * (oc * du[i] + double(f.rp[i]) * pd + double(f.rm[i]) * md);
         }
       }
     }
   }
+  const double phi0 = group_sum<G>(phi0_l);
 
   // ---- E: blending, outputs
   double theta = 1.0;
@@ -593,26 +846,31 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
-// NT: threads per block. kBlock unless the per-cell shared memory would then leave the SM
-// with fewer warps than its registers allow (Euler 3D FP64: 3.9 KB per cell, so 56 cells in
-// one block of 224 threads use the SM's 227 KB instead of one block of 32 cells).
+// NT: threads per block; NCH: chunks of the flux nodes (shared memory per cell), MINB: blocks
+// per SM the register allocation must allow (0: the compiler's own choice, which for blocks of
+// 128 threads is usually 3; an explicit 1 lets it take all 255 registers). Euler 3D FP64 runs 96 cells in a block of 384
+// threads with the flux in 3 chunks (2.3 KB per cell instead of 3.9 KB: 12 warps per SM instead
+// of 7); the FP64 P3 triangles and quadrilaterals (25 points) take 3 blocks of 128 threads per
+// SM (12 warps).
 template <int PHYS, int SCHEME, typename T, int NDOF, int NQ, int NFL, int NGEO, int G,
-          int NT = kBlock>
+          int NT = kBlock, int NCH = 1, int MINB = 0>
 cudaError_t launch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream_t s)
 {
   constexpr int D = (PHYS == RDS_EULER3D) ? 3 : 2;
   Tables<T, D, NDOF, NQ, NFL, NGEO> tb;
   fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
-  constexpr int CPB  = NT / G;
-  static_assert(CPB * EulerSmem<T, D, NDOF, NQ, NFL>::BYTES <= 227 * 1024,
-                "per-block shared memory above the sm_100 limit");
-  const int smem     = CPB * EulerSmem<T, D, NDOF, NQ, NFL>::BYTES;
-  const int grid     = (a.ncells + CPB - 1) / CPB;
+  constexpr int CPB = NT / G;
+  constexpr int NFC = (NFL + NCH - 1) / NCH;
+  static_assert((NCH - 1) * NFC < NFL, "every chunk of flux nodes must be non-empty");
+  using SM = EulerSmem<T, D, NDOF, NQ, NFL, NFC>;
+  static_assert(CPB * SM::BYTES <= 227 * 1024, "per-block shared memory above the sm_100 limit");
+  const int smem = CPB * SM::BYTES;
+  const int grid = (a.ncells + CPB - 1) / CPB;
   // the shared-memory opt-in is set once per instantiation (not a stream operation, so it
   // also stays out of captured graphs)
   static bool attr_set = false;
-  auto k_aff           = cells_euler<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, true, G, NT>;
-  auto k_gen           = cells_euler<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, false, G, NT>;
+  auto k_aff = cells_euler<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, true, G, NT, NCH, MINB>;
+  auto k_gen = cells_euler<PHYS, SCHEME, T, NDOF, NQ, NFL, NGEO, false, G, NT, NCH, MINB>;
   if (!attr_set)
   {
     cudaError_t e = cudaFuncSetAttribute(k_aff, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -645,7 +903,8 @@ cudaError_t dispatch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream
       if (d.ndof == 6 && d.nq == 7 && d.nfl == 10)
         return launch_euler<PHYS, SCHEME, T, 6, 7, 10, 3, 4>(g, a, s);
       if (d.ndof == 10 && d.nq == 16 && d.nfl == 15)
-        return launch_euler<PHYS, SCHEME, T, 10, 16, 15, 3, 4>(g, a, s);
+        return launch_euler<PHYS, SCHEME, T, 10, 16, 15, 3, 4, kBlock, 1, (sizeof(T) == 8 ? 3 : 0)>(
+            g, a, s);
     }
     if (d.shape == RDS_QUAD && d.ngeo == 4)
     {
@@ -662,7 +921,8 @@ cudaError_t dispatch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream
       if (d.ndof == 16 && d.nq == 20 && d.nfl == 25)
         return launch_euler<PHYS, SCHEME, T, 16, 20, 25, 4, 8>(g, a, s);
       if (d.ndof == 16 && d.nq == 25 && d.nfl == 25)
-        return launch_euler<PHYS, SCHEME, T, 16, 25, 25, 4, 8>(g, a, s);
+        return launch_euler<PHYS, SCHEME, T, 16, 25, 25, 4, 8, kBlock, 1, (sizeof(T) == 8 ? 3 : 0)>(
+            g, a, s);
     }
   }
   else
@@ -670,8 +930,12 @@ cudaError_t dispatch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream
     if (d.shape == RDS_TETRA && d.ngeo == 4)
     {
       if (d.ndof == 10 && d.nq == 14 && d.nfl == 20)
-        return launch_euler<PHYS, SCHEME, T, 10, 14, 20, 4, 4, (sizeof(T) == 8 ? 224 : kBlock)>(
-            g, a, s);
+      {
+        if constexpr (sizeof(T) == 8)
+          return launch_euler<PHYS, SCHEME, T, 10, 14, 20, 4, 4, 384, 3>(g, a, s);
+        else
+          return launch_euler<PHYS, SCHEME, T, 10, 14, 20, 4, 4>(g, a, s);
+      }
     }
   }
   *ok = false;

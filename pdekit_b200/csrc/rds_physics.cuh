@@ -265,11 +265,22 @@ __device__ __forceinline__ void euler_acoustic(const EulerProps<T, D> &p, T gamm
 //   K = op(lam_c) I + (op(lam_+) - op(lam_c)) r_+ l_+^T + (op(lam_-) - op(lam_c)) r_- l_-^T
 // where r_+- = rho/(2a) (1, V +- a n, H +- a u.n) and l_+- are the acoustic eigenvector pairs
 // (columns / rows D and D + 1 of R and L in euler_eigen): two rank-one updates instead of the
-// product of three N x N matrices. Returns max_k max(1e-6, |lam_k|).
+// product of three N x N matrices. The factors: K = oc I + rp lp^T + rm lm^T.
+template <typename T, int D>
+struct EulerKFactors
+{
+  T oc;         // op(lam_c)
+  T rp[D + 2];  // (op(lam_+) - op(lam_c)) r_+
+  T rm[D + 2];  // (op(lam_-) - op(lam_c)) r_-
+  T lp[D + 2];  // l_+
+  T lm[D + 2];  // l_-
+};
+
+// The factors of K for direction dir; returns max_k max(1e-6, |lam_k|).
 template <int SIGN, typename T, int D>
-__device__ __forceinline__ T euler_K_split(const EulerProps<T, D> &p,
-                                           const EulerAcoustic<T, D> &c, const T *dir,
-                                           T K[D + 2][D + 2])
+__device__ __forceinline__ T euler_K_factors(const EulerProps<T, D> &p,
+                                             const EulerAcoustic<T, D> &c, const T *dir,
+                                             EulerKFactors<T, D> &f)
 {
   constexpr int N = D + 2;
   T n2            = dir[0] * dir[0] + dir[1] * dir[1];
@@ -295,32 +306,44 @@ __device__ __forceinline__ T euler_K_split(const EulerProps<T, D> &p,
   };
   const T oc = op(lc);
   const T ap = (op(lp) - oc) * c.ra, am = (op(lm) - oc) * c.ra;
-  T rp[N], rm[N], lpv[N], lmv[N];
-  rp[0] = ap;
-  rm[0] = am;
+  f.oc       = oc;
+  f.rp[0]    = ap;
+  f.rm[0]    = am;
 #pragma unroll
   for (int d = 0; d < D; ++d)
   {
-    rp[1 + d]  = ap * (p.V[d] + a * n[d]);
-    rm[1 + d]  = am * (p.V[d] - a * n[d]);
-    lpv[1 + d] = p.inv_rho * (n[d] - c.gV[d]);
-    lmv[1 + d] = -p.inv_rho * (n[d] + c.gV[d]);
+    f.rp[1 + d] = ap * (p.V[d] + a * n[d]);
+    f.rm[1 + d] = am * (p.V[d] - a * n[d]);
+    f.lp[1 + d] = p.inv_rho * (n[d] - c.gV[d]);
+    f.lm[1 + d] = -p.inv_rho * (n[d] + c.gV[d]);
   }
-  rp[N - 1]  = ap * (p.H + a * um);
-  rm[N - 1]  = am * (p.H - a * um);
-  lpv[0]     = a * p.inv_rho * (c.kin - um * c.inv_a);
-  lmv[0]     = a * p.inv_rho * (c.kin + um * c.inv_a);
-  lpv[N - 1] = c.g_rhoa;
-  lmv[N - 1] = c.g_rhoa;
+  f.rp[N - 1] = ap * (p.H + a * um);
+  f.rm[N - 1] = am * (p.H - a * um);
+  f.lp[0]     = a * p.inv_rho * (c.kin - um * c.inv_a);
+  f.lm[0]     = a * p.inv_rho * (c.kin + um * c.inv_a);
+  f.lp[N - 1] = c.g_rhoa;
+  f.lm[N - 1] = c.g_rhoa;
+  return fmax(fmax(T(1.e-6), fabs(lc)), fmax(fabs(lp), fabs(lm)));
+}
+
+// K itself, from its factors; returns max_k max(1e-6, |lam_k|).
+template <int SIGN, typename T, int D>
+__device__ __forceinline__ T euler_K_split(const EulerProps<T, D> &p,
+                                           const EulerAcoustic<T, D> &c, const T *dir,
+                                           T K[D + 2][D + 2])
+{
+  constexpr int N = D + 2;
+  EulerKFactors<T, D> f;
+  const T ws = euler_K_factors<SIGN, T, D>(p, c, dir, f);
 #pragma unroll
   for (int i = 0; i < N; ++i)
 #pragma unroll
     for (int j = 0; j < N; ++j)
     {
-      const T s = rp[i] * lpv[j] + rm[i] * lmv[j];
-      K[i][j]   = (i == j) ? oc + s : s;
+      const T s = f.rp[i] * f.lp[j] + f.rm[i] * f.lm[j];
+      K[i][j]   = (i == j) ? f.oc + s : s;
     }
-  return fmax(fmax(T(1.e-6), fabs(lc)), fmax(fabs(lp), fabs(lm)));
+  return ws;
 }
 
 } // namespace rds
