@@ -44,6 +44,7 @@ struct rds_ctx
   long long launches = 0;
 
   std::vector<HostCellGroup> groups;
+  std::vector<double> hX; // geometry coordinates [dim][node] (constant-Jacobian checks)
   std::vector<HostBC> bcs;
 
   double *d_X       = nullptr; // SoA coords [dim][ngeo_nodes]
@@ -641,9 +642,58 @@ rds_status rds_create(rds_ctx **out, const rds_desc *desc, void *stream)
     return st;
   if ((st = upload(ctx, ctx->d_X, X.data(), X.size())) != RDS_OK)
     return st;
+  ctx->hX = X;
   RDS_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->desc.geo_coords = nullptr;
   return RDS_OK;
+}
+
+// True when the bilinear map of every cell of a 4-node quadrilateral group has a constant
+// Jacobian (all cells parallelograms, to 1e-14 of the cell's extent). The per-point Jacobian
+// derivatives of the geometry basis then differ from those at point 0 by multiples of one
+// nodal "twist" vector t (the bilinear mode); a cell is a parallelogram when sum_g t_g X_g = 0.
+static bool parallelogram_cells(const rds_ctx *ctx, const rds_cell_group &g)
+{
+  const int D = ctx->desc.dim, NG = g.ngeo;
+  if (ctx->hX.empty() || D != 2)
+    return false;
+  double t[4] = {0, 0, 0, 0}, best = 0.0;
+  for (int xi = 0; xi < D; ++xi)
+    for (int q = 1; q < g.nq; ++q)
+    {
+      double dv[4], nrm = 0.0;
+      for (int k = 0; k < NG; ++k)
+      {
+        dv[k] = g.dVgeo[((size_t)xi * g.nq + q) * NG + k] - g.dVgeo[((size_t)xi * g.nq) * NG + k];
+        nrm += dv[k] * dv[k];
+      }
+      if (nrm > best)
+      {
+        best = nrm;
+        for (int k = 0; k < NG; ++k)
+          t[k] = dv[k];
+      }
+    }
+  if (best == 0.0)
+    return true;
+  const size_t ng = (size_t)ctx->desc.ngeo_nodes;
+  for (int c = 0; c < g.ncells; ++c)
+  {
+    const int32_t *cn = g.geo_conn + (size_t)c * NG;
+    for (int x = 0; x < D; ++x)
+    {
+      const double *Xx = ctx->hX.data() + (size_t)x * ng;
+      double tw = 0.0, ext = 0.0;
+      for (int k = 0; k < NG; ++k)
+      {
+        tw += t[k] * Xx[cn[k]];
+        ext = std::max(ext, std::fabs(Xx[cn[k]] - Xx[cn[0]]));
+      }
+      if (std::fabs(tw) > 1.e-14 * ext * std::sqrt(best))
+        return false;
+    }
+  }
+  return true;
 }
 
 rds_status rds_add_cell_group(rds_ctx *ctx, const rds_cell_group *g)
@@ -679,6 +729,8 @@ rds_status rds_add_cell_group(rds_ctx *ctx, const rds_cell_group *g)
     h.dVgeo_v.assign(g->dVgeo_v, g->dVgeo_v + (size_t)D * g->nqv * g->ngeo);
   }
   h.affine = (g->shape == RDS_TRIAG && g->ngeo == 3) || (g->shape == RDS_TETRA && g->ngeo == 4);
+  h.const_jac = h.affine || (g->shape == RDS_QUAD && g->ngeo == 4 &&
+                                parallelogram_cells(ctx, *g));
   h.physics = ctx->desc.physics;
   h.scheme  = ctx->desc.scheme;
   rds_status st;
@@ -1027,6 +1079,25 @@ rds_status rds_finalize(rds_ctx *ctx)
         return st;
       ctx->extra.push_back(g.d_tc);
       g.tune_tile[0] = 128; // one cell per TMEM lane
+    }
+  // Euler 2D: lane-indexed tables of the cell kernels (FP64, and FP32 for the mixed form)
+  if (NEQ > 1 && d.dim == 2)
+    for (HostCellGroup &g : ctx->groups)
+    {
+      std::vector<double> lt;
+      euler_lane_tables(g, d.dim, lt);
+      if ((st = dalloc(ctx, &g.d_lt64, lt.size())) != RDS_OK ||
+          (st = upload(ctx, g.d_lt64, lt.data(), lt.size())) != RDS_OK)
+        return st;
+      ctx->extra.push_back(g.d_lt64);
+      if (d.precision == RDS_MIXED)
+      {
+        std::vector<float> lt32(lt.begin(), lt.end());
+        if ((st = dalloc(ctx, &g.d_lt32, lt32.size())) != RDS_OK ||
+            (st = upload(ctx, g.d_lt32, lt32.data(), lt32.size())) != RDS_OK)
+          return st;
+        ctx->extra.push_back(g.d_lt32);
+      }
     }
   // side streams of the weak conditions after the first (rds_ctx::sides)
   for (int k = 1; k < std::min((int)ctx->bcs.size(), rds_ctx::kMaxSides); ++k)

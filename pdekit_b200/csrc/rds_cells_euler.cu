@@ -223,6 +223,44 @@ __device__ __forceinline__ T jacobian_at(const Tables<T, D, NDOF, NQ, NFL, NGEO>
   }
 }
 
+// The same from a lane-indexed geometry table dvg [D][NGEO][NQ] (global memory).
+template <typename T, int D, int NQ, int NGEO>
+__device__ __forceinline__ T jacobian_lt(const T *__restrict__ dvg, int q, const T (&X)[NGEO][D],
+                                         T (&ij)[D][D])
+{
+  Tables<T, D, 1, 1, 1, NGEO> t1; // only dVgeo[.][0][.] is read
+#pragma unroll
+  for (int xi = 0; xi < D; ++xi)
+#pragma unroll
+    for (int g = 0; g < NGEO; ++g)
+      t1.dVgeo[xi][0][g] = __ldg(dvg + (xi * NGEO + g) * NQ + q);
+  return jacobian_at(t1, 0, X, ij);
+}
+
+template <typename T>
+__device__ __forceinline__ T ldt(const T *p)
+{
+  return __ldg(p);
+}
+
+// Lane-indexed copies of a cell group's tables in global memory (read through L1): the entries
+// that the lanes of a warp read at different points (phases C, D1), flux nodes (B) or nodes (D2),
+// each laid out with that index fastest, so that a warp's reads fall in one or two sectors. The
+// kernel-parameter copy (constant bank, whose reads at different addresses are serialised) keeps
+// the reads that are uniform across the warp. Offsets in elements; euler_lane_tables fills it.
+template <int D, int NDOF, int NQ, int NFL, int NGEO>
+struct LaneTab
+{
+  static constexpr int VSF  = 0;                   // Vsf [NDOF][NFL]
+  static constexpr int V    = VSF + NDOF * NFL;    // V [NDOF][NQ]
+  static constexpr int DVF  = V + NDOF * NQ;       // dVf [D][NFL][NQ]
+  static constexpr int DVG  = DVF + D * NFL * NQ;  // dVgeo [D][NGEO][NQ]
+  static constexpr int DVQ  = DVG + D * NGEO * NQ; // dV [D][NDOF][NQ] (lanes over points)
+  static constexpr int DVN  = DVQ + D * NDOF * NQ; // dV [D][NQ][NDOF] (lanes over nodes)
+  static constexpr int W    = DVN + D * NQ * NDOF; // w [NQ]
+  static constexpr int SIZE = W + NQ;
+};
+
 // Shared-memory footprint per cell (bytes): nodal states (FP64), the flux values of one chunk of
 // NFC flux nodes in phases B-C aliased with the per-point solutions of D1 (FP64, 8-byte
 // aligned: u_bar - u_0, and for T = float also v, which otherwise overwrites r_q), u_q and r_q.
@@ -253,6 +291,47 @@ __global__ void __launch_bounds__(NT, MINB)
   constexpr int NPT = (NDOF + G - 1) / G; // nodes per lane
   constexpr int NFC = (NFL + NCH - 1) / NCH; // flux nodes per chunk
   using SM          = EulerSmem<T, D, NDOF, NQ, NFL, NFC>;
+  using LT          = LaneTab<D, NDOF, NQ, NFL, NGEO>;
+  // 2D: divergent table reads from the lane-indexed copy; 3D keeps the kernel-parameter tables
+  // (its 96-cell blocks leave too little L1 next to their shared memory)
+  constexpr bool LTB       = (D == 2);
+  const T *__restrict__ lt = static_cast<const T *>(a.lt);
+  auto tVsf = [&](int f, int n) -> T {
+    if constexpr (LTB)
+      return ldt(lt + LT::VSF + n * NFL + f);
+    else
+      return tb.Vsf[f][n];
+  };
+  auto tV = [&](int q, int n) -> T {
+    if constexpr (LTB)
+      return ldt(lt + LT::V + n * NQ + q);
+    else
+      return tb.V[q][n];
+  };
+  auto tdVf = [&](int xi, int q, int f) -> T {
+    if constexpr (LTB)
+      return ldt(lt + LT::DVF + (xi * NFL + f) * NQ + q);
+    else
+      return tb.dVf[xi][q][f];
+  };
+  auto tdVq = [&](int xi, int q, int n) -> T { // lanes over points
+    if constexpr (LTB)
+      return ldt(lt + LT::DVQ + (xi * NDOF + n) * NQ + q);
+    else
+      return tb.dV[xi][q][n];
+  };
+  auto tdVn = [&](int xi, int q, int n) -> T { // lanes over nodes
+    if constexpr (LTB)
+      return ldt(lt + LT::DVN + (xi * NQ + q) * NDOF + n);
+    else
+      return tb.dV[xi][q][n];
+  };
+  auto tw = [&](int q) -> T {
+    if constexpr (LTB)
+      return ldt(lt + LT::W + q);
+    else
+      return tb.w[q];
+  };
   constexpr int CPB = NT / G; // cells per block
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -291,10 +370,17 @@ __global__ void __launch_bounds__(NT, MINB)
   }
   __syncwarp();
 
+  auto jac_q = [&](int q, T(&ij)[D][D]) -> T { // lanes over points
+    if constexpr (LTB)
+      return jacobian_lt<T, D, NQ, NGEO>(lt + LT::DVG, q, X, ij);
+    else
+      return jacobian_at(tb, q, X, ij);
+  };
+
   const T gamma = T(a.gamma);
   bool bad      = false;
 
-  // affine cells: one Jacobian for all points
+  // constant-Jacobian cells (simplices, parallelogram quadrilaterals): one Jacobian for all points
   T ijc[D][D];
   T detc = T(0);
   if (AFFINE)
@@ -310,7 +396,7 @@ __global__ void __launch_bounds__(NT, MINB)
     {
       T s[NEQ];
       {
-        const T c = tb.Vsf[f][0];
+        const T c = tVsf(f, 0);
 #pragma unroll
         for (int e = 0; e < NEQ; ++e)
           s[e] = c * T(su[e]);
@@ -318,7 +404,7 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
       for (int n = 1; n < NDOF; ++n)
       {
-        const T c = tb.Vsf[f][n];
+        const T c = tVsf(f, n);
 #pragma unroll
         for (int e = 0; e < NEQ; ++e)
           s[e] = s[e] + c * T(su[n * NEQ + e]);
@@ -350,7 +436,7 @@ __global__ void __launch_bounds__(NT, MINB)
     {
       T uq[NEQ];
       {
-        const T c = tb.V[q][0];
+        const T c = tV(q, 0);
 #pragma unroll
         for (int e = 0; e < NEQ; ++e)
           uq[e] = c * T(su[e]);
@@ -358,7 +444,7 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
       for (int n = 1; n < NDOF; ++n)
       {
-        const T c = tb.V[q][n];
+        const T c = tV(q, n);
 #pragma unroll
         for (int e = 0; e < NEQ; ++e)
           uq[e] = uq[e] + c * T(su[n * NEQ + e]);
@@ -378,7 +464,7 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
           for (int f = 0; f < NFL; ++f)
           {
-            const T c = tb.dVf[xi][q][f];
+            const T c = tdVf(xi, q, f);
 #pragma unroll
             for (int e = 0; e < NEQ; ++e)
               r[e] = r[e] + c * sfk[(f * NEQ + e) * D + xi];
@@ -391,13 +477,13 @@ __global__ void __launch_bounds__(NT, MINB)
       {
         // r_e = sum_ic sum_xi invJ[ic][xi] (sum_f dVf[xi][q][f] F[f][e][ic])
         T ij[D][D];
-        jacobian_at(tb, q, X, ij);
+        jac_q(q, ij);
         T dref[NEQ][D][D]; // [e][ic][xi]
 #pragma unroll
         for (int xi = 0; xi < D; ++xi)
         {
           {
-            const T c = tb.dVf[xi][q][0];
+            const T c = tdVf(xi, q, 0);
 #pragma unroll
             for (int e = 0; e < NEQ; ++e)
 #pragma unroll
@@ -407,7 +493,7 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
           for (int f = 1; f < NFL; ++f)
           {
-            const T c = tb.dVf[xi][q][f];
+            const T c = tdVf(xi, q, f);
 #pragma unroll
             for (int e = 0; e < NEQ; ++e)
 #pragma unroll
@@ -451,7 +537,7 @@ __global__ void __launch_bounds__(NT, MINB)
         const int f = c0 + fl;
         T s[NEQ];
         {
-          const T c = tb.Vsf[f][0];
+          const T c = tVsf(f, 0);
 #pragma unroll
           for (int e = 0; e < NEQ; ++e)
             s[e] = c * T(su[e]);
@@ -459,7 +545,7 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
         for (int n = 1; n < NDOF; ++n)
         {
-          const T c = tb.Vsf[f][n];
+          const T c = tVsf(f, n);
 #pragma unroll
           for (int e = 0; e < NEQ; ++e)
             s[e] = s[e] + c * T(su[n * NEQ + e]);
@@ -492,7 +578,7 @@ __global__ void __launch_bounds__(NT, MINB)
         {
           T uq[NEQ];
           {
-            const T c = tb.V[q][0];
+            const T c = tV(q, 0);
 #pragma unroll
             for (int e = 0; e < NEQ; ++e)
               uq[e] = c * T(su[e]);
@@ -500,7 +586,7 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
           for (int n = 1; n < NDOF; ++n)
           {
-            const T c = tb.V[q][n];
+            const T c = tV(q, n);
 #pragma unroll
             for (int e = 0; e < NEQ; ++e)
               uq[e] = uq[e] + c * T(su[n * NEQ + e]);
@@ -522,7 +608,7 @@ __global__ void __launch_bounds__(NT, MINB)
             for (int fl = 0; fl < NFC; ++fl)
               if (c0 + fl < NFL)
               {
-                const T c = tb.dVf[xi][q][c0 + fl];
+                const T c = tdVf(xi, q, c0 + fl);
 #pragma unroll
                 for (int e = 0; e < NEQ; ++e)
                   r[e] = r[e] + c * sfk[(fl * NEQ + e) * D + xi];
@@ -532,13 +618,13 @@ __global__ void __launch_bounds__(NT, MINB)
         {
           // r_e += sum_ic sum_xi invJ[ic][xi] (sum_f dVf[xi][q][f] F[f][e][ic])
           T ij[D][D];
-          jacobian_at(tb, q, X, ij);
+          jac_q(q, ij);
           T dref[NEQ][D][D]; // [e][ic][xi]
 #pragma unroll
           for (int xi = 0; xi < D; ++xi)
           {
             {
-              const T c = tb.dVf[xi][q][c0];
+              const T c = tdVf(xi, q, c0);
 #pragma unroll
               for (int e = 0; e < NEQ; ++e)
 #pragma unroll
@@ -549,7 +635,7 @@ __global__ void __launch_bounds__(NT, MINB)
             for (int fl = 1; fl < NFC; ++fl)
               if (c0 + fl < NFL)
               {
-                const T c = tb.dVf[xi][q][c0 + fl];
+                const T c = tdVf(xi, q, c0 + fl);
 #pragma unroll
                 for (int e = 0; e < NEQ; ++e)
 #pragma unroll
@@ -602,7 +688,7 @@ __global__ void __launch_bounds__(NT, MINB)
           ij[i][j] = ijc[i][j];
     }
     else
-      det = jacobian_at(tb, q, X, ij);
+      det = jac_q(q, ij);
     T uq[NEQ];
 #pragma unroll
     for (int e = 0; e < NEQ; ++e)
@@ -628,10 +714,10 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
       for (int x = 0; x < D; ++x)
       {
-        T acc = ij[x][0] * tb.dV[0][q][n];
+        T acc = ij[x][0] * tdVq(0, q, n);
 #pragma unroll
         for (int xi = 1; xi < D; ++xi)
-          acc = acc + ij[x][xi] * tb.dV[xi][q][n];
+          acc = acc + ij[x][xi] * tdVq(xi, q, n);
         gphys[x] = acc;
       }
       EulerKFactors<T, D> f;
@@ -678,7 +764,7 @@ __global__ void __launch_bounds__(NT, MINB)
       v[e]  = double(srq[q * NEQ + e]);
       ub[e] = SKu[e];
     }
-    phi0_l += double(tb.w[q] * det) * v[0];
+    phi0_l += double(tw(q) * det) * v[0];
     if constexpr (NEQ == 4)
       adj_solve4<SCHEME != RDS_PGLDA>(SK, v, ub);
     else
@@ -747,10 +833,10 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
         for (int x = 0; x < D; ++x)
         {
-          T acc = ij[x][0] * tb.dV[0][q][n];
+          T acc = ij[x][0] * tdVn(0, q, n);
 #pragma unroll
           for (int xi = 1; xi < D; ++xi)
-            acc = acc + ij[x][xi] * tb.dV[xi][q][n];
+            acc = acc + ij[x][xi] * tdVn(xi, q, n);
           gphys[x] = acc;
         }
         EulerKFactors<T, D> f;
@@ -880,10 +966,17 @@ cudaError_t launch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream_t
       return e;
     attr_set = true;
   }
-  if (g.affine)
-    k_aff<<<grid, NT, smem, s>>>(a, tb);
+  CellArgs al = a;
+  if constexpr (sizeof(T) == 8)
+    al.lt = g.d_lt64;
   else
-    k_gen<<<grid, NT, smem, s>>>(a, tb);
+    al.lt = g.d_lt32;
+  if (D == 2 && !al.lt)
+    return cudaErrorInvalidValue;
+  if (g.const_jac)
+    k_aff<<<grid, NT, smem, s>>>(al, tb);
+  else
+    k_gen<<<grid, NT, smem, s>>>(al, tb);
   return cudaGetLastError();
 }
 
@@ -950,6 +1043,40 @@ const char *euler_name(int physics, int scheme)
 }
 
 } // namespace
+
+void euler_lane_tables(const HostCellGroup &g, int dim, std::vector<double> &out)
+{
+  // the layout of LaneTab, with run-time sizes
+  const int D = dim, NDOF = g.desc.ndof, NQ = g.desc.nq, NFL = g.desc.nfl, NGEO = g.desc.ngeo;
+  out.assign((size_t)NDOF * NFL + (size_t)NDOF * NQ + (size_t)D * NFL * NQ + (size_t)D * NGEO * NQ +
+                 2 * (size_t)D * NDOF * NQ + NQ,
+             0.0);
+  size_t o = 0;
+  for (int n = 0; n < NDOF; ++n)
+    for (int f = 0; f < NFL; ++f)
+      out[o++] = g.Vsf[(size_t)f * NDOF + n];
+  for (int n = 0; n < NDOF; ++n)
+    for (int q = 0; q < NQ; ++q)
+      out[o++] = g.V[(size_t)q * NDOF + n];
+  for (int d = 0; d < D; ++d)
+    for (int f = 0; f < NFL; ++f)
+      for (int q = 0; q < NQ; ++q)
+        out[o++] = g.dVf[((size_t)d * NQ + q) * NFL + f];
+  for (int d = 0; d < D; ++d)
+    for (int k = 0; k < NGEO; ++k)
+      for (int q = 0; q < NQ; ++q)
+        out[o++] = g.dVgeo[((size_t)d * NQ + q) * NGEO + k];
+  for (int d = 0; d < D; ++d)
+    for (int n = 0; n < NDOF; ++n)
+      for (int q = 0; q < NQ; ++q)
+        out[o++] = g.dV[((size_t)d * NQ + q) * NDOF + n];
+  for (int d = 0; d < D; ++d)
+    for (int q = 0; q < NQ; ++q)
+      for (int n = 0; n < NDOF; ++n)
+        out[o++] = g.dV[((size_t)d * NQ + q) * NDOF + n];
+  for (int q = 0; q < NQ; ++q)
+    out[o++] = g.w[q];
+}
 
 cudaError_t launch_cells_euler(const HostCellGroup &g, const CellArgs &a, int physics, int scheme,
                                int precision, cudaStream_t s, const char **name, bool *ok)

@@ -75,6 +75,7 @@ struct HostCellGroup
   long long slot_base = 0;       // first contribution slot of this group
   long long ws_base   = 0;       // first wave-speed slot of this group
   bool affine         = false;   // simplex with straight edges: Jacobian constant per cell
+  bool const_jac      = false;   // every cell's Jacobian constant (simplices, parallelograms)
   int physics         = 0;       // physics / scheme of this group's cells
   int scheme          = 0;
   // batched problems: cells of problem p are [cbeg[p], cend[p]) of this group
@@ -83,6 +84,8 @@ struct HostCellGroup
   int tune_tile[2] = {128, 128}; // cells per CTA tile (phase 0 FP32, phase 1 FP64)
   int tune_grid[2] = {0, 0};     // persistent grid (CTAs), 0: 4 per SM
   float *d_tc      = nullptr;    // tensor-core tables of the FP32 kernel (rds_cells_scalar_tc.cu)
+  double *d_lt64   = nullptr;    // lane-indexed tables of the Euler kernels (FP64, FP32)
+  float *d_lt32    = nullptr;
 };
 
 struct HostBC
@@ -187,6 +190,7 @@ struct CellArgs
   double *theta;   // PGB: the cell's blending coefficient [ncells] when not null (Jacobians)
   const double *blend; // PGB: external nodal blending coefficient [nnodes] when not null
   int pdl;         // launch with programmatic dependent launch (loop graphs)
+  const void *lt;  // Euler cells: lane-indexed tables in the kernel's precision (set at launch)
 };
 
 // FP32 correction sweep of the defect-correction loop (rds_cells_scalar_dc.cu): the change of
@@ -207,6 +211,7 @@ struct DcCellArgs
   const int *stop;
   BatchTileMap bt; // batch form only
   int pdl;         // launch with programmatic dependent launch (loop graphs)
+  const void *lt;  // Euler cells: lane-indexed tables in the kernel's precision (set at launch)
 };
 
 struct BCArgs
@@ -307,6 +312,9 @@ cudaError_t launch_cell_volume_raw(int ncells, int dim, int nq, int ngeo, const 
 cudaError_t launch_cells_scalar(const HostCellGroup &g, const CellArgs &a, int physics,
                                 int scheme, int precision, cudaStream_t s, const char **name,
                                 bool *ok);
+// lane-indexed tables of an Euler cell group (rds_cells_euler.cu); empty for other shapes
+void euler_lane_tables(const HostCellGroup &g, int dim, std::vector<double> &out);
+
 cudaError_t launch_cells_euler(const HostCellGroup &g, const CellArgs &a, int physics,
                                int scheme, int precision, cudaStream_t s, const char **name,
                                bool *ok);
