@@ -166,35 +166,37 @@ def scalar_flops(physics, scheme, ndof, nq, nfl):
     return fl + nq * per_q + (27 if scheme == "b" else 5)
 
 
-def euler_flops(dim, neq, ndof, nq, nfl, ngeo, scheme):
-    """Count of one Euler cell in the form the kernel evaluates (affine = straight-sided
-    triangle / tetrahedron):
-      geometry    (1 if affine else nq) (2 D^2 ngeo + c_invJ)        c_invJ 10 (2D) / 60 (3D)
-      flux nodes  nfl (2 NEQ ndof + c_props + c_flux                 state, properties, flux
-                       + 2 NEQ D^2 if affine)                        flux contracted with invJ
-      points      nq (2 NEQ ndof                                     u_q
-                      + 2 NEQ D nfl (affine) or 2 NEQ D (D nfl + D)  flux divergence
-                      + c_props + c_ac + c_solve                     state, acoustic factors,
-                                                                     (sum K+)^-1 [r, sum K+ u]
-                      + ndof (2 D^2 + c_K + 5 NEQ^2 + 2 NEQ)         grad phi, K+ (split form),
-                                                                     sum K+, sum K+ u, LDA part
-                      + ndof (2 NEQ^2 + 3 NEQ) for N / B)            N dissipation
-      c_props 20 / 22, c_flux 12 / 24, c_ac 15 / 17, c_K 110 / 150, c_solve 190 (adjugate) /
-      165 (LU) for 2D / 3D.
-    Configuration 3: 50,914 (P3 triangle, 16 points) and 134,675 (P3 quadrilateral, 25
-    points); configuration 4: 59,928 (P2 tetrahedron, 14 points, LDA)."""
-    affine = (dim == 2 and ngeo == 3) or (dim == 3 and ngeo == 4)
-    c_invj, c_props, c_flux, c_ac, c_k, c_solve = (10, 20, 12, 15, 110, 190) if dim == 2 else \
-        (60, 22, 24, 17, 150, 165)
-    f = (1 if affine else nq) * (2 * dim * dim * ngeo + c_invj)
-    f += nfl * (2 * neq * ndof + c_props + c_flux + (2 * neq * dim * dim if affine else 0))
+def euler_flops(dim, neq, ndof, nq, nfl, ngeo, scheme, const_jac=None):
+    """Count of one Euler cell in the algorithm the kernel evaluates, each quantity counted once
+    (the kernel's second evaluation of the upwind factors and point states in its node pass is
+    not counted):
+      geometry    (1 if const_jac else nq) (2 D^2 ngeo + c_invJ)      c_invJ 10 (2D) / 60 (3D)
+      flux nodes  nfl (2 NEQ ndof + c_props + c_flux                  state, properties, flux
+                       + 2 NEQ D^2 if const_jac)                      flux contracted with invJ
+      points      nq (2 NEQ ndof                                      u_q
+                      + 2 NEQ D nfl (const_jac) or 2 NEQ D (D nfl + D)  flux divergence
+                      + c_props + c_ac + c_solve + 2)                 state, acoustic factors,
+                                                                      (sum K+)^-1 [r, sum K+ u]
+      point-node  nq ndof (2 D^2 + c_F + 4 NEQ^2 + NEQ + 11 NEQ       grad phi, upwind factors,
+                           + 24 NEQ for N / B)                        sum K+, K+ v (factored),
+                                                                      sum K+ du, K+ (u - u_bar)
+      c_props 20 / 22, c_flux 12 / 24, c_ac 15 / 17, c_F 58 / 69, c_solve 190 (adjugate) / 165
+      (LU) for 2D / 3D. const_jac defaults to straight-sided simplices.
+    Configuration 3: 54,786 (P3 triangle, 16 points) and 144,325 (P3 quadrilateral on the bump,
+    25 points); configuration 4: 52,116 (P2 tetrahedron, 14 points, LDA)."""
+    if const_jac is None:
+        const_jac = (dim == 2 and ngeo == 3) or (dim == 3 and ngeo == 4)
+    c_invj, c_props, c_flux, c_ac, c_f, c_solve = (10, 20, 12, 15, 58, 190) if dim == 2 else \
+        (60, 22, 24, 17, 69, 165)
+    f = (1 if const_jac else nq) * (2 * dim * dim * ngeo + c_invj)
+    f += nfl * (2 * neq * ndof + c_props + c_flux + (2 * neq * dim * dim if const_jac else 0))
     per_q = 2 * neq * ndof
-    per_q += 2 * neq * dim * nfl if affine else 2 * neq * dim * (dim * nfl + dim)
-    per_q += c_props + c_ac + c_solve
-    per_q += ndof * (2 * dim * dim + c_k + 5 * neq * neq + 2 * neq)
+    per_q += 2 * neq * dim * nfl if const_jac else 2 * neq * dim * (dim * nfl + dim)
+    per_q += c_props + c_ac + c_solve + 2
+    per_qn = 2 * dim * dim + c_f + 4 * neq * neq + neq + 11 * neq
     if scheme != "lda":
-        per_q += ndof * (2 * neq * neq + 3 * neq)
-    return f + nq * per_q
+        per_qn += 24 * neq
+    return f + nq * per_q + nq * ndof * per_qn
 
 
 def dc_flops(physics, scheme, ndof, nq, nfl):
@@ -814,9 +816,9 @@ def measure_stab(args, solver, prob, u0, cfl, steps, flush, world):
 
 def run_partitioned(args, rank, world, local):
     """c1-c4 with the one mesh split over the ranks (pdekit_b200.partition): per step every rank
-    assembles its cells, the interface sums are all-reduced, every rank updates its nodes and the
-    norm parts are all-reduced. Strong scaling: value = the whole mesh's cells x steps / the
-    slowest rank's time."""
+    assembles the cells at its interface, all-reduces the interface sums while it assembles the
+    rest, updates its nodes and all-reduces the norm parts; the step is one CUDA graph replay.
+    Strong scaling: value = the whole mesh's cells x steps / the slowest rank's time."""
     import torch
 
     from pdekit_b200.partition import PartitionedRDS
@@ -827,25 +829,26 @@ def run_partitioned(args, rank, world, local):
     pr.set_solution(u0)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
     for _ in range(max(args.warmup, 3)):
-        pr.step(cfl)
+        pr.graph_step(cfl, norm=False)  # captures the graph of the timed steps
     torch.cuda.synchronize()
     pr.set_solution(u0)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(steps)]
     barrier(world)
     torch.cuda.synchronize()
-    launches0 = pr.rank.solver.launch_count()
+    launches0 = pr.rank.solver.launch_count() + pr.graph_launches
     with ClockSampler(local) as clk:
         with torch.cuda.stream(pr.rank.stream):
             for k in range(steps):
                 flush.zero_()
                 ev[k][0].record(pr.rank.stream)
-                pr.step(cfl)
+                pr.graph_step(cfl, norm=False)  # the work of the fused step (rds_run)
                 ev[k][1].record(pr.rank.stream)
         torch.cuda.synchronize()
     barrier(world)
-    launches = pr.rank.solver.launch_count() - launches0
+    launches = pr.rank.solver.launch_count() + pr.graph_launches - launches0
     ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world)
+    pr.graph_step(cfl)  # one more step with its norm (reported, not timed)
     norm = pr.norm()
     part = pr.partition.parts[rank]
     line = {"metric": "cell-residual updates/s", "value": prob.ncells * steps / (ms * 1e-3),
@@ -856,7 +859,10 @@ def run_partitioned(args, rank, world, local):
                        "l2": "L2 flushed (256 MB write) before every timed step",
                        "parallelism": f"one mesh split over {world} ranks along x "
                                       f"({pr.partition.nslots:,} interface nodes), interface "
-                                      "sums all-reduced per step"},
+                                      "sums all-reduced per step while the interior cells "
+                                      "run, one CUDA graph per step; timed steps write the "
+                                      "norm's block sums without adding them, like the fused "
+                                      "step"},
             "final_norm": [float(x) for x in norm], "clocks": clk.summary(),
             "gpu_launches": int(launches),
             "cells_rank0": int(sum(len(c) for c in part.cells))}

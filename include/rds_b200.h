@@ -302,6 +302,34 @@ RDS_API rds_status rds_set_interface(rds_ctx *ctx, int n, const int32_t *nodes,
 RDS_API rds_status rds_pack_interface(rds_ctx *ctx, double *buf);
 RDS_API rds_status rds_unpack_interface(rds_ctx *ctx, const double *buf);
 RDS_API rds_status rds_finish(rds_ctx *ctx, double cfl, int update, double *sq);
+
+/* The assembly of rds_assemble_rhs in two parts, so that a partitioned iteration can send the
+ * interface sums while the remaining cells run (local node numbering with the interface nodes
+ * first, each cell group split into the cells touching an interface node and the rest):
+ *   rds_assemble_rhs_cells: the cell kernels of groups [g0, g1) and, when with_bcs != 0, the
+ *     weak boundary conditions; no nodal sums.
+ *   rds_gather_rhs: the nodal sums of residual and wave speed of nodes [v0, v1) from the
+ *     contribution slots (every cell and facet of those nodes must have run).
+ * rds_assemble_rhs_cells(ctx, 0, ngroups, 1) then rds_gather_rhs(ctx, 0, nnodes) is
+ * rds_assemble_rhs. Reference: the cell loop and nodal sums of PGRDMethodExplicit::assemble_rhs
+ * (PGRDMethodExplicit.hpp:428-463, PGRDMExplicitCellWorker.hpp:549-567). */
+RDS_API rds_status rds_assemble_rhs_cells(rds_ctx *ctx, int g0, int g1, int with_bcs);
+RDS_API rds_status rds_gather_rhs(rds_ctx *ctx, int v0, int v1);
+
+/* The finish of a partitioned iteration in two node ranges: the nodes whose sums are complete on
+ * this rank finish right after their gather, the interface nodes after the exchange.
+ *   rds_gather_finish: nodal sums of nodes [v0, v1), dt = CFL V / ws, u -= dt res, and their
+ *     block sums of (res dt)^2 (all of them counted: nodes outside the interface are this
+ *     rank's own); with sq (device, neq doubles) non-null, also their sum into sq (for a rank
+ *     without interface nodes, which then needs no rds_finish_nodes).
+ *   rds_finish_nodes: rds_finish for nodes [v0, v1) (owned ones in the norm); sq[neq] (device)
+ *     = the sum of its and the preceding rds_gather_finish's block sums, in a fixed order (sq
+ *     null: the block sums only, for a step whose norm is not needed).
+ * rds_finish(ctx, cfl, update, sq) is rds_finish_nodes(ctx, cfl, update, 0, nnodes, sq) without
+ * a preceding rds_gather_finish. */
+RDS_API rds_status rds_gather_finish(rds_ctx *ctx, int v0, int v1, double cfl, double *sq);
+RDS_API rds_status rds_finish_nodes(rds_ctx *ctx, double cfl, int update, int v0, int v1,
+                                    double *sq);
 RDS_API rds_status rds_check(rds_ctx *ctx);
 
 /* Copy out any of: residual [node][neq], dt [node], nodal wave speed [node], dual volume [node]

@@ -143,6 +143,10 @@ struct rds_ctx
   bool dc_ok         = false;
   int dc_m           = 32;
   int dc_phase       = 0; // launch_residual_kernels: 0 plain, 1 exact DC sweep, 2 correction
+  int part_used      = 0;     // norm partials written by rds_gather_finish (partitioned)
+  int grp_beg        = 0;     // launch_residual_kernels: cell groups [grp_beg, grp_end)
+  int grp_end        = -1;    //   (-1: all) and the weak conditions unless no_bcs
+  bool no_bcs        = false;
   // loop graphs: the main-stream kernels of an iteration (first cell group, gather) with
   // programmatic dependent launch (option "loop_pdl", default off: measured no gain on the
   // configurations, whose critical path runs through the side-stream boundary kernels)
@@ -437,7 +441,8 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
   bool strong = false;
   for (const HostBC &b : ctx->bcs)
     strong |= b.desc.kind == RDS_BC_STRONG_DIRICHLET;
-  const bool fork = !ctx->bcs.empty() && !strong;
+  const bool with_bcs = !ctx->bcs.empty() && !ctx->no_bcs;
+  const bool fork     = with_bcs && !strong;
   // stream of the k-th condition: all on s (in order), or one side stream each when forked
   auto launch_bcs = [&](cudaStream_t s, bool spread) -> rds_status {
     for (size_t k = 0; k < ctx->bcs.size(); ++k)
@@ -463,7 +468,8 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
     if (st != RDS_OK)
       return st;
   }
-  for (size_t ig = 0; ig < ctx->groups.size(); ++ig)
+  const size_t gend = ctx->grp_end < 0 ? ctx->groups.size() : (size_t)ctx->grp_end;
+  for (size_t ig = (size_t)ctx->grp_beg; ig < gend; ++ig)
   {
     const HostCellGroup &g = ctx->groups[ig];
     CellArgs a             = cell_args(ctx, g, stop);
@@ -523,7 +529,7 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
   }
   if (fork)
     return join_sides(ctx);
-  if (!ctx->bcs.empty())
+  if (with_bcs)
     return launch_bcs(ctx->stream, false);
   return RDS_OK;
 }
@@ -1016,7 +1022,7 @@ rds_status rds_finalize(rds_ctx *ctx)
       (st = dalloc(ctx, &ctx->d_contrib, (size_t)S * NEQ)) || (st = dalloc(ctx, &ctx->d_wsc, W)) ||
       (st = dalloc(ctx, &ctx->d_stage, (size_t)N * NEQ)) || (st = dalloc(ctx, &ctx->d_row, N + 1)) ||
       (st = dalloc(ctx, &ctx->d_ent_slot, E)) || (st = dalloc(ctx, &ctx->d_ent_ws, E)) ||
-      (st = dalloc(ctx, &ctx->d_part, (size_t)ctx->gblocks * NEQ)) ||
+      (st = dalloc(ctx, &ctx->d_part, (size_t)(ctx->gblocks + 1) * NEQ)) || // +1: two node ranges
       (st = dalloc(ctx, &ctx->d_norm, NEQ)) || (st = dalloc(ctx, &ctx->d_norm0, NEQ)) ||
       (st = dalloc(ctx, &ctx->d_iter, 1)) || (st = dalloc(ctx, &ctx->d_stop, 1)) ||
       (st = dalloc(ctx, &ctx->d_zero, 1)) || (st = dalloc(ctx, &ctx->d_status, 1)) ||
@@ -1218,6 +1224,39 @@ rds_status rds_assemble(rds_ctx *ctx, double cfl)
 rds_status rds_assemble_rhs(rds_ctx *ctx)
 {
   return assemble_impl(ctx, 0.0, 0);
+}
+
+rds_status rds_assemble_rhs_cells(rds_ctx *ctx, int g0, int g1, int with_bcs)
+{
+  if (!ctx || !ctx->finalized)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "not finalized") : RDS_ERR_INVALID;
+  if (g0 < 0 || g1 < g0 || g1 > (int)ctx->groups.size())
+    return fail(ctx, RDS_ERR_INVALID, "rds_assemble_rhs_cells: group range out of bounds");
+  ctx->grp_beg         = g0;
+  ctx->grp_end         = g1;
+  ctx->no_bcs          = with_bcs == 0;
+  const rds_status st  = launch_residual_kernels(ctx, ctx->d_zero);
+  ctx->grp_beg         = 0;
+  ctx->grp_end         = -1;
+  ctx->no_bcs          = false;
+  return st;
+}
+
+rds_status rds_gather_rhs(rds_ctx *ctx, int v0, int v1)
+{
+  if (!ctx || !ctx->finalized)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "not finalized") : RDS_ERR_INVALID;
+  if (v0 < 0 || v1 < v0 || v1 > ctx->desc.nnodes)
+    return fail(ctx, RDS_ERR_INVALID, "rds_gather_rhs: node range out of bounds");
+  if (v1 == v0)
+    return RDS_OK;
+  GatherArgs ga = gather_args(ctx, 0.0, ctx->d_zero);
+  ga.vbeg       = v0;
+  ga.vend       = v1;
+  const int nb  = (v1 - v0 + kGBlock - 1) / kGBlock;
+  return launch(ctx, [&](const char **name) {
+    return launch_gather(ga, 0, nb, ctx->stream, name);
+  });
 }
 
 rds_status rds_update(rds_ctx *ctx)
@@ -1820,6 +1859,8 @@ rds_status rds_pack_interface(rds_ctx *ctx, double *buf)
     return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_pack_interface: rds_set_interface first")
                : RDS_ERR_INVALID;
   const int NEQ = ctx->desc.neq;
+  if (ctx->n_slots == 0)
+    return RDS_OK; // nothing is exchanged (one rank)
   return launch(ctx, [&](const char **name) {
     *name = "pack_interface";
     return launch_pack_interface(ctx->n_if, NEQ, ctx->desc.nnodes, ctx->d_if_nodes,
@@ -1842,14 +1883,51 @@ rds_status rds_unpack_interface(rds_ctx *ctx, const double *buf)
 
 rds_status rds_finish(rds_ctx *ctx, double cfl, int update, double *sq)
 {
-  if (!ctx || !sq || !ctx->d_owned)
+  if (ctx && !sq)
+    return fail(ctx, RDS_ERR_INVALID, "rds_finish: sq is null");
+  if (ctx)
+    ctx->part_used = 0;
+  return rds_finish_nodes(ctx, cfl, update, 0, ctx ? ctx->desc.nnodes : 0, sq);
+}
+
+rds_status rds_gather_finish(rds_ctx *ctx, int v0, int v1, double cfl, double *sq)
+{
+  if (!ctx || !ctx->finalized)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "not finalized") : RDS_ERR_INVALID;
+  if (v0 < 0 || v1 < v0 || v1 > ctx->desc.nnodes)
+    return fail(ctx, RDS_ERR_INVALID, "rds_gather_finish: node range out of bounds");
+  ctx->part_used = 0;
+  if (v1 == v0)
+    return RDS_OK;
+  GatherArgs ga = gather_args(ctx, cfl, ctx->d_zero);
+  ga.vbeg       = v0;
+  ga.vend       = v1;
+  ga.sq_out     = sq;
+  ga.counter    = ctx->d_counter; // last-block-done (with sq)
+  const int nb  = (v1 - v0 + kGBlock - 1) / kGBlock;
+  // sums, dt, update, block sums of (res dt)^2; with sq, also their sum (last block)
+  const rds_status st = launch(ctx, [&](const char **name) {
+    return launch_gather(ga, sq ? 15 : 7, nb, ctx->stream, name);
+  });
+  if (st == RDS_OK && !sq)
+    ctx->part_used = nb;
+  return st;
+}
+
+rds_status rds_finish_nodes(rds_ctx *ctx, double cfl, int update, int v0, int v1, double *sq)
+{
+  if (!ctx || !ctx->d_owned)
     return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_finish: rds_set_interface first")
                : RDS_ERR_INVALID;
+  if (v0 < 0 || v1 < v0 || v1 > ctx->desc.nnodes)
+    return fail(ctx, RDS_ERR_INVALID, "rds_finish_nodes: node range out of bounds");
+  const int off  = ctx->part_used;
+  ctx->part_used = 0;
   return launch(ctx, [&](const char **name) {
     *name = "finish_nodes";
-    return launch_finish(ctx->desc.nnodes, ctx->desc.neq, cfl, update, ctx->d_vol, ctx->d_ws,
-                         ctx->d_res, ctx->d_dt, ctx->d_u, ctx->d_owned, ctx->d_part, sq,
-                         ctx->stream);
+    return launch_finish(v0, v1, ctx->desc.nnodes, ctx->desc.neq, cfl, update, ctx->d_vol,
+                         ctx->d_ws, ctx->d_res, ctx->d_dt, ctx->d_u, ctx->d_owned, ctx->d_part,
+                         off, ctx->d_counter, sq, ctx->stream);
   });
 }
 

@@ -214,12 +214,12 @@ __global__ void __launch_bounds__(kGBlock) gather_nodes(const __grid_constant__ 
   pdl_wait_and_release();
   if (*a.stop)
     return;
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  const int v = a.vbeg + blockIdx.x * blockDim.x + threadIdx.x;
   double sq[NEQ];
 #pragma unroll
   for (int e = 0; e < NEQ; ++e)
     sq[e] = 0.0;
-  if (v < a.nnodes)
+  if (v < (a.vend > 0 ? a.vend : a.nnodes))
     gather_node<NEQ, DT, UPDATE, NORM, RK, DC>(a, v, a.loop ? a.loop->cfl : a.cfl, sq);
   if (NORM)
   {
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(kGBlock) gather_nodes(const __grid_constant__ 
     {
       const double s = block_sum<kGBlock>(sq[e], smem);
       if (threadIdx.x == 0)
-        a.part[(size_t)blockIdx.x * NEQ + e] = s;
+        a.part[(size_t)(a.part_off + blockIdx.x) * NEQ + e] = s;
     }
     if (FINAL)
     {
@@ -246,10 +246,27 @@ __global__ void __launch_bounds__(kGBlock) gather_nodes(const __grid_constant__ 
       if (last)
       {
         __threadfence();
-        const int max_iter = a.loop ? a.loop->max_iter : a.max_iter;
-        const double drop  = a.loop ? a.loop->drop : a.drop;
-        reduce_final(a.part, gridDim.x, NEQ, a.nnodes, a.norm, a.norm0, a.hist, a.iter,
-                     max_iter, drop, a.stop_w, a.status, smem, nv, a.stall, a.loop);
+        if (a.sq_out)
+        {
+          // partitioned form: the plain sum of the block sums (fixed order) for the caller
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e)
+          {
+            double t = 0.0;
+            for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+              t += a.part[(size_t)(a.part_off + b) * NEQ + e];
+            t = block_sum<kGBlock>(t, smem);
+            if (threadIdx.x == 0)
+              a.sq_out[e] = t;
+          }
+        }
+        else
+        {
+          const int max_iter = a.loop ? a.loop->max_iter : a.max_iter;
+          const double drop  = a.loop ? a.loop->drop : a.drop;
+          reduce_final(a.part, gridDim.x, NEQ, a.nnodes, a.norm, a.norm0, a.hist, a.iter,
+                       max_iter, drop, a.stop_w, a.status, smem, nv, a.stall, a.loop);
+        }
         if (threadIdx.x == 0)
           *a.counter = 0u;
       }

@@ -246,6 +246,9 @@ struct GatherArgs
 {
   int nnodes;
   int neq;
+  int vbeg, vend; // node range of the launch (vend 0: all nodes)
+  int part_off;    // first block partial written (norm modes)
+  double *sq_out;  // fused final (mode bit 3) when set: the plain sum of the block sums here
   const int32_t *__restrict__ row;     // [nnodes+1]
   const int32_t *__restrict__ ent_slot; // [E]
   const int32_t *__restrict__ ent_ws;   // [E]
@@ -359,9 +362,10 @@ cudaError_t launch_pack_interface(int n, int neq, int nnodes, const int32_t *nod
 cudaError_t launch_unpack_interface(int n, int neq, int nnodes, const int32_t *nodes,
                                     const int32_t *slots, const double *buf, double *res,
                                     double *ws, cudaStream_t s);
-cudaError_t launch_finish(int nnodes, int neq, double cfl, int update, const double *vol,
-                          const double *ws, const double *res, double *dt, double *u,
-                          const uint8_t *owned, double *part, double *sq, cudaStream_t s);
+cudaError_t launch_finish(int v0, int v1, int nnodes, int neq, double cfl, int update,
+                          const double *vol, const double *ws, const double *res, double *dt,
+                          double *u, const uint8_t *owned, double *part, int part_off,
+                          unsigned *counter, double *sq, cudaStream_t s);
 
 // stabilisation operators (rds_stab.cu)
 constexpr int kStabMaxGroups = 8;

@@ -8,7 +8,11 @@
 //            (the buffer is zeroed first, so a sum over the ranks' buffers is the full sum)
 //   unpack   res[.][v], ws[v] = buf[slot] (after the sum over the ranks)
 //   finish   dt = CFL V / ws, u -= dt res, and per block the sum over the nodes this rank owns
-//            of (res dt)^2; a one-block pass adds the block sums in a fixed order.
+//            of (res dt)^2 (for a node range, after the block sums of the other nodes that
+//            rds_gather_finish wrote); the block that finishes last adds the block sums in a
+//            fixed order.
+
+#include <algorithm>
 
 #include "rds_internal.h"
 
@@ -67,14 +71,16 @@ __device__ __forceinline__ double sum_over_block(double v, double *smem)
 }
 
 __global__ void __launch_bounds__(kGBlock)
-    finish_nodes(int nnodes, int neq, double cfl, int update, const double *__restrict__ vol,
-                 const double *__restrict__ ws, const double *__restrict__ res,
-                 double *__restrict__ dt, double *__restrict__ u,
-                 const uint8_t *__restrict__ owned, double *__restrict__ part)
+    finish_nodes(int v0, int v1, int nnodes, int neq, double cfl, int update,
+                 const double *__restrict__ vol, const double *__restrict__ ws,
+                 const double *__restrict__ res, double *__restrict__ dt, double *__restrict__ u,
+                 const uint8_t *__restrict__ owned, double *__restrict__ part, int part_off,
+                 unsigned *counter, double *__restrict__ sq_out)
 {
   __shared__ double smem[kGBlock / 32];
-  const int v   = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool in = v < nnodes;
+  __shared__ bool last;
+  const int v   = v0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in = v < v1;
   double dtv    = 0.0;
   if (in)
   {
@@ -100,23 +106,33 @@ __global__ void __launch_bounds__(kGBlock)
     }
     const double s = sum_over_block(sq, smem);
     if (threadIdx.x == 0)
-      part[(size_t)blockIdx.x * neq + e] = s;
+      part[(size_t)(part_off + blockIdx.x) * neq + e] = s;
   }
-}
-
-__global__ void __launch_bounds__(kGBlock)
-    sum_partials(const double *__restrict__ part, int nblocks, int neq, double *__restrict__ out)
-{
-  __shared__ double smem[kGBlock / 32];
+  // last-block-done: the block that finishes last adds all block sums in a fixed order (those
+  // of a preceding rds_gather_finish first); no block waits for another
+  if (!sq_out)
+    return;
+  if (threadIdx.x == 0)
+  {
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last)
+    return;
+  __threadfence();
+  const int nb = part_off + (int)gridDim.x;
   for (int e = 0; e < neq; ++e)
   {
-    double s = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-      s += part[(size_t)b * neq + e];
-    s = sum_over_block(s, smem);
+    double t = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+      t += part[(size_t)b * neq + e];
+    t = sum_over_block(t, smem);
     if (threadIdx.x == 0)
-      out[e] = s;
+      sq_out[e] = t;
   }
+  if (threadIdx.x == 0)
+    *counter = 0u;
 }
 
 } // namespace
@@ -144,16 +160,15 @@ cudaError_t launch_unpack_interface(int n, int neq, int nnodes, const int32_t *n
   return cudaGetLastError();
 }
 
-cudaError_t launch_finish(int nnodes, int neq, double cfl, int update, const double *vol,
-                          const double *ws, const double *res, double *dt, double *u,
-                          const uint8_t *owned, double *part, double *sq, cudaStream_t s)
+cudaError_t launch_finish(int v0, int v1, int nnodes, int neq, double cfl, int update,
+                          const double *vol, const double *ws, const double *res, double *dt,
+                          double *u, const uint8_t *owned, double *part, int part_off,
+                          unsigned *counter, double *sq, cudaStream_t s)
 {
-  const int nb = (nnodes + kGBlock - 1) / kGBlock;
-  finish_nodes<<<nb, kGBlock, 0, s>>>(nnodes, neq, cfl, update, vol, ws, res, dt, u, owned, part);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess)
-    return e;
-  sum_partials<<<1, kGBlock, 0, s>>>(part, nb, neq, sq);
+  // at least one block: with an empty range it only adds the preceding block sums
+  const int nb = std::max(1, (v1 - v0 + kGBlock - 1) / kGBlock);
+  finish_nodes<<<nb, kGBlock, 0, s>>>(v0, v1, nnodes, neq, cfl, update, vol, ws, res, dt, u,
+                                      owned, part, part_off, counter, sq);
   return cudaGetLastError();
 }
 

@@ -20,6 +20,18 @@ interface nodes are summed over the ranks once, the same way. Results equal the 
 ones up to the order in which the partial sums of interface nodes are added (rounding).
 Strong Dirichlet conditions are not supported in this form (each rank would have to write its
 copies of the shared dofs the same way).
+
+The exchange overlaps the interior of the mesh: each rank numbers its interface nodes first and
+splits every cell group into the cells touching an interface node and the rest, so that
+
+    interface cells + facets, sums of the interface nodes, pack      (rds_assemble_rhs_cells,
+                                                                      rds_gather_rhs)
+    sum over the ranks of the buffer  ||  interior cells; the other nodes' sums, dt, update and
+                                          norm parts                 (rds_gather_finish)
+    unpack, finish of the interface nodes, norm parts of the rank    (rds_finish_nodes)
+    sum over the ranks of the norm parts
+
+and a step (its NCCL calls included) is captured once in a CUDA graph and replayed.
 """
 
 from __future__ import annotations
@@ -42,6 +54,7 @@ class RankPart:
     if_slots: np.ndarray  # [n_if] their slots in the exchange buffer
     owned: np.ndarray  # [n_local] uint8, 1 where this rank counts the node in the norm
     cells: list  # per group: global cell indices of this rank (ascending)
+    n_if_groups: int = 0  # local groups [0, n_if_groups) hold the cells touching interface nodes
 
 
 @dataclasses.dataclass
@@ -100,19 +113,25 @@ def partition(prob: Problem, nparts: int) -> Partition:
             h = np.where(has & (h == nparts), r, h)
         holder.append(h)
 
+    is_if = np.zeros(prob.nnodes, dtype=bool)
+    is_if[iface] = True
     parts = []
     for r, ns in enumerate(node_sets):
+        # local numbering: this rank's interface nodes first
+        ns = np.concatenate([ns[is_if[ns]], ns[~is_if[ns]]])
         loc = np.full(prob.nnodes, -1, dtype=np.int64)
         loc[ns] = np.arange(len(ns))
-        groups, cells = [], []
+        groups_if, groups_in, cells = [], [], []
         for ig, g in enumerate(prob.groups):
             cid = np.flatnonzero(rank_of[offs[ig]:offs[ig + 1]] == r)
             cells.append(cid)
-            if len(cid) == 0:
-                continue
-            groups.append(dataclasses.replace(
-                g, sol_conn=loc[g.sol_conn[cid]].astype(np.int32),
-                geo_conn=np.ascontiguousarray(g.geo_conn[cid])))
+            touch = is_if[g.sol_conn[cid]].any(axis=1)
+            for sel, out in ((cid[touch], groups_if), (cid[~touch], groups_in)):
+                if len(sel):
+                    out.append(dataclasses.replace(
+                        g, sol_conn=loc[g.sol_conn[sel]].astype(np.int32),
+                        geo_conn=np.ascontiguousarray(g.geo_conn[sel])))
+        groups = groups_if + groups_in
         bcs = []
         for b, h in zip(prob.bcs, holder):
             fid = np.flatnonzero(h == r)
@@ -125,11 +144,13 @@ def partition(prob: Problem, nparts: int) -> Partition:
         local = Problem(physics=prob.physics, scheme=prob.scheme, dim=prob.dim, neq=prob.neq,
                         nnodes=len(ns), geo_coords=prob.geo_coords, groups=groups, bcs=bcs,
                         adv=prob.adv, gamma=prob.gamma)
-        ifl = loc[np.intersect1d(ns, iface)]
+        n_if = int(is_if[ns].sum())
+        ifl = np.arange(n_if)
         parts.append(RankPart(rank=r, problem=local, nodes=ns,
                               if_nodes=ifl.astype(np.int32),
                               if_slots=slot_of[ns[ifl]].astype(np.int32),
-                              owned=(first[ns] == r).astype(np.uint8), cells=cells))
+                              owned=(first[ns] == r).astype(np.uint8), cells=cells,
+                              n_if_groups=len(groups_if)))
     return Partition(parts=parts, nslots=len(iface), nnodes=prob.nnodes)
 
 
@@ -172,18 +193,43 @@ class RankSolver:
         self.solver.set_solution(np.asarray(u_global).reshape(-1, self.part.problem.neq)[
             self.part.nodes])
 
-    def assemble_and_pack(self):
-        """Partial residual and wave speed of this rank; the interface values into self.buf."""
-        self._check(lib().rds_assemble_rhs(self.solver._ctx))
-        self._check(lib().rds_pack_interface(self.solver._ctx,
-                                             C.c_void_p(self.buf.data_ptr())))
+    def assemble_interface(self):
+        """Cells touching interface nodes and the boundary facets, the sums of the interface
+        nodes (this rank's parts), those into self.buf."""
+        ctx, p = self.solver._ctx, self.part
+        if len(p.if_nodes) == 0:
+            return  # the facets then run beside the interior cells
+        self._check(lib().rds_assemble_rhs_cells(ctx, 0, p.n_if_groups, 1))
+        self._check(lib().rds_gather_rhs(ctx, 0, len(p.if_nodes)))
+        self._check(lib().rds_pack_interface(ctx, C.c_void_p(self.buf.data_ptr())))
 
-    def unpack_and_finish(self, cfl: float, update: bool = True):
-        """Full sums from self.buf, then dt, update and this rank's norm part into self.sq."""
-        self._check(lib().rds_unpack_interface(self.solver._ctx,
-                                               C.c_void_p(self.buf.data_ptr())))
-        self._check(lib().rds_finish(self.solver._ctx, float(cfl), int(update),
-                                     C.c_void_p(self.sq.data_ptr())))
+    def assemble_interior(self, cfl: float, norm: bool = True):
+        """The other cells, and the other nodes (complete on this rank) finished: their sums,
+        dt, update and block sums of (res dt)^2."""
+        ctx, p = self.solver._ctx, self.part
+        alone = len(p.if_nodes) == 0
+        self._check(lib().rds_assemble_rhs_cells(ctx, p.n_if_groups, len(p.problem.groups),
+                                                 int(alone)))
+        # a rank without interface nodes has its norm part here (no finish after the exchange)
+        sq = C.c_void_p(self.sq.data_ptr()) if alone and norm else None
+        self._check(lib().rds_gather_finish(ctx, len(p.if_nodes), p.problem.nnodes, float(cfl),
+                                            sq))
+
+    def assemble_and_pack(self, cfl: float):
+        """This rank's partial sums at the interface nodes into self.buf, the other nodes
+        finished."""
+        self.assemble_interface()
+        self.assemble_interior(cfl)
+
+    def unpack_and_finish(self, cfl: float, norm: bool = True):
+        """Full sums of the interface nodes from self.buf, their dt and update, and (norm)
+        this rank's norm part (all its owned nodes) into self.sq."""
+        ctx, n_if = self.solver._ctx, len(self.part.if_nodes)
+        if n_if == 0:
+            return  # norm part already summed by assemble_interior
+        self._check(lib().rds_unpack_interface(ctx, C.c_void_p(self.buf.data_ptr())))
+        sq = C.c_void_p(self.sq.data_ptr()) if norm else None
+        self._check(lib().rds_finish_nodes(ctx, float(cfl), 1, 0, n_if, sq))
 
     def check(self):
         self._check(lib().rds_check(self.solver._ctx))
@@ -207,8 +253,15 @@ class PartitionedRDS:
 
         if dist.is_initialized():
             self._sum = lambda t: dist.all_reduce(t, group=group)
+            self._sum_async = lambda t: dist.all_reduce(t, group=group, async_op=True)
+            # collectives of other backends (gloo: through the host) cannot be captured
+            self._graphs_ok = dist.get_backend(group) == "nccl"
         else:
             self._sum = lambda t: None
+            self._sum_async = lambda t: None
+            self._graphs_ok = True
+        self._graphs = {}  # (cfl, norm) -> (CUDA graph of one step, kernel launches per step)
+        self.graph_launches = 0  # kernel launches replayed through the graphs
         self.partition = partition(prob, world)
         part = self.partition.parts[rank]
         self.rank = RankSolver(part, self.partition.nslots, precision)
@@ -222,15 +275,45 @@ class PartitionedRDS:
     def set_solution(self, u_global):
         self.rank.set_solution(u_global)
 
-    def step(self, cfl: float):
-        """One pseudo-time iteration; the summed norm parts stay on the device (self.rank.sq)."""
+    def step(self, cfl: float, norm: bool = True):
+        """One pseudo-time iteration, enqueued: the interface cells and sums, the sum of the
+        exchange buffer over the ranks while the interior cells run, then unpack, finish and
+        (norm) the sum of the norm parts (they stay on the device, self.rank.sq)."""
         import torch
 
         with torch.cuda.stream(self.rank.stream):
-            self.rank.assemble_and_pack()
-            self._sum(self.rank.buf)
-            self.rank.unpack_and_finish(cfl)
-            self._sum(self.rank.sq)
+            self.rank.assemble_interface()
+            work = self._sum_async(self.rank.buf) if self.partition.nslots else None
+            self.rank.assemble_interior(cfl, norm)
+            if work is not None:
+                work.wait()
+            self.rank.unpack_and_finish(cfl, norm)
+            if norm:
+                self._sum(self.rank.sq)
+
+    def graph_step(self, cfl: float, norm: bool = True):
+        """step() through a CUDA graph of one step, captured at the first call for this
+        (cfl, norm) (NCCL collectives included) and replayed after; eager where capture is not
+        possible."""
+        import torch
+
+        if not self._graphs_ok:
+            self.step(cfl, norm)
+            return
+        key = (cfl, norm)
+        if key not in self._graphs:
+            stream = self.rank.stream
+            stream.synchronize()
+            n0 = self.rank.solver.launch_count()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=stream):
+                self.step(cfl, norm)
+            self._graphs[key] = (g, self.rank.solver.launch_count() - n0)
+            # the capture ran nothing: the replay below takes the step
+        g, n = self._graphs[key]
+        with torch.cuda.stream(self.rank.stream):
+            g.replay()
+        self.graph_launches += n
 
     def norm(self):
         """sqrt(sum_n (res dt)^2 / N) per equation of the last step."""
@@ -243,7 +326,7 @@ class PartitionedRDS:
         n0 = None
         it = 0
         while it < max_iter:
-            self.step(cfl)
+            self.graph_step(cfl)
             it += 1
             if it == 1 or it % check_every == 0 or it == max_iter:
                 nrm = self.norm()
@@ -270,6 +353,7 @@ class PartitionedRDS:
         return u.cpu().numpy()
 
     def close(self):
+        self._graphs = {}  # before the process group goes (a graph may hold NCCL calls)
         self.rank.close()
 
 
@@ -291,7 +375,7 @@ def emulate(prob: Problem, nparts: int, u0, cfl: float, iters: int, precision: s
     norms = np.zeros((iters, prob.neq))
     for it in range(iters):
         for r in ranks:
-            r.assemble_and_pack()
+            r.assemble_and_pack(cfl)
         torch.cuda.synchronize()
         total = sum(r.buf for r in ranks)
         for r in ranks:

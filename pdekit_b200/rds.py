@@ -126,6 +126,10 @@ def lib():
         "rds_pack_interface": ([vp, vp], ip),
         "rds_unpack_interface": ([vp, vp], ip),
         "rds_finish": ([vp, dp, ip, vp], ip),
+        "rds_assemble_rhs_cells": ([vp, ip, ip, ip], ip),
+        "rds_gather_rhs": ([vp, ip, ip], ip),
+        "rds_gather_finish": ([vp, ip, ip, dp, vp], ip),
+        "rds_finish_nodes": ([vp, dp, ip, ip, ip, vp], ip),
         "rds_check": ([vp], ip),
         "rds_element_jacobians": ([vp, ip, vp], ip),
         "rds_jacobian_pattern": ([vp, vp, vp, vp], ip),

@@ -46,3 +46,29 @@ def test_partitioned_larger_mesh_four_ranks():
     u1, hist = _single(prob, u0, 0.5, 30)
     assert rel_err(u, u1) < 1e-11
     np.testing.assert_allclose(norms, hist, rtol=1e-10)
+
+
+@pytest.mark.parametrize("case", ["burgers_p2_b", "euler2d_tri_p3_b", "euler3d_tet_p2_lda"])
+def test_one_rank_graph_steps_match_single_context(case):
+    """PartitionedRDS on one rank (no process group): the steps replayed from a CUDA graph, the
+    norm summed by the gather's last block (no interface nodes), and steps without the norm's
+    sum between them, against the single context."""
+    from pdekit_b200.partition import PartitionedRDS
+
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    cfl = meta["cfl"]
+    u1, hist = _single(prob, a["u0"], cfl, 5)
+    pr = PartitionedRDS(prob, 0, 1)
+    try:
+        pr.set_solution(a["u0"])
+        norms = []
+        for k in range(5):
+            pr.graph_step(cfl, norm=(k % 2 == 0))
+            if k % 2 == 0:
+                norms.append(pr.norm())
+        u = pr.solution_global()
+    finally:
+        pr.close()
+    assert rel_err(u, u1) < 1e-12
+    np.testing.assert_allclose(np.array(norms), hist[0::2], rtol=1e-11)
+    assert pr.graph_launches > 0

@@ -43,6 +43,27 @@ def test_partition_invariants(case, nparts):
         assert n == b.nfacets
 
 
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("nparts", [1, 2, 3])
+def test_interface_first_layout(case, nparts):
+    """The overlapped step's layout: a rank's interface nodes are its first local nodes, its
+    first n_if_groups groups hold exactly the cells touching one, and the other groups touch none
+    (so the interface sums need only the first groups and the facets)."""
+    prob, _, _ = load_golden(os.path.join(GOLDEN, case))
+    pt = partition(prob, nparts)
+    for p in pt.parts:
+        n_if = len(p.if_nodes)
+        assert np.array_equal(p.if_nodes, np.arange(n_if))
+        groups = p.problem.groups
+        assert 0 <= p.n_if_groups <= len(groups)
+        for k, g in enumerate(groups):
+            touches = (g.sol_conn < n_if).any(axis=1)
+            assert touches.all() if k < p.n_if_groups else not touches.any()
+        assert sum(g.ncells for g in groups) == sum(len(c) for c in p.cells)
+    if nparts == 1:
+        assert pt.nslots == 0 and pt.parts[0].n_if_groups == 0
+
+
 def test_partition_rejects_strong_conditions():
     prob, _, _ = load_golden(os.path.join(GOLDEN, "adv_p1_strong"))
     with pytest.raises(NotImplementedError):
