@@ -236,7 +236,7 @@ RDS_API rds_status rds_set_artificial_viscosity(rds_ctx *ctx, const double *eps)
 
 /* Stabilisation operators on the current state (its first component), the producers of those
  * fields: solver/art_visc/ArtificialViscosity.hpp and solver/rdm/blending_coeff/ (the
- * RDBlendingCoeff types LF_Blend, ViscosityIndicator, WongJansen).
+ * RDBlendingCoeff types LF_Blend, ViscosityIndicator, WongJansen, Bonanni2D / Bonanni3D).
  *   rds_set_stab_tables (after rds_finalize), per cell group:
  *     nq, w [nq], Vn [nq][ndof], R [nq][ndof]: the smoothness sensor's rule (exact to degree
  *       2p on the reference element), the nodal basis there, and the map from nodal values to
@@ -258,13 +258,29 @@ typedef enum
   RDS_STAB_INDICATOR         = 1, /* compute_indicator_normalized (cells only); p0 = kappa */
   RDS_STAB_BLEND_LF          = 2, /* "LF_Blend" */
   RDS_STAB_BLEND_VISC        = 3, /* "ViscosityIndicator"; p0 = kappa */
-  RDS_STAB_BLEND_WONG_JANSEN = 4  /* "WongJansen"; p0 = u_inf */
+  RDS_STAB_BLEND_WONG_JANSEN = 4, /* "WongJansen"; p0 = u_inf */
+  RDS_STAB_BLEND_BONANNI     = 5  /* "Bonanni2D" / "Bonanni3D" (Euler 2D / 3D); needs the tables
+                                     of rds_set_bonanni_tables */
 } rds_stab_op;
 RDS_API rds_status rds_set_stab_tables(rds_ctx *ctx, int group, int nq, const double *w,
                                        const double *Vn, const double *R, int nvert,
                                        const double *P1);
 RDS_API rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
                                              int install, double *cells_out, double *nodes_out);
+
+/* Bonanni's pressure-based blending coefficient (solver/rdm/blending_coeff/
+ * BonanniBlendingCoeffImpl.hpp:171-392, selected as "Bonanni2D" / "Bonanni3D" by
+ * RDBlendingCoeff.hpp:139-160): per cell c, with the reference's Gauss rule of order
+ * max(p, geometry order), f_c = (v_c . gp_c) |v_c| where v_c, gp_c are the cell means of the
+ * velocity and of grad p (p, V from the nodal states), and lc = |K_c|^(1/D); then
+ * theta_c = min(1, max(f_c / ((p_max - p_min) |v_dom|^2), 0)^2 lc), p_min / p_max over the
+ * nodal pressures and v_dom the mesh's mean velocity. rds_set_bonanni_tables (after
+ * rds_finalize), per cell group: that rule's nq points, w [nq], the solution basis
+ * V [nq][ndof] and its reference derivatives dV [dim][nq][ndof], the geometry basis derivatives
+ * dVgeo [dim][nq][ngeo] (straight-sided cells: ngeo <= 4). */
+RDS_API rds_status rds_set_bonanni_tables(rds_ctx *ctx, int group, int nq, const double *w,
+                                          const double *V, const double *dV,
+                                          const double *dVgeo);
 
 /* One step on host buffers, pipelined: upload u_in ([nnodes][neq], pinned host memory for the
  * copies to overlap), one assemble_lhs_and_rhs + solve, residual norm into norm[neq] (may be

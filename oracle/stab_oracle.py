@@ -20,9 +20,18 @@ the reference's stabilisation operators that sit either side of the cell residua
   values of the last cell (in cell order) that holds it.
 * `blend_cells`: LF_Blend (blending_coeff/LFBlendingCoeffImpl.hpp:76-126), WongJansen
   (WongJansenBlendingCoeffImpl.hpp:80-116), ViscosityIndicator (the sensor with eps0 = 1).
+* `bonanni`: Bonanni's pressure-based coefficient (BonanniBlendingCoeffImpl.hpp:171-392) of an
+  Euler state: per cell, with a Gauss rule of order max(p, 1), the volume, the integrals of the
+  velocity and of grad p (p = (gamma - 1)(rhoE - rho |V|^2 / 2) and V from the nodal states,
+  physics/euler/Euler2DCons.hpp:160-190), f = (v_m . gp_m)|v_m| (means over the cell) and
+  lc = |K|^(1/D); over the mesh p_min, p_max and v_dom = sum int V / sum |K|;
+  theta = min(1, max(f / ((p_max - p_min)|v_dom|^2), 0)^2 lc) with std::min / std::max's
+  comparisons. Quadrilaterals use the reference's rule (tensor Gauss-Legendre, order // 2 + 1
+  points per direction, mesh/point_set/QdPointSetQuadGauss.cpp); simplices a collapsed rule
+  exact to degree 2p (their integrands have degree <= p on affine cells).
 
-Pinned against the reference's own outputs (tests/golden/*_av, *_lf, *_wj, *_visc, dumped by
-oracle/ref_harness.cpp through the reference's classes).
+Pinned against the reference's own outputs (tests/golden/*_av, *_lf, *_wj, *_visc, *_bonanni,
+dumped by oracle/ref_harness.cpp through the reference's classes).
 """
 
 from __future__ import annotations
@@ -96,6 +105,14 @@ def _monomials(dim: int, p: int, pts: np.ndarray):
 def lagrange_at(dim: int, p: int, nodes: np.ndarray, pts: np.ndarray):
     """Nodal Lagrange basis through `nodes` (reference coordinates) evaluated at `pts`."""
     return _monomials(dim, p, pts) @ np.linalg.inv(_monomials(dim, p, nodes))
+
+
+def q1_at(nodes: np.ndarray):
+    """[ndof, 4] bilinear values of the square's corners (-1,-1), (1,-1), (1,1), (-1,1) at the
+    solution nodes of a quadrilateral."""
+    x, y = nodes[:, 0], nodes[:, 1]
+    return np.stack([(1 - x) * (1 - y), (1 + x) * (1 - y), (1 + x) * (1 + y),
+                     (1 - x) * (1 + y)], 1) / 4
 
 
 def p1_at(dim: int, nodes: np.ndarray):
@@ -178,3 +195,95 @@ def blend_cells(kind, sol_conn, u0, param=None):
             den += t[:, n]
         return nom / den
     raise ValueError(kind)
+
+
+# ---- Bonanni's pressure-based coefficient
+_QUAD_CORNERS = np.array([[-1.0, -1.0], [1.0, -1.0], [1.0, 1.0], [-1.0, 1.0]])
+
+
+def _mono_terms(dim, p, tensor):
+    if dim == 2:
+        return [(i, j) for i in range(p + 1) for j in range(p + 1) if tensor or i + j <= p]
+    return [(i, j, k) for i in range(p + 1) for j in range(p + 1) for k in range(p + 1)
+            if i + j + k <= p]
+
+
+def _mono(terms, pts):
+    return np.stack([np.prod([pts[:, d] ** e[d] for d in range(len(e))], 0) for e in terms], 1)
+
+
+def _mono_d(terms, pts, axis):
+    cols = []
+    for e in terms:
+        if e[axis] == 0:
+            cols.append(np.zeros(len(pts)))
+            continue
+        c = float(e[axis])
+        for d in range(len(e)):
+            c = c * pts[:, d] ** (e[d] - 1 if d == axis else e[d])
+        cols.append(c)
+    return np.stack(cols, 1)
+
+
+def _basis(dim, p, nodes, pts, tensor):
+    """Lagrange basis through `nodes` at `pts`: values [npts, n] and derivatives [dim, npts, n]."""
+    terms = _mono_terms(dim, p, tensor)
+    inv = np.linalg.inv(_mono(terms, nodes))
+    return _mono(terms, pts) @ inv, np.stack([_mono_d(terms, pts, a) @ inv for a in range(dim)])
+
+
+def _bonanni_rule(dim, shape, p):
+    if shape == "quad":
+        x, w = np.polynomial.legendre.leggauss(max(p, 1) // 2 + 1)
+        X, Y = np.meshgrid(x, x, indexing="ij")
+        return np.stack([X.ravel(), Y.ravel()], 1), np.outer(w, w).ravel()
+    return _simplex_rule(dim, p + 1)
+
+
+def bonanni(groups, u0, gamma, dim):
+    """theta per cell (groups in order). groups: (shape, p, sol_nodes [ndof, dim] reference
+    coordinates, geo_coords [n, dim], geo_conn [ncells, ngeo], sol_conn [ncells, ndof])."""
+    gm1 = gamma - 1.0
+    rho = u0[:, 0]
+    V = u0[:, 1:1 + dim] / rho[:, None]
+    v2 = np.zeros(len(rho))
+    for d in range(dim):
+        v2 = V[:, 0] * V[:, 0] if d == 0 else v2 + V[:, d] * V[:, d]
+    P = gm1 * (u0[:, dim + 1] - 0.5 * rho * v2)
+    f_all, lc_all = [], []
+    dom_vol, v_dom = 0.0, np.zeros(dim)
+    p_min, p_max = np.inf, -np.inf
+    for shape, p, sol_nodes, geo_coords, geo_conn, sol_conn in groups:
+        tensor = shape == "quad"
+        pts, w = _bonanni_rule(dim, shape, p)
+        B, dB = _basis(dim, p, sol_nodes, pts, tensor)
+        corners = _QUAD_CORNERS if tensor else np.vstack([-np.ones(dim), -np.ones(dim) +
+                                                         2 * np.eye(dim)])
+        _, dG = _basis(dim, 1, corners, pts, tensor)
+        for c in range(len(sol_conn)):
+            dofs = sol_conn[c]
+            p_min = min(p_min, P[dofs].min())
+            p_max = max(p_max, P[dofs].max())
+            Xg = geo_coords[geo_conn[c]]
+            vol, vint, pint = 0.0, np.zeros(dim), np.zeros(dim)
+            for q in range(len(w)):
+                J = dG[:, q, :] @ Xg  # J[xi][x] = dx / dxi
+                jw = np.linalg.det(J) * w[q]
+                vol += jw
+                gp = np.linalg.solve(J, dB[:, q, :] @ P[dofs])
+                vint += jw * (B[q] @ V[dofs])
+                pint += jw * gp
+            dom_vol += vol
+            v_dom += vint
+            vm, gm = vint / vol, pint / vol
+            f_all.append(float(vm @ gm) * np.sqrt(vm @ vm))
+            lc_all.append(vol ** (1.0 / dim))
+    v_dom = v_dom / dom_vol
+    nv = np.sqrt(v_dom @ v_dom)
+    delta = (p_max - p_min) * nv * nv
+    f = np.asarray(f_all)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        q = f / delta
+    sc = np.where(q < 0.0, 0.0, q)  # std::max(q, 0.0)
+    t = sc * sc * np.asarray(lc_all)
+    return np.where(t < 1.0, t, 1.0)  # std::min(1., t)

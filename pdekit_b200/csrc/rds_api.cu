@@ -89,8 +89,12 @@ struct rds_ctx
     int nq = 0, nvert = 0;
     double *w = nullptr, *Vn = nullptr, *R = nullptr, *P1 = nullptr;
     double *vw = nullptr, *vV = nullptr, *vdV = nullptr, *vdVgeo = nullptr;
+    int bnq    = 0; // Bonanni's coefficient: its rule, basis and geometry derivatives
+    double *bw = nullptr, *bV = nullptr, *bdV = nullptr, *bdVgeo = nullptr;
   };
   std::vector<StabTab> stab;
+  double *d_bon = nullptr; // Bonanni's coefficient: lc per cell, block sums, delta
+  size_t bon_len = 0;
 
   // pipelined host-buffer steps (rds_step_host): copy streams, double-buffered staging
   cudaStream_t h_in = nullptr, h_out = nullptr;
@@ -1594,6 +1598,34 @@ rds_status rds_set_stab_tables(rds_ctx *ctx, int group, int nq, const double *w,
   return RDS_OK;
 }
 
+rds_status rds_set_bonanni_tables(rds_ctx *ctx, int group, int nq, const double *w,
+                                  const double *V, const double *dV, const double *dVgeo)
+{
+  rds_status st = stab_check(ctx, "rds_set_bonanni_tables");
+  if (st != RDS_OK)
+    return st;
+  if (group < 0 || group >= (int)ctx->groups.size())
+    return fail(ctx, RDS_ERR_INVALID, "rds_set_bonanni_tables: invalid group");
+  const HostCellGroup &g = ctx->groups[group];
+  const int D = ctx->desc.dim, ndof = g.desc.ndof, ngeo = g.desc.ngeo;
+  rds_ctx::StabTab &t = ctx->stab[group];
+  if (nq <= 0 || nq > 64 || !w || !V || !dV || !dVgeo || ngeo > 4)
+    return fail(ctx, RDS_ERR_INVALID, "rds_set_bonanni_tables: invalid sizes or missing tables "
+                                      "(straight-sided cells, at most 64 points)");
+  if (t.bw && t.bnq != nq)
+    return fail(ctx, RDS_ERR_INVALID, "rds_set_bonanni_tables: table sizes differ from the first call");
+  if ((!t.bw && ((st = stab_alloc(ctx, &t.bw, nq)) || (st = stab_alloc(ctx, &t.bV, (size_t)nq * ndof)) ||
+                 (st = stab_alloc(ctx, &t.bdV, (size_t)D * nq * ndof)) ||
+                 (st = stab_alloc(ctx, &t.bdVgeo, (size_t)D * nq * ngeo)))) ||
+      (st = upload(ctx, t.bw, w, nq)) || (st = upload(ctx, t.bV, V, (size_t)nq * ndof)) ||
+      (st = upload(ctx, t.bdV, dV, (size_t)D * nq * ndof)) ||
+      (st = upload(ctx, t.bdVgeo, dVgeo, (size_t)D * nq * ngeo)))
+    return st;
+  t.bnq = nq;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RDS_OK;
+}
+
 rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1, int install,
                                      double *cells_out, double *nodes_out)
 {
@@ -1603,7 +1635,8 @@ rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
   const int G = (int)ctx->groups.size(), N = ctx->desc.nnodes;
   const bool sensor = op == RDS_STAB_ART_VISC || op == RDS_STAB_INDICATOR || op == RDS_STAB_BLEND_VISC;
   const bool nodal  = install || nodes_out;
-  if (op < RDS_STAB_ART_VISC || op > RDS_STAB_BLEND_WONG_JANSEN ||
+  const bool bonanni = op == RDS_STAB_BLEND_BONANNI;
+  if (op < RDS_STAB_ART_VISC || op > RDS_STAB_BLEND_BONANNI ||
       (op == RDS_STAB_INDICATOR && nodal))
     return fail(ctx, RDS_ERR_INVALID, "rds_compute_stabilisation: unknown operator, or a nodal "
                                       "field of the normalised indicator");
@@ -1611,6 +1644,9 @@ rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
     return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_compute_stabilisation: more than 8 cell groups");
   if (sensor && !(p0 > 0.0))
     return fail(ctx, RDS_ERR_INVALID, "rds_compute_stabilisation: kappa must be positive");
+  if (bonanni && ctx->desc.neq != ctx->desc.dim + 2)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_compute_stabilisation: Bonanni's coefficient needs "
+                                          "Euler physics");
   long long wc = 0, sc = 0;
   for (int k = 0; k < G; ++k)
   {
@@ -1621,6 +1657,9 @@ rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
     if (nodal && t.nvert == 0)
       return fail(ctx, RDS_ERR_INVALID, "rds_compute_stabilisation: no vertex interpolant "
                                         "(rds_set_stab_tables) for a group");
+    if (bonanni && t.bnq == 0)
+      return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_compute_stabilisation: no Bonanni tables "
+                                            "(rds_set_bonanni_tables) for a group");
     wc += ctx->groups[k].desc.ncells;
     sc += (long long)ctx->groups[k].desc.ncells * ctx->groups[k].desc.ndof;
   }
@@ -1628,6 +1667,23 @@ rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
       (!ctx->d_nodef && (st = stab_alloc(ctx, &ctx->d_nodef, N))))
     return st;
   cudaStream_t s = ctx->stream;
+  int bon_blocks = 0; // Bonanni: block sums of all groups, after the cells' lc values
+  if (bonanni)
+  {
+    for (int k = 0; k < G; ++k)
+      bon_blocks += bonanni_blocks(ctx->groups[k].desc.ncells);
+    const size_t need = (size_t)wc + (size_t)bon_blocks * (ctx->desc.dim + 3) + 1;
+    if (need > ctx->bon_len)
+    {
+      cudaFree(ctx->d_bon);
+      ctx->d_bon   = nullptr;
+      ctx->bon_len = 0;
+      if ((st = dalloc(ctx, &ctx->d_bon, need)) != RDS_OK)
+        return st;
+      ctx->bon_len = need;
+    }
+  }
+  int bon_done = 0;
   for (int k = 0; k < G; ++k)
   {
     const HostCellGroup &g    = ctx->groups[k];
@@ -1654,10 +1710,38 @@ rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
       a.out        = out;
       RDS_CUDA(launch_sensor(a, ctx->desc.dim, s));
     }
+    else if (bonanni)
+    {
+      BonanniArgs a{};
+      a.ncells     = g.desc.ncells;
+      a.ndof       = g.desc.ndof;
+      a.nq         = t.bnq;
+      a.ngeo       = g.desc.ngeo;
+      a.nnodes     = N;
+      a.ngeo_nodes = ctx->desc.ngeo_nodes;
+      a.sol_conn   = g.d_sol_conn;
+      a.geo_conn   = g.d_geo_conn;
+      a.X          = ctx->d_X;
+      a.u          = ctx->d_u;
+      a.w          = t.bw;
+      a.V          = t.bV;
+      a.dV         = t.bdV;
+      a.dVgeo      = t.bdVgeo;
+      a.gamma      = ctx->desc.gamma;
+      a.f          = out;
+      a.lc         = ctx->d_bon + g.ws_base;
+      a.part       = ctx->d_bon + wc + (size_t)bon_done * (ctx->desc.dim + 3);
+      RDS_CUDA(launch_bonanni_cells(a, ctx->desc.dim, s));
+      bon_done += bonanni_blocks(g.desc.ncells);
+    }
     else
       RDS_CUDA(launch_blend_cells(op == RDS_STAB_BLEND_LF ? 0 : 1, g.desc.ncells, g.desc.ndof,
                                   g.d_sol_conn, ctx->d_u, p0, out, s));
   }
+  if (bonanni)
+    RDS_CUDA(launch_bonanni_finish(ctx->desc.dim, bon_blocks, ctx->d_bon + wc,
+                                   ctx->d_bon + wc + (size_t)bon_blocks * (ctx->desc.dim + 3),
+                                   (int)wc, ctx->d_cellf, ctx->d_bon, s));
   if (op == RDS_STAB_INDICATOR)
     RDS_CUDA(launch_normalise_max((int)wc, ctx->d_cellf, s));
   if (op == RDS_STAB_BLEND_LF)
@@ -2915,6 +2999,7 @@ rds_status rds_destroy(rds_ctx *ctx)
     cudaFree(b.d_geo_conn);
     cudaFree(b.d_gq);
   }
+  cudaFree(ctx->d_bon);
   cudaFree(ctx->d_if_nodes);
   cudaFree(ctx->d_if_slots);
   cudaFree(ctx->d_owned);

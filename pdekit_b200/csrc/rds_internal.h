@@ -402,6 +402,24 @@ cudaError_t launch_viscous(const ViscArgs &a, int dim, int neq, cudaStream_t s, 
 cudaError_t launch_sensor(const SensorArgs &a, int dim, cudaStream_t s);
 cudaError_t launch_normalise_max(int n, double *v, cudaStream_t s);
 // kind 0: LF_Blend cell values ksi (pass 1), 1: Wong-Jansen (u_inf)
+// Bonanni's pressure-based blending coefficient (rds_stab.cu)
+struct BonanniArgs
+{
+  int ncells, ndof, nq, ngeo, nnodes, ngeo_nodes;
+  const int32_t *sol_conn, *geo_conn; // SoA [ndof][ncells], [ngeo][ncells]
+  const double *X, *u;                // SoA coordinates, state
+  const double *w, *V, *dV, *dVgeo;   // the coefficient's rule: [nq], [nq][ndof], [D][nq][..]
+  double gamma;
+  double *f, *lc;                     // per cell: (v . grad p) |v| (cell means), |K|^(1/D)
+  double *part;                       // per block: |K|, int V [D], p_min, p_max
+};
+cudaError_t launch_bonanni_cells(const BonanniArgs &a, int dim, cudaStream_t s);
+// the block sums of all groups' launches ([nblocks][dim + 3]) -> delta = (p_max - p_min)|v_dom|^2,
+// then theta = min(1, max(f / delta, 0)^2 lc) for the n cells of f / lc (in place in f)
+cudaError_t launch_bonanni_finish(int dim, int nblocks, const double *part, double *delta, int n,
+                                  double *f, const double *lc, cudaStream_t s);
+int bonanni_blocks(int ncells);
+
 cudaError_t launch_blend_cells(int kind, int ncells, int ndof, const int32_t *sol_conn,
                                const double *u, double param, double *out, cudaStream_t s);
 // LF_Blend pass 2 / 3: nodal max of the cells' values; 1 - max over each cell's nodes

@@ -23,6 +23,15 @@
 //              cells (node-parallel over the gather lists), per cell 1 - max over its nodes;
 //              Wong-Jansen (WongJansenBlendingCoeffImpl.hpp:80-116): per cell
 //              sum_n t_n / (u_inf^4 + sum_n t_n), t_n = (u_n^2 - u_avg^2)^2.
+//   bonanni    Bonanni's pressure-based coefficient (blending_coeff/BonanniBlendingCoeffImpl.hpp:
+//              171-392, Euler 2D / 3D): per cell, with the coefficient's own Gauss rule, the
+//              volume |K|, the integrals of the velocity and of grad p (p and V from the nodal
+//              states), f = (v_m . gp_m) |v_m| with v_m, gp_m those integrals over |K|, and
+//              lc = |K|^(1/D); over the mesh p_min, p_max of the nodal pressures and the mean
+//              velocity v_dom = sum int V / sum |K|; then per cell
+//              theta = min(1, max(f / ((p_max - p_min) |v_dom|^2), 0)^2 lc), min and max with
+//              std::min / std::max's comparisons (so a NaN or infinite quotient ends as there).
+//              Mesh sums over block sums in a fixed order.
 //   transfer   cell values -> nodal field (interpolation/mesh_function/MeshFunctionTools.hpp:
 //              52-397, no adaptation): every vertex node max(0, max over its cells), every
 //              other node the vertex interpolant of the last cell (in cell order) holding it.
@@ -505,6 +514,205 @@ __global__ void __launch_bounds__(kGBlock)
   nodef[v] = f;
 }
 
+
+// ---- Bonanni's coefficient
+
+constexpr int kBonBlock = 128;
+
+__device__ __forceinline__ double std_max(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double std_min(double a, double b) { return (b < a) ? b : a; }
+
+// sum / min / max over a block of kBonBlock threads (the result valid in thread 0)
+template <int OP>
+__device__ __forceinline__ double bon_reduce(double v, double *smem)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+  {
+    const double t = __shfl_down_sync(0xffffffffu, v, o);
+    v              = OP == 0 ? v + t : OP == 1 ? fmin(v, t) : fmax(v, t);
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0)
+    smem[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = smem[0];
+  if (threadIdx.x == 0)
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k)
+      r = OP == 0 ? r + smem[k] : OP == 1 ? fmin(r, smem[k]) : fmax(r, smem[k]);
+  return r;
+}
+
+template <int D>
+__global__ void __launch_bounds__(kBonBlock) bonanni_cells(const BonanniArgs a)
+{
+  __shared__ double smem[kBonBlock / 32];
+  const int c   = blockIdx.x * blockDim.x + threadIdx.x;
+  double vol    = 0.0, vint[D], pmin = 1.7976931348623157e308, pmax = -1.7976931348623157e308;
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+    vint[d] = 0.0;
+  if (c < a.ncells)
+  {
+    const double gm1 = a.gamma - 1.0;
+    // nodal pressure and velocity (physics/euler/Euler2DCons.hpp:160-190)
+    auto node = [&](int n, double V[D]) -> double {
+      const int v        = __ldg(a.sol_conn + (size_t)n * a.ncells + c);
+      const double rho   = __ldg(a.u + v);
+      const double inv   = 1. / rho;
+      double v2          = 0.0;
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+      {
+        V[d] = __ldg(a.u + (size_t)(1 + d) * a.nnodes + v) * inv;
+        v2   = d == 0 ? V[0] * V[0] : v2 + V[d] * V[d];
+      }
+      const double rhoE = __ldg(a.u + (size_t)(D + 1) * a.nnodes + v);
+      return gm1 * (rhoE - 0.5 * rho * v2);
+    };
+    for (int n = 0; n < a.ndof; ++n)
+    {
+      double V[D];
+      const double p = node(n, V);
+      pmin           = fmin(pmin, p);
+      pmax           = fmax(pmax, p);
+    }
+    double X[4][D];
+    for (int g = 0; g < a.ngeo && g < 4; ++g)
+    {
+      const int v = __ldg(a.geo_conn + (size_t)g * a.ncells + c);
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+        X[g][d] = __ldg(a.X + (size_t)d * a.ngeo_nodes + v);
+    }
+    double pint[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+      pint[d] = 0.0;
+    for (int q = 0; q < a.nq; ++q)
+    {
+      double J[D][D], iJ[D][D];
+#pragma unroll
+      for (int xi = 0; xi < D; ++xi)
+#pragma unroll
+        for (int x = 0; x < D; ++x)
+        {
+          double sj = 0.0;
+          for (int g = 0; g < a.ngeo && g < 4; ++g)
+            sj += __ldg(a.dVgeo + ((size_t)xi * a.nq + q) * a.ngeo + g) * X[g][x];
+          J[xi][x] = sj;
+        }
+      const double jw = invert<D>(J, iJ) * __ldg(a.w + q);
+      vol += jw;
+      double vq[D], gref[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+        vq[d] = gref[d] = 0.0;
+      for (int n = 0; n < a.ndof; ++n)
+      {
+        double V[D];
+        const double p  = node(n, V);
+        const double bn = __ldg(a.V + (size_t)q * a.ndof + n);
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+        {
+          vq[d] += bn * V[d];
+          gref[d] += __ldg(a.dV + ((size_t)d * a.nq + q) * a.ndof + n) * p;
+        }
+      }
+#pragma unroll
+      for (int x = 0; x < D; ++x)
+      {
+        double gp = 0.0;
+#pragma unroll
+        for (int xi = 0; xi < D; ++xi)
+          gp += iJ[x][xi] * gref[xi];
+        vint[x] += jw * vq[x];
+        pint[x] += jw * gp;
+      }
+    }
+    double f = 0.0, vn = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+    {
+      const double vm = vint[d] / vol;
+      f += vm * (pint[d] / vol);
+      vn += vm * vm;
+    }
+    a.f[c]  = f * sqrt(vn);
+    a.lc[c] = pow(vol, 1. / D);
+  }
+  else
+    vol = 0.0;
+  // block sums for the mesh-wide quantities
+  double *pb = a.part + (size_t)blockIdx.x * (D + 3);
+  const double bv = bon_reduce<0>(vol, smem);
+  if (threadIdx.x == 0)
+    pb[0] = bv;
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+  {
+    const double t = bon_reduce<0>(vint[d], smem);
+    if (threadIdx.x == 0)
+      pb[1 + d] = t;
+  }
+  const double mn = bon_reduce<1>(pmin, smem);
+  if (threadIdx.x == 0)
+    pb[D + 1] = mn;
+  const double mx = bon_reduce<2>(pmax, smem);
+  if (threadIdx.x == 0)
+    pb[D + 2] = mx;
+}
+
+template <int D>
+__global__ void __launch_bounds__(kBonBlock)
+    bonanni_reduce(int nblocks, const double *__restrict__ part, double *__restrict__ delta)
+{
+  __shared__ double smem[kBonBlock / 32];
+  double r[D + 3];
+#pragma unroll
+  for (int k = 0; k < D + 3; ++k)
+    r[k] = k == D + 1 ? 1.7976931348623157e308 : k == D + 2 ? -1.7976931348623157e308 : 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+  {
+    const double *pb = part + (size_t)b * (D + 3);
+#pragma unroll
+    for (int k = 0; k <= D; ++k)
+      r[k] += pb[k];
+    r[D + 1] = fmin(r[D + 1], pb[D + 1]);
+    r[D + 2] = fmax(r[D + 2], pb[D + 2]);
+  }
+  double t[D + 3];
+#pragma unroll
+  for (int k = 0; k <= D; ++k)
+    t[k] = bon_reduce<0>(r[k], smem);
+  t[D + 1] = bon_reduce<1>(r[D + 1], smem);
+  t[D + 2] = bon_reduce<2>(r[D + 2], smem);
+  if (threadIdx.x == 0)
+  {
+    double n2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+    {
+      const double vd = t[1 + d] / t[0];
+      n2 += vd * vd;
+    }
+    const double nv = sqrt(n2);
+    delta[0]        = (t[D + 2] - t[D + 1]) * nv * nv;
+  }
+}
+
+__global__ void __launch_bounds__(kGBlock)
+    bonanni_finish(int n, const double *__restrict__ delta, double *__restrict__ f,
+                   const double *__restrict__ lc)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n)
+    return;
+  const double sc = std_max(f[c] / delta[0], 0.0);
+  f[c]            = std_min(1., sc * sc * lc[c]);
+}
+
 } // namespace
 
 cudaError_t launch_viscous(const ViscArgs &a, int dim, int neq, cudaStream_t s, const char **name)
@@ -579,6 +787,39 @@ cudaError_t launch_cells_to_nodes(int nnodes, const int32_t *row, const int32_t 
   if ((e = cudaGetLastError()) != cudaSuccess)
     return e;
   interior_interp<<<grid, kGBlock, 0, s>>>(nnodes, row, ent_slot, scells, g, nodef);
+  return cudaGetLastError();
+}
+
+int bonanni_blocks(int ncells)
+{
+  return (ncells + kBonBlock - 1) / kBonBlock;
+}
+
+cudaError_t launch_bonanni_cells(const BonanniArgs &a, int dim, cudaStream_t s)
+{
+  if (a.ncells == 0)
+    return cudaSuccess;
+  if (a.ngeo > 4)
+    return cudaErrorInvalidValue;
+  const int grid = bonanni_blocks(a.ncells);
+  if (dim == 2)
+    bonanni_cells<2><<<grid, kBonBlock, 0, s>>>(a);
+  else
+    bonanni_cells<3><<<grid, kBonBlock, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bonanni_finish(int dim, int nblocks, const double *part, double *delta, int n,
+                                  double *f, const double *lc, cudaStream_t s)
+{
+  if (dim == 2)
+    bonanni_reduce<2><<<1, kBonBlock, 0, s>>>(nblocks, part, delta);
+  else
+    bonanni_reduce<3><<<1, kBonBlock, 0, s>>>(nblocks, part, delta);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || n == 0)
+    return e;
+  bonanni_finish<<<(n + kGBlock - 1) / kGBlock, kGBlock, 0, s>>>(n, delta, f, lc);
   return cudaGetLastError();
 }
 

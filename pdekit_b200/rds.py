@@ -139,6 +139,7 @@ def lib():
         "rds_set_blending_coeff": ([vp, vp], ip),
         "rds_set_artificial_viscosity": ([vp, vp], ip),
         "rds_set_stab_tables": ([vp, ip, ip, vp, vp, vp, ip, vp], ip),
+        "rds_set_bonanni_tables": ([vp, ip, ip, vp, vp, vp, vp], ip),
         "rds_compute_stabilisation": ([vp, ip, dp, dp, ip, vp, vp], ip),
     }
     for name, (args, res) in sig.items():
@@ -232,13 +233,20 @@ class PGRDMethodExplicit:
         self._check(lib().rds_finalize(self._ctx))
         # tables of the stabilisation operators: the vertex interpolant of every group, the
         # smoothness sensor's where it is defined (affine simplices)
-        from .reference_element import stab_tables
+        from .reference_element import bonanni_tables, stab_tables
         for ig, g in enumerate(self.problem.groups):
             t = stab_tables(g.shape, g.order, g.ngeo)
             arrs = [t[k] for k in ("w", "Vn", "R", "P1")]
             self._keep += arrs
             self._check(lib().rds_set_stab_tables(self._ctx, ig, t["nq"], *[_ptr(a) for a in arrs[:3]],
                                                   t["P1"].shape[1], _ptr(arrs[3])))
+            if self.problem.neq > 1:  # Bonanni's coefficient (Euler)
+                b = bonanni_tables(g.shape, g.order, g.ngeo)
+                if b["nq"]:
+                    arrs = [b[k] for k in ("w", "V", "dV", "dVgeo")]
+                    self._keep += arrs
+                    self._check(lib().rds_set_bonanni_tables(self._ctx, ig, b["nq"],
+                                                             *[_ptr(a) for a in arrs]))
         return self
 
     # ---- stabilisation fields (RDMethod::set_blending_coeff / set_artificial_viscosity) -------

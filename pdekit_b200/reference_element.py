@@ -420,3 +420,31 @@ def stab_tables(shape: str, p: int, ngeo: int) -> dict:
                    R=np.ascontiguousarray(R))
     _STAB_CACHE[key] = out
     return out
+
+
+def bonanni_tables(shape: str, p: int, ngeo: int) -> dict:
+    """Tables of Bonanni's pressure-based blending coefficient
+    (src/solver/rdm/blending_coeff/BonanniBlendingCoeffImpl.hpp:102-168): the reference
+    integrates the velocity and the pressure gradient over a cell with its Gauss rule of order
+    max(p, geometry order). Quadrilaterals use that rule (tensor Gauss-Legendre, order // 2 + 1
+    points per direction); on affine simplices the integrands are polynomials of degree <= p,
+    so a rule exact to degree p gives the same integrals. w [nq], V [nq, ndof],
+    dV [D, nq, ndof], dVgeo [D, nq, ngeo]; nq = 0 where not provided (curved cells)."""
+    order = max(p, 1)
+    if shape == "triag" and ngeo == 3:
+        qp, w = triag_gauss(min(o for o in _DUNAVANT if o >= order))
+        V, dV = lagrange_triag(p, qp)
+        _, dVgeo = lagrange_triag(1, qp)
+    elif shape == "quad" and ngeo == 4:
+        qp, w = quad_gauss(order)
+        V, dV = lagrange_quad(p, qp)
+        _, dVgeo = lagrange_quad(1, qp)
+    elif shape == "tetra" and ngeo == 4:
+        qp, w = tet_gauss(min(o for o in _TET_RULES if o >= order))
+        V, dV = lagrange_tet(p, qp)
+        _, dVgeo = lagrange_tet(1, qp)
+    else:
+        z = np.zeros(1)
+        return dict(nq=0, w=z, V=z, dV=z, dVgeo=z)
+    c = np.ascontiguousarray
+    return dict(nq=len(w), w=c(w), V=c(V), dV=c(dV), dVgeo=c(dVgeo))

@@ -20,8 +20,8 @@ when asked for. Cell values are in the solver's cell order (groups in order).
   affine triangles (orders 1-3) and tetrahedra (orders 1-2).
 * RDBlendingCoeff (src/solver/rdm/blending_coeff/RDBlendingCoeff.hpp): "LF_Blend" (any cell
   type), "ViscosityIndicator" (param "kappa", the sensor as a coefficient in [0, 1]; affine
-  simplices), "WongJansen" (param "u_inf", default 1e-14; any cell type). "Bonanni2D/3D" are
-  not provided.
+  simplices), "WongJansen" (param "u_inf", default 1e-14; any cell type), "Bonanni2D" /
+  "Bonanni3D" (Euler; the pressure-based coefficient, no parameters; straight-sided cells).
 """
 
 from __future__ import annotations
@@ -29,7 +29,7 @@ from __future__ import annotations
 from .rds import PGRDMethodExplicit
 
 # rds_stab_op (include/rds_b200.h)
-ART_VISC, INDICATOR, BLEND_LF, BLEND_VISC, BLEND_WONG_JANSEN = range(5)
+ART_VISC, INDICATOR, BLEND_LF, BLEND_VISC, BLEND_WONG_JANSEN, BLEND_BONANNI = range(6)
 
 
 class ArtificialViscosity:
@@ -69,7 +69,8 @@ class ArtificialViscosity:
 
 class RDBlendingCoeff:
     _TYPES = {"LF_Blend": BLEND_LF, "ViscosityIndicator": BLEND_VISC,
-              "WongJansen": BLEND_WONG_JANSEN}
+              "WongJansen": BLEND_WONG_JANSEN, "Bonanni2D": BLEND_BONANNI,
+              "Bonanni3D": BLEND_BONANNI}
 
     def __init__(self):
         self.solver, self.op = None, None
@@ -79,6 +80,8 @@ class RDBlendingCoeff:
         if coeff_type not in self._TYPES:
             raise ValueError(f"blending coefficient type {coeff_type!r} is not provided "
                              f"(have {sorted(self._TYPES)})")
+        if coeff_type.startswith("Bonanni") and solver.problem.dim != int(coeff_type[-2]):
+            raise ValueError(f"{coeff_type} on a {solver.problem.dim}D problem")
         self.solver, self.op = solver, self._TYPES[coeff_type]
         return self
 

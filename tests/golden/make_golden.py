@@ -134,6 +134,16 @@ CASES = {
     # come from the reference, the nodal field handed to its solver from the oracle's transfer
     "euler3d_tet_p2_lda_av": ("euler3d", "lda", 2, 5, ("box_tet", 4, 2, 2), 0.1, 59,
                               "bump3d_jump", EULER3D_BCS, 0.5, 3, "av3d:4.0:1.0"),
+    # Bonanni's pressure-based blending coefficient into PGB (3D: cellwise values from the
+    # reference, the nodal field from the oracle's transfer, as for the viscosity above)
+    "euler2d_tri_p2_b_bonanni": ("euler2d", "b", 2, 5, ("channel_tri", 5, 3), 0.15, 61,
+                                 "bump2d_jump", EULER2D_BCS, 0.5, 3, "blend:Bonanni2D:0"),
+    "euler2d_tri_p3_b_bonanni": ("euler2d", "b", 3, 8, ("channel_tri", 4, 3), 0.15, 62,
+                                 "bump2d_jump", EULER2D_BCS, 0.5, 3, "blend:Bonanni2D:0"),
+    "euler2d_quad_p2_b_bonanni": ("euler2d", "b", 2, 5, ("channel_quad", 5, 3), 0.15, 63,
+                                  "bump2d_jump", EULER2D_BCS, 0.5, 3, "blend:Bonanni2D:0"),
+    "euler3d_tet_p2_b_bonanni": ("euler3d", "b", 2, 5, ("box_tet", 4, 2, 2), 0.1, 64,
+                                 "bump3d_jump", EULER3D_BCS, 0.5, 3, "blend3d:Bonanni3D:0"),
 }
 
 
@@ -171,30 +181,33 @@ def make(name, spec):
         env["RDS_HARNESS_JACOBIAN"] = "1"
     else:
         env.pop("RDS_HARNESS_JACOBIAN", None)
-    if not stab.startswith("av3d:"):
+    if not (stab.startswith("av3d:") or stab.startswith("blend3d:")):
         subprocess.run(cmd + [stab], check=True, stdout=subprocess.DEVNULL, env=env)
         return
-    # two passes: the reference's cellwise viscosity, then the solver with the nodal field
+    # two passes: the reference's cellwise field, then the solver with the nodal field
     import json
     import numpy as np
     from oracle import stab_oracle
-    _, kappa, factor = stab.split(":")
+    blend = stab.startswith("blend3d:")
+    _, a1, a2 = stab.split(":")
     tmp = out + "_cells"
     os.makedirs(tmp, exist_ok=True)
-    subprocess.run(cmd[:7] + [tmp] + cmd[8:] + [f"avcells:{kappa}:{factor}"], check=True,
-                   stdout=subprocess.DEVNULL)
+    first = f"blendcells:{a1}:{a2}" if blend else f"avcells:{a1}:{a2}"
+    subprocess.run(cmd[:7] + [tmp] + cmd[8:] + [first], check=True, stdout=subprocess.DEVNULL)
     meta = json.load(open(os.path.join(tmp, "meta.json")))
     shp = meta["arrays"]
     rd = lambda n, t: np.fromfile(os.path.join(tmp, f"{n}.{t}"),
                                   dtype=np.float64 if t == "f64" else np.int32).reshape(shp[n])
     sol_conn, sol_nodes = rd("sol_conn", "i32"), rd("sol_nodes", "f64")
-    av = stab_oracle.nodal_from_cells(rd("av_cell", "f64"), sol_conn, meta["nsol"],
-                                      stab_oracle.p1_at(meta["dim"], sol_nodes))
+    cells = ("blend_cell",) if blend else ("av_cell", "indicator")
+    nodal = stab_oracle.nodal_from_cells(rd(cells[0], "f64"), sol_conn, meta["nsol"],
+                                         stab_oracle.p1_at(meta["dim"], sol_nodes))
     field = os.path.join(tmp, "field.f64")
-    av.tofile(field)
-    subprocess.run(cmd + [f"avfield:{field}"], check=True, stdout=subprocess.DEVNULL)
+    nodal.tofile(field)
+    second = f"blendfield:{field}" if blend else f"avfield:{field}"
+    subprocess.run(cmd + [second], check=True, stdout=subprocess.DEVNULL)
     meta2 = json.load(open(os.path.join(out, "meta.json")))
-    for n in ("av_cell", "indicator"):
+    for n in cells:
         shutil.copy(os.path.join(tmp, f"{n}.f64"), os.path.join(out, f"{n}.f64"))
         meta2["arrays"][n] = shp[n]
     meta2["stab"] = stab

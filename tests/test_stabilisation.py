@@ -15,8 +15,9 @@ from oracle import stab_oracle as so
 from golden_io import load_golden
 from pdekit_b200.reference_element import stab_tables
 
-# FP64 restatement: rounding only; the reference's tetrahedron rule of order 4 is tabulated to
-# about 10 digits (its results differ from exact integration by ~1e-9 relative)
+# FP64 restatement: rounding only; the reference's tetrahedron rules of orders 2 and 4 are
+# tabulated to about 10 digits (its results differ from exact integration by ~1e-10 - 1e-9
+# relative)
 TOL = {2: 1e-12, 3: 1e-8}
 
 
@@ -36,7 +37,8 @@ def test_oracle_matches_reference(case):
     prob, a, meta, kind, par = _case(case)
     dim, p = meta["dim"], meta["p"]
     u0 = a["u0"][:, 0]
-    P1 = so.p1_at(dim, a["sol_nodes"])
+    quad = prob.groups[0].shape == "quad"
+    P1 = so.q1_at(a["sol_nodes"]) if quad else so.p1_at(dim, a["sol_nodes"])
     tol = TOL[dim]
     if kind.startswith("av"):
         kappa, factor = float(par[0]), float(par[1])
@@ -56,6 +58,10 @@ def test_oracle_matches_reference(case):
         if typ == "ViscosityIndicator":
             bc = so.sensor_cells(dim, p, a["sol_nodes"], a["geo_coords"], a["geo_conn"],
                                  a["sol_conn"], u0, prm, blend=True)
+        elif typ.startswith("Bonanni"):
+            g = prob.groups[0]
+            bc = so.bonanni([(g.shape, g.order, a["sol_nodes"], a["geo_coords"], a["geo_conn"],
+                              a["sol_conn"])], a["u0"], prob.gamma, dim)
         else:
             bc = so.blend_cells(typ, a["sol_conn"], u0, prm)
         assert _rel(bc, a["blend_cell"]) < tol
@@ -75,7 +81,8 @@ def test_cases_exercise_every_branch():
         seen.add(kind if kind.startswith("av") else par[0])
         if kind.startswith("av"):
             assert (v == 0.0).any() or meta["p"] == 1, c
-    assert {"av", "av3d", "LF_Blend", "WongJansen", "ViscosityIndicator"} <= seen
+    assert {"av", "av3d", "LF_Blend", "WongJansen", "ViscosityIndicator", "Bonanni2D",
+            "Bonanni3D"} <= seen
 
 
 @pytest.mark.parametrize("case", [c for c in stab_cases()
@@ -122,4 +129,39 @@ def test_vertex_interpolant_matches_oracle(shape, p):
 def test_fixture_meta_names_its_operator():
     for c in stab_cases():
         meta = json.load(open(os.path.join(GOLDEN, c, "meta.json")))
-        assert meta["stab"].split(":")[0] in ("av", "av3d", "blend")
+        assert meta["stab"].split(":")[0] in ("av", "av3d", "blend", "blend3d")
+
+
+@pytest.mark.parametrize("case", [c for c in stab_cases() if c.endswith("_bonanni")])
+def test_host_bonanni_tables_give_reference_values(case):
+    """reference_element.bonanni_tables + the kernel's formula in numpy (per cell: Jacobian from
+    dVgeo, |K|, the integrals of V and grad p; over the mesh p_min, p_max, v_dom; the clipped
+    ratio) against the reference's cellwise coefficient."""
+    from pdekit_b200.reference_element import bonanni_tables
+
+    prob, a, meta, kind, par = _case(case)
+    dim = meta["dim"]
+    g = prob.groups[0]
+    t = bonanni_tables(g.shape, g.order, g.ngeo)
+    assert t["nq"] > 0
+    u = a["u0"]
+    rho = u[:, 0]
+    V = u[:, 1:1 + dim] / rho[:, None]
+    P = (prob.gamma - 1.0) * (u[:, dim + 1] - 0.5 * rho * (V * V).sum(1))
+    X = a["geo_coords"][a["geo_conn"]]  # [nc, ngeo, dim]
+    J = np.einsum("aqg,cgx->cqax", t["dVgeo"], X)  # [nc, nq, xi, x]
+    jw = np.linalg.det(J) * t["w"][None, :]
+    gref = np.einsum("aqn,cn->cqa", t["dV"], P[a["sol_conn"]])
+    gp = np.linalg.solve(J, gref[..., None])[..., 0]
+    vq = np.einsum("qn,cnd->cqd", t["V"], V[a["sol_conn"]])
+    vol = jw.sum(1)
+    vint = (jw[..., None] * vq).sum(1)
+    pint = (jw[..., None] * gp).sum(1)
+    vm, gm = vint / vol[:, None], pint / vol[:, None]
+    f = (vm * gm).sum(1) * np.sqrt((vm * vm).sum(1))
+    vdom = vint.sum(0) / vol.sum()
+    pc = P[a["sol_conn"]]
+    delta = (pc.max() - pc.min()) * (vdom @ vdom)
+    sc = np.maximum(f / delta, 0.0)
+    th = np.minimum(1.0, sc * sc * vol ** (1.0 / dim))
+    assert _rel(th, a["blend_cell"]) < TOL[dim]
