@@ -747,7 +747,7 @@ def run_ours(args, rank, world, local):
         "mixed": dict(rates["mixed"], loop_fp64=rates["fp64"],
                       speedup_per_sweep_vs_fp64_loop=round(rates["mixed"]["value"] /
                                                            rates["fp64"]["value"], 3),
-                      form="defect correction: an exact FP64 sweep every 32 sweeps, FP32 "
+                      form="defect correction: an exact FP64 sweep every 24 sweeps, FP32 "
                            "correction sweeps between (the cell and facet changes computed from "
                            "the correction itself); rds_iterate, no stop test, CUDA events",
                       kernels_ms_per_launch=rates["mixed_kernels_ms_per_launch"],

@@ -360,11 +360,13 @@ RDS_API rds_status rds_get_fields(rds_ctx *ctx, double *res_aos, double *dt, dou
 RDS_API rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int *it_done,
                        double *hist);
 
-/* Options: "mixed_refresh" (default 32): with RDS_MIXED and scalar physics, rds_iterate and
+/* Options: "mixed_refresh" (default 24): with RDS_MIXED and scalar physics, rds_iterate and
  * rds_iterate_batch run the defect-correction loop: an exact FP64 sweep every mixed_refresh
  * sweeps, FP32 correction sweeps between (the change of every contribution computed from the
- * correction itself, the coefficients of the exact sweep's state); the loop stops only at an
- * exact sweep and converges to the FP64 scheme's fixed point.
+ * correction itself, the coefficients and time steps of the exact sweep's state); the loop
+ * stops only at an exact sweep and converges to the FP64 scheme's fixed point. Longer periods
+ * save exact sweeps but hold the time steps longer: at 32, three Burgers P1 N-scheme problems
+ * at CFL 0.53 diverged (RDS_ERR_NONFINITE), none at 24.
  * "mixed_switch" (default 1e-6): with RDS_MIXED and Euler physics (or a stabilisation field
  * installed), rds_iterate runs FP32 cell kernels
  * until max_eq norm/norm(iter 0) <= mixed_switch, or, once that drop has halved at least
@@ -388,8 +390,10 @@ RDS_API rds_status rds_run(rds_ctx *ctx, double cfl, int n);
  * context's residual and dt are those of the last step's first stage, as the reference's solver
  * holds them, so rds_residual_norm / rds_get_fields give what compute_residual_norm and the
  * solver's functions give after advance_in_time. One step is captured in a CUDA graph and
- * replayed; enqueued without waiting. Single-mesh FP64 contexts only (RDS_ERR_UNSUPPORTED
- * otherwise); the three stage buffers are allocated on the first call. */
+ * replayed; enqueued without waiting. The stages run the FP64 cell kernels in every context (a
+ * mixed context's steps equal an FP64 context's). Single-mesh contexts only (batched and
+ * partitioned ones return RDS_ERR_UNSUPPORTED); the three stage buffers are allocated on the
+ * first call. */
 RDS_API rds_status rds_advance_rk3tvd(rds_ctx *ctx, double cfl, int nsteps);
 
 /* Batched independent problems (no counterpart in the reference, which solves one problem per

@@ -78,10 +78,21 @@ def test_rk3tvd_cfl_change_recaptures():
     s.close()
 
 
-def test_rk3tvd_rejects_mixed_context():
-    prob, a, meta = load_golden(os.path.join(GOLDEN, "burgers_p2_b"))
-    s = _solver(prob, "mixed")
-    s.set_solution(a["u0"])
-    with pytest.raises(RDSError):
-        s.advance_rk3tvd(meta["cfl"], 1)
-    s.close()
+@pytest.mark.parametrize("case", ["burgers_p2_b", "euler2d_tri_p2_n"])
+def test_rk3tvd_in_mixed_context_runs_fp64_stages(case):
+    """A mixed context's RK3TVD steps run the FP64 cell kernels: the same bits as an FP64
+    context's, and the oracle's steps to the usual tolerance."""
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    sm, sd = _solver(prob, "mixed"), _solver(prob)
+    for s in (sm, sd):
+        s.set_solution(a["u0"])
+        s.advance_rk3tvd(meta["cfl"], 2)
+    assert np.array_equal(sm.solution(), sd.solution())
+    assert np.array_equal(sm.fields()[0], sd.fields()[0])
+    u, _, _, _ = Oracle(prob).rk3tvd(a["u0"], meta["cfl"], 2)
+    assert rel_err(sm.solution(), u) < TOL
+    # the context's own loop still runs in its precision afterwards
+    sm.set_solution(a["u0"])
+    sm.iterate(meta["cfl"], 3, 0.0)
+    sm.close()
+    sd.close()
