@@ -247,9 +247,9 @@ def group_work(prob):
 PROFILED_TRAFFIC = {
     "c1": (0.30771e6, "profiles/dram_traffic_cell_kernels.md"),
     "c2": (31.508736e6 + 0.380416e6, "profiles/cells_burgers_b_p2_512.md"),
-    "c3": ((102.85 + 118.34 + 193.39 + 220.73) * 1e6,  # both groups, per iteration
-           "profiles/dram_traffic_cell_kernels.md"),
-    "c4": ((91.59 + 271.63) * 1e6, "profiles/dram_traffic_cell_kernels.md"),
+    "c3": ((102.96 + 119.78 + 192.94 + 217.37) * 1e6,  # both groups, per iteration
+           "profiles/cells_euler_c3_c4.md"),
+    "c4": ((91.06 + 268.62) * 1e6, "profiles/cells_euler_c3_c4.md"),
 }
 
 
