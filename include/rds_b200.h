@@ -391,9 +391,10 @@ RDS_API rds_status rds_run(rds_ctx *ctx, double cfl, int n);
  * holds them, so rds_residual_norm / rds_get_fields give what compute_residual_norm and the
  * solver's functions give after advance_in_time. One step is captured in a CUDA graph and
  * replayed; enqueued without waiting. The stages run the FP64 cell kernels in every context (a
- * mixed context's steps equal an FP64 context's). Single-mesh contexts only (batched and
- * partitioned ones return RDS_ERR_UNSUPPORTED); the three stage buffers are allocated on the
- * first call. */
+ * mixed context's steps equal an FP64 context's). In a batched context every problem takes the
+ * steps with its own CFL (cfl is ignored), bit for bit its single-problem steps; partitioned
+ * contexts return RDS_ERR_UNSUPPORTED. The three stage buffers are allocated on the first
+ * call. */
 RDS_API rds_status rds_advance_rk3tvd(rds_ctx *ctx, double cfl, int nsteps);
 
 /* Batched independent problems (no counterpart in the reference, which solves one problem per

@@ -245,6 +245,12 @@ class BatchedRDS:
             self._check(st)
         return iters, rel
 
+    def advance_rk3tvd(self, nsteps: int = 1):
+        """nsteps RK3TVD steps of every problem, each with its own CFL (the single-problem
+        stepper's stages over the batch's kernels, FP64 in both precisions); waits for them."""
+        self._check(lib().rds_advance_rk3tvd(self._ctx, 0.0, int(nsteps)))
+        self._check(lib().rds_check(self._ctx))
+
     def set_option(self, key: str, value: float):
         self._check(lib().rds_set_option(self._ctx, key.encode(), float(value)))
 

@@ -2409,14 +2409,61 @@ static rds_status enqueue_rk3tvd(rds_ctx *ctx, double cfl)
   return st;
 }
 
+// One Runge-Kutta stage of a batched RK3TVD step (enqueue_batch_iteration's gather ends in the
+// stage combination instead of the update, norm and stop test)
+struct RkStage
+{
+  int k;                  // 1, 2, 3
+  const double *un, *us;  // u_n and the stage state
+  double *out;            // u_1, u_2 or u_n+1
+  double ca, cb, cc;
+};
+
+static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed, int dc = 0,
+                                          const RkStage *rk = nullptr);
+
+// One RK3TVD step of every problem of a batched context (the stages of enqueue_rk3tvd over the
+// batch's persistent kernels, each problem with its own CFL).
+static rds_status enqueue_rk3tvd_batch(rds_ctx *ctx)
+{
+  double *const u = ctx->d_u, *const res = ctx->d_res;
+  auto stage = [&](int k) -> rds_status {
+    RkStage rk{};
+    rk.k   = k;
+    rk.un  = u;
+    rk.us  = ctx->d_u;
+    rk.out = k == 1 ? ctx->d_rk_u1 : k == 2 ? ctx->d_rk_u2 : u;
+    rk.ca  = k == 2 ? 3. / 4. : 1. / 3.;
+    rk.cb  = k == 2 ? 1. / 4. : 2. / 3;
+    rk.cc  = k == 2 ? 1. / 4. : 2. / 3.;
+    return enqueue_batch_iteration(ctx, false, 0, &rk);
+  };
+  rds_status st = stage(1);
+  if (st == RDS_OK)
+  {
+    ctx->d_u   = ctx->d_rk_u1;
+    ctx->d_res = ctx->d_rk_res;
+    st         = stage(2);
+  }
+  if (st == RDS_OK)
+  {
+    ctx->d_u = ctx->d_rk_u2;
+    st       = stage(3);
+  }
+  ctx->d_u   = u;
+  ctx->d_res = res;
+  return st;
+}
+
 rds_status rds_advance_rk3tvd(rds_ctx *ctx, double cfl, int nsteps)
 {
   if (!ctx || !ctx->finalized || nsteps <= 0)
     return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_advance_rk3tvd: not finalized or nsteps <= 0")
                : RDS_ERR_INVALID;
-  if (ctx->nprob > 0 || ctx->d_if_nodes)
+  if (ctx->d_if_nodes)
     return fail(ctx, RDS_ERR_UNSUPPORTED,
-                "rds_advance_rk3tvd: single-mesh contexts only (not batched or partitioned)");
+                "rds_advance_rk3tvd: not in partitioned contexts");
+  const bool batched = ctx->nprob > 0;
   // the stages run the FP64 cell kernels in every context (a mixed context's time steps equal
   // an FP64 context's)
   struct Fp64Stages
@@ -2431,24 +2478,37 @@ rds_status rds_advance_rk3tvd(rds_ctx *ctx, double cfl, int nsteps)
   for (double **p : {&ctx->d_rk_u1, &ctx->d_rk_u2, &ctx->d_rk_res})
     if (!*p && (st = dalloc(ctx, p, n)) != RDS_OK)
       return st;
+  if (batched)
+  {
+    // every problem takes part (phase 1: FP64 cells; rds_iterate_batch resets the phases)
+    const std::vector<int32_t> ph(ctx->nprob, 1);
+    const int32_t one = 1;
+    if ((st = upload(ctx, ctx->d_phase, ph.data(), ctx->nprob)) ||
+        (st = upload(ctx, ctx->d_changed, &one, 1)))
+      return st;
+    RDS_CUDA(cudaMemsetAsync(ctx->d_stop, 0, sizeof(int), ctx->stream));
+  }
+  auto step = [&]() { return batched ? enqueue_rk3tvd_batch(ctx) : enqueue_rk3tvd(ctx, cfl); };
   if (ctx->timing)
   {
     for (int i = 0; i < nsteps; ++i)
-      if ((st = enqueue_rk3tvd(ctx, cfl)) != RDS_OK)
+      if ((st = step()) != RDS_OK)
         return st;
     return RDS_OK;
   }
-  // one step captured once (graph slot 5, recaptured when the CFL changes) and replayed
+  // one step captured once (graph slot 5, recaptured when the CFL changes; batched contexts use
+  // their problems' own CFLs) and replayed
   const int gi = 5;
-  if (ctx->graph_exec[gi] && ctx->rk_cfl != cfl)
+  if (ctx->graph_exec[gi] && !batched && ctx->rk_cfl != cfl)
   {
     cudaGraphExecDestroy(ctx->graph_exec[gi]);
     ctx->graph_exec[gi] = nullptr;
   }
   ctx->rk_cfl = cfl;
-  if ((st = capture_graph(ctx, gi, 1, [&] { return enqueue_rk3tvd(ctx, cfl); })) != RDS_OK)
+  if ((st = capture_graph(ctx, gi, 1, step)) != RDS_OK)
     return st;
-  const long long per_step = 3 * ((long long)ctx->groups.size() + (long long)ctx->bcs.size() + 1);
+  const long long per_step = 3 * ((long long)ctx->groups.size() + (long long)ctx->bcs.size() +
+                                  (batched ? 2 : 1));
   for (int i = 0; i < nsteps; ++i)
   {
     RDS_CUDA(cudaGraphLaunch(ctx->graph_exec[gi], ctx->stream));
@@ -2641,7 +2701,7 @@ rds_status rds_add_batch_bc(rds_ctx *ctx, const rds_bc_group *b, int physics)
 // dc: 0 plain iteration (FP32 tiles of the problems in phase 0 when mixed, FP64 tiles of those
 // in phase 1); 1 exact sweep of the defect-correction loop (FP64 cells of every active problem,
 // blending coefficients kept for the corrections); 2 correction sweep (FP32 cell changes).
-static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed, int dc = 0)
+static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed, int dc, const RkStage *rk)
 {
   const rds_desc &d = ctx->desc;
   const int P = ctx->nprob, G = (int)ctx->groups.size();
@@ -2736,6 +2796,16 @@ static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed, int dc = 0)
   ga.dres       = ctx->d_dres;
   ga.dtv        = ctx->d_dtv;
   ga.ur         = ctx->d_ur;
+  if (rk)
+  {
+    ga.rk_first = rk->k == 1;
+    ga.rk_un    = rk->un;
+    ga.rk_us    = rk->us;
+    ga.rk_out   = rk->out;
+    ga.rk_ca    = rk->ca;
+    ga.rk_cb    = rk->cb;
+    ga.rk_cc    = rk->cc;
+  }
   BatchArgs b{};
   b.nprob     = P;
   b.node_off  = ctx->d_node_off;
@@ -2752,7 +2822,8 @@ static rds_status enqueue_batch_iteration(rds_ctx *ctx, bool mixed, int dc = 0)
   b.loop      = ctx->d_loop;
   b.stall     = ctx->d_pstall;
   return launch(ctx, [&](const char **name) {
-    return launch_gather_batch(ga, b, ctx->batch_grid, ctx->stream, name, dc);
+    return launch_gather_batch(ga, b, ctx->batch_grid, ctx->stream, name, dc,
+                               rk ? (rk->k == 1 ? 1 : 2) : 0);
   });
 }
 

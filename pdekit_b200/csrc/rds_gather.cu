@@ -528,7 +528,9 @@ __device__ void problem_final(const GatherArgs &a, const BatchArgs &b, const int
 // splits them, and the block that completes a problem's iteration reduces its norm.
 // DC: 0 plain; 1 exact sweep of the defect-correction loop (also keeps dres / dtv / ur);
 // 2 correction sweep (FP32 changes of every slot, no norm or stop test).
-template <int NEQ, int DC = 0>
+// RKS: a Runge-Kutta stage instead (1 the first: residual, dt and u_1; 2 a later one), with each
+// problem's CFL, no norm or stop test.
+template <int NEQ, int DC = 0, int RKS = 0>
 __global__ void __launch_bounds__(kGBlock)
     gather_batch(const __grid_constant__ GatherArgs a, const __grid_constant__ BatchArgs b)
 {
@@ -550,8 +552,13 @@ __global__ void __launch_bounds__(kGBlock)
     for (int e = 0; e < NEQ; ++e)
       sq[e] = 0.0;
     if (v < n1)
-      gather_node<NEQ, DC != 2, DC != 2, DC != 2, false, DC>(a, v, b.cfl[p], sq);
-    if (DC == 2)
+    {
+      if constexpr (RKS != 0)
+        gather_node<NEQ, RKS == 1, false, false, true, 0>(a, v, b.cfl[p], sq);
+      else
+        gather_node<NEQ, DC != 2, DC != 2, DC != 2, false, DC>(a, v, b.cfl[p], sq);
+    }
+    if (DC == 2 || RKS != 0)
       continue; // uniform over the block: no barrier is skipped by part of it
     const int slot = b.nb_base[p] + j;
 #pragma unroll
@@ -789,8 +796,30 @@ cudaError_t launch_dual_volume(int nnodes, const int32_t *row, const int32_t *en
 }
 
 cudaError_t launch_gather_batch(const GatherArgs &a, const BatchArgs &b, int grid, cudaStream_t s,
-                                const char **name, int dc)
+                                const char **name, int dc, int rk)
 {
+  if (rk == 1 || rk == 2)
+  {
+    *name = "gather_batch_rk_stage";
+    switch (a.neq)
+    {
+    case 1:
+      rk == 1 ? gather_batch<1, 0, 1><<<grid, kGBlock, 0, s>>>(a, b)
+              : gather_batch<1, 0, 2><<<grid, kGBlock, 0, s>>>(a, b);
+      break;
+    case 4:
+      rk == 1 ? gather_batch<4, 0, 1><<<grid, kGBlock, 0, s>>>(a, b)
+              : gather_batch<4, 0, 2><<<grid, kGBlock, 0, s>>>(a, b);
+      break;
+    case 5:
+      rk == 1 ? gather_batch<5, 0, 1><<<grid, kGBlock, 0, s>>>(a, b)
+              : gather_batch<5, 0, 2><<<grid, kGBlock, 0, s>>>(a, b);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+  }
   if (dc == 1 || dc == 2)
   {
     if (a.neq != 1)

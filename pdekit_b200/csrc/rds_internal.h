@@ -332,7 +332,8 @@ cudaError_t launch_cells_scalar_batch(const HostCellGroup &g, const CellArgs &a,
 // dc: 0 plain, 1 exact sweep of the defect-correction loop (keeps rcell / ur), 2 correction
 // sweep (no norm, no stop test).
 cudaError_t launch_gather_batch(const GatherArgs &a, const BatchArgs &b, int grid, cudaStream_t s,
-                                const char **name, int dc = 0);
+                                const char **name, int dc = 0,
+                                int rk = 0);
 cudaError_t launch_batch_rebuild(const RebuildArgs &r, cudaStream_t s, const char **name);
 // Mixed form, scalar physics on straight-sided triangles: the cell kernel with the basis
 // contractions on the tensor cores (persistent over 128-cell tiles; batch: active tiles).

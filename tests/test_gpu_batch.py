@@ -111,3 +111,36 @@ def test_batch_tensor_core_cells(batch_case):
         b.close()
     for u0, u1 in zip(us[0], us[1]):
         assert np.linalg.norm(u1 - u0) <= 1e-9 * np.linalg.norm(u0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_rk3tvd_equals_single_problem_steps(batch_case, precision):
+    """RK3TVD in a batched context: every problem takes three steps with its own CFL through the
+    batch's persistent kernels, bit for bit the steps of its own single-problem context (FP64
+    stages in both precisions); a later iterate still runs the batch's own loop."""
+    from pdekit_b200.batch import BatchedRDS
+    from pdekit_b200.rds import PGRDMethodExplicit
+
+    probs, states, cfls, info = batch_case
+    b = BatchedRDS(probs, cfls, precision)
+    b.set_solutions(states)
+    b.advance_rk3tvd(3)
+    got = b.solutions()
+    for prob, u0, cfl, ub in zip(probs, states, cfls, got):
+        s = PGRDMethodExplicit(prob.physics, prob.scheme, "fp64").configure_mesh_data(prob)
+        s.initialize_work_data()
+        s.set_solution(u0)
+        s.advance_rk3tvd(float(cfl), 3)
+        assert np.array_equal(s.solution(), ub)
+        s.close()
+    # the batch's own loop afterwards: as from a batch that never stepped
+    b.set_solutions(states)
+    it, _ = b.iterate(200, 0.0, raise_on_cap=False)
+    u = b.solutions()
+    b.close()
+    b2 = BatchedRDS(probs, cfls, precision)
+    b2.set_solutions(states)
+    it2, _ = b2.iterate(200, 0.0, raise_on_cap=False)
+    assert np.array_equal(it, it2)
+    assert all(np.array_equal(x, y) for x, y in zip(u, b2.solutions()))
+    b2.close()
