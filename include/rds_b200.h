@@ -346,6 +346,24 @@ RDS_API rds_status rds_gather_rhs(rds_ctx *ctx, int v0, int v1);
 RDS_API rds_status rds_gather_finish(rds_ctx *ctx, int v0, int v1, double cfl, double *sq);
 RDS_API rds_status rds_finish_nodes(rds_ctx *ctx, double cfl, int update, int v0, int v1,
                                     double *sq);
+
+/* RK3TVD in a partitioned context (RK3TVD::advance_in_time, solver/time/ExplicitTimeStepper.cpp:
+ * 66-100, with the exchange in every stage): per stage k = 1, 2, 3
+ *   rds_rk_stage_state(ctx, k): the following calls read the stage state (u_n, u_1, u_2) and
+ *     write the stage residual (the context's own, then a scratch buffer), as the reference's
+ *     stepper points its solver at them; rds_rk_stage_state(ctx, 0) restores the context's
+ *     own state and residual (required before any other call); the first call allocates the
+ *     stage buffers (make it outside a stream capture);
+ *   the assembly of the partitioned iteration (rds_assemble_rhs_cells, rds_gather_rhs over the
+ *     interface nodes, rds_pack_interface, the sum over the ranks, rds_unpack_interface);
+ *   rds_gather_rk: the nodal sums of nodes [v0, v1) ending in the stage combination (stage 1:
+ *     dt = CFL V / ws and u_1 = u_n - dt r; 2: u_2 = 3/4 u_n + 1/4 u_1 - 1/4 dt r; 3:
+ *     u_n+1 = 1/3 u_n + 2/3 u_2 - 2/3 dt r, dt of stage 1), for the nodes complete on the rank;
+ *   rds_combine_rk: the same combination for nodes [v0, v1) from their summed residual and wave
+ *     speed (the interface nodes, after the exchange). */
+RDS_API rds_status rds_rk_stage_state(rds_ctx *ctx, int stage);
+RDS_API rds_status rds_gather_rk(rds_ctx *ctx, int v0, int v1, double cfl);
+RDS_API rds_status rds_combine_rk(rds_ctx *ctx, int v0, int v1, double cfl);
 RDS_API rds_status rds_check(rds_ctx *ctx);
 
 /* Copy out any of: residual [node][neq], dt [node], nodal wave speed [node], dual volume [node]
@@ -393,8 +411,8 @@ RDS_API rds_status rds_run(rds_ctx *ctx, double cfl, int n);
  * replayed; enqueued without waiting. The stages run the FP64 cell kernels in every context (a
  * mixed context's steps equal an FP64 context's). In a batched context every problem takes the
  * steps with its own CFL (cfl is ignored), bit for bit its single-problem steps; partitioned
- * contexts return RDS_ERR_UNSUPPORTED. The three stage buffers are allocated on the first
- * call. */
+ * contexts return RDS_ERR_UNSUPPORTED (their steps: rds_rk_stage_state, rds_gather_rk,
+ * rds_combine_rk below). The three stage buffers are allocated on the first call. */
 RDS_API rds_status rds_advance_rk3tvd(rds_ctx *ctx, double cfl, int nsteps);
 
 /* Batched independent problems (no counterpart in the reference, which solves one problem per

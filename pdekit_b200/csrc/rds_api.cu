@@ -126,6 +126,8 @@ struct rds_ctx
 
   // Runge-Kutta stage states u_1, u_2 and the later stages' residual (SoA [neq][nnodes])
   double *d_rk_u1 = nullptr, *d_rk_u2 = nullptr, *d_rk_res = nullptr;
+  int rk_stage = 0; // partitioned RK3TVD: the stage rds_rk_stage_state selected (0: none)
+  double *rk_base_u = nullptr, *rk_base_res = nullptr; // the context's own state / residual
 
   // precision of the cell kernels being launched (the mixed loop finishes in FP64)
   int active_precision = RDS_FP64;
@@ -2012,6 +2014,86 @@ rds_status rds_finish_nodes(rds_ctx *ctx, double cfl, int update, int v0, int v1
     return launch_finish(v0, v1, ctx->desc.nnodes, ctx->desc.neq, cfl, update, ctx->d_vol,
                          ctx->d_ws, ctx->d_res, ctx->d_dt, ctx->d_u, ctx->d_owned, ctx->d_part,
                          off, ctx->d_counter, sq, ctx->stream);
+  });
+}
+
+static rds_status rk_buffers(rds_ctx *ctx)
+{
+  rds_status st;
+  const size_t n = (size_t)ctx->desc.nnodes * ctx->desc.neq;
+  for (double **p : {&ctx->d_rk_u1, &ctx->d_rk_u2, &ctx->d_rk_res})
+    if (!*p && (st = dalloc(ctx, p, n)) != RDS_OK)
+      return st;
+  return RDS_OK;
+}
+
+// RK3TVD stage coefficients (solver/time/ExplicitTimeStepper.cpp:66-100)
+static void rk_coeffs(int k, double &ca, double &cb, double &cc)
+{
+  ca = k == 2 ? 3. / 4. : 1. / 3.;
+  cb = k == 2 ? 1. / 4. : 2. / 3;
+  cc = k == 2 ? 1. / 4. : 2. / 3.;
+}
+
+rds_status rds_rk_stage_state(rds_ctx *ctx, int stage)
+{
+  if (!ctx || !ctx->finalized || stage < 0 || stage > 3)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_rk_stage_state: stage 0-3 of a finalized context")
+               : RDS_ERR_INVALID;
+  rds_status st = rk_buffers(ctx);
+  if (st != RDS_OK)
+    return st;
+  if (ctx->rk_stage == 0)
+  {
+    ctx->rk_base_u   = ctx->d_u;
+    ctx->rk_base_res = ctx->d_res;
+  }
+  ctx->d_u      = stage <= 1 ? ctx->rk_base_u : stage == 2 ? ctx->d_rk_u1 : ctx->d_rk_u2;
+  ctx->d_res    = stage <= 1 ? ctx->rk_base_res : ctx->d_rk_res;
+  ctx->rk_stage = stage;
+  return RDS_OK;
+}
+
+rds_status rds_gather_rk(rds_ctx *ctx, int v0, int v1, double cfl)
+{
+  if (!ctx || !ctx->finalized || ctx->rk_stage == 0)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_gather_rk: select a stage (rds_rk_stage_state)")
+               : RDS_ERR_INVALID;
+  if (v0 < 0 || v1 < v0 || v1 > ctx->desc.nnodes)
+    return fail(ctx, RDS_ERR_INVALID, "rds_gather_rk: node range out of bounds");
+  if (v1 == v0)
+    return RDS_OK;
+  const int k   = ctx->rk_stage;
+  GatherArgs ga = gather_args(ctx, k == 1 ? cfl : 0.0, ctx->d_zero);
+  ga.vbeg       = v0;
+  ga.vend       = v1;
+  ga.rk_first   = k == 1;
+  ga.rk_un      = ctx->rk_base_u;
+  ga.rk_us      = ctx->d_u;
+  ga.rk_out     = k == 1 ? ctx->d_rk_u1 : k == 2 ? ctx->d_rk_u2 : ctx->rk_base_u;
+  rk_coeffs(k, ga.rk_ca, ga.rk_cb, ga.rk_cc);
+  const int nb = (v1 - v0 + kGBlock - 1) / kGBlock;
+  return launch(ctx, [&](const char **name) {
+    return launch_gather(ga, k == 1 ? 17 : 16, nb, ctx->stream, name);
+  });
+}
+
+rds_status rds_combine_rk(rds_ctx *ctx, int v0, int v1, double cfl)
+{
+  if (!ctx || !ctx->finalized || ctx->rk_stage == 0)
+    return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_combine_rk: select a stage (rds_rk_stage_state)")
+               : RDS_ERR_INVALID;
+  if (v0 < 0 || v1 < v0 || v1 > ctx->desc.nnodes)
+    return fail(ctx, RDS_ERR_INVALID, "rds_combine_rk: node range out of bounds");
+  const int k = ctx->rk_stage;
+  double ca, cb, cc;
+  rk_coeffs(k, ca, cb, cc);
+  double *out = k == 1 ? ctx->d_rk_u1 : k == 2 ? ctx->d_rk_u2 : ctx->rk_base_u;
+  return launch(ctx, [&](const char **name) {
+    *name = "rk_combine";
+    return launch_rk_combine(v0, v1, ctx->desc.nnodes, ctx->desc.neq, k == 1, cfl, ca, cb, cc,
+                             ctx->d_vol, ctx->d_ws, ctx->d_res, ctx->d_dt, ctx->rk_base_u,
+                             ctx->d_u, out, ctx->stream);
   });
 }
 

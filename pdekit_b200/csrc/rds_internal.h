@@ -363,6 +363,10 @@ cudaError_t launch_pack_interface(int n, int neq, int nnodes, const int32_t *nod
 cudaError_t launch_unpack_interface(int n, int neq, int nnodes, const int32_t *nodes,
                                     const int32_t *slots, const double *buf, double *res,
                                     double *ws, cudaStream_t s);
+cudaError_t launch_rk_combine(int v0, int v1, int nnodes, int neq, int first, double cfl, double ca,
+                              double cb, double cc, const double *vol, const double *ws,
+                              const double *res, double *dt, const double *un, const double *us,
+                              double *out, cudaStream_t s);
 cudaError_t launch_finish(int v0, int v1, int nnodes, int neq, double cfl, int update,
                           const double *vol, const double *ws, const double *res, double *dt,
                           double *u, const uint8_t *owned, double *part, int part_off,

@@ -7,6 +7,8 @@
 //   pack     buf[slot][0..neq-1] = res[.][v], buf[slot][neq] = ws[v] for the shared nodes v
 //            (the buffer is zeroed first, so a sum over the ranks' buffers is the full sum)
 //   unpack   res[.][v], ws[v] = buf[slot] (after the sum over the ranks)
+//   combine  a Runge-Kutta stage of nodes whose sums came through the exchange (partitioned
+//            RK3TVD), with the arithmetic of the gather's stage branch
 //   finish   dt = CFL V / ws, u -= dt res, and per block the sum over the nodes this rank owns
 //            of (res dt)^2 (for a node range, after the block sums of the other nodes that
 //            rds_gather_finish wrote); the block that finishes last adds the block sums in a
@@ -135,6 +137,37 @@ __global__ void __launch_bounds__(kGBlock)
     *counter = 0u;
 }
 
+
+// Runge-Kutta stage combination of nodes [v0, v1) from their summed residual and wave speed
+// (after the exchange): the arithmetic of gather_node's stage branch (rds_gather.cu).
+__global__ void __launch_bounds__(kGBlock)
+    rk_combine(int v0, int v1, int nnodes, int neq, int first, double cfl, double ca, double cb,
+               double cc, const double *__restrict__ vol, const double *__restrict__ ws,
+               const double *__restrict__ res, double *__restrict__ dt,
+               const double *__restrict__ un, const double *__restrict__ us,
+               double *__restrict__ out)
+{
+  const int v = v0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= v1)
+    return;
+  double d;
+  if (first)
+  {
+    d     = __ddiv_rn(__dmul_rn(cfl, vol[v]), ws[v]);
+    dt[v] = d;
+  }
+  else
+    d = dt[v];
+  for (int e = 0; e < neq; ++e)
+  {
+    const size_t k = (size_t)e * nnodes + v;
+    const double r = __dmul_rn(d, res[k]);
+    out[k]         = first ? __dsub_rn(un[k], r)
+                           : __dsub_rn(__dadd_rn(__dmul_rn(ca, un[k]), __dmul_rn(cb, us[k])),
+                                       __dmul_rn(cc, r));
+  }
+}
+
 } // namespace
 
 cudaError_t launch_pack_interface(int n, int neq, int nnodes, const int32_t *nodes,
@@ -169,6 +202,19 @@ cudaError_t launch_finish(int v0, int v1, int nnodes, int neq, double cfl, int u
   const int nb = std::max(1, (v1 - v0 + kGBlock - 1) / kGBlock);
   finish_nodes<<<nb, kGBlock, 0, s>>>(v0, v1, nnodes, neq, cfl, update, vol, ws, res, dt, u,
                                       owned, part, part_off, counter, sq);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rk_combine(int v0, int v1, int nnodes, int neq, int first, double cfl, double ca,
+                              double cb, double cc, const double *vol, const double *ws,
+                              const double *res, double *dt, const double *un, const double *us,
+                              double *out, cudaStream_t s)
+{
+  if (v1 <= v0)
+    return cudaSuccess;
+  rk_combine<<<(v1 - v0 + kGBlock - 1) / kGBlock, kGBlock, 0, s>>>(v0, v1, nnodes, neq, first, cfl,
+                                                                  ca, cb, cc, vol, ws, res, dt, un,
+                                                                  us, out);
   return cudaGetLastError();
 }
 

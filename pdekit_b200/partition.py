@@ -215,6 +215,27 @@ class RankSolver:
         self._check(lib().rds_gather_finish(ctx, len(p.if_nodes), p.problem.nnodes, float(cfl),
                                             sq))
 
+    # ---- RK3TVD stages (the stage state and residual selected by rk_select)
+    def rk_select(self, stage: int):
+        """Stage 1-3: the following phases read u_n, u_1, u_2 and write the stage residual;
+        0: back to the context's own state and residual."""
+        self._check(lib().rds_rk_stage_state(self.solver._ctx, int(stage)))
+
+    def rk_interior(self, cfl: float):
+        """The other cells, and the other nodes' sums ending in the stage combination."""
+        ctx, p = self.solver._ctx, self.part
+        alone = len(p.if_nodes) == 0
+        self._check(lib().rds_assemble_rhs_cells(ctx, p.n_if_groups, len(p.problem.groups),
+                                                 int(alone)))
+        self._check(lib().rds_gather_rk(ctx, len(p.if_nodes), p.problem.nnodes, float(cfl)))
+
+    def rk_interface(self, cfl: float):
+        """After the exchange: the interface nodes' summed residual and their combination."""
+        ctx, n_if = self.solver._ctx, len(self.part.if_nodes)
+        if n_if:
+            self._check(lib().rds_unpack_interface(ctx, C.c_void_p(self.buf.data_ptr())))
+            self._check(lib().rds_combine_rk(ctx, 0, n_if, float(cfl)))
+
     def assemble_and_pack(self, cfl: float):
         """This rank's partial sums at the interface nodes into self.buf, the other nodes
         finished."""
@@ -290,6 +311,48 @@ class PartitionedRDS:
             self.rank.unpack_and_finish(cfl, norm)
             if norm:
                 self._sum(self.rank.sq)
+
+    def rk3tvd_step(self, cfl: float):
+        """One RK3TVD step (RK3TVD::advance_in_time), enqueued: per stage the interface cells
+        and sums, their sum over the ranks while the interior cells run and finish their stage
+        combination, then the interface nodes' combination."""
+        import torch
+
+        r = self.rank
+        with torch.cuda.stream(r.stream):
+            for k in (1, 2, 3):
+                r.rk_select(k)
+                r.assemble_interface()
+                work = self._sum_async(r.buf) if self.partition.nslots else None
+                r.rk_interior(cfl)
+                if work is not None:
+                    work.wait()
+                r.rk_interface(cfl)
+            r.rk_select(0)
+
+    def graph_rk3tvd(self, cfl: float, nsteps: int = 1):
+        """nsteps rk3tvd_step through a CUDA graph of one step (captured at the first call for
+        this cfl, NCCL calls included); eager where capture is not possible."""
+        import torch
+
+        for _ in range(nsteps):
+            if not self._graphs_ok:
+                self.rk3tvd_step(cfl)
+                continue
+            key = ("rk3tvd", cfl)
+            if key not in self._graphs:
+                self.rank.rk_select(0)  # allocates the stage buffers outside the capture
+                stream = self.rank.stream
+                stream.synchronize()
+                n0 = self.rank.solver.launch_count()
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, stream=stream):
+                    self.rk3tvd_step(cfl)
+                self._graphs[key] = (g, self.rank.solver.launch_count() - n0)
+            g, n = self._graphs[key]
+            with torch.cuda.stream(self.rank.stream):
+                g.replay()
+            self.graph_launches += n
 
     def graph_step(self, cfl: float, norm: bool = True):
         """step() through a CUDA graph of one step, captured at the first call for this
@@ -394,3 +457,47 @@ def emulate(prob: Problem, nparts: int, u0, cfl: float, iters: int, precision: s
     for r in ranks:
         r.close()
     return u, norms
+
+
+def emulate_rk3tvd(prob: Problem, nparts: int, u0, cfl: float, nsteps: int,
+                   precision: str = "fp64"):
+    """RK3TVD steps of a partitioned problem with all ranks in one process on one GPU (as
+    `emulate`: every rank's phases in turn, the sums between them with the device synchronised).
+    Returns the global state after `nsteps` steps."""
+    import torch
+
+    pt = partition(prob, nparts)
+    ranks = [RankSolver(p, pt.nslots, precision) for p in pt.parts]
+    vol = np.zeros(prob.nnodes)
+    for r in ranks:
+        vol[r.part.nodes] += r.local_volume()
+    for r in ranks:
+        r.set_volume(vol[r.part.nodes])
+        r.set_solution(u0)
+    for _ in range(nsteps):
+        for k in (1, 2, 3):
+            for r in ranks:
+                r.rk_select(k)
+                r.assemble_interface()
+                r.rk_interior(cfl)
+            torch.cuda.synchronize()
+            if pt.nslots:
+                total = sum(r.buf for r in ranks)
+                for r in ranks:
+                    r.buf.copy_(total)
+            torch.cuda.synchronize()
+            for r in ranks:
+                r.rk_interface(cfl)
+        for r in ranks:
+            r.rk_select(0)
+    torch.cuda.synchronize()
+    for r in ranks:
+        r.check()
+    u = np.zeros((prob.nnodes, prob.neq))
+    for r in ranks:
+        own = r.part.owned.astype(bool)
+        u[r.part.nodes[own]] = r.solution()[own]
+    for r in ranks:
+        r.close()
+    return u
+

@@ -129,6 +129,9 @@ def lib():
         "rds_assemble_rhs_cells": ([vp, ip, ip, ip], ip),
         "rds_gather_rhs": ([vp, ip, ip], ip),
         "rds_gather_finish": ([vp, ip, ip, dp, vp], ip),
+        "rds_rk_stage_state": ([vp, ip], ip),
+        "rds_gather_rk": ([vp, ip, ip, dp], ip),
+        "rds_combine_rk": ([vp, ip, ip, dp], ip),
         "rds_finish_nodes": ([vp, dp, ip, ip, ip, vp], ip),
         "rds_check": ([vp], ip),
         "rds_element_jacobians": ([vp, ip, vp], ip),

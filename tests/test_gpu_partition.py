@@ -72,3 +72,41 @@ def test_one_rank_graph_steps_match_single_context(case):
     assert rel_err(u, u1) < 1e-12
     np.testing.assert_allclose(np.array(norms), hist[0::2], rtol=1e-11)
     assert pr.graph_launches > 0
+
+
+def _single_rk(prob, u0, cfl, nsteps):
+    s = PGRDMethodExplicit(prob.physics, prob.scheme, "fp64").configure_mesh_data(prob)
+    s.initialize_work_data()
+    s.set_solution(u0)
+    s.advance_rk3tvd(cfl, nsteps)
+    u = s.solution()
+    s.close()
+    return u
+
+
+@pytest.mark.parametrize("case", ["burgers_p2_b", "euler2d_tri_p3_b", "euler3d_tet_p2_lda",
+                                  "euler2d_tri_p2_farfield"])
+@pytest.mark.parametrize("nparts", [2, 3])
+def test_partitioned_rk3tvd_matches_single_context(case, nparts):
+    """RK3TVD with the exchange in every stage, ranks emulated on one GPU, against the single
+    context's device stepper (which the reference's RK3TVD pins)."""
+    from pdekit_b200.partition import emulate_rk3tvd
+
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    u = emulate_rk3tvd(prob, nparts, a["u0"], meta["cfl"], 2)
+    assert rel_err(u, _single_rk(prob, a["u0"], meta["cfl"], 2)) < 1e-12
+
+
+@pytest.mark.parametrize("case", ["burgers_p2_b", "euler2d_tri_p2_n"])
+def test_one_rank_rk3tvd_graph_matches_single_context(case):
+    from pdekit_b200.partition import PartitionedRDS
+
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    pr = PartitionedRDS(prob, 0, 1)
+    try:
+        pr.set_solution(a["u0"])
+        pr.graph_rk3tvd(meta["cfl"], 3)
+        u = pr.solution_global()
+    finally:
+        pr.close()
+    assert rel_err(u, _single_rk(prob, a["u0"], meta["cfl"], 3)) < 1e-13
