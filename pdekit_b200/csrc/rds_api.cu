@@ -150,6 +150,7 @@ struct rds_ctx
   int dc_m           = 24; // 32 let 3 of configuration 5's Burgers P1 problems diverge
   int dc_phase       = 0; // launch_residual_kernels: 0 plain, 1 exact DC sweep, 2 correction
   int part_used      = 0;     // norm partials written by rds_gather_finish (partitioned)
+  int tc_test_wait   = 0;     // option "tc_test_wait" (the bounded-wait test)
   int grp_beg        = 0;     // launch_residual_kernels: cell groups [grp_beg, grp_end)
   int grp_end        = -1;    //   (-1: all) and the weak conditions unless no_bcs
   bool no_bcs        = false;
@@ -315,6 +316,7 @@ CellArgs cell_args(rds_ctx *ctx, const HostCellGroup &g, const int *stop)
   a.status     = ctx->d_status;
   a.stop       = stop;
   a.blend      = ctx->blend_on ? ctx->d_blend : nullptr;
+  a.tc_test_wait = ctx->tc_test_wait;
   return a;
 }
 
@@ -2608,6 +2610,16 @@ rds_status rds_set_option(rds_ctx *ctx, const char *key, double value)
     if (!(value > 0.0 && value < 1.0))
       return fail(ctx, RDS_ERR_INVALID, "mixed_switch must be in (0, 1)");
     ctx->mixed_switch = value;
+    return RDS_OK;
+  }
+  if (std::strcmp(key, "tc_test_wait") == 0)
+  {
+    // test of the tensor-core kernel's bounded wait: each CTA first waits up to `value` tries on
+    // a barrier nothing completes, so the call reports the timeout (0: off)
+    if (!(value >= 0.0 && value <= 1048576.0))
+      return fail(ctx, RDS_ERR_INVALID, "tc_test_wait must be in [0, 2^20]");
+    ctx->tc_test_wait = (int)value;
+    release_graph(ctx);
     return RDS_OK;
   }
   if (std::strcmp(key, "tensor_cores") == 0)

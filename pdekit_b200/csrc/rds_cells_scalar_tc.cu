@@ -110,10 +110,10 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar)
                : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase)
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, int limit = 1 << 22)
 {
-  // bounded: every try_wait suspends for a limited time; give up after 2^22 tries
-  for (int i = 0; i < (1 << 22); ++i)
+  // bounded: every try_wait suspends for a limited time; give up after `limit` tries
+  for (int i = 0; i < limit; ++i)
   {
     uint32_t done;
     asm volatile("{\n\t.reg .pred P1;\n\t"
@@ -182,6 +182,7 @@ __global__ void __launch_bounds__(kTcCells)
   float *sB2h = sB1l + TD::N1 * TD::K1;
   float *sB2l = sB2h + TD::N2 * TD::K2;
   __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar_idle; // nothing arrives on it (the timeout test)
   __shared__ uint32_t tmem_base;
 
   const int tid  = threadIdx.x;
@@ -195,6 +196,7 @@ __global__ void __launch_bounds__(kTcCells)
   if (tid == 0)
   {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar_idle)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0)
@@ -211,6 +213,10 @@ __global__ void __launch_bounds__(kTcCells)
   const uint32_t mb    = smem_addr(&mbar);
   uint32_t phase       = 0;
   bool timed_out       = false;
+  // test of the bounded-wait path: a limited wait on a barrier that nothing completes runs out,
+  // and the kernel goes on as after a timed-out commit (status bit, TMEM released)
+  if (a.tc_test_wait > 0 && !mbar_wait(smem_addr(&mbar_idle), 0u, a.tc_test_wait))
+    timed_out = true;
 
   const uint32_t aAh = smem_addr(sAh), aAl = smem_addr(sAl);
   const uint32_t aB1h = smem_addr(sB1h), aB1l = smem_addr(sB1l);

@@ -191,6 +191,7 @@ struct CellArgs
   const double *blend; // PGB: external nodal blending coefficient [nnodes] when not null
   int pdl;         // launch with programmatic dependent launch (loop graphs)
   const void *lt;  // Euler cells: lane-indexed tables in the kernel's precision (set at launch)
+  int tc_test_wait; // tensor-core cells: tries of a wait nothing completes (timeout test; 0 none)
 };
 
 // FP32 correction sweep of the defect-correction loop (rds_cells_scalar_dc.cu): the change of
@@ -212,6 +213,7 @@ struct DcCellArgs
   BatchTileMap bt; // batch form only
   int pdl;         // launch with programmatic dependent launch (loop graphs)
   const void *lt;  // Euler cells: lane-indexed tables in the kernel's precision (set at launch)
+  int tc_test_wait; // tensor-core cells: tries of a wait nothing completes (timeout test; 0 none)
 };
 
 struct BCArgs

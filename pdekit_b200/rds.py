@@ -383,6 +383,11 @@ class PGRDMethodExplicit:
     def set_option(self, key: str, value: float):
         self._check(lib().rds_set_option(self._ctx, key.encode(), float(value)))
 
+    def check(self):
+        """Waits for the context's stream and raises the status the device recorded (a
+        non-finite norm, a non-positive pressure, a bounded wait that gave up)."""
+        self._check(lib().rds_check(self._ctx))
+
     def run(self, cfl: float, n: int):
         """Enqueue n fused iterations without waiting (for event timing on stream_handle())."""
         self._check(lib().rds_run(self._ctx, float(cfl), int(n)))

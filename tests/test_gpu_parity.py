@@ -10,7 +10,7 @@ from conftest import GOLDEN, golden_cases
 from helpers import rel_err
 from oracle.rds_oracle import Oracle
 from golden_io import load_golden
-from pdekit_b200.rds import PGRDMethodExplicit
+from pdekit_b200.rds import PGRDMethodExplicit, RDSError
 
 pytestmark = pytest.mark.gpu
 
@@ -164,3 +164,33 @@ def test_tensor_core_contraction_matches_fp32_path(case):
     for i in range(3):
         ref, got = out[0][i], out[1][i]
         assert np.abs(got - ref).max() <= 2e-6 * np.abs(ref).max(), (case, i)
+
+
+def test_tensor_core_bounded_wait_reports_timeout_and_recovers():
+    """The tensor-core kernel's bounded mbarrier wait: with the test option each CTA waits a few
+    tries on a barrier that nothing completes; the call reports the timeout (RDS_ERR_CUDA, the
+    bounded-wait message), TMEM is released, and the context then runs as a fresh one."""
+    prob, a, meta = load_golden(os.path.join(GOLDEN, "burgers_p2_b"))
+    cfl = meta["cfl"]
+    s = _solver(prob, "mixed")
+    s.set_option("tensor_cores", 1)
+    s.set_option("tc_test_wait", 64)
+    s.set_solution(a["u0"])
+    s.run(cfl, 2)
+    with pytest.raises(RDSError) as err:
+        s.check()
+    assert err.value.status == 2 and "bounded device wait" in str(err.value)
+    s.set_option("tc_test_wait", 0)
+    s.set_solution(a["u0"])
+    s.iterate(cfl, 1, 0.0)  # clears the status word
+    s.set_solution(a["u0"])
+    s.run(cfl, 3)
+    s.check()
+    u = s.solution()
+    s.close()
+    f = _solver(prob, "mixed")
+    f.set_option("tensor_cores", 1)
+    f.set_solution(a["u0"])
+    f.run(cfl, 3)
+    assert np.array_equal(u, f.solution())
+    f.close()
