@@ -150,6 +150,10 @@ struct rds_ctx
   int dc_m           = 24; // 32 let 3 of configuration 5's Burgers P1 problems diverge
   int dc_phase       = 0; // launch_residual_kernels: 0 plain, 1 exact DC sweep, 2 correction
   int part_used      = 0;     // norm partials written by rds_gather_finish (partitioned)
+  LoopParams *h_loop = nullptr;   // pinned host copy of the loop parameters (set_loop_params)
+  cudaEvent_t ev_loop = nullptr;  // the last copy from it
+  LoopParams loop_last{};         // the parameters on the device
+  bool loop_set = false;
   int tc_test_wait   = 0;     // option "tc_test_wait" (the bounded-wait test)
   int grp_beg        = 0;     // launch_residual_kernels: cell groups [grp_beg, grp_end)
   int grp_end        = -1;    //   (-1: all) and the weak conditions unless no_bcs
@@ -1680,6 +1684,10 @@ rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
     if (need > ctx->bon_len)
     {
       cudaFree(ctx->d_bon);
+  if (ctx->h_loop)
+    cudaFreeHost(ctx->h_loop);
+  if (ctx->ev_loop)
+    cudaEventDestroy(ctx->ev_loop);
       ctx->d_bon   = nullptr;
       ctx->bon_len = 0;
       if ((st = dalloc(ctx, &ctx->d_bon, need)) != RDS_OK)
@@ -2150,6 +2158,29 @@ static rds_status enqueue_iteration(rds_ctx *ctx, double cfl, int max_iter, doub
   });
 }
 
+// The loop parameters to the device: from a pinned host copy, and only when they changed, so the
+// per-step paths (rds_run, rds_step_host) issue no copy (a copy from pageable memory, like a
+// stack variable, lets the driver synchronise with the stream). Not inside a stream capture.
+extern "C++" static rds_status set_loop_params(rds_ctx *ctx, const LoopParams &lp)
+{
+  if (ctx->loop_set && std::memcmp(&ctx->loop_last, &lp, sizeof(LoopParams)) == 0)
+    return RDS_OK;
+  if (!ctx->h_loop)
+  {
+    RDS_CUDA(cudaMallocHost((void **)&ctx->h_loop, sizeof(LoopParams)));
+    RDS_CUDA(cudaEventCreateWithFlags(&ctx->ev_loop, cudaEventDisableTiming));
+  }
+  else
+    RDS_CUDA(cudaEventSynchronize(ctx->ev_loop)); // the previous copy has read the buffer
+  *ctx->h_loop = lp;
+  RDS_CUDA(cudaMemcpyAsync(ctx->d_loop, ctx->h_loop, sizeof(LoopParams), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  RDS_CUDA(cudaEventRecord(ctx->ev_loop, ctx->stream));
+  ctx->loop_last = lp;
+  ctx->loop_set  = true;
+  return RDS_OK;
+}
+
 // Captures `count` iterations (enqueued by `one`) into graph slot gi once; later calls reuse
 // it.
 extern "C++" template <typename F>
@@ -2224,7 +2255,8 @@ static rds_status run_loop(rds_ctx *ctx, double cfl, int max_iter, double drop)
   lp.stall      = ctx->active_precision == RDS_MIXED ? 1 : 0;
   lp.stall_min  = ctx->stall_min;
   lp.stall_mult = ctx->stall_mult;
-  RDS_CUDA(cudaMemcpyAsync(ctx->d_loop, &lp, sizeof(lp), cudaMemcpyHostToDevice, ctx->stream));
+  if ((st = set_loop_params(ctx, lp)) != RDS_OK)
+    return st;
   if (ctx->timing)
   {
     // event timing wants plain launches: run the loop without a graph
@@ -2293,7 +2325,8 @@ static rds_status run_loop_dc(rds_ctx *ctx, double cfl, int max_iter, double dro
   lp.drop     = drop;
   lp.max_iter = max_iter;
   lp.dc_m     = m;
-  RDS_CUDA(cudaMemcpyAsync(ctx->d_loop, &lp, sizeof(lp), cudaMemcpyHostToDevice, ctx->stream));
+  if ((st = set_loop_params(ctx, lp)) != RDS_OK)
+    return st;
   ctx->active_precision = RDS_FP64;
   if (ctx->timing)
   {
@@ -2428,7 +2461,8 @@ rds_status rds_run(rds_ctx *ctx, double cfl, int n)
   };
   LoopParams lp{};
   lp.cfl = cfl;
-  RDS_CUDA(cudaMemcpyAsync(ctx->d_loop, &lp, sizeof(lp), cudaMemcpyHostToDevice, ctx->stream));
+  if ((st = set_loop_params(ctx, lp)) != RDS_OK)
+    return st;
   if (ctx->timing)
   {
     for (int i = 0; i < n; ++i)
@@ -2942,7 +2976,8 @@ rds_status rds_iterate_batch(rds_ctx *ctx, int max_iter, double drop, int32_t *i
   lp.stall_min  = ctx->stall_min;
   lp.stall_mult = ctx->stall_mult;
   lp.dc_m       = dc ? m : 0;
-  RDS_CUDA(cudaMemcpyAsync(ctx->d_loop, &lp, sizeof(lp), cudaMemcpyHostToDevice, ctx->stream));
+  if ((st = set_loop_params(ctx, lp)) != RDS_OK)
+    return st;
   const std::vector<int32_t> phase0(P, (mixed && !dc) ? 0 : 1);
   const int32_t one = 1;
   if ((st = upload(ctx, ctx->d_phase, phase0.data(), P)) ||
@@ -3174,6 +3209,10 @@ rds_status rds_destroy(rds_ctx *ctx)
     cudaFree(b.d_gq);
   }
   cudaFree(ctx->d_bon);
+  if (ctx->h_loop)
+    cudaFreeHost(ctx->h_loop);
+  if (ctx->ev_loop)
+    cudaEventDestroy(ctx->ev_loop);
   cudaFree(ctx->d_if_nodes);
   cudaFree(ctx->d_if_slots);
   cudaFree(ctx->d_owned);
