@@ -251,7 +251,13 @@ RDS_API rds_status rds_set_artificial_viscosity(rds_ctx *ctx, const double *eps)
  *     when not NULL; install != 0 makes the nodal field the context's artificial viscosity
  *     (RDS_STAB_ART_VISC) or blending coefficient (the blend operators), as
  *     rds_set_artificial_viscosity / rds_set_blending_coeff would, without a host copy.
- *     The sensor operators need affine simplex groups with sensor tables. */
+ *     The sensor operators need sensor tables on every group, and on groups that are not
+ *     affine simplices (bilinear quadrilaterals) the geometry tables of
+ *     rds_set_stab_geo_tables.
+ *   rds_set_stab_geo_tables (after rds_set_stab_tables with nq > 0): dVgeo [dim][nq][ngeo],
+ *     the derivatives of the group's geometry basis (ngeo <= 4 nodes) at the sensor's points;
+ *     the sensor then takes detJ at every point, as the reference's geometry metric does
+ *     (ArtificialViscosity.hpp:388-426). Replaces the affine detJ of simplex groups. */
 typedef enum
 {
   RDS_STAB_ART_VISC          = 0, /* compute_artificial_viscosity; p0 = kappa, p1 = factor */
@@ -265,6 +271,8 @@ typedef enum
 RDS_API rds_status rds_set_stab_tables(rds_ctx *ctx, int group, int nq, const double *w,
                                        const double *Vn, const double *R, int nvert,
                                        const double *P1);
+RDS_API rds_status rds_set_stab_geo_tables(rds_ctx *ctx, int group, int ngeo,
+                                           const double *dVgeo);
 RDS_API rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
                                              int install, double *cells_out, double *nodes_out);
 

@@ -5,8 +5,8 @@ the reference's stabilisation operators that sit either side of the cell residua
   (src/solver/art_visc/ArtificialViscosity.hpp:300-455, and the same sensor as a blending
   coefficient in src/solver/rdm/blending_coeff/ArtViscIndicatorCoeffImpl.hpp:261-425): the
   first state component is projected in L2 onto the cell's modal basis of order p, the modes
-  of total degree p are dropped (at p = 1 all modes), Se = int (u - u_{p-1})^2 / int u^2 (0 when the denominator
-  is <= 1e-10), se = log10 Se, s0 = 1/p^4, and the value is 0 below s0 - kappa, eps0 above
+  of total degree p are dropped (at p = 1 all modes), Se = int (u - u_{p-1})^2 / int u^2 (0
+  when the denominator is <= 1e-10), se = log10 Se, s0 = 1/p^4, and the value is 0 below s0 - kappa, eps0 above
   s0 + kappa, 0.5 eps0 (1 + sin(pi (se - s0) / (2 kappa))) between; eps0 = factor h / p with
   h = |K|^(1/D) for the viscosity, eps0 = 1 for the blending coefficient.
   Restated with an explicit orthogonal (Dubiner) basis in collapsed coordinates
@@ -14,6 +14,10 @@ the reference's stabilisation operators that sit either side of the cell residua
   of triangles and tetrahedra, mesh/shape_function/ModalBasisFactory.cpp:36-46) and
   collapsed-coordinate Gauss-Legendre quadrature exact to degree 2p (the reference integrates
   with its Gauss rule of order max(2p, geometry order); on affine cells both are exact).
+  Bilinear quadrilaterals follow the reference step by step: its tensor Legendre modal basis
+  and leading-term flags, its Gauss rule of order 2p, detJ at every point, the cell's mass
+  matrix and its solve (at p >= 2 that mass matrix is singular in the reference; the
+  projection there uses a rule that keeps it regular, see sensor_cells).
 * `nodal_from_cells`: the cell-to-node transfer
   (src/interpolation/mesh_function/MeshFunctionTools.hpp:52-397 without adaptation): every
   vertex takes max(0, max over its cells), every other node the P1 interpolant of the vertex
@@ -26,8 +30,9 @@ the reference's stabilisation operators that sit either side of the cell residua
   physics/euler/Euler2DCons.hpp:160-190), f = (v_m . gp_m)|v_m| (means over the cell) and
   lc = |K|^(1/D); over the mesh p_min, p_max and v_dom = sum int V / sum |K|;
   theta = min(1, max(f / ((p_max - p_min)|v_dom|^2), 0)^2 lc) with std::min / std::max's
-  comparisons. Quadrilaterals use the reference's rule (tensor Gauss-Legendre, order // 2 + 1
-  points per direction, mesh/point_set/QdPointSetQuadGauss.cpp); simplices a collapsed rule
+  comparisons. Quadrilaterals use the reference's rule (at the orders max(p, 1) <= 3 used here,
+  tensor Gauss-Legendre with order // 2 + 1 points per direction,
+  mesh/point_set/QdPointSetQuadGauss.cpp); simplices a collapsed rule
   exact to degree 2p (their integrands have degree <= p on affine cells).
 
 Pinned against the reference's own outputs (tests/golden/*_av, *_lf, *_wj, *_visc, *_bonanni,
@@ -127,27 +132,104 @@ def _ramp(se, s0, kappa, eps0):
                              0.5 * eps0 * (1 + np.sin(np.pi * (se - s0) / (2 * kappa)))))
 
 
+def _legendre_quad(p: int, pts: np.ndarray):
+    """The reference's modal basis of quadrilaterals (mesh/shape_function/
+    ModalExpansionQuad.cpp:60-73): mode (m, n), m-major, P_m(xi) P_n(eta) / sqrt(g_m g_n) with
+    g_k = 2 / (2k + 1); and its leading-term flags (ModalExpansionQuad.cpp:240-257), which
+    advance the mode index only on modes with m == p or n == p and so set the FIRST 2p + 1 flags
+    (the constant mode among them), not those of the modes of degree p."""
+    cols = []
+    for m in range(p + 1):
+        for n in range(p + 1):
+            cols.append(eval_jacobi(m, 0, 0, pts[:, 0]) * eval_jacobi(n, 0, 0, pts[:, 1]) /
+                        np.sqrt(2.0 / (2 * m + 1) * 2.0 / (2 * n + 1)))
+    flags = np.zeros((p + 1) ** 2, dtype=bool)
+    flags[:2 * p + 1] = True
+    return np.stack(cols, 1), flags
+
+
+def _gauss_quad(order: int):
+    """The reference's Gauss rule of the square for orders 2 - 7
+    (mesh/point_set/QdPointSetQuadGauss.cpp): 2 x 2 Gauss-Legendre up to order 3, then the fully
+    symmetric rules of degree 5 (8 points) and 7 (12 points) of A. H. Stroud (1971, region C2)
+    in closed form: orbits (+-a, 0), (0, +-a) of weight A and (+-b, +-b) of weight B (and
+    (+-c, +-c) of weight C), from the moment equations of the square."""
+    if order <= 3:
+        x, w = np.polynomial.legendre.leggauss(2)
+        X, Y = np.meshgrid(x, x, indexing="ij")
+        return np.stack([X.ravel(), Y.ravel()], 1), np.outer(w, w).ravel()
+    if order <= 5:
+        # int x^4 y^0 and int x^2 y^2 fix A a^4 = 8/45 and B b^4 = 1/9
+        orbits = [("a0", 40.0 / 49.0, np.sqrt(7.0 / 15.0)), ("aa", 9.0 / 49.0, np.sqrt(7.0 / 9.0))]
+    elif order <= 7:
+        # int x^4 - int x^2 y^2 and int x^6 - int x^4 y^2 give a^2 = 6/7, A = 98/405; the two
+        # diagonal orbits are then the 2-point Gauss rule of the moments m0..m3 left for them
+        A, a2 = 98.0 / 405.0, 6.0 / 7.0
+        m = [1.0 - A, 1.0 / 3.0 - A * a2 / 2.0, 1.0 / 9.0, 1.0 / 15.0]
+        p1, p0 = np.linalg.solve([[m[1], m[0]], [m[2], m[1]]], [-m[2], -m[3]])
+        u, v = np.roots([1.0, p1, p0])
+        B = (m[1] - v * m[0]) / (u - v)
+        orbits = [("a0", A, np.sqrt(a2)), ("aa", B, np.sqrt(u)), ("aa", m[0] - B, np.sqrt(v))]
+    else:
+        raise ValueError(f"no square rule of order {order} here")
+    pts, w = [], []
+    for kind, wt, a in orbits:
+        orb = ([(a, 0.0), (-a, 0.0), (0.0, a), (0.0, -a)] if kind == "a0" else
+               [(a, a), (a, -a), (-a, a), (-a, -a)])
+        pts += orb
+        w += [wt] * 4
+    return np.asarray(pts), np.asarray(w)
+
+
 def sensor_cells(dim, p, sol_nodes, geo_coords, geo_conn, sol_conn, u0, kappa=5.0, factor=1.0,
                  blend=False):
     """Cellwise artificial viscosity (blend=False) or ViscosityIndicator blending coefficient
-    (blend=True) of the first state component u0 [nnodes] on affine simplices."""
-    qp, qw = _simplex_rule(dim, p + 2)
-    Vn = lagrange_at(dim, p, sol_nodes, qp)
-    Vm, deg = _dubiner(dim, p, qp)
-    # the modes of degree p switched off; at p = 1 the reference marks every mode, the
-    # constant included, as leading (mesh/shape_function/DubinerExpansionTriag.cpp:460-467,
-    # DubinerExpansionTetra.cpp:715-723), so u_{p-1} = 0 there
-    Vl = Vm * (deg < p) if p > 1 else 0.0 * Vm
-    X = geo_coords[geo_conn[:, :dim + 1]]     # [nc, dim+1, dim] vertex coordinates
-    J = np.stack([X[:, k + 1] - X[:, 0] for k in range(dim)], 2) / 2  # dx/dxi
-    jdet = np.linalg.det(J)
+    (blend=True) of the first state component u0 [nnodes] on affine simplices, or on bilinear
+    quadrilaterals (dim 2 with 4 geometry nodes a cell: the Gauss rule of order 2p, detJ per
+    point, the reference's quadrilateral modal basis and flags). On quadrilaterals of order
+    p >= 2 the reference's rule has fewer points than the cell has modes and its mass matrix is
+    singular (its result follows the rounding of the inversion); there the projection is taken
+    with the (p + 1)^2-point tensor Gauss rule, which makes the mass matrix regular, and the
+    integrals of Se with the reference's rule."""
+    quad = dim == 2 and geo_conn.shape[1] == 4
+    proj = None
+    if quad:
+        qp, qw = _gauss_quad(2 * p)
+        Vn, _ = _basis(2, p, sol_nodes, qp, True)
+        Vm, flags = _legendre_quad(p, qp)
+        Vl = Vm * ~flags
+        _, dG = _basis(2, 1, _QUAD_CORNERS, qp, True)                 # [2, nq, 4]
+        Jq = np.einsum("aqg,cgx->cqax", dG, geo_coords[geo_conn])    # [nc, nq, xi, x]
+        jdet = np.linalg.det(Jq)                                      # [nc, nq]
+        if p >= 2:
+            x, w1 = np.polynomial.legendre.leggauss(p + 1)
+            X, Y = np.meshgrid(x, x, indexing="ij")
+            pp, pw = np.stack([X.ravel(), Y.ravel()], 1), np.outer(w1, w1).ravel()
+            _, dGp = _basis(2, 1, _QUAD_CORNERS, pp, True)
+            proj = (pw, _basis(2, p, sol_nodes, pp, True)[0], _legendre_quad(p, pp)[0],
+                    np.linalg.det(np.einsum("aqg,cgx->cqax", dGp, geo_coords[geo_conn])))
+    else:
+        qp, qw = _simplex_rule(dim, p + 2)
+        Vn = lagrange_at(dim, p, sol_nodes, qp)
+        Vm, deg = _dubiner(dim, p, qp)
+        # the modes of degree p switched off; at p = 1 the reference marks every mode, the
+        # constant included, as leading (mesh/shape_function/DubinerExpansionTriag.cpp:460-467,
+        # DubinerExpansionTetra.cpp:715-723), so u_{p-1} = 0 there
+        Vl = Vm * (deg < p) if p > 1 else 0.0 * Vm
+        X = geo_coords[geo_conn[:, :dim + 1]]     # [nc, dim+1, dim] vertex coordinates
+        J = np.stack([X[:, k + 1] - X[:, 0] for k in range(dim)], 2) / 2  # dx/dxi
+        jdet = np.linalg.det(J)[:, None] * np.ones(len(qw))
     out = np.empty(len(sol_conn))
     s0 = 1.0 / p ** 4
     for c in range(len(sol_conn)):
         wj = jdet[c] * qw
-        uq = Vn @ u0[sol_conn[c]]
-        M = (Vm * wj[:, None]).T @ Vm
-        cm = np.linalg.solve(M, (Vm * (wj * uq)[:, None]).sum(0))
+        if proj is None:
+            wp, Vnp, Vmp = wj, Vn, Vm
+        else:
+            wp, Vnp, Vmp = proj[3][c] * proj[0], proj[1], proj[2]
+        up = Vnp @ u0[sol_conn[c]]
+        M = (Vmp * wp[:, None]).T @ Vmp
+        cm = np.linalg.solve(M, (Vmp * (wp * up)[:, None]).sum(0))
         uq = Vm @ cm
         ul = Vl @ cm
         nom = np.sum(wj * (uq - ul) ** 2)

@@ -89,6 +89,8 @@ struct rds_ctx
     int nq = 0, nvert = 0;
     double *w = nullptr, *Vn = nullptr, *R = nullptr, *P1 = nullptr;
     double *vw = nullptr, *vV = nullptr, *vdV = nullptr, *vdVgeo = nullptr;
+    int sngeo  = 0; // the sensor's geometry derivatives at its points (non-affine cells)
+    double *sdVgeo = nullptr;
     int bnq    = 0; // Bonanni's coefficient: its rule, basis and geometry derivatives
     double *bw = nullptr, *bV = nullptr, *bdV = nullptr, *bdVgeo = nullptr;
   };
@@ -1606,6 +1608,27 @@ rds_status rds_set_stab_tables(rds_ctx *ctx, int group, int nq, const double *w,
   return RDS_OK;
 }
 
+rds_status rds_set_stab_geo_tables(rds_ctx *ctx, int group, int ngeo, const double *dVgeo)
+{
+  rds_status st = stab_check(ctx, "rds_set_stab_geo_tables");
+  if (st != RDS_OK)
+    return st;
+  if (group < 0 || group >= (int)ctx->groups.size())
+    return fail(ctx, RDS_ERR_INVALID, "rds_set_stab_geo_tables: invalid group");
+  rds_ctx::StabTab &t = ctx->stab[group];
+  const int D = ctx->desc.dim;
+  if (t.nq == 0 || !dVgeo || ngeo != ctx->groups[group].desc.ngeo || ngeo > kStabMaxGeo)
+    return fail(ctx, RDS_ERR_INVALID, "rds_set_stab_geo_tables: no sensor rule for the group "
+                                      "(rds_set_stab_tables first), or ngeo is not the group's "
+                                      "(at most 4)");
+  if ((!t.sdVgeo && (st = stab_alloc(ctx, &t.sdVgeo, (size_t)D * t.nq * ngeo))) ||
+      (st = upload(ctx, t.sdVgeo, dVgeo, (size_t)D * t.nq * ngeo)))
+    return st;
+  t.sngeo = ngeo;
+  RDS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RDS_OK;
+}
+
 rds_status rds_set_bonanni_tables(rds_ctx *ctx, int group, int nq, const double *w,
                                   const double *V, const double *dV, const double *dVgeo)
 {
@@ -1659,9 +1682,11 @@ rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
   for (int k = 0; k < G; ++k)
   {
     const rds_ctx::StabTab &t = ctx->stab[k];
-    if (sensor && (t.nq == 0 || !ctx->groups[k].affine))
+    if (sensor && (t.nq == 0 || (!ctx->groups[k].affine && !t.sdVgeo)))
       return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_compute_stabilisation: the smoothness sensor "
-                                            "needs affine simplex cells with sensor tables");
+                                            "needs sensor tables, and geometry tables "
+                                            "(rds_set_stab_geo_tables) where cells are not "
+                                            "affine simplices");
     if (nodal && t.nvert == 0)
       return fail(ctx, RDS_ERR_INVALID, "rds_compute_stabilisation: no vertex interpolant "
                                         "(rds_set_stab_tables) for a group");
@@ -1684,10 +1709,6 @@ rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
     if (need > ctx->bon_len)
     {
       cudaFree(ctx->d_bon);
-  if (ctx->h_loop)
-    cudaFreeHost(ctx->h_loop);
-  if (ctx->ev_loop)
-    cudaEventDestroy(ctx->ev_loop);
       ctx->d_bon   = nullptr;
       ctx->bon_len = 0;
       if ((st = dalloc(ctx, &ctx->d_bon, need)) != RDS_OK)
@@ -1717,6 +1738,8 @@ rds_status rds_compute_stabilisation(rds_ctx *ctx, int op, double p0, double p1,
       a.w          = t.w;
       a.Vn         = t.Vn;
       a.R          = t.R;
+      a.dVgeo      = g.affine ? nullptr : t.sdVgeo;
+      a.ngeo       = t.sngeo;
       a.kappa      = p0;
       a.factor     = op == RDS_STAB_ART_VISC ? p1 : 1.0;
       a.out        = out;

@@ -376,6 +376,7 @@ cudaError_t launch_finish(int v0, int v1, int nnodes, int neq, double cfl, int u
 
 // stabilisation operators (rds_stab.cu)
 constexpr int kStabMaxGroups = 8;
+constexpr int kStabMaxGeo    = 4; // geometry nodes of a cell the sensor maps (bilinear quads)
 // cell groups as the node-parallel kernels decode them from the gather lists
 struct StabGroups
 {
@@ -402,6 +403,8 @@ struct SensorArgs
   const int32_t *sol_conn, *geo_conn;
   const double *X, *u;           // u: the first state component [nnodes]
   const double *w, *Vn, *R;      // [nq], [nq][ndof], [nq][ndof]
+  const double *dVgeo;           // [D][nq][ngeo] at the points: detJ per point (bilinear
+  int ngeo;                      // quadrilaterals); NULL: affine simplices, detJ constant
   double kappa, factor;
   double *out;                   // [ncells]
 };

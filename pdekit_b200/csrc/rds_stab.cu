@@ -280,11 +280,22 @@ __global__ void __launch_bounds__(kBlock) sensor_cells_2d(const SensorArgs a);
 __global__ void __launch_bounds__(kBlock) sensor_cells_3d(const SensorArgs a);
 
 template <int D>
+__device__ __forceinline__ double sensor_value(const SensorArgs &a, double nom, double den,
+                                               double vol);
+template <int D>
+__device__ __forceinline__ void sensor_cell_mapped(const SensorArgs &a, int c);
+
+template <int D>
 __device__ __forceinline__ void sensor_cell(const SensorArgs &a)
 {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.ncells)
     return;
+  if (a.dVgeo)
+  {
+    sensor_cell_mapped<D>(a, c);
+    return;
+  }
   // affine simplex on the reference element with vertices (-1,..,-1) and -1 + 2 e_k:
   // d x / d xi_k = (X_{k+1} - X_0) / 2
   double X0[D], J[D][D];
@@ -325,6 +336,16 @@ __device__ __forceinline__ void sensor_cell(const SensorArgs &a)
     nom += wj * r * r;
     den += wj * s * s;
   }
+  a.out[c] = sensor_value<D>(a, nom, den, vol);
+}
+
+// Se = nom / den (0 when den <= 1e-10), se = log10 Se, and the ramp around s0 = 1 / p^4
+// (ArtificialViscosity.hpp:468-510); eps0 = factor |K|^(1/D) / p, or 1 for the blending
+// coefficient
+template <int D>
+__device__ __forceinline__ double sensor_value(const SensorArgs &a, double nom, double den,
+                                               double vol)
+{
   const double Se = (den <= 1.e-10) ? 0.0 : nom / den;
   const double se = log(Se) / log(10.0);
   const double p  = (double)a.order;
@@ -337,7 +358,66 @@ __device__ __forceinline__ void sensor_cell(const SensorArgs &a)
     val = e0;
   else
     val = 0.5 * e0 * (1.0 + sin(kPi * (se - s0) / (2.0 * a.kappa)));
-  a.out[c] = val;
+  return val;
+}
+
+// Cells whose Jacobian varies (bilinear quadrilaterals): J = sum_g dVgeo[.][q][g] X_g at every
+// point (the geometry metric the reference evaluates at its rule's points).
+template <int D>
+__device__ __forceinline__ void sensor_cell_mapped(const SensorArgs &a, int c)
+{
+  double Xg[kStabMaxGeo][D];
+#pragma unroll
+  for (int g = 0; g < kStabMaxGeo; ++g)
+    if (g < a.ngeo)
+    {
+      const int v = __ldg(a.geo_conn + (size_t)g * a.ncells + c);
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+        Xg[g][i] = __ldg(a.X + (size_t)i * a.ngeo_nodes + v);
+    }
+  double nom = 0.0, den = 0.0, vol = 0.0;
+  for (int q = 0; q < a.nq; ++q)
+  {
+    double J[D][D];
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+        J[k][i] = 0.0;
+#pragma unroll
+    for (int g = 0; g < kStabMaxGeo; ++g)
+      if (g < a.ngeo)
+      {
+#pragma unroll
+        for (int k = 0; k < D; ++k)
+        {
+          const double d = __ldg(a.dVgeo + ((size_t)k * a.nq + q) * a.ngeo + g);
+#pragma unroll
+          for (int i = 0; i < D; ++i)
+            J[k][i] += d * Xg[g][i];
+        }
+      }
+    double det;
+    if constexpr (D == 2)
+      det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    else
+      det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) +
+            J[0][1] * (J[1][2] * J[2][0] - J[1][0] * J[2][2]) +
+            J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+    double s = 0.0, r = 0.0;
+    for (int n = 0; n < a.ndof; ++n)
+    {
+      const double un = __ldg(a.u + __ldg(a.sol_conn + (size_t)n * a.ncells + c));
+      s += __ldg(a.Vn + (size_t)q * a.ndof + n) * un;
+      r += __ldg(a.R + (size_t)q * a.ndof + n) * un;
+    }
+    const double wj = det * __ldg(a.w + q);
+    vol += wj;
+    nom += wj * r * r;
+    den += wj * s * s;
+  }
+  a.out[c] = sensor_value<D>(a, nom, den, vol);
 }
 
 __global__ void __launch_bounds__(kBlock) sensor_cells_2d(const SensorArgs a)

@@ -143,6 +143,7 @@ def lib():
         "rds_set_artificial_viscosity": ([vp, vp], ip),
         "rds_set_stab_tables": ([vp, ip, ip, vp, vp, vp, ip, vp], ip),
         "rds_set_bonanni_tables": ([vp, ip, ip, vp, vp, vp, vp], ip),
+        "rds_set_stab_geo_tables": ([vp, ip, ip, vp], ip),
         "rds_compute_stabilisation": ([vp, ip, dp, dp, ip, vp, vp], ip),
     }
     for name, (args, res) in sig.items():
@@ -235,7 +236,7 @@ class PGRDMethodExplicit:
     def initialize_work_data(self):
         self._check(lib().rds_finalize(self._ctx))
         # tables of the stabilisation operators: the vertex interpolant of every group, the
-        # smoothness sensor's where it is defined (affine simplices)
+        # smoothness sensor's where it is defined (affine simplices, bilinear quadrilaterals)
         from .reference_element import bonanni_tables, stab_tables
         for ig, g in enumerate(self.problem.groups):
             t = stab_tables(g.shape, g.order, g.ngeo)
@@ -243,6 +244,10 @@ class PGRDMethodExplicit:
             self._keep += arrs
             self._check(lib().rds_set_stab_tables(self._ctx, ig, t["nq"], *[_ptr(a) for a in arrs[:3]],
                                                   t["P1"].shape[1], _ptr(arrs[3])))
+            if t["nq"] and "dVgeo" in t:
+                self._keep.append(t["dVgeo"])
+                self._check(lib().rds_set_stab_geo_tables(self._ctx, ig, t["dVgeo"].shape[2],
+                                                          _ptr(t["dVgeo"])))
             if self.problem.neq > 1:  # Bonanni's coefficient (Euler)
                 b = bonanni_tables(g.shape, g.order, g.ngeo)
                 if b["nq"]:

@@ -14,7 +14,8 @@ a modal Vandermonde matrix inverted with LAPACK gives the nodal Lagrange basis
   symmetrical Gaussian quadrature rules for the triangle", IJNME 21, 1985), the same published
   rules the reference tabulates, expanded over their symmetry orbits and mapped to the
   reference triangle (-1,-1),(1,-1),(-1,1) (weights sum to 2);
-* line rules are Gauss-Legendre with n = order // 2 + 1 points.
+* line rules are Gauss-Legendre with n = order // 2 + 1 points; the square's rules are the
+  reference's (2 x 2 Gauss-Legendre up to order 3, Stroud's symmetric rules above).
 
 The tables agree with the reference's to rounding (tests/test_reference_element.py compares
 them with the golden tables dumped from the reference).
@@ -231,13 +232,95 @@ def lagrange_quad(p: int, pts: np.ndarray):
     return V, dV
 
 
-def quad_gauss(order: int):
+def quad_tensor_gauss(order: int):
     """Tensor Gauss-Legendre rule on [-1,1]^2 with n = order // 2 + 1 points per direction."""
     x, w = line_gauss(order)
     x = x.ravel()
     X, Y = np.meshgrid(x, x, indexing="ij")
     W = np.outer(w, w)
     return np.stack([X.ravel(), Y.ravel()], axis=1), W.ravel()
+
+
+# The square's rules of orders 4 - 8 the reference uses (src/mesh/point_set/
+# QdPointSetQuadGauss.cpp): fully symmetric rules of degree 5 (8 points), 7 (12 points) and
+# 9 (20 points, two orbit points outside the square), A. H. Stroud, "Approximate calculation of
+# multiple integrals" (1971), region C2. Each is computed here from its orbit structure as the
+# solution of the moment equations int x^2i y^2j (2(i + j) < degree) by Newton's method from
+# the rough start given; orbits (weight, coordinates):
+#   "a0" (a)      (a, 0), (-a, 0), (0, a), (0, -a)
+#   "aa" (a)      (a, a), (a, -a), (-a, a), (-a, -a)
+#   "ab" (a, b)   (a, b), (a, -b), (-a, b), (-a, -b), (b, a), (b, -a), (-b, a), (-b, -a)
+_SQUARE_RULES = {
+    5: [("a0", 0.8, (0.7,)), ("aa", 0.2, (0.9,))],
+    7: [("a0", 0.24, (0.93,)), ("aa", 0.24, (0.8,)), ("aa", 0.52, (0.38,))],
+    9: [("a0", 0.02, (1.1,)), ("a0", 0.39, (0.45,)), ("aa", 0.08, (0.9,)),
+        ("ab", 0.25, (0.82, 0.41))],
+}
+_SQUARE_CACHE = {}
+
+
+def _square_orbit(kind, c):
+    z = 0.0 * c[0]
+    if kind == "a0":
+        a = c[0]
+        return [(a, z), (-a, z), (z, a), (z, -a)]
+    if kind == "aa":
+        a = c[0]
+        return [(a, a), (a, -a), (-a, a), (-a, -a)]
+    a, b = c
+    return [(a, b), (a, -b), (-a, b), (-a, -b), (b, a), (b, -a), (-b, a), (-b, -a)]
+
+
+def _square_symmetric(deg: int):
+    if deg in _SQUARE_CACHE:
+        return _SQUARE_CACHE[deg]
+    orbits = _SQUARE_RULES[deg]
+    sizes = [len(o[2]) for o in orbits]
+    x = np.array([v for o in orbits for v in (o[1],) + tuple(o[2])], dtype=float)
+    mons = [(i, s - i) for s in range((deg - 1) // 2 + 1) for i in range(s, -1, -1) if 2 * i >= s]
+    exact = np.array([4.0 / ((2 * i + 1) * (2 * j + 1)) for i, j in mons])
+
+    def rule(x):
+        pts, w, k = [], [], 0
+        for (kind, _, _), n in zip(orbits, sizes):
+            for pt in _square_orbit(kind, x[k + 1:k + 1 + n]):
+                pts.append(pt)
+                w.append(x[k])
+            k += 1 + n
+        return pts, w
+
+    def moments(x):
+        pts, w = rule(x)
+        return sum(wt * np.array([px ** (2 * i) * py ** (2 * j) for i, j in mons])
+                   for (px, py), wt in zip(pts, w)) - exact
+
+    for _ in range(50):
+        f = moments(x)
+        if np.abs(f).max() < 4e-15:
+            break
+        # complex-step derivatives: the moments are polynomials in the unknowns
+        h = 1e-30
+        J = np.stack([moments(x + 1j * h * e).imag / h for e in np.eye(len(x))], 1)
+        x = x - np.linalg.solve(J, f)
+    else:
+        raise RuntimeError(f"square rule of degree {deg} did not converge")
+    pts, w = rule(x)
+    out = (np.asarray(pts, dtype=float), np.asarray(w, dtype=float))
+    _SQUARE_CACHE[deg] = out
+    return out
+
+
+def quad_gauss(order: int):
+    """The reference's rule of the square [-1,1]^2 for `order` (QdPointSetQuadGauss.cpp): the
+    centre (order 1), 2 x 2 Gauss-Legendre (orders 2, 3), then the symmetric rules of degree 5
+    (orders 4, 5), 7 (orders 6, 7) and 9 (order 8). Weights sum to 4."""
+    if order <= 1:
+        return np.zeros((1, 2)), np.array([4.0])
+    if order <= 3:
+        return quad_tensor_gauss(2)
+    if order <= 8:
+        return _square_symmetric(order + 1 if order % 2 == 0 else order)
+    raise ValueError(f"no quadrilateral rule of order {order} (the reference's go up to 8)")
 
 
 _TET_V = np.array([[-1.0, -1.0, -1.0], [1.0, -1.0, -1.0], [-1.0, 1.0, -1.0], [-1.0, -1.0, 1.0]])
@@ -330,9 +413,11 @@ def tet_gauss(order: int):
     return pts, 8.0 * np.asarray(w)
 
 
-def quad_tables(p: int, quad_order: int, vol_order: int = None) -> dict:
-    """Tables for P p quadrilaterals with bilinear (P1) geometry."""
-    qp, w = quad_gauss(quad_order)
+def quad_tables(p: int, quad_order: int, vol_order: int = None, tensor: bool = False) -> dict:
+    """Tables for P p quadrilaterals with bilinear (P1) geometry: the cell rule of quad_order is
+    the reference's (quad_gauss), or with tensor=True the tensor Gauss-Legendre rule with
+    quad_order // 2 + 1 points per direction."""
+    qp, w = (quad_tensor_gauss if tensor else quad_gauss)(quad_order)
     V, dV = lagrange_quad(p, qp)
     _, dVgeo = lagrange_quad(1, qp)
     _, dVf = lagrange_quad(p + 1, qp)
@@ -385,7 +470,8 @@ def stab_tables(shape: str, p: int, ngeo: int) -> dict:
       R = Vn - Vl (Vl^T W Vl)^-1 Vl^T W Vn. At p = 1 the reference switches off every mode
       (mesh/shape_function/DubinerExpansionTriag.cpp:460-467), u_{p-1} = 0 and R = Vn.
       On affine cells detJ is constant, so any rule exact to degree 2p gives the reference's
-      integrals. nq = 0 elsewhere (no sensor).
+      integrals. Bilinear quadrilaterals (ngeo = 4): the tables of _quad_sensor, with
+      dVgeo [2, nq, 4] for detJ at every point. nq = 0 elsewhere (no sensor).
     """
     key = (shape, p, ngeo)
     if key in _STAB_CACHE:
@@ -404,6 +490,10 @@ def stab_tables(shape: str, p: int, ngeo: int) -> dict:
     elif shape == "quad":
         P1, _ = lagrange_quad(1, quad_nodes(p))
         rule = None
+        if ngeo == 4:
+            out = dict(P1=np.ascontiguousarray(P1), **_quad_sensor(p))
+            _STAB_CACHE[key] = out
+            return out
     else:
         raise ValueError(f"no stabilisation tables for {shape}")
     out = dict(nq=0, w=empty, Vn=empty, R=empty, P1=np.ascontiguousarray(P1))
@@ -422,12 +512,46 @@ def stab_tables(shape: str, p: int, ngeo: int) -> dict:
     return out
 
 
+def _legendre_square(p: int, pts: np.ndarray):
+    """The reference's modal basis of the square (src/mesh/shape_function/
+    ModalExpansionQuad.cpp:60-73): mode (m, n), m-major, P_m(xi) P_n(eta) sqrt((2m+1)(2n+1)) / 2;
+    and the modes its leading-term flags select (ModalExpansionQuad.cpp:240-257): the flag index
+    advances only on modes with m == p or n == p, so the FIRST 2p + 1 modes are flagged."""
+    from numpy.polynomial import legendre as L
+    E = np.eye(p + 1)
+    cols = [L.legval(pts[:, 0], E[m]) * L.legval(pts[:, 1], E[n]) *
+            np.sqrt((2 * m + 1) * (2 * n + 1)) / 2.0 for m in range(p + 1) for n in range(p + 1)]
+    flags = np.zeros((p + 1) ** 2, dtype=bool)
+    flags[:2 * p + 1] = True
+    return np.stack(cols, 1), flags
+
+
+def _quad_sensor(p: int) -> dict:
+    """The sensor on bilinear quadrilaterals (ArtificialViscosity.hpp:388-455): the reference's
+    rule of order 2p (quad_gauss), Vn the nodal basis there, R = Vm[:, F] T^-1[F, :] the flagged
+    modes' part of u (T the modal basis at the nodes, F the flags), and dVgeo [2, nq, 4] for detJ
+    at every point. The reference projects u in L2 on its modal basis with the cell's mass matrix;
+    when that matrix is regular the projection of the interpolant is the interpolant, whose modal
+    coefficients are T^-1 u, independent of the cell's shape. At p = 1 the rule has 4 points for
+    4 modes. At p >= 2 it has fewer points than modes (8 for 9, 12 for 16), the reference's mass
+    matrix is singular and its coefficients follow the rounding of the inversion; T^-1 u is the
+    value every regular projection gives."""
+    qp, w = quad_gauss(2 * p)
+    Vn, _ = lagrange_quad(p, qp)
+    Vm, flags = _legendre_square(p, qp)
+    T, _ = _legendre_square(p, quad_nodes(p))
+    R = Vm[:, flags] @ np.linalg.inv(T)[flags, :]
+    _, dVgeo = lagrange_quad(1, qp)
+    return dict(nq=len(w), w=np.ascontiguousarray(w), Vn=np.ascontiguousarray(Vn),
+                R=np.ascontiguousarray(R), dVgeo=np.ascontiguousarray(dVgeo))
+
+
 def bonanni_tables(shape: str, p: int, ngeo: int) -> dict:
     """Tables of Bonanni's pressure-based blending coefficient
     (src/solver/rdm/blending_coeff/BonanniBlendingCoeffImpl.hpp:102-168): the reference
     integrates the velocity and the pressure gradient over a cell with its Gauss rule of order
-    max(p, geometry order). Quadrilaterals use that rule (tensor Gauss-Legendre, order // 2 + 1
-    points per direction); on affine simplices the integrands are polynomials of degree <= p,
+    max(p, geometry order). Quadrilaterals use that rule (quad_gauss: at the orders <= 3 of
+    p <= 3 tensor Gauss-Legendre, order // 2 + 1 points per direction); on affine simplices the integrands are polynomials of degree <= p,
     so a rule exact to degree p gives the same integrals. w [nq], V [nq, ndof],
     dV [D, nq, ndof], dVgeo [D, nq, ngeo]; nq = 0 where not provided (curved cells)."""
     order = max(p, 1)

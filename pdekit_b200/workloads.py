@@ -178,7 +178,7 @@ def config3(nx_tri=500, nx_quad=1000, ny=500, seed=3):
     mesh = meshgen.channel_2d(nx_tri, nx_quad, ny, jitter=0.0, seed=seed)
     tables = {"triag": dict(R.triag_tables(3, 8), wv=R.triag_gauss(3)[1],
                             dVgeo_v=R.lagrange_triag(1, R.triag_gauss(3)[0])[1]),
-              "quad": R.quad_tables(3, 8)}
+              "quad": R.quad_tables(3, 8, tensor=True)}
     prob = mesh_problem(mesh, "euler2d", "b", 3, tables, euler_bcs(2))
     return prob, bump_state(prob.sol_coords, 2, 0.5)
 

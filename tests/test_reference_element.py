@@ -67,3 +67,35 @@ def test_lagrange_partition_of_unity_and_kronecker(p):
     V, dV = re_.lagrange_triag(p, qp)
     np.testing.assert_allclose(V.sum(axis=1), 1.0, atol=1e-14)
     np.testing.assert_allclose(dV.sum(axis=2), 0.0, atol=1e-12)
+
+
+@pytest.mark.parametrize("case,order", [("euler2d_quad_p2_b_bonanni", 5),
+                                        ("euler2d_quad_p3_b", 8)])
+def test_square_rules_match_reference(case, order):
+    """quad_gauss against the rule the reference integrated the fixture's cells with (its
+    symmetric 8- and 20-point rules, points in the same order). The reference tabulates them
+    to 14 - 15 digits."""
+    _, a, _ = load_golden(os.path.join(GOLDEN, case))
+    qp, w = re_.quad_gauss(order)
+    np.testing.assert_allclose(qp, a["qp"], rtol=0, atol=5e-14)
+    np.testing.assert_allclose(w, a["w"], rtol=0, atol=5e-14)
+
+
+@pytest.mark.parametrize("order", range(1, 9))
+def test_square_rules_exact(order):
+    """Every rule integrates the monomials of its degree exactly on [-1,1]^2 (degree 1, 3, 3, 5,
+    5, 7, 7, 9 for orders 1 - 8) and the rule of order 6 is the oracle's closed form."""
+    qp, w = re_.quad_gauss(order)
+    deg = order if order % 2 else order + 1
+    for i in range(deg + 1):
+        for j in range(deg + 1 - i):
+            ex = (0.0 if i % 2 or j % 2 else 4.0 / ((i + 1) * (j + 1)))
+            assert abs(np.sum(w * qp[:, 0] ** i * qp[:, 1] ** j) - ex) < 1e-14
+    if order in (4, 6):
+        from oracle.stab_oracle import _gauss_quad
+        oq, ow = _gauss_quad(order)
+        key = lambda q: np.lexsort((q[:, 1], q[:, 0]))
+        np.testing.assert_allclose(qp[key(qp)], oq[key(oq)], atol=1e-14)
+        np.testing.assert_allclose(w[key(qp)], ow[key(oq)], atol=1e-14)
+    with pytest.raises(ValueError):
+        re_.quad_gauss(9)
