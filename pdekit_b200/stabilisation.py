@@ -17,10 +17,12 @@ when asked for. Cell values are in the solver's cell order (groups in order).
 
 * ArtificialViscosity (src/solver/art_visc/ArtificialViscosity.hpp): the Persson-Peraire
   smoothness sensor of the first state component, kappa (default 5) and factor (default 1);
-  affine triangles (orders 1-3) and tetrahedra (orders 1-2).
+  affine triangles (orders 1-3), tetrahedra (orders 1-2) and bilinear quadrilaterals (orders
+  1-3; from order 2 the reference's own value there follows the rounding of a singular mass
+  matrix, and the sensor takes the projection every regular mass matrix gives).
 * RDBlendingCoeff (src/solver/rdm/blending_coeff/RDBlendingCoeff.hpp): "LF_Blend" (any cell
-  type), "ViscosityIndicator" (param "kappa", the sensor as a coefficient in [0, 1]; affine
-  simplices), "WongJansen" (param "u_inf", default 1e-14; any cell type), "Bonanni2D" /
+  type), "ViscosityIndicator" (param "kappa", the sensor as a coefficient in [0, 1]; the
+  sensor's cells), "WongJansen" (param "u_inf", default 1e-14; any cell type), "Bonanni2D" /
   "Bonanni3D" (Euler; the pressure-based coefficient, no parameters; straight-sided cells).
 """
 

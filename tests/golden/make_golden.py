@@ -147,9 +147,9 @@ CASES = {
     # the smoothness sensor on bilinear quadrilaterals (detJ varies inside the cell); P1 only:
     # at p >= 2 the reference's rule of order 2p has fewer points than the cell has modes, its
     # modal mass matrix is singular and the sensor follows the rounding of its inversion
-    "euler2d_quad_p1_lda_av": ("euler2d", "lda", 1, 3, ("channel_quad", 8, 4), 0.15, 65,
+    "euler2d_quad_p1_lda_av": ("euler2d", "lda", 1, 5, ("channel_quad", 8, 4), 0.15, 65,
                                "bump2d_jump", EULER2D_BCS, 0.5, 3, "av:4.0:1.0"),
-    "euler2d_quad_p1_b_visc": ("euler2d", "b", 1, 3, ("channel_quad", 8, 4), 0.15, 66,
+    "euler2d_quad_p1_b_visc": ("euler2d", "b", 1, 5, ("channel_quad", 8, 4), 0.15, 66,
                                "bump2d_jump", EULER2D_BCS, 0.5, 3,
                                "blend:ViscosityIndicator:1.5"),
 }
