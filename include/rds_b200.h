@@ -69,7 +69,14 @@ typedef enum
 {
   RDS_PGLDA = 0,
   RDS_PGN   = 1,
-  RDS_PGB   = 2
+  RDS_PGB   = 2,
+  /* PSI: the N scheme's node residuals phi_n limited per cell with the reference's residual
+   * limiter (solver/rdm/cellsplitters/LFResidualLimiter.hpp:37-110): where |phi| > 1e-14,
+   * x_n = max(phi_n / phi, 0) + 1e-12 and phi_n <- x_n / sum x * phi (phi the cell residual).
+   * The reference applies that limiter only to its Lax-Friedrichs schemes and has no PSI
+   * scheme: this one has no reference to be pinned on. Scalar physics (the reference's limiter
+   * is empty for systems), FP64 contexts, single and batched; no element Jacobians. */
+  RDS_PGPSI = 3
 } rds_scheme;
 
 typedef enum

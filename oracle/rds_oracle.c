@@ -420,6 +420,8 @@ static int cell_residual_theta(const rdso_model *m, const rdso_cells *g, const d
 {
   const int D = m->dim, NEQ = m->neq;
   const int ndof = g->ndof, nq = g->nq, nfl = g->nfl, ngeo = g->ngeo;
+  /* PSI distributes with the N scheme first */
+  const int nlike = m->scheme == RDSO_N || m->scheme == RDSO_PSI;
   int bad = 0;
 
   /* geometry at quadrature points */
@@ -575,7 +577,7 @@ static int cell_residual_theta(const rdso_model *m, const rdso_cells *g, const d
           B[n][i][j] = s;
         }
 
-    if (m->scheme == RDSO_N)
+    if (nlike)
     {
       /* PGN accumulates the LDA part and then the dissipation into the same nodal residual
        * at every quadrature point (PGN.hpp:246-269) */
@@ -589,10 +591,10 @@ static int cell_residual_theta(const rdso_model *m, const rdso_cells *g, const d
         }
     }
 
-    if (m->scheme == RDSO_B || m->scheme == RDSO_N)
+    if (m->scheme == RDSO_B || nlike)
     {
       /* N-type dissipation sum_{m != n} Kp[n] inv Kp[m] (u_n - u_m) */
-      double(*acc)[NEQ_MAX] = (m->scheme == RDSO_N) ? lda : diss;
+      double(*acc)[NEQ_MAX] = nlike ? lda : diss;
       for (int n = 0; n < ndof; ++n)
         for (int mm = 0; mm < ndof; ++mm)
         {
@@ -623,7 +625,7 @@ static int cell_residual_theta(const rdso_model *m, const rdso_cells *g, const d
     for (int e = 0; e < NEQ; ++e)
       phi[e] += wj * rq[e];
 
-    for (int n = 0; n < ndof && m->scheme != RDSO_N; ++n)
+    for (int n = 0; n < ndof && !nlike; ++n)
       for (int i = 0; i < NEQ; ++i)
       {
         double s = B[n][i][0] * rq[0];
@@ -644,6 +646,29 @@ static int cell_residual_theta(const rdso_model *m, const rdso_cells *g, const d
     for (int n = 0; n < ndof; ++n)
       for (int e = 0; e < NEQ; ++e)
         elem_res[n * NEQ + e] = lda[n][e];
+  }
+  else if (m->scheme == RDSO_PSI)
+  {
+    /* the reference's residual limiter on the N residuals, per equation of a scalar problem
+     * (LFResidualLimiter.hpp:37-110; for systems it does nothing, :18-30): where the cell
+     * residual is above 1e-14 in magnitude, x_n = max(phi_n / phi, 0) + 1e-12 and
+     * phi_n = x_n / sum_m x_m * phi */
+    for (int e = 0; e < NEQ; ++e)
+    {
+      double x[NDOF_MAX], sum_xp = 0.0;
+      const int lim = NEQ == 1 && fabs(phi[e]) > 1.e-14;
+      for (int n = 0; n < ndof; ++n)
+      {
+        if (lim)
+        {
+          const double r = lda[n][e] / phi[e];
+          x[n]           = (r < 0.0 ? 0.0 : r) + 1.e-12; /* std::max(r, 0.0) */
+          sum_xp += x[n];
+        }
+      }
+      for (int n = 0; n < ndof; ++n)
+        elem_res[n * NEQ + e] = lim ? x[n] / sum_xp * phi[e] : lda[n][e];
+    }
   }
   else
   {

@@ -11,7 +11,10 @@
  *   GeometryMetric / SolutionSpaceMetric / FluxSpaceMetric evaluation
  *     (src/interpolation/GeometryMetric.hpp:364-478, FluxSpaceMetric.hpp:545-746)
  *   PGLDA / PGN / PGB cell splitters
- *     (src/solver/rdm/cellsplitters/PGLDA.hpp:111-311, PGN.hpp:98-290, PGB.hpp:314-498)
+ *     (src/solver/rdm/cellsplitters/PGLDA.hpp:111-311, PGN.hpp:98-290, PGB.hpp:314-498);
+ *     PSI, the N residuals limited with the reference's residual limiter
+ *     (cellsplitters/LFResidualLimiter.hpp:37-110), which the reference applies only to its
+ *     Lax-Friedrichs schemes: that scheme is unpinned (no reference counterpart)
  *   WeakBC::apply + WeakDirichletBC::compute_on_element_weak
  *     (src/solver/rdm/bc/WeakBC.hpp:227-360,786-832, WeakDirichletBC.hpp:159-265)
  *   RDTimeUpdate (src/solver/rdm/RDTimeUpdate.hpp:71-194, RDTimeUpdate.cpp:41-67).
@@ -41,7 +44,8 @@ enum
 {
   RDSO_LDA = 0,
   RDSO_N   = 1,
-  RDSO_B   = 2
+  RDSO_B   = 2,
+  RDSO_PSI = 3 /* the N residuals limited with LFResidualLimiter.hpp:37-110 (scalar) */
 };
 
 enum

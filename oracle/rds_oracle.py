@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(_HERE, "_ref", "librds_oracle.so")
 HARNESS_PATH = os.path.join(_HERE, "_ref", "rds_ref_harness")
 
 PHYSICS = {"advconst": 0, "burgers": 1, "euler2d": 2, "euler3d": 3}
-SCHEME = {"lda": 0, "n": 1, "b": 2}
+SCHEME = {"lda": 0, "n": 1, "b": 2, "psi": 3}
 BC_KIND = {"WeakDirichlet": 0, "WeakWall": 1, "WeakSubInlet": 2, "WeakSubOutlet": 3,
            "WeakFarfield": 4, "StrongDirichlet": 5,
            "WeakSuperInlet": 6, "WeakSymmetry": 7}
@@ -187,6 +187,8 @@ class Oracle:
     def element_jacobian(self, group, cell, u):
         """Element Jacobian [ndof * neq, ndof * neq] of one cell at the state u (PGLDA, or PGN
         when the problem's scheme is "n")."""
+        if self.prob.scheme == "psi":
+            raise ValueError("no element Jacobians for the PSI scheme")
         prob, g = self.prob, self.prob.groups[group]
         X = np.ascontiguousarray(prob.geo_coords[g.geo_conn[cell]], dtype=np.float64)
         un = np.ascontiguousarray(np.asarray(u).reshape(-1, prob.neq)[g.sol_conn[cell]])

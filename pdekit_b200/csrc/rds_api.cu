@@ -631,13 +631,18 @@ rds_status rds_create(rds_ctx **out, const rds_desc *desc, void *stream)
   ctx->desc    = *desc;
   ctx->active_precision = desc->precision;
   const rds_desc &d = ctx->desc;
-  if (!supported_physics(d) || d.scheme < RDS_PGLDA || d.scheme > RDS_PGB ||
+  if (!supported_physics(d) || d.scheme < RDS_PGLDA || d.scheme > RDS_PGPSI ||
       (d.precision != RDS_FP64 && d.precision != RDS_MIXED) || d.nnodes <= 0 ||
       d.ngeo_nodes <= 0 || !desc->geo_coords)
   {
     rds_status st = RDS_ERR_INVALID;
     *out          = ctx;
     return fail(ctx, st, "invalid descriptor (physics/dim/neq/scheme/precision/sizes)");
+  }
+  if (d.scheme == RDS_PGPSI && (d.neq != 1 || d.precision != RDS_FP64))
+  {
+    *out = ctx;
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "the PSI scheme: scalar physics in FP64 contexts only");
   }
   *out = ctx;
   if (cudaGetDevice(&ctx->device) != cudaSuccess)
@@ -1346,6 +1351,8 @@ rds_status rds_element_jacobians(rds_ctx *ctx, int group, double *jac)
                : RDS_ERR_INVALID;
   if (ctx->nprob > 0)
     return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_element_jacobians: not in batched contexts");
+  if (ctx->desc.scheme == RDS_PGPSI)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_element_jacobians: not for the PSI scheme");
   const HostCellGroup &g = ctx->groups[group];
   if (ctx->blend_on && ctx->desc.scheme == RDS_PGB)
     return fail(ctx, RDS_ERR_UNSUPPORTED,
@@ -1462,6 +1469,8 @@ rds_status rds_assemble_jacobian(rds_ctx *ctx, double *values)
   if (!ctx || !values || !ctx->finalized || ctx->nprob > 0)
     return ctx ? fail(ctx, RDS_ERR_INVALID, "rds_assemble_jacobian: not a finalized single context")
                : RDS_ERR_INVALID;
+  if (ctx->desc.scheme == RDS_PGPSI)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_assemble_jacobian: not for the PSI scheme");
   rds_status st = build_jac_pattern(ctx);
   if (st != RDS_OK)
     return st;
@@ -2804,10 +2813,13 @@ rds_status rds_add_batch_cell_group(rds_ctx *ctx, const rds_cell_group *g, int p
     return fail(ctx, RDS_ERR_INVALID, "rds_add_batch_cell_group: rds_set_problems first");
   if (physics != RDS_ADVECTION_CONST && physics != RDS_BURGERS2D)
     return fail(ctx, RDS_ERR_UNSUPPORTED, "batched problems: scalar 2D physics only");
-  if (scheme < RDS_PGLDA || scheme > RDS_PGB || !problem_cells || !g->sol_conn ||
+  if (scheme < RDS_PGLDA || scheme > RDS_PGPSI || !problem_cells || !g->sol_conn ||
       g->ncells <= 0 || g->ndof <= 0 || problem_cells[0] != 0 || problem_cells[P] != g->ncells)
     return fail(ctx, RDS_ERR_INVALID,
                 "rds_add_batch_cell_group: invalid scheme or problem cell offsets");
+  if (scheme == RDS_PGPSI && ctx->desc.precision != RDS_FP64)
+    return fail(ctx, RDS_ERR_UNSUPPORTED, "rds_add_batch_cell_group: the PSI scheme in FP64 "
+                                          "contexts only");
   for (int p = 0; p < P; ++p)
   {
     if (problem_cells[p + 1] < problem_cells[p])

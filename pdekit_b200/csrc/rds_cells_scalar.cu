@@ -251,6 +251,23 @@ __device__ __forceinline__ void scalar_cell(const CellArgs &a,
     for (int n = 0; n < NDOF; ++n)
       out[(size_t)n * a.ncells] = skip ? lda[n] : lda[n] + tn[n] * diss[n];
   }
+  else if (SCHEME == RDS_PGPSI && fabs(phi) > 1.e-14)
+  {
+    // PSI: the N residuals limited with the reference's residual limiter
+    // (LFResidualLimiter.hpp:37-110): x_n = max(phi_n / phi, 0) + 1e-12 (std::max's NaN
+    // rule), phi_n = x_n / sum x * phi; cells with |phi| <= 1e-14 keep the N residuals
+    double x[NDOF], sx = 0.0;
+#pragma unroll
+    for (int n = 0; n < NDOF; ++n)
+    {
+      const double r = (lda[n] + diss[n]) / phi;
+      x[n]           = (r < 0.0 ? 0.0 : r) + 1.e-12;
+      sx += x[n];
+    }
+#pragma unroll
+    for (int n = 0; n < NDOF; ++n)
+      out[(size_t)n * a.ncells] = x[n] / sx * phi;
+  }
   else
   {
 #pragma unroll
@@ -393,8 +410,9 @@ cudaError_t dispatch_batch(const HostCellGroup &g, const CellArgs &a, int grid, 
 
 const char *kernel_name(int physics, int scheme)
 {
-  static const char *names[2][3] = {{"cells_adv_lda", "cells_adv_n", "cells_adv_b"},
-                                    {"cells_burgers_lda", "cells_burgers_n", "cells_burgers_b"}};
+  static const char *names[2][4] = {
+      {"cells_adv_lda", "cells_adv_n", "cells_adv_b", "cells_adv_psi"},
+      {"cells_burgers_lda", "cells_burgers_n", "cells_burgers_b", "cells_burgers_psi"}};
   return names[physics == RDS_BURGERS2D ? 1 : 0][scheme];
 }
 
@@ -417,6 +435,14 @@ cudaError_t launch_cells_scalar(const HostCellGroup &g, const CellArgs &a, int p
   RDS_SCALAR_CASE(RDS_BURGERS2D, RDS_PGN)
   RDS_SCALAR_CASE(RDS_BURGERS2D, RDS_PGB)
 #undef RDS_SCALAR_CASE
+  // PSI: FP64 contexts only
+  if (scheme == RDS_PGPSI && precision != RDS_MIXED)
+  {
+    if (physics == RDS_ADVECTION_CONST)
+      return dispatch_shape<RDS_ADVECTION_CONST, RDS_PGPSI, double>(g, a, s, ok);
+    if (physics == RDS_BURGERS2D)
+      return dispatch_shape<RDS_BURGERS2D, RDS_PGPSI, double>(g, a, s, ok);
+  }
   *ok = false;
   return cudaSuccess;
 }
@@ -425,16 +451,18 @@ cudaError_t launch_cells_scalar_batch(const HostCellGroup &g, const CellArgs &a,
                                       int grid, int tile, cudaStream_t s, const char **name,
                                       bool *ok)
 {
-  static const char *names[2][3][2] = {
+  static const char *names[2][4][2] = {
       {{"cells_adv_lda_batch", "cells_adv_lda_batch_f32"},
        {"cells_adv_n_batch", "cells_adv_n_batch_f32"},
-       {"cells_adv_b_batch", "cells_adv_b_batch_f32"}},
+       {"cells_adv_b_batch", "cells_adv_b_batch_f32"},
+       {"cells_adv_psi_batch", "cells_adv_psi_batch_f32"}},
       {{"cells_burgers_lda_batch", "cells_burgers_lda_batch_f32"},
        {"cells_burgers_n_batch", "cells_burgers_n_batch_f32"},
-       {"cells_burgers_b_batch", "cells_burgers_b_batch_f32"}}};
+       {"cells_burgers_b_batch", "cells_burgers_b_batch_f32"},
+       {"cells_burgers_psi_batch", "cells_burgers_psi_batch_f32"}}};
   const int physics = g.physics, scheme = g.scheme;
   *ok               = false;
-  if ((physics != RDS_ADVECTION_CONST && physics != RDS_BURGERS2D) || scheme < 0 || scheme > 2 ||
+  if ((physics != RDS_ADVECTION_CONST && physics != RDS_BURGERS2D) || scheme < 0 || scheme > 3 ||
       tile <= 0 || tile > 128 || grid <= 0)
     return cudaSuccess;
   *name = names[physics == RDS_BURGERS2D][scheme][precision == RDS_MIXED];
@@ -449,6 +477,12 @@ cudaError_t launch_cells_scalar_batch(const HostCellGroup &g, const CellArgs &a,
   RDS_BATCH_CASE(RDS_BURGERS2D, RDS_PGN)
   RDS_BATCH_CASE(RDS_BURGERS2D, RDS_PGB)
 #undef RDS_BATCH_CASE
+  if (scheme == RDS_PGPSI && precision != RDS_MIXED)
+  {
+    if (physics == RDS_ADVECTION_CONST)
+      return dispatch_batch<RDS_ADVECTION_CONST, RDS_PGPSI, double>(g, a, grid, tile, s, ok);
+    return dispatch_batch<RDS_BURGERS2D, RDS_PGPSI, double>(g, a, grid, tile, s, ok);
+  }
   return cudaSuccess;
 }
 

@@ -28,7 +28,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "librds_b200.so")
 
 PHYSICS = {"advconst": 0, "burgers": 1, "euler2d": 2, "euler3d": 3}
-SCHEME = {"lda": 0, "n": 1, "b": 2}
+SCHEME = {"lda": 0, "n": 1, "b": 2, "psi": 3}
 PRECISION = {"fp64": 0, "mixed": 1}
 SHAPE = {"line": 2, "triag": 3, "quad": 4, "tetra": 10}
 BC_KIND = {"WeakDirichlet": 0, "WeakWall": 1, "WeakSubInlet": 2, "WeakSubOutlet": 3,
