@@ -456,7 +456,10 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
   for (const HostBC &b : ctx->bcs)
     strong |= b.desc.kind == RDS_BC_STRONG_DIRICHLET;
   const bool with_bcs = !ctx->bcs.empty() && !ctx->no_bcs;
-  const bool fork     = with_bcs && !strong;
+  // per-kernel event timing: every kernel alone on the main stream, so that each event pair
+  // brackets one kernel and not its overlap with the others (the results do not change: the
+  // conditions write their own slots)
+  const bool fork     = with_bcs && !strong && !ctx->timing;
   // stream of the k-th condition: all on s (in order), or one side stream each when forked
   auto launch_bcs = [&](cudaStream_t s, bool spread) -> rds_status {
     for (size_t k = 0; k < ctx->bcs.size(); ++k)
