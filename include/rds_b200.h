@@ -400,6 +400,15 @@ RDS_API rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double dr
  * stops only at an exact sweep and converges to the FP64 scheme's fixed point. Longer periods
  * save exact sweeps but hold the time steps longer: at 32, three Burgers P1 N-scheme problems
  * at CFL 0.53 diverged (RDS_ERR_NONFINITE), none at 24.
+ * "mixed_fuse_cells" (default 65536): in a single context with one triangle group of at most
+ * that many cells and weak Dirichlet conditions only, the mixed_refresh - 1 correction sweeps
+ * of a cycle run as one launch, a barrier between the cells-and-facets phase and the node
+ * phase of every sweep: the same arithmetic as the separate launches, bit for bit, without
+ * their launch latency. Meshes of up to two items a thread of a 16-CTA cluster run as one
+ * thread-block cluster with its hardware barrier; larger ones as a grid of resident CTAs with
+ * a bounded barrier in global memory. 0 keeps separate launches. A barrier wait that
+ * gives up makes the call return RDS_ERR_CUDA ("bounded device wait"); "fuse_test_wait" (> 0,
+ * a test option) forces that after the given number of polls.
  * "mixed_switch" (default 1e-6): with RDS_MIXED and Euler physics (or a stabilisation field
  * installed), rds_iterate runs FP32 cell kernels
  * until max_eq norm/norm(iter 0) <= mixed_switch, or, once that drop has halved at least

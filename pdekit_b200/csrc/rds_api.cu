@@ -166,6 +166,11 @@ struct rds_ctx
   int loop_pdl       = 0;
   double *d_ur = nullptr, *d_dres = nullptr, *d_dc_theta = nullptr;
   float *d_c32 = nullptr, *d_dtv = nullptr;
+  // the correction sweeps of a cycle in one launch (dc_sweeps_fused) for meshes of at most
+  // dc_fuse_cells cells (option "mixed_fuse_cells"; 0: separate launches); d_fbar its barrier
+  long long dc_fuse_cells = 1LL << 16;
+  unsigned *d_fbar        = nullptr;
+  int fuse_test_wait      = 0; // option "fuse_test_wait" (the barrier's bounded-wait test)
   std::vector<long long> dc_cell_base; // first cell of each group in d_dc_theta
   StallRec *d_pstall  = nullptr; // the same per batched problem
 
@@ -443,6 +448,27 @@ rds_status join_sides(rds_ctx *ctx)
   return RDS_OK;
 }
 
+// Arguments of a correction sweep's cell kernel (defect-correction loop) for group ig.
+static DcCellArgs dc_cell_args(rds_ctx *ctx, size_t ig, const int *stop)
+{
+  const HostCellGroup &g = ctx->groups[ig];
+  DcCellArgs da{};
+  da.ncells     = g.desc.ncells;
+  da.sol_conn   = g.d_sol_conn;
+  da.geo_conn   = g.d_geo_conn;
+  da.X          = ctx->d_X;
+  da.ngeo_nodes = ctx->desc.ngeo_nodes;
+  da.u          = ctx->d_u;
+  da.ur         = ctx->d_ur;
+  da.c32        = ctx->d_c32;
+  da.slot_base  = g.slot_base;
+  da.theta      = ctx->d_dc_theta + ctx->dc_cell_base[ig];
+  da.adv0       = ctx->desc.adv[0];
+  da.adv1       = ctx->desc.adv[1];
+  da.stop       = stop;
+  return da;
+}
+
 // Residual contributions of all cells and boundary facets (assemble_rhs without the gather).
 // The boundary-facet kernels only touch their own contribution slots, so they run on a side
 // stream concurrently with the cell kernels (a parallel branch when captured in a graph) and
@@ -499,20 +525,7 @@ rds_status launch_residual_kernels(rds_ctx *ctx, const int *stop)
       if (ctx->dc_phase == 2)
       {
         // correction sweep: the FP32 change of the cell residual since the exact sweep
-        DcCellArgs da{};
-        da.ncells     = g.desc.ncells;
-        da.sol_conn   = g.d_sol_conn;
-        da.geo_conn   = g.d_geo_conn;
-        da.X          = ctx->d_X;
-        da.ngeo_nodes = ctx->desc.ngeo_nodes;
-        da.u          = ctx->d_u;
-        da.ur         = ctx->d_ur;
-        da.c32        = ctx->d_c32;
-        da.slot_base  = g.slot_base;
-        da.theta      = ctx->d_dc_theta + ctx->dc_cell_base[ig];
-        da.adv0       = ctx->desc.adv[0];
-        da.adv1       = ctx->desc.adv[1];
-        da.stop       = stop;
+        DcCellArgs da = dc_cell_args(ctx, ig, stop);
         da.pdl        = (ctx->loop_pdl && !ctx->timing && ig == 0) ? 1 : 0;
         bool ok       = false;
         const cudaError_t e = launch_cells_scalar_dc(g, da, 0, 0, ctx->stream, name, &ok);
@@ -562,7 +575,7 @@ rds_status check_status(rds_ctx *ctx)
   if (st & kFlagNegPressure)
     return fail(ctx, RDS_ERR_NEG_PRESSURE, "non-positive pressure met");
   if (st & kFlagTimeout)
-    return fail(ctx, RDS_ERR_CUDA, "a bounded device wait (tensor-core commit) gave up");
+    return fail(ctx, RDS_ERR_CUDA, "a bounded device wait (tensor-core commit or fused-sweep barrier) gave up");
   return RDS_OK;
 }
 
@@ -1152,8 +1165,10 @@ rds_status rds_finalize(rds_ctx *ctx)
           (st = dalloc(ctx, &ctx->d_dres, N)) != RDS_OK ||
           (st = dalloc(ctx, &ctx->d_dtv, N)) != RDS_OK ||
           (st = dalloc(ctx, &ctx->d_c32, (size_t)S)) != RDS_OK ||
-          (st = dalloc(ctx, &ctx->d_dc_theta, (size_t)nc)) != RDS_OK)
+          (st = dalloc(ctx, &ctx->d_dc_theta, (size_t)nc)) != RDS_OK ||
+          (st = dalloc(ctx, &ctx->d_fbar, 2)) != RDS_OK)
         return st;
+      ctx->extra.push_back(ctx->d_fbar);
       ctx->extra.push_back(ctx->d_ur);
       ctx->extra.push_back(ctx->d_dres);
       ctx->extra.push_back(ctx->d_dtv);
@@ -2347,8 +2362,52 @@ static rds_status enqueue_dc_sweep(rds_ctx *ctx, bool exact, double cfl, int max
   });
 }
 
+// Whether a cycle's correction sweeps run as one launch (dc_sweeps_fused): a single context
+// with one triangle group of at most dc_fuse_cells cells and weak Dirichlet conditions only.
+static bool dc_fused_ok(rds_ctx *ctx)
+{
+  if (ctx->nprob > 0 || ctx->groups.size() != 1 || ctx->bcs.size() > (size_t)kFuseMaxBC ||
+      ctx->no_bcs || ctx->grp_beg != 0 || ctx->grp_end >= 0 || !ctx->d_fbar ||
+      (long long)ctx->groups[0].desc.ncells > ctx->dc_fuse_cells)
+    return false;
+  const HostBC *bcs[kFuseMaxBC];
+  for (size_t k = 0; k < ctx->bcs.size(); ++k)
+    bcs[k] = &ctx->bcs[k];
+  return dc_fused_supported(ctx->groups[0], bcs, (int)ctx->bcs.size());
+}
+
+// `nsweeps` correction sweeps in one launch (after an exact sweep; see dc_sweeps_fused).
+static rds_status enqueue_dc_fused(rds_ctx *ctx, int nsweeps)
+{
+  DcFusedArgs fa{};
+  fa.cell = dc_cell_args(ctx, 0, ctx->d_stop);
+  const HostBC *bcs[kFuseMaxBC];
+  fa.nbc = (int)ctx->bcs.size();
+  for (int k = 0; k < fa.nbc; ++k)
+  {
+    bcs[k]       = &ctx->bcs[k];
+    fa.bc[k]     = bc_args(ctx, ctx->bcs[k], ctx->d_stop);
+    fa.bc[k].c32 = ctx->d_c32;
+  }
+  fa.ga            = gather_args(ctx, 0.0, ctx->d_stop);
+  fa.ga.c32        = ctx->d_c32;
+  fa.ga.dres       = ctx->d_dres;
+  fa.ga.dtv        = ctx->d_dtv;
+  fa.ga.ur         = ctx->d_ur;
+  fa.nsweeps       = nsweeps;
+  fa.bar           = ctx->d_fbar;
+  fa.status        = ctx->d_status;
+  fa.wait_limit    = ctx->fuse_test_wait > 0 ? ctx->fuse_test_wait : 1 << 22;
+  fa.test_extra    = ctx->fuse_test_wait > 0 ? 1 : 0;
+  return launch(ctx, [&](const char **name) {
+    bool ok             = false;
+    const cudaError_t e = launch_dc_fused(ctx->groups[0], bcs, fa, ctx->stream, name, &ok);
+    return ok ? e : cudaErrorNotSupported;
+  });
+}
+
 // Defect-correction loop of the mixed form: cycles of one exact FP64 sweep and dc_m - 1 FP32
-// correction sweeps, captured once (graph slot 6, several cycles per graph) and replayed until
+// correction sweeps (one launch for all of them on small meshes, dc_fused_ok), captured once (graph slot 6, several cycles per graph) and replayed until
 // an exact sweep raises the stop flag. The stop test sees only exact FP64 norms, and the fixed
 // point is the FP64 scheme's: at convergence the correction is zero and R64 = 0.
 static rds_status run_loop_dc(rds_ctx *ctx, double cfl, int max_iter, double drop)
@@ -2363,17 +2422,31 @@ static rds_status run_loop_dc(rds_ctx *ctx, double cfl, int max_iter, double dro
   if ((st = set_loop_params(ctx, lp)) != RDS_OK)
     return st;
   ctx->active_precision = RDS_FP64;
+  const bool fused      = m > 1 && dc_fused_ok(ctx);
   if (ctx->timing)
   {
     for (int it = 0; it < max_iter; ++it)
+    {
+      if (fused && it % m == 1)
+      {
+        // the rest of the cycle in one launch (its sweeps end at max_iter at the latest)
+        const int n = std::min(m - 1, max_iter - it);
+        if ((st = enqueue_dc_fused(ctx, n)) != RDS_OK)
+          return st;
+        it += n - 1;
+        continue;
+      }
       if ((st = enqueue_dc_sweep(ctx, it % m == 0, cfl, max_iter, drop)) != RDS_OK)
         return st;
+    }
     return RDS_OK;
   }
   const int cycles = std::max(1, 32 / m); // sweeps per graph launch: cycles x m
   auto cycle       = [&]() -> rds_status {
     for (int j = 0; j < m; ++j)
     {
+      if (fused && j == 1)
+        return enqueue_dc_fused(ctx, m - 1);
       const rds_status s2 = enqueue_dc_sweep(ctx, j == 0, cfl, max_iter, drop);
       if (s2 != RDS_OK)
         return s2;
@@ -2384,7 +2457,9 @@ static rds_status run_loop_dc(rds_ctx *ctx, double cfl, int max_iter, double dro
     return st;
   const long long per_sweep = (long long)ctx->groups.size() + (long long)ctx->bcs.size() + 1;
   const int per_graph       = cycles * m;
-  return replay_chunks(ctx, 6, (max_iter + per_graph - 1) / per_graph, per_sweep * per_graph);
+  const long long per_launch =
+      fused ? (long long)cycles * (per_sweep + 1) : per_sweep * per_graph;
+  return replay_chunks(ctx, 6, (max_iter + per_graph - 1) / per_graph, per_launch);
 }
 
 rds_status rds_iterate(rds_ctx *ctx, double cfl, int max_iter, double drop, int *it_done,
@@ -2717,6 +2792,37 @@ rds_status rds_set_option(rds_ctx *ctx, const char *key, double value)
           ctx->graph_exec[gi] = nullptr;
         }
     ctx->dc_m = (int)value;
+    return RDS_OK;
+  }
+  if (std::strcmp(key, "fuse_test_wait") == 0)
+  {
+    // test of the fused sweeps' bounded barrier wait: > 0 makes every barrier of the next
+    // fused launches wait for one arrival more than the grid has and give up after `value`
+    // polls (the call then reports RDS_ERR_CUDA); 0 restores the normal barrier
+    if (!(value >= 0.0 && value <= 1.0e6))
+      return fail(ctx, RDS_ERR_INVALID, "fuse_test_wait must be in [0, 1e6]");
+    ctx->fuse_test_wait = (int)value;
+    for (int gi : {2, 6})
+      if (ctx->graph_exec[gi])
+      {
+        cudaGraphExecDestroy(ctx->graph_exec[gi]);
+        ctx->graph_exec[gi] = nullptr;
+      }
+    return RDS_OK;
+  }
+  if (std::strcmp(key, "mixed_fuse_cells") == 0)
+  {
+    // defect-correction loop: one launch for a cycle's correction sweeps on meshes of at most
+    // `value` cells (0: one launch per kernel and sweep)
+    if (!(value >= 0.0 && value <= 2.0e9))
+      return fail(ctx, RDS_ERR_INVALID, "mixed_fuse_cells must be in [0, 2e9]");
+    ctx->dc_fuse_cells = (long long)value;
+    for (int gi : {2, 6})
+      if (ctx->graph_exec[gi])
+      {
+        cudaGraphExecDestroy(ctx->graph_exec[gi]);
+        ctx->graph_exec[gi] = nullptr;
+      }
     return RDS_OK;
   }
   if (std::strcmp(key, "mixed_stall_min") == 0)

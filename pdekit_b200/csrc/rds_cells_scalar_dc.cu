@@ -24,6 +24,8 @@
 // Schemes follow src/solver/rdm/cellsplitters/PGLDA.hpp:171-310, PGN.hpp:154-289 and
 // PGB.hpp:314-498 (the plain kernels restate them; this is their linearisation at u_r).
 
+#include "rds_bc_facet.cuh"
+#include "rds_gather_dc.cuh"
 #include "rds_internal.h"
 #include "rds_tables.cuh"
 
@@ -33,30 +35,41 @@ namespace rds
 namespace
 {
 
-template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL, int NGEO>
-__device__ __forceinline__ void dc_cell(const DcCellArgs &a,
-                                        const Tables<float, 2, NDOF, NQ, NFL, NGEO> &tb,
-                                        const int c)
+// What a cell's correction reads that stays the same within a cycle: its nodes, the reference
+// state there (in deviation form too), its inverse Jacobian and the frozen blending coefficient.
+template <int NDOF>
+struct DcCellState
+{
+  int v[NDOF];
+  double r[NDOF];
+  float ut[NDOF], u0;
+  float ij00, ij01, ij10, ij11, detj;
+  float theta;
+};
+
+template <int SCHEME, int NDOF, int NQ, int NFL, int NGEO>
+__device__ __forceinline__ void dc_cell_state(const DcCellArgs &a,
+                                              const Tables<float, 2, NDOF, NQ, NFL, NGEO> &tb,
+                                              const int c, DcCellState<NDOF> &st)
 {
   using T = float;
-  // reference state in deviation form (coefficients) and the correction d = u - u_r
+  // reference state in deviation form (coefficients)
   double ur0 = 0.0;
-  T ut[NDOF], dn[NDOF];
 #pragma unroll
   for (int n = 0; n < NDOF; ++n)
   {
-    const int v     = __ldg(a.sol_conn + (size_t)n * a.ncells + c);
-    const double r  = __ldg(a.ur + v);
-    const double uu = __ldg(a.u + v);
+    const int v    = __ldg(a.sol_conn + (size_t)n * a.ncells + c);
+    const double r = __ldg(a.ur + v);
     if (n == 0)
       ur0 = r;
-    ut[n] = T(r - ur0);
-    dn[n] = T(uu - r);
+    st.v[n]  = v;
+    st.r[n]  = r;
+    st.ut[n] = T(r - ur0);
   }
-  const T u0 = T(ur0);
+  st.u0 = T(ur0);
 
   // straight-sided triangle (deviation form of the vertex coordinates)
-  T ij00, ij01, ij10, ij11, detj;
+  T &ij00 = st.ij00, &ij01 = st.ij01, &ij10 = st.ij10, &ij11 = st.ij11, &detj = st.detj;
   {
     T X0[NGEO], X1[NGEO];
     double xg0 = 0.0, yg0 = 0.0;
@@ -90,6 +103,28 @@ __device__ __forceinline__ void dc_cell(const DcCellArgs &a,
     ij01            = -inv_det * J01;
     ij10            = -inv_det * J10;
   }
+  st.theta = (SCHEME == RDS_PGB) ? T(__ldg(a.theta + c)) : T(1);
+}
+
+// The cell's FP32 change from the correction d = u - u_r (the state is read each sweep).
+// COHERENT: the state is read through L2 (ld.global.cg), as the fused sweeps must (other blocks
+// of the same launch write it between sweeps)
+template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL, int NGEO, bool COHERENT>
+__device__ __forceinline__ void dc_cell_sweep(const DcCellArgs &a,
+                                              const Tables<float, 2, NDOF, NQ, NFL, NGEO> &tb,
+                                              const int c, const DcCellState<NDOF> &st)
+{
+  using T = float;
+  T dn[NDOF];
+#pragma unroll
+  for (int n = 0; n < NDOF; ++n)
+  {
+    const double uu = COHERENT ? __ldcg(a.u + st.v[n]) : __ldg(a.u + st.v[n]);
+    dn[n]           = T(uu - st.r[n]);
+  }
+  const T *ut = st.ut;
+  const T u0  = st.u0;
+  const T ij00 = st.ij00, ij01 = st.ij01, ij10 = st.ij10, ij11 = st.ij11, detj = st.detj;
 
   // change of the flux divergence at the points, dr_q = sum_f dVf[.][q][f] dG_f, with the flux
   // change at each flux node contracted with invJ once (constant over the cell)
@@ -142,7 +177,7 @@ __device__ __forceinline__ void dc_cell(const DcCellArgs &a,
   //   sum_q e K+_n dr_q + theta sum_q e K+_n (d_n sum K+ - sum_m K+_m d_m)
   //   = sum_q K+_n [e (dr_q - theta sum_m K+_m d_m)] + theta d_n sum_q w_q detJ K+_n,
   // two FMAs per point and node (theta = 1 for PGN, the N part absent for PGLDA).
-  const T theta = (SCHEME == RDS_PGB) ? T(__ldg(a.theta + c)) : T(1);
+  const T theta = st.theta;
   T racc[NDOF], wacc[NDOF];
 #pragma unroll
   for (int n = 0; n < NDOF; ++n)
@@ -209,6 +244,16 @@ __device__ __forceinline__ void dc_cell(const DcCellArgs &a,
         (SCHEME == RDS_PGLDA) ? racc[n] : racc[n] + (theta * dd[n]) * wacc[n];
 }
 
+template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL, int NGEO, bool COHERENT = false>
+__device__ __forceinline__ void dc_cell(const DcCellArgs &a,
+                                        const Tables<float, 2, NDOF, NQ, NFL, NGEO> &tb,
+                                        const int c)
+{
+  DcCellState<NDOF> st;
+  dc_cell_state<SCHEME, NDOF, NQ, NFL, NGEO>(a, tb, c, st);
+  dc_cell_sweep<PHYS, SCHEME, NDOF, NQ, NFL, NGEO, COHERENT>(a, tb, c, st);
+}
+
 template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL, int NGEO>
 __global__ void __launch_bounds__(kBlock)
     cells_scalar2d_dc(const __grid_constant__ DcCellArgs a,
@@ -252,6 +297,232 @@ __global__ void __launch_bounds__(128)
     if (c < a.bt.cend[lo])
       dc_cell<PHYS, SCHEME, NDOF, NQ, NFL, NGEO>(a, tb, c);
   }
+}
+
+// ---- fused correction sweeps ------------------------------------------------------------
+// A small mesh's correction sweep is a chain of short launches (cells, facets, gather) whose
+// cost is mostly their latency. dc_sweeps_fused runs the m - 1 correction sweeps between two
+// exact sweeps in one launch: per sweep, phase 1 the cells' and facets' FP32 changes (a
+// grid-stride loop over cells, then the facets of each condition), a grid barrier, phase 2 the
+// node updates, a grid barrier. The arithmetic is that of the separate kernels (dc_cell,
+// bc_weak_facet, dc_correction_node), so the results are theirs bit for bit; only the loads of
+// what other blocks wrote in the same launch (the state, the changes) go through L2. The grid
+// is at most what is resident at once (occupancy x SMs), and every barrier wait is bounded:
+// a barrier that gives up sets kFlagTimeout in the status word and the launch returns.
+
+constexpr int kClusterCtas = 16; // the cluster form's CTAs (a non-portable cluster size)
+// and threads per CTA: as many as the order's registers allow (P1 <= 102, P2 <= 128 a thread)
+constexpr int cluster_threads(int ndof) { return ndof == 3 ? 640 : ndof == 6 ? 512 : 256; }
+
+template <int NFDOF, int NFQ>
+struct FusedFacetTables
+{
+  FacetTables<double, 2, NFDOF, NFQ, 2> t[kFuseMaxBC];
+};
+
+// Grid barrier: bar[0] counts arrivals, bar[1] is the generation. Both are zero at launch (the
+// host clears them before every launch); the last block to arrive resets the count and
+// advances the generation. Returns false when the wait gave up after `limit` polls. `extra`
+// (a test option) raises the arrivals awaited beyond the grid, so that no wait completes.
+__device__ __forceinline__ bool fused_barrier(unsigned *bar, int limit, int extra)
+{
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    int ok           = 1;
+    const unsigned g = __ldcg(bar + 1);
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1 + (unsigned)extra)
+    {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    }
+    else
+    {
+      int t = 0;
+      while (__ldcg(bar + 1) == g)
+      {
+        if (++t > limit)
+        {
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+// Cluster form: the whole grid is one thread-block cluster (at most 16 CTAs, co-scheduled by
+// the launch), and the barrier is the cluster's hardware barrier with release / acquire
+// semantics at cluster scope (every block of the launch is in the cluster).
+__device__ __forceinline__ void cluster_barrier()
+{
+  __syncwarp(); // the .aligned barrier wants converged warps
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\t"
+               "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+template <bool CLUSTER>
+__device__ __forceinline__ bool sweep_barrier(const DcFusedArgs &a)
+{
+  if constexpr (CLUSTER)
+  {
+    cluster_barrier();
+    return true;
+  }
+  else
+    return fused_barrier(a.bar, a.wait_limit, a.test_extra);
+}
+
+template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL, int NFDOF, int NFQ, int NT,
+          bool CLUSTER>
+__global__ void __launch_bounds__(NT)
+    dc_sweeps_fused(const __grid_constant__ DcFusedArgs a,
+                    const __grid_constant__ Tables<float, 2, NDOF, NQ, NFL, 3> tb,
+                    const __grid_constant__ FusedFacetTables<NFDOF, NFQ> ft)
+{
+  if (*a.cell.stop)
+    return;
+  const int nthreads = gridDim.x * blockDim.x;
+  const int tid      = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ncells   = a.cell.ncells;
+  int nitems         = ncells;
+  for (int k = 0; k < a.nbc; ++k)
+    nitems += a.bc[k].nfacets;
+  // a thread's first cell and first node are the same in every sweep: what they read that
+  // does not change within the cycle is read once, into registers
+  DcCellState<NDOF> cs;
+  if (tid < ncells)
+    dc_cell_state<SCHEME, NDOF, NQ, NFL, 3>(a.cell, tb, tid, cs);
+  DcNodeState ns;
+  if (tid < a.ga.nnodes)
+    dc_node_state(a.ga, tid, ns);
+  for (int sweep = 0; sweep < a.nsweeps; ++sweep)
+  {
+    for (int i = tid; i < nitems; i += nthreads)
+    {
+      if (i == tid && i < ncells)
+        dc_cell_sweep<PHYS, SCHEME, NDOF, NQ, NFL, 3, true>(a.cell, tb, i, cs);
+      else if (i < ncells)
+        dc_cell<PHYS, SCHEME, NDOF, NQ, NFL, 3, true>(a.cell, tb, i);
+      else
+      {
+        int j = i - ncells, k = 0;
+        while (j >= a.bc[k].nfacets)
+          j -= a.bc[k++].nfacets;
+        bc_weak_facet<RDS_BC_WEAK_DIRICHLET, PHYS, 2, 1, NFDOF, NFQ, 2, true>(a.bc[k], ft.t[k], j);
+      }
+    }
+    if (!sweep_barrier<CLUSTER>(a))
+    {
+      if (threadIdx.x == 0)
+        atomicOr(a.status, kFlagTimeout);
+      return;
+    }
+    for (int v = tid; v < a.ga.nnodes; v += nthreads)
+    {
+      if (v == tid)
+        dc_node_sweep(a.ga, v, ns);
+      else
+        dc_correction_node<true>(a.ga, v);
+    }
+    if (sweep + 1 < a.nsweeps && !sweep_barrier<CLUSTER>(a))
+    {
+      if (threadIdx.x == 0)
+        atomicOr(a.status, kFlagTimeout);
+      return;
+    }
+  }
+}
+
+template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL, int NFDOF, int NFQ>
+cudaError_t launch_fused_one(const HostCellGroup &g, const HostBC *const *bcs,
+                             const DcFusedArgs &a, cudaStream_t s, bool *cluster)
+{
+  Tables<float, 2, NDOF, NQ, NFL, 3> tb;
+  fill_tables(tb, g.w, g.V, g.dV, g.dVgeo, g.dVf, g.Vsf);
+  FusedFacetTables<NFDOF, NFQ> ft{};
+  for (int k = 0; k < a.nbc; ++k)
+  {
+    const HostBC &b = *bcs[k];
+    for (int q = 0; q < NFQ; ++q)
+    {
+      ft.t[k].fw[q] = b.fw[q];
+      for (int n = 0; n < NFDOF; ++n)
+        ft.t[k].fV[q][n] = b.fV[q * NFDOF + n];
+      for (int gg = 0; gg < 2; ++gg)
+        ft.t[k].fdVgeo[0][q][gg] = b.fdVgeo[q * 2 + gg];
+    }
+  }
+  int items = a.cell.ncells;
+  for (int j = 0; j < a.nbc; ++j)
+    items += a.bc[j].nfacets;
+  if (a.ga.nnodes > items)
+    items = a.ga.nnodes;
+  // small meshes (at most two items a thread): one cluster of kClusterCtas CTAs of NTC
+  // threads and the hardware cluster barrier (no bounded-wait test there: the launch
+  // co-schedules the cluster and the barrier is not a poll)
+  constexpr int NTC = cluster_threads(NDOF);
+  *cluster           = false;
+  if (a.test_extra == 0 && items <= 2 * kClusterCtas * NTC)
+  {
+    auto kc = dc_sweeps_fused<PHYS, SCHEME, NDOF, NQ, NFL, NFDOF, NFQ, NTC, true>;
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    attr[0].id               = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClusterCtas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim              = dim3(kClusterCtas);
+    cfg.blockDim             = dim3(NTC);
+    cfg.attrs                = attr;
+    cfg.numAttrs             = 1;
+    // whether the cluster fits, asked once per kernel (the first call usually comes during a
+    // stream capture: the queries then run in relaxed capture mode and on no stream)
+    static int fits = -1;
+    if (fits < 0)
+    {
+      cudaStreamCaptureMode mode = cudaStreamCaptureModeRelaxed;
+      cudaThreadExchangeStreamCaptureMode(&mode);
+      int nclusters = 0;
+      cudaError_t e = cudaFuncSetAttribute(kc, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveClusters(&nclusters, kc, &cfg);
+      fits = (e == cudaSuccess && nclusters >= 1) ? 1 : 0;
+      cudaGetLastError();
+      cudaThreadExchangeStreamCaptureMode(&mode);
+    }
+    if (fits == 1)
+    {
+      *cluster   = true;
+      cfg.stream = s;
+      return cudaLaunchKernelEx(&cfg, kc, a, tb, ft);
+    }
+  }
+  auto k = dc_sweeps_fused<PHYS, SCHEME, NDOF, NQ, NFL, NFDOF, NFQ, kBlock, false>;
+  // every block must be resident at once (the blocks wait for one another at the barriers):
+  // the grid is capped at this kernel's occupancy on all SMs
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kBlock, 0);
+  if (per_sm < 1)
+    return cudaErrorInvalidConfiguration;
+  int grid = (items + kBlock - 1) / kBlock;
+  if (grid > per_sm * nsm)
+    grid = per_sm * nsm;
+  cudaError_t e = cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned), s);
+  if (e != cudaSuccess)
+    return e;
+  k<<<grid, kBlock, 0, s>>>(a, tb, ft);
+  return cudaGetLastError();
 }
 
 template <int PHYS, int SCHEME, int NDOF, int NQ, int NFL>
@@ -343,6 +614,76 @@ cudaError_t launch_cells_scalar_dc(const HostCellGroup &g, const DcCellArgs &a, 
   RDS_DC_CASE(RDS_BURGERS2D, RDS_PGN)
   RDS_DC_CASE(RDS_BURGERS2D, RDS_PGB)
 #undef RDS_DC_CASE
+  return cudaSuccess;
+}
+
+// The fused correction sweeps cover one straight-sided triangle group with the facet rule of
+// its order's usual cell rule (P1: 2 dofs / 3 points, P2: 3 / 4, P3: 4 / 5) and up to
+// kFuseMaxBC weak Dirichlet conditions.
+namespace
+{
+bool fused_facets(int ndof, const rds_bc_group &d)
+{
+  const int nfdof = ndof == 3 ? 2 : ndof == 6 ? 3 : 4;
+  return d.nfgeo == 2 && d.nfdof == nfdof && d.nfq == nfdof + 1;
+}
+} // namespace
+
+bool dc_fused_supported(const HostCellGroup &g, const HostBC *const *bcs, int nbc)
+{
+  if (!dc_supported(g) || g.scheme < 0 || g.scheme > 2 || nbc > kFuseMaxBC)
+    return false;
+  for (int k = 0; k < nbc; ++k)
+    if (bcs[k]->desc.kind != RDS_BC_WEAK_DIRICHLET || !fused_facets(g.desc.ndof, bcs[k]->desc))
+      return false;
+  return true;
+}
+
+cudaError_t launch_dc_fused(const HostCellGroup &g, const HostBC *const *bcs,
+                            const DcFusedArgs &a, cudaStream_t s, const char **name, bool *ok)
+{
+  // [cluster form][physics][scheme]
+  static const char *names[2][2][3] = {
+      {{"dc_sweeps_fused_adv_lda", "dc_sweeps_fused_adv_n", "dc_sweeps_fused_adv_b"},
+       {"dc_sweeps_fused_burgers_lda", "dc_sweeps_fused_burgers_n", "dc_sweeps_fused_burgers_b"}},
+      {{"dc_sweeps_cluster_adv_lda", "dc_sweeps_cluster_adv_n", "dc_sweeps_cluster_adv_b"},
+       {"dc_sweeps_cluster_burgers_lda", "dc_sweeps_cluster_burgers_n",
+        "dc_sweeps_cluster_burgers_b"}}};
+  *ok = false;
+  if (!dc_fused_supported(g, bcs, a.nbc))
+    return cudaSuccess;
+  const rds_cell_group &d = g.desc;
+  *ok                     = true;
+  bool cl                 = false;
+  const int ip = g.physics == RDS_BURGERS2D ? 1 : 0, is = g.scheme;
+  *name                   = names[0][ip][is];
+  // the launch name tells the two forms apart
+  auto named = [&](cudaError_t e) {
+    *name = names[cl ? 1 : 0][ip][is];
+    return e;
+  };
+#define RDS_FUSED(PH, SC)                                                                          \
+  if (g.physics == PH && g.scheme == SC)                                                           \
+  {                                                                                                \
+    if (d.ndof == 3 && d.nq == 6)                                                                  \
+      return named(launch_fused_one<PH, SC, 3, 6, 6, 2, 3>(g, bcs, a, s, &cl));                    \
+    if (d.ndof == 3 && d.nq == 7)                                                                  \
+      return named(launch_fused_one<PH, SC, 3, 7, 6, 2, 3>(g, bcs, a, s, &cl));                    \
+    if (d.ndof == 6 && d.nq == 6)                                                                  \
+      return named(launch_fused_one<PH, SC, 6, 6, 10, 3, 4>(g, bcs, a, s, &cl));                   \
+    if (d.ndof == 6 && d.nq == 7)                                                                  \
+      return named(launch_fused_one<PH, SC, 6, 7, 10, 3, 4>(g, bcs, a, s, &cl));                   \
+    if (d.ndof == 10 && d.nq == 16)                                                                \
+      return named(launch_fused_one<PH, SC, 10, 16, 15, 4, 5>(g, bcs, a, s, &cl));                 \
+  }
+  RDS_FUSED(RDS_ADVECTION_CONST, RDS_PGLDA)
+  RDS_FUSED(RDS_ADVECTION_CONST, RDS_PGN)
+  RDS_FUSED(RDS_ADVECTION_CONST, RDS_PGB)
+  RDS_FUSED(RDS_BURGERS2D, RDS_PGLDA)
+  RDS_FUSED(RDS_BURGERS2D, RDS_PGN)
+  RDS_FUSED(RDS_BURGERS2D, RDS_PGB)
+#undef RDS_FUSED
+  *ok = false;
   return cudaSuccess;
 }
 

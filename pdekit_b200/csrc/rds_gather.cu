@@ -10,6 +10,7 @@
 // Multiplies and adds are issued as separate round-to-nearest operations (no fused
 // multiply-add) so the sums match the reference's x86-64 arithmetic.
 
+#include "rds_gather_dc.cuh"
 #include "rds_internal.h"
 
 namespace rds
@@ -81,24 +82,7 @@ __device__ __forceinline__ void gather_node(const GatherArgs &a, const int v, co
   static_assert(DC == 0 || NEQ == 1, "the defect-correction gather is scalar");
   if (DC == 2)
   {
-    const int i0 = a.row[v], i1 = a.row[v + 1];
-    double sum   = 0.0;
-    int i        = i0;
-    constexpr int B = 4;
-    for (; i + B <= i1; i += B)
-    {
-      float c[B];
-#pragma unroll
-      for (int k = 0; k < B; ++k)
-        c[k] = __ldcs(a.c32 + __ldg(a.ent_slot + i + k));
-#pragma unroll
-      for (int k = 0; k < B; ++k)
-        sum += double(c[k]);
-    }
-    for (; i < i1; ++i)
-      sum += double(__ldcs(a.c32 + __ldg(a.ent_slot + i)));
-    double *pu = a.u + v;
-    *pu        = *pu - (a.dres[v] + double(a.dtv[v]) * sum);
+    dc_correction_node<false>(a, v);
     return;
   }
   double acc[NEQ];

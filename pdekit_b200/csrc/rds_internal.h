@@ -350,6 +350,26 @@ cudaError_t launch_update(int nnodes, int neq, const double *dt, const double *r
 bool dc_supported(const HostCellGroup &g);
 cudaError_t launch_cells_scalar_dc(const HostCellGroup &g, const DcCellArgs &a, int grid,
                                    int tile, cudaStream_t s, const char **name, bool *ok);
+// The correction sweeps between two exact sweeps in one launch (rds_cells_scalar_dc.cu,
+// dc_sweeps_fused): one triangle group, up to kFuseMaxBC weak Dirichlet conditions. bar: two
+// device words the launcher clears before the launch (grid barrier).
+constexpr int kFuseMaxBC = 4;
+struct DcFusedArgs
+{
+  DcCellArgs cell;
+  BCArgs bc[kFuseMaxBC]; // with c32 set: the facets' changes
+  int nbc;
+  GatherArgs ga; // mode 19 fields: row, ent_slot, c32, dres, dtv, u, nnodes
+  int nsweeps;
+  unsigned *bar;
+  unsigned *status;  // kFlagTimeout when a barrier wait gives up
+  int wait_limit;    // polls of a barrier wait
+  int test_extra;    // test option: arrivals a barrier waits for beyond the grid (0; 1 never
+                     // completes, so every wait runs out)
+};
+bool dc_fused_supported(const HostCellGroup &g, const HostBC *const *bcs, int nbc);
+cudaError_t launch_dc_fused(const HostCellGroup &g, const HostBC *const *bcs,
+                            const DcFusedArgs &a, cudaStream_t s, const char **name, bool *ok);
 // PGLDA / PGN element Jacobians (rds_jacobian.cu): jac [ncells][ndof*neq][ndof*neq]
 cudaError_t launch_jacobians(const HostCellGroup &g, const CellArgs &a, int physics, int scheme,
                              int dim, int neq, double *jac, cudaStream_t s);

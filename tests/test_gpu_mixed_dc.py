@@ -81,3 +81,50 @@ def test_loop_reaches_the_fp64_solution(case, cfl, m):
     assert itm <= 1.25 * it64 + m, (itm, it64)
     assert len(hm) == itm
     assert np.array_equal(hm[1:m], np.repeat(hm[:1], m - 1, axis=0))
+
+
+FUSABLE = [c for c in SCALAR if "strong" not in c]
+
+
+@pytest.mark.parametrize("case", FUSABLE)
+@pytest.mark.parametrize("m", [4, 24])
+def test_fused_correction_sweeps_equal_separate_launches(case, m):
+    """The correction sweeps of a cycle in one launch (dc_sweeps_fused, the default on these
+    small meshes) against one launch per kernel and sweep: states and exact-sweep norms equal
+    bit for bit, including a run that stops inside a cycle."""
+    prob, a, meta = load_golden(os.path.join(GOLDEN, case))
+    out = []
+    for fuse in (0, 1 << 16):
+        s = _solver(prob, "mixed", m)
+        s.set_option("mixed_fuse_cells", fuse)
+        s.set_solution(a["u0"])
+        it, hist = s.iterate(meta["cfl"], 3 * m + 5)
+        out.append((it, s.solution(), hist))
+        s.close()
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
+
+
+def test_fused_barrier_bounded_wait_reports_timeout_and_recovers():
+    """With the test option every barrier of the fused sweeps waits for one block more than the
+    grid holds: each wait gives up after the given polls, the call reports RDS_ERR_CUDA with the
+    bounded-wait message, and the context then runs as a fresh one."""
+    from pdekit_b200.rds import RDSError
+    prob, a, meta = load_golden(os.path.join(GOLDEN, "burgers_p2_n"))
+    s = _solver(prob, "mixed", 8)
+    s.set_solution(a["u0"])
+    s.set_option("fuse_test_wait", 200)
+    with pytest.raises(RDSError) as err:
+        s.iterate(meta["cfl"], 16)
+    assert err.value.status == 2 and "bounded device wait" in str(err.value)
+    s.set_option("fuse_test_wait", 0)
+    s.set_solution(a["u0"])
+    it, hist = s.iterate(meta["cfl"], 16)
+    u = s.solution()
+    s.close()
+    f = _solver(prob, "mixed", 8)
+    f.set_solution(a["u0"])
+    it2, hist2 = f.iterate(meta["cfl"], 16)
+    assert it == it2 and np.array_equal(u, f.solution()) and np.array_equal(hist, hist2)
+    f.close()
