@@ -496,7 +496,9 @@ def loop_rates(prob, u0, cfl, sweeps, world):
         if prec == "mixed":
             s.set_solution(u0)
             s.kernel_timing(True)
-            s.iterate(cfl, 33, 0.0)
+            # two full cycles of the default period (24): the loop stops at an exact sweep once
+            # the next cycle would pass max_iter, so 2 x 24 + 1 sweeps
+            s.iterate(cfl, 49, 0.0)
             out["mixed_kernels_ms_per_launch"] = {k: round(v[0] / v[1], 5)
                                                   for k, v in s.kernel_times().items()}
             s.kernel_timing(False)
