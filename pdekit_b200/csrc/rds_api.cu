@@ -1200,11 +1200,10 @@ rds_status rds_set_state(rds_ctx *ctx, const double *u)
   {
     RDS_CUDA(cudaMemcpyAsync(ctx->d_stage, u, (size_t)N * NEQ * sizeof(double),
                              cudaMemcpyHostToDevice, ctx->stream));
-    // strided device-to-device copies: AoS column e -> SoA row e
-    for (int e = 0; e < NEQ; ++e)
-      RDS_CUDA(cudaMemcpy2DAsync(ctx->d_u + (size_t)e * N, sizeof(double), ctx->d_stage + e,
-                                 NEQ * sizeof(double), sizeof(double), N,
-                                 cudaMemcpyDeviceToDevice, ctx->stream));
+    // node-major staging -> equation-major state
+    return launch(ctx, [&](const char **name) {
+      return launch_transpose_state(N, NEQ, ctx->d_stage, ctx->d_u, true, ctx->stream, name);
+    });
   }
   return RDS_OK;
 }
@@ -1219,10 +1218,11 @@ static rds_status get_soa(rds_ctx *ctx, const double *d_soa, double *h_aos, int 
   }
   else
   {
-    for (int e = 0; e < neq; ++e)
-      RDS_CUDA(cudaMemcpy2DAsync(ctx->d_stage + e, neq * sizeof(double), d_soa + (size_t)e * N,
-                                 sizeof(double), sizeof(double), N, cudaMemcpyDeviceToDevice,
-                                 ctx->stream));
+    const rds_status st = launch(ctx, [&](const char **name) {
+      return launch_transpose_state(N, neq, d_soa, ctx->d_stage, false, ctx->stream, name);
+    });
+    if (st != RDS_OK)
+      return st;
     RDS_CUDA(cudaMemcpyAsync(h_aos, ctx->d_stage, (size_t)N * neq * sizeof(double),
                              cudaMemcpyDeviceToHost, ctx->stream));
   }
@@ -1902,11 +1902,10 @@ rds_status rds_step_host(rds_ctx *ctx, const double *u_in, double *u_out, double
   RDS_CUDA(cudaStreamWaitEvent(s, ctx->ev_in_ready[k], 0));
   if (NEQ == 1)
     RDS_CUDA(cudaMemcpyAsync(ctx->d_u, ctx->d_hin[k], bytes, cudaMemcpyDeviceToDevice, s));
-  else
-    for (int e = 0; e < NEQ; ++e)
-      RDS_CUDA(cudaMemcpy2DAsync(ctx->d_u + (size_t)e * N, sizeof(double), ctx->d_hin[k] + e,
-                                 NEQ * sizeof(double), sizeof(double), N,
-                                 cudaMemcpyDeviceToDevice, s));
+  else if ((st = launch(ctx, [&](const char **name) {
+             return launch_transpose_state(N, NEQ, ctx->d_hin[k], ctx->d_u, true, s, name);
+           })) != RDS_OK)
+    return st;
   RDS_CUDA(cudaEventRecord(ctx->ev_in_free[k], s));
   if ((st = rds_run(ctx, cfl, 1)) != RDS_OK)
     return st;
@@ -1919,11 +1918,10 @@ rds_status rds_step_host(rds_ctx *ctx, const double *u_in, double *u_out, double
   RDS_CUDA(cudaStreamWaitEvent(s, ctx->ev_out_free[k], 0));
   if (NEQ == 1)
     RDS_CUDA(cudaMemcpyAsync(ctx->d_hout[k], ctx->d_u, bytes, cudaMemcpyDeviceToDevice, s));
-  else
-    for (int e = 0; e < NEQ; ++e)
-      RDS_CUDA(cudaMemcpy2DAsync(ctx->d_hout[k] + e, NEQ * sizeof(double),
-                                 ctx->d_u + (size_t)e * N, sizeof(double), sizeof(double), N,
-                                 cudaMemcpyDeviceToDevice, s));
+  else if ((st = launch(ctx, [&](const char **name) {
+             return launch_transpose_state(N, NEQ, ctx->d_u, ctx->d_hout[k], false, s, name);
+           })) != RDS_OK)
+    return st;
   RDS_CUDA(cudaEventRecord(ctx->ev_out_ready[k], s));
 
   // download

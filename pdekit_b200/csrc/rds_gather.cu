@@ -374,6 +374,22 @@ __global__ void update_kernel(int n, const double *dt, const double *res, double
   }
 }
 
+// The host's node-major state [n][neq] and the device's equation-major one [neq][n]: one thread
+// per element, the node-major side read or written contiguously (to_soa: aos -> soa).
+__global__ void transpose_state(long long total, int n, int neq, const double *__restrict__ src,
+                                double *__restrict__ dst, int to_soa)
+{
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total)
+    return;
+  const long long v = i / neq;
+  const int e       = (int)(i - v * neq);
+  if (to_soa)
+    dst[(size_t)e * n + v] = src[i];
+  else
+    dst[i] = src[(size_t)e * n + v];
+}
+
 // Cell volume sum_q w_q detJ_q (set-up only; tables read from global memory).
 __global__ void cell_volume_kernel(int ncells, int dim, int nq, int ngeo,
                                    const int32_t *geo_conn, const double *X, int ngeo_nodes,
@@ -751,6 +767,16 @@ cudaError_t launch_norm_final(const double *part, int nblocks, int neq, int nnod
   *name = "norm_final";
   norm_final<<<1, kGBlock, 0, s>>>(part, nblocks, neq, nnodes, norm, norm0, hist, iter, max_hist,
                                    drop, stop, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_state(int nnodes, int neq, const double *src, double *dst,
+                                   bool to_soa, cudaStream_t s, const char **name)
+{
+  *name                 = to_soa ? "state_to_soa" : "state_to_aos";
+  const long long total = (long long)nnodes * neq;
+  transpose_state<<<(unsigned)((total + kGBlock - 1) / kGBlock), kGBlock, 0, s>>>(
+      total, nnodes, neq, src, dst, to_soa ? 1 : 0);
   return cudaGetLastError();
 }
 

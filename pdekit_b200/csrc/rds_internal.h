@@ -343,6 +343,9 @@ bool tc_supported(const HostCellGroup &g);
 void tc_tables(const HostCellGroup &g, std::vector<float> &out);
 cudaError_t launch_cells_scalar_tc(const HostCellGroup &g, const CellArgs &a, bool batch, int grid,
                                    int ntiles, cudaStream_t s, const char **name, bool *ok);
+// node-major [n][neq] <-> equation-major [neq][n] state (to_soa: the former to the latter)
+cudaError_t launch_transpose_state(int nnodes, int neq, const double *src, double *dst,
+                                   bool to_soa, cudaStream_t s, const char **name);
 cudaError_t launch_update(int nnodes, int neq, const double *dt, const double *res, double *u,
                           cudaStream_t s, const char **name);
 // Mixed form, scalar physics: FP32 correction-sweep cell kernels of the defect-correction loop;
