@@ -347,7 +347,7 @@ cudaError_t dispatch_shape(const HostCellGroup &g, const CellArgs &a, cudaStream
   *ok                     = true;
   if (d.shape == RDS_TRIAG && d.ngeo == 3)
   {
-    // (order, quadrature points, flux nodes): P1/P4-rule, P1/P5, P2/P4, P2/P5, P3/P8
+    // (order, quadrature points, flux nodes): P1/P4-rule, P1/P5, P2/P4, P2/P5, P3/P6, P3/P8
     if (d.ndof == 3 && d.nq == 6 && d.nfl == 6)
       return launch_one<PHYS, SCHEME, T, 3, 6, 6, 3>(g, a, s);
     if (d.ndof == 3 && d.nq == 7 && d.nfl == 6)
@@ -356,6 +356,8 @@ cudaError_t dispatch_shape(const HostCellGroup &g, const CellArgs &a, cudaStream
       return launch_one<PHYS, SCHEME, T, 6, 6, 10, 3>(g, a, s);
     if (d.ndof == 6 && d.nq == 7 && d.nfl == 10)
       return launch_one<PHYS, SCHEME, T, 6, 7, 10, 3>(g, a, s);
+    if (d.ndof == 10 && d.nq == 12 && d.nfl == 15)
+      return launch_one<PHYS, SCHEME, T, 10, 12, 15, 3>(g, a, s);
     if (d.ndof == 10 && d.nq == 16 && d.nfl == 15)
       return launch_one<PHYS, SCHEME, T, 10, 16, 15, 3>(g, a, s);
   }
@@ -396,11 +398,13 @@ cudaError_t dispatch_batch(const HostCellGroup &g, const CellArgs &a, int grid, 
   *ok                     = true;
   if (d.shape == RDS_TRIAG && d.ngeo == 3)
   {
-    // straight-sided triangles, P1 / P4 rule, P2 / P5 rule, P3 / P8 rule
+    // straight-sided triangles, P1 / P4 rule, P2 / P5 rule, P3 / P6 and P8 rules
     if (d.ndof == 3 && d.nq == 6 && d.nfl == 6)
       return launch_batch_one<PHYS, SCHEME, T, 3, 6, 6>(g, a, grid, tile, s);
     if (d.ndof == 6 && d.nq == 7 && d.nfl == 10)
       return launch_batch_one<PHYS, SCHEME, T, 6, 7, 10>(g, a, grid, tile, s);
+    if (d.ndof == 10 && d.nq == 12 && d.nfl == 15)
+      return launch_batch_one<PHYS, SCHEME, T, 10, 12, 15>(g, a, grid, tile, s);
     if (d.ndof == 10 && d.nq == 16 && d.nfl == 15)
       return launch_batch_one<PHYS, SCHEME, T, 10, 16, 15>(g, a, grid, tile, s);
   }

@@ -566,11 +566,12 @@ cudaError_t dispatch_shape(const HostCellGroup &g, const DcCellArgs &a, int grid
                     : launch_one<PHYS, SCHEME, ND, NQ_, NF>(g, a, s);
   if (d.shape == RDS_TRIAG && d.ngeo == 3)
   {
-    // (order, quadrature points, flux nodes): P1/P4-rule, P1/P5, P2/P4, P2/P5, P3/P8
+    // (order, quadrature points, flux nodes): P1/P4-rule, P1/P5, P2/P4, P2/P5, P3/P6, P3/P8
     RDS_DC_SHAPE(3, 6, 6)
     RDS_DC_SHAPE(3, 7, 6)
     RDS_DC_SHAPE(6, 6, 10)
     RDS_DC_SHAPE(6, 7, 10)
+    RDS_DC_SHAPE(10, 12, 15)
     RDS_DC_SHAPE(10, 16, 15)
   }
 #undef RDS_DC_SHAPE
@@ -588,7 +589,7 @@ bool dc_supported(const HostCellGroup &g)
     return false;
   return (d.ndof == 3 && (d.nq == 6 || d.nq == 7) && d.nfl == 6) ||
          (d.ndof == 6 && (d.nq == 6 || d.nq == 7) && d.nfl == 10) ||
-         (d.ndof == 10 && d.nq == 16 && d.nfl == 15);
+         (d.ndof == 10 && (d.nq == 12 || d.nq == 16) && d.nfl == 15);
 }
 
 cudaError_t launch_cells_scalar_dc(const HostCellGroup &g, const DcCellArgs &a, int grid,
@@ -618,14 +619,16 @@ cudaError_t launch_cells_scalar_dc(const HostCellGroup &g, const DcCellArgs &a, 
 }
 
 // The fused correction sweeps cover one straight-sided triangle group with the facet rule of
-// its order's usual cell rule (P1: 2 dofs / 3 points, P2: 3 / 4, P3: 4 / 5) and up to
+// its order's usual cell rule (P1: 2 dofs / 3 points, P2: 3 / 4, P3: 4 / 5, P3 with the order-6
+// cell rule: 4 / 4) and up to
 // kFuseMaxBC weak Dirichlet conditions.
 namespace
 {
-bool fused_facets(int ndof, const rds_bc_group &d)
+bool fused_facets(int ndof, int nq, const rds_bc_group &d)
 {
   const int nfdof = ndof == 3 ? 2 : ndof == 6 ? 3 : 4;
-  return d.nfgeo == 2 && d.nfdof == nfdof && d.nfq == nfdof + 1;
+  const int nfq   = (ndof == 10 && nq == 12) ? 4 : nfdof + 1; // P3 / P6 rule: facets of order 7
+  return d.nfgeo == 2 && d.nfdof == nfdof && d.nfq == nfq;
 }
 } // namespace
 
@@ -634,7 +637,8 @@ bool dc_fused_supported(const HostCellGroup &g, const HostBC *const *bcs, int nb
   if (!dc_supported(g) || g.scheme < 0 || g.scheme > 2 || nbc > kFuseMaxBC)
     return false;
   for (int k = 0; k < nbc; ++k)
-    if (bcs[k]->desc.kind != RDS_BC_WEAK_DIRICHLET || !fused_facets(g.desc.ndof, bcs[k]->desc))
+    if (bcs[k]->desc.kind != RDS_BC_WEAK_DIRICHLET ||
+        !fused_facets(g.desc.ndof, g.desc.nq, bcs[k]->desc))
       return false;
   return true;
 }
@@ -675,6 +679,8 @@ cudaError_t launch_dc_fused(const HostCellGroup &g, const HostBC *const *bcs,
       return named(launch_fused_one<PH, SC, 6, 7, 10, 3, 4>(g, bcs, a, s, &cl));                   \
     if (d.ndof == 10 && d.nq == 16)                                                                \
       return named(launch_fused_one<PH, SC, 10, 16, 15, 4, 5>(g, bcs, a, s, &cl));                 \
+    if (d.ndof == 10 && d.nq == 12)                                                                \
+      return named(launch_fused_one<PH, SC, 10, 12, 15, 4, 4>(g, bcs, a, s, &cl));                 \
   }
   RDS_FUSED(RDS_ADVECTION_CONST, RDS_PGLDA)
   RDS_FUSED(RDS_ADVECTION_CONST, RDS_PGN)

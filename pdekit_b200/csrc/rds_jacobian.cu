@@ -370,6 +370,7 @@ cudaError_t dispatch_jac(const HostCellGroup &g, const CellArgs &a, double *jac,
     RDS_JAC(RDS_TRIAG, 3, 3, 7, 6)
     RDS_JAC(RDS_TRIAG, 3, 6, 6, 10)
     RDS_JAC(RDS_TRIAG, 3, 6, 7, 10)
+    RDS_JAC(RDS_TRIAG, 3, 10, 12, 15)
     RDS_JAC(RDS_TRIAG, 3, 10, 16, 15)
     if constexpr (NEQ > 1)
     {
@@ -380,6 +381,7 @@ cudaError_t dispatch_jac(const HostCellGroup &g, const CellArgs &a, double *jac,
   }
   else
   {
+    RDS_JAC(RDS_TETRA, 4, 4, 4, 10)
     RDS_JAC(RDS_TETRA, 4, 10, 14, 20)
   }
 #undef RDS_JAC

@@ -144,6 +144,15 @@ CASES = {
                                   "bump2d_jump", EULER2D_BCS, 0.5, 3, "blend:Bonanni2D:0"),
     "euler3d_tet_p2_b_bonanni": ("euler3d", "b", 2, 5, ("box_tet", 4, 2, 2), 0.1, 64,
                                  "bump3d_jump", EULER3D_BCS, 0.5, 3, "blend3d:Bonanni3D:0"),
+    # rules the reference's own examples use: P3 triangles with the order-6 rule (12 points,
+    # examples/testcases-rdm/Burgers-RDS-2D.cpp), P1 tetrahedra with the order-2 rule (4 points,
+    # Bump-RDS-3D-Explicit.cpp)
+    "burgers_p3_q6_b": ("burgers", "b", 3, 6, 5, 0.15, 67, "burgers", BURG_BCS, 0.5, 3),
+    "adv_p3_q6_n": ("advconst", "n", 3, 6, 5, 0.2, 68, "smooth", ADV_BCS, 0.9, 3),
+    "euler3d_tet_p1_lda": ("euler3d", "lda", 1, 2, ("box_tet", 4, 2, 2), 0.1, 69, "bump3d",
+                           EULER3D_BCS, 0.5, 3),
+    "euler3d_tet_p1_b": ("euler3d", "b", 1, 2, ("box_tet", 4, 2, 2), 0.1, 70, "bump3d",
+                         EULER3D_BCS, 0.5, 3),
     # the smoothness sensor on bilinear quadrilaterals (detJ varies inside the cell); P1 only:
     # at p >= 2 the reference's rule of order 2p has fewer points than the cell has modes, its
     # modal mass matrix is singular and the sensor follows the rounding of its inversion

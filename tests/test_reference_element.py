@@ -10,7 +10,8 @@ from conftest import GOLDEN
 from pdekit_b200 import reference_element as re_
 from golden_io import load_golden
 
-CASES = {(1, 4): "adv_p1_lda", (2, 5): "burgers_p2_b", (3, 8): "burgers_p3_b"}
+CASES = {(1, 4): "adv_p1_lda", (2, 5): "burgers_p2_b", (3, 8): "burgers_p3_b",
+         (3, 6): "burgers_p3_q6_b"}
 
 
 def _match_rows(a, b, tol=1e-13):
@@ -99,3 +100,19 @@ def test_square_rules_exact(order):
         np.testing.assert_allclose(w[key(qp)], ow[key(oq)], atol=1e-14)
     with pytest.raises(ValueError):
         re_.quad_gauss(9)
+
+
+def test_p1_tet_tables_match_reference():
+    """P1 tetrahedra with the order-2 rule (4 points) and P1 triangle facets (order 3). The
+    reference tabulates the tetrahedron rule's points to about ten digits (5e-11 here)."""
+    _, a, _ = load_golden(os.path.join(GOLDEN, "euler3d_tet_p1_lda"))
+    t = re_.tet_tables(1, 2)
+    perm = _match_rows(t["qp"], a["qp"], tol=1e-10)
+    np.testing.assert_allclose(t["w"], a["w"][perm], rtol=0, atol=1e-14)
+    np.testing.assert_allclose(t["V"], a["V"][perm], rtol=0, atol=1e-10)
+    for d in range(3):
+        np.testing.assert_allclose(t["dV"][d], a[f"dV{d}"][perm], rtol=0, atol=1e-12)
+        np.testing.assert_allclose(t["dVf"][d], a[f"dVf{d}"][perm], rtol=0, atol=1e-9)
+    np.testing.assert_allclose(t["Vsf"], a["Vsf"], rtol=0, atol=1e-13)
+    fperm = _match_rows(t["fqp"], a["fqp"])
+    np.testing.assert_allclose(t["fw"], a["fw"][fperm], rtol=0, atol=1e-14)
