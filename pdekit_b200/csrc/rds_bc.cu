@@ -63,7 +63,7 @@ cudaError_t launch_weak(const HostBC &b, const BCArgs &a, cudaStream_t s)
 }
 
 // Facet types: 2D lines P1-P3 with 3-5 point Gauss rules; 3D P1 triangles with 4 points and P2
-// triangles with 12.
+// triangles with 7 or 12.
 template <int KIND, int PHYS, int D, int NEQ>
 cudaError_t dispatch_facets(const HostBC &b, const BCArgs &a, cudaStream_t s, bool *ok)
 {
@@ -91,6 +91,8 @@ cudaError_t dispatch_facets(const HostBC &b, const BCArgs &a, cudaStream_t s, bo
       return launch_weak<KIND, PHYS, D, NEQ, 6, 12, 3>(b, a, s);
     if (d.nfgeo == 3 && d.nfdof == 3 && d.nfq == 4)
       return launch_weak<KIND, PHYS, D, NEQ, 3, 4, 3>(b, a, s);
+    if (d.nfgeo == 3 && d.nfdof == 6 && d.nfq == 7)
+      return launch_weak<KIND, PHYS, D, NEQ, 6, 7, 3>(b, a, s);
   }
   *ok = false;
   return cudaSuccess;

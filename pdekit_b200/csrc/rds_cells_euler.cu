@@ -1022,9 +1022,11 @@ cudaError_t dispatch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream
   {
     if (d.shape == RDS_TETRA && d.ngeo == 4)
     {
-      // P1 with the order-2 rule (4 points), P2 with the order-5 rule (14 points)
+      // P1 with the order-2 rule (4 points), P2 with the order-4 (11) and order-5 (14) rules
       if (d.ndof == 4 && d.nq == 4 && d.nfl == 10)
         return launch_euler<PHYS, SCHEME, T, 4, 4, 10, 4, 4>(g, a, s);
+      if (d.ndof == 10 && d.nq == 11 && d.nfl == 20)
+        return launch_euler<PHYS, SCHEME, T, 10, 11, 20, 4, 4>(g, a, s);
       if (d.ndof == 10 && d.nq == 14 && d.nfl == 20)
       {
         if constexpr (sizeof(T) == 8)

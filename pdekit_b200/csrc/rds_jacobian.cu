@@ -382,6 +382,7 @@ cudaError_t dispatch_jac(const HostCellGroup &g, const CellArgs &a, double *jac,
   else
   {
     RDS_JAC(RDS_TETRA, 4, 4, 4, 10)
+    RDS_JAC(RDS_TETRA, 4, 10, 11, 20)
     RDS_JAC(RDS_TETRA, 4, 10, 14, 20)
   }
 #undef RDS_JAC

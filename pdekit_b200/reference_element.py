@@ -374,6 +374,10 @@ def lagrange_tet(p: int, pts: np.ndarray):
 _TET_RULES = {
     1: [("s4", 1.0 / 6.0)],
     2: [("s31", 1.0 / 24.0, (5.0 - np.sqrt(5.0)) / 20.0)],
+    # 11-point degree-4 rule (P. Keast, "Moderate-degree tetrahedral quadrature formulas",
+    # CMAME 55, 1986; negative centroid weight), in closed form
+    4: [("s4", -74.0 / 5625.0), ("s31", 343.0 / 45000.0, 1.0 / 14.0),
+        ("s22", 56.0 / 2250.0, (1.0 + np.sqrt(5.0 / 14.0)) / 4.0)],
     # 14-point degree-5 rule (Walkington; the rule pdekit tabulates for order 5)
     5: [("s31", 0.01224884051939366, 0.0927352503108912),
         ("s31", 0.01878132095300264, 0.3108859192633006),

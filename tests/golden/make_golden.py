@@ -153,6 +153,9 @@ CASES = {
                            EULER3D_BCS, 0.5, 3),
     "euler3d_tet_p1_b": ("euler3d", "b", 1, 2, ("box_tet", 4, 2, 2), 0.1, 70, "bump3d",
                          EULER3D_BCS, 0.5, 3),
+    # P2 tetrahedra with the order-4 rule (11 points; examples/testcases-rdm/OneraM6-RDS.cpp)
+    "euler3d_tet_p2_q4_n": ("euler3d", "n", 2, 4, ("box_tet", 3, 2, 2), 0.1, 71, "bump3d",
+                            EULER3D_BCS, 0.5, 3),
     # the smoothness sensor on bilinear quadrilaterals (detJ varies inside the cell); P1 only:
     # at p >= 2 the reference's rule of order 2p has fewer points than the cell has modes, its
     # modal mass matrix is singular and the sensor follows the rounding of its inversion

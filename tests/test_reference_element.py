@@ -116,3 +116,23 @@ def test_p1_tet_tables_match_reference():
     np.testing.assert_allclose(t["Vsf"], a["Vsf"], rtol=0, atol=1e-13)
     fperm = _match_rows(t["fqp"], a["fqp"])
     np.testing.assert_allclose(t["fw"], a["fw"][fperm], rtol=0, atol=1e-14)
+
+
+def test_p2_tet_order4_rule_matches_reference():
+    """The 11-point order-4 tetrahedron rule (negative centroid weight) against the one the
+    reference integrated the fixture with (its points tabulated to about ten digits)."""
+    _, a, _ = load_golden(os.path.join(GOLDEN, "euler3d_tet_p2_q4_n"))
+    qp, w = re_.tet_gauss(4)
+    perm = _match_rows(qp, a["qp"], tol=1e-10)
+    np.testing.assert_allclose(w, a["w"][perm], rtol=0, atol=1e-10)
+    # exact to degree 4 on the reference tetrahedron (volume 4/3): in barycentric coordinates
+    # int l1^a l2^b l3^c = a! b! c! 3! V / (a + b + c + 3)!
+    from math import factorial
+    lam = (1.0 + qp) / 2.0
+    for i in range(5):
+        for j in range(5 - i):
+            for k in range(5 - i - j):
+                got = np.sum(w * lam[:, 0] ** i * lam[:, 1] ** j * lam[:, 2] ** k)
+                ex = factorial(i) * factorial(j) * factorial(k) * 6 * (4.0 / 3.0) / \
+                    factorial(i + j + k + 3)
+                assert abs(got - ex) < 1e-14
