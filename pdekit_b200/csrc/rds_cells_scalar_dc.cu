@@ -306,9 +306,14 @@ __global__ void __launch_bounds__(128)
 // grid-stride loop over cells, then the facets of each condition), a grid barrier, phase 2 the
 // node updates, a grid barrier. The arithmetic is that of the separate kernels (dc_cell,
 // bc_weak_facet, dc_correction_node), so the results are theirs bit for bit; only the loads of
-// what other blocks wrote in the same launch (the state, the changes) go through L2. The grid
-// is at most what is resident at once (occupancy x SMs), and every barrier wait is bounded:
-// a barrier that gives up sets kFlagTimeout in the status word and the launch returns.
+// what other blocks wrote in the same launch (the state, the changes) go through L2, and what
+// stays the same within the cycle (a thread's first cell's connectivity, reference state and
+// inverse Jacobian, its first node's entry slots, dt R64, dt / V and value) is read once into
+// registers. Two forms: meshes whose items fit two per thread of one 16-CTA cluster run as a
+// single thread-block cluster (co-scheduled by the launch) with the hardware cluster barrier;
+// larger ones as a grid of at most what is resident at once (occupancy x SMs) with a barrier
+// in global memory whose waits are bounded: a wait that gives up sets kFlagTimeout in the
+// status word and the launch returns.
 
 constexpr int kClusterCtas = 16; // the cluster form's CTAs (a non-portable cluster size)
 // and threads per CTA: as many as the order's registers allow (P1 <= 102, P2 <= 128 a thread)
