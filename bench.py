@@ -501,6 +501,9 @@ def loop_rates(prob, u0, cfl, sweeps, world):
             s.iterate(cfl, 49, 0.0)
             out["mixed_kernels_ms_per_launch"] = {k: round(v[0] / v[1], 5)
                                                   for k, v in s.kernel_times().items()}
+            if any(k.startswith("dc_sweeps") for k in out["mixed_kernels_ms_per_launch"]):
+                # a fused launch runs the 23 correction sweeps of a cycle (period 24)
+                out["mixed_fused_sweeps_per_launch"] = 23
             s.kernel_timing(False)
         s.close()
     return out
@@ -578,6 +581,7 @@ def compact_config(name, args, world):
                    "d2h_bytes_per_step": int(u_host.numel() * 8 + 8 * prob.neq)},
            "loop_fp64": rates["fp64"], "mixed": rates["mixed"],
            "mixed_kernels_ms_per_launch": rates["mixed_kernels_ms_per_launch"],
+           "mixed_fused_sweeps_per_launch": rates.get("mixed_fused_sweeps_per_launch"),
            "roofline": roof, "mixed_roofline": dc_roofline(prob, rates["mixed_kernels_ms_per_launch"])}
     if not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -753,6 +757,7 @@ def run_ours(args, rank, world, local):
                            "correction sweeps between (the cell and facet changes computed from "
                            "the correction itself); rds_iterate, no stop test, CUDA events",
                       kernels_ms_per_launch=rates["mixed_kernels_ms_per_launch"],
+                      fused_sweeps_per_launch=rates.get("mixed_fused_sweeps_per_launch"),
                       roofline=dc_roofline(prob, rates["mixed_kernels_ms_per_launch"])),
         "rk3tvd": rk3,
         "time_to_drop_1e-10": drop,
