@@ -995,14 +995,19 @@ cudaError_t dispatch_euler(const HostCellGroup &g, const CellArgs &a, cudaStream
         return launch_euler<PHYS, SCHEME, T, 6, 6, 10, 3, 4>(g, a, s);
       if (d.ndof == 6 && d.nq == 7 && d.nfl == 10)
         return launch_euler<PHYS, SCHEME, T, 6, 7, 10, 3, 4>(g, a, s);
+      if (d.ndof == 10 && d.nq == 12 && d.nfl == 15)
+        return launch_euler<PHYS, SCHEME, T, 10, 12, 15, 3, 4>(g, a, s);
       if (d.ndof == 10 && d.nq == 16 && d.nfl == 15)
         return launch_euler<PHYS, SCHEME, T, 10, 16, 15, 3, 4, kBlock, 1, (sizeof(T) == 8 ? 3 : 0)>(
             g, a, s);
     }
     if (d.shape == RDS_QUAD && d.ngeo == 4)
     {
-      // P1 and P2 with the reference's 8-point rule of orders 4-5 or a 3x3 Gauss rule, P3 with
-      // the reference's 20-point rule of order 8 or a 5x5 Gauss rule
+      // P1 with the 2x2 Gauss rule (orders 2-3), P1 and P2 with the reference's 8-point rule of
+      // orders 4-5 or a 3x3 Gauss rule, P3 with the reference's 20-point rule of order 8 or a 5x5
+      // Gauss rule
+      if (d.ndof == 4 && d.nq == 4 && d.nfl == 9)
+        return launch_euler<PHYS, SCHEME, T, 4, 4, 9, 4, 4>(g, a, s);
       if (d.ndof == 4 && d.nq == 8 && d.nfl == 9)
         return launch_euler<PHYS, SCHEME, T, 4, 8, 9, 4, 4>(g, a, s);
       if (d.ndof == 4 && d.nq == 9 && d.nfl == 9)

@@ -374,6 +374,7 @@ cudaError_t dispatch_jac(const HostCellGroup &g, const CellArgs &a, double *jac,
     RDS_JAC(RDS_TRIAG, 3, 10, 16, 15)
     if constexpr (NEQ > 1)
     {
+      RDS_JAC(RDS_QUAD, 4, 4, 4, 9)
       RDS_JAC(RDS_QUAD, 4, 4, 8, 9)
       RDS_JAC(RDS_QUAD, 4, 9, 8, 16)
       RDS_JAC(RDS_QUAD, 4, 16, 20, 25)

@@ -153,6 +153,12 @@ CASES = {
                            EULER3D_BCS, 0.5, 3),
     "euler3d_tet_p1_b": ("euler3d", "b", 1, 2, ("box_tet", 4, 2, 2), 0.1, 70, "bump3d",
                          EULER3D_BCS, 0.5, 3),
+    # Euler 2D P3 triangles with the order-6 rule and P1 quadrilaterals with the order-3 rule
+    # (the 2 x 2 Gauss rule)
+    "euler2d_tri_p3_q6_b": ("euler2d", "b", 3, 6, ("channel_tri", 4, 3), 0.15, 72, "bump2d",
+                            EULER2D_BCS, 0.5, 3),
+    "euler2d_quad_p1_q3_lda": ("euler2d", "lda", 1, 3, ("channel_quad", 6, 3), 0.15, 73,
+                               "bump2d", EULER2D_BCS, 0.5, 3),
     # P2 tetrahedra with the order-4 rule (11 points; examples/testcases-rdm/OneraM6-RDS.cpp)
     "euler3d_tet_p2_q4_n": ("euler3d", "n", 2, 4, ("box_tet", 3, 2, 2), 0.1, 71, "bump3d",
                             EULER3D_BCS, 0.5, 3),
