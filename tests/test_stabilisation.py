@@ -213,3 +213,19 @@ def test_host_bonanni_tables_give_reference_values(case):
     sc = np.maximum(f / delta, 0.0)
     th = np.minimum(1.0, sc * sc * vol ** (1.0 / dim))
     assert _rel(th, a["blend_cell"]) < TOL[dim]
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_quad_sensor_table_separates_the_flagged_modes(p):
+    """R maps nodal values to the part of u on the modes the reference flags (the first 2p + 1
+    of its tensor Legendre basis): a u on the other modes gives R u = 0, a u on the flagged
+    modes gives R u = u at the points."""
+    from pdekit_b200.reference_element import _legendre_square, quad_nodes
+    t = stab_tables("quad", p, 4)
+    Tm, flags = _legendre_square(p, quad_nodes(p))
+    rng = np.random.default_rng(p)
+    c = rng.standard_normal(len(flags))
+    kept, flagged = c * ~flags, c * flags
+    assert np.abs(t["R"] @ (Tm @ kept)).max() < 1e-12
+    np.testing.assert_allclose(t["R"] @ (Tm @ flagged), t["Vn"] @ (Tm @ flagged), atol=1e-12)
+    assert flags.sum() == 2 * p + 1 and flags[:2 * p + 1].all()
