@@ -489,8 +489,10 @@ cudaError_t launch_fused_one(const HostCellGroup &g, const HostBC *const *bcs,
     cfg.blockDim             = dim3(NTC);
     cfg.attrs                = attr;
     cfg.numAttrs             = 1;
-    // whether the cluster fits, asked once per kernel (the first call usually comes during a
-    // stream capture: the queries then run in relaxed capture mode and on no stream)
+    // whether the cluster fits, asked once per kernel and process, on the device current at
+    // the first call (one device a process, as the library is used; the first call usually
+    // comes during a stream capture: the queries then run in relaxed capture mode and on no
+    // stream)
     static int fits = -1;
     if (fits < 0)
     {
